@@ -1,0 +1,239 @@
+"""CPU oracle for the DNDSR implicit residual path -- test infrastructure only.
+
+``oracle/oracle.cpp`` restates the reference's algorithms on the CPU; this
+module binds it with ctypes.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg use it, as the checker (or the timed CPU
+baseline); the GPU library in ``dndsr_b200/`` never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build():
+    """Compile oracle/oracle.cpp into oracle/liboracle.so (g++ + OpenMP)."""
+    root = os.path.dirname(_HERE)
+    subprocess.check_call(["make", "-s", "-f", os.path.join("oracle", "Makefile")], cwd=root)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "oracle.cpp")
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+class VRSettings(ctypes.Structure):
+    """Mirror of ``OrcVRSettings`` (field names follow CFV/VRSettings.hpp)."""
+    _fields_ = [
+        ("maxOrder", ctypes.c_int), ("intOrder", ctypes.c_int),
+        ("jacobiRelax", ctypes.c_double), ("SORInstead", ctypes.c_int),
+        ("anisotropicLengths", ctypes.c_int), ("scaleType", ctypes.c_int),
+        ("scaleMultiplier", ctypes.c_double), ("dirWeightScheme", ctypes.c_int),
+        ("manualDirWeights", ctypes.c_double * 4), ("geomWeightScheme", ctypes.c_int),
+        ("geomWeightBias", ctypes.c_double), ("geomWeightPower", ctypes.c_double),
+        ("geomWeightPower1", ctypes.c_double), ("geomWeightPower2", ctypes.c_double),
+        ("bcWeight", ctypes.c_double),
+    ]
+
+
+class EulerSettings(ctypes.Structure):
+    """Mirror of ``OrcEulerSettings`` (Euler/EulerEvaluatorSettings.hpp names)."""
+    _fields_ = [
+        ("nVars", ctypes.c_int), ("rsType", ctypes.c_int),
+        ("rsFixScale", ctypes.c_double), ("rsIncFScale", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("Rgas", ctypes.c_double), ("muGas", ctypes.c_double),
+        ("prGas", ctypes.c_double), ("TRef", ctypes.c_double), ("CSutherland", ctypes.c_double),
+        ("muModel", ctypes.c_int), ("ignoreVis", ctypes.c_int),
+    ]
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_L = ctypes.POINTER(ctypes.c_long)
+_I = ctypes.POINTER(ctypes.c_int)
+_V = ctypes.c_void_p
+
+
+def _declare(L):
+    L.orc_create.restype = _V
+    L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, _D, ctypes.c_long, ctypes.c_int, _L, _D,
+                             ctypes.c_long, ctypes.c_int, _L, _D, _L, _I, _D, ctypes.c_int, _L,
+                             ctypes.POINTER(VRSettings), ctypes.POINTER(EulerSettings)]
+    L.orc_destroy.argtypes = [_V]
+    L.orc_construct.restype = ctypes.c_int
+    L.orc_construct.argtypes = [_V, _D, ctypes.c_int]
+    L.orc_sizes.argtypes = [_V, _L]
+    L.orc_get.restype = ctypes.c_long
+    L.orc_get.argtypes = [_V, ctypes.c_char_p, _D]
+    L.orc_set_delta_lambda.argtypes = [_V, _D]
+    L.orc_init_field.argtypes = [_V, ctypes.c_int, ctypes.c_double, _D]
+    L.orc_vr_iter.argtypes = [_V, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+    L.orc_eval_dt.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D]
+    L.orc_eval_rhs.argtypes = [_V, _D, _D, _D, _D]
+    L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
+    L.orc_update_sgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
+    L.orc_lusgs_matvec.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D]
+    L.orc_riemann.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_double, _D, _D]
+    L.orc_viscous_flux.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int, _D]
+    L.orc_cell_point_values.argtypes = [_V, _D, _D, _D]
+    L.orc_cell_quad_weights.argtypes = [_V, _D]
+
+
+def _p(a, t=_D):
+    return a.ctypes.data_as(t)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# Riemann solver codes: Euler/Gas.hpp:61-96
+RS = dict(Roe=1, HLLC=2, HLLEP=3, HLLEP_V1=21, Roe_M1=11, Roe_M2=12, Roe_M3=13, Roe_M4=14,
+          Roe_M5=15, Roe_M6=16, Roe_M7=17, Roe_M8=18)
+
+
+def riemann(rs, UL, UR, n, gamma=1.4, ULm=None, URm=None, dLambda=0.0, fixScale=0.0, incFScale=0.0):
+    """One call of the reference's InviscidFlux_IdealGas_Dispatcher (Gas.hpp:1434)."""
+    UL, UR, n = _f64(UL), _f64(UR), _f64(n)
+    ULm = UL if ULm is None else _f64(ULm)
+    URm = UR if URm is None else _f64(URm)
+    F = np.zeros(5)
+    lam = np.zeros(3)
+    code = RS[rs] if isinstance(rs, str) else int(rs)
+    lib().orc_riemann(code, _p(UL), _p(UR), _p(ULm), _p(URm), _p(n), gamma, dLambda, fixScale, incFScale, _p(F), _p(lam))
+    return F, lam
+
+
+def viscous_flux(U, gradU, n, gamma, mu, k, Cp, adiabatic=False):
+    U, gradU, n = _f64(U), _f64(gradU), _f64(n)
+    F = np.zeros(5)
+    lib().orc_viscous_flux(_p(U), _p(gradU), _p(n), gamma, mu, k, Cp, int(adiabatic), _p(F))
+    return F
+
+
+class Oracle:
+    """One mesh + VR + evaluator instance of the CPU restatement."""
+
+    def __init__(self, mesh, vr: dict, euler: dict):
+        self.mesh = mesh
+        L = lib()
+        a = mesh.arrays()
+        self._keep = a
+        vs = VRSettings()
+        for k, v in vr.items():
+            if k == "manualDirWeights":
+                for i, x in enumerate(v):
+                    vs.manualDirWeights[i] = x
+            else:
+                setattr(vs, k, v)
+        es = EulerSettings()
+        for k, v in euler.items():
+            setattr(es, k, v)
+        self.vs, self.es = vs, es
+        ctype = {1: 1, 2: 2, 3: 3, 4: 4}[mesh.cell_type]
+        nf = mesh.cell2face.shape[1]
+        self.nf = nf
+        self.h = L.orc_create(mesh.dim, ctype, mesh.face_type, mesh.n_node, _p(a["coords"]), mesh.n_cell,
+                              a["cell2node"].shape[1], _p(a["cell2node"], _L), _p(a["cell_shift"]), mesh.n_face,
+                              a["face2node"].shape[1], _p(a["face2node"], _L), _p(a["face_shift"]), _p(a["face2cell"], _L),
+                              _p(a["face_zone"], _I), _p(a["face_pshift"]), nf, _p(a["cell2face"], _L),
+                              ctypes.byref(vs), ctypes.byref(es))
+        self.nv = es.nVars
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def construct(self, bc_dir_weight=None):
+        if bc_dir_weight is None:
+            bad = lib().orc_construct(self.h, None, 0)
+        else:
+            w = _f64(bc_dir_weight)
+            bad = lib().orc_construct(self.h, _p(w), w.shape[0])
+        out = np.zeros(4, dtype=np.int64)
+        lib().orc_sizes(self.h, _p(out, _L))
+        self.NDOF, self.R, self.nGf, self.nGc = [int(x) for x in out]
+        return bad
+
+    def get(self, name):
+        n = lib().orc_get(self.h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        lib().orc_get(self.h, name.encode(), _p(out))
+        return out
+
+    def init_field(self, kind, chi=5.0):
+        u = np.zeros((self.mesh.n_cell, self.nv))
+        lib().orc_init_field(self.h, kind, chi, _p(u))
+        return u
+
+    def vr_iter(self, uRec, u, recordInc=False, uRecIsZero=False):
+        uRec, u = _f64(uRec), _f64(u)
+        out = np.zeros_like(uRec)
+        lib().orc_vr_iter(self.h, _p(uRec), _p(out), _p(u), int(recordInc), int(uRecIsZero))
+        return out
+
+    def eval_dt(self, u, CFL, MaxDt=1e100, useLocalDt=True):
+        u = _f64(u)
+        dt = np.zeros(self.mesh.n_cell)
+        mn = np.zeros(1)
+        lib().orc_eval_dt(self.h, _p(u), CFL, MaxDt, int(useLocalDt), _p(dt), _p(mn))
+        return dt, float(mn[0])
+
+    def set_delta_lambda(self, dl):
+        dl = _f64(dl)
+        lib().orc_set_delta_lambda(self.h, _p(dl))
+
+    def eval_rhs(self, u, uRec, want_face_flux=False):
+        u, uRec = _f64(u), _f64(uRec)
+        rhs = np.zeros_like(u)
+        ff = np.zeros((self.mesh.n_face, self.nv)) if want_face_flux else None
+        lib().orc_eval_rhs(self.h, _p(u), _p(uRec), _p(rhs), _p(ff) if ff is not None else None)
+        return (rhs, ff) if want_face_flux else rhs
+
+    def lusgs_init(self, dTau, dt, alphaDiag):
+        dTau = _f64(dTau)
+        jd = np.zeros(self.mesh.n_cell)
+        lib().orc_lusgs_init(self.h, _p(dTau), dt, alphaDiag, _p(jd))
+        return jd
+
+    def update_sgs(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False):
+        rhs, u, uInc, jdiag = _f64(rhs), _f64(u), _f64(uInc), _f64(jdiag)
+        out = np.array(uIncNew, dtype=np.float64, copy=True, order="C")
+        s = np.zeros(self.nv)
+        lib().orc_update_sgs(self.h, alphaDiag, _p(rhs), _p(u), _p(uInc), _p(out), _p(jdiag), int(forward), int(gsUpdate),
+                             int(uIncIsZero), _p(s))
+        return out, s
+
+    def lusgs_matvec(self, alphaDiag, u, uInc, jdiag):
+        u, uInc, jdiag = _f64(u), _f64(uInc), _f64(jdiag)
+        out = np.zeros_like(uInc)
+        lib().orc_lusgs_matvec(self.h, alphaDiag, _p(u), _p(uInc), _p(jdiag), _p(out))
+        return out
+
+    def cell_point_values(self, u, uRec):
+        u, uRec = _f64(u), _f64(uRec)
+        out = np.zeros((self.mesh.n_cell, self.nGc, self.nv))
+        lib().orc_cell_point_values(self.h, _p(u), _p(uRec), _p(out))
+        return out
+
+    def cell_quad_weights(self):
+        w = np.zeros(self.nGc)
+        lib().orc_cell_quad_weights(self.h, _p(w))
+        return w

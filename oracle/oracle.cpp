@@ -1,0 +1,1870 @@
+// CPU oracle for the DNDSR implicit residual path -- TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, in plain C++17 + OpenMP, the reference algorithms the
+// GPU library implements, so that tests/, __graft_entry__.smoke() and the
+// bench's CPU-baseline leg can check and time them.  Nothing in the product
+// (dndsr_b200/) links, loads or calls this code.
+//
+// Parity pin: the reference cannot be compiled here (it needs Eigen, Boost,
+// CGAL, HDF5, CGNS, Metis and MPI), so this restatement is pinned to the
+// reference's own golden vectors that need no mesh file:
+//   * Riemann fluxes  test/cpp/Euler/test_RiemannSolvers.cpp:242-294
+//   * flux consistency/symmetry cases of the same file
+//   * VR exactness / convergence properties (test_Reconstruction.cpp:454-506)
+// Each function below cites the reference file:line it follows (paths are
+// relative to the reference project root).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace orc
+{
+using real = double;
+constexpr real verySmallReal = 1e-200; // DNDS/Defines.hpp:199
+constexpr real smallReal = 1e-10;      // DNDS/Defines.hpp:201
+constexpr real veryLargeReal = 3e200;  // DNDS/Defines.hpp:195
+constexpr real pi = 3.14159265358979323846;
+constexpr int INT_ORDER_MAX = 6; // Geom/Quadratures/QuadratureBase.hpp:70
+
+enum Elem
+{
+    LINE2 = 0,
+    TRI3 = 1,
+    QUAD4 = 2,
+    TET4 = 3,
+    HEX8 = 4
+};
+
+static inline real sqr(real x) { return x * x; }
+static inline real signTol(real a, real tol) { return a > tol ? 1 : (a < -tol ? -1 : 0); } // Defines.hpp:543
+static inline real signP(real a) { return a >= 0 ? 1 : -1; }                              // Defines.hpp:549
+
+// ---------------------------------------------------------------------------
+// Quadrature: Geom/QuadratureHub.hpp:39-140 (scheme choice), Quadratures/*.hpp
+// (tabulated points as the reference prints them).
+// ---------------------------------------------------------------------------
+static const real GL1[2][1] = {{0}, {2}};
+static const real GL2[2][2] = {{-0.577350269189626, 0.577350269189626}, {1, 1}};
+static const real GL3[2][3] = {{-0.774596669241483, 0, 0.774596669241483},
+                               {0.555555555555555, 0.888888888888889, 0.555555555555555}};
+static const real GL4[2][4] = {{-0.861136311594053, -0.339981043584856, 0.339981043584856, 0.861136311594053},
+                               {0.347854845137454, 0.652145154862546, 0.652145154862546, 0.347854845137454}};
+
+static const real Tri1[3][1] = {{1. / 3.}, {1. / 3.}, {1. / 2.}};
+static const real Tri3[3][3] = {{2. / 3., 1. / 6., 1. / 6.}, {1. / 6., 2. / 3., 1. / 6.}, {1. / 6., 1. / 6., 1. / 6.}};
+static const real Tri6[3][6] = {{0.09157621350977102, 0.8168475729804585, 0.09157621350977052, 0.445948490915965, 0.10810301816807, 0.445948490915965},
+                                {0.09157621350977102, 0.09157621350977052, 0.8168475729804585, 0.445948490915965, 0.445948490915965, 0.10810301816807},
+                                {0.054975871827661, 0.054975871827661, 0.054975871827661, 0.1116907948390057, 0.1116907948390057, 0.1116907948390057}};
+static const real Tri7[3][7] = {{0.3333333333333335, 0.470142064105115, 0.05971587178977, 0.470142064105115, 0.1012865073234565, 0.7974269853530875, 0.1012865073234565},
+                                {0.3333333333333335, 0.470142064105115, 0.470142064105115, 0.05971587178977, 0.1012865073234565, 0.1012865073234565, 0.7974269853530875},
+                                {0.1125, 0.066197076394253, 0.066197076394253, 0.066197076394253, 0.0629695902724135, 0.0629695902724135, 0.0629695902724135}};
+static const real Tri12[3][12] = {{0.2492867451709105, 0.501426509658179, 0.2492867451709105, 0.063089014491502, 0.8738219710169954, 0.063089014491502,
+                                   0.3103524510337845, 0.05314504984481699, 0.6365024991213986, 0.05314504984481699, 0.6365024991213986, 0.3103524510337845},
+                                  {0.2492867451709105, 0.2492867451709105, 0.501426509658179, 0.063089014491502, 0.063089014491502, 0.8738219710169954,
+                                   0.05314504984481699, 0.3103524510337845, 0.05314504984481699, 0.6365024991213986, 0.3103524510337845, 0.6365024991213986},
+                                  {0.05839313786318975, 0.05839313786318975, 0.05839313786318975, 0.0254224531851035, 0.0254224531851035, 0.0254224531851035,
+                                   0.04142553780918675, 0.04142553780918675, 0.04142553780918675, 0.04142553780918675, 0.04142553780918675, 0.04142553780918675}};
+static const real Tet1[4][1] = {{0.25}, {0.25}, {0.25}, {0.1666666666666667}};
+static const real Tet4[4][4] = {{0.1381966011250105, 0.1381966011250105, 0.5854101966249685, 0.1381966011250105},
+                                {0.1381966011250105, 0.5854101966249684, 0.1381966011250105, 0.1381966011250105},
+                                {0.5854101966249684, 0.1381966011250105, 0.1381966011250105, 0.1381966011250105},
+                                {0.04166666666666666, 0.04166666666666666, 0.04166666666666666, 0.04166666666666666}};
+static const real Tet8[4][8] = {{0.1069940147705369, 0.1069940147705369, 0.6790179556883893, 0.1069940147705369, 0.3280585716625127, 0.3280585716625127, 0.01582428501246191, 0.3280585716625127},
+                                {0.1069940147705369, 0.6790179556883893, 0.1069940147705369, 0.1069940147705369, 0.3280585716625127, 0.01582428501246191, 0.3280585716625127, 0.3280585716625127},
+                                {0.6790179556883893, 0.1069940147705369, 0.1069940147705369, 0.1069940147705369, 0.01582428501246191, 0.3280585716625127, 0.3280585716625127, 0.3280585716625127},
+                                {0.01859314997209119, 0.01859314997209119, 0.01859314997209119, 0.01859314997209119, 0.02307351669457548, 0.02307351669457548, 0.02307351669457548, 0.02307351669457548}};
+static const real Tet14[4][14] = {{0.09273525031089125, 0.09273525031089125, 0.7217942490673263, 0.09273525031089125, 0.3108859192633008, 0.3108859192633008, 0.06734224221009777,
+                                   0.3108859192633008, 0.04550370412564952, 0.4544962958743505, 0.04550370412564952, 0.04550370412564952, 0.4544962958743505, 0.4544962958743505},
+                                  {0.09273525031089125, 0.7217942490673263, 0.09273525031089125, 0.09273525031089125, 0.3108859192633008, 0.06734224221009777, 0.3108859192633008,
+                                   0.3108859192633008, 0.4544962958743505, 0.04550370412564952, 0.04550370412564952, 0.4544962958743505, 0.04550370412564952, 0.4544962958743505},
+                                  {0.7217942490673263, 0.09273525031089125, 0.09273525031089125, 0.09273525031089125, 0.06734224221009777, 0.3108859192633008, 0.3108859192633008,
+                                   0.3108859192633008, 0.4544962958743505, 0.4544962958743505, 0.4544962958743505, 0.04550370412564952, 0.04550370412564952, 0.04550370412564952},
+                                  {0.01224884051939367, 0.01224884051939367, 0.01224884051939367, 0.01224884051939367, 0.01878132095300264, 0.01878132095300264, 0.01878132095300264,
+                                   0.01878132095300264, 0.0070910034628469, 0.0070910034628469, 0.0070910034628469, 0.0070910034628469, 0.0070910034628469, 0.0070910034628469}};
+static const real Tet24[4][24] = {{0.2146028712591523, 0.2146028712591523, 0.3561913862225431, 0.2146028712591523, 0.3223378901422754, 0.3223378901422754, 0.0329863295731736, 0.3223378901422754,
+                                   0.04067395853461131, 0.04067395853461131, 0.8779781243961661, 0.04067395853461131, 0.6030056647916491, 0.6030056647916491, 0.06366100187501755, 0.2696723314583158,
+                                   0.06366100187501755, 0.06366100187501755, 0.2696723314583158, 0.06366100187501755, 0.06366100187501755, 0.06366100187501755, 0.2696723314583158, 0.6030056647916491},
+                                  {0.2146028712591523, 0.3561913862225431, 0.2146028712591523, 0.2146028712591523, 0.3223378901422754, 0.0329863295731736, 0.3223378901422754, 0.3223378901422754,
+                                   0.04067395853461131, 0.8779781243961661, 0.04067395853461131, 0.04067395853461131, 0.06366100187501755, 0.06366100187501755, 0.06366100187501755, 0.6030056647916491,
+                                   0.2696723314583158, 0.6030056647916491, 0.06366100187501755, 0.2696723314583158, 0.06366100187501755, 0.6030056647916491, 0.06366100187501755, 0.2696723314583158},
+                                  {0.3561913862225431, 0.2146028712591523, 0.2146028712591523, 0.2146028712591523, 0.0329863295731736, 0.3223378901422754, 0.3223378901422754, 0.3223378901422754,
+                                   0.8779781243961661, 0.04067395853461131, 0.04067395853461131, 0.04067395853461131, 0.2696723314583158, 0.06366100187501755, 0.6030056647916491, 0.06366100187501755,
+                                   0.6030056647916491, 0.06366100187501755, 0.6030056647916491, 0.06366100187501755, 0.2696723314583158, 0.2696723314583158, 0.06366100187501755, 0.06366100187501755},
+                                  {0.006653791709694545, 0.006653791709694545, 0.006653791709694545, 0.006653791709694545, 0.009226196923942479, 0.009226196923942479, 0.009226196923942479,
+                                   0.009226196923942479, 0.001679535175886773, 0.001679535175886773, 0.001679535175886773, 0.001679535175886773, 0.008035714285714285, 0.008035714285714285,
+                                   0.008035714285714285, 0.008035714285714285, 0.008035714285714285, 0.008035714285714285, 0.008035714285714285, 0.008035714285714285, 0.008035714285714285,
+                                   0.008035714285714285, 0.008035714285714285, 0.008035714285714285}};
+
+static int glSize(int order)
+{
+    if (order <= 1)
+        return 1;
+    if (order <= 3)
+        return 2;
+    if (order <= 5)
+        return 3;
+    return 4;
+}
+
+static const real *glData(int n, int row)
+{
+    switch (n)
+    {
+    case 1:
+        return GL1[row];
+    case 2:
+        return GL2[row];
+    case 3:
+        return GL3[row];
+    default:
+        return GL4[row];
+    }
+}
+
+// QuadratureHub.hpp:39-140
+static int quadNPoints(int elem, int order)
+{
+    switch (elem)
+    {
+    case LINE2:
+        return glSize(order);
+    case QUAD4:
+        return glSize(order) * glSize(order);
+    case HEX8:
+        return glSize(order) * glSize(order) * glSize(order);
+    case TRI3:
+        return order <= 1 ? 1 : order == 2 ? 3 : order <= 4 ? 6 : order == 5 ? 7 : 12;
+    case TET4:
+        return order <= 1 ? 1 : order == 2 ? 4 : order == 3 ? 8 : order <= 5 ? 14 : 24;
+    }
+    return 0;
+}
+
+// QuadratureHub.hpp:188-380
+static void quadPoint(int elem, int order, int iG, real p[3], real &w)
+{
+    p[0] = p[1] = p[2] = 0;
+    if (elem == LINE2 || elem == QUAD4 || elem == HEX8)
+    {
+        int n = glSize(order);
+        const real *x = glData(n, 0), *wt = glData(n, 1);
+        if (elem == LINE2)
+        {
+            p[0] = x[iG];
+            w = wt[iG];
+        }
+        else if (elem == QUAD4)
+        {
+            int i = iG % n, j = iG / n;
+            p[0] = x[i], p[1] = x[j];
+            w = wt[i] * wt[j];
+        }
+        else
+        {
+            int i = iG % n, j = (iG / n) % n, k = iG / (n * n);
+            p[0] = x[i], p[1] = x[j], p[2] = x[k];
+            w = wt[i] * wt[j] * wt[k];
+        }
+        return;
+    }
+    int np = quadNPoints(elem, order);
+    if (elem == TRI3)
+    {
+        const real *t = nullptr;
+        switch (np)
+        {
+        case 1:
+            p[0] = Tri1[0][iG], p[1] = Tri1[1][iG], w = Tri1[2][iG];
+            return;
+        case 3:
+            p[0] = Tri3[0][iG], p[1] = Tri3[1][iG], w = Tri3[2][iG];
+            return;
+        case 6:
+            p[0] = Tri6[0][iG], p[1] = Tri6[1][iG], w = Tri6[2][iG];
+            return;
+        case 7:
+            p[0] = Tri7[0][iG], p[1] = Tri7[1][iG], w = Tri7[2][iG];
+            return;
+        default:
+            p[0] = Tri12[0][iG], p[1] = Tri12[1][iG], w = Tri12[2][iG];
+            (void)t;
+            return;
+        }
+    }
+    switch (np)
+    {
+    case 1:
+        p[0] = Tet1[0][iG], p[1] = Tet1[1][iG], p[2] = Tet1[2][iG], w = Tet1[3][iG];
+        return;
+    case 4:
+        p[0] = Tet4[0][iG], p[1] = Tet4[1][iG], p[2] = Tet4[2][iG], w = Tet4[3][iG];
+        return;
+    case 8:
+        p[0] = Tet8[0][iG], p[1] = Tet8[1][iG], p[2] = Tet8[2][iG], w = Tet8[3][iG];
+        return;
+    case 14:
+        p[0] = Tet14[0][iG], p[1] = Tet14[1][iG], p[2] = Tet14[2][iG], w = Tet14[3][iG];
+        return;
+    default:
+        p[0] = Tet24[0][iG], p[1] = Tet24[1][iG], p[2] = Tet24[2][iG], w = Tet24[3][iG];
+        return;
+    }
+}
+
+static int elemNNode(int elem)
+{
+    static const int n[] = {2, 3, 4, 4, 8};
+    return n[elem];
+}
+
+// Shape functions N and dN/dxi (Geom/Elements/{Line2,Tri3,Quad4,Tet4,Hex8}.hpp)
+static void shapeD01(int elem, const real p[3], real N[8], real dN[3][8])
+{
+    real xi = p[0], et = p[1], zt = p[2];
+    for (int d = 0; d < 3; d++)
+        for (int i = 0; i < 8; i++)
+            dN[d][i] = 0;
+    switch (elem)
+    {
+    case LINE2:
+        N[0] = 0.5 - 0.5 * xi, N[1] = 0.5 * xi + 0.5;
+        dN[0][0] = -0.5, dN[0][1] = 0.5;
+        break;
+    case TRI3:
+        N[0] = 1 - xi - et, N[1] = xi, N[2] = et;
+        dN[0][0] = -1, dN[0][1] = 1;
+        dN[1][0] = -1, dN[1][2] = 1;
+        break;
+    case QUAD4:
+    {
+        real t1 = 0.25 * et - 0.25, t3 = 0.25 * et + 0.25;
+        N[0] = (xi - 1) * t1, N[1] = -t1 * (xi + 1), N[2] = (xi + 1) * t3, N[3] = -(xi - 1) * t3;
+        real a = 0.25 * xi - 0.25, b = 0.25 * xi + 0.25;
+        dN[0][0] = t1, dN[0][1] = -t1, dN[0][2] = t3, dN[0][3] = -t3;
+        dN[1][0] = a, dN[1][1] = -b, dN[1][2] = b, dN[1][3] = -a;
+        break;
+    }
+    case TET4:
+        N[0] = 1 - xi - et - zt, N[1] = xi, N[2] = et, N[3] = zt;
+        dN[0][0] = -1, dN[0][1] = 1;
+        dN[1][0] = -1, dN[1][2] = 1;
+        dN[2][0] = -1, dN[2][3] = 1;
+        break;
+    case HEX8:
+    {
+        static const int s[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}, {-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1}};
+        for (int i = 0; i < 8; i++)
+        {
+            real a = 1 + s[i][0] * xi, b = 1 + s[i][1] * et, c = 1 + s[i][2] * zt;
+            N[i] = 0.125 * a * b * c;
+            dN[0][i] = 0.125 * s[i][0] * b * c;
+            dN[1][i] = 0.125 * a * s[i][1] * c;
+            dN[2][i] = 0.125 * a * b * s[i][2];
+        }
+        break;
+    }
+    }
+}
+
+struct PointGeo
+{
+    real x[3];
+    real J[3][3]; // J[r][c] = d x_r / d xi_c
+};
+
+static PointGeo pointGeo(int elem, const real *coords /*nn x 3*/, const real p[3])
+{
+    real N[8], dN[3][8];
+    shapeD01(elem, p, N, dN);
+    PointGeo g{};
+    int nn = elemNNode(elem);
+    for (int r = 0; r < 3; r++)
+    {
+        g.x[r] = 0;
+        for (int i = 0; i < nn; i++)
+            g.x[r] += coords[i * 3 + r] * N[i];
+        for (int c = 0; c < 3; c++)
+        {
+            g.J[r][c] = 0;
+            for (int i = 0; i < nn; i++)
+                g.J[r][c] += coords[i * 3 + r] * dN[c][i];
+        }
+    }
+    return g;
+}
+
+static void cross(const real a[3], const real b[3], real c[3])
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+static real norm3(const real a[3]) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+static real dot3(const real a[3], const real b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// Geom/Quadrature.hpp:480-490
+static real cellJacDet(int dim, const PointGeo &g)
+{
+    if (dim == 2)
+    {
+        real a[3] = {g.J[0][0], g.J[1][0], g.J[2][0]}, b[3] = {g.J[0][1], g.J[1][1], g.J[2][1]}, c[3];
+        cross(a, b, c);
+        return norm3(c);
+    }
+    const auto &J = g.J;
+    return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+
+// Geom/Quadrature.hpp:500-511 and Geom/Geometric.hpp:113-128
+static real faceJDetNorm(int dim, const PointGeo &g, real n[3])
+{
+    real a[3] = {g.J[0][0], g.J[1][0], g.J[2][0]};
+    if (dim == 2)
+    {
+        n[0] = a[1], n[1] = -a[0], n[2] = 0;
+        return norm3(a);
+    }
+    real b[3] = {g.J[0][1], g.J[1][1], g.J[2][1]};
+    cross(a, b, n);
+    return norm3(n);
+}
+
+// ---------------------------------------------------------------------------
+// Polynomial basis: Geom/BaseFunction.hpp:55-79 (3D order list), :96-107 (2D),
+// :239-279 (factorials/comb counts), :285-700 (FPolynomialFill2D/3D)
+// ---------------------------------------------------------------------------
+static const int dOrder3[20][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1},
+                                   {3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0}, {1, 2, 0}, {0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {2, 0, 1}, {1, 1, 1}};
+static const int dOrder2[10][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {2, 0, 0}, {1, 1, 0}, {0, 2, 0}, {3, 0, 0}, {2, 1, 0}, {1, 2, 0}, {0, 3, 0}};
+static const int dFact[4][4] = {{1, 0, 0, 0}, {1, 1, 0, 0}, {1, 2, 2, 0}, {1, 3, 6, 6}};
+static const int nComb2[10] = {1, 1, 1, 1, 2, 1, 1, 3, 3, 1};
+static const int nComb3[20] = {1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
+static const int factorials[10] = {1, 1, 2, 6, 24, 120, 720, 5040, 40320, 362880};
+
+static real iPow(int p, real x)
+{
+    switch (p)
+    {
+    case 0:
+        return 1.;
+    case 1:
+        return x;
+    case 2:
+        return x * x;
+    case 3:
+        return x * x * x;
+    }
+    return 1e300;
+}
+
+static int nDofOf(int dim, int order)
+{
+    static const int n2[] = {1, 3, 6, 10}, n3[] = {1, 4, 10, 20};
+    return dim == 2 ? n2[order] : n3[order];
+}
+
+// fills T[rows][cols] (row-major, cols = NDOF)
+static void polyFill(int dim, real *T, real x, real y, real z, real lx, real ly, real lz, int rows, int cols)
+{
+    for (int idiff = 0; idiff < rows; idiff++)
+        for (int ib = 0; ib < cols; ib++)
+        {
+            const int *pb = dim == 2 ? dOrder2[ib] : dOrder3[ib];
+            const int *pd = dim == 2 ? dOrder2[idiff] : dOrder3[idiff];
+            int c = dFact[pb[0]][pd[0]] * dFact[pb[1]][pd[1]] * dFact[pb[2]][pd[2]];
+            real v = c ? c * iPow(pb[0] - pd[0], x) * iPow(pb[1] - pd[1], y) * iPow(pb[2] - pd[2], z) : 0.;
+            real l = iPow(pd[0], lx) * iPow(pd[1], ly) * iPow(pd[2], dim == 2 ? 1.0 : lz);
+            T[idiff * cols + ib] = v / l;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Gas thermodynamics and Riemann solvers: Euler/Gas.hpp, DNDS/IdealGasPhysics.hpp
+// Physical dimension is always 3 (models NS / NS_3D / NS_SA / NS_SA_3D).
+// ---------------------------------------------------------------------------
+constexpr int D = 3;
+
+// IdealGasPhysics.hpp:38-44
+static void idealGasThermal(real E, real rho, real vSqr, real gamma, real &p, real &asqr, real &H)
+{
+    p = (gamma - 1) * (E - rho * 0.5 * vSqr);
+    asqr = gamma * p / rho;
+    H = (E + p) / rho;
+}
+
+struct RoePre
+{
+    real veloLm[3], veloRm[3], asqrLm, asqrRm, pLm, pRm, HLm, HRm, vsqrLm, vsqrRm;
+    real veloRoe[3], sqrtRhoLm, sqrtRhoRm, vsqrRoe, HRoe, asqrRoe, rhoRoe, aRoe;
+};
+
+// Gas.hpp:229-259
+static RoePre roePreamble(const real *ULm, const real *URm, real gamma)
+{
+    RoePre r{};
+    for (int d = 0; d < 3; d++)
+        r.veloLm[d] = ULm[1 + d] / ULm[0], r.veloRm[d] = URm[1 + d] / URm[0];
+    r.vsqrLm = dot3(r.veloLm, r.veloLm);
+    r.vsqrRm = dot3(r.veloRm, r.veloRm);
+    idealGasThermal(ULm[4], ULm[0], r.vsqrLm, gamma, r.pLm, r.asqrLm, r.HLm);
+    idealGasThermal(URm[4], URm[0], r.vsqrRm, gamma, r.pRm, r.asqrRm, r.HRm);
+    r.sqrtRhoLm = std::sqrt(ULm[0]);
+    r.sqrtRhoRm = std::sqrt(URm[0]);
+    for (int d = 0; d < 3; d++)
+        r.veloRoe[d] = (r.sqrtRhoLm * r.veloLm[d] + r.sqrtRhoRm * r.veloRm[d]) / (r.sqrtRhoLm + r.sqrtRhoRm);
+    r.vsqrRoe = dot3(r.veloRoe, r.veloRoe);
+    r.HRoe = (r.sqrtRhoLm * r.HLm + r.sqrtRhoRm * r.HRm) / (r.sqrtRhoLm + r.sqrtRhoRm);
+    r.asqrRoe = (gamma - 1) * (r.HRoe - 0.5 * r.vsqrRoe);
+    r.rhoRoe = r.sqrtRhoLm * r.sqrtRhoRm;
+    r.aRoe = std::sqrt(r.asqrRoe);
+    return r;
+}
+
+// Gas.hpp:390-397 GasInviscidFlux_XY
+static void inviscidFluxXY(const real *U, const real velo[3], const real vg[3], const real n[3], real p, real F[5])
+{
+    real vrel[3] = {velo[0] - vg[0], velo[1] - vg[1], velo[2] - vg[2]};
+    real vn = dot3(vrel, n);
+    for (int i = 0; i < 5; i++)
+        F[i] = U[i] * vn;
+    for (int d = 0; d < 3; d++)
+        F[1 + d] += p * n[d];
+    F[4] += dot3(velo, n) * p;
+}
+
+// Gas.hpp:878-1007 Roe_EntropyFixer
+static void roeEntropyFix(int eigScheme, real aL, real aR, real aAve, real uL, real uR, real uAve, real VL, real VR, real VAve,
+                          real dLambda, real fixScale, real incFScale, real &lam0, real &lam123, real &lam4)
+{
+    const real scaleHartenYee = 0.05 * fixScale, scaleLD = 0.2 * fixScale, scaleHFix = 0.25 * fixScale;
+    const real incFScaleA = 1.0;
+    (void)VL, (void)VR;
+    if (eigScheme == 0)
+    {
+        auto Flim = [=](real v, real lam, real lamL, real lamR)
+        {
+            const real thresH = std::max({0., lam - lamL, lamR - lam}) * scaleHartenYee;
+            if (v < thresH)
+                return (sqr(v) / thresH + thresH) * 0.5;
+            return v;
+        };
+        lam0 = Flim(lam0 * incFScaleA, uAve - aAve, uL - aL, uR - aR);
+        lam123 = Flim(lam123 * incFScale, uAve, uL, uR);
+        lam4 = Flim(lam4 * incFScaleA, uAve + aAve, uL + aL, uR + aR);
+    }
+    else if (eigScheme == 1)
+    {
+        const real aLm = aL * incFScaleA, aRm = aR * incFScaleA;
+        const real uLm = signTol(uL, aLm * smallReal) * std::max(std::abs(uL) * incFScale, aLm * scaleLD);
+        const real uRm = signTol(uR, aRm * smallReal) * std::max(std::abs(uR) * incFScale, aRm * scaleLD);
+        lam0 = std::max(std::abs(uLm - aLm), std::abs(uRm - aRm));
+        lam123 = std::max(std::abs(uLm), std::abs(uRm));
+        lam4 = std::max(std::abs(uLm + aLm), std::abs(uRm + aRm));
+    }
+    else if (eigScheme == 3)
+    {
+        const real LDthreshold = std::abs(uAve) / scaleLD;
+        const real aRoeStar = std::min(LDthreshold, aAve * incFScaleA);
+        lam0 = std::abs(uAve * incFScale - aRoeStar);
+        lam4 = std::abs(uAve * incFScale + aRoeStar);
+    }
+    else if (eigScheme == 4)
+    {
+        const real uStar = signTol(uAve, aAve * smallReal) * std::max(aAve * scaleLD, std::abs(uAve) * incFScale);
+        lam0 = std::abs(uStar - aAve * incFScaleA);
+        lam123 = std::abs(uStar);
+        lam4 = std::abs(uStar + aAve * incFScaleA);
+    }
+    else if (eigScheme == 5)
+    {
+        const real vL = uL * incFScale, vR = uR * incFScale;
+        const real aLm = std::min(aL * incFScaleA, std::abs(vL) / scaleLD);
+        const real aRm = std::min(aR * incFScaleA, std::abs(vR) / scaleLD);
+        lam0 = std::max(std::abs(vL - aLm), std::abs(vR - aRm));
+        lam123 = std::max(std::abs(vL), std::abs(vR));
+        lam4 = std::max(std::abs(vL + aLm), std::abs(vR + aRm));
+    }
+    else if (eigScheme == 6)
+    {
+        lam0 = std::max(std::abs(uAve * incFScale - aAve * incFScaleA), dLambda * scaleHFix);
+        lam4 = std::max(std::abs(uAve * incFScale + aAve * incFScaleA), dLambda * scaleHFix);
+        lam123 = std::max(std::abs(uAve * incFScale), dLambda * scaleHFix);
+    }
+    else if (eigScheme == 7 || eigScheme == 8)
+    {
+        if (eigScheme == 7)
+        {
+            lam0 *= std::abs(uAve * incFScale - aAve * incFScaleA);
+            lam4 *= std::abs(uAve * incFScale + aAve * incFScaleA);
+            lam123 *= std::abs(uAve * incFScale);
+        }
+        else
+        {
+            lam0 = std::max(std::abs(uAve * incFScale - aAve * incFScaleA), dLambda * scaleHFix);
+            lam4 = std::max(std::abs(uAve * incFScale + aAve * incFScaleA), dLambda * scaleHFix);
+            lam123 = std::max(std::abs(uAve * incFScale), dLambda * scaleHFix);
+        }
+        const real th = scaleHartenYee * (VAve + aAve), thS = sqr(th);
+        if (lam0 < th)
+            lam0 = (sqr(lam0) + thS) / (2 * th);
+        if (lam4 < th)
+            lam4 = (sqr(lam4) + thS) / (2 * th);
+        if (lam123 < th)
+            lam123 = (sqr(lam123) + thS) / (2 * th);
+    }
+}
+
+// Gas.hpp:1038-1126 RoeFlux_IdealGas_HartenYee
+static void roeFlux(int eigScheme, const real *UL, const real *UR, const real *ULm, const real *URm, const real vg[3], const real n[3],
+                    real gamma, real F[5], real dLambda, real fixScale, real incFScale, real &lam0, real &lam123, real &lam4)
+{
+    real veloL[3], veloR[3];
+    for (int d = 0; d < 3; d++)
+        veloL[d] = UL[1 + d] / UL[0], veloR[d] = UR[1 + d] / UR[0];
+    real asqrL, asqrR, pL, pR, HL, HR;
+    idealGasThermal(UL[4], UL[0], dot3(veloL, veloL), gamma, pL, asqrL, HL);
+    idealGasThermal(UR[4], UR[0], dot3(veloR, veloR), gamma, pR, asqrR, HR);
+    RoePre rp = roePreamble(ULm, URm, gamma);
+    real FL[5], FR[5];
+    inviscidFluxXY(UL, veloL, vg, n, pL, FL);
+    inviscidFluxXY(UR, veloR, vg, n, pR, FR);
+    real veloRoeN = dot3(rp.veloRoe, n), vgN = dot3(vg, n);
+    real veloRoe0 = veloRoeN - vgN;
+    lam0 = std::abs(veloRoe0 - rp.aRoe);
+    lam123 = std::abs(veloRoe0);
+    lam4 = std::abs(veloRoe0 + rp.aRoe);
+    real dvL[3], dvR[3], dvRoe[3];
+    for (int d = 0; d < 3; d++)
+        dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d], dvRoe[d] = rp.veloRoe[d] - vg[d];
+    real veloLm0 = dot3(dvL, n), veloRm0 = dot3(dvR, n);
+    if (eigScheme == 2)
+    {
+        lam0 = lam123 = lam4 = std::max(std::abs(veloLm0) + std::sqrt(rp.asqrLm), std::abs(veloRm0) + std::sqrt(rp.asqrRm));
+        for (int i = 0; i < 5; i++)
+            F[i] = (FL[i] + FR[i]) * 0.5 - 0.5 * lam0 * (UR[i] - UL[i]);
+        return;
+    }
+    roeEntropyFix(eigScheme, std::sqrt(rp.asqrLm), std::sqrt(rp.asqrRm), rp.aRoe, veloLm0, veloRm0, veloRoe0,
+                  norm3(dvL), norm3(dvR), norm3(dvRoe), dLambda, fixScale, incFScale, lam0, lam123, lam4);
+    real incU[5];
+    for (int i = 0; i < 5; i++)
+        incU[i] = UR[i] - UL[i];
+    real incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
+    real a23[3];
+    for (int d = 0; d < 3; d++)
+        a23[d] = incU[1 + d] - incU[0] * rp.veloRoe[d];
+    real a23n = dot3(a23, n);
+    real a23T[3];
+    for (int d = 0; d < 3; d++)
+        a23T[d] = a23[d] - n[d] * a23n;
+    real incU4b = incU[4] - dot3(a23T, rp.veloRoe);
+    real alpha1 = (gamma - 1) / rp.asqrRoe * (incU[0] * (rp.HRoe - veloRoeN * veloRoeN) + veloRoeN * incU123N - incU4b);
+    real alpha0 = (incU[0] * (veloRoeN + rp.aRoe) - incU123N - rp.aRoe * alpha1) / (2 * rp.aRoe);
+    real alpha4 = incU[0] - (alpha0 + alpha1);
+    alpha0 *= lam0;
+    alpha1 *= lam123;
+    for (int d = 0; d < 3; d++)
+        a23T[d] *= lam123;
+    alpha4 *= lam4;
+    real incF[5];
+    incF[0] = alpha0 + alpha1 + alpha4;
+    incF[4] = (rp.HRoe - veloRoeN * rp.aRoe) * alpha0 + 0.5 * rp.vsqrRoe * alpha1 + (rp.HRoe + veloRoeN * rp.aRoe) * alpha4 + dot3(a23T, rp.veloRoe);
+    for (int d = 0; d < 3; d++)
+        incF[1 + d] = (rp.veloRoe[d] - rp.aRoe * n[d]) * alpha0 + (rp.veloRoe[d] + rp.aRoe * n[d]) * alpha4 + rp.veloRoe[d] * alpha1 + a23T[d];
+    for (int i = 0; i < 5; i++)
+        F[i] = (FL[i] + FR[i]) * 0.5 - 0.5 * incF[i];
+}
+
+// Gas.hpp:601-714 HLLEPFlux_IdealGas
+static void hllepFlux(int type, const real *UL, const real *UR, const real *ULm, const real *URm, const real vg[3], const real n[3],
+                      real gamma, real F[5], real dLambda, real fixScale, real &lam0, real &lam123, real &lam4)
+{
+    real veloL[3], veloR[3];
+    for (int d = 0; d < 3; d++)
+        veloL[d] = UL[1 + d] / UL[0], veloR[d] = UR[1 + d] / UR[0];
+    real asqrL, asqrR, pL, pR, HL, HR;
+    idealGasThermal(UL[4], UL[0], dot3(veloL, veloL), gamma, pL, asqrL, HL);
+    idealGasThermal(UR[4], UR[0], dot3(veloR, veloR), gamma, pR, asqrR, HR);
+    RoePre rp = roePreamble(ULm, URm, gamma);
+    real FL[5], FR[5];
+    inviscidFluxXY(UL, veloL, vg, n, pL, FL);
+    inviscidFluxXY(UR, veloR, vg, n, pR, FR);
+    real veloRoeN = dot3(rp.veloRoe, n), vgN = dot3(vg, n);
+    real veloRoe0 = veloRoeN - vgN;
+    lam0 = std::abs(veloRoe0 - rp.aRoe);
+    lam123 = std::abs(veloRoe0);
+    lam4 = std::abs(veloRoe0 + rp.aRoe);
+    real dvL[3], dvR[3];
+    for (int d = 0; d < 3; d++)
+        dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d];
+    real veloLm0 = dot3(dvL, n), veloRm0 = dot3(dvR, n);
+    real incU[5];
+    for (int i = 0; i < 5; i++)
+        incU[i] = UR[i] - UL[i];
+    real incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
+    real a23[3];
+    for (int d = 0; d < 3; d++)
+        a23[d] = incU[1 + d] - incU[0] * rp.veloRoe[d];
+    real a23n = dot3(a23, n);
+    real a23T[3];
+    for (int d = 0; d < 3; d++)
+        a23T[d] = a23[d] - n[d] * a23n;
+    real incU4b = incU[4] - dot3(a23T, rp.veloRoe);
+    real alpha1 = (gamma - 1) / rp.asqrRoe * (incU[0] * (rp.HRoe - veloRoeN * veloRoeN) + veloRoeN * incU123N - incU4b);
+    real alpha0 = (incU[0] * (veloRoeN + rp.aRoe) - incU123N - rp.aRoe * alpha1) / (2 * rp.aRoe);
+    real alpha4 = incU[0] - (alpha0 + alpha1);
+    real SL = std::min(veloRoe0 - rp.aRoe, veloLm0 - std::sqrt(asqrL));
+    real SR = std::max(veloRoe0 + rp.aRoe, veloRm0 + std::sqrt(asqrR));
+    real UU = std::abs(veloRoe0);
+    real dfix = rp.aRoe / (rp.aRoe + std::max(UU, dLambda * fixScale));
+    real SP = std::max(SR, 0.0), SM = std::min(SL, 0.0);
+    if (type != 1)
+    {
+        real ReV1[5] = {1, rp.veloRoe[0], rp.veloRoe[1], rp.veloRoe[2], rp.vsqrRoe * 0.5};
+        real div = SP - SM;
+        div += signP(div) * verySmallReal;
+        for (int i = 0; i < 5; i++)
+            F[i] = (SP * FL[i] - SM * FR[i]) / div + (SP * SM / div) * (UR[i] - UL[i] - dfix * ReV1[i] * alpha1);
+    }
+    else
+    {
+        real delta1 = dfix, delta2 = 0.0, delta3 = 0.0;
+        lam123 = ((SP + SM) * (veloRoe0)-2.0 * (1.0 - delta1) * (SP * SM)) / (SP - SM);
+        lam4 = ((SP + SM) * (veloRoe0 + rp.aRoe) - 2.0 * (1.0 - delta2) * (SP * SM)) / (SP - SM);
+        lam0 = ((SP + SM) * (veloRoe0 - rp.aRoe) - 2.0 * (1.0 - delta3) * (SP * SM)) / (SP - SM);
+        lam123 = std::abs(lam123), lam0 = std::abs(lam0), lam4 = std::abs(lam4);
+        alpha0 *= lam0;
+        alpha1 *= lam123;
+        for (int d = 0; d < 3; d++)
+            a23T[d] *= lam123;
+        alpha4 *= lam4;
+        real incF[5];
+        incF[0] = alpha0 + alpha1 + alpha4;
+        incF[4] = (rp.HRoe - veloRoeN * rp.aRoe) * alpha0 + 0.5 * rp.vsqrRoe * alpha1 + (rp.HRoe + veloRoeN * rp.aRoe) * alpha4 + dot3(a23T, rp.veloRoe);
+        for (int d = 0; d < 3; d++)
+            incF[1 + d] = (rp.veloRoe[d] - rp.aRoe * n[d]) * alpha0 + (rp.veloRoe[d] + rp.aRoe * n[d]) * alpha4 + rp.veloRoe[d] * alpha1 + a23T[d];
+        for (int i = 0; i < 5; i++)
+            F[i] = (FL[i] + FR[i]) * 0.5 - 0.5 * incF[i];
+    }
+}
+
+// Gas.hpp:737-~860 HLLCFlux_IdealGas_HartenYee
+static void hllcFlux(const real *UL, const real *UR, const real *ULm, const real *URm, const real vg[3], const real n[3],
+                     real gamma, real F[5], real dLambda, real &lam0, real &lam123, real &lam4)
+{
+    real veloL[3], veloR[3];
+    for (int d = 0; d < 3; d++)
+        veloL[d] = UL[1 + d] / UL[0], veloR[d] = UR[1 + d] / UR[0];
+    real asqrL, asqrR, pL, pR, HL, HR;
+    idealGasThermal(UL[4], UL[0], dot3(veloL, veloL), gamma, pL, asqrL, HL);
+    idealGasThermal(UR[4], UR[0], dot3(veloR, veloR), gamma, pR, asqrR, HR);
+    RoePre rp = roePreamble(ULm, URm, gamma);
+    real FL[5], FR[5];
+    inviscidFluxXY(UL, veloL, vg, n, pL, FL);
+    inviscidFluxXY(UR, veloR, vg, n, pR, FR);
+    real veloRoeN = dot3(rp.veloRoe, n), vgN = dot3(vg, n);
+    real veloRoe0 = veloRoeN - vgN;
+    lam0 = std::abs(veloRoe0 - rp.aRoe);
+    lam123 = std::abs(veloRoe0);
+    lam4 = std::abs(veloRoe0 + rp.aRoe);
+    real dvL[3], dvR[3];
+    for (int d = 0; d < 3; d++)
+        dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d];
+    real veloLm0 = dot3(dvL, n), veloRm0 = dot3(dvR, n);
+    auto HLLCq = [&](real p, real pS)
+    {
+        real q = std::sqrt(1 + (gamma + 1) / 2 / gamma * (pS / p - 1));
+        if (pS <= p)
+            q = 1;
+        return q;
+    };
+    real pS = 0.5 * (rp.pLm + rp.pRm) - 0.5 * (veloLm0 - veloRm0) * rp.rhoRoe * rp.aRoe;
+    pS = std::max(0.0, pS);
+    real SL = veloLm0 - std::sqrt(rp.asqrLm) * HLLCq(rp.pLm, pS);
+    real SR = veloRm0 + std::sqrt(rp.asqrRm) * HLLCq(rp.pRm, pS);
+    (void)dLambda;
+    if (0 <= SL)
+    {
+        std::copy(FL, FL + 5, F);
+        return;
+    }
+    if (SR <= 0)
+    {
+        std::copy(FR, FR + 5, F);
+        return;
+    }
+    real SS = 0;
+    real div = (UL[0] * (SL - veloLm0) - UR[0] * (SR - veloRm0));
+    real ULn = UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2], URn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
+    if (std::abs(div) > verySmallReal)
+        SS = (pR - pL + (ULn - vgN * UL[0]) * (SL - veloLm0) - (URn - vgN * UR[0]) * (SR - veloRm0)) / div;
+    real DS[5] = {0, n[0], n[1], n[2], SS};
+    if (SS >= 0)
+    {
+        real dv = SL - SS;
+        if (std::abs(dv) < verySmallReal)
+            std::copy(FL, FL + 5, F);
+        else
+            for (int i = 0; i < 5; i++)
+                F[i] = ((UL[i] * SL - FL[i]) * SS + DS[i] * ((pL + UL[0] * (SL - veloLm0) * (SS - veloLm0)) * SL)) / dv;
+    }
+    else
+    {
+        real dv = SR - SS;
+        if (std::abs(dv) < verySmallReal)
+            std::copy(FR, FR + 5, F);
+        else
+            for (int i = 0; i < 5; i++)
+                F[i] = ((UR[i] * SR - FR[i]) * SS + DS[i] * ((pR + UR[0] * (SR - veloRm0) * (SS - veloRm0)) * SR)) / dv;
+    }
+}
+
+// Riemann solver codes follow Gas.hpp:61-96 RiemannSolverType
+enum RS
+{
+    RS_Roe = 1,
+    RS_HLLC = 2,
+    RS_HLLEP = 3,
+    RS_HLLEP_V1 = 21,
+    RS_Roe_M1 = 11,
+    RS_Roe_M8 = 18
+};
+
+// Gas.hpp:1434-1490 InviscidFlux_IdealGas_Dispatcher
+static void riemann(int type, const real *UL, const real *UR, const real *ULm, const real *URm, const real vg[3], const real n[3], real gamma,
+                    real F[5], real dLambda, real fixScale, real incFScale, real &lam0, real &lam123, real &lam4)
+{
+    if (type == RS_Roe)
+        roeFlux(0, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, incFScale, lam0, lam123, lam4);
+    else if (type >= 11 && type <= 18)
+        roeFlux(type - 10, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, incFScale, lam0, lam123, lam4);
+    else if (type == RS_HLLEP)
+        hllepFlux(0, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, lam0, lam123, lam4);
+    else if (type == RS_HLLEP_V1)
+        hllepFlux(1, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, lam0, lam123, lam4);
+    else if (type == RS_HLLC)
+        hllcFlux(UL, UR, ULm, URm, vg, n, gamma, F, dLambda, lam0, lam123, lam4);
+}
+
+// Gas.hpp:1677-1698 GradientCons2Prim_IdealGas; G is [3][nv]
+static void gradCons2Prim(int nv, const real *U, const real *G, real *GP, real gamma)
+{
+    real velo[3] = {U[1] / U[0], U[2] / U[0], U[3] / U[0]};
+    for (int i = 0; i < 3 * nv; i++)
+        GP[i] = G[i];
+    for (int r = 0; r < 3; r++)
+        for (int j = 0; j < 3; j++)
+            GP[r * nv + 1 + j] = (1.0 / sqr(U[0])) * (U[0] * G[r * nv + 1 + j] - G[r * nv + 0] * U[1 + j]);
+    for (int r = 0; r < 3; r++)
+    {
+        real s = 0;
+        for (int j = 0; j < 3; j++)
+            s += G[r * nv + 1 + j] * velo[j] + GP[r * nv + 1 + j] * U[1 + j];
+        GP[r * nv + 4] = (gamma - 1) * (G[r * nv + 4] - 0.5 * s);
+    }
+    for (int r = 0; r < 3; r++)
+        for (int j = 5; j < nv; j++)
+        {
+            GP[r * nv + j] -= G[r * nv + 0] * U[j] / U[0];
+            GP[r * nv + j] /= U[0];
+        }
+}
+
+// Gas.hpp:1594-1655 ViscousFlux_IdealGas (no QCR)
+static void viscousFlux(int nv, const real *U, const real *GP, const real n[3], bool adiabatic, real gamma, real mu, real k, real Cp, real *Flux)
+{
+    real velo[3] = {U[1] / U[0], U[2] / U[0], U[3] / U[0]};
+    const real lambda = -2. / 3.;
+    real dV[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            dV[i][j] = GP[i * nv + 1 + j];
+    real gradP[3] = {GP[0 * nv + 4], GP[1 * nv + 4], GP[2 * nv + 4]};
+    real vSqr = dot3(velo, velo);
+    real p = (gamma - 1) * (U[4] - U[0] * 0.5 * vSqr);
+    real gradT[3];
+    for (int i = 0; i < 3; i++)
+        gradT[i] = (gamma / ((gamma - 1) * Cp * U[0] * U[0])) * (U[0] * gradP[i] - p * GP[i * nv + 0]);
+    if (adiabatic)
+    {
+        real gn = dot3(gradT, n);
+        for (int i = 0; i < 3; i++)
+            gradT[i] -= gn * n[i];
+    }
+    real tr = dV[0][0] + dV[1][1] + dV[2][2];
+    real S[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            S[i][j] = (dV[i][j] + dV[j][i]) * mu + (i == j ? lambda * mu * tr : 0.0);
+    Flux[0] = 0;
+    real Sv[3];
+    for (int i = 0; i < 3; i++)
+    {
+        Flux[1 + i] = S[i][0] * n[0] + S[i][1] * n[1] + S[i][2] * n[2];
+        Sv[i] = S[i][0] * velo[0] + S[i][1] * velo[1] + S[i][2] * velo[2] + k * gradT[i];
+    }
+    Flux[4] = dot3(Sv, n);
+    for (int j = 5; j < nv; j++)
+        Flux[j] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Settings (field names follow CFV/VRSettings.hpp and Euler/EulerEvaluatorSettings.hpp)
+// ---------------------------------------------------------------------------
+} // namespace orc
+
+extern "C"
+{
+    struct OrcVRSettings
+    {
+        int maxOrder, intOrder;
+        double jacobiRelax;
+        int SORInstead;
+        int anisotropicLengths;
+        int scaleType; // 0 MeanAACBB, 1 BaryDiff
+        double scaleMultiplier;
+        int dirWeightScheme; // 0 Factorial, 1 HQM_OPT, 999 manual
+        double manualDirWeights[4];
+        int geomWeightScheme; // 0 none, 1 HQM_SD, 2 SD_Power
+        double geomWeightBias, geomWeightPower, geomWeightPower1, geomWeightPower2;
+        double bcWeight;
+    };
+    struct OrcEulerSettings
+    {
+        int nVars;
+        int rsType;
+        double rsFixScale, rsIncFScale;
+        double gamma, Rgas, muGas, prGas, TRef, CSutherland;
+        int muModel;
+        int ignoreVis;
+    };
+}
+
+namespace orc
+{
+struct Oracle
+{
+    // mesh
+    int dim, cellType, faceType, nvert, nfv, nf;
+    long nNode, nCell, nFace;
+    std::vector<real> coords, cellShift, faceShift, facePShift;
+    std::vector<long> cell2node, face2node, face2cell, cell2face;
+    std::vector<int> faceZone;
+    OrcVRSettings vs;
+    OrcEulerSettings es;
+    int NDOF, R, nGf, nGc;
+    // geometry (FiniteVolume.hpp:42-56)
+    std::vector<real> vol, cellBary, cellCent, cellHBox, cellJDet, cellPP, smoothRatio;
+    std::vector<real> faceArea, faceCent, faceJDet, facePP, faceNorm, faceMeanNorm;
+    // VR (VariationalReconstruction.hpp:162-233)
+    std::vector<real> baseMoment, faceWeight, faceScale;
+    std::vector<real> AAInvB, AInvb, matA;
+    // evaluator state (EulerEvaluator.hpp lambdaFace*, deltaLambda*)
+    std::vector<real> lambdaFace, lambdaFaceC, lambdaFaceVis, lambdaFace0, deltaLambdaFace, deltaLambdaCell;
+
+    void cellCoords(long c, real *out) const
+    {
+        for (int v = 0; v < nvert; v++)
+            for (int d = 0; d < 3; d++)
+                out[v * 3 + d] = coords[cell2node[c * nvert + v] * 3 + d] + cellShift[(c * nvert + v) * 3 + d];
+    }
+    void faceCoords(long f, real *out) const
+    {
+        for (int v = 0; v < nfv; v++)
+            for (int d = 0; d < 3; d++)
+                out[v * 3 + d] = coords[face2node[f * nfv + v] * 3 + d] + faceShift[(f * nfv + v) * 3 + d];
+    }
+    int sideOf(long c, long f) const { return face2cell[f * 2 + 0] == c ? 0 : 1; }
+    long otherOf(long c, long f) const { return face2cell[f * 2 + 0] == c ? face2cell[f * 2 + 1] : face2cell[f * 2 + 0]; }
+    // point on face f seen from side s (FiniteVolume.hpp:254-271 GetFaceQuadraturePPhysFromCell)
+    void fromSide(long f, int s, const real *p, real *out) const
+    {
+        for (int d = 0; d < 3; d++)
+            out[d] = p[d] + (s == 1 ? facePShift[f * 3 + d] : 0.0);
+    }
+    // barycentre of the other cell seen from cell c (FiniteVolume.hpp:292-311)
+    void otherBary(long c, long f, real *out) const
+    {
+        long o = otherOf(c, f);
+        int s = sideOf(c, f);
+        for (int d = 0; d < 3; d++)
+            out[d] = cellBary[o * 3 + d] + (s == 0 ? -facePShift[f * 3 + d] : facePShift[f * 3 + d]);
+    }
+
+    // FiniteVolume.cpp:22-330 + VariationalReconstruction.cpp:10-43
+    void constructMetrics()
+    {
+        vol.assign(nCell, 0);
+        cellBary.assign(nCell * 3, 0);
+        cellCent.assign(nCell * 3, 0);
+        cellHBox.assign(nCell * 3, 0);
+        nGc = quadNPoints(cellType, vs.intOrder);
+        cellJDet.assign(nCell * nGc, 0);
+        cellPP.assign(nCell * nGc * 3, 0);
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            real cc[24];
+            cellCoords(c, cc);
+            real v = 0;
+            for (int g = 0; g < quadNPoints(cellType, INT_ORDER_MAX); g++)
+            {
+                real p[3], w;
+                quadPoint(cellType, INT_ORDER_MAX, g, p, w);
+                PointGeo pg = pointGeo(cellType, cc, p);
+                v += cellJacDet(dim, pg) * w;
+            }
+            v += verySmallReal;
+            vol[c] = v;
+            real b[3] = {0, 0, 0};
+            for (int g = 0; g < nGc; g++)
+            {
+                real p[3], w;
+                quadPoint(cellType, vs.intOrder, g, p, w);
+                PointGeo pg = pointGeo(cellType, cc, p);
+                real J = cellJacDet(dim, pg);
+                for (int d = 0; d < 3; d++)
+                    b[d] += pg.x[d] * J * w;
+                cellJDet[c * nGc + g] = J + verySmallReal;
+                for (int d = 0; d < 3; d++)
+                    cellPP[(c * nGc + g) * 3 + d] = pg.x[d];
+            }
+            for (int d = 0; d < 3; d++)
+                cellBary[c * 3 + d] = b[d] / v;
+            {
+                real p[3], w;
+                quadPoint(cellType, 1, 0, p, w);
+                PointGeo pg = pointGeo(cellType, cc, p);
+                for (int d = 0; d < 3; d++)
+                    cellCent[c * 3 + d] = pg.x[d];
+            }
+            for (int d = 0; d < 3; d++)
+            {
+                real m = 0;
+                for (int k = 0; k < nvert; k++)
+                    m = std::max(m, std::abs(cc[k * 3 + d] - cellBary[c * 3 + d]));
+                cellHBox[c * 3 + d] = m;
+            }
+            if (dim == 2)
+                cellHBox[c * 3 + 2] = 1;
+        }
+        nGf = quadNPoints(faceType, vs.intOrder);
+        faceArea.assign(nFace, 0);
+        faceCent.assign(nFace * 3, 0);
+        faceJDet.assign(nFace * nGf, 0);
+        facePP.assign(nFace * nGf * 3, 0);
+        faceNorm.assign(nFace * nGf * 3, 0);
+        faceMeanNorm.assign(nFace * 3, 0);
+#pragma omp parallel for schedule(static)
+        for (long f = 0; f < nFace; f++)
+        {
+            real fc[12];
+            faceCoords(f, fc);
+            real a = 0, nm[3] = {0, 0, 0};
+            for (int g = 0; g < nGf; g++)
+            {
+                real p[3], w, n[3];
+                quadPoint(faceType, vs.intOrder, g, p, w);
+                PointGeo pg = pointGeo(faceType, fc, p);
+                real J = faceJDetNorm(dim, pg, n);
+                a += J * w;
+                faceJDet[f * nGf + g] = J + verySmallReal;
+                real nn = norm3(n);
+                for (int d = 0; d < 3; d++)
+                {
+                    facePP[(f * nGf + g) * 3 + d] = pg.x[d];
+                    faceNorm[(f * nGf + g) * 3 + d] = n[d] / nn;
+                    nm[d] += n[d] / nn * J * w;
+                }
+            }
+            faceArea[f] = a + verySmallReal;
+            real nn = norm3(nm);
+            for (int d = 0; d < 3; d++)
+                faceMeanNorm[f * 3 + d] = nm[d] / nn;
+            real p[3], w;
+            quadPoint(faceType, 1, 0, p, w);
+            PointGeo pg = pointGeo(faceType, fc, p);
+            for (int d = 0; d < 3; d++)
+                faceCent[f * 3 + d] = pg.x[d];
+        }
+        // FiniteVolume.cpp:590-648 ConstructCellSmoothScale (nIterCellSmoothScale = 15)
+        std::vector<real> scale(nCell), cur(nCell), nxt(nCell);
+        for (long c = 0; c < nCell; c++)
+        {
+            real s = 0;
+            for (int k = 0; k < nf; k++)
+                s += faceArea[cell2face[c * nf + k]];
+            scale[c] = vol[c] / (s + verySmallReal);
+            cur[c] = scale[c];
+        }
+        for (int it = 1; it <= 15; it++)
+        {
+            for (long c = 0; c < nCell; c++)
+            {
+                real nAdj = 0, sum = 0;
+                for (int k = 0; k < nf; k++)
+                {
+                    long o = otherOf(c, cell2face[c * nf + k]);
+                    if (o >= 0)
+                        nAdj += 1., sum += cur[o];
+                }
+                sum += nAdj * 1 * cur[c];
+                sum /= nAdj * 2;
+                nxt[c] = std::min(cur[c], sum);
+            }
+            cur = nxt;
+        }
+        smoothRatio.resize(nCell);
+        for (long c = 0; c < nCell; c++)
+            smoothRatio[c] = cur[c] / scale[c];
+    }
+
+    // VariationalReconstruction.hpp:319-368 FDiffBaseValue (localOrientation = false)
+    void diffBase(long c, const real *p, real *T, int rows, bool subtractMoment) const
+    {
+        real s[3] = {cellHBox[c * 3 + 0], cellHBox[c * 3 + 1], cellHBox[c * 3 + 2]};
+        if (!vs.anisotropicLengths)
+        {
+            if (dim == 2)
+                s[0] = s[1] = std::max(s[0], s[1]);
+            else
+                s[0] = s[1] = s[2] = std::max({s[0], s[1], s[2]});
+        }
+        real x = (p[0] - cellCent[c * 3 + 0]) / s[0], y = (p[1] - cellCent[c * 3 + 1]) / s[1], z = (p[2] - cellCent[c * 3 + 2]) / s[2];
+        polyFill(dim, T, x, y, z, s[0], s[1], s[2], rows, NDOF);
+        if (subtractMoment)
+            for (int j = 0; j < NDOF; j++)
+                T[j] -= baseMoment[c * NDOF + j];
+    }
+
+    // VariationalReconstruction.hpp:460-590 FFaceFunctional (isotropic path) + AccumulateDiffOrderContributions :32-98
+    // DiffI: [cn][nI] rows of all diff orders (row-major, leading dim ldI), DiffJ likewise.
+    void faceFunctional(long f, const real *DI, int nI, const real *DJ, int nJ, int cn, real *Conj /*nI x nJ*/) const
+    {
+        real fl[3] = {faceScale[f * 3 + 0], faceScale[f * 3 + 1], faceScale[f * 3 + 2]};
+        real faceL = 0;
+        if (vs.scaleType == 0)
+        {
+            real s = 0;
+            for (int d = 0; d < dim; d++)
+                s += fl[d] * fl[d];
+            faceL = std::sqrt(s / dim);
+        }
+        else
+        {
+            real s = 0;
+            for (int d = 0; d < dim; d++)
+                s += fl[d] * fl[d];
+            faceL = std::sqrt(s);
+        }
+        faceL *= vs.scaleMultiplier;
+        for (int i = 0; i < nI * nJ; i++)
+            Conj[i] = 0;
+        const int *nc = dim == 2 ? nComb2 : nComb3;
+        const int starts2[5] = {0, 1, 3, 6, 10}, starts3[5] = {0, 1, 4, 10, 20};
+        const int *st = dim == 2 ? starts2 : starts3;
+        int maxOrd = 0; // highest derivative order present in the cn diff rows
+        while (maxOrd < 3 && st[maxOrd + 1] < cn)
+            maxOrd++;
+        for (int ord = maxOrd; ord >= 0; ord--)
+        {
+            real w = faceWeight[f * (vs.maxOrder + 1) + ord];
+            real fLP = 1;
+            for (int k = 0; k < ord; k++)
+                fLP *= faceL * faceL;
+            real scale = w * w * (faceL == 0 ? 1.0 : fLP);
+            for (int i = 0; i < nI; i++)
+                for (int j = 0; j < nJ; j++)
+                {
+                    real acc = 0;
+                    for (int k = st[ord]; k < st[ord + 1]; k++)
+                        acc += DI[k * nI + i] * DJ[k * nJ + j] * nc[k];
+                    Conj[i * nJ + j] += acc * scale;
+                }
+        }
+    }
+
+    // VariationalReconstruction.cpp:56-498 ConstructBaseAndWeight (cacheDiffBase = false)
+    void constructBaseAndWeight(const real *bcDirWeight /*per zone per order, may be null*/, int nZone)
+    {
+        baseMoment.assign(nCell * NDOF, 0);
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            real cc[24];
+            cellCoords(c, cc);
+            std::vector<real> m(NDOF, 0.0), vv(NDOF);
+            for (int g = 0; g < quadNPoints(cellType, INT_ORDER_MAX); g++)
+            {
+                real p[3], w;
+                quadPoint(cellType, INT_ORDER_MAX, g, p, w);
+                PointGeo pg = pointGeo(cellType, cc, p);
+                real J = cellJacDet(dim, pg);
+                diffBase(c, pg.x, vv.data(), 1, false);
+                for (int j = 0; j < NDOF; j++)
+                    m[j] += vv[j] * J * w;
+            }
+            for (int j = 0; j < NDOF; j++)
+                baseMoment[c * NDOF + j] = m[j] / m[0];
+        }
+        int P = vs.maxOrder;
+        faceWeight.assign(nFace * (P + 1), 0);
+        faceScale.assign(nFace * 3, 0);
+        for (long f = 0; f < nFace; f++)
+        {
+            long c0 = face2cell[f * 2 + 0], c1 = face2cell[f * 2 + 1];
+            real dv[3];
+            if (c1 >= 0)
+            {
+                real b1[3];
+                otherBary(c0, f, b1);
+                for (int d = 0; d < 3; d++)
+                    dv[d] = b1[d] - cellBary[c0 * 3 + d];
+            }
+            else
+            {
+                real vCB[3];
+                for (int d = 0; d < 3; d++)
+                    vCB[d] = faceCent[f * 3 + d] - cellBary[c0 * 3 + d];
+                real vn = dot3(vCB, &faceMeanNorm[f * 3]);
+                for (int d = 0; d < 3; d++)
+                    dv[d] = 2 * vn * faceMeanNorm[f * 3 + d];
+            }
+            if (vs.scaleType == 1)
+            {
+                for (int d = 0; d < 3; d++)
+                    faceScale[f * 3 + d] = dv[d];
+                if (dim == 2)
+                    faceScale[f * 3 + 2] = 1;
+            }
+            else
+            {
+                // MeanAACBB: average of the sides' aligned boxes
+                int n = 0;
+                for (int s = 0; s < 2; s++)
+                {
+                    long c = face2cell[f * 2 + s];
+                    if (c < 0)
+                        continue;
+                    for (int d = 0; d < 3; d++)
+                        faceScale[f * 3 + d] += cellHBox[c * 3 + d];
+                    n++;
+                }
+                for (int d = 0; d < 3; d++)
+                    faceScale[f * 3 + d] /= n;
+            }
+            real wg = 1;
+            real dn = norm3(dv);
+            if (vs.geomWeightScheme == 1)
+                wg = vs.geomWeightBias + std::pow(std::pow(faceArea[f], 1. / real(dim - 1)) / dn, vs.geomWeightPower * 0.5);
+            if (vs.geomWeightScheme == 2)
+                wg = vs.geomWeightBias + std::pow(faceArea[f], vs.geomWeightPower1 * 0.5) * std::pow(dn, vs.geomWeightPower2 * 0.5);
+            real wd[4] = {0, 0, 0, 0};
+            if (vs.dirWeightScheme == 0)
+                for (int p = 0; p <= P; p++)
+                    wd[p] = 1. / factorials[p];
+            else if (vs.dirWeightScheme == 1)
+            {
+                if (P == 1)
+                    wd[0] = wd[1] = 1;
+                else if (P == 2)
+                    wd[0] = 1, wd[1] = 0.4643, wd[2] = 0.1559;
+                else
+                    wd[0] = 1, wd[1] = .5295, wd[2] = wd[3] = .2117;
+            }
+            else
+                for (int p = 0; p <= P; p++)
+                    wd[p] = vs.manualDirWeights[p];
+            int zone = faceZone[f];
+            if (c1 < 0)
+                for (int p = 0; p <= P; p++)
+                    wd[p] *= (bcDirWeight && zone < nZone ? bcDirWeight[zone * 4 + p] : 1.0) * vs.bcWeight;
+            for (int p = 0; p <= P; p++)
+                faceWeight[f * (P + 1) + p] = wd[p] * wg;
+        }
+    }
+
+    // Gauss-Jordan inverse with partial pivoting (equals the reference's
+    // Jacobi-SVD pseudo-inverse, HardEigen.cpp:13-23, when A has full rank)
+    static bool invert(int n, const real *A, real *Ainv)
+    {
+        std::vector<real> M(n * 2 * n);
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < 2 * n; j++)
+                M[i * 2 * n + j] = j < n ? A[i * n + j] : (j - n == i ? 1.0 : 0.0);
+        for (int col = 0; col < n; col++)
+        {
+            int piv = col;
+            for (int r = col + 1; r < n; r++)
+                if (std::abs(M[r * 2 * n + col]) > std::abs(M[piv * 2 * n + col]))
+                    piv = r;
+            if (M[piv * 2 * n + col] == 0)
+                return false;
+            if (piv != col)
+                for (int j = 0; j < 2 * n; j++)
+                    std::swap(M[piv * 2 * n + j], M[col * 2 * n + j]);
+            real d = M[col * 2 * n + col];
+            for (int j = 0; j < 2 * n; j++)
+                M[col * 2 * n + j] /= d;
+            for (int r = 0; r < n; r++)
+                if (r != col)
+                {
+                    real fct = M[r * 2 * n + col];
+                    if (fct != 0)
+                        for (int j = 0; j < 2 * n; j++)
+                            M[r * 2 * n + j] -= fct * M[col * 2 * n + j];
+                }
+        }
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+                Ainv[i * n + j] = M[i * 2 * n + n + j];
+        return true;
+    }
+
+    // VariationalReconstruction.cpp:507-872 ConstructRecCoeff (greenGauss1Weight = 0, intOrderVR = intOrder)
+    int constructRecCoeff()
+    {
+        AAInvB.assign(nCell * (nf + 1) * R * R, 0);
+        AInvb.assign(nCell * nf * R, 0);
+        matA.assign(nCell * R * R, 0);
+        int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+        for (long c = 0; c < nCell; c++)
+        {
+            std::vector<real> A(R * R, 0.0), Ai(R * R), Bs(nf * R * R, 0.0), bs(nf * R, 0.0);
+            std::vector<real> TI(NDOF * NDOF), TJ(NDOF * NDOF), DI(NDOF * R), DJ(NDOF * R), Cj(R * R), one(1, 1.0);
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                int s = sideOf(c, f);
+                long o = otherOf(c, f);
+                for (int g = 0; g < nGf; g++)
+                {
+                    real p[3], pq[3], w;
+                    quadPoint(faceType, vs.intOrder, g, pq, w);
+                    fromSide(f, s, &facePP[(f * nGf + g) * 3], p);
+                    diffBase(c, p, TI.data(), NDOF, true);
+                    for (int r = 0; r < NDOF; r++)
+                        for (int j = 0; j < R; j++)
+                            DI[r * R + j] = TI[r * NDOF + 1 + j];
+                    real JD = faceJDet[f * nGf + g];
+                    faceFunctional(f, DI.data(), R, DI.data(), R, NDOF, Cj.data());
+                    for (int i = 0; i < R * R; i++)
+                        A[i] += Cj[i] * JD * w;
+                    if (o >= 0)
+                    {
+                        real po[3];
+                        fromSide(f, 1 - s, &facePP[(f * nGf + g) * 3], po);
+                        diffBase(o, po, TJ.data(), NDOF, true);
+                        for (int r = 0; r < NDOF; r++)
+                            for (int j = 0; j < R; j++)
+                                DJ[r * R + j] = TJ[r * NDOF + 1 + j];
+                        faceFunctional(f, DI.data(), R, DJ.data(), R, NDOF, Cj.data());
+                        for (int i = 0; i < R * R; i++)
+                            Bs[k * R * R + i] += Cj[i] * JD * w;
+                    }
+                    // b: only the 0-th diff row, against a 1x1 unit
+                    faceFunctional(f, DI.data(), R, one.data(), 1, 1, Cj.data());
+                    for (int i = 0; i < R; i++)
+                        bs[k * R + i] += Cj[i] * JD * w;
+                }
+            }
+            if (!invert(R, A.data(), Ai.data()))
+                bad++;
+            for (int i = 0; i < R * R; i++)
+            {
+                matA[c * R * R + i] = A[i];
+                AAInvB[(c * (nf + 1) + 0) * R * R + i] = Ai[i];
+            }
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                if (otherOf(c, f) < 0)
+                    continue;
+                for (int i = 0; i < R; i++)
+                {
+                    for (int j = 0; j < R; j++)
+                    {
+                        real acc = 0;
+                        for (int l = 0; l < R; l++)
+                            acc += Ai[i * R + l] * Bs[k * R * R + l * R + j];
+                        AAInvB[(c * (nf + 1) + 1 + k) * R * R + i * R + j] = acc;
+                    }
+                    real acc = 0;
+                    for (int l = 0; l < R; l++)
+                        acc += Ai[i * R + l] * bs[k * R + l];
+                    AInvb[(c * nf + k) * R + i] = acc;
+                }
+            }
+        }
+        return bad;
+    }
+
+    // VariationalReconstruction_Reconstruction.hxx:485-615 DoReconstructionIter, Jacobi branch
+    // (SORInstead = false), periodic/interior faces.  uRec rows: [cell][R][nv].
+    void vrIterJacobi(const real *uRec, real *uRecNew, const real *u, bool recordInc, bool uRecIsZero) const
+    {
+        int nv = es.nVars;
+        real relax = vs.jacobiRelax;
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            real *out = uRecNew + c * R * nv;
+            const real *in = uRec + c * R * nv;
+            for (int i = 0; i < R * nv; i++)
+                out[i] = recordInc ? (uRecIsZero ? 0.0 : in[i]) : in[i] * (1 - relax);
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                long o = otherOf(c, f);
+                if (o < 0)
+                    continue; // boundary faces: handled by the BC restatement (not used by periodic cases)
+                const real *M = &AAInvB[(c * (nf + 1) + 1 + k) * R * R];
+                const real *b = &AInvb[(c * nf + k) * R];
+                for (int i = 0; i < R; i++)
+                    for (int v = 0; v < nv; v++)
+                    {
+                        real acc = 0;
+                        if (!(recordInc && uRecIsZero))
+                            for (int j = 0; j < R; j++)
+                                acc += M[i * R + j] * uRec[(o * R + j) * nv + v];
+                        acc += b[i] * (u[o * nv + v] - u[c * nv + v]);
+                        if (recordInc)
+                            out[i * nv + v] -= acc;
+                        else
+                            out[i * nv + v] += relax * acc;
+                    }
+            }
+        }
+    }
+
+    // EulerEvaluator.hpp:751-789 muEff
+    real muEff(const real *U, real T) const
+    {
+        switch (es.muModel)
+        {
+        case 0:
+            return es.muGas;
+        case 1:
+        {
+            real TRel = T / es.TRef;
+            return es.muGas * TRel * std::sqrt(TRel) * (es.TRef + es.CSutherland) / (T + es.CSutherland);
+        }
+        case 2:
+            return es.muGas * U[0];
+        }
+        return std::nan("0");
+    }
+
+    real cp() const { return es.Rgas * es.gamma / (es.gamma - 1); }
+
+    // EulerEvaluator_EvaluateDt.hxx:840-1048 EvaluateDt (no grid velocity, laminar)
+    void evaluateDt(const real *u, real CFL, real MaxDt, bool useLocalDt, real *dt, real *dtMin)
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        lambdaFace.assign(nFace, 0);
+        lambdaFaceC.assign(nFace, 0);
+        lambdaFaceVis.assign(nFace, 0);
+        lambdaFace0.assign(nFace, 0);
+        deltaLambdaFace.assign(nFace, 0);
+        deltaLambdaCell.assign(nCell, 0);
+#pragma omp parallel for schedule(static)
+        for (long f = 0; f < nFace; f++)
+        {
+            long c0 = face2cell[f * 2 + 0], c1 = face2cell[f * 2 + 1];
+            const real *n = &faceMeanNorm[f * 3];
+            std::vector<real> uMean(u + c0 * nv, u + c0 * nv + nv);
+            const real *UL = u + c0 * nv;
+            real vL[3] = {UL[1] / UL[0], UL[2] / UL[0], UL[3] / UL[0]}, vR[3];
+            real pL, asqrL, HL, pR, asqrR, HR;
+            idealGasThermal(UL[4], UL[0], dot3(vL, vL), gamma, pL, asqrL, HL);
+            std::copy(vL, vL + 3, vR);
+            pR = pL, HR = HL, asqrR = asqrL;
+            if (c1 >= 0)
+            {
+                const real *UR = u + c1 * nv;
+                for (int i = 0; i < nv; i++)
+                    uMean[i] = (uMean[i] + UR[i]) * 0.5;
+                for (int d = 0; d < 3; d++)
+                    vR[d] = UR[1 + d] / UR[0];
+                idealGasThermal(UR[4], UR[0], dot3(vR, vR), gamma, pR, asqrR, HR);
+            }
+            real vsum[3] = {vL[0] + vR[0], vL[1] + vR[1], vL[2] + vR[2]};
+            real veloNMean = 0.5 * dot3(vsum, n);
+            real veloNL = dot3(vL, n), veloNR = dot3(vR, n), vgN = 0;
+            real pMean = (pL + pR) * 0.5;
+            real aL = std::sqrt(asqrL), aR = std::sqrt(asqrR);
+            real lambdaConvection = std::max(aL + std::abs(veloNL - vgN), aR + std::abs(veloNR - vgN));
+            real T = pMean / ((gamma - 1) / gamma * cp() * uMean[0]);
+            real muf = muEff(uMean.data(), T);
+            real lamVis = muf / uMean[0] * std::max(4. / 3., gamma / es.prGas);
+            real area = faceArea[f];
+            real volR = c1 >= 0 ? vol[c1] : vol[c0];
+            lambdaFace[f] = lambdaConvection + lamVis * area * (1. / vol[c0] + 1. / volR);
+            lambdaFaceC[f] = std::abs(veloNMean - vgN) + lamVis * area * (1. / vol[c0] + 1. / volR);
+            lambdaFaceVis[f] = lamVis * area * (1. / vol[c0] + 1. / volR);
+            lambdaFace0[f] = lambdaConvection;
+            real dvn = veloNR - veloNL;
+            deltaLambdaFace[f] = std::max({std::abs(dvn + aR - aL), std::abs(dvn - aR + aL), std::abs(aL - aR)});
+        }
+        real mn = veryLargeReal;
+        for (long c = 0; c < nCell; c++)
+        {
+            real lc = 0;
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                lc += lambdaFace[f] * faceArea[f];
+            }
+            dt[c] = std::min(CFL * vol[c] * smoothRatio[c] / (lc + 1e-100), MaxDt);
+            mn = std::min(mn, dt[c]);
+            real dl = 0;
+            for (int k = 0; k < nf; k++)
+                dl = std::max(dl, deltaLambdaFace[cell2face[c * nf + k]]);
+            deltaLambdaCell[c] = dl;
+        }
+        *dtMin = mn;
+        if (!useLocalDt)
+            for (long c = 0; c < nCell; c++)
+                dt[c] = mn;
+    }
+
+    // EulerEvaluator_EvaluateRHS.hxx:55-818 EvaluateRHS with the flux of
+    // EulerEvaluator_EvaluateDt.hxx:1084-1511 fluxFace (interior/periodic faces,
+    // no limiter, source term ignored, no grid velocity)
+    void evaluateRHS(const real *u, const real *uRec, real *rhs, real *faceFluxOut)
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        std::vector<real> faceFlux(nFace * nv, 0.0);
+        if (deltaLambdaCell.empty())
+            deltaLambdaCell.assign(nCell, 0.0);
+#pragma omp parallel for schedule(static)
+        for (long f = 0; f < nFace; f++)
+        {
+            long c0 = face2cell[f * 2 + 0], c1 = face2cell[f * 2 + 1];
+            if (c1 < 0)
+                continue;
+            std::vector<real> T0(4 * NDOF), T1(4 * NDOF);
+            real fluxEs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            const real *ULm = u + c0 * nv, *URm = u + c1 * nv;
+            real dLambda = std::max(deltaLambdaCell[c0], deltaLambdaCell[c1]);
+            for (int g = 0; g < nGf; g++)
+            {
+                real pq[3], w;
+                quadPoint(faceType, vs.intOrder, g, pq, w);
+                const real *n = &faceNorm[(f * nGf + g) * 3];
+                real p0[3], p1[3];
+                fromSide(f, 0, &facePP[(f * nGf + g) * 3], p0);
+                fromSide(f, 1, &facePP[(f * nGf + g) * 3], p1);
+                int rows = dim + 1;
+                diffBase(c0, p0, T0.data(), rows, true);
+                diffBase(c1, p1, T1.data(), rows, true);
+                real UL[8], UR[8], GL[3 * 8] = {0}, GR[3 * 8] = {0};
+                for (int v = 0; v < nv; v++)
+                {
+                    real a = 0, b = 0;
+                    for (int j = 0; j < R; j++)
+                    {
+                        a += T0[1 + j] * uRec[(c0 * R + j) * nv + v];
+                        b += T1[1 + j] * uRec[(c1 * R + j) * nv + v];
+                    }
+                    UL[v] = u[c0 * nv + v] + a;
+                    UR[v] = u[c1 * nv + v] + b;
+                    for (int d = 0; d < dim; d++)
+                    {
+                        real ga = 0, gb = 0;
+                        for (int j = 0; j < R; j++)
+                        {
+                            ga += T0[(1 + d) * NDOF + 1 + j] * uRec[(c0 * R + j) * nv + v];
+                            gb += T1[(1 + d) * NDOF + 1 + j] * uRec[(c1 * R + j) * nv + v];
+                        }
+                        GL[d * nv + v] = ga, GR[d * nv + v] = gb;
+                    }
+                }
+                real minVol = std::min(vol[c0], vol[c1]);
+                real b1[3];
+                otherBary(c0, f, b1);
+                real db[3] = {b1[0] - cellBary[c0 * 3 + 0], b1[1] - cellBary[c0 * 3 + 1], b1[2] - cellBary[c0 * 3 + 2]};
+                real distBaryPerp = std::abs(dot3(db, n));
+                real distGRP = minVol / faceArea[f] * 2;
+                distGRP = std::max(std::min(distBaryPerp, distGRP * 2), distGRP * 0.25);
+                real UM[8], GM[3 * 8], GMP[3 * 8];
+                for (int v = 0; v < nv; v++)
+                    UM[v] = 0.5 * (UL[v] + UR[v]);
+                for (int d = 0; d < 3; d++)
+                    for (int v = 0; v < nv; v++)
+                        GM[d * nv + v] = (GR[d * nv + v] + GL[d * nv + v]) * 0.5 + (1.0 / distGRP) * (n[d] * (UR[v] - UL[v]));
+                if (es.ignoreVis)
+                    for (int i = 0; i < 3 * nv; i++)
+                        GM[i] = 0;
+                gradCons2Prim(nv, UM, GM, GMP, gamma);
+                // fluxFace (EulerEvaluator_EvaluateDt.hxx:1084-1511)
+                real vis[8] = {0};
+                {
+                    real velo2 = (sqr(UM[1]) + sqr(UM[2]) + sqr(UM[3])) / sqr(UM[0]);
+                    real pM, aM, HM;
+                    idealGasThermal(UM[4], UM[0], velo2, gamma, pM, aM, HM);
+                    real Tm = pM / ((gamma - 1) / gamma * cp() * UM[0]);
+                    real muf = muEff(UM, Tm);
+                    real k = cp() * muf / es.prGas;
+                    if (!es.ignoreVis)
+                        viscousFlux(nv, UM, GMP, n, false, gamma, muf, k, cp(), vis);
+                }
+                real F[8] = {0}, l0, l1, l4, vg[3] = {0, 0, 0};
+                riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4);
+                real JD = faceJDet[f * nGf + g];
+                for (int v = 0; v < nv; v++)
+                    fluxEs[v] += -(F[v] - vis[v]) * JD * w;
+            }
+            for (int v = 0; v < nv; v++)
+                faceFlux[f * nv + v] = fluxEs[v];
+        }
+        // cell-wise gather (equivalent to the reference's face scatter, EvaluateRHS.hxx:550-562)
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            for (int v = 0; v < nv; v++)
+                rhs[c * nv + v] = 0;
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                real sgn = sideOf(c, f) == 0 ? 1.0 : -1.0;
+                for (int v = 0; v < nv; v++)
+                    rhs[c * nv + v] += sgn * faceFlux[f * nv + v] / vol[c];
+            }
+        }
+        if (faceFluxOut)
+            std::copy(faceFlux.begin(), faceFlux.end(), faceFluxOut);
+    }
+
+    // EulerEvaluator.hxx:37-159 LUSGSMatrixInit, scalar Jacobian, source ignored
+    void lusgsInit(const real *dTau, real dt, real alphaDiag, real *jdiag) const
+    {
+        for (long c = 0; c < nCell; c++)
+        {
+            real fp = 1.0 / dTau[c] + 1.0 / dt;
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                fp += (0.5 * alphaDiag) * faceArea[f] * lambdaFace[f] / vol[c];
+            }
+            jdiag[c] = fp;
+        }
+    }
+
+    // EulerEvaluator.hpp:1100-1158 fluxJacobian0_Right_Times_du, useRoeTerm = 0
+    void fluxJacTimesDu(const real *U, const real n[3], const real *dU, real lambdaMain, real *dF) const
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        real velo[3] = {U[1] / U[0], U[2] / U[0], U[3] / U[0]};
+        real p, H, asqr;
+        idealGasThermal(U[4], U[0], dot3(velo, velo), gamma, p, asqr, H);
+        // Gas.hpp:462-471 IdealGasUIncrement
+        real dVelo[3];
+        for (int d = 0; d < 3; d++)
+            dVelo[d] = (dU[1 + d] - U[1 + d] / U[0] * dU[0]) / U[0];
+        real dp = (gamma - 1) * (dU[4] - 0.5 * (dU[1] * velo[0] + dU[2] * velo[1] + dU[3] * velo[2] + U[1] * dVelo[0] + U[2] * dVelo[1] + U[3] * dVelo[2]));
+        // Gas.hpp:495-513 GasInviscidFluxFacialIncrement (vg = 0)
+        real vn = dot3(velo, n), dvn = dot3(dVelo, n);
+        dF[0] = dU[1] * n[0] + dU[2] * n[1] + dU[3] * n[2];
+        for (int d = 0; d < 3; d++)
+            dF[1 + d] = dU[1 + d] * vn + U[1 + d] * dvn + n[d] * dp;
+        dF[4] = (dU[4] + dp) * vn + (U[4] + p) * dvn;
+        for (int j = 5; j < nv; j++)
+            dF[j] = dU[j] * vn + U[j] * dvn;
+        for (int j = 0; j < nv; j++)
+            dF[j] += -1 * lambdaMain * dU[j];
+    }
+
+    // EulerEvaluator.hxx:550-693 UpdateSGS (sequential, natural cell order)
+    void updateSGS(real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew, const real *jdiag, bool forward,
+                   bool gsUpdate, bool uIncIsZero, real *sumInc) const
+    {
+        int nv = es.nVars;
+        for (int v = 0; v < nv; v++)
+            sumInc[v] = 0;
+        for (long s = 0; s < nCell; s++)
+        {
+            long c = forward ? s : nCell - 1 - s;
+            real buf[8];
+            for (int v = 0; v < nv; v++)
+                buf[v] = rhs[c * nv + v];
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                long o = otherOf(c, f);
+                if (o < 0 || o == c)
+                    continue;
+                bool useNew = gsUpdate && (forward ? (o < c) : (o > c));
+                if (uIncIsZero && !useNew)
+                    continue;
+                int side = sideOf(c, f);
+                real n[3];
+                for (int d = 0; d < 3; d++)
+                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+                const real *dU = useNew ? uIncNew + o * nv : uInc + o * nv;
+                real dF[8];
+                fluxJacTimesDu(u + o * nv, n, dU, lambdaFace[f], dF);
+                for (int v = 0; v < nv; v++)
+                    buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
+            }
+            for (int v = 0; v < nv; v++)
+            {
+                real old = uIncNew[c * nv + v];
+                uIncNew[c * nv + v] = buf[v] / jdiag[c];
+                sumInc[v] += std::abs(uIncNew[c * nv + v] - old);
+            }
+        }
+    }
+
+    // EulerEvaluator.hxx:175-274 LUSGSMatrixVec
+    void lusgsMatVec(real alphaDiag, const real *u, const real *uInc, const real *jdiag, real *AuInc) const
+    {
+        int nv = es.nVars;
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            real buf[8] = {0};
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                long o = otherOf(c, f);
+                if (o < 0)
+                    continue;
+                int side = sideOf(c, f);
+                real n[3];
+                for (int d = 0; d < 3; d++)
+                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+                real dF[8];
+                fluxJacTimesDu(u + o * nv, n, uInc + o * nv, lambdaFace[f], dF);
+                for (int v = 0; v < nv; v++)
+                    buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
+            }
+            for (int v = 0; v < nv; v++)
+                AuInc[c * nv + v] = jdiag[c] * uInc[c * nv + v] - buf[v];
+        }
+    }
+
+    // EulerEvaluator.hxx:1039-1143 InitializeUDOF: 2 = isentropic vortex (chi given), 3 = Taylor-Green (M0 = 0.1)
+    void initField(int kind, real chi, real *u) const
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        for (long c = 0; c < nCell; c++)
+        {
+            real um[8] = {0};
+            for (int g = 0; g < nGc; g++)
+            {
+                real pq[3], w;
+                quadPoint(cellType, vs.intOrder, g, pq, w);
+                const real *x = &cellPP[(c * nGc + g) * 3];
+                real inc[8] = {0};
+                if (kind == 2)
+                {
+                    // SpecialFields.hpp:42-77 IsentropicVortex10 at t = 0
+                    real xyc = 5;
+                    real px = x[0] - std::floor(x[0] / 10) * 10, py = x[1] - std::floor(x[1] / 10) * 10;
+                    real r = std::sqrt(sqr(px - xyc) + sqr(py - xyc));
+                    real dT = -(gamma - 1) / (8 * gamma * sqr(pi)) * sqr(chi) * std::exp(1 - sqr(r));
+                    real dux = chi / 2 / pi * std::exp((1 - sqr(r)) / 2) * -(py - xyc);
+                    real duy = chi / 2 / pi * std::exp((1 - sqr(r)) / 2) * +(px - xyc);
+                    real T = dT + 1, ux = dux + 1, uy = duy + 1;
+                    real rho = std::pow(T, 1 / (gamma - 1));
+                    real p = T * rho;
+                    inc[0] = rho, inc[1] = rho * ux, inc[2] = rho * uy, inc[4] = 0.5 * (sqr(ux) + sqr(uy)) * rho + p / (gamma - 1);
+                }
+                else
+                {
+                    real M0 = 0.1;
+                    real ux = std::sin(x[0]) * std::cos(x[1]) * std::cos(x[2]);
+                    real uy = -std::cos(x[0]) * std::sin(x[1]) * std::cos(x[2]);
+                    real p = 1. / (gamma * sqr(M0)) + 1. / 16 * ((std::cos(2 * x[0]) + std::cos(2 * x[1])) * (2 + std::cos(2 * x[2])));
+                    real rho = gamma * sqr(M0) * p;
+                    inc[0] = rho, inc[1] = rho * ux, inc[2] = rho * uy, inc[4] = 0.5 * (sqr(ux) + sqr(uy)) * rho + p / (gamma - 1);
+                }
+                for (int v = 0; v < nv; v++)
+                    um[v] += inc[v] * cellJDet[c * nGc + g] * w;
+            }
+            for (int v = 0; v < nv; v++)
+                u[c * nv + v] = um[v] / vol[c];
+        }
+    }
+};
+} // namespace orc
+
+using namespace orc;
+
+extern "C"
+{
+    void *orc_create(int dim, int cellType, int faceType, long nNode, const double *coords, long nCell, int nvert, const long *cell2node,
+                     const double *cellShift, long nFace, int nfv, const long *face2node, const double *faceShift, const long *face2cell,
+                     const int *faceZone, const double *facePShift, int nf, const long *cell2face, const OrcVRSettings *vs,
+                     const OrcEulerSettings *es)
+    {
+        auto *o = new Oracle();
+        o->dim = dim, o->cellType = cellType, o->faceType = faceType;
+        o->nNode = nNode, o->nCell = nCell, o->nFace = nFace, o->nvert = nvert, o->nfv = nfv, o->nf = nf;
+        o->coords.assign(coords, coords + nNode * 3);
+        o->cell2node.assign(cell2node, cell2node + nCell * nvert);
+        o->cellShift.assign(cellShift, cellShift + nCell * nvert * 3);
+        o->face2node.assign(face2node, face2node + nFace * nfv);
+        o->faceShift.assign(faceShift, faceShift + nFace * nfv * 3);
+        o->face2cell.assign(face2cell, face2cell + nFace * 2);
+        o->faceZone.assign(faceZone, faceZone + nFace);
+        o->facePShift.assign(facePShift, facePShift + nFace * 3);
+        o->cell2face.assign(cell2face, cell2face + nCell * nf);
+        o->vs = *vs;
+        o->es = *es;
+        o->NDOF = nDofOf(dim, vs->maxOrder);
+        o->R = o->NDOF - 1;
+        return o;
+    }
+    void orc_destroy(void *h) { delete (Oracle *)h; }
+
+    int orc_construct(void *h, const double *bcDirWeight, int nZone)
+    {
+        auto *o = (Oracle *)h;
+        o->constructMetrics();
+        o->constructBaseAndWeight(bcDirWeight, nZone);
+        return o->constructRecCoeff();
+    }
+
+    void orc_sizes(void *h, long *out)
+    {
+        auto *o = (Oracle *)h;
+        out[0] = o->NDOF, out[1] = o->R, out[2] = o->nGf, out[3] = o->nGc;
+    }
+
+    // copies a named internal array; returns its length (copies only if out != null)
+    long orc_get(void *h, const char *name, double *out)
+    {
+        auto *o = (Oracle *)h;
+        const std::vector<real> *v = nullptr;
+        std::string n(name);
+        if (n == "volume") v = &o->vol;
+        else if (n == "cellBary") v = &o->cellBary;
+        else if (n == "cellCent") v = &o->cellCent;
+        else if (n == "cellHBox") v = &o->cellHBox;
+        else if (n == "cellJDet") v = &o->cellJDet;
+        else if (n == "smoothRatio") v = &o->smoothRatio;
+        else if (n == "faceArea") v = &o->faceArea;
+        else if (n == "cellPP") v = &o->cellPP;
+        else if (n == "faceCent") v = &o->faceCent;
+        else if (n == "faceJDet") v = &o->faceJDet;
+        else if (n == "facePP") v = &o->facePP;
+        else if (n == "faceNorm") v = &o->faceNorm;
+        else if (n == "faceMeanNorm") v = &o->faceMeanNorm;
+        else if (n == "baseMoment") v = &o->baseMoment;
+        else if (n == "faceWeight") v = &o->faceWeight;
+        else if (n == "faceScale") v = &o->faceScale;
+        else if (n == "matrixAAInvB") v = &o->AAInvB;
+        else if (n == "vectorAInvB") v = &o->AInvb;
+        else if (n == "matrixA") v = &o->matA;
+        else if (n == "lambdaFace") v = &o->lambdaFace;
+        else if (n == "lambdaFaceC") v = &o->lambdaFaceC;
+        else if (n == "lambdaFaceVis") v = &o->lambdaFaceVis;
+        else if (n == "deltaLambdaCell") v = &o->deltaLambdaCell;
+        if (!v)
+            return -1;
+        if (out)
+            std::copy(v->begin(), v->end(), out);
+        return (long)v->size();
+    }
+
+    void orc_set_delta_lambda(void *h, const double *dl)
+    {
+        auto *o = (Oracle *)h;
+        o->deltaLambdaCell.assign(dl, dl + o->nCell);
+    }
+
+    void orc_init_field(void *h, int kind, double chi, double *u) { ((Oracle *)h)->initField(kind, chi, u); }
+
+    void orc_vr_iter(void *h, const double *uRec, double *uRecNew, const double *u, int recordInc, int uRecIsZero)
+    {
+        ((Oracle *)h)->vrIterJacobi(uRec, uRecNew, u, recordInc, uRecIsZero);
+    }
+
+    void orc_eval_dt(void *h, const double *u, double CFL, double MaxDt, int useLocalDt, double *dt, double *dtMin)
+    {
+        ((Oracle *)h)->evaluateDt(u, CFL, MaxDt, useLocalDt, dt, dtMin);
+    }
+
+    void orc_eval_rhs(void *h, const double *u, const double *uRec, double *rhs, double *faceFlux)
+    {
+        ((Oracle *)h)->evaluateRHS(u, uRec, rhs, faceFlux);
+    }
+
+    void orc_lusgs_init(void *h, const double *dTau, double dt, double alphaDiag, double *jdiag)
+    {
+        ((Oracle *)h)->lusgsInit(dTau, dt, alphaDiag, jdiag);
+    }
+
+    void orc_update_sgs(void *h, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
+                        const double *jdiag, int forward, int gsUpdate, int uIncIsZero, double *sumInc)
+    {
+        ((Oracle *)h)->updateSGS(alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate, uIncIsZero, sumInc);
+    }
+
+    void orc_lusgs_matvec(void *h, double alphaDiag, const double *u, const double *uInc, const double *jdiag, double *AuInc)
+    {
+        ((Oracle *)h)->lusgsMatVec(alphaDiag, u, uInc, jdiag, AuInc);
+    }
+
+    // single Riemann flux evaluation (Gas.hpp:1434 dispatcher), 5 conservative variables
+    void orc_riemann(int type, const double *UL, const double *UR, const double *ULm, const double *URm, const double *n, double gamma,
+                     double dLambda, double fixScale, double incFScale, double *F, double *lam)
+    {
+        real vg[3] = {0, 0, 0};
+        riemann(type, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, incFScale, lam[0], lam[1], lam[2]);
+    }
+
+    void orc_viscous_flux(const double *U, const double *GradU /*3 x 5 cons*/, const double *n, double gamma, double mu, double k, double Cp,
+                          int adiabatic, double *Flux)
+    {
+        real GP[15];
+        gradCons2Prim(5, U, GradU, GP, gamma);
+        viscousFlux(5, U, GP, n, adiabatic, gamma, mu, k, Cp, Flux);
+    }
+
+    // point values u + D0 . uRec at the cell quadrature points: out[nCell][nGc][nv]
+    void orc_cell_point_values(void *h, const double *u, const double *uRec, double *out)
+    {
+        auto *o = (Oracle *)h;
+        int nv = o->es.nVars, R = o->R, NDOF = o->NDOF;
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < o->nCell; c++)
+        {
+            std::vector<real> T(NDOF);
+            for (int g = 0; g < o->nGc; g++)
+            {
+                o->diffBase(c, &o->cellPP[(c * o->nGc + g) * 3], T.data(), 1, true);
+                for (int v = 0; v < nv; v++)
+                {
+                    real acc = u[c * nv + v];
+                    for (int j = 0; j < R; j++)
+                        acc += T[1 + j] * uRec[(c * R + j) * nv + v];
+                    out[(c * o->nGc + g) * nv + v] = acc;
+                }
+            }
+        }
+    }
+
+    // cell quadrature weights (intOrder rule of the cell element)
+    void orc_cell_quad_weights(void *h, double *w)
+    {
+        auto *o = (Oracle *)h;
+        for (int g = 0; g < o->nGc; g++)
+        {
+            real p[3];
+            quadPoint(o->cellType, o->vs.intOrder, g, p, w[g]);
+        }
+    }
+}

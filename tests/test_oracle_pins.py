@@ -1,0 +1,88 @@
+"""Pins the CPU oracle to the reference's own golden vectors (no GPU needed)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from dndsr_b200 import mesh as M
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_goldens.json")))
+
+
+def _prim2cons(r, u, v, w, p, g=1.4):
+    return np.array([r, r * u, r * v, r * w, p / (g - 1) + 0.5 * r * (u * u + v * v + w * w)])
+
+
+@pytest.mark.parametrize("rs", ["Roe", "HLLC", "HLLEP"])
+def test_riemann_golden(rs):
+    G = GOLD["riemann_mixed_state"]
+    UL, UR = _prim2cons(*G["primL"]), _prim2cons(*G["primR"])
+    n = np.array(G["normal_unnormalised"]) / np.linalg.norm(G["normal_unnormalised"])
+    F, _ = oracle.riemann(rs, UL, UR, n, gamma=G["gamma"])
+    np.testing.assert_allclose(F, G["flux"][rs], rtol=G["rel_tol"])
+
+
+def _exact_flux(U, n, g=1.4):
+    v = U[1:4] / U[0]
+    p = (g - 1) * (U[4] - 0.5 * U[0] * v @ v)
+    vn = v @ n
+    return np.array([U[0] * vn, *(U[1:4] * vn + p * n), (U[4] + p) * vn])
+
+
+@pytest.mark.parametrize("rs", ["Roe", "HLLC", "HLLEP", "Roe_M1", "Roe_M3", "Roe_M4", "Roe_M5", "Roe_M6", "Roe_M7", "Roe_M8"])
+def test_riemann_consistency(rs):
+    # test_RiemannSolvers.cpp:85-158: identical states give the physical flux
+    U = _prim2cons(1.225, 100.0, -50.0, 25.0, 101325.0)
+    n = np.array([0.6, -0.8, 0.0])
+    F, _ = oracle.riemann(rs, U, U, n)
+    np.testing.assert_allclose(F, _exact_flux(U, n), rtol=1e-8, atol=1e-8 * np.abs(_exact_flux(U, n)).max())
+
+
+@pytest.mark.parametrize("rs", ["Roe", "HLLC", "HLLEP"])
+def test_riemann_symmetry(rs):
+    # test_RiemannSolvers.cpp:164-200: F(UL,UR,n) = -F(UR,UL,-n)
+    UL = _prim2cons(1.0, 100.0, 0.0, 0.0, 100000.0)
+    UR = _prim2cons(0.125, 0.0, 0.0, 0.0, 10000.0)
+    n = np.array([1.0, 0.0, 0.0])
+    F1, _ = oracle.riemann(rs, UL, UR, n)
+    F2, _ = oracle.riemann(rs, UR, UL, -n)
+    np.testing.assert_allclose(F1, -F2, rtol=1e-10, atol=1e-10 * np.abs(F1).max())
+
+
+def _vr_error(n, p, hqm, f):
+    m = M.periodic_quad_2d(n, L=10.0, jitter=0.0)
+    vr = dict(maxOrder=p, intOrder=max(p + 2, 5), jacobiRelax=1.0, SORInstead=0, scaleType=1, scaleMultiplier=1.0,
+              dirWeightScheme=1 if hqm else 0, geomWeightScheme=1 if hqm else 0, geomWeightBias=1.0,
+              geomWeightPower=0.5, bcWeight=1.0)
+    o = oracle.Oracle(m, vr, dict(nVars=1, gamma=1.4))
+    assert o.construct() == 0
+    pp = o.get("cellPP").reshape(m.n_cell, o.nGc, 3)
+    jd = o.get("cellJDet").reshape(m.n_cell, o.nGc)
+    w = o.cell_quad_weights()
+    vol = o.get("volume")
+    u = ((f(pp) * jd * w).sum(1) / vol)[:, None]
+    uRec = np.zeros((m.n_cell, o.R, 1))
+    for _ in range(200):  # test_Reconstruction.cpp:345-375 (Jacobi to an RMS increment below 1e-14)
+        new = o.vr_iter(uRec, u)
+        inc = np.sqrt(((new - uRec) ** 2).sum() / m.n_cell)
+        uRec = new
+        if inc < 1e-14:
+            break
+    vals = o.cell_point_values(u, uRec)[..., 0]
+    return (np.abs(vals - f(pp)) * jd * w).sum() / vol.sum()
+
+
+_K = 2 * np.pi / 10
+_FUNCS = {
+    "vr_iv10_sincos": lambda x: np.sin(_K * x[..., 0]) * np.cos(_K * x[..., 1]),
+    "vr_iv10_cospluscos": lambda x: np.cos(_K * x[..., 0]) + np.cos(_K * x[..., 1]),
+}
+_CASES = [(key, c, ib) for key in _FUNCS for c in GOLD[key]["cases"] for ib in range(3)]
+
+
+@pytest.mark.parametrize("key,case,ib", _CASES, ids=[f"{k}-p{c['p']}-{c['weights']}-bis{ib}" for k, c, ib in _CASES])
+def test_vr_iv10_golden(key, case, ib):
+    err = _vr_error([10, 20, 40][ib], case["p"], case["weights"] == "HQM", _FUNCS[key])
+    assert abs(err - case["golden"][ib]) <= GOLD[key]["rel_tol"] * case["golden"][ib]
