@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Throughput of the implicit residual path on one B200: Mcell*RHS/s in FP64.
+
+Workload (the 3-D Navier-Stokes Taylor-Green configuration): periodic
+[0, 2 pi]^3, 64^3 hexahedra (262,144 cells) with seeded +-5% node jitter,
+Re = 1600 (mu = 1/1600, constant viscosity), Mach 0.1 Taylor-Green initial
+field, VR degree 2 (intOrder 5: 9 Gauss points per face), HLLE+ convective
+flux with the compact viscous flux.  One step = one RHS evaluation as the
+reference's solver performs it per pseudo-iteration: one VR block-Jacobi
+sweep followed by EvaluateRHS (Gauss-point reconstruction, Riemann and
+viscous flux, per-cell gather).
+
+Arms:
+  default           the CUDA library through the C-ABI (value: device-resident
+                    inputs; e2e: host buffers with the copies inside the timing)
+  --impl reference  the reference's CPU algorithm (the oracle port, OpenMP on
+                    all host cores; the reference itself cannot be built here)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell*RHS/s FP64 (one VR sweep + EvaluateRHS per step)"
+UNIT = "Mcell*RHS/s"
+# algorithmic bytes per cell (compulsory FP64 traffic under the reference data model, basis recomputed):
+#   RHS:  8*[(R+2)*nv + (2d+1+R) + (nf/2)*(gF*(2d+1)+1)] with d=3, nv=5, R=9, nf=6, gF=9 -> 2104 B
+#   VR:   8*(nf*R^2 + nf*R) + 8*(2*R*nv + nv) -> 5080 B
+B_RHS = 8 * ((9 + 2) * 5 + (2 * 3 + 1 + 9) + 3 * (9 * (2 * 3 + 1) + 1))
+B_VR = 8 * (6 * 81 + 6 * 9) + 8 * (2 * 9 * 5 + 5)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_config(n, p):
+    return {"workload": f"Taylor-Green vortex NS, periodic [0,2pi]^3, {n}^3 hex ({n ** 3} cells), +-5% jitter, Re=1600, "
+                        f"VR degree {p} (intOrder 5), HLLE+ + compact viscous flux; step = VR Jacobi sweep + EvaluateRHS",
+            "cells": n ** 3, "vr_degree": p, "riemann": "HLLEP", "gauss_points_per_face": 9,
+            "l2": "working set (VR matrices 1.19 GB) exceeds the 126 MB L2; no flush needed"}
+
+
+VR_SETTINGS = dict(intOrder=5, dirWeightScheme="HQM_OPT", geomWeightScheme="HQM_SD", geomWeightBias=1.0, geomWeightPower=0.5)
+EULER_SETTINGS = dict(nVars=5, riemannSolverType="HLLEP", muGas=1.0 / 1600, muModel=0, prGas=0.71, gamma=1.4, Rgas=1.0)
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 2 + i and r[2 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_baseline_oracle(n_sample, p, seconds, threads=None):
+    """Times the oracle port (OpenMP) on a bounded sample of the same workload: a smaller TGV mesh with the same settings."""
+    import oracle
+    from dndsr_b200 import mesh as M
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    m = M.tgv_mesh(n_sample)
+    vr = dict(maxOrder=p, intOrder=5, jacobiRelax=1.0, SORInstead=0, scaleType=1, scaleMultiplier=1.0, dirWeightScheme=1,
+              geomWeightScheme=1, geomWeightBias=1.0, geomWeightPower=0.5, bcWeight=1.0)
+    es = dict(nVars=5, rsType=oracle.RS["HLLEP"], rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=1.0 / 1600, prGas=0.71,
+              TRef=273.15, CSutherland=110.4, muModel=0, ignoreVis=0)
+    o = oracle.Oracle(m, vr, es)
+    o.construct()
+    u = o.init_field(3)
+    uRec = np.zeros((m.n_cell, o.R, 5))
+    o.eval_dt(u, 5.0)
+    for _ in range(2):
+        uRec = o.vr_iter(uRec, u)
+        o.eval_rhs(u, uRec)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        uRec = o.vr_iter(uRec, u)
+        o.eval_rhs(u, uRec)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > seconds:
+            break
+    return m.n_cell * steps / el / 1e6, steps, el, m.n_cell
+
+
+def n_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cores = n_cores()
+    per_step = []
+    value = None
+    n_sample = args.sample_n
+    per_step_seconds = max(0.2, min(args.sample_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    for i in range(args.warmup + args.steps):
+        v, steps, el, cells = cpu_baseline_oracle(n_sample, args.p, 0.2 if i < args.warmup else per_step_seconds, cores)
+        if i >= args.warmup:
+            per_step.append(v)
+    value = float(np.mean(per_step))
+    sample = f"oracle port (OpenMP, {cores} threads): VR sweep + EvaluateRHS on the same TGV settings at {n_sample}^3 = {n_sample ** 3} cells, " \
+             f"~{per_step_seconds:.1f} s of repeated steps per timed step"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * (n_sample ** 3) / (value * 1e6), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": workload_config(args.n, args.p),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from dndsr_b200 import mesh as M
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    n, p = args.n, args.p
+    mesh = M.tgv_mesh(n, seed=0x1234 + rank)
+    vr = VariationalReconstruction(mesh, dict(VR_SETTINGS, maxOrder=p)).construct()
+    ev = EulerEvaluator(vr, EULER_SETTINGS)
+    nc = mesh.n_cell
+    u = vr.BuildUDof(5)
+    ev.InitializeUDOF(u, 3)
+    uRec, uRecNew = vr.BuildURec(5), vr.BuildURec(5)
+    rhs = torch.zeros_like(u)
+    dt = torch.zeros(nc, dtype=torch.float64, device=dev)
+    for _ in range(5):  # converge the reconstruction a little so the RHS sees realistic gradients
+        vr.DoReconstructionIter(uRec, uRecNew, u, putIntoNew=False)
+    ev.EvaluateDt(dt, u, 5.0)  # spectral radii for the HLLE+ fix (deltaLambdaCell)
+
+    def step(a, b):
+        vr.DoReconstructionIter(a, b, u, putIntoNew=True)
+        ev.EvaluateRHS(rhs, u, b)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    bufs = [uRec, uRecNew]
+    for i in range(args.warmup):
+        step(bufs[i % 2], bufs[(i + 1) % 2])
+    K = args.steps
+    ev_vr = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    ev_rhs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        start.record()
+        for i in range(K):
+            a, b = bufs[i % 2], bufs[(i + 1) % 2]
+            ev_vr[i][0].record()
+            vr.DoReconstructionIter(a, b, u, putIntoNew=True)
+            ev_vr[i][1].record()
+            ev_rhs[i][0].record()
+            ev.EvaluateRHS(rhs, u, b)
+            ev_rhs[i][1].record()
+        stop.record()
+        barrier()
+    ms = start.elapsed_time(stop)
+    t_vr = float(np.mean([s.elapsed_time(e) for s, e in ev_vr]))
+    t_rhs = float(np.mean([s.elapsed_time(e) for s, e in ev_rhs]))
+    # end to end through the public API with host buffers: H2D u, uRec; D2H rhs, uRecNew
+    u_h = u.cpu().pin_memory()
+    rec_h = bufs[0].cpu().pin_memory()
+    rhs_h = torch.empty_like(rhs, device="cpu").pin_memory()
+    recn_h = torch.empty_like(rec_h).pin_memory()
+    u_d, rec_d, recn_d = torch.empty_like(u), torch.empty_like(uRec), torch.empty_like(uRec)
+
+    def e2e_step():
+        u_d.copy_(u_h, non_blocking=True)
+        rec_d.copy_(rec_h, non_blocking=True)
+        vr.DoReconstructionIter(rec_d, recn_d, u_d, putIntoNew=True)
+        ev.EvaluateRHS(rhs, u_d, recn_d)
+        rhs_h.copy_(rhs, non_blocking=True)
+        recn_h.copy_(recn_d, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record()
+    for _ in range(K):
+        e2e_step()
+    e2.record()
+    barrier()
+    ms_e2e = s2.elapsed_time(e2)
+    h2d = u_h.numel() * 8 + rec_h.numel() * 8
+    d2h = rhs_h.numel() * 8 + recn_h.numel() * 8
+    if dist:
+        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    if rank != 0:
+        return
+    value = world * nc * K / (ms * 1e-3) / 1e6
+    e2e = world * nc * K / (ms_e2e * 1e-3) / 1e6
+    hbm, src = peaks()
+    dom_name, dom_t, dom_b = ("vr_jacobi_sweep", t_vr, B_VR) if t_vr >= t_rhs else ("evaluate_rhs", t_rhs, B_RHS)
+    achieved = dom_b * nc / (dom_t * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_config(n, p), parallelism=f"replicas{world}" if world > 1 else "single GPU"),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * K,
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback 6650 GB/s",
+                         "traffic": None, "algorithmic_bytes_per_cell": dom_b},
+            "kernels_ms": {"vr_jacobi_sweep": t_vr, "evaluate_rhs": t_rhs,
+                           "vr_GBps": B_VR * nc / (t_vr * 1e-3) / 1e9, "rhs_GBps": B_RHS * nc / (t_rhs * 1e-3) / 1e9},
+            "clocks": clk.summary()}
+    if world == 1 and not args.no_cpu_baseline:
+        v, steps, el, cells = cpu_baseline_oracle(args.sample_n, p, args.sample_seconds, n_cores())
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": n_cores(), "kind": "port",
+                                "sample": f"oracle port, OpenMP: {steps} steps of VR sweep + EvaluateRHS on TGV {args.sample_n}^3 "
+                                          f"({cells} cells, same settings) in {el:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--p", type=int, default=2)
+    ap.add_argument("--sample-n", type=int, default=32)
+    ap.add_argument("--sample-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,518 @@
+// C-ABI entry points (include/dndsb.h): argument checks, host-side topology
+// preparation (packed cell-to-face rows, neighbour lists, multicolouring),
+// device allocation of the handle-owned arrays, and dispatch to the kernels.
+#include "../../include/dndsb.h"
+#include "solver.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace dndsb;
+
+struct dndsb_mesh
+{
+    MeshD d;
+    std::vector<int32_t> cellColorHost;
+    int64_t nBndFace = 0;
+};
+
+struct dndsb_vr
+{
+    dndsb_mesh *mesh = nullptr;
+    GeomD g;
+    VRD vr;
+    int *errWord = nullptr;
+    bool metrics = false, base = false, coeff = false;
+};
+
+struct dndsb_eval
+{
+    dndsb_vr *vr = nullptr;
+    EvalD e;
+};
+
+namespace
+{
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(const char *where)
+{
+    cudaError_t e = cudaGetLastError();
+    return fail(DNDSB_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+int upload(T **dst, const T *src, int64_t n)
+{
+    if (dev_alloc((void **)dst, sizeof(T) * n) != cudaSuccess)
+        return ST_CUDA;
+    if (n > 0 && cudaMemcpy(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        return ST_CUDA;
+    return ST_OK;
+}
+
+int status_msg(int rc, const char *where)
+{
+    if (rc == ST_OK)
+        return DNDSB_OK;
+    if (rc == ST_CUDA)
+        return cuda_fail(where);
+    if (rc == ST_NONPHYSICAL)
+        return fail(rc, std::string(where) + ": non-physical state (density or pressure <= 0)");
+    if (rc == ST_NONFINITE)
+        return fail(rc, std::string(where) + ": non-finite value or singular matrix");
+    if (rc == ST_UNSUPPORTED)
+        return fail(rc, std::string(where) + ": configuration not supported");
+    return fail(rc, std::string(where) + ": error");
+}
+
+cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+bool device_ok()
+{
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+} // namespace
+
+extern "C"
+{
+    const char *dndsb_last_error(void) { return g_err.c_str(); }
+    int dndsb_version(void) { return 1; }
+
+    int dndsb_mesh_create(dndsb_mesh **out, int dim, int cellType, int faceType, int64_t nNode, const double *coords, int64_t nCell,
+                          int nvert, const int64_t *cell2node, const double *cellShift, int64_t nFace, int nfv, const int64_t *face2node,
+                          const double *faceShift, const int64_t *face2cell, const int32_t *faceZone, const double *facePShift, int nf,
+                          const int64_t *cell2face)
+    {
+        if (!out || !coords || !cell2node || !cellShift || !face2node || !faceShift || !face2cell || !faceZone || !facePShift || !cell2face)
+            return fail(DNDSB_E_BADARG, "dndsb_mesh_create: null argument");
+        if ((dim != 2 && dim != 3) || nCell <= 0 || nFace <= 0 || nf <= 0 || nf > 6 || nvert > 8 || nfv > 4)
+            return fail(DNDSB_E_BADARG, "dndsb_mesh_create: bad sizes");
+        if (nCell >= (1LL << 30) || nFace >= (1LL << 30) || nNode >= (1LL << 31))
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_mesh_create: mesh too large for 32-bit device indices");
+        if (!device_ok())
+            return fail(DNDSB_E_CUDA, "dndsb_mesh_create: no CUDA device");
+        auto *m = new dndsb_mesh();
+        MeshD &d = m->d;
+        d.dim = dim, d.cellType = cellType, d.faceType = faceType, d.nvert = nvert, d.nfv = nfv, d.nf = nf;
+        d.nNode = nNode, d.nCell = nCell, d.nFace = nFace;
+        std::vector<int32_t> c2n(nCell * nvert), f2n(nFace * nfv), f2c(nFace * 2), c2f(nCell * nf), nbr(nCell * nf);
+        for (int64_t i = 0; i < nCell * nvert; i++)
+        {
+            if (cell2node[i] < 0 || cell2node[i] >= nNode)
+            {
+                delete m;
+                return fail(DNDSB_E_BADARG, "dndsb_mesh_create: cell2node out of range");
+            }
+            c2n[i] = (int32_t)cell2node[i];
+        }
+        for (int64_t i = 0; i < nFace * nfv; i++)
+            f2n[i] = (int32_t)face2node[i];
+        for (int64_t f = 0; f < nFace; f++)
+        {
+            f2c[f * 2] = (int32_t)face2cell[f * 2];
+            f2c[f * 2 + 1] = (int32_t)face2cell[f * 2 + 1];
+            if (f2c[f * 2] < 0 || f2c[f * 2] >= nCell || f2c[f * 2 + 1] >= nCell)
+            {
+                delete m;
+                return fail(DNDSB_E_BADARG, "dndsb_mesh_create: face2cell out of range");
+            }
+            if (f2c[f * 2 + 1] < 0)
+                m->nBndFace++;
+        }
+        for (int64_t c = 0; c < nCell; c++)
+            for (int k = 0; k < nf; k++)
+            {
+                int64_t f = cell2face[c * nf + k];
+                if (f < 0 || f >= nFace || (face2cell[f * 2] != c && face2cell[f * 2 + 1] != c))
+                {
+                    delete m;
+                    return fail(DNDSB_E_BADARG, "dndsb_mesh_create: cell2face inconsistent with face2cell");
+                }
+                int side = face2cell[f * 2] == c ? 0 : 1;
+                c2f[c * nf + k] = (int32_t)((f << 1) | side);
+                nbr[c * nf + k] = f2c[f * 2 + 1 - side];
+            }
+        // greedy multicolouring, first fit in cell order: on a mesh numbered
+        // colour by colour this reproduces the numbering's own classes, and the
+        // colour-ordered sweep equals the sequential sweep of the reference
+        std::vector<int32_t> color(nCell, -1);
+        int nColor = 0;
+        for (int64_t c = 0; c < nCell; c++)
+        {
+            uint64_t used = 0;
+            for (int k = 0; k < nf; k++)
+            {
+                int o = nbr[c * nf + k];
+                if (o >= 0 && o != c && color[o] >= 0 && color[o] < 64)
+                    used |= 1ULL << color[o];
+            }
+            int col = 0;
+            while (col < 64 && (used >> col & 1ULL))
+                col++;
+            color[c] = col;
+            nColor = std::max(nColor, col + 1);
+        }
+        std::vector<int64_t> start(nColor + 1, 0);
+        for (int64_t c = 0; c < nCell; c++)
+            start[color[c] + 1]++;
+        for (int i = 0; i < nColor; i++)
+            start[i + 1] += start[i];
+        std::vector<int32_t> cells(nCell);
+        std::vector<int64_t> pos(start.begin(), start.end() - 1);
+        for (int64_t c = 0; c < nCell; c++)
+            cells[pos[color[c]]++] = (int32_t)c;
+        d.nColor = nColor;
+        d.colorStart = start;
+        m->cellColorHost = color;
+        int rc = 0;
+        rc |= upload(&d.coords, coords, nNode * 3);
+        rc |= upload(&d.cell2node, c2n.data(), nCell * nvert);
+        rc |= upload(&d.cellShift, cellShift, nCell * nvert * 3);
+        rc |= upload(&d.face2node, f2n.data(), nFace * nfv);
+        rc |= upload(&d.faceShift, faceShift, nFace * nfv * 3);
+        rc |= upload(&d.face2cell, f2c.data(), nFace * 2);
+        rc |= upload(&d.faceZone, faceZone, nFace);
+        rc |= upload(&d.facePShift, facePShift, nFace * 3);
+        rc |= upload(&d.cell2face, c2f.data(), nCell * nf);
+        rc |= upload(&d.cellNbr, nbr.data(), nCell * nf);
+        rc |= upload(&d.colorCells, cells.data(), nCell);
+        rc |= upload(&d.cellColor, color.data(), nCell);
+        if (rc)
+        {
+            dndsb_mesh_destroy(m);
+            return cuda_fail("dndsb_mesh_create");
+        }
+        *out = m;
+        return DNDSB_OK;
+    }
+
+    int dndsb_mesh_destroy(dndsb_mesh *m)
+    {
+        if (!m)
+            return DNDSB_OK;
+        MeshD &d = m->d;
+        for (void *p : {(void *)d.coords, (void *)d.cell2node, (void *)d.cellShift, (void *)d.face2node, (void *)d.faceShift, (void *)d.face2cell,
+                        (void *)d.faceZone, (void *)d.facePShift, (void *)d.cell2face, (void *)d.cellNbr, (void *)d.colorCells, (void *)d.cellColor})
+            dev_free(p);
+        delete m;
+        return DNDSB_OK;
+    }
+
+    int dndsb_mesh_colors(const dndsb_mesh *m, int *nColor, int32_t *cellColorHost)
+    {
+        if (!m || !nColor)
+            return fail(DNDSB_E_BADARG, "dndsb_mesh_colors: null argument");
+        *nColor = m->d.nColor;
+        if (cellColorHost)
+            std::memcpy(cellColorHost, m->cellColorHost.data(), sizeof(int32_t) * m->d.nCell);
+        return DNDSB_OK;
+    }
+
+    int dndsb_vr_create(dndsb_vr **out, dndsb_mesh *mesh, const dndsb_vr_settings *s)
+    {
+        if (!out || !mesh || !s)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_create: null argument");
+        if (s->maxOrder < 1 || s->maxOrder > 3 || s->intOrder < 0 || s->intOrder > 6)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_create: maxOrder must be 1..3 and intOrder 0..6");
+        if (s->SORInstead)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_create: SORInstead is not available; use the Jacobi sweep");
+        auto *v = new dndsb_vr();
+        v->mesh = mesh;
+        VRSettingsD &d = v->vr.s;
+        d.maxOrder = s->maxOrder, d.intOrder = s->intOrder, d.jacobiRelax = s->jacobiRelax, d.SORInstead = s->SORInstead;
+        d.anisotropicLengths = s->anisotropicLengths, d.scaleType = s->scaleType, d.scaleMultiplier = s->scaleMultiplier;
+        d.dirWeightScheme = s->dirWeightScheme;
+        for (int i = 0; i < 4; i++)
+            d.manualDirWeights[i] = s->manualDirWeights[i];
+        d.geomWeightScheme = s->geomWeightScheme, d.geomWeightBias = s->geomWeightBias, d.geomWeightPower = s->geomWeightPower;
+        d.geomWeightPower1 = s->geomWeightPower1, d.geomWeightPower2 = s->geomWeightPower2, d.bcWeight = s->bcWeight;
+        if (dev_alloc((void **)&v->errWord, sizeof(int)) != cudaSuccess)
+        {
+            delete v;
+            return cuda_fail("dndsb_vr_create");
+        }
+        *out = v;
+        return DNDSB_OK;
+    }
+
+    int dndsb_vr_destroy(dndsb_vr *v)
+    {
+        if (!v)
+            return DNDSB_OK;
+        GeomD &g = v->g;
+        for (void *p : {(void *)g.vol, (void *)g.cellBary, (void *)g.cellCent, (void *)g.cellScale, (void *)g.cellJDet, (void *)g.cellPP,
+                        (void *)g.smoothRatio, (void *)g.faceArea, (void *)g.faceCent, (void *)g.faceJDet, (void *)g.facePP, (void *)g.faceNorm,
+                        (void *)g.faceMeanNorm, (void *)g.cellQw, (void *)g.faceQw, (void *)v->vr.baseMoment, (void *)v->vr.faceWeight,
+                        (void *)v->vr.faceL, (void *)v->vr.AAInvB, (void *)v->vr.AInvb, (void *)v->vr.matA, (void *)v->vr.AAInvB32,
+                        (void *)v->vr.AInvb32, (void *)v->errWord})
+            dev_free(p);
+        delete v;
+        return DNDSB_OK;
+    }
+
+    int dndsb_vr_construct_metrics(dndsb_vr *v)
+    {
+        if (!v)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_construct_metrics: null");
+        int rc = geom_construct(v->mesh->d, v->vr.s, v->g, 0);
+        v->metrics = rc == ST_OK;
+        return status_msg(rc, "dndsb_vr_construct_metrics");
+    }
+
+    int dndsb_vr_construct_base_and_weight(dndsb_vr *v, const double *bcDirWeight, int nZone)
+    {
+        if (!v || !v->metrics)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_construct_base_and_weight: call construct_metrics first");
+        int rc = vr_construct_base_and_weight(v->mesh->d, v->g, v->vr, bcDirWeight, nZone, 0);
+        v->base = rc == ST_OK;
+        return status_msg(rc, "dndsb_vr_construct_base_and_weight");
+    }
+
+    int dndsb_vr_construct_rec_coeff(dndsb_vr *v)
+    {
+        if (!v || !v->base)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_construct_rec_coeff: call construct_base_and_weight first");
+        int rc = vr_construct_rec_coeff(v->mesh->d, v->g, v->vr, v->errWord, 0);
+        v->coeff = rc == ST_OK;
+        return status_msg(rc, "dndsb_vr_construct_rec_coeff");
+    }
+
+    int dndsb_vr_sizes(const dndsb_vr *v, int64_t *out4)
+    {
+        if (!v || !out4)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_sizes: null");
+        out4[0] = v->vr.NDOF, out4[1] = v->vr.R, out4[2] = v->g.nGf, out4[3] = v->g.nGc;
+        return DNDSB_OK;
+    }
+
+    int dndsb_vr_get_array(const dndsb_vr *v, const char *name, double *hostOut, int64_t cap, int64_t *len)
+    {
+        if (!v || !name)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_get_array: null");
+        const MeshD &m = v->mesh->d;
+        const GeomD &g = v->g;
+        const VRD &r = v->vr;
+        std::string n(name);
+        const double *src = nullptr;
+        int64_t cnt = 0;
+        int R = r.R;
+        if (n == "volume") src = g.vol, cnt = m.nCell;
+        else if (n == "cellBary") src = g.cellBary, cnt = m.nCell * 3;
+        else if (n == "cellCent") src = g.cellCent, cnt = m.nCell * 3;
+        else if (n == "cellHBox") src = g.cellScale, cnt = m.nCell * 3;
+        else if (n == "cellJDet") src = g.cellJDet, cnt = m.nCell * g.nGc;
+        else if (n == "cellPP") src = g.cellPP, cnt = m.nCell * g.nGc * 3;
+        else if (n == "smoothRatio") src = g.smoothRatio, cnt = m.nCell;
+        else if (n == "faceArea") src = g.faceArea, cnt = m.nFace;
+        else if (n == "faceCent") src = g.faceCent, cnt = m.nFace * 3;
+        else if (n == "faceJDet") src = g.faceJDet, cnt = m.nFace * g.nGf;
+        else if (n == "facePP") src = g.facePP, cnt = m.nFace * g.nGf * 3;
+        else if (n == "faceNorm") src = g.faceNorm, cnt = m.nFace * g.nGf * 3;
+        else if (n == "faceMeanNorm") src = g.faceMeanNorm, cnt = m.nFace * 3;
+        else if (n == "baseMoment") src = r.baseMoment, cnt = m.nCell * r.NDOF;
+        else if (n == "faceWeight") src = r.faceWeight, cnt = m.nFace * (r.P + 1);
+        else if (n == "faceL") src = r.faceL, cnt = m.nFace;
+        else if (n == "matrixAAInvB") src = r.AAInvB, cnt = m.nCell * (m.nf + 1) * R * R;
+        else if (n == "vectorAInvB") src = r.AInvb, cnt = m.nCell * m.nf * R;
+        else if (n == "matrixA") src = r.matA, cnt = m.nCell * R * R;
+        else
+            return fail(DNDSB_E_BADARG, "dndsb_vr_get_array: unknown name " + n);
+        if (!src)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_get_array: array not constructed yet: " + n);
+        if (len)
+            *len = cnt;
+        if (hostOut)
+        {
+            if (cap < cnt)
+                return fail(DNDSB_E_BADARG, "dndsb_vr_get_array: buffer too small");
+            if (cudaMemcpy(hostOut, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess)
+                return cuda_fail("dndsb_vr_get_array");
+        }
+        return DNDSB_OK;
+    }
+
+    int dndsb_vr_do_reconstruction_iter(dndsb_vr *v, double *uRec, double *uRecNew, const double *u, int nVars, int putIntoNew,
+                                        int recordInc, int uRecIsZero, int precision, void *stream)
+    {
+        if (!v || !uRec || !uRecNew || !u)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: null argument");
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: call construct_rec_coeff first");
+        if (recordInc && !putIntoNew)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: recordInc needs putIntoNew"); // _Reconstruction.hxx:502
+        if (uRec == uRecNew)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: uRec and uRecNew must differ");
+        if (v->mesh->nBndFace > 0)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_do_reconstruction_iter: boundary faces need a BC table (not yet accepted)");
+        int rc = vr_iter(v->mesh->d, v->vr, nVars, uRec, uRecNew, u, recordInc, uRecIsZero, precision, S(stream));
+        if (rc == ST_OK && !putIntoNew && !recordInc)
+            rc = vr_swap(v->mesh->d.nCell * v->vr.R * nVars, uRec, uRecNew, S(stream));
+        return status_msg(rc, "dndsb_vr_do_reconstruction_iter");
+    }
+
+    int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s)
+    {
+        if (!out || !vr || !s)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_create: null argument");
+        if (s->nVars != 5 && s->nVars != 6)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_create: nVars must be 5 (NS) or 6 (NS_SA)");
+        if (vr->mesh->nBndFace > 0)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_create: boundary faces need a BC table (not yet accepted)");
+        auto *e = new dndsb_eval();
+        e->vr = vr;
+        EulerSettingsD &d = e->e.s;
+        d.nVars = s->nVars, d.rsType = s->rsType, d.rsFixScale = s->rsFixScale, d.rsIncFScale = s->rsIncFScale;
+        d.gamma = s->gamma, d.Rgas = s->Rgas, d.muGas = s->muGas, d.prGas = s->prGas, d.TRef = s->TRef, d.CSutherland = s->CSutherland;
+        d.muModel = s->muModel, d.ignoreVis = s->ignoreVis;
+        const MeshD &m = vr->mesh->d;
+        int rc = 0;
+        rc |= dev_alloc((void **)&e->e.lambdaFace, sizeof(real) * m.nFace);
+        rc |= dev_alloc((void **)&e->e.lambdaFaceC, sizeof(real) * m.nFace);
+        rc |= dev_alloc((void **)&e->e.lambdaFaceVis, sizeof(real) * m.nFace);
+        rc |= dev_alloc((void **)&e->e.lambdaConv, sizeof(real) * m.nFace);
+        rc |= dev_alloc((void **)&e->e.deltaLambdaFace, sizeof(real) * m.nFace);
+        rc |= dev_alloc((void **)&e->e.deltaLambdaCell, sizeof(real) * m.nCell);
+        rc |= dev_alloc((void **)&e->e.faceFlux, sizeof(real) * std::max(m.nFace, m.nCell) * s->nVars);
+        rc |= dev_alloc((void **)&e->e.redBuf, sizeof(real) * kRedBufLen);
+        rc |= dev_alloc((void **)&e->e.errWord, sizeof(int));
+        if (rc)
+        {
+            dndsb_eval_destroy(e);
+            return cuda_fail("dndsb_eval_create");
+        }
+        cudaMemset(e->e.deltaLambdaCell, 0, sizeof(real) * m.nCell);
+        cudaMemset(e->e.lambdaFace, 0, sizeof(real) * m.nFace);
+        *out = e;
+        return DNDSB_OK;
+    }
+
+    int dndsb_eval_destroy(dndsb_eval *e)
+    {
+        if (!e)
+            return DNDSB_OK;
+        for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
+                        (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord})
+            dev_free(p);
+        delete e;
+        return DNDSB_OK;
+    }
+
+    int dndsb_eval_initialize_udof(dndsb_eval *e, int kind, double chi, double *u, void *stream)
+    {
+        if (!e || !u || (kind != 2 && kind != 3))
+            return fail(DNDSB_E_BADARG, "dndsb_eval_initialize_udof: bad argument");
+        return status_msg(init_field(e->vr->mesh->d, e->vr->g, e->e, kind, chi, u, S(stream)), "dndsb_eval_initialize_udof");
+    }
+
+    int dndsb_eval_evaluate_dt(dndsb_eval *e, const double *u, double CFL, double MaxDt, int useLocalDt, double *dt, double *dtMinHost,
+                               void *stream)
+    {
+        if (!e || !u || !dt)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_dt: null argument");
+        return status_msg(eval_dt(e->vr->mesh->d, e->vr->g, e->e, u, CFL, MaxDt, useLocalDt, dt, dtMinHost, S(stream)),
+                          "dndsb_eval_evaluate_dt");
+    }
+
+    int dndsb_eval_evaluate_rhs(dndsb_eval *e, double *rhs, const double *u, const double *uRec, void *stream)
+    {
+        if (!e || !rhs || !u || !uRec)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: VR not constructed");
+        return status_msg(eval_rhs(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, u, uRec, rhs, nullptr, S(stream)), "dndsb_eval_evaluate_rhs");
+    }
+
+    int dndsb_eval_lusgs_matrix_init(dndsb_eval *e, const double *dTau, double dt, double alphaDiag, double *jdiag, void *stream)
+    {
+        if (!e || !dTau || !jdiag)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_init: null argument");
+        return status_msg(lusgs_init(e->vr->mesh->d, e->vr->g, e->e, dTau, dt, alphaDiag, jdiag, S(stream)), "dndsb_eval_lusgs_matrix_init");
+    }
+
+    int dndsb_eval_update_sgs(dndsb_eval *e, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
+                              const double *jdiag, int forward, int gsUpdate, int uIncIsZero, double *sumIncHost, void *stream)
+    {
+        if (!e || !rhs || !u || !uInc || !uIncNew || !jdiag)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs: null argument");
+        if (uInc == uIncNew)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs: uInc and uIncNew must differ"); // EulerEvaluator.hxx:563
+        return status_msg(update_sgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate, uIncIsZero,
+                                     sumIncHost, S(stream)),
+                          "dndsb_eval_update_sgs");
+    }
+
+    int dndsb_eval_lusgs_matrix_vec(dndsb_eval *e, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
+                                    double *AuInc, void *stream)
+    {
+        if (!e || !u || !uInc || !jdiag || !AuInc)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_vec: null argument");
+        return status_msg(lusgs_matvec(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, uInc, jdiag, AuInc, S(stream)),
+                          "dndsb_eval_lusgs_matrix_vec");
+    }
+
+    int dndsb_eval_evaluate_norm(dndsb_eval *e, const double *x, int P, int volWise, double *resHost, void *stream)
+    {
+        if (!e || !x || !resHost || P < 1)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_norm: bad argument");
+        const MeshD &m = e->vr->mesh->d;
+        int nv = e->e.s.nVars;
+        int rc;
+        if (P < 3)
+        {
+            rc = reduce_norm(m.nCell, nv, x, volWise ? e->vr->g.vol : nullptr, 0, P, e->e.redBuf, resHost, S(stream));
+            if (rc == ST_OK)
+                for (int v = 0; v < nv; v++)
+                    resHost[v] = P == 1 ? resHost[v] : std::sqrt(resHost[v]);
+        }
+        else
+            rc = reduce_norm(m.nCell, nv, x, nullptr, 2, 1, e->e.redBuf, resHost, S(stream));
+        return status_msg(rc, "dndsb_eval_evaluate_norm");
+    }
+
+    int dndsb_eval_get_array(const dndsb_eval *e, const char *name, double *hostOut, int64_t cap, int64_t *len)
+    {
+        if (!e || !name)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_get_array: null");
+        const MeshD &m = e->vr->mesh->d;
+        std::string n(name);
+        const double *src = nullptr;
+        int64_t cnt = 0;
+        if (n == "lambdaFace") src = e->e.lambdaFace, cnt = m.nFace;
+        else if (n == "lambdaFaceC") src = e->e.lambdaFaceC, cnt = m.nFace;
+        else if (n == "lambdaFaceVis") src = e->e.lambdaFaceVis, cnt = m.nFace;
+        else if (n == "deltaLambdaCell") src = e->e.deltaLambdaCell, cnt = m.nCell;
+        else if (n == "faceFlux") src = e->e.faceFlux, cnt = m.nFace * e->e.s.nVars;
+        else
+            return fail(DNDSB_E_BADARG, "dndsb_eval_get_array: unknown name " + n);
+        if (len)
+            *len = cnt;
+        if (hostOut)
+        {
+            if (cap < cnt)
+                return fail(DNDSB_E_BADARG, "dndsb_eval_get_array: buffer too small");
+            if (cudaMemcpy(hostOut, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess)
+                return cuda_fail("dndsb_eval_get_array");
+        }
+        return DNDSB_OK;
+    }
+
+    int dndsb_eval_set_delta_lambda(dndsb_eval *e, const double *dl, void *stream)
+    {
+        if (!e || !dl)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_delta_lambda: null");
+        if (cudaMemcpyAsync(e->e.deltaLambdaCell, dl, sizeof(double) * e->vr->mesh->d.nCell, cudaMemcpyDeviceToDevice, S(stream)) !=
+            cudaSuccess)
+            return cuda_fail("dndsb_eval_set_delta_lambda");
+        return DNDSB_OK;
+    }
+}

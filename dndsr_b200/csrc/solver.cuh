@@ -1,0 +1,140 @@
+// Device-resident state of one mesh + variational reconstruction + Euler
+// evaluator, and the launch functions the C-ABI layer calls.
+//
+// Layout in HBM (all arrays structure-of-arrays, 64-bit reals unless noted):
+//   cell rows   : vol, smooth ratio [nCell]; bary, cent, scale [nCell][3];
+//                 cellJDet [nCell][nGc]; cellPP [nCell][nGc][3];
+//                 baseMoment [nCell][NDOF]
+//   face rows   : area [nFace]; meanNorm, cent, pshift [nFace][3];
+//                 faceJDet [nFace][nGf]; facePP, faceNorm [nFace][nGf][3];
+//                 faceWeight [nFace][P+1]; faceL [nFace]
+//   VR matrices : AAInvB [nCell][nf+1][R][R] (block 0 = A^-1, block 1+k = A^-1 B_k)
+//                 AInvb  [nCell][nf][R]; FP32 copies for the mixed-precision path
+//   state       : u [nCell][nv], uRec [nCell][R][nv] (caller-owned device buffers)
+#pragma once
+#include "core.cuh"
+#include <vector>
+
+namespace dndsb
+{
+// error classes returned by every C-ABI entry point (also in include/dndsb.h)
+enum Status : int
+{
+    ST_OK = 0,
+    ST_BADARG = -1,
+    ST_CUDA = -2,
+    ST_NONFINITE = -3,
+    ST_NONPHYSICAL = -4,
+    ST_UNSUPPORTED = -5,
+    ST_DIVERGED = -6,
+    ST_TIMEOUT = -7,
+};
+
+// device error word bits (set by kernels, read back by the host)
+enum DevErr : int
+{
+    DE_NONFINITE = 1,
+    DE_NONPHYSICAL = 2,
+    DE_SINGULAR = 4,
+};
+
+struct MeshD
+{
+    int dim = 0, cellType = 0, faceType = 0, nvert = 0, nfv = 0, nf = 0;
+    int64_t nNode = 0, nCell = 0, nFace = 0;
+    real *coords = nullptr;     // [nNode][3]
+    int32_t *cell2node = nullptr; // [nCell][nvert]
+    real *cellShift = nullptr;  // [nCell][nvert][3]
+    int32_t *face2node = nullptr; // [nFace][nfv]
+    real *faceShift = nullptr;  // [nFace][nfv][3]
+    int32_t *face2cell = nullptr; // [nFace][2], -1 on boundary side 1
+    int32_t *faceZone = nullptr;  // [nFace]
+    real *facePShift = nullptr; // [nFace][3]
+    int32_t *cell2face = nullptr; // [nCell][nf], packed (face << 1) | side
+    int32_t *cellNbr = nullptr;   // [nCell][nf], neighbour cell or -1
+    // multicolour ordering for Gauss-Seidel type sweeps
+    int nColor = 0;
+    int32_t *colorCells = nullptr; // cells grouped by colour
+    int32_t *cellColor = nullptr;  // colour of each cell
+    std::vector<int64_t> colorStart; // host copy, size nColor + 1
+};
+
+struct VRSettingsD
+{
+    int maxOrder = 1, intOrder = 1;
+    real jacobiRelax = 1;
+    int SORInstead = 0;
+    int anisotropicLengths = 0;
+    int scaleType = 1; // 0 MeanAACBB, 1 BaryDiff
+    real scaleMultiplier = 1;
+    int dirWeightScheme = 0; // 0 Factorial, 1 HQM_OPT, 999 manual
+    real manualDirWeights[4] = {1, 1, 0.5, 1. / 6};
+    int geomWeightScheme = 0; // 0 none, 1 HQM_SD, 2 SD_Power
+    real geomWeightBias = 0, geomWeightPower = 0.5, geomWeightPower1 = 0, geomWeightPower2 = 0;
+    real bcWeight = 1;
+};
+
+struct GeomD
+{
+    int nGc = 0, nGf = 0;
+    real *vol = nullptr, *cellBary = nullptr, *cellCent = nullptr, *cellScale = nullptr, *cellJDet = nullptr, *cellPP = nullptr,
+         *smoothRatio = nullptr;
+    real *faceArea = nullptr, *faceCent = nullptr, *faceJDet = nullptr, *facePP = nullptr, *faceNorm = nullptr, *faceMeanNorm = nullptr;
+    real *cellQw = nullptr, *faceQw = nullptr; // quadrature weights of the cell / face rule at intOrder
+};
+
+struct VRD
+{
+    VRSettingsD s;
+    int P = 1, NDOF = 1, R = 0;
+    real *baseMoment = nullptr, *faceWeight = nullptr, *faceL = nullptr;
+    real *AAInvB = nullptr, *AInvb = nullptr, *matA = nullptr;
+    float *AAInvB32 = nullptr, *AInvb32 = nullptr;
+};
+
+struct EulerSettingsD
+{
+    int nVars = 5;
+    int rsType = RS_Roe;
+    real rsFixScale = 1, rsIncFScale = 1;
+    real gamma = 1.4, Rgas = 1, muGas = 1, prGas = 0.72, TRef = 273.15, CSutherland = 110.4;
+    int muModel = 1;
+    int ignoreVis = 0;
+    real cp() const { return Rgas * gamma / (gamma - 1); }
+};
+
+struct EvalD
+{
+    EulerSettingsD s;
+    real *lambdaFace = nullptr, *lambdaFaceC = nullptr, *lambdaFaceVis = nullptr, *lambdaConv = nullptr, *deltaLambdaFace = nullptr;
+    real *deltaLambdaCell = nullptr;
+    real *faceFlux = nullptr; // scratch [nFace][nv]
+    real *redBuf = nullptr;   // scratch for reductions
+    int *errWord = nullptr;   // device error word
+};
+
+// ---- setup (setup.cu) ----
+int geom_construct(const MeshD &m, const VRSettingsD &s, GeomD &g, cudaStream_t st);
+int vr_construct_base_and_weight(const MeshD &m, const GeomD &g, VRD &vr, const real *bcDirWeightHost, int nZone, cudaStream_t st);
+int vr_construct_rec_coeff(const MeshD &m, const GeomD &g, VRD &vr, int *errWord, cudaStream_t st);
+
+// ---- hot path (hotpath.cu) ----
+int vr_iter(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
+            int useFP32, cudaStream_t st);
+int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, real MaxDt, int useLocalDt, real *dt, real *dtMin,
+            cudaStream_t st);
+int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *u, const real *uRec, real *rhs, real *faceFlux,
+             cudaStream_t st);
+int lusgs_init(const MeshD &m, const GeomD &g, EvalD &ev, const real *dTau, real dt, real alphaDiag, real *jdiag, cudaStream_t st);
+int update_sgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc,
+               real *uIncNew, const real *jdiag, int forward, int gsUpdate, int uIncIsZero, real *sumIncHost, cudaStream_t st);
+int lusgs_matvec(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jdiag,
+                 real *AuInc, cudaStream_t st);
+int init_field(const MeshD &m, const GeomD &g, const EvalD &ev, int kind, real chi, real *u, cudaStream_t st);
+int vr_swap(int64_t n, real *a, real *b, cudaStream_t st);
+int reduce_norm(int64_t n, int ncol, const real *x, const real *w, int op, int powP, real *redBuf, real *outHost, cudaStream_t st);
+constexpr int kRedBlocks = 592;                  // 4 x 148 SMs
+constexpr int kRedBufLen = kRedBlocks * 8 + 64; // partials of the deterministic reductions + final values
+// column reduction of x [n][ncol] (op 0 sum of |x|^powP * w, 1 min, 2 max); returns the device address of the ncol results
+real *reduce_cols(int op, int64_t n, int ncol, const real *x, const real *w, int powP, real *redBuf, cudaStream_t st);
+} // namespace dndsb

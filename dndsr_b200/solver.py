@@ -1,0 +1,214 @@
+"""Python mirror of the reference's VR / Euler evaluator call surface on torch CUDA tensors.
+
+Class and method names follow CFV::VariationalReconstruction
+(src/CFV/VariationalReconstruction.hpp:108-1114, bound in
+src/CFV/VariationalReconstruction_bind.hpp:19-145) and
+Euler::EulerEvaluator (src/Euler/EulerEvaluator.hpp:76-1980).  State arrays
+are caller-owned contiguous float64 CUDA tensors; every call goes through the
+C-ABI of include/dndsb.h on torch's current stream.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import capi
+from .mesh import Mesh
+
+# reference setting names -> C struct codes
+_SCALE = {"MeanAACBB": 0, "BaryDiff": 1}
+_DIRW = {"Factorial": 0, "HQM_OPT": 1, "ManualDirWeight": 999}
+_GEOMW = {"GWNone": 0, "HQM_SD": 1, "SD_Power": 2}
+RS = dict(Roe=1, HLLC=2, HLLEP=3, HLLEP_V1=21, Roe_M1=11, Roe_M2=12, Roe_M3=13, Roe_M4=14, Roe_M5=15, Roe_M6=16, Roe_M7=17,
+          Roe_M8=18)
+
+VR_DEFAULTS = dict(maxOrder=1, intOrder=1, jacobiRelax=1.0, SORInstead=False, anisotropicLengths=False, scaleType="BaryDiff",
+                   scaleMultiplier=1.0, dirWeightScheme="Factorial", manualDirWeights=(1, 1, 0.5, 1.0 / 6), geomWeightScheme="GWNone",
+                   geomWeightBias=0.0, geomWeightPower=0.5, geomWeightPower1=0.0, geomWeightPower2=0.0, bcWeight=1.0)
+EULER_DEFAULTS = dict(nVars=5, riemannSolverType="Roe", rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=1.0, prGas=0.72,
+                      TRef=273.15, CSutherland=110.4, muModel=1, ignoreVis=False)
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor, nm="tensor"):
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise ValueError(f"{nm} must be a contiguous float64 CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Handle:
+    _destroy = None
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h and self._destroy:
+            try:
+                capi.load(require_device=False)
+                getattr(capi._lib, self._destroy)(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+class DeviceMesh(Handle):
+    """Uploads a :class:`dndsr_b200.mesh.Mesh` (replaces Geom::UnstructuredMesh as the VR input)."""
+    _destroy = "dndsb_mesh_destroy"
+
+    def __init__(self, mesh: Mesh):
+        capi.load()
+        self.mesh = mesh
+        a = mesh.arrays()
+        self._keep = a
+        h = ctypes.c_void_p()
+        D = capi.dptr
+        I64 = lambda x: x.ctypes.data_as(capi._I64)
+        capi.call("dndsb_mesh_create", ctypes.byref(h), mesh.dim, mesh.cell_type, mesh.face_type, mesh.n_node, D(a["coords"]), mesh.n_cell,
+                  a["cell2node"].shape[1], I64(a["cell2node"]), D(a["cell_shift"]), mesh.n_face, a["face2node"].shape[1],
+                  I64(a["face2node"]), D(a["face_shift"]), I64(a["face2cell"]), a["face_zone"].ctypes.data_as(capi._I32), D(a["face_pshift"]),
+                  a["cell2face"].shape[1], I64(a["cell2face"]))
+        self.h = h
+
+    def colors(self):
+        n = ctypes.c_int()
+        col = np.zeros(self.mesh.n_cell, dtype=np.int32)
+        capi.call("dndsb_mesh_colors", self.h, ctypes.byref(n), col.ctypes.data_as(capi._I32))
+        return n.value, col
+
+
+class VariationalReconstruction(Handle):
+    """CFV::VariationalReconstruction<dim> on the GPU."""
+    _destroy = "dndsb_vr_destroy"
+
+    def __init__(self, mesh, settings: dict | None = None):
+        self.dmesh = mesh if isinstance(mesh, DeviceMesh) else DeviceMesh(mesh)
+        self.mesh = self.dmesh.mesh
+        s = dict(VR_DEFAULTS)
+        s.update(settings or {})
+        self.settings = s
+        cs = capi.VRSettings()
+        cs.maxOrder, cs.intOrder, cs.jacobiRelax = int(s["maxOrder"]), int(s["intOrder"]), float(s["jacobiRelax"])
+        cs.SORInstead, cs.anisotropicLengths = int(bool(s["SORInstead"])), int(bool(s["anisotropicLengths"]))
+        cs.scaleType = _SCALE[s["scaleType"]] if isinstance(s["scaleType"], str) else int(s["scaleType"])
+        cs.scaleMultiplier = float(s["scaleMultiplier"])
+        cs.dirWeightScheme = _DIRW[s["dirWeightScheme"]] if isinstance(s["dirWeightScheme"], str) else int(s["dirWeightScheme"])
+        for i, x in enumerate(s["manualDirWeights"][:4]):
+            cs.manualDirWeights[i] = float(x)
+        cs.geomWeightScheme = _GEOMW[s["geomWeightScheme"]] if isinstance(s["geomWeightScheme"], str) else int(s["geomWeightScheme"])
+        cs.geomWeightBias, cs.geomWeightPower = float(s["geomWeightBias"]), float(s["geomWeightPower"])
+        cs.geomWeightPower1, cs.geomWeightPower2, cs.bcWeight = float(s["geomWeightPower1"]), float(s["geomWeightPower2"]), float(s["bcWeight"])
+        h = ctypes.c_void_p()
+        capi.call("dndsb_vr_create", ctypes.byref(h), self.dmesh.h, ctypes.byref(cs))
+        self.h = h
+        self._cs = cs
+
+    # VariationalReconstruction.cpp:10-43, :56-498, :507-872
+    def ConstructMetrics(self):
+        capi.call("dndsb_vr_construct_metrics", self.h)
+
+    def ConstructBaseAndWeight(self, bc_dir_weight=None):
+        if bc_dir_weight is None:
+            capi.call("dndsb_vr_construct_base_and_weight", self.h, None, 0)
+        else:
+            w = np.ascontiguousarray(bc_dir_weight, dtype=np.float64).reshape(-1, 4)
+            capi.call("dndsb_vr_construct_base_and_weight", self.h, capi.dptr(w), w.shape[0])
+
+    def ConstructRecCoeff(self):
+        capi.call("dndsb_vr_construct_rec_coeff", self.h)
+        out = np.zeros(4, dtype=np.int64)
+        capi.call("dndsb_vr_sizes", self.h, out.ctypes.data_as(capi._I64))
+        self.NDOF, self.R, self.nGf, self.nGc = [int(x) for x in out]
+
+    def construct(self, bc_dir_weight=None):
+        self.ConstructMetrics()
+        self.ConstructBaseAndWeight(bc_dir_weight)
+        self.ConstructRecCoeff()
+        return self
+
+    def get(self, name):
+        n = ctypes.c_int64()
+        capi.call("dndsb_vr_get_array", self.h, name.encode(), None, 0, ctypes.byref(n))
+        out = np.zeros(n.value)
+        capi.call("dndsb_vr_get_array", self.h, name.encode(), capi.dptr(out), n.value, ctypes.byref(n))
+        return out
+
+    # VariationalReconstruction.hpp:920-1000 BuildURec / FiniteVolume BuildUDof
+    def BuildURec(self, nVars):
+        return torch.zeros((self.mesh.n_cell, self.R, nVars), dtype=torch.float64, device="cuda")
+
+    def BuildUDof(self, nVars):
+        return torch.zeros((self.mesh.n_cell, nVars), dtype=torch.float64, device="cuda")
+
+    def DoReconstructionIter(self, uRec, uRecNew, u, putIntoNew=False, recordInc=False, uRecIsZero=False, precision="fp64"):
+        """VariationalReconstruction_Reconstruction.hxx:485-615 (Jacobi sweep)."""
+        nv = u.shape[1]
+        capi.call("dndsb_vr_do_reconstruction_iter", self.h, _ptr(uRec, "uRec"), _ptr(uRecNew, "uRecNew"), _ptr(u, "u"), nv,
+                  int(putIntoNew), int(recordInc), int(uRecIsZero), 1 if precision == "fp32" else 0, _stream())
+
+
+class EulerEvaluator(Handle):
+    """Euler::EulerEvaluator<model> on the GPU (models NS / NS_3D with 5 variables)."""
+    _destroy = "dndsb_eval_destroy"
+
+    def __init__(self, vr: VariationalReconstruction, settings: dict | None = None):
+        self.vr = vr
+        s = dict(EULER_DEFAULTS)
+        s.update(settings or {})
+        self.settings = s
+        cs = capi.EulerSettings()
+        cs.nVars = int(s["nVars"])
+        rs = s["riemannSolverType"]
+        cs.rsType = RS[rs] if isinstance(rs, str) else int(rs)
+        cs.rsFixScale, cs.rsIncFScale = float(s["rsFixScale"]), float(s["rsIncFScale"])
+        cs.gamma, cs.Rgas, cs.muGas, cs.prGas = float(s["gamma"]), float(s["Rgas"]), float(s["muGas"]), float(s["prGas"])
+        cs.TRef, cs.CSutherland, cs.muModel, cs.ignoreVis = float(s["TRef"]), float(s["CSutherland"]), int(s["muModel"]), int(bool(s["ignoreVis"]))
+        h = ctypes.c_void_p()
+        capi.call("dndsb_eval_create", ctypes.byref(h), vr.h, ctypes.byref(cs))
+        self.h = h
+        self.nVars = cs.nVars
+        self._cs = cs
+
+    def InitializeUDOF(self, u, kind, chi=5.0):
+        capi.call("dndsb_eval_initialize_udof", self.h, kind, float(chi), _ptr(u, "u"), _stream())
+
+    def EvaluateDt(self, dt, u, CFL, MaxDt=1e100, UseLocaldt=True):
+        mn = ctypes.c_double()
+        capi.call("dndsb_eval_evaluate_dt", self.h, _ptr(u, "u"), float(CFL), float(MaxDt), int(UseLocaldt), _ptr(dt, "dt"),
+                  ctypes.byref(mn), _stream())
+        return mn.value
+
+    def EvaluateRHS(self, rhs, u, uRec):
+        capi.call("dndsb_eval_evaluate_rhs", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+
+    def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag):
+        capi.call("dndsb_eval_lusgs_matrix_init", self.h, _ptr(dTau, "dTau"), float(dt), float(alphaDiag), _ptr(jdiag, "jdiag"), _stream())
+
+    def UpdateSGS(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False, want_sum=True):
+        s = np.zeros(self.nVars)
+        capi.call("dndsb_eval_update_sgs", self.h, float(alphaDiag), _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uInc, "uInc"),
+                  _ptr(uIncNew, "uIncNew"), _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), int(uIncIsZero),
+                  capi.dptr(s) if want_sum else None, _stream())
+        return s
+
+    def LUSGSMatrixVec(self, alphaDiag, u, uInc, jdiag, AuInc):
+        capi.call("dndsb_eval_lusgs_matrix_vec", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(uInc, "uInc"), _ptr(jdiag, "jdiag"),
+                  _ptr(AuInc, "AuInc"), _stream())
+
+    def EvaluateNorm(self, x, P=1, volWise=True):
+        out = np.zeros(self.nVars)
+        capi.call("dndsb_eval_evaluate_norm", self.h, _ptr(x, "x"), int(P), int(volWise), capi.dptr(out), _stream())
+        return out
+
+    def get(self, name):
+        n = ctypes.c_int64()
+        capi.call("dndsb_eval_get_array", self.h, name.encode(), None, 0, ctypes.byref(n))
+        out = np.zeros(n.value)
+        capi.call("dndsb_eval_get_array", self.h, name.encode(), capi.dptr(out), n.value, ctypes.byref(n))
+        return out
+
+    def SetDeltaLambda(self, dl):
+        capi.call("dndsb_eval_set_delta_lambda", self.h, _ptr(dl, "deltaLambdaCell"), _stream())

@@ -1,0 +1,157 @@
+/*
+ * dndsb.h -- C-ABI of the B200 implementation of DNDSR's implicit residual
+ * path: variational reconstruction (VR), Euler/NS right-hand side, local time
+ * step and LU-SGS.
+ *
+ * Plain C: opaque handles, host pointers for setup data, caller-owned DEVICE
+ * pointers for all state arrays, an optional cudaStream_t passed as void*,
+ * and an int status on every call (0 = OK, < 0 = DNDSB_E_*).  No call aborts
+ * or traps; dndsb_last_error() returns a message for the last failure of the
+ * calling thread.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the reference project root):
+ *   CFV::VariationalReconstruction<dim>  src/CFV/VariationalReconstruction.hpp
+ *   Euler::EulerEvaluator<model>         src/Euler/EulerEvaluator.hpp
+ *
+ * Array layouts (row-major):
+ *   u, rhs, uInc          [nCell][nVars]
+ *   uRec                  [nCell][R][nVars], R = NDOF - 1 (reference tURec rows)
+ *   dt, dTau, jdiag       [nCell]
+ *   matrixAAInvB          [nCell][nf+1][R][R] (block 0 = A^-1, 1+k = A^-1 B_k)
+ *   vectorAInvB           [nCell][nf][R]
+ */
+#ifndef DNDSB_H
+#define DNDSB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DNDSB_OK 0
+#define DNDSB_E_BADARG (-1)
+#define DNDSB_E_CUDA (-2)
+#define DNDSB_E_NONFINITE (-3)
+#define DNDSB_E_NONPHYSICAL (-4) /* density or pressure <= 0 seen in a kernel */
+#define DNDSB_E_UNSUPPORTED (-5)
+#define DNDSB_E_DIVERGED (-6)
+#define DNDSB_E_TIMEOUT (-7)
+
+/* element kinds */
+#define DNDSB_ELEM_LINE2 0
+#define DNDSB_ELEM_TRI3 1
+#define DNDSB_ELEM_QUAD4 2
+#define DNDSB_ELEM_TET4 3
+#define DNDSB_ELEM_HEX8 4
+
+/* Riemann solver codes: src/Euler/Gas.hpp:61-96 RiemannSolverType */
+#define DNDSB_RS_ROE 1
+#define DNDSB_RS_HLLC 2
+#define DNDSB_RS_HLLEP 3
+#define DNDSB_RS_HLLEP_V1 21
+#define DNDSB_RS_ROE_M1 11 /* ... DNDSB_RS_ROE_M8 = 18 */
+
+typedef struct dndsb_mesh dndsb_mesh;
+typedef struct dndsb_vr dndsb_vr;
+typedef struct dndsb_eval dndsb_eval;
+
+/* src/CFV/VRSettings.hpp:32-211 (fields of the same names) */
+typedef struct dndsb_vr_settings
+{
+    int maxOrder, intOrder;
+    double jacobiRelax;
+    int SORInstead;
+    int anisotropicLengths;  /* baseSettings.anisotropicLengths */
+    int scaleType;           /* functionalSettings.scaleType: 0 MeanAACBB, 1 BaryDiff */
+    double scaleMultiplier;
+    int dirWeightScheme;     /* 0 Factorial, 1 HQM_OPT, 999 ManualDirWeight */
+    double manualDirWeights[4];
+    int geomWeightScheme;    /* 0 GWNone, 1 HQM_SD, 2 SD_Power */
+    double geomWeightBias, geomWeightPower, geomWeightPower1, geomWeightPower2;
+    double bcWeight;
+} dndsb_vr_settings;
+
+/* src/Euler/EulerEvaluatorSettings.hpp:40-330 (fields of the same names) */
+typedef struct dndsb_euler_settings
+{
+    int nVars;
+    int rsType; /* riemannSolverType */
+    double rsFixScale, rsIncFScale;
+    double gamma, Rgas, muGas, prGas, TRef, CSutherland; /* idealGasProperty */
+    int muModel;
+    int ignoreVis; /* RHS_Ignore_Viscosity flag of EvaluateRHS */
+} dndsb_euler_settings;
+
+/* ---- mesh (replaces Geom::UnstructuredMesh as input; src/Geom/Mesh/Mesh.hpp) ----
+ * cell2face rows list each cell's faces; face2cell[f][1] = -1 on a boundary
+ * face; a face's node order makes its normal point out of face2cell[f][0];
+ * facePShift[f] maps points seen from side 0 into side 1's frame (periodic
+ * translation, zero elsewhere).  All pointers are host pointers. */
+int dndsb_mesh_create(dndsb_mesh **out, int dim, int cellType, int faceType, int64_t nNode, const double *coords, int64_t nCell,
+                      int nvert, const int64_t *cell2node, const double *cellShift, int64_t nFace, int nfv, const int64_t *face2node,
+                      const double *faceShift, const int64_t *face2cell, const int32_t *faceZone, const double *facePShift, int nf,
+                      const int64_t *cell2face);
+int dndsb_mesh_destroy(dndsb_mesh *m);
+/* multicolour ordering used by the SGS sweeps (greedy, first fit in cell order) */
+int dndsb_mesh_colors(const dndsb_mesh *m, int *nColor, int32_t *cellColorHost /* [nCell] or NULL */);
+
+/* ---- variational reconstruction: VariationalReconstruction.hpp:108-1114 ---- */
+int dndsb_vr_create(dndsb_vr **out, dndsb_mesh *mesh, const dndsb_vr_settings *s);
+int dndsb_vr_destroy(dndsb_vr *vr);
+/* ConstructMetrics(), VariationalReconstruction.cpp:10-43 */
+int dndsb_vr_construct_metrics(dndsb_vr *vr);
+/* ConstructBaseAndWeight(id2faceDircWeight), VariationalReconstruction.cpp:56-498;
+ * the callback becomes a table bcDirWeight[zone][4] (NULL = all 1) */
+int dndsb_vr_construct_base_and_weight(dndsb_vr *vr, const double *bcDirWeight, int nZone);
+/* ConstructRecCoeff(), VariationalReconstruction.cpp:507-872 */
+int dndsb_vr_construct_rec_coeff(dndsb_vr *vr);
+/* out4 = {NDOF, R, Gauss points per face, Gauss points per cell} */
+int dndsb_vr_sizes(const dndsb_vr *vr, int64_t *out4);
+/* copies a named device array to host ("volume", "cellBary", "faceArea",
+ * "matrixAAInvB", "vectorAInvB", ...); *len receives the element count */
+int dndsb_vr_get_array(const dndsb_vr *vr, const char *name, double *hostOut, int64_t cap, int64_t *len);
+/* DoReconstructionIter(uRec, uRecNew, u, FBoundary, putIntoNew, recordInc, uRecIsZero),
+ * VariationalReconstruction_Reconstruction.hxx:485-615 (Jacobi sweep).
+ * putIntoNew = 0 swaps the contents of uRec and uRecNew afterwards, like the reference.
+ * precision: 0 FP64 coefficients, 1 FP32 coefficients (FP64 state and accumulation). */
+int dndsb_vr_do_reconstruction_iter(dndsb_vr *vr, double *uRec, double *uRecNew, const double *u, int nVars, int putIntoNew,
+                                    int recordInc, int uRecIsZero, int precision, void *stream);
+
+/* ---- Euler evaluator: EulerEvaluator.hpp:76-1980 ---- */
+int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s);
+int dndsb_eval_destroy(dndsb_eval *ev);
+/* InitializeUDOF special initialisers, EulerEvaluator.hxx:1039-1143:
+ * kind 2 = isentropic vortex of strength chi, 3 = Taylor-Green vortex (M0 = 0.1) */
+int dndsb_eval_initialize_udof(dndsb_eval *ev, int kind, double chi, double *u, void *stream);
+/* EvaluateDt(dt, u, uRec, CFL, dtMinall, MaxDt, UseLocaldt, t), EulerEvaluator_EvaluateDt.hxx:840-1048 */
+int dndsb_eval_evaluate_dt(dndsb_eval *ev, const double *u, double CFL, double MaxDt, int useLocalDt, double *dt, double *dtMinHost,
+                           void *stream);
+/* EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, ...), EulerEvaluator_EvaluateRHS.hxx:55-818
+ * (no limiter: uRecUnlim == uRec; source term ignored) */
+int dndsb_eval_evaluate_rhs(dndsb_eval *ev, double *rhs, const double *u, const double *uRec, void *stream);
+/* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, 0, t), EulerEvaluator.hxx:37-159 (scalar Jacobian) */
+int dndsb_eval_lusgs_matrix_init(dndsb_eval *ev, const double *dTau, double dt, double alphaDiag, double *jdiag, void *stream);
+/* UpdateSGS(alphaDiag, t, rhs, u, uInc, uIncNew, JDiag, forward, gsUpdate, sumInc, uIncIsZero),
+ * EulerEvaluator.hxx:550-693, swept colour by colour; sumIncHost [nVars] may be NULL */
+int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
+                          const double *jdiag, int forward, int gsUpdate, int uIncIsZero, double *sumIncHost, void *stream);
+/* LUSGSMatrixVec(alphaDiag, t, u, uInc, JDiag, AuInc), EulerEvaluator.hxx:175-274 */
+int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
+                                double *AuInc, void *stream);
+/* EvaluateNorm(res, rhs, P, volWise), EulerEvaluator.hxx:1394-1439; P = 1, 2 or >= 3 (max norm) */
+int dndsb_eval_evaluate_norm(dndsb_eval *ev, const double *x, int P, int volWise, double *resHost, void *stream);
+/* named evaluator arrays to host: "lambdaFace", "lambdaFaceC", "lambdaFaceVis", "deltaLambdaCell" */
+int dndsb_eval_get_array(const dndsb_eval *ev, const char *name, double *hostOut, int64_t cap, int64_t *len);
+/* sets deltaLambdaCell (normally produced by EvaluateDt) from a device array [nCell] */
+int dndsb_eval_set_delta_lambda(dndsb_eval *ev, const double *deltaLambdaCell, void *stream);
+
+const char *dndsb_last_error(void);
+int dndsb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
