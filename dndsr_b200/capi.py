@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdndsb.so")
 
 DNDSB_OK = 0
+NOALLOC_SCRATCH_DOUBLES = 1 << 20  # DNDSB_NOALLOC_SCRATCH_DOUBLES in include/dndsb.h
 ERRORS = {-1: "BADARG", -2: "CUDA", -3: "NONFINITE", -4: "NONPHYSICAL", -5: "UNSUPPORTED", -6: "DIVERGED", -7: "TIMEOUT"}
 
 
@@ -74,6 +75,7 @@ SIGNATURES = {
     "dndsb_eval_evaluate_norm": [_P, _P, _i, _i, _D, _P],
     "dndsb_eval_get_array": [_P, ctypes.c_char_p, _D, _l, _I64],
     "dndsb_eval_set_delta_lambda": [_P, _P, _P],
+    "dndsb_eval_evaluate_rhs_noalloc": [_P, _P, _P, _P, _P],
     "dndsb_last_error": [],
     "dndsb_version": [],
 }

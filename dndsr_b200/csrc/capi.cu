@@ -75,6 +75,20 @@ int status_msg(int rc, const char *where)
 }
 
 cudaStream_t S(void *s) { return (cudaStream_t)s; }
+} // namespace
+
+namespace dndsb
+{
+const MeshD &mesh_of(const dndsb_eval *e) { return e->vr->mesh->d; }
+const GeomD &geom_of(const dndsb_eval *e) { return e->vr->g; }
+const VRD &vr_of(const dndsb_eval *e) { return e->vr->vr; }
+bool vr_ready(const dndsb_eval *e) { return e->vr->coeff; }
+EvalD &eval_of(dndsb_eval *e) { return e->e; }
+int set_error(int code, const std::string &msg) { return fail(code, msg); }
+} // namespace dndsb
+
+namespace
+{
 
 bool device_ok()
 {

@@ -184,6 +184,13 @@ class EulerEvaluator(Handle):
     def EvaluateRHS(self, rhs, u, uRec):
         capi.call("dndsb_eval_evaluate_rhs", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
 
+    def EvaluateRHSNoAlloc(self, rhs, u, uRec):
+        """EvaluateRHS without any device allocation: the face-flux scratch is a
+        static 8 MiB device array (nFace * nVars <= capi.NOALLOC_SCRATCH_DOUBLES).
+        For callers that cannot allocate device memory when they evaluate a
+        residual; calls that overlap on the same GPU share the array and race."""
+        capi.call("dndsb_eval_evaluate_rhs_noalloc", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+
     def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag):
         capi.call("dndsb_eval_lusgs_matrix_init", self.h, _ptr(dTau, "dTau"), float(dt), float(alphaDiag), _ptr(jdiag, "jdiag"), _stream())
 

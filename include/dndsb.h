@@ -148,6 +148,21 @@ int dndsb_eval_get_array(const dndsb_eval *ev, const char *name, double *hostOut
 /* sets deltaLambdaCell (normally produced by EvaluateDt) from a device array [nCell] */
 int dndsb_eval_set_delta_lambda(dndsb_eval *ev, const double *deltaLambdaCell, void *stream);
 
+/* Allocation-free EvaluateRHS.  No counterpart in the reference: it exists
+ * for callers that must not allocate device memory when they evaluate a
+ * residual (for example a program whose GPU memory belongs to its own pool
+ * allocator, or a latency-critical loop that cannot take the synchronisation
+ * of cudaMalloc/cudaFree).  The per-face flux scratch lives in a static device
+ * array of DNDSB_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB, held by every GPU
+ * that loads the library until exit); meshes with nFace * nVars above that
+ * are rejected with DNDSB_E_UNSUPPORTED.  The first call on a device looks up
+ * the array's address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls on a device share the array: calls whose
+ * kernels overlap on the GPU race and must be serialised by the caller.
+ * Results equal dndsb_eval_evaluate_rhs. */
+#define DNDSB_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+int dndsb_eval_evaluate_rhs_noalloc(dndsb_eval *ev, double *rhs, const double *u, const double *uRec, void *stream);
+
 const char *dndsb_last_error(void);
 int dndsb_version(void);
 
