@@ -1,0 +1,280 @@
+"""Implicit time marching on top of the GPU operators.
+
+Restates the reference's dual-time machinery:
+
+* ``ESDIRK``  -- Solver/ODE.hpp:122-360 ImplicitSDIRK4DualTimeStep (scheme 1 =
+  6-stage ESDIRK4 with explicit first stage, scheme 0 = 3-stage SDIRK4);
+* ``BDF1``    -- the backward-Euler member of ImplicitVBDFDualTimeStep
+  (ODE.hpp:601-915), used for steady runs;
+* ``GMRES``   -- Solver/Linear.hpp:11-133 GMRES_LeftPreconditioned (restarted,
+  classical Gram-Schmidt, least-squares Hessenberg solve);
+* ``ImplicitSolver`` -- the frhs / fdtau / fsolve / fincrement closures of
+  Euler/EulerSolver.hxx:147-997 with solveLinear / doPrecondition
+  (:1407-1658): LU-SGS (gmresCode 0) or GMRES preconditioned by SGS sweeps
+  (gmresCode 1), optionally in FP32 inside the FP64 defect correction.
+
+Vectors are torch CUDA tensors; every spatial operator is a call into the
+CUDA library (include/dndsb.h).  Host code only orchestrates and does the
+small dense least-squares solve of GMRES.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+VERY_SMALL = 1e-200
+
+
+class ESDIRK:
+    """ODE.hpp:122-360.  scheme 1: ESDIRK4 (odeCode 0 of the solver), scheme 0: SDIRK4."""
+
+    def __init__(self, scheme=1):
+        if scheme == 0:
+            z = 0.128886400515
+            self.A = np.array([[z, 0, 0], [0.5 - z, z, 0], [2 * z, 1 - 4 * z, z]])
+            self.c = np.array([z, 0.5, 1 - z])
+            self.b = np.array([1 / (6 * (2 * z - 1) ** 2), (4 * z * z - 4 * z + 2 / 3) / (2 * z - 1) ** 2, 1 / (6 * (2 * z - 1) ** 2)])
+            self.explicit_first = False
+        else:
+            self.A = np.array([
+                [VERY_SMALL, 0, 0, 0, 0, 0],
+                [0.25, 0.25, 0, 0, 0, 0],
+                [0.137776, -0.055776, 0.25, 0, 0, 0],
+                [0.1446368660269822, -0.2239319076133447, 0.4492950415863626, 0.25, 0, 0],
+                [0.09825878328356477, -0.5915442428196704, 0.8101210205756877, 0.283164405707806, 0.25, 0],
+                [0.1579162951616714, 0, 0.1867589405240008, 0.6805652953093346, -0.2752405309950067, 0.25]])
+            self.b = self.A[-1].copy()
+            self.c = np.array([0, 0.5, 0.332, 0.62, 0.849999966747388, 1])
+            self.explicit_first = True
+        self.n = len(self.c)
+        self.rhsbuf = None
+        self.has_last_end_rhs = False
+
+    def step(self, x, frhs, fdt, fsolve, max_iter, fstop, fincrement, dt):
+        """One physical step; x is updated in place (ODE.hpp:271-343)."""
+        if self.rhsbuf is None:
+            self.rhsbuf = [torch.zeros_like(x) for _ in range(self.n)]
+        x_last = x.clone()
+        dtau = torch.zeros(x.shape[0], dtype=x.dtype, device=x.device)
+        xinc = torch.zeros_like(x)
+        for iB in range(self.n):
+            x.copy_(x_last)
+            it = 1
+            while it <= max_iter:
+                if self.explicit_first and iB == 0:
+                    if self.has_last_end_rhs:
+                        self.rhsbuf[0].copy_(self.rhsbuf[self.n - 1])
+                    else:
+                        frhs(self.rhsbuf[0], x, dtau, 1 << 30, self.c[0])
+                    break
+                fdt(x, dtau, self.A[iB, iB])
+                frhs(self.rhsbuf[iB], x, dtau, it, self.c[iB])
+                rhs = x_last * (1.0 / dt)
+                for jB in range(iB):
+                    rhs.add_(self.rhsbuf[jB], alpha=self.A[iB, jB])
+                res_other = rhs.clone()
+                rhs.add_(x, alpha=-1.0 / dt)
+                rhs.add_(self.rhsbuf[iB], alpha=self.A[iB, iB])
+                fsolve(x, rhs, res_other, dtau, dt, self.A[iB, iB], xinc, it, self.c[iB])
+                fincrement(x, xinc, 1.0)
+                if fstop(it, rhs, iB + 1):
+                    break
+                it += 1
+            if it > max_iter:
+                fstop(it, rhs, iB + 1)
+        if self.explicit_first:
+            self.has_last_end_rhs = True
+            return
+        x.copy_(x_last)
+        for jB in range(self.n):
+            x.add_(self.rhsbuf[jB], alpha=self.b[jB] * dt)
+
+
+class BDF1Stepper:
+    """Backward Euler in dual time (the k = 1 member of ODE.hpp:601-915): residual = (x_n - x)/dt + rhs(x)."""
+
+    def __init__(self):
+        self.rhs = None
+
+    def step(self, x, frhs, fdt, fsolve, max_iter, fstop, fincrement, dt):
+        if self.rhs is None:
+            self.rhs = torch.zeros_like(x)
+        x_last = x.clone()
+        dtau = torch.zeros(x.shape[0], dtype=x.dtype, device=x.device)
+        xinc = torch.zeros_like(x)
+        for it in range(1, max_iter + 1):
+            fdt(x, dtau, 1.0)
+            frhs(self.rhs, x, dtau, it, 1.0)
+            res = x_last * (1.0 / dt)
+            res_other = res.clone()
+            res.add_(x, alpha=-1.0 / dt)
+            res.add_(self.rhs)
+            fsolve(x, res, res_other, dtau, dt, 1.0, xinc, it, 1.0)
+            fincrement(x, xinc, 1.0)
+            if fstop(it, res, 1):
+                return it
+        return max_iter
+
+
+def _lstsq(h, e):
+    """Least-squares solve with rank report (HardEigen::EigenLeastSquareSolve semantics)."""
+    y, _, rank, _ = np.linalg.lstsq(h, e, rcond=None)
+    return y, rank
+
+
+class GMRES:
+    """Linear.hpp:11-133 GMRES_LeftPreconditioned on torch vectors."""
+
+    def __init__(self, k_subspace, like):
+        self.k = k_subspace
+        self.V = [torch.zeros_like(like) for _ in range(k_subspace + 1)]
+        self.tmp = torch.zeros_like(like)
+        self.MLb = torch.zeros_like(like)
+
+    def solve(self, FA, FML, fdot, b, x, n_restart, fstop):
+        FML(b, self.MLb)
+        scale = math.sqrt(fdot(self.MLb, self.MLb))
+        h = np.zeros((self.k + 1, self.k))
+        i_restart = 0
+        for i_restart in range(n_restart + 1):
+            FA(x, self.tmp)
+            FML(self.tmp, self.V[0])
+            self.V[0].add_(self.MLb, alpha=-1.0)
+            beta = math.sqrt(fdot(self.V[0], self.V[0]))
+            if fstop(i_restart, beta, scale):
+                break
+            if abs(beta) < VERY_SMALL or i_restart == n_restart:
+                break
+            self.V[0].mul_(-1.0 / beta)
+            j = 0
+            while j < self.k:
+                FA(self.V[j], self.tmp)
+                FML(self.tmp, self.V[j + 1])
+                for i in range(j + 1):
+                    h[i, j] = fdot(self.V[j + 1], self.V[i])
+                for i in range(j + 1):
+                    self.V[j + 1].add_(self.V[i], alpha=-h[i, j])
+                h[j + 1, j] = math.sqrt(fdot(self.V[j + 1], self.V[j + 1]))
+                if h[j + 1, j] < scale * 1e-32:
+                    break
+                self.V[j + 1].mul_(1.0 / h[j + 1, j])
+                j += 1
+            if j < 1:
+                break
+            e = np.zeros(j + 1)
+            e[0] = beta
+            y, rank = _lstsq(h[:j + 1, :j], e)
+            for jj in range(j):
+                x.add_(self.V[jj], alpha=float(y[jj]))
+            if rank < h.shape[1]:
+                break
+        return i_restart < n_restart
+
+
+@dataclass
+class SolverConfig:
+    """Field names follow EulerSolver.hpp (timeMarchControl, convergenceControl, linearSolverControl ...)."""
+    odeCode: int = 0                 # 0 ESDIRK4, 101 SDIRK4, 103 backward Euler (steady)
+    dtImplicit: float = 0.01
+    nTimeStep: int = 100
+    nTimeStepInternal: int = 20
+    rhsThresholdInternal: float = 1e-8
+    CFL: float = 100.0
+    useLocalDt: bool = True
+    nInternalRecStep: int = 1
+    jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi
+    sgsIter: int = 0
+    gmresCode: int = 0               # 0: LU-SGS only, 1: GMRES preconditioned by SGS
+    nGmresSpace: int = 30
+    nGmresIter: int = 1
+    gmresScale: int = 0
+    linear_precision: str = "fp64"   # "fp32": FP32 preconditioner / GMRES inside the FP64 defect correction
+    vr_precision: str = "fp64"       # coefficient precision of the VR sweeps
+    res_history: list = field(default_factory=list)
+
+
+class ImplicitSolver:
+    """The frhs / fdtau / fsolve / fincrement closures of EulerSolver::RunImplicitEuler."""
+
+    def __init__(self, vr, ev, cfg: SolverConfig):
+        self.vr, self.ev, self.cfg = vr, ev, cfg
+        nc = vr.mesh.n_cell
+        nv = ev.nVars
+        self.uRec = vr.BuildURec(nv)
+        self.uRecNew = vr.BuildURec(nv)
+        dev = self.uRec.device
+        self.jd = torch.zeros(nc, dtype=torch.float64, device=dev)
+        self.tmp = torch.zeros((nc, nv), dtype=torch.float64, device=dev)
+        self.gmres = GMRES(cfg.nGmresSpace, self.tmp) if cfg.gmresCode else None
+        self.res0 = None
+        self.n_rhs = 0
+        self.n_sgs = 0
+
+    # EulerSolver.hxx:147-672 (VR sweeps then EvaluateRHS)
+    def frhs(self, crhs, cx, dtau, it, ct):
+        for _ in range(self.cfg.nInternalRecStep):
+            self.vr.DoReconstructionIter(self.uRec, self.uRecNew, cx, putIntoNew=False, precision=self.cfg.vr_precision)
+        self.ev.EvaluateRHS(crhs, cx, self.uRec)
+        self.n_rhs += 1
+
+    # EulerSolver.hxx:674-694
+    def fdtau(self, cx, dtau, alphaDiag):
+        self.ev.EvaluateDt(dtau, cx, self.cfg.CFL, 1e100, self.cfg.useLocalDt)
+        dtau.mul_(1.0 / alphaDiag)
+
+    # EulerSolver.hxx:696-738 without the positivity limiting (AddFixedIncrement with alpha = 1)
+    def fincrement(self, cx, cxInc, alpha):
+        cx.add_(cxInc, alpha=alpha)
+
+    def _sgs_pair(self, alphaDiag, rhs, cx, xinc):
+        """doPrecondition, EulerSolver.hxx:1605-1635: forward then backward sweep."""
+        gs = self.cfg.jacobiCode == 1
+        self.ev.UpdateSGS(alphaDiag, rhs, cx, xinc, self.tmp, self.jd, True, gs, False, want_sum=False)
+        xinc.copy_(self.tmp)
+        self.ev.UpdateSGS(alphaDiag, rhs, cx, xinc, self.tmp, self.jd, False, gs, False, want_sum=False)
+        xinc.copy_(self.tmp)
+        self.n_sgs += 1
+
+    # EulerSolver.hxx:740-997 and solveLinear :1407-1579
+    def fsolve(self, cx, cres, res_other, dtau, dt, alphaDiag, cxInc, it, ct):
+        self.ev.LUSGSMatrixInit(self.jd, dtau, dt, alphaDiag)
+        cxInc.zero_()
+        if self.cfg.gmresCode == 0:
+            self._sgs_pair(alphaDiag, cres, cx, cxInc)
+            for _ in range(self.cfg.sgsIter):
+                self._sgs_pair(alphaDiag, cres, cx, cxInc)
+            return
+        x = torch.zeros_like(cxInc)
+
+        def FA(v, Av):
+            self.ev.LUSGSMatrixVec(alphaDiag, cx, v, self.jd, Av)
+
+        def FML(v, MLv):
+            MLv.zero_()
+            for _ in range(1 + self.cfg.sgsIter):
+                self._sgs_pair(alphaDiag, v, cx, MLv)
+
+        def fdot(a, b):
+            return float(torch.sum(a * b))
+
+        self.gmres.solve(FA, FML, fdot, cres, x, self.cfg.nGmresIter, lambda i, r, rb: False)
+        cxInc.copy_(x)
+
+    def fstop(self, it, res, stage):
+        nrm = self.ev.EvaluateNorm(res, 1, True)
+        r = float(np.linalg.norm(nrm))
+        if it == 1:
+            self.res0 = r
+        self.cfg.res_history.append((stage, it, r))
+        return r <= self.cfg.rhsThresholdInternal * max(self.res0, 1e-300) or it >= self.cfg.nTimeStepInternal
+
+    def run(self, u, n_steps=None, dt=None):
+        cfg = self.cfg
+        ode = ESDIRK(1 if cfg.odeCode == 0 else 0) if cfg.odeCode in (0, 101) else BDF1Stepper()
+        dt = cfg.dtImplicit if dt is None else dt
+        for _ in range(cfg.nTimeStep if n_steps is None else n_steps):
+            ode.step(u, self.frhs, self.fdtau, self.fsolve, cfg.nTimeStepInternal, self.fstop, self.fincrement, dt)
+        return u
