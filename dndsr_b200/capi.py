@@ -43,6 +43,13 @@ class EulerSettings(ctypes.Structure):
     ]
 
 
+class LinearSettings(ctypes.Structure):
+    _fields_ = [
+        ("gmresCode", ctypes.c_int), ("jacobiCode", ctypes.c_int), ("sgsIter", ctypes.c_int), ("nGmresSpace", ctypes.c_int),
+        ("nGmresIter", ctypes.c_int), ("precision", ctypes.c_int), ("useGraph", ctypes.c_int), ("meanScale", ctypes.c_double * 8),
+    ]
+
+
 # every function the header declares, with its ctypes signature
 _P = ctypes.c_void_p
 _PP = ctypes.POINTER(ctypes.c_void_p)
@@ -73,6 +80,9 @@ SIGNATURES = {
     "dndsb_eval_update_sgs": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _D, _P],
     "dndsb_eval_lusgs_matrix_vec": [_P, _d, _P, _P, _P, _P, _P],
     "dndsb_eval_evaluate_norm": [_P, _P, _i, _i, _D, _P],
+    "dndsb_eval_solve_linear": [_P, _P, _d, _P, _d, _P, _P, _P, _P],
+    "dndsb_vr_set_boundary": [_P, _i, _I32, _D, _i, _d, _d],
+    "dndsb_eval_set_bc": [_P, _i, _I32, _D],
     "dndsb_eval_get_array": [_P, ctypes.c_char_p, _D, _l, _I64],
     "dndsb_eval_set_delta_lambda": [_P, _P, _P],
     "dndsb_eval_evaluate_rhs_noalloc": [_P, _P, _P, _P, _P],

@@ -15,6 +15,7 @@ struct dndsb_mesh
 {
     MeshD d;
     std::vector<int32_t> cellColorHost;
+    std::vector<int32_t> bndZoneHost; // zones of the boundary faces, for checking boundary tables
     int64_t nBndFace = 0;
 };
 
@@ -25,12 +26,14 @@ struct dndsb_vr
     VRD vr;
     int *errWord = nullptr;
     bool metrics = false, base = false, coeff = false;
+    int bndNVars = 0; // number of variables of the boundary table's values
 };
 
 struct dndsb_eval
 {
     dndsb_vr *vr = nullptr;
     EvalD e;
+    LinWs *lin = nullptr; // workspace of dndsb_eval_solve_linear
 };
 
 namespace
@@ -187,6 +190,18 @@ extern "C"
             cells[pos[color[c]]++] = (int32_t)c;
         d.nColor = nColor;
         d.colorStart = start;
+        // boundary faces and the cells that own them (in face / cell order)
+        std::vector<int32_t> bFace, bCell;
+        std::vector<char> isB(nCell, 0);
+        for (int64_t f = 0; f < nFace; f++)
+            if (f2c[f * 2 + 1] < 0)
+                bFace.push_back((int32_t)f), isB[f2c[f * 2]] = 1;
+        for (int64_t c = 0; c < nCell; c++)
+            if (isB[c])
+                bCell.push_back((int32_t)c);
+        d.nBndFace = (int64_t)bFace.size(), d.nBndCell = (int64_t)bCell.size();
+        for (int32_t f : bFace)
+            m->bndZoneHost.push_back(faceZone[f]);
         m->cellColorHost = color;
         int rc = 0;
         rc |= upload(&d.coords, coords, nNode * 3);
@@ -201,6 +216,11 @@ extern "C"
         rc |= upload(&d.cellNbr, nbr.data(), nCell * nf);
         rc |= upload(&d.colorCells, cells.data(), nCell);
         rc |= upload(&d.cellColor, color.data(), nCell);
+        if (!bFace.empty())
+        {
+            rc |= upload(&d.bndFace, bFace.data(), (int64_t)bFace.size());
+            rc |= upload(&d.bndCell, bCell.data(), (int64_t)bCell.size());
+        }
         if (rc)
         {
             dndsb_mesh_destroy(m);
@@ -216,7 +236,8 @@ extern "C"
             return DNDSB_OK;
         MeshD &d = m->d;
         for (void *p : {(void *)d.coords, (void *)d.cell2node, (void *)d.cellShift, (void *)d.face2node, (void *)d.faceShift, (void *)d.face2cell,
-                        (void *)d.faceZone, (void *)d.facePShift, (void *)d.cell2face, (void *)d.cellNbr, (void *)d.colorCells, (void *)d.cellColor})
+                        (void *)d.faceZone, (void *)d.facePShift, (void *)d.cell2face, (void *)d.cellNbr, (void *)d.colorCells, (void *)d.cellColor,
+                        (void *)d.bndFace, (void *)d.bndCell})
             dev_free(p);
         delete m;
         return DNDSB_OK;
@@ -268,7 +289,7 @@ extern "C"
                         (void *)g.smoothRatio, (void *)g.faceArea, (void *)g.faceCent, (void *)g.faceJDet, (void *)g.facePP, (void *)g.faceNorm,
                         (void *)g.faceMeanNorm, (void *)g.cellQw, (void *)g.faceQw, (void *)v->vr.baseMoment, (void *)v->vr.faceWeight,
                         (void *)v->vr.faceL, (void *)v->vr.AAInvB, (void *)v->vr.AInvb, (void *)v->vr.matA, (void *)v->vr.AAInvB32,
-                        (void *)v->vr.AInvb32, (void *)v->errWord})
+                        (void *)v->vr.AInvb32, (void *)v->errWord, (void *)v->vr.bnd.type, (void *)v->vr.bnd.val})
             dev_free(p);
         delete v;
         return DNDSB_OK;
@@ -366,12 +387,45 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: recordInc needs putIntoNew"); // _Reconstruction.hxx:502
         if (uRec == uRecNew)
             return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: uRec and uRecNew must differ");
-        if (v->mesh->nBndFace > 0)
-            return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_do_reconstruction_iter: boundary faces need a BC table (not yet accepted)");
-        int rc = vr_iter(v->mesh->d, v->vr, nVars, uRec, uRecNew, u, recordInc, uRecIsZero, precision, S(stream));
+        if (v->mesh->nBndFace > 0 && v->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: the mesh has boundary faces; set their boundary table first");
+        if (v->vr.bnd.nZone > 0 && nVars != v->bndNVars)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: nVars differs from the boundary table's");
+        int rc = vr_iter(v->mesh->d, v->g, v->vr, nVars, uRec, uRecNew, u, recordInc, uRecIsZero, precision, S(stream));
         if (rc == ST_OK && !putIntoNew && !recordInc)
             rc = vr_swap(v->mesh->d.nCell * v->vr.R * nVars, uRec, uRecNew, S(stream));
         return status_msg(rc, "dndsb_vr_do_reconstruction_iter");
+    }
+
+    int dndsb_vr_set_boundary(dndsb_vr *v, int nZone, const int32_t *type, const double *value, int nVars, double gamma, double Rgas)
+    {
+        if (!v || nZone < 0 || (nZone > 0 && (!type || !value)) || nVars < 1 || nVars > 8 || !(gamma > 1) || !(Rgas > 0))
+            return fail(DNDSB_E_BADARG, "dndsb_vr_set_boundary: bad argument");
+        const dndsb_mesh *m = v->mesh;
+        for (int z = 0; z < nZone; z++)
+        {
+            int t = type[z];
+            if (t != 0 && t != BC_FAR && t != BC_WALL && t != BC_WALL_INVIS && t != BC_WALL_ISOTHERMAL && t != BC_OUT && t != BC_OUTP &&
+                t != BC_IN && t != BC_SYM)
+                return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_set_boundary: boundary type " + std::to_string(t) + " is not available");
+        }
+        for (int32_t z : m->bndZoneHost) // every boundary face needs a zone with a boundary type
+            if (z < 0 || z >= nZone || type[z] == 0)
+                return fail(DNDSB_E_BADARG, "dndsb_vr_set_boundary: boundary zone " + std::to_string(z) + " has no boundary type");
+        std::vector<double> val(std::max(nZone, 1) * 8, 0.0);
+        for (int z = 0; z < nZone; z++)
+            for (int i = 0; i < nVars; i++)
+                val[z * 8 + i] = value[z * nVars + i];
+        BoundaryD &b = v->vr.bnd;
+        dev_free(b.type);
+        dev_free(b.val);
+        b.type = nullptr, b.val = nullptr, b.nZone = 0;
+        std::vector<int32_t> ty(type, type + nZone);
+        if (nZone > 0 && (upload(&b.type, ty.data(), nZone) || upload(&b.val, val.data(), (int64_t)nZone * 8)))
+            return cuda_fail("dndsb_vr_set_boundary");
+        b.nZone = nZone, b.gamma = gamma, b.Rgas = Rgas;
+        v->bndNVars = nVars;
+        return DNDSB_OK;
     }
 
     int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s)
@@ -380,8 +434,6 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_create: null argument");
         if (s->nVars != 5 && s->nVars != 6)
             return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_create: nVars must be 5 (NS) or 6 (NS_SA)");
-        if (vr->mesh->nBndFace > 0)
-            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_create: boundary faces need a BC table (not yet accepted)");
         auto *e = new dndsb_eval();
         e->vr = vr;
         EulerSettingsD &d = e->e.s;
@@ -404,9 +456,24 @@ extern "C"
             dndsb_eval_destroy(e);
             return cuda_fail("dndsb_eval_create");
         }
+        if (fast_geometry(m, vr->g, vr->vr, e->e, 0) != ST_OK)
+        {
+            dndsb_eval_destroy(e);
+            return cuda_fail("dndsb_eval_create");
+        }
         cudaMemset(e->e.deltaLambdaCell, 0, sizeof(real) * m.nCell);
         cudaMemset(e->e.lambdaFace, 0, sizeof(real) * m.nFace);
         *out = e;
+        return DNDSB_OK;
+    }
+
+    int dndsb_eval_set_bc(dndsb_eval *e, int nZone, const int32_t *type, const double *value)
+    {
+        if (!e)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_bc: null argument");
+        int rc = dndsb_vr_set_boundary(e->vr, nZone, type, value, e->e.s.nVars, e->e.s.gamma, e->e.s.Rgas);
+        if (rc != DNDSB_OK)
+            return rc;
         return DNDSB_OK;
     }
 
@@ -415,8 +482,10 @@ extern "C"
         if (!e)
             return DNDSB_OK;
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
-                        (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord})
+                        (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
+                        (void *)e->e.facePt, (void *)e->e.cellPar})
             dev_free(p);
+        linws_free(e->lin);
         delete e;
         return DNDSB_OK;
     }
@@ -443,6 +512,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: null argument");
         if (!e->vr->coeff)
             return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: the mesh has boundary faces; call dndsb_eval_set_bc first");
         return status_msg(eval_rhs(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, u, uRec, rhs, nullptr, S(stream)), "dndsb_eval_evaluate_rhs");
     }
 
@@ -472,6 +543,26 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_vec: null argument");
         return status_msg(lusgs_matvec(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, uInc, jdiag, AuInc, S(stream)),
                           "dndsb_eval_lusgs_matrix_vec");
+    }
+
+    int dndsb_eval_solve_linear(dndsb_eval *e, const dndsb_linear_settings *ls, double alphaDiag, const double *dTau, double dt,
+                                const double *u, const double *rhs, double *xInc, void *stream)
+    {
+        if (!e || !ls || !dTau || !u || !rhs || !xInc)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: null argument");
+        LinSettings s;
+        s.gmresCode = ls->gmresCode, s.jacobiCode = ls->jacobiCode, s.sgsIter = ls->sgsIter;
+        s.nGmresSpace = ls->nGmresSpace, s.nGmresIter = ls->nGmresIter, s.precision = ls->precision, s.useGraph = ls->useGraph;
+        for (int v = 0; v < 8; v++)
+        {
+            double ms = ls->meanScale[v] > 0 ? ls->meanScale[v] : 1.0;
+            double inv = 1.0 / (ms + 1e-200);
+            s.scale2[v] = inv * inv;
+        }
+        int rc = linear_solve(e->vr->mesh->d, e->vr->g, e->e, e->lin, s, alphaDiag, dTau, dt, u, rhs, xInc, S(stream));
+        if (rc == ST_BADARG)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..1, nGmresSpace 1..32, precision 0..1");
+        return status_msg(rc, "dndsb_eval_solve_linear");
     }
 
     int dndsb_eval_evaluate_norm(dndsb_eval *e, const double *x, int P, int volWise, double *resHost, void *stream)

@@ -600,14 +600,14 @@ DNDSB_HD void roe_entropy_fix(int es, real aL, real aR, real aAve, real uL, real
 
 // Approximate Riemann flux F(UL,UR; ULm,URm) . n for the 5 Euler variables.
 // Returns false when a state is non-physical (the caller records an error).
-DNDSB_HD bool riemann_flux(int rs, const real *UL, const real *UR, const real *ULm, const real *URm, const real *n, real gamma,
-                           real dLambda, real fixScale, real incFScale, real F[5], real &lam0, real &lam123, real &lam4)
+// The Roe averages r come from the cell-mean states (Gas.hpp:229-259) and are
+// shared by all Gauss points of a face.
+DNDSB_HD bool riemann_flux_pre(int rs, const real *UL, const real *UR, const RoeAvg &r, const real *n, real gamma, real dLambda,
+                               real fixScale, real incFScale, real F[5], real &lam0, real &lam123, real &lam4)
 {
     real FL[5], FR[5], pL, pR, aL2, aR2;
     phys_flux(UL, n, gamma, FL, pL, aL2);
     phys_flux(UR, n, gamma, FR, pR, aR2);
-    RoeAvg r;
-    roe_average(ULm, URm, gamma, r);
     bool ok = UL[0] > 0 && UR[0] > 0 && r.asqr > 0;
     real vRoe0 = dot3(r.v, n);
     lam0 = fabs(vRoe0 - r.a), lam123 = fabs(vRoe0), lam4 = fabs(vRoe0 + r.a);
@@ -698,6 +698,14 @@ DNDSB_HD bool riemann_flux(int rs, const real *UL, const real *UR, const real *U
     for (int i = 0; i < 5; i++)
         F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * incF[i];
     return ok;
+}
+
+DNDSB_HD bool riemann_flux(int rs, const real *UL, const real *UR, const real *ULm, const real *URm, const real *n, real gamma,
+                           real dLambda, real fixScale, real incFScale, real F[5], real &lam0, real &lam123, real &lam4)
+{
+    RoeAvg r;
+    roe_average(ULm, URm, gamma, r);
+    return riemann_flux_pre(rs, UL, UR, r, n, gamma, dLambda, fixScale, incFScale, F, lam0, lam123, lam4);
 }
 
 // Gas.hpp:1677-1698 GradientCons2Prim_IdealGas; G and GP are [3][NV]

@@ -450,9 +450,12 @@ int check(cudaStream_t st, int *errWord, bool syncErr)
 }
 } // namespace
 
-int vr_iter(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
-            int useFP32, cudaStream_t st)
+int vr_iter(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc,
+            int uRecIsZero, int useFP32, cudaStream_t st)
 {
+    // interior faces (tuned kernel when one is instantiated), then the boundary faces
+    if (vr_iter_fast(m, vr, nv, uRec, uRecNew, u, recordInc, uRecIsZero, useFP32, st) == ST_OK)
+        return vr_iter_bc(m, g, vr, nv, uRec, uRecNew, u, recordInc, uRecIsZero, useFP32, st);
     real relax = vr.s.jacobiRelax;
 #define DNDSB_VRJ(RR, NVV)                                                                                                             \
     do                                                                                                                                 \
@@ -498,7 +501,9 @@ int vr_iter(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecN
     }
 #undef DNDSB_VRJ_NV
 #undef DNDSB_VRJ
-    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+    if (last_error() != cudaSuccess)
+        return ST_CUDA;
+    return vr_iter_bc(m, g, vr, nv, uRec, uRecNew, u, recordInc, uRecIsZero, useFP32, st);
 }
 
 int vr_swap(int64_t n, real *a, real *b, cudaStream_t st)
@@ -515,6 +520,17 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
     int nv = ev.s.nVars;
     if (nv != 5)
         return ST_UNSUPPORTED;
+    int frc = rhs_face_fast(m, g, vr, ev, u, uRec, ff, st);
+    if (frc == ST_CUDA)
+        return ST_CUDA;
+    if (frc == ST_OK)
+    {
+        int brc = rhs_bc(m, g, vr, ev, u, uRec, ff, st);
+        if (brc != ST_OK)
+            return brc;
+        DNDSB_LAUNCH(k_rhs_gather<5>, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ff, rhs);
+        return check(st, ev.errWord, true);
+    }
 #define DNDSB_RF(D, PP) DNDSB_LAUNCH((k_rhs_face<D, PP, 5>), m.nFace, 128, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord)
     if (m.dim == 2)
     {
@@ -535,6 +551,9 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
             DNDSB_RF(3, 3);
     }
 #undef DNDSB_RF
+    int brc = rhs_bc(m, g, vr, ev, u, uRec, ff, st);
+    if (brc != ST_OK)
+        return brc;
     DNDSB_LAUNCH(k_rhs_gather<5>, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ff, rhs);
     return check(st, ev.errWord, true);
 }

@@ -1,0 +1,584 @@
+// Native implicit linear solve: LU-SGS sweeps and left-preconditioned
+// restarted GMRES in FP64 or FP32, with every scalar kept on the device.
+//
+// Replaces EulerSolver::solveLinear / doPrecondition
+// (src/Euler/EulerSolver.hxx:1407-1579, 1605-1658) together with
+// LUSGSMatrixInit (src/Euler/EulerEvaluator.hxx:37-159, scalar Jacobian),
+// UpdateSGS (:550-693), LUSGSMatrixVec (:175-274) and
+// GMRES_LeftPreconditioned::solve (src/Solver/Linear.hpp:46-133).
+//
+// Layout.  Inside the solve every cell vector is stored in colour-position
+// order (position p holds cell colorCells[p]), so one colour class is one
+// contiguous range and "neighbour already updated in this sweep" is a range
+// test on the neighbour's position.  Per (position, face slot) the operator
+// keeps {w*n, w*lambda} with w = alpha * A_f / (2 V_c) as one 4-vector and the
+// neighbour's position; per position the scalar diagonal.  The state u is
+// converted once per solve into the solve precision T.
+//
+// Precision.  T = double reproduces the FP64 operators; T = float is the
+// FP32 preconditioner of the mixed-precision defect correction (the caller's
+// residual and state update stay FP64).  Dot products accumulate in FP64 in
+// both cases.  Reductions use a fixed partition and fixed trees, so results
+// are bitwise reproducible.
+//
+// GMRES scalars (Hessenberg, norms, least-squares solution, breakdown index)
+// never leave the device: the whole solve is a fixed kernel sequence and is
+// captured once into a CUDA graph that later solves replay.
+#include "solver.cuh"
+
+namespace dndsb
+{
+namespace
+{
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float>
+{
+    using type = float4;
+};
+template <>
+struct Vec4<double>
+{
+    using type = double4;
+};
+
+// ---------------------------------------------------------------------------
+// operator build: LUSGSMatrixInit (EulerEvaluator.hxx:37-159) + packing
+// ---------------------------------------------------------------------------
+template <typename T, int NV>
+DNDSB_GLOBAL void k_sgsop_build(MeshD m, GeomD g, const real *__restrict__ lamFace, const real *__restrict__ dTau, real dt, real alphaDiag,
+                                const real *__restrict__ u, const int32_t *__restrict__ cellPos, int32_t *nbrPos,
+                                typename Vec4<T>::type *op, T *jd, T *uT)
+{
+    DNDSB_KERNEL_LOOP(p, m.nCell)
+    {
+        int64_t c = m.colorCells[p];
+        real iv = 1.0 / g.vol[c];
+        real cf = 0.5 * alphaDiag / g.vol[c];
+        real fp = 1.0 / dTau[c] + 1.0 / dt;
+        for (int k = 0; k < m.nf; k++)
+        {
+            int pk = m.cell2face[c * m.nf + k];
+            int64_t f = pk >> 1;
+            real sg = (pk & 1) ? -1.0 : 1.0;
+            fp += (0.5 * alphaDiag) * g.faceArea[f] * lamFace[f] * iv;
+            real w = cf * g.faceArea[f];
+            typename Vec4<T>::type o4;
+            o4.x = (T)(w * g.faceMeanNorm[f * 3] * sg);
+            o4.y = (T)(w * g.faceMeanNorm[f * 3 + 1] * sg);
+            o4.z = (T)(w * g.faceMeanNorm[f * 3 + 2] * sg);
+            o4.w = (T)(w * lamFace[f]);
+            op[p * m.nf + k] = o4;
+            int o = m.cellNbr[c * m.nf + k];
+            nbrPos[p * m.nf + k] = o < 0 ? -1 : cellPos[o];
+        }
+        jd[p] = (T)fp;
+        for (int v = 0; v < NV; v++)
+            uT[p * NV + v] = (T)u[c * NV + v];
+    }
+}
+
+// natural order FP64 -> position order T, and back
+template <typename T, int NV>
+DNDSB_GLOBAL void k_gather_T(int64_t n, const int32_t *__restrict__ pos2cell, const real *__restrict__ x, T *y)
+{
+    DNDSB_KERNEL_LOOP(p, n)
+    {
+        int64_t c = pos2cell[p];
+        for (int v = 0; v < NV; v++)
+            y[p * NV + v] = (T)x[c * NV + v];
+    }
+}
+
+template <typename T, int NV>
+DNDSB_GLOBAL void k_scatter_T(int64_t n, const int32_t *__restrict__ pos2cell, const T *__restrict__ y, real *x)
+{
+    DNDSB_KERNEL_LOOP(p, n)
+    {
+        int64_t c = pos2cell[p];
+        for (int v = 0; v < NV; v++)
+            x[c * NV + v] = (real)y[p * NV + v];
+    }
+}
+
+template <typename T>
+DNDSB_GLOBAL void k_zero_T(int64_t n, T *x)
+{
+    DNDSB_KERNEL_LOOP(i, n)
+    x[i] = (T)0;
+}
+
+template <typename T>
+DNDSB_GLOBAL void k_copy_T(int64_t n, const T *__restrict__ a, T *b)
+{
+    DNDSB_KERNEL_LOOP(i, n)
+    b[i] = a[i];
+}
+
+// scaled flux-increment Jacobian times dU (EulerEvaluator.hpp:1100-1158 with
+// Gas.hpp:462-513), minus w*lambda*dU; o4 = {w n, w lambda}
+template <typename T, int NV>
+DNDSB_D void jac_du_scaled(const T *U, const T *dU, const typename Vec4<T>::type &o4, T gamma, T *dF)
+{
+    T ir = T(1) / U[0];
+    T v0 = U[1] * ir, v1 = U[2] * ir, v2 = U[3] * ir;
+    T p = (gamma - T(1)) * (U[4] - U[0] * T(0.5) * (v0 * v0 + v1 * v1 + v2 * v2));
+    T dv0 = (dU[1] - U[1] * ir * dU[0]) * ir;
+    T dv1 = (dU[2] - U[2] * ir * dU[0]) * ir;
+    T dv2 = (dU[3] - U[3] * ir * dU[0]) * ir;
+    T dp = (gamma - T(1)) * (dU[4] - T(0.5) * (dU[1] * v0 + dU[2] * v1 + dU[3] * v2 + U[1] * dv0 + U[2] * dv1 + U[3] * dv2));
+    T vn = v0 * o4.x + v1 * o4.y + v2 * o4.z;
+    T dvn = dv0 * o4.x + dv1 * o4.y + dv2 * o4.z;
+    dF[0] = dU[1] * o4.x + dU[2] * o4.y + dU[3] * o4.z;
+    dF[1] = dU[1] * vn + U[1] * dvn + o4.x * dp;
+    dF[2] = dU[2] * vn + U[2] * dvn + o4.y * dp;
+    dF[3] = dU[3] * vn + U[3] * dvn + o4.z * dp;
+    dF[4] = (dU[4] + dp) * vn + (U[4] + p) * dvn;
+    for (int j = 5; j < NV; j++)
+        dF[j] = dU[j] * vn + U[j] * dvn;
+    for (int j = 0; j < NV; j++)
+        dF[j] -= o4.w * dU[j];
+}
+
+// one colour class of a forward / backward sweep (UpdateSGS, EulerEvaluator.hxx:550-693)
+template <typename T, int NV, int NF>
+DNDSB_GLOBAL void k_sgs_pos(int64_t pBeg, int64_t pEnd, const int32_t *__restrict__ nbrPos, const typename Vec4<T>::type *__restrict__ op,
+                            const T *__restrict__ jd, const T *__restrict__ uT, const T *__restrict__ rhs, const T *__restrict__ xOld,
+                            T *xNew, T gamma, int forward, int gsUpdate, int uIncIsZero)
+{
+    DNDSB_KERNEL_LOOP(ii, pEnd - pBeg)
+    {
+        int64_t p = pBeg + ii;
+        T buf[NV];
+        for (int v = 0; v < NV; v++)
+            buf[v] = rhs[p * NV + v];
+#pragma unroll
+        for (int k = 0; k < NF; k++)
+        {
+            int q = nbrPos[p * NF + k];
+            if (q < 0 || q == p)
+                continue;
+            bool useNew = gsUpdate && (forward ? q < pBeg : q >= pEnd);
+            if (uIncIsZero && !useNew)
+                continue;
+            typename Vec4<T>::type o4 = op[p * NF + k];
+            const T *dU = (useNew ? xNew : xOld) + (int64_t)q * NV;
+            T dF[NV];
+            jac_du_scaled<T, NV>(uT + (int64_t)q * NV, dU, o4, gamma, dF);
+            for (int v = 0; v < NV; v++)
+                buf[v] -= dF[v];
+        }
+        T id = T(1) / jd[p];
+        for (int v = 0; v < NV; v++)
+            xNew[p * NV + v] = buf[v] * id;
+    }
+}
+
+// LUSGSMatrixVec (EulerEvaluator.hxx:175-274)
+template <typename T, int NV, int NF>
+DNDSB_GLOBAL void k_matvec_pos(int64_t n, const int32_t *__restrict__ nbrPos, const typename Vec4<T>::type *__restrict__ op,
+                               const T *__restrict__ jd, const T *__restrict__ uT, const T *__restrict__ x, T *Ax, T gamma)
+{
+    DNDSB_KERNEL_LOOP(p, n)
+    {
+        T buf[NV];
+        for (int v = 0; v < NV; v++)
+            buf[v] = 0;
+#pragma unroll
+        for (int k = 0; k < NF; k++)
+        {
+            int q = nbrPos[p * NF + k];
+            if (q < 0)
+                continue;
+            typename Vec4<T>::type o4 = op[p * NF + k];
+            T dF[NV];
+            jac_du_scaled<T, NV>(uT + (int64_t)q * NV, x + (int64_t)q * NV, o4, gamma, dF);
+            for (int v = 0; v < NV; v++)
+                buf[v] -= dF[v];
+        }
+        for (int v = 0; v < NV; v++)
+            Ax[p * NV + v] = jd[p] * x[p * NV + v] - buf[v];
+    }
+}
+
+// GMRES bookkeeping kernels on device scalars.  sc layout: [0] scale = |M b|,
+// [1] beta, [2] number of valid Arnoldi columns, [8 ...] least-squares y.
+constexpr int kScY = 8;
+
+// v = -(w - MLb) / beta  with beta = |w - MLb| already in sc[1]; x = 0 start uses w = 0
+template <typename T>
+DNDSB_GLOBAL void k_gmres_v0(int64_t n, const T *__restrict__ w, const T *__restrict__ MLb, T *v0, const real *sc, int wIsZero)
+{
+    real beta = sc[1];
+    real s = beta > kVerySmall ? -1.0 / beta : 0.0;
+    DNDSB_KERNEL_LOOP(i, n)
+    {
+        real d = (wIsZero ? 0.0 : (real)w[i]) - (real)MLb[i];
+        v0[i] = (T)(d * s);
+    }
+}
+
+// v_{j+1} = w / h[j+1][j], or 0 after a breakdown; records the first breakdown
+template <typename T>
+DNDSB_GLOBAL void k_gmres_next(int64_t n, T *w, const real *hcol, int j, real *sc)
+{
+    real h = hcol[j + 1];
+    bool broken = !(h > sc[0] * 1e-32) || sc[2] <= j;
+    real s = broken ? 0.0 : 1.0 / h;
+    DNDSB_KERNEL_LOOP(i, n)
+    w[i] = (T)((real)w[i] * s);
+    if (broken && blockIdx.x == 0 && threadIdx.x == 0 && sc[2] > j)
+        sc[2] = j;
+}
+
+// least squares  min |beta e1 - H y|  by Givens rotations on the Hessenberg
+// (HardEigen::EigenLeastSquareSolve on the (j+1) x j leading block)
+DNDSB_GLOBAL void k_gmres_lsq(int k, const real *H, real *sc)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0)
+        return;
+    int nv = (int)sc[2];
+    if (nv > k)
+        nv = k;
+    real R[33 * 32];
+    real gv[33];
+    for (int i = 0; i <= nv; i++)
+        gv[i] = i == 0 ? sc[1] : 0.0;
+    for (int jj = 0; jj < nv; jj++)
+        for (int i = 0; i <= nv; i++)
+            R[i * 32 + jj] = i <= jj + 1 ? H[jj * (k + 1) + i] : 0.0;
+    for (int jj = 0; jj < nv; jj++)
+    {
+        real a = R[jj * 32 + jj], b = R[(jj + 1) * 32 + jj];
+        real r = sqrt(a * a + b * b);
+        real c = r > 0 ? a / r : 1.0, s = r > 0 ? b / r : 0.0;
+        for (int l = jj; l < nv; l++)
+        {
+            real x0 = R[jj * 32 + l], x1 = R[(jj + 1) * 32 + l];
+            R[jj * 32 + l] = c * x0 + s * x1;
+            R[(jj + 1) * 32 + l] = -s * x0 + c * x1;
+        }
+        real g0 = gv[jj], g1 = gv[jj + 1];
+        gv[jj] = c * g0 + s * g1;
+        gv[jj + 1] = -s * g0 + c * g1;
+    }
+    real rmax = 0;
+    for (int jj = 0; jj < nv; jj++)
+        rmax = dmax(rmax, fabs(R[jj * 32 + jj]));
+    for (int jj = nv - 1; jj >= 0; jj--)
+    {
+        real acc = gv[jj];
+        for (int l = jj + 1; l < nv; l++)
+            acc -= R[jj * 32 + l] * sc[kScY + l];
+        real d = R[jj * 32 + jj];
+        sc[kScY + jj] = fabs(d) > 1e-14 * rmax ? acc / d : 0.0;
+    }
+    for (int jj = nv; jj < k; jj++)
+        sc[kScY + jj] = 0;
+}
+
+// x += sum_i y_i v_i over the valid columns
+template <typename T>
+DNDSB_GLOBAL void k_gmres_update(int64_t n, int k, const T *__restrict__ V, const real *__restrict__ sc, T *x)
+{
+    int nv = (int)sc[2];
+    if (nv > k)
+        nv = k;
+    DNDSB_KERNEL_LOOP(i, n)
+    {
+        real acc = (real)x[i];
+        for (int jj = 0; jj < nv; jj++)
+            acc += sc[kScY + jj] * (real)V[jj * n + i];
+        x[i] = (T)acc;
+    }
+}
+
+DNDSB_GLOBAL void k_gmres_reset(real *sc, int k)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        sc[2] = k;
+}
+
+DNDSB_GLOBAL void k_copy_scalar(const real *a, real *b)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *b = *a;
+}
+} // namespace
+
+// workspace owned by an evaluator handle
+struct LinWs
+{
+    int prec = -1, k = 0, nv = 0, nf = 0;
+    int64_t nCell = 0;
+    int32_t *cellPos = nullptr, *nbrPos = nullptr;
+    void *op = nullptr, *jd = nullptr, *uT = nullptr, *rhsT = nullptr, *x = nullptr, *tmp = nullptr, *tmp2 = nullptr, *MLb = nullptr,
+         *V = nullptr;
+    real *H = nullptr, *sc = nullptr, *s2 = nullptr, *red = nullptr;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t evIn = nullptr, evOut = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    LinSettings key{};
+    bool keyValid = false;
+};
+
+void linws_free(LinWs *w)
+{
+    if (!w)
+        return;
+    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
+                    (void *)w->sc, (void *)w->s2, (void *)w->red})
+        dev_free(p);
+    graph_free(w->graph);
+    stream_free(w->cs);
+    event_free(w->evIn);
+    event_free(w->evOut);
+    delete w;
+}
+
+namespace
+{
+bool same_key(const LinSettings &a, const LinSettings &b)
+{
+    if (a.gmresCode != b.gmresCode || a.jacobiCode != b.jacobiCode || a.sgsIter != b.sgsIter || a.nGmresSpace != b.nGmresSpace ||
+        a.nGmresIter != b.nGmresIter || a.precision != b.precision)
+        return false;
+    return true;
+}
+
+int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv)
+{
+    int k = ls.gmresCode ? ls.nGmresSpace : 0;
+    size_t es = ls.precision ? sizeof(float) : sizeof(double);
+    if (w && w->prec == ls.precision && w->k >= k && w->nv == nv && w->nCell == m.nCell)
+        return ST_OK;
+    linws_free(w);
+    w = new LinWs();
+    w->prec = ls.precision, w->k = k, w->nv = nv, w->nf = m.nf, w->nCell = m.nCell;
+    int64_t n = m.nCell * nv;
+    bool ok = dev_alloc((void **)&w->cellPos, sizeof(int32_t) * m.nCell) == cudaSuccess &&
+              dev_alloc((void **)&w->nbrPos, sizeof(int32_t) * m.nCell * m.nf) == cudaSuccess &&
+              dev_alloc(&w->op, 4 * es * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->jd, es * m.nCell) == cudaSuccess &&
+              dev_alloc(&w->uT, es * n) == cudaSuccess && dev_alloc(&w->rhsT, es * n) == cudaSuccess &&
+              dev_alloc(&w->x, es * n) == cudaSuccess && dev_alloc(&w->tmp, es * n) == cudaSuccess &&
+              dev_alloc(&w->tmp2, es * n) == cudaSuccess && dev_alloc(&w->MLb, es * n) == cudaSuccess &&
+              dev_alloc(&w->V, es * n * (k + 1)) == cudaSuccess &&
+              dev_alloc((void **)&w->H, sizeof(real) * (k + 1) * (k > 0 ? k : 1)) == cudaSuccess &&
+              dev_alloc((void **)&w->sc, sizeof(real) * (kScY + 40)) == cudaSuccess &&
+              dev_alloc((void **)&w->s2, sizeof(real) * 8) == cudaSuccess &&
+              dev_alloc((void **)&w->red, sizeof(real) * kRedBufLenK) == cudaSuccess;
+    if (!ok || stream_create(&w->cs) != cudaSuccess || event_create(&w->evIn) != cudaSuccess || event_create(&w->evOut) != cudaSuccess)
+    {
+        linws_free(w);
+        w = nullptr;
+        return ST_CUDA;
+    }
+    // position of every cell in the colour order
+    std::vector<int32_t> pos2cell(m.nCell), pos(m.nCell);
+    d2h(pos2cell.data(), m.colorCells, sizeof(int32_t) * m.nCell, nullptr);
+    if (dev_sync(nullptr) != cudaSuccess)
+        return ST_CUDA;
+    for (int64_t p = 0; p < m.nCell; p++)
+        pos[pos2cell[p]] = (int32_t)p;
+    h2d(w->cellPos, pos.data(), sizeof(int32_t) * m.nCell, nullptr);
+    return dev_sync(nullptr) == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+template <typename T, int NV, int NF>
+struct Solve
+{
+    const MeshD &m;
+    LinWs &w;
+    const LinSettings &ls;
+    T gamma;
+    cudaStream_t st;
+    int64_t n() const { return m.nCell * NV; }
+    using T4 = typename Vec4<T>::type;
+    T *V(int i) const { return (T *)w.V + (int64_t)i * n(); }
+
+    // one colour sweep over all classes; result in xNew
+    void sweep(const T *rhs, const T *xOld, T *xNew, bool forward, bool gs, bool zeroIn) const
+    {
+        if (!gs)
+        {
+            auto kern = k_sgs_pos<T, NV, NF>;
+            DNDSB_LAUNCH(kern, m.nCell, 128, st, 0, m.nCell, w.nbrPos, (const T4 *)w.op, (const T *)w.jd,
+                         (const T *)w.uT, rhs, xOld, xNew, gamma, (int)forward, 0, (int)zeroIn);
+            return;
+        }
+        auto kern = k_sgs_pos<T, NV, NF>;
+        for (int ci = 0; ci < m.nColor; ci++)
+        {
+            int col = forward ? ci : m.nColor - 1 - ci;
+            int64_t b = m.colorStart[col], e = m.colorStart[col + 1];
+            DNDSB_LAUNCH(kern, e - b, 128, st, b, e, w.nbrPos, (const T4 *)w.op, (const T *)w.jd, (const T *)w.uT, rhs,
+                         xOld, xNew, gamma, (int)forward, 1, (int)zeroIn);
+        }
+    }
+
+    // doPrecondition (EulerSolver.hxx:1605-1635): forward then backward sweep; x in, x out (ping-pong through tmp2)
+    void sgs_pair(const T *rhs, T *x, bool zeroIn) const
+    {
+        bool gs = ls.jacobiCode == 1;
+        sweep(rhs, x, (T *)w.tmp2, true, gs, zeroIn);
+        sweep(rhs, (T *)w.tmp2, x, false, gs, false);
+    }
+
+    // the GMRES preconditioner: MLx = (1 + sgsIter) SGS pairs from zero
+    void FML(const T *b, T *MLx) const
+    {
+        for (int i = 0; i <= ls.sgsIter; i++)
+            sgs_pair(b, MLx, i == 0);
+    }
+
+    void FA(const T *x, T *Ax) const
+    {
+        auto kern = k_matvec_pos<T, NV, NF>;
+        DNDSB_LAUNCH(kern, m.nCell, 128, st, m.nCell, w.nbrPos, (const T4 *)w.op, (const T *)w.jd, (const T *)w.uT, x,
+                     Ax, gamma);
+    }
+
+    void body() const
+    {
+        T *x = (T *)w.x;
+        const T *b = (const T *)w.rhsT;
+        int64_t nn = n();
+        DNDSB_LAUNCH(k_zero_T<T>, nn, 256, st, nn, x);
+        bool xZero = true;
+        if (ls.gmresCode == 0 || ls.gmresCode == 2)
+        {
+            // solveLinear gmresCode 0/2 (EulerSolver.hxx:1462-1517): (1 + sgsIter) SGS pairs
+            for (int i = 0; i <= ls.sgsIter; i++)
+                sgs_pair(b, x, i == 0);
+            xZero = false;
+        }
+        if (ls.gmresCode == 0)
+            return;
+        // GMRES_LeftPreconditioned::solve (Linear.hpp:46-133)
+        int k = ls.nGmresSpace;
+        T *MLb = (T *)w.MLb, *tmp = (T *)w.tmp;
+        FML(b, MLb);
+        krylov_norm(prec(), nn, NV, MLb, w.s2, w.red, w.sc + 0, st); // scale
+        for (int r = 0; r < ls.nGmresIter; r++)
+        {
+            // V0 = M (A x) - M b; beta = |V0|; V0 = -V0 / beta
+            if (xZero)
+            {
+                DNDSB_LAUNCH(k_copy_scalar, 1, 32, st, w.sc + 0, w.sc + 1);
+                DNDSB_LAUNCH(k_gmres_v0<T>, nn, 256, st, nn, (const T *)nullptr, MLb, V(0), w.sc, 1);
+            }
+            else
+            {
+                FA(x, tmp);
+                FML(tmp, V(0));
+                krylov_diff_norm(prec(), nn, NV, V(0), MLb, w.s2, w.red, w.sc + 1, st);
+                DNDSB_LAUNCH(k_gmres_v0<T>, nn, 256, st, nn, V(0), MLb, V(0), w.sc, 0);
+            }
+            DNDSB_LAUNCH(k_gmres_reset, 1, 32, st, w.sc, k);
+            for (int j = 0; j < k; j++)
+            {
+                FA(V(j), tmp);
+                FML(tmp, V(j + 1));
+                real *hcol = w.H + (int64_t)j * (k + 1);
+                // classical Gram-Schmidt: h = V^T w, w -= V h, h[j+1] = |w|
+                krylov_mdot(prec(), nn, NV, j + 1, w.V, V(j + 1), w.s2, w.red, hcol, st);
+                krylov_maxpy_norm(prec(), nn, NV, j + 1, w.V, hcol, V(j + 1), w.s2, w.red, hcol + j + 1, st);
+                DNDSB_LAUNCH(k_gmres_next<T>, nn, 256, st, nn, V(j + 1), hcol, j, w.sc);
+            }
+            DNDSB_LAUNCH(k_gmres_lsq, 1, 32, st, k, w.H, w.sc);
+            DNDSB_LAUNCH(k_gmres_update<T>, nn, 256, st, nn, k, (const T *)w.V, w.sc, x);
+            xZero = false;
+        }
+    }
+    static int prec() { return sizeof(T) == 4 ? 1 : 0; }
+};
+
+template <typename T, int NV, int NF>
+int run(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
+        const real *u, const real *rhs, real *xInc, cudaStream_t st)
+{
+    using T4 = typename Vec4<T>::type;
+    // the caller's stream -> the solver's stream
+    event_record(w.evIn, st);
+    stream_wait(w.cs, w.evIn);
+    cudaStream_t cs = w.cs;
+    h2d(w.s2, ls.scale2, sizeof(real) * 8, cs);
+    auto kbuild = k_sgsop_build<T, NV>;
+    auto kgather = k_gather_T<T, NV>;
+    auto kscatter = k_scatter_T<T, NV>;
+    DNDSB_LAUNCH(kbuild, m.nCell, 128, cs, m, g, ev.lambdaFace, dTau, dt, alphaDiag, u, w.cellPos, w.nbrPos, (T4 *)w.op,
+                 (T *)w.jd, (T *)w.uT);
+    DNDSB_LAUNCH(kgather, m.nCell, 256, cs, m.nCell, m.colorCells, rhs, (T *)w.rhsT);
+    Solve<T, NV, NF> S{m, w, ls, (T)ev.s.gamma, cs};
+    if (ls.useGraph)
+    {
+        if (!(w.graph && w.keyValid && same_key(w.key, ls)))
+        {
+            graph_free(w.graph);
+            w.graph = nullptr;
+            w.keyValid = false;
+            if (graph_begin(cs) == cudaSuccess)
+            {
+                S.body();
+                if (graph_end(cs, &w.graph) != cudaSuccess)
+                    w.graph = nullptr;
+            }
+            last_error();
+        }
+        if (w.graph)
+        {
+            w.key = ls, w.keyValid = true;
+            if (graph_launch(w.graph, cs) != cudaSuccess)
+                return ST_CUDA;
+        }
+        else
+            S.body();
+    }
+    else
+    {
+        w.key = ls, w.keyValid = true;
+        S.body();
+    }
+    DNDSB_LAUNCH(kscatter, m.nCell, 256, cs, m.nCell, m.colorCells, (const T *)w.x, xInc);
+    event_record(w.evOut, cs);
+    stream_wait(st, w.evOut);
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+template <typename T, int NV>
+int run_nf(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
+           const real *u, const real *rhs, real *xInc, cudaStream_t st)
+{
+    switch (m.nf)
+    {
+    case 3:
+        return run<T, NV, 3>(m, g, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+    case 4:
+        return run<T, NV, 4>(m, g, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+    case 6:
+        return run<T, NV, 6>(m, g, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+    }
+    return ST_UNSUPPORTED;
+}
+} // namespace
+
+int linear_solve(const MeshD &m, const GeomD &g, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
+                 const real *u, const real *rhs, real *xInc, cudaStream_t st)
+{
+    if (ls.gmresCode < 0 || ls.gmresCode > 2 || ls.jacobiCode < 0 || ls.jacobiCode > 1 || ls.sgsIter < 0 || ls.nGmresIter < 0 ||
+        (ls.gmresCode && (ls.nGmresSpace < 1 || ls.nGmresSpace > 32)) || ls.precision < 0 || ls.precision > 1)
+        return ST_BADARG;
+    int nv = ev.s.nVars;
+    int rc = ws_prepare(m, ws, ls, nv);
+    if (rc != ST_OK)
+        return rc;
+    if (nv == 5)
+        return ls.precision ? run_nf<float, 5>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
+                            : run_nf<double, 5>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+    if (nv == 6)
+        return ls.precision ? run_nf<float, 6>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
+                            : run_nf<double, 6>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+    return ST_UNSUPPORTED;
+}
+} // namespace dndsb

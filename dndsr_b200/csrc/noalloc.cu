@@ -80,6 +80,8 @@ extern "C" int dndsb_eval_evaluate_rhs_noalloc(dndsb_eval *ev, double *rhs, cons
         return set_error(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs_noalloc: VR not constructed");
     const MeshD &m = mesh_of(ev);
     EvalD &e = eval_of(ev);
+    if (m.nBndFace > 0 && vr_of(ev).bnd.nZone == 0)
+        return set_error(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs_noalloc: the mesh has boundary faces; call dndsb_eval_set_bc first");
     int64_t need = m.nFace * (int64_t)e.s.nVars;
     if (need > (int64_t)DNDSB_NOALLOC_SCRATCH_DOUBLES)
         return set_error(DNDSB_E_UNSUPPORTED, "dndsb_eval_evaluate_rhs_noalloc: nFace * nVars = " + std::to_string(need) +

@@ -48,4 +48,36 @@ inline cudaError_t d2d(void *dst, const void *src, size_t bytes, cudaStream_t s)
 inline cudaError_t dev_zero(void *p, size_t bytes, cudaStream_t s) { return cudaMemsetAsync(p, 0, bytes, s); }
 inline cudaError_t dev_sync(cudaStream_t s) { return cudaStreamSynchronize(s); }
 inline cudaError_t last_error() { return cudaGetLastError(); }
+// private streams, events and captured graphs (the native linear solve)
+inline cudaError_t stream_create(cudaStream_t *s) { return cudaStreamCreateWithFlags(s, cudaStreamNonBlocking); }
+inline void stream_free(cudaStream_t s)
+{
+    if (s)
+        cudaStreamDestroy(s);
+}
+inline cudaError_t event_create(cudaEvent_t *e) { return cudaEventCreateWithFlags(e, cudaEventDisableTiming); }
+inline void event_free(cudaEvent_t e)
+{
+    if (e)
+        cudaEventDestroy(e);
+}
+inline cudaError_t event_record(cudaEvent_t e, cudaStream_t s) { return cudaEventRecord(e, s); }
+inline cudaError_t stream_wait(cudaStream_t s, cudaEvent_t e) { return cudaStreamWaitEvent(s, e, 0); }
+inline cudaError_t graph_begin(cudaStream_t s) { return cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal); }
+inline cudaError_t graph_end(cudaStream_t s, cudaGraphExec_t *exec)
+{
+    cudaGraph_t g = nullptr;
+    cudaError_t r = cudaStreamEndCapture(s, &g);
+    if (r != cudaSuccess)
+        return r;
+    r = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    return r;
+}
+inline cudaError_t graph_launch(cudaGraphExec_t e, cudaStream_t s) { return cudaGraphLaunch(e, s); }
+inline void graph_free(cudaGraphExec_t e)
+{
+    if (e)
+        cudaGraphExecDestroy(e);
+}
 } // namespace dndsb

@@ -57,6 +57,30 @@ struct MeshD
     int32_t *colorCells = nullptr; // cells grouped by colour
     int32_t *cellColor = nullptr;  // colour of each cell
     std::vector<int64_t> colorStart; // host copy, size nColor + 1
+    // boundary faces (face2cell side 1 = -1) and the cells that own them
+    int64_t nBndFace = 0, nBndCell = 0;
+    int32_t *bndFace = nullptr, *bndCell = nullptr;
+};
+
+// per-zone boundary table: the FBoundary of the VR sweep and the ghost states
+// of the RHS (Euler/EulerBC.hpp types, EulerEvaluator_EvaluateDt.hxx:1743-2468)
+enum BCType : int
+{
+    BC_FAR = 1,
+    BC_WALL = 2,
+    BC_WALL_INVIS = 3,
+    BC_WALL_ISOTHERMAL = 4,
+    BC_OUT = 5,
+    BC_OUTP = 6,
+    BC_IN = 7,
+    BC_SYM = 9,
+};
+struct BoundaryD
+{
+    int nZone = 0;
+    int32_t *type = nullptr; // [nZone], 0 for zones without a boundary condition
+    real *val = nullptr;     // [nZone][8]: far-field / inflow state, or wall temperature
+    real gamma = 1.4, Rgas = 1;
 };
 
 struct VRSettingsD
@@ -90,6 +114,7 @@ struct VRD
     real *baseMoment = nullptr, *faceWeight = nullptr, *faceL = nullptr;
     real *AAInvB = nullptr, *AInvb = nullptr, *matA = nullptr;
     float *AAInvB32 = nullptr, *AInvb32 = nullptr;
+    BoundaryD bnd; // boundary values for the BC faces of the sweep
 };
 
 struct EulerSettingsD
@@ -109,6 +134,8 @@ struct EvalD
     real *lambdaFace = nullptr, *lambdaFaceC = nullptr, *lambdaFaceVis = nullptr, *lambdaConv = nullptr, *deltaLambdaFace = nullptr;
     real *deltaLambdaCell = nullptr;
     real *faceFlux = nullptr; // scratch [nFace][nv]
+    real *facePt = nullptr;   // [nGf][nFace][7]: point, unit normal, |J| w (layout of the tuned face kernel)
+    real *cellPar = nullptr;  // [nCell][6]: centre, 1/L
     real *redBuf = nullptr;   // scratch for reductions
     int *errWord = nullptr;   // device error word
 };
@@ -119,8 +146,8 @@ int vr_construct_base_and_weight(const MeshD &m, const GeomD &g, VRD &vr, const 
 int vr_construct_rec_coeff(const MeshD &m, const GeomD &g, VRD &vr, int *errWord, cudaStream_t st);
 
 // ---- hot path (hotpath.cu) ----
-int vr_iter(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
-            int useFP32, cudaStream_t st);
+int vr_iter(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc,
+            int uRecIsZero, int useFP32, cudaStream_t st);
 int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, real MaxDt, int useLocalDt, real *dt, real *dtMin,
             cudaStream_t st);
 int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *u, const real *uRec, real *rhs, real *faceFlux,
@@ -132,9 +159,45 @@ int lusgs_matvec(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, cons
                  real *AuInc, cudaStream_t st);
 int init_field(const MeshD &m, const GeomD &g, const EvalD &ev, int kind, real chi, real *u, cudaStream_t st);
 int vr_swap(int64_t n, real *a, real *b, cudaStream_t st);
+// tuned kernels (fast.cu); ST_UNSUPPORTED means "use the generic kernel"
+int fast_geometry(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, cudaStream_t st);
+int rhs_face_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st);
+int vr_iter_fast(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
+                 int useFP32, cudaStream_t st);
 int reduce_norm(int64_t n, int ncol, const real *x, const real *w, int op, int powP, real *redBuf, real *outHost, cudaStream_t st);
 constexpr int kRedBlocks = 592;                  // 4 x 148 SMs
 constexpr int kRedBufLen = kRedBlocks * 8 + 64; // partials of the deterministic reductions + final values
+constexpr int kRedBufLenK = kRedBlocks * 33;    // partials of the Krylov reductions (up to 33 columns)
 // column reduction of x [n][ncol] (op 0 sum of |x|^powP * w, 1 min, 2 max); returns the device address of the ncol results
 real *reduce_cols(int op, int64_t n, int ncol, const real *x, const real *w, int powP, real *redBuf, cudaStream_t st);
+
+// ---- boundary faces (bc.cu) ----
+// adds relax A^-1 BCC (GetBoundaryRHS) of every boundary cell to uRecNew
+int vr_iter_bc(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc,
+               int uRecIsZero, int useFP32, cudaStream_t st);
+// writes the face flux of every boundary face
+int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st);
+
+// ---- native linear solve (linsolve.cu) and its Krylov reductions (reduce.cu) ----
+struct LinSettings
+{
+    int gmresCode = 0;   // 0 LU-SGS pairs, 1 GMRES from zero, 2 LU-SGS pairs then GMRES
+    int jacobiCode = 1;  // 1 Gauss-Seidel sweeps, 0 Jacobi sweeps
+    int sgsIter = 0;     // extra SGS pairs
+    int nGmresSpace = 5; // Krylov subspace size (<= 32)
+    int nGmresIter = 1;  // restarts
+    int precision = 0;   // 0 FP64, 1 FP32
+    int useGraph = 1;    // capture the solve once and replay it
+    real scale2[8] = {1, 1, 1, 1, 1, 1, 1, 1}; // per-variable weights of the GMRES dot (meanScaleInv^2)
+};
+struct LinWs;
+int linear_solve(const MeshD &m, const GeomD &g, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
+                 const real *u, const real *rhs, real *xInc, cudaStream_t st);
+void linws_free(LinWs *w);
+// prec 0: double vectors, 1: float vectors; nv 5 or 6; FP64 accumulation, deterministic
+void krylov_mdot(int prec, int64_t n, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st);
+void krylov_maxpy_norm(int prec, int64_t n, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm,
+                       cudaStream_t st);
+void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st);
+void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st);
 } // namespace dndsb

@@ -193,6 +193,8 @@ class SolverConfig:
     gmresScale: int = 0
     linear_precision: str = "fp64"   # "fp32": FP32 preconditioner / GMRES inside the FP64 defect correction
     vr_precision: str = "fp64"       # coefficient precision of the VR sweeps
+    native_linear: bool = True       # one device call per linear solve (dndsb_eval_solve_linear) when the evaluator has it
+    meanScale: tuple = ()            # GMRES dot weights (gmresScale), empty = ones
     res_history: list = field(default_factory=list)
 
 
@@ -240,13 +242,23 @@ class ImplicitSolver:
 
     # EulerSolver.hxx:740-997 and solveLinear :1407-1579
     def fsolve(self, cx, cres, res_other, dtau, dt, alphaDiag, cxInc, it, ct):
+        cfg = self.cfg
+        if cfg.native_linear and hasattr(self.ev, "SolveLinear"):
+            self.ev.SolveLinear(alphaDiag, dtau, dt, cx, cres, cxInc, gmresCode=cfg.gmresCode, jacobiCode=cfg.jacobiCode, sgsIter=cfg.sgsIter,
+                                nGmresSpace=cfg.nGmresSpace, nGmresIter=cfg.nGmresIter, precision=cfg.linear_precision,
+                                meanScale=cfg.meanScale or None)
+            self.n_sgs += 1 + cfg.sgsIter
+            return
+        if cfg.linear_precision != "fp64":
+            raise ValueError("an FP32 linear solve needs the device evaluator (native_linear)")
         self.ev.LUSGSMatrixInit(self.jd, dtau, dt, alphaDiag)
         cxInc.zero_()
-        if self.cfg.gmresCode == 0:
+        if self.cfg.gmresCode in (0, 2):
             self._sgs_pair(alphaDiag, cres, cx, cxInc)
             for _ in range(self.cfg.sgsIter):
                 self._sgs_pair(alphaDiag, cres, cx, cxInc)
-            return
+            if self.cfg.gmresCode == 0:
+                return
         x = torch.zeros_like(cxInc)
 
         def FA(v, Av):
@@ -257,9 +269,15 @@ class ImplicitSolver:
             for _ in range(1 + self.cfg.sgsIter):
                 self._sgs_pair(alphaDiag, v, cx, MLv)
 
-        def fdot(a, b):
-            return float(torch.sum(a * b))
+        nv = cres.shape[1]
+        ms = [m if m > 0 else 1.0 for m in (list(self.cfg.meanScale) + [1.0] * nv)[:nv]]
+        s2 = torch.tensor([1.0 / (m + 1e-200) ** 2 for m in ms], dtype=cres.dtype, device=cres.device)
 
+        def fdot(a, b):
+            return float(torch.sum(a * b * s2))
+
+        if self.cfg.gmresCode == 2:
+            x.copy_(cxInc)
         self.gmres.solve(FA, FML, fdot, cres, x, self.cfg.nGmresIter, lambda i, r, rb: False)
         cxInc.copy_(x)
 

@@ -212,6 +212,73 @@ def tgv_mesh(n=64, seed=0x1234, jitter=0.05):
     return periodic_hex_3d(n, L=2 * np.pi, jitter=jitter, seed=seed)
 
 
+# boundary zones of the bump channel and their EulerBC.hpp types (BCFar 1, BCWallInvis 3, BCSym 9)
+BUMP_ZONES = {"inflow": 1, "outflow": 2, "bump": 3, "top": 4, "side0": 5, "side1": 6}
+BUMP_BC_TYPES = {1: 1, 2: 1, 3: 3, 4: 3, 5: 9, 6: 9}
+
+
+def bump_height(x, amp=0.05, width=25.0):
+    return amp * np.exp(-width * x * x)
+
+
+def bump_channel_tet(nx=160, ny=80, nz=26, jitter=0.05, seed=0x1234, amp=0.05, L=(4.0, 1.0, 0.5)):
+    """Channel [-2,2] x [0,1] x [0,0.5] over the bump y = amp exp(-25 x^2), in tetrahedra.
+
+    A structured nx x ny x nz hexahedral grid whose vertical lines follow the bump
+    (y = h(x) + eta (1 - h(x))) is split into 6 tetrahedra per hexahedron along its
+    main diagonal (Kuhn split); interior nodes are jittered by a uniform fraction
+    ``jitter`` of the grid step in every parametric direction.  Boundary faces carry
+    the zones of ``BUMP_ZONES``.  Cells: 6 nx ny nz.
+    """
+    rng = np.random.default_rng(seed)
+    Lx, Ly, Lz = L
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    xi, eta, zeta = i / nx, j / ny, k / nz
+    interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
+    if jitter:
+        for a, n in ((xi, nx), (eta, ny), (zeta, nz)):
+            a += np.where(interior, rng.uniform(-jitter / n, jitter / n, size=a.shape), 0.0)
+    x = -Lx / 2 + Lx * xi
+    h = bump_height(x, amp)
+    y = h + eta * (Ly - h)
+    z = Lz * zeta
+    nid = lambda a, b, c: (a * (ny + 1) + b) * (nz + 1) + c
+    coords = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    ci, cj, ck = [a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")]
+    tets = []
+    for perm in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+        off = np.zeros((4, 3), dtype=np.int64)
+        off[1, perm[0]] = 1
+        off[2] = off[1]
+        off[2, perm[1]] = 1
+        off[3] = 1
+        tets.append(np.stack([nid(ci + o[0], cj + o[1], ck + o[2]) for o in off], axis=1))
+    c2n = np.stack(tets, axis=1).reshape(-1, 4).astype(np.int64)  # 6 tets of one hexahedron are consecutive
+    X = coords[c2n]
+    vol6 = np.einsum("ij,ij->i", np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0]), X[:, 3] - X[:, 0])
+    neg = vol6 < 0
+    c2n[neg, 1], c2n[neg, 2] = c2n[neg, 2].copy(), c2n[neg, 1].copy()
+    csh = np.zeros((c2n.shape[0], 4, 3))
+    f2n, fsh, f2c, fps, c2f, fz = _build_faces(TET4, c2n, csh)
+    bnd = f2c[:, 1] < 0
+    I, J, K = i.ravel(), j.ravel(), k.ravel()
+    fn = f2n[bnd]
+    zone = np.zeros(fn.shape[0], dtype=np.int32)
+    for nm, test in (("inflow", I == 0), ("outflow", I == nx), ("bump", J == 0), ("top", J == ny), ("side0", K == 0), ("side1", K == nz)):
+        zone[np.all(test[fn], axis=1)] = BUMP_ZONES[nm]
+    if np.any(zone == 0):
+        raise RuntimeError("unclassified boundary face")
+    fz[bnd] = zone
+    return Mesh(3, TET4, coords, c2n, csh, f2n, fsh, f2c, fz, fps, c2f, TRI3)
+
+
+def freestream(mach, gamma=1.4, rho=1.0, p=1.0, direction=(1.0, 0.0, 0.0)):
+    """Conservative state [rho, rho u, rho v, rho w, E] of a uniform flow at Mach ``mach``."""
+    a = np.sqrt(gamma * p / rho)
+    v = mach * a * np.asarray(direction, dtype=np.float64) / np.linalg.norm(direction)
+    return np.array([rho, rho * v[0], rho * v[1], rho * v[2], p / (gamma - 1) + 0.5 * rho * v @ v])
+
+
 def greedy_colors(mesh):
     """First-fit colouring of the cell adjacency graph in cell order."""
     nbr = np.where(mesh.face2cell[mesh.cell2face, 0] == np.arange(mesh.n_cell)[:, None],

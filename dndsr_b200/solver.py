@@ -31,6 +31,26 @@ EULER_DEFAULTS = dict(nVars=5, riemannSolverType="Roe", rsFixScale=1.0, rsIncFSc
                       TRef=273.15, CSutherland=110.4, muModel=1, ignoreVis=False)
 
 
+# boundary condition codes, Euler/EulerBC.hpp:35-48
+BC = dict(BCFar=1, BCWall=2, BCWallInvis=3, BCWallIsothermal=4, BCOut=5, BCOutP=6, BCIn=7, BCSym=9)
+
+
+def euler_bc_dir_weights(types, maxOrder=3):
+    """Per-zone VR face weights of the Euler boundary types (EulerEvaluator.hpp:138-152, the
+    callback InitializeFV passes to ConstructBaseAndWeight): Dirichlet-type {1, 0, 0, 0} for
+    far-field, walls, symmetry and inflow, nothing for outflow; interior zones keep 1."""
+    w = np.ones((len(types), 4))
+    for z, t in enumerate(types):
+        t = BC[t] if isinstance(t, str) else int(t)
+        if t == 0:
+            continue
+        if t == BC["BCOut"]:
+            w[z] = 0.0
+        else:
+            w[z] = (1.0, 0.0, 0.0, 0.0)
+    return w
+
+
 def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -172,6 +192,15 @@ class EulerEvaluator(Handle):
         self.nVars = cs.nVars
         self._cs = cs
 
+    def SetBC(self, types, values):
+        """BoundaryHandler of the evaluator (Euler/EulerBC.hpp) as a per-zone table: types[zone]
+        (EulerBC.hpp codes or names, 0 for interior zones) and values[zone] (far-field / inflow
+        state, or wall temperature first).  Also the reconstruction's FBoundary."""
+        t = np.array([BC[x] if isinstance(x, str) else int(x) for x in types], dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(len(t), self.nVars)
+        self._bc = (t, v)
+        capi.call("dndsb_eval_set_bc", self.h, len(t), t.ctypes.data_as(capi._I32), capi.dptr(v))
+
     def InitializeUDOF(self, u, kind, chi=5.0):
         capi.call("dndsb_eval_initialize_udof", self.h, kind, float(chi), _ptr(u, "u"), _stream())
 
@@ -204,6 +233,21 @@ class EulerEvaluator(Handle):
     def LUSGSMatrixVec(self, alphaDiag, u, uInc, jdiag, AuInc):
         capi.call("dndsb_eval_lusgs_matrix_vec", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(uInc, "uInc"), _ptr(jdiag, "jdiag"),
                   _ptr(AuInc, "AuInc"), _stream())
+
+    def SolveLinear(self, alphaDiag, dTau, dt, u, rhs, xInc, gmresCode=0, jacobiCode=1, sgsIter=0, nGmresSpace=5, nGmresIter=1,
+                    precision="fp64", meanScale=None, useGraph=True):
+        """EulerSolver::solveLinear with LUSGSMatrixInit (EulerSolver.hxx:1407-1579, EulerEvaluator.hxx:37-159):
+        xInc = M^-1 rhs by LU-SGS pairs (gmresCode 0), GMRES preconditioned by SGS pairs (1), or both (2),
+        in FP64 or FP32; all on the device, no host synchronisation."""
+        ls = capi.LinearSettings()
+        ls.gmresCode, ls.jacobiCode, ls.sgsIter = int(gmresCode), int(jacobiCode), int(sgsIter)
+        ls.nGmresSpace, ls.nGmresIter = int(nGmresSpace), int(nGmresIter)
+        ls.precision = 1 if precision == "fp32" else 0
+        ls.useGraph = int(bool(useGraph))
+        for i, x in enumerate(meanScale if meanScale is not None else []):
+            ls.meanScale[i] = float(x)
+        capi.call("dndsb_eval_solve_linear", self.h, ctypes.byref(ls), float(alphaDiag), _ptr(dTau, "dTau"), float(dt), _ptr(u, "u"),
+                  _ptr(rhs, "rhs"), _ptr(xInc, "xInc"), _stream())
 
     def EvaluateNorm(self, x, P=1, volWise=True):
         out = np.zeros(self.nVars)

@@ -120,9 +120,29 @@ int dndsb_vr_get_array(const dndsb_vr *vr, const char *name, double *hostOut, in
 int dndsb_vr_do_reconstruction_iter(dndsb_vr *vr, double *uRec, double *uRecNew, const double *u, int nVars, int putIntoNew,
                                     int recordInc, int uRecIsZero, int precision, void *stream);
 
+/* Boundary condition codes, Euler/EulerBC.hpp:35-48 EulerBCType */
+#define DNDSB_BC_FAR 1
+#define DNDSB_BC_WALL 2
+#define DNDSB_BC_WALL_INVIS 3
+#define DNDSB_BC_WALL_ISOTHERMAL 4
+#define DNDSB_BC_OUT 5
+#define DNDSB_BC_OUTP 6
+#define DNDSB_BC_IN 7
+#define DNDSB_BC_SYM 9
+/* The FBoundary argument of DoReconstructionIter as a table: per face zone (the mesh's faceZone
+ * values index it; zones of interior faces may hold 0) the boundary type and its value row
+ * (far-field / inflow state, or the wall temperature in entry 0), nVars values per zone.  Ghost
+ * values follow EulerEvaluator::generateBoundaryValue (EulerEvaluator_EvaluateDt.hxx:1743-2468).
+ * A mesh with boundary faces needs this table before its first sweep. */
+int dndsb_vr_set_boundary(dndsb_vr *vr, int nZone, const int32_t *type, const double *value, int nVars, double gamma, double Rgas);
+
 /* ---- Euler evaluator: EulerEvaluator.hpp:76-1980 ---- */
 int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s);
 int dndsb_eval_destroy(dndsb_eval *ev);
+/* The evaluator's BoundaryHandler (Euler/EulerBC.hpp): the same per-zone table as
+ * dndsb_vr_set_boundary, with nVars, gamma and Rgas of the evaluator; it also becomes the
+ * reconstruction's FBoundary (EulerSolver.hxx:163-175). */
+int dndsb_eval_set_bc(dndsb_eval *ev, int nZone, const int32_t *type, const double *value);
 /* InitializeUDOF special initialisers, EulerEvaluator.hxx:1039-1143:
  * kind 2 = isentropic vortex of strength chi, 3 = Taylor-Green vortex (M0 = 0.1) */
 int dndsb_eval_initialize_udof(dndsb_eval *ev, int kind, double chi, double *u, void *stream);
@@ -141,6 +161,28 @@ int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, c
 /* LUSGSMatrixVec(alphaDiag, t, u, uInc, JDiag, AuInc), EulerEvaluator.hxx:175-274 */
 int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
                                 double *AuInc, void *stream);
+/* Linear-solver controls, EulerSolver.hpp linearSolverControl (fields of the same names) plus the
+ * precision of the solve.  meanScale: the GMRES dot weights of EulerSolver.hxx:1518-1540
+ * (dot(a, b) = sum a_v b_v / (meanScale_v + 1e-200)^2); entries <= 0 count as 1. */
+typedef struct dndsb_linear_settings
+{
+    int gmresCode;   /* 0 LU-SGS pairs, 1 GMRES from zero, 2 LU-SGS pairs then GMRES */
+    int jacobiCode;  /* 1 Gauss-Seidel sweeps (multicolour), 0 Jacobi sweeps */
+    int sgsIter;     /* extra SGS pairs (also inside the GMRES preconditioner) */
+    int nGmresSpace; /* Krylov subspace size, 1..32 */
+    int nGmresIter;  /* restart cycles */
+    int precision;   /* 0 FP64, 1 FP32 (preconditioner and Krylov vectors; dots accumulate in FP64) */
+    int useGraph;    /* 1: capture the fixed kernel sequence once and replay it */
+    double meanScale[8];
+} dndsb_linear_settings;
+/* EulerSolver::solveLinear + doPrecondition (EulerSolver.hxx:1407-1579, 1605-1658) with
+ * LUSGSMatrixInit (EulerEvaluator.hxx:37-159) and GMRES_LeftPreconditioned::solve
+ * (Solver/Linear.hpp:46-133) in one call: xInc = M^-1 rhs, for the scalar-diagonal LU-SGS
+ * operator at state u, pseudo time step dTau, physical step dt and alphaDiag.  Uses the face
+ * eigenvalues of the last dndsb_eval_evaluate_dt.  xInc is overwritten (the solve starts from
+ * zero, as the reference's fsolve does).  No host synchronisation. */
+int dndsb_eval_solve_linear(dndsb_eval *ev, const dndsb_linear_settings *ls, double alphaDiag, const double *dTau, double dt,
+                            const double *u, const double *rhs, double *xInc, void *stream);
 /* EvaluateNorm(res, rhs, P, volWise), EulerEvaluator.hxx:1394-1439; P = 1, 2 or >= 3 (max norm) */
 int dndsb_eval_evaluate_norm(dndsb_eval *ev, const double *x, int P, int volWise, double *resHost, void *stream);
 /* named evaluator arrays to host: "lambdaFace", "lambdaFaceC", "lambdaFaceVis", "deltaLambdaCell" */

@@ -78,6 +78,7 @@ def _declare(L):
     L.orc_get.restype = ctypes.c_long
     L.orc_get.argtypes = [_V, ctypes.c_char_p, _D]
     L.orc_set_delta_lambda.argtypes = [_V, _D]
+    L.orc_set_bc.argtypes = [_V, ctypes.c_int, _I, _D, ctypes.c_int]
     L.orc_init_field.argtypes = [_V, ctypes.c_int, ctypes.c_double, _D]
     L.orc_vr_iter.argtypes = [_V, _D, _D, _D, ctypes.c_int, ctypes.c_int]
     L.orc_eval_dt.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D]
@@ -177,6 +178,14 @@ class Oracle:
         out = np.zeros(n)
         lib().orc_get(self.h, name.encode(), _p(out))
         return out
+
+    def set_bc(self, types, values):
+        """Boundary table per face zone (index = zone id, zone 0 interior): EulerBC.hpp type codes
+        and the far-field / inflow state (or wall temperature) of each zone."""
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(len(t), self.nv)
+        self._bc = (t, v)
+        lib().orc_set_bc(self.h, len(t), t.ctypes.data_as(_I), _p(v), self.nv)
 
     def init_field(self, kind, chi=5.0):
         u = np.zeros((self.mesh.n_cell, self.nv))

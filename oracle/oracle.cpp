@@ -866,6 +866,14 @@ struct Oracle
     std::vector<real> AAInvB, AInvb, matA;
     // evaluator state (EulerEvaluator.hpp lambdaFace*, deltaLambda*)
     std::vector<real> lambdaFace, lambdaFaceC, lambdaFaceVis, lambdaFace0, deltaLambdaFace, deltaLambdaCell;
+    // boundary table indexed by face zone (EulerBC.hpp:35-48 types; value = far / inflow state or wall temperature)
+    std::vector<int> bcType;
+    std::vector<real> bcVal; // [zone][8]
+    int zoneType(long f) const
+    {
+        int z = faceZone[f];
+        return z >= 0 && z < (int)bcType.size() ? bcType[z] : 0;
+    }
 
     void cellCoords(long c, real *out) const
     {
@@ -1305,6 +1313,155 @@ struct Oracle
         return bad;
     }
 
+
+    // Gas.hpp IdealGasThermalConservative2Primitive / Primitive2Conservative (dim = 3, 5 variables)
+    void cons2prim(const real *U, real *P) const
+    {
+        real g = es.gamma;
+        P[0] = U[0];
+        for (int d = 0; d < 3; d++)
+            P[1 + d] = U[1 + d] / U[0];
+        real vsqr = sqr(P[1]) + sqr(P[2]) + sqr(P[3]);
+        P[4] = (g - 1) * (U[4] - 0.5 * U[0] * vsqr);
+        for (int j = 5; j < es.nVars; j++)
+            P[j] = U[j] / U[0];
+    }
+    void prim2cons(const real *P, real *U) const
+    {
+        real g = es.gamma;
+        U[0] = P[0];
+        for (int d = 0; d < 3; d++)
+            U[1 + d] = P[1 + d] * P[0];
+        real vsqr = sqr(P[1]) + sqr(P[2]) + sqr(P[3]);
+        U[4] = P[4] / (g - 1) + 0.5 * P[0] * vsqr;
+        for (int j = 5; j < es.nVars; j++)
+            U[j] = P[j] * P[0];
+    }
+
+    // EulerEvaluator_EvaluateDt.hxx:1743-2468 generateBoundaryValue, linMode 0, no rotating frame,
+    // no anchors or CL driver, zero grid velocity.  Types: 1 BCFar, 2 BCWall, 3 BCWallInvis,
+    // 4 BCWallIsothermal, 5 BCOut, 6 BCOutP, 7 BCIn, 9 BCSym.  Returns false for an unsupported type.
+    bool bcValue(int type, int zone, const real *UL, const real *n, real *UR) const
+    {
+        int nv = es.nVars;
+        real g = es.gamma;
+        const real *far = &bcVal[zone * 8];
+        switch (type)
+        {
+        case 1:
+        case 6:
+        {
+            // generateBV_FarField (:1870-1945): characteristic switching on the normal velocity
+            real un = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) / UL[0];
+            real vsqr = (sqr(UL[1]) + sqr(UL[2]) + sqr(UL[3])) / sqr(UL[0]);
+            real p, asqr, H;
+            idealGasThermal(UL[4], UL[0], vsqr, g, p, asqr, H);
+            real a = std::sqrt(asqr);
+            if (un - a > 0)
+                std::copy(UL, UL + nv, UR);
+            else if (un > 0)
+            {
+                real fp[8], lp[8];
+                cons2prim(far, fp), cons2prim(UL, lp);
+                lp[4] = fp[4];
+                prim2cons(lp, UR);
+            }
+            else if (un + a > 0)
+            {
+                real fp[8], lp[8];
+                cons2prim(far, fp), cons2prim(UL, lp);
+                fp[4] = lp[4];
+                prim2cons(fp, UR);
+            }
+            else
+                std::copy(far, far + nv, UR);
+            return true;
+        }
+        case 3:
+        case 9:
+        {
+            // generateBV_InviscidWall (:2199-2215): mirrored momentum
+            std::copy(UL, UL + nv, UR);
+            real mn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
+            for (int d = 0; d < 3; d++)
+                UR[1 + d] -= 2 * mn * n[d];
+            return true;
+        }
+        case 2:
+        case 4:
+        {
+            // generateBV_ViscousWall (:2241-2330): reversed momentum (and SA variable); isothermal density
+            std::copy(UL, UL + nv, UR);
+            for (int d = 0; d < 3; d++)
+                UR[1 + d] = -UR[1 + d];
+            if (type == 4)
+            {
+                real P[8];
+                cons2prim(UR, P);
+                P[0] = P[4] / far[0] / es.Rgas;
+                prim2cons(P, UR);
+            }
+            for (int j = 5; j < nv; j++)
+                UR[j] = -UR[j];
+            return true;
+        }
+        case 5:
+            std::copy(UL, UL + nv, UR); // generateBV_Outflow
+            return true;
+        case 7:
+            std::copy(far, far + nv, UR); // generateBV_Inflow
+            return true;
+        }
+        return false;
+    }
+
+    // EulerEvaluator.hpp:1541-1625 CompressRecPart: fall back to the mean when rho or e < 0
+    void compressRec(const real *um, const real *U, real *out) const
+    {
+        int nv = es.nVars;
+        std::copy(U, U + nv, out);
+        if (out[0] < 0)
+            std::copy(um, um + nv, out);
+        real eK = (sqr(out[1]) + sqr(out[2]) + sqr(out[3])) * 0.5 / (verySmallReal + out[0]);
+        if (out[4] - eK < 0)
+            std::copy(um, um + nv, out);
+    }
+
+    // VariationalReconstruction_Reconstruction.hxx:19-176 GetBoundaryRHS with the Euler FBoundary of
+    // EulerSolver.hxx:163-175 (intOrderVRBC = intOrder): sum over Gauss points of
+    // w0^2 phi_i (uBV - u_c) |J| w, returned as [R][nv]
+    void boundaryRHS(long c, long f, const real *uRec, const real *u, real *BCC) const
+    {
+        int nv = es.nVars;
+        std::fill(BCC, BCC + R * nv, 0.0);
+        int type = zoneType(f);
+        real w0 = faceWeight[f * (vs.maxOrder + 1) + 0];
+        std::vector<real> T(NDOF);
+        for (int g = 0; g < nGf; g++)
+        {
+            real pq[3], w;
+            quadPoint(faceType, vs.intOrder, g, pq, w);
+            const real *p = &facePP[(f * nGf + g) * 3];
+            const real *n = &faceNorm[(f * nGf + g) * 3];
+            diffBase(c, p, T.data(), 1, true);
+            real UL[8], ULf[8], UB[8];
+            for (int v = 0; v < nv; v++)
+            {
+                real a = 0;
+                for (int j = 0; j < R; j++)
+                    a += T[1 + j] * uRec[(c * R + j) * nv + v];
+                UL[v] = u[c * nv + v] + a;
+            }
+            compressRec(u + c * nv, UL, ULf);
+            if (!bcValue(type, faceZone[f], ULf, n, UB))
+                std::copy(ULf, ULf + nv, UB);
+            real JW = faceJDet[f * nGf + g] * w * w0 * w0;
+            for (int i = 0; i < R; i++)
+                for (int v = 0; v < nv; v++)
+                    BCC[i * nv + v] += T[1 + i] * (UB[v] - u[c * nv + v]) * JW;
+        }
+    }
+
     // VariationalReconstruction_Reconstruction.hxx:485-615 DoReconstructionIter, Jacobi branch
     // (SORInstead = false), periodic/interior faces.  uRec rows: [cell][R][nv].
     void vrIterJacobi(const real *uRec, real *uRecNew, const real *u, bool recordInc, bool uRecIsZero) const
@@ -1323,7 +1480,26 @@ struct Oracle
                 long f = cell2face[c * nf + k];
                 long o = otherOf(c, f);
                 if (o < 0)
-                    continue; // boundary faces: handled by the BC restatement (not used by periodic cases)
+                {
+                    // boundary face: + relax A^-1 BCC (recordInc: - A^-1 BCC, skipped when uRecIsZero)
+                    if (recordInc && uRecIsZero)
+                        continue;
+                    std::vector<real> BCC(R * nv);
+                    boundaryRHS(c, f, uRec, u, BCC.data());
+                    const real *Ai = &AAInvB[(c * (nf + 1)) * R * R];
+                    for (int i = 0; i < R; i++)
+                        for (int v = 0; v < nv; v++)
+                        {
+                            real acc = 0;
+                            for (int j = 0; j < R; j++)
+                                acc += Ai[i * R + j] * BCC[j * nv + v];
+                            if (recordInc)
+                                out[i * nv + v] -= acc;
+                            else
+                                out[i * nv + v] += relax * acc;
+                        }
+                    continue;
+                }
                 const real *M = &AAInvB[(c * (nf + 1) + 1 + k) * R * R];
                 const real *b = &AInvb[(c * nf + k) * R];
                 for (int i = 0; i < R; i++)
@@ -1435,6 +1611,87 @@ struct Oracle
                 dt[c] = mn;
     }
 
+    // EulerEvaluator_EvaluateRHS.hxx:171-562 for a boundary face (f2c[1] == UnInitIndex): ghost
+    // state from generateBoundaryValue at every Gauss point, Roe means from the ghost of the cell
+    // mean at the face centre (:198-210), gradient copied from the inside (:360-362), GRP
+    // distance from the face centre (:363-386), viscous flux removed on slip, far-field and
+    // outflow faces (:423-430, EvaluateDt.hxx:1203-1207)
+    void boundaryFaceFlux(long f, const real *u, const real *uRec, real *fluxEs) const
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        long c0 = face2cell[f * 2 + 0];
+        int type = zoneType(f);
+        int zone = faceZone[f];
+        std::vector<real> T0(4 * NDOF);
+        for (int v = 0; v < nv; v++)
+            fluxEs[v] = 0;
+        const real *ULm = u + c0 * nv;
+        real URm[8];
+        if (!bcValue(type, zone, ULm, &faceMeanNorm[f * 3], URm))
+            std::copy(ULm, ULm + nv, URm);
+        real dLambda = deltaLambdaCell[c0];
+        bool zeroGrad = type == 3 || type == 5 || type == 1 || type == 9; // BCWallInvis, BCOut, BCFar, BCSym
+        bool noVis = type == 3 || type == 9;
+        for (int g = 0; g < nGf; g++)
+        {
+            real pq[3], w;
+            quadPoint(faceType, vs.intOrder, g, pq, w);
+            const real *n = &faceNorm[(f * nGf + g) * 3];
+            const real *p0 = &facePP[(f * nGf + g) * 3];
+            diffBase(c0, p0, T0.data(), dim + 1, true);
+            real UL[8], UR[8], GL[3 * 8] = {0};
+            for (int v = 0; v < nv; v++)
+            {
+                real a = 0;
+                for (int j = 0; j < R; j++)
+                    a += T0[1 + j] * uRec[(c0 * R + j) * nv + v];
+                UL[v] = u[c0 * nv + v] + a;
+                for (int d = 0; d < dim; d++)
+                {
+                    real ga = 0;
+                    for (int j = 0; j < R; j++)
+                        ga += T0[(1 + d) * NDOF + 1 + j] * uRec[(c0 * R + j) * nv + v];
+                    GL[d * nv + v] = ga;
+                }
+            }
+            if (!bcValue(type, zone, UL, n, UR))
+                std::copy(UL, UL + nv, UR);
+            real dc[3] = {faceCent[f * 3 + 0] - cellBary[c0 * 3 + 0], faceCent[f * 3 + 1] - cellBary[c0 * 3 + 1],
+                          faceCent[f * 3 + 2] - cellBary[c0 * 3 + 2]};
+            real distBaryPerp = std::abs(dot3(dc, n)) * 2.;
+            real distGRP = vol[c0] / faceArea[f] * 2;
+            distGRP = std::max(std::min(distBaryPerp, distGRP * 2), distGRP * 0.25);
+            if (type == 3 || type == 9)
+                distGRP += veryLargeReal;
+            real UM[8], GM[3 * 8], GMP[3 * 8];
+            for (int v = 0; v < nv; v++)
+                UM[v] = 0.5 * (UL[v] + UR[v]);
+            for (int d = 0; d < 3; d++)
+                for (int v = 0; v < nv; v++)
+                    GM[d * nv + v] = GL[d * nv + v] + (1.0 / distGRP) * (n[d] * (UR[v] - UL[v]));
+            if (es.ignoreVis || zeroGrad)
+                for (int i = 0; i < 3 * nv; i++)
+                    GM[i] = 0;
+            gradCons2Prim(nv, UM, GM, GMP, gamma);
+            real vis[8] = {0};
+            if (!es.ignoreVis && !noVis)
+            {
+                real velo2 = (sqr(UM[1]) + sqr(UM[2]) + sqr(UM[3])) / sqr(UM[0]);
+                real pM, aM, HM;
+                idealGasThermal(UM[4], UM[0], velo2, gamma, pM, aM, HM);
+                real Tm = pM / ((gamma - 1) / gamma * cp() * UM[0]);
+                real muf = muEff(UM, Tm);
+                viscousFlux(nv, UM, GMP, n, type == 2, gamma, muf, cp() * muf / es.prGas, cp(), vis);
+            }
+            real F[8] = {0}, l0, l1, l4, vg[3] = {0, 0, 0};
+            riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4);
+            real JD = faceJDet[f * nGf + g];
+            for (int v = 0; v < nv; v++)
+                fluxEs[v] += -(F[v] - vis[v]) * JD * w;
+        }
+    }
+
     // EulerEvaluator_EvaluateRHS.hxx:55-818 EvaluateRHS with the flux of
     // EulerEvaluator_EvaluateDt.hxx:1084-1511 fluxFace (interior/periodic faces,
     // no limiter, source term ignored, no grid velocity)
@@ -1450,7 +1707,10 @@ struct Oracle
         {
             long c0 = face2cell[f * 2 + 0], c1 = face2cell[f * 2 + 1];
             if (c1 < 0)
+            {
+                boundaryFaceFlux(f, u, uRec, &faceFlux[f * nv]);
                 continue;
+            }
             std::vector<real> T0(4 * NDOF), T1(4 * NDOF);
             real fluxEs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             const real *ULm = u + c0 * nv, *URm = u + c1 * nv;
@@ -1728,6 +1988,17 @@ extern "C"
         return o;
     }
     void orc_destroy(void *h) { delete (Oracle *)h; }
+
+    // boundary table per face zone (zone 0 = interior): EulerBC.hpp:35-48 type codes, values [nZone][nVars]
+    void orc_set_bc(void *h, int nZone, const int *type, const double *value, int nv)
+    {
+        Oracle *o = (Oracle *)h;
+        o->bcType.assign(type, type + nZone);
+        o->bcVal.assign(nZone * 8, 0.0);
+        for (int z = 0; z < nZone; z++)
+            for (int v = 0; v < nv && v < 8; v++)
+                o->bcVal[z * 8 + v] = value[z * nv + v];
+    }
 
     int orc_construct(void *h, const double *bcDirWeight, int nZone)
     {
