@@ -7,25 +7,25 @@
 namespace dndsb
 {
 // Gas.hpp IdealGasThermalConservative2Primitive / Primitive2Conservative (3 velocity components)
-template <int NV>
-DNDSB_HD void bc_cons2prim(const real *U, real *P, real gamma)
+template <int NV, typename T>
+DNDSB_HD void bc_cons2prim(const T *U, T *P, real gamma)
 {
     P[0] = U[0];
     for (int d = 0; d < 3; d++)
         P[1 + d] = U[1 + d] / U[0];
-    real vsqr = P[1] * P[1] + P[2] * P[2] + P[3] * P[3];
+    T vsqr = P[1] * P[1] + P[2] * P[2] + P[3] * P[3];
     P[4] = (gamma - 1) * (U[4] - 0.5 * U[0] * vsqr);
     for (int j = 5; j < NV; j++)
         P[j] = U[j] / U[0];
 }
 
-template <int NV>
-DNDSB_HD void bc_prim2cons(const real *P, real *U, real gamma)
+template <int NV, typename T>
+DNDSB_HD void bc_prim2cons(const T *P, T *U, real gamma)
 {
     U[0] = P[0];
     for (int d = 0; d < 3; d++)
         U[1 + d] = P[1 + d] * P[0];
-    real vsqr = P[1] * P[1] + P[2] * P[2] + P[3] * P[3];
+    T vsqr = P[1] * P[1] + P[2] * P[2] + P[3] * P[3];
     U[4] = P[4] / (gamma - 1) + 0.5 * P[0] * vsqr;
     for (int j = 5; j < NV; j++)
         U[j] = P[j] * P[0];
@@ -33,8 +33,8 @@ DNDSB_HD void bc_prim2cons(const real *P, real *U, real gamma)
 
 // ghost state UR of the boundary zone for the inner state UL and outward unit normal n;
 // false for a zone without a supported boundary type
-template <int NV>
-DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real *n, real *UR)
+template <int NV, typename T>
+DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const T *UL, const real *n, T *UR)
 {
     if (zone < 0 || zone >= b.nZone)
         return false;
@@ -48,11 +48,11 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real 
     {
         // generateBV_FarField: supersonic out / subsonic out (far pressure) / subsonic in
         // (inner pressure) / supersonic in, switched on the normal velocity
-        real un = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) / UL[0];
-        real vsqr = (UL[1] * UL[1] + UL[2] * UL[2] + UL[3] * UL[3]) / (UL[0] * UL[0]);
-        real p, asqr, H;
+        T un = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) / UL[0];
+        T vsqr = (UL[1] * UL[1] + UL[2] * UL[2] + UL[3] * UL[3]) / (UL[0] * UL[0]);
+        T p, asqr, H;
         gas_thermal(UL[4], UL[0], vsqr, g, p, asqr, H);
-        real a = sqrt(asqr);
+        T a = sqrt(asqr);
         if (un - a > 0)
         {
             for (int v = 0; v < NV; v++)
@@ -60,7 +60,8 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real 
         }
         else if (un > 0)
         {
-            real fp[NV], lp[NV];
+            real fp[NV];
+            T lp[NV];
             bc_cons2prim<NV>(far, fp, g);
             bc_cons2prim<NV>(UL, lp, g);
             lp[4] = fp[4];
@@ -68,8 +69,11 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real 
         }
         else if (un + a > 0)
         {
-            real fp[NV], lp[NV];
-            bc_cons2prim<NV>(far, fp, g);
+            real fp0[NV];
+            T fp[NV], lp[NV];
+            bc_cons2prim<NV>(far, fp0, g);
+            for (int v = 0; v < NV; v++)
+                fp[v] = fp0[v];
             bc_cons2prim<NV>(UL, lp, g);
             fp[4] = lp[4];
             bc_prim2cons<NV>(fp, UR, g);
@@ -87,7 +91,7 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real 
         // generateBV_InviscidWall: momentum mirrored about the face
         for (int v = 0; v < NV; v++)
             UR[v] = UL[v];
-        real mn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
+        T mn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
         for (int d = 0; d < 3; d++)
             UR[1 + d] -= 2 * mn * n[d];
         return true;
@@ -102,7 +106,7 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real 
             UR[1 + d] = -UR[1 + d];
         if (type == BC_WALL_ISOTHERMAL)
         {
-            real P[NV];
+            T P[NV];
             bc_cons2prim<NV>(UR, P, g);
             P[0] = P[4] / far[0] / b.Rgas;
             bc_prim2cons<NV>(P, UR, g);
@@ -124,15 +128,15 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const real *UL, const real 
 }
 
 // CompressRecPart: the cell mean replaces a reconstructed value with rho < 0 or e < 0
-template <int NV>
-DNDSB_HD void compress_rec(const real *um, const real *U, real *out)
+template <int NV, typename T>
+DNDSB_HD void compress_rec(const T *um, const T *U, T *out)
 {
     for (int v = 0; v < NV; v++)
         out[v] = U[v];
     if (out[0] < 0)
         for (int v = 0; v < NV; v++)
             out[v] = um[v];
-    real eK = (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) * 0.5 / (kVerySmall + out[0]);
+    T eK = (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) * 0.5 / (kVerySmall + out[0]);
     if (out[4] - eK < 0)
         for (int v = 0; v < NV; v++)
             out[v] = um[v];

@@ -159,6 +159,20 @@ extern "C"
                 c2f[c * nf + k] = (int32_t)((f << 1) | side);
                 nbr[c * nf + k] = f2c[f * 2 + 1 - side];
             }
+        // slot of each face in the neighbour's row (for transposed sweeps gathered per cell)
+        std::vector<int32_t> slot(nCell * nf, -1);
+        for (int64_t c = 0; c < nCell; c++)
+            for (int k = 0; k < nf; k++)
+            {
+                int o = nbr[c * nf + k];
+                if (o < 0)
+                    continue;
+                int64_t f = cell2face[c * nf + k];
+                int side = face2cell[f * 2] == c ? 0 : 1;
+                for (int j = 0; j < nf; j++)
+                    if (cell2face[(int64_t)o * nf + j] == f && (o != c || (c2f[(int64_t)o * nf + j] & 1) != side))
+                        slot[c * nf + k] = j;
+            }
         // greedy multicolouring, first fit in cell order: on a mesh numbered
         // colour by colour this reproduces the numbering's own classes, and the
         // colour-ordered sweep equals the sequential sweep of the reference
@@ -214,6 +228,7 @@ extern "C"
         rc |= upload(&d.facePShift, facePShift, nFace * 3);
         rc |= upload(&d.cell2face, c2f.data(), nCell * nf);
         rc |= upload(&d.cellNbr, nbr.data(), nCell * nf);
+        rc |= upload(&d.nbrSlot, slot.data(), nCell * nf);
         rc |= upload(&d.colorCells, cells.data(), nCell);
         rc |= upload(&d.cellColor, color.data(), nCell);
         if (!bFace.empty())
@@ -236,7 +251,7 @@ extern "C"
             return DNDSB_OK;
         MeshD &d = m->d;
         for (void *p : {(void *)d.coords, (void *)d.cell2node, (void *)d.cellShift, (void *)d.face2node, (void *)d.faceShift, (void *)d.face2cell,
-                        (void *)d.faceZone, (void *)d.facePShift, (void *)d.cell2face, (void *)d.cellNbr, (void *)d.colorCells, (void *)d.cellColor,
+                        (void *)d.faceZone, (void *)d.facePShift, (void *)d.cell2face, (void *)d.cellNbr, (void *)d.nbrSlot, (void *)d.colorCells, (void *)d.cellColor,
                         (void *)d.bndFace, (void *)d.bndCell})
             dev_free(p);
         delete m;
@@ -428,6 +443,29 @@ extern "C"
         return DNDSB_OK;
     }
 
+    int dndsb_vr_iter_vjp(dndsb_vr *v, const double *cot, const double *uRec, const double *u, int nVars, double *vRec, double *vU, void *stream)
+    {
+        if (!v || !cot || !uRec || !u || !vRec || !vU)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp: null argument");
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp: call construct_rec_coeff first");
+        if (v->mesh->nBndFace > 0 && v->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp: the mesh has boundary faces; set their boundary table first");
+        return status_msg(vr_vjp(v->mesh->d, v->g, v->vr, nVars, cot, uRec, u, vRec, vU, S(stream)), "dndsb_vr_iter_vjp");
+    }
+
+    int dndsb_vr_iter_jvp(dndsb_vr *v, const double *dRec, const double *du, const double *uRec, const double *u, int nVars, double *dRecNew,
+                          void *stream)
+    {
+        if (!v || !dRec || !du || !uRec || !u || !dRecNew)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp: null argument");
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp: call construct_rec_coeff first");
+        if (v->mesh->nBndFace > 0 && v->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp: the mesh has boundary faces; set their boundary table first");
+        return status_msg(vr_jvp(v->mesh->d, v->g, v->vr, nVars, dRec, du, uRec, u, dRecNew, S(stream)), "dndsb_vr_iter_jvp");
+    }
+
     int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s)
     {
         if (!out || !vr || !s)
@@ -483,7 +521,7 @@ extern "C"
             return DNDSB_OK;
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
-                        (void *)e->e.facePt, (void *)e->e.cellPar})
+                        (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -515,6 +553,34 @@ extern "C"
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: the mesh has boundary faces; call dndsb_eval_set_bc first");
         return status_msg(eval_rhs(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, u, uRec, rhs, nullptr, S(stream)), "dndsb_eval_evaluate_rhs");
+    }
+
+    int dndsb_eval_rhs_vjp(dndsb_eval *e, const double *w, const double *u, const double *uRec, double *du, double *duRec, void *stream)
+    {
+        if (!e || !w || !u || !uRec || !du || !duRec)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        int rc = rhs_vjp(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, w, u, uRec, du, duRec, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(rc, "dndsb_eval_rhs_vjp: needs nVars = 5 and ignoreVis (the viscous flux is not differentiated yet)");
+        return status_msg(rc, "dndsb_eval_rhs_vjp");
+    }
+
+    int dndsb_eval_rhs_jvp(dndsb_eval *e, const double *du, const double *duRec, const double *u, const double *uRec, double *dRhs, void *stream)
+    {
+        if (!e || !du || !duRec || !u || !uRec || !dRhs)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        int rc = rhs_jvp(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, du, duRec, u, uRec, dRhs, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(rc, "dndsb_eval_rhs_jvp: needs nVars = 5 and ignoreVis (the viscous flux is not differentiated yet)");
+        return status_msg(rc, "dndsb_eval_rhs_jvp");
     }
 
     int dndsb_eval_lusgs_matrix_init(dndsb_eval *e, const double *dTau, double dt, double alphaDiag, double *jdiag, void *stream)

@@ -8,6 +8,7 @@
 // reproduce (paths relative to the reference project root).
 #pragma once
 #include "platform.cuh"
+#include "dual.cuh"
 #include <math.h>
 
 namespace dndsb
@@ -434,7 +435,10 @@ DNDSB_HD void basis_table(real *T, int rows, real x, real y, real z, const real 
 // entropy fixes, :1434-1490 dispatch).  Physics is 3-D with 5 conservative
 // variables (NS / NS_3D; the SA variable is handled by the caller).
 // ---------------------------------------------------------------------------
-DNDSB_HD void gas_thermal(real E, real rho, real vSqr, real gamma, real &p, real &asqr, real &H)
+// The state-dependent routines below are templated on the scalar type T: real
+// for the solver, Dual<N> (dual.cuh) for directional derivatives.
+template <typename T>
+DNDSB_HD void gas_thermal(T E, T rho, T vSqr, real gamma, T &p, T &asqr, T &H)
 {
     p = (gamma - 1) * (E - rho * 0.5 * vSqr);
     asqr = gamma * p / rho;
@@ -457,28 +461,37 @@ enum RSType : int
     RS_Roe_M8 = 18
 };
 
-DNDSB_HD real sign_tol(real a, real tol) { return a > tol ? 1 : (a < -tol ? -1 : 0); }
+template <typename T>
+DNDSB_HD real sign_tol(const T &a, const T &tol) { return a > tol ? 1 : (a < -tol ? -1 : 0); }
 
-struct RoeAvg
+template <typename T>
+DNDSB_HD T dot3v(const T *a, const real *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+template <typename T>
+DNDSB_HD T dot3s(const T *a, const T *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+template <typename T>
+struct RoeAvgT
 {
-    real vL[3], vR[3], aL, aR, pLm, pRm;
-    real v[3], vsqr, H, asqr, a, rho;
+    T vL[3], vR[3], aL, aR, pLm, pRm;
+    T v[3], vsqr, H, asqr, a, rho;
 };
+using RoeAvg = RoeAvgT<real>;
 
-DNDSB_HD void roe_average(const real *ULm, const real *URm, real gamma, RoeAvg &r)
+template <typename T>
+DNDSB_HD void roe_average(const T *ULm, const T *URm, real gamma, RoeAvgT<T> &r)
 {
-    real iL = 1.0 / ULm[0], iR = 1.0 / URm[0];
+    T iL = 1.0 / ULm[0], iR = 1.0 / URm[0];
     for (int d = 0; d < 3; d++)
         r.vL[d] = ULm[1 + d] * iL, r.vR[d] = URm[1 + d] * iR;
-    real pL, pR, aL2, aR2, HL, HR;
-    gas_thermal(ULm[4], ULm[0], dot3(r.vL, r.vL), gamma, pL, aL2, HL);
-    gas_thermal(URm[4], URm[0], dot3(r.vR, r.vR), gamma, pR, aR2, HR);
+    T pL, pR, aL2, aR2, HL, HR;
+    gas_thermal(ULm[4], ULm[0], dot3s(r.vL, r.vL), gamma, pL, aL2, HL);
+    gas_thermal(URm[4], URm[0], dot3s(r.vR, r.vR), gamma, pR, aR2, HR);
     r.aL = sqrt(aL2), r.aR = sqrt(aR2), r.pLm = pL, r.pRm = pR;
-    real sL = sqrt(ULm[0]), sR = sqrt(URm[0]);
-    real is = 1.0 / (sL + sR);
+    T sL = sqrt(ULm[0]), sR = sqrt(URm[0]);
+    T is = 1.0 / (sL + sR);
     for (int d = 0; d < 3; d++)
         r.v[d] = (sL * r.vL[d] + sR * r.vR[d]) * is;
-    r.vsqr = dot3(r.v, r.v);
+    r.vsqr = dot3s(r.v, r.v);
     r.H = (sL * HL + sR * HR) * is;
     r.asqr = (gamma - 1) * (r.H - 0.5 * r.vsqr);
     r.rho = sL * sR;
@@ -486,13 +499,14 @@ DNDSB_HD void roe_average(const real *ULm, const real *URm, real gamma, RoeAvg &
 }
 
 // physical flux through n (no grid velocity): Gas.hpp:390-397
-DNDSB_HD void phys_flux(const real *U, const real *n, real gamma, real F[5], real &p, real &asqr)
+template <typename T>
+DNDSB_HD void phys_flux(const T *U, const real *n, real gamma, T F[5], T &p, T &asqr)
 {
-    real ir = 1.0 / U[0];
-    real v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
-    real H;
-    gas_thermal(U[4], U[0], dot3(v, v), gamma, p, asqr, H);
-    real vn = dot3(v, n);
+    T ir = 1.0 / U[0];
+    T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
+    T H;
+    gas_thermal(U[4], U[0], dot3s(v, v), gamma, p, asqr, H);
+    T vn = dot3v(v, n);
     F[0] = U[0] * vn;
     F[1] = U[1] * vn + p * n[0];
     F[2] = U[2] * vn + p * n[1];
@@ -501,47 +515,51 @@ DNDSB_HD void phys_flux(const real *U, const real *n, real gamma, real F[5], rea
 }
 
 // Roe wave strengths (Gas.hpp:1098-1109): jump incU projected on the Roe eigenvectors
-struct RoeWaves
+template <typename T>
+struct RoeWavesT
 {
-    real a0, a1, a4, a23T[3], vRoeN;
+    T a0, a1, a4, a23T[3], vRoeN;
 };
 
-DNDSB_HD void roe_waves(const real *incU, const real *n, const RoeAvg &r, real gamma, RoeWaves &w)
+template <typename T>
+DNDSB_HD void roe_waves(const T *incU, const real *n, const RoeAvgT<T> &r, real gamma, RoeWavesT<T> &w)
 {
-    w.vRoeN = dot3(r.v, n);
-    real incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
-    real a23[3] = {incU[1] - incU[0] * r.v[0], incU[2] - incU[0] * r.v[1], incU[3] - incU[0] * r.v[2]};
-    real a23n = dot3(a23, n);
+    w.vRoeN = dot3v(r.v, n);
+    T incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
+    T a23[3] = {incU[1] - incU[0] * r.v[0], incU[2] - incU[0] * r.v[1], incU[3] - incU[0] * r.v[2]};
+    T a23n = dot3v(a23, n);
     for (int d = 0; d < 3; d++)
         w.a23T[d] = a23[d] - n[d] * a23n;
-    real incU4b = incU[4] - dot3(w.a23T, r.v);
+    T incU4b = incU[4] - dot3s(w.a23T, r.v);
     w.a1 = (gamma - 1) / r.asqr * (incU[0] * (r.H - w.vRoeN * w.vRoeN) + w.vRoeN * incU123N - incU4b);
     w.a0 = (incU[0] * (w.vRoeN + r.a) - incU123N - r.a * w.a1) / (2 * r.a);
     w.a4 = incU[0] - (w.a0 + w.a1);
 }
 
 // |A| dU assembled from wave strengths times eigenvalues (Gas.hpp:1110-1124)
-DNDSB_HD void roe_dissipation(const RoeWaves &w, const real *n, const RoeAvg &r, real l0, real l123, real l4, real incF[5])
+template <typename T>
+DNDSB_HD void roe_dissipation(const RoeWavesT<T> &w, const real *n, const RoeAvgT<T> &r, const T &l0, const T &l123, const T &l4, T incF[5])
 {
-    real a0 = w.a0 * l0, a1 = w.a1 * l123, a4 = w.a4 * l4;
-    real t[3] = {w.a23T[0] * l123, w.a23T[1] * l123, w.a23T[2] * l123};
+    T a0 = w.a0 * l0, a1 = w.a1 * l123, a4 = w.a4 * l4;
+    T t[3] = {w.a23T[0] * l123, w.a23T[1] * l123, w.a23T[2] * l123};
     incF[0] = a0 + a1 + a4;
-    incF[4] = (r.H - w.vRoeN * r.a) * a0 + 0.5 * r.vsqr * a1 + (r.H + w.vRoeN * r.a) * a4 + dot3(t, r.v);
+    incF[4] = (r.H - w.vRoeN * r.a) * a0 + 0.5 * r.vsqr * a1 + (r.H + w.vRoeN * r.a) * a4 + dot3s(t, r.v);
     for (int d = 0; d < 3; d++)
         incF[1 + d] = (r.v[d] - r.a * n[d]) * a0 + (r.v[d] + r.a * n[d]) * a4 + r.v[d] * a1 + t[d];
 }
 
 // Gas.hpp:878-1007 Roe_EntropyFixer (eigScheme 0,1,3..8)
-DNDSB_HD void roe_entropy_fix(int es, real aL, real aR, real aAve, real uL, real uR, real uAve, real VAve, real dLambda,
-                              real fixScale, real incFScale, real &lam0, real &lam123, real &lam4)
+template <typename T>
+DNDSB_HD void roe_entropy_fix(int es, const T &aL, const T &aR, const T &aAve, const T &uL, const T &uR, const T &uAve, const T &VAve,
+                              real dLambda, real fixScale, real incFScale, T &lam0, T &lam123, T &lam4)
 {
     const real sHY = 0.05 * fixScale, sLD = 0.2 * fixScale, sHF = 0.25 * fixScale;
     if (es == 0)
     {
-        auto flim = [&](real v, real lam, real lamL, real lamR)
+        auto flim = [&](const T &v, const T &lam, const T &lamL, const T &lamR)
         {
-            real th = dmax(dmax(0.0, lam - lamL), lamR - lam) * sHY;
-            return v < th ? (v * v / th + th) * 0.5 : v;
+            T th = dmax(dmax(T(0.0), lam - lamL), lamR - lam) * sHY;
+            return v < th ? T((v * v / th + th) * 0.5) : v;
         };
         lam0 = flim(lam0, uAve - aAve, uL - aL, uR - aR);
         lam123 = flim(lam123 * incFScale, uAve, uL, uR);
@@ -549,46 +567,46 @@ DNDSB_HD void roe_entropy_fix(int es, real aL, real aR, real aAve, real uL, real
     }
     else if (es == 1)
     {
-        real uLm = sign_tol(uL, aL * kSmall) * dmax(fabs(uL) * incFScale, aL * sLD);
-        real uRm = sign_tol(uR, aR * kSmall) * dmax(fabs(uR) * incFScale, aR * sLD);
+        T uLm = sign_tol(uL, T(aL * kSmall)) * dmax(T(fabs(uL) * incFScale), T(aL * sLD));
+        T uRm = sign_tol(uR, T(aR * kSmall)) * dmax(T(fabs(uR) * incFScale), T(aR * sLD));
         lam0 = dmax(fabs(uLm - aL), fabs(uRm - aR));
         lam123 = dmax(fabs(uLm), fabs(uRm));
         lam4 = dmax(fabs(uLm + aL), fabs(uRm + aR));
     }
     else if (es == 3)
     {
-        real aS = dmin(fabs(uAve) / sLD, aAve);
+        T aS = dmin(T(fabs(uAve) / sLD), aAve);
         lam0 = fabs(uAve * incFScale - aS);
         lam4 = fabs(uAve * incFScale + aS);
     }
     else if (es == 4)
     {
-        real uS = sign_tol(uAve, aAve * kSmall) * dmax(aAve * sLD, fabs(uAve) * incFScale);
+        T uS = sign_tol(uAve, T(aAve * kSmall)) * dmax(T(aAve * sLD), T(fabs(uAve) * incFScale));
         lam0 = fabs(uS - aAve), lam123 = fabs(uS), lam4 = fabs(uS + aAve);
     }
     else if (es == 5)
     {
-        real vL = uL * incFScale, vR = uR * incFScale;
-        real aLm = dmin(aL, fabs(vL) / sLD), aRm = dmin(aR, fabs(vR) / sLD);
+        T vL = uL * incFScale, vR = uR * incFScale;
+        T aLm = dmin(aL, T(fabs(vL) / sLD)), aRm = dmin(aR, T(fabs(vR) / sLD));
         lam0 = dmax(fabs(vL - aLm), fabs(vR - aRm));
         lam123 = dmax(fabs(vL), fabs(vR));
         lam4 = dmax(fabs(vL + aLm), fabs(vR + aRm));
     }
     else if (es == 6 || es == 8)
     {
-        lam0 = dmax(fabs(uAve * incFScale - aAve), dLambda * sHF);
-        lam4 = dmax(fabs(uAve * incFScale + aAve), dLambda * sHF);
-        lam123 = dmax(fabs(uAve * incFScale), dLambda * sHF);
+        lam0 = dmax(T(fabs(uAve * incFScale - aAve)), T(dLambda * sHF));
+        lam4 = dmax(T(fabs(uAve * incFScale + aAve)), T(dLambda * sHF));
+        lam123 = dmax(T(fabs(uAve * incFScale)), T(dLambda * sHF));
     }
     else if (es == 7)
     {
-        lam0 *= fabs(uAve * incFScale - aAve);
-        lam4 *= fabs(uAve * incFScale + aAve);
-        lam123 *= fabs(uAve * incFScale);
+        lam0 = lam0 * fabs(uAve * incFScale - aAve);
+        lam4 = lam4 * fabs(uAve * incFScale + aAve);
+        lam123 = lam123 * fabs(uAve * incFScale);
     }
     if (es == 7 || es == 8)
     {
-        real th = sHY * (VAve + aAve), th2 = th * th;
+        T th = sHY * (VAve + aAve), th2 = th * th;
         if (lam0 < th)
             lam0 = (lam0 * lam0 + th2) / (2 * th);
         if (lam4 < th)
@@ -602,43 +620,44 @@ DNDSB_HD void roe_entropy_fix(int es, real aL, real aR, real aAve, real uL, real
 // Returns false when a state is non-physical (the caller records an error).
 // The Roe averages r come from the cell-mean states (Gas.hpp:229-259) and are
 // shared by all Gauss points of a face.
-DNDSB_HD bool riemann_flux_pre(int rs, const real *UL, const real *UR, const RoeAvg &r, const real *n, real gamma, real dLambda,
-                               real fixScale, real incFScale, real F[5], real &lam0, real &lam123, real &lam4)
+template <typename T>
+DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T> &r, const real *n, real gamma, real dLambda, real fixScale,
+                               real incFScale, T F[5], T &lam0, T &lam123, T &lam4)
 {
-    real FL[5], FR[5], pL, pR, aL2, aR2;
+    T FL[5], FR[5], pL, pR, aL2, aR2;
     phys_flux(UL, n, gamma, FL, pL, aL2);
     phys_flux(UR, n, gamma, FR, pR, aR2);
     bool ok = UL[0] > 0 && UR[0] > 0 && r.asqr > 0;
-    real vRoe0 = dot3(r.v, n);
+    T vRoe0 = dot3v(r.v, n);
     lam0 = fabs(vRoe0 - r.a), lam123 = fabs(vRoe0), lam4 = fabs(vRoe0 + r.a);
-    real vLm0 = dot3(r.vL, n), vRm0 = dot3(r.vR, n);
-    real incU[5];
+    T vLm0 = dot3v(r.vL, n), vRm0 = dot3v(r.vR, n);
+    T incU[5];
     for (int i = 0; i < 5; i++)
         incU[i] = UR[i] - UL[i];
     if (rs == RS_HLLEP || rs == RS_HLLEP_V1)
     {
-        RoeWaves w;
+        RoeWavesT<T> w;
         roe_waves(incU, n, r, gamma, w);
-        real SL = dmin(vRoe0 - r.a, vLm0 - sqrt(aL2));
-        real SR = dmax(vRoe0 + r.a, vRm0 + sqrt(aR2));
-        real dfix = r.a / (r.a + dmax(fabs(vRoe0), dLambda * fixScale));
-        real SP = dmax(SR, 0.0), SM = dmin(SL, 0.0);
+        T SL = dmin(T(vRoe0 - r.a), T(vLm0 - sqrt(aL2)));
+        T SR = dmax(T(vRoe0 + r.a), T(vRm0 + sqrt(aR2)));
+        T dfix = r.a / (r.a + dmax(T(fabs(vRoe0)), T(dLambda * fixScale)));
+        T SP = dmax(SR, T(0.0)), SM = dmin(SL, T(0.0));
         if (rs == RS_HLLEP)
         {
-            real div = SP - SM;
-            div += (div >= 0 ? 1 : -1) * kVerySmall;
-            real id = 1.0 / div;
-            real rv1[5] = {1, r.v[0], r.v[1], r.v[2], 0.5 * r.vsqr};
+            T div = SP - SM;
+            div = div + (div >= 0 ? 1 : -1) * kVerySmall;
+            T id = 1.0 / div;
+            T rv1[5] = {T(1), r.v[0], r.v[1], r.v[2], T(0.5 * r.vsqr)};
             for (int i = 0; i < 5; i++)
                 F[i] = (SP * FL[i] - SM * FR[i]) * id + (SP * SM * id) * (incU[i] - dfix * rv1[i] * w.a1);
         }
         else
         {
-            real dd = 1.0 / (SP - SM);
+            T dd = 1.0 / (SP - SM);
             lam123 = fabs(((SP + SM) * vRoe0 - 2.0 * (1.0 - dfix) * (SP * SM)) * dd);
             lam4 = fabs(((SP + SM) * (vRoe0 + r.a) - 2.0 * (SP * SM)) * dd);
             lam0 = fabs(((SP + SM) * (vRoe0 - r.a) - 2.0 * (SP * SM)) * dd);
-            real incF[5];
+            T incF[5];
             roe_dissipation(w, n, r, lam0, lam123, lam4, incF);
             for (int i = 0; i < 5; i++)
                 F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * incF[i];
@@ -647,11 +666,11 @@ DNDSB_HD bool riemann_flux_pre(int rs, const real *UL, const real *UR, const Roe
     }
     if (rs == RS_HLLC)
     {
-        auto q = [&](real p, real pS)
-        { return pS <= p ? 1.0 : sqrt(1 + (gamma + 1) / 2 / gamma * (pS / p - 1)); };
-        real pS = dmax(0.0, 0.5 * (r.pLm + r.pRm) - 0.5 * (vLm0 - vRm0) * r.rho * r.a);
-        real SL = vLm0 - r.aL * q(r.pLm, pS);
-        real SR = vRm0 + r.aR * q(r.pRm, pS);
+        auto q = [&](const T &p, const T &pS)
+        { return pS <= p ? T(1.0) : T(sqrt(1 + (gamma + 1) / 2 / gamma * (pS / p - 1))); };
+        T pS = dmax(T(0.0), T(0.5 * (r.pLm + r.pRm) - 0.5 * (vLm0 - vRm0) * r.rho * r.a));
+        T SL = vLm0 - r.aL * q(r.pLm, pS);
+        T SR = vRm0 + r.aR * q(r.pRm, pS);
         if (0 <= SL)
         {
             for (int i = 0; i < 5; i++)
@@ -664,14 +683,14 @@ DNDSB_HD bool riemann_flux_pre(int rs, const real *UL, const real *UR, const Roe
                 F[i] = FR[i];
             return ok;
         }
-        real div = UL[0] * (SL - vLm0) - UR[0] * (SR - vRm0);
-        real ULn = UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2], URn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
-        real SS = fabs(div) > kVerySmall ? (pR - pL + ULn * (SL - vLm0) - URn * (SR - vRm0)) / div : 0.0;
-        real DS[5] = {0, n[0], n[1], n[2], SS};
-        const real *U = SS >= 0 ? UL : UR;
-        const real *FF = SS >= 0 ? FL : FR;
-        real S = SS >= 0 ? SL : SR, vm = SS >= 0 ? vLm0 : vRm0, pp = SS >= 0 ? pL : pR;
-        real dv = S - SS;
+        T div = UL[0] * (SL - vLm0) - UR[0] * (SR - vRm0);
+        T ULn = UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2], URn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
+        T SS = fabs(div) > kVerySmall ? T((pR - pL + ULn * (SL - vLm0) - URn * (SR - vRm0)) / div) : T(0.0);
+        T DS[5] = {T(0), T(n[0]), T(n[1]), T(n[2]), SS};
+        const T *U = SS >= 0 ? UL : UR;
+        const T *FF = SS >= 0 ? FL : FR;
+        T S = SS >= 0 ? SL : SR, vm = SS >= 0 ? vLm0 : vRm0, pp = SS >= 0 ? pL : pR;
+        T dv = S - SS;
         if (fabs(dv) < kVerySmall)
             for (int i = 0; i < 5; i++)
                 F[i] = FF[i];
@@ -684,26 +703,27 @@ DNDSB_HD bool riemann_flux_pre(int rs, const real *UL, const real *UR, const Roe
     int es = rs == RS_Roe ? 0 : rs - 10;
     if (es == 2)
     {
-        lam0 = lam123 = lam4 = dmax(fabs(vLm0) + r.aL, fabs(vRm0) + r.aR);
+        lam0 = lam123 = lam4 = dmax(T(fabs(vLm0) + r.aL), T(fabs(vRm0) + r.aR));
         for (int i = 0; i < 5; i++)
             F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * lam0 * incU[i];
         return ok;
     }
-    real VAve = sqrt(r.vsqr);
+    T VAve = sqrt(r.vsqr);
     roe_entropy_fix(es, r.aL, r.aR, r.a, vLm0, vRm0, vRoe0, VAve, dLambda, fixScale, incFScale, lam0, lam123, lam4);
-    RoeWaves w;
+    RoeWavesT<T> w;
     roe_waves(incU, n, r, gamma, w);
-    real incF[5];
+    T incF[5];
     roe_dissipation(w, n, r, lam0, lam123, lam4, incF);
     for (int i = 0; i < 5; i++)
         F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * incF[i];
     return ok;
 }
 
-DNDSB_HD bool riemann_flux(int rs, const real *UL, const real *UR, const real *ULm, const real *URm, const real *n, real gamma,
-                           real dLambda, real fixScale, real incFScale, real F[5], real &lam0, real &lam123, real &lam4)
+template <typename T>
+DNDSB_HD bool riemann_flux(int rs, const T *UL, const T *UR, const T *ULm, const T *URm, const real *n, real gamma, real dLambda,
+                           real fixScale, real incFScale, T F[5], T &lam0, T &lam123, T &lam4)
 {
-    RoeAvg r;
+    RoeAvgT<T> r;
     roe_average(ULm, URm, gamma, r);
     return riemann_flux_pre(rs, UL, UR, r, n, gamma, dLambda, fixScale, incFScale, F, lam0, lam123, lam4);
 }

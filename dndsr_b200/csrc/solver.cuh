@@ -52,6 +52,7 @@ struct MeshD
     real *facePShift = nullptr; // [nFace][3]
     int32_t *cell2face = nullptr; // [nCell][nf], packed (face << 1) | side
     int32_t *cellNbr = nullptr;   // [nCell][nf], neighbour cell or -1
+    int32_t *nbrSlot = nullptr;   // [nCell][nf], slot of the same face in the neighbour's row (-1 on boundaries)
     // multicolour ordering for Gauss-Seidel type sweeps
     int nColor = 0;
     int32_t *colorCells = nullptr; // cells grouped by colour
@@ -137,6 +138,7 @@ struct EvalD
     real *facePt = nullptr;   // [nGf][nFace][7]: point, unit normal, |J| w (layout of the tuned face kernel)
     real *cellPar = nullptr;  // [nCell][6]: centre, 1/L
     real *redBuf = nullptr;   // scratch for reductions
+    real *adjBuf = nullptr;   // scratch of the derivative kernels [nFace][2][(R+1) nv], allocated on first use
     int *errWord = nullptr;   // device error word
 };
 
@@ -177,6 +179,18 @@ int vr_iter_bc(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real
                int uRecIsZero, int useFP32, cudaStream_t st);
 // writes the face flux of every boundary face
 int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st);
+
+// ---- derivatives (adjoint.cu): VJP / JVP of EvaluateRHS and of one VR Jacobi sweep ----
+// deltaLambdaCell (the entropy-fix scale of the last EvaluateDt) is held fixed, as between the
+// reference's EvaluateDt and EvaluateRHS calls
+int rhs_vjp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *w, const real *u, const real *uRec, real *du, real *duRec,
+            cudaStream_t st);
+int rhs_jvp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *du, const real *duRec, const real *u, const real *uRec,
+            real *dRhs, cudaStream_t st);
+int vr_vjp(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *v, const real *uRec, const real *u, real *vRec, real *vU,
+           cudaStream_t st);
+int vr_jvp(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *dRec, const real *du, const real *uRec, const real *u,
+           real *dRecNew, cudaStream_t st);
 
 // ---- native linear solve (linsolve.cu) and its Krylov reductions (reduce.cu) ----
 struct LinSettings

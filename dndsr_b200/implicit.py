@@ -181,9 +181,15 @@ class SolverConfig:
     dtImplicit: float = 0.01
     nTimeStep: int = 100
     nTimeStepInternal: int = 20
-    rhsThresholdInternal: float = 1e-8
+    nTimeStepInternalMin: int = 5
+    rhsThresholdInternal: float = 1e-10
+    normOrd: int = 1
+    useVolWiseResidual: bool = False
     CFL: float = 100.0
     useLocalDt: bool = True
+    nCFLRampStart: int = 2 ** 31 - 1
+    nCFLRampLength: int = 2 ** 31 - 1
+    CFLRampEnd: float = 0.0
     nInternalRecStep: int = 1
     jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi
     sgsIter: int = 0
@@ -211,7 +217,8 @@ class ImplicitSolver:
         self.jd = torch.zeros(nc, dtype=torch.float64, device=dev)
         self.tmp = torch.zeros((nc, nv), dtype=torch.float64, device=dev)
         self.gmres = GMRES(cfg.nGmresSpace, self.tmp) if cfg.gmresCode else None
-        self.res0 = None
+        self.resBase = None
+        self.CFLNow = cfg.CFL
         self.n_rhs = 0
         self.n_sgs = 0
 
@@ -224,7 +231,7 @@ class ImplicitSolver:
 
     # EulerSolver.hxx:674-694
     def fdtau(self, cx, dtau, alphaDiag):
-        self.ev.EvaluateDt(dtau, cx, self.cfg.CFL, 1e100, self.cfg.useLocalDt)
+        self.ev.EvaluateDt(dtau, cx, self.CFLNow, 1e100, self.cfg.useLocalDt)
         dtau.mul_(1.0 / alphaDiag)
 
     # EulerSolver.hxx:696-738 without the positivity limiting (AddFixedIncrement with alpha = 1)
@@ -281,13 +288,23 @@ class ImplicitSolver:
         self.gmres.solve(FA, FML, fdot, cres, x, self.cfg.nGmresIter, lambda i, r, rb: False)
         cxInc.copy_(x)
 
+    # EulerSolver_Init.hxx:490-733 functor_fstop: per-variable norm of the unsteady residual against
+    # the running maximum of the step, density only; CFL ramp in log space
     def fstop(self, it, res, stage):
-        nrm = self.ev.EvaluateNorm(res, 1, True)
-        r = float(np.linalg.norm(nrm))
-        if it == 1:
-            self.res0 = r
-        self.cfg.res_history.append((stage, it, r))
-        return r <= self.cfg.rhsThresholdInternal * max(self.res0, 1e-300) or it >= self.cfg.nTimeStepInternal
+        cfg = self.cfg
+        nrm = np.asarray(self.ev.EvaluateNorm(res, cfg.normOrd, cfg.useVolWiseResidual), dtype=np.float64)
+        if it == 1 or self.resBase is None:
+            self.resBase = np.zeros_like(nrm)
+        self.resBase = np.maximum(self.resBase, nrm)
+        rel = nrm / (self.resBase + VERY_SMALL)
+        stop = bool(rel[0] < cfg.rhsThresholdInternal) and it >= cfg.nTimeStepInternalMin
+        cfg.res_history.append((stage, it, float(rel[0])))
+        if cfg.nCFLRampStart <= it <= cfg.nCFLRampLength + cfg.nCFLRampStart:
+            inter = (it - cfg.nCFLRampStart) / cfg.nCFLRampLength
+            self.CFLNow = math.exp(math.log(cfg.CFL) + math.log(cfg.CFLRampEnd / cfg.CFL) * inter)
+        if stop or it >= cfg.nTimeStepInternal:
+            self.CFLNow = cfg.CFL
+        return stop
 
     def run(self, u, n_steps=None, dt=None):
         cfg = self.cfg

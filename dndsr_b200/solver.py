@@ -170,6 +170,23 @@ class VariationalReconstruction(Handle):
                   int(putIntoNew), int(recordInc), int(uRecIsZero), 1 if precision == "fp32" else 0, _stream())
 
 
+    def DoReconstructionIterVJP(self, cot, uRec, u):
+        """Vector-Jacobian product of one Jacobi sweep uRecNew = S(uRec, u): returns
+        ((dS/duRec)^T cot, (dS/du)^T cot)."""
+        vRec, vU = torch.empty_like(uRec), torch.empty_like(u)
+        capi.call("dndsb_vr_iter_vjp", self.h, _ptr(cot, "cot"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1], _ptr(vRec, "vRec"),
+                  _ptr(vU, "vU"), _stream())
+        return vRec, vU
+
+    def DoReconstructionIterJVP(self, dRec, du, uRec, u):
+        """Jacobian-vector product of one Jacobi sweep (DoReconstructionIterDiff with the
+        linearised boundary term): dS/duRec dRec + dS/du du."""
+        out = torch.empty_like(uRec)
+        capi.call("dndsb_vr_iter_jvp", self.h, _ptr(dRec, "dRec"), _ptr(du, "du"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1],
+                  _ptr(out, "dRecNew"), _stream())
+        return out
+
+
 class EulerEvaluator(Handle):
     """Euler::EulerEvaluator<model> on the GPU (models NS / NS_3D with 5 variables)."""
     _destroy = "dndsb_eval_destroy"
@@ -219,6 +236,20 @@ class EulerEvaluator(Handle):
         For callers that cannot allocate device memory when they evaluate a
         residual; calls that overlap on the same GPU share the array and race."""
         capi.call("dndsb_eval_evaluate_rhs_noalloc", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+
+    def EvaluateRHSVJP(self, w, u, uRec):
+        """(dR/du)^T w and (dR/duRec)^T w of EvaluateRHS at (u, uRec), deltaLambdaCell held fixed."""
+        du, duRec = torch.empty_like(u), torch.empty_like(uRec)
+        capi.call("dndsb_eval_rhs_vjp", self.h, _ptr(w, "w"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(du, "du"), _ptr(duRec, "duRec"),
+                  _stream())
+        return du, duRec
+
+    def EvaluateRHSJVP(self, du, duRec, u, uRec):
+        """dR/du du + dR/duRec duRec of EvaluateRHS at (u, uRec), deltaLambdaCell held fixed."""
+        out = torch.empty_like(u)
+        capi.call("dndsb_eval_rhs_jvp", self.h, _ptr(du, "du"), _ptr(duRec, "duRec"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(out, "dRhs"),
+                  _stream())
+        return out
 
     def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag):
         capi.call("dndsb_eval_lusgs_matrix_init", self.h, _ptr(dTau, "dTau"), float(dt), float(alphaDiag), _ptr(jdiag, "jdiag"), _stream())

@@ -136,6 +136,15 @@ int dndsb_vr_do_reconstruction_iter(dndsb_vr *vr, double *uRec, double *uRecNew,
  * A mesh with boundary faces needs this table before its first sweep. */
 int dndsb_vr_set_boundary(dndsb_vr *vr, int nZone, const int32_t *type, const double *value, int nVars, double gamma, double Rgas);
 
+/* Derivatives of one DoReconstructionIter Jacobi sweep uRecNew = S(uRec, u) (putIntoNew, FP64
+ * coefficients), including the boundary term GetBoundaryRHS and its linearisation (the
+ * reference's DoReconstructionIterDiff / GetBoundaryRHSDiff, _Reconstruction.hxx:99-176,617-670):
+ * vjp: cot [nCell][R][nVars] -> vRec = (dS/duRec)^T cot, vU = (dS/du)^T cot
+ * jvp: (dRec, du) -> dRecNew = dS/duRec dRec + dS/du du */
+int dndsb_vr_iter_vjp(dndsb_vr *vr, const double *cot, const double *uRec, const double *u, int nVars, double *vRec, double *vU, void *stream);
+int dndsb_vr_iter_jvp(dndsb_vr *vr, const double *dRec, const double *du, const double *uRec, const double *u, int nVars, double *dRecNew,
+                      void *stream);
+
 /* ---- Euler evaluator: EulerEvaluator.hpp:76-1980 ---- */
 int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s);
 int dndsb_eval_destroy(dndsb_eval *ev);
@@ -161,6 +170,14 @@ int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, c
 /* LUSGSMatrixVec(alphaDiag, t, u, uInc, JDiag, AuInc), EulerEvaluator.hxx:175-274 */
 int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
                                 double *AuInc, void *stream);
+/* Derivatives of EvaluateRHS (EulerEvaluator_EvaluateRHS.hxx:55-818) with respect to the cell
+ * means u and the reconstruction uRec, at the deltaLambdaCell of the last evaluate_dt (held
+ * fixed): vjp: w [nCell][5] -> du = (dR/du)^T w, duRec = (dR/duRec)^T w; jvp: (du, duRec) -> dRhs.
+ * Inviscid (ignoreVis) 5-variable models; Gauss-point states are recomputed, not stored.  The
+ * reference has no hand-written adjoint of this path (its Python package differentiates nothing). */
+int dndsb_eval_rhs_vjp(dndsb_eval *ev, const double *w, const double *u, const double *uRec, double *du, double *duRec, void *stream);
+int dndsb_eval_rhs_jvp(dndsb_eval *ev, const double *du, const double *duRec, const double *u, const double *uRec, double *dRhs, void *stream);
+
 /* Linear-solver controls, EulerSolver.hpp linearSolverControl (fields of the same names) plus the
  * precision of the solve.  meanScale: the GMRES dot weights of EulerSolver.hxx:1518-1540
  * (dot(a, b) = sum a_v b_v / (meanScale_v + 1e-200)^2); entries <= 0 count as 1. */
