@@ -128,7 +128,7 @@ def test_solve_linear_weighted_dot_and_errors():
 def test_driver_gpu_matches_oracle_driver():
     """Three ESDIRK4 steps of the isentropic vortex, 4 pseudo iterations each:
     the GPU driver (native linear solve) against the same driver on the oracle."""
-    m, o, vr, ev = _setup(lambda: M.iv_mesh(10), 2, 2, "Roe", 0.0)
+    m, o, vr, ev = _setup(lambda: M.iv_mesh(10), 2, "Roe", 0.0)
     kw = dict(odeCode=0, dtImplicit=0.05, nTimeStep=3, nTimeStepInternal=4, CFL=20.0, gmresCode=1, nGmresSpace=5, sgsIter=0)
     u_o = torch.tensor(o.init_field(2, 5.0))
     I.ImplicitSolver(OracleVR(o), OracleEval(o), I.SolverConfig(**kw)).run(u_o)
