@@ -39,6 +39,14 @@ UNIT = "Mcell*RHS/s"
 B_RHS = 8 * ((9 + 2) * 5 + (2 * 3 + 1 + 9) + 3 * (9 * (2 * 3 + 1) + 1))
 B_VR = 8 * (6 * 81 + 6 * 9) + 8 * (2 * 9 * 5 + 5)
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes per cell of one k_rhs_face_fast launch (the face kernel: 97% of EvaluateRHS; the per-cell
+# gather adds ~4% more bytes), from the ncu capture of the same workload at 48^3 (dram__bytes_read.sum +
+# dram__bytes_write.sum = 258.0 MB for 110,592 cells); traffic grows in proportion to cells and faces, so
+# a 64^3 launch is scaled by the cell count
+RHS_TRAFFIC_PER_CELL = 258.0e6 / 48 ** 3
+RHS_FP64_PIPE_PCT = 25.2  # sm__pipe_fp64_cycles_active of the same capture
+# the reference's published TGV throughput for this path: 71.8 M cell-iterations/s on 10,240 CPU ranks
+REF_PUBLISHED_MCIPS = 71.8
 
 
 def workload_config(n, p):
@@ -258,13 +266,16 @@ def run_ours(args, rank, world, local_rank):
     dom_name, dom_t, dom_b = ("vr_jacobi_sweep", t_vr, B_VR) if t_vr >= t_rhs else ("evaluate_rhs", t_rhs, B_RHS)
     achieved = dom_b * nc / (dom_t * 1e-3) / 1e9
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": value / REF_PUBLISHED_MCIPS, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(n, p), parallelism=f"replicas{world}" if world > 1 else "single GPU"),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 3 * K,
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback 6650 GB/s",
-                         "traffic": None, "algorithmic_bytes_per_cell": dom_b},
+                         "traffic": RHS_TRAFFIC_PER_CELL * nc if dom_name == "evaluate_rhs" else None,
+                         "traffic_source": "ncu dram bytes of k_rhs_face_fast at 48^3 (profiles/), scaled by cells",
+                         "fp64_pipe_pct": RHS_FP64_PIPE_PCT if dom_name == "evaluate_rhs" else None,
+                         "algorithmic_bytes_per_cell": dom_b},
             "kernels_ms": {"vr_jacobi_sweep": t_vr, "evaluate_rhs": t_rhs,
                            "vr_GBps": B_VR * nc / (t_vr * 1e-3) / 1e9, "rhs_GBps": B_RHS * nc / (t_rhs * 1e-3) / 1e9},
             "clocks": clk.summary()}

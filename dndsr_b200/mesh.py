@@ -221,50 +221,71 @@ def bump_height(x, amp=0.05, width=25.0):
     return amp * np.exp(-width * x * x)
 
 
-def bump_channel_tet(nx=160, ny=80, nz=26, jitter=0.05, seed=0x1234, amp=0.05, L=(4.0, 1.0, 0.5)):
-    """Channel [-2,2] x [0,1] x [0,0.5] over the bump y = amp exp(-25 x^2), in tetrahedra.
-
-    A structured nx x ny x nz hexahedral grid whose vertical lines follow the bump
-    (y = h(x) + eta (1 - h(x))) is split into 6 tetrahedra per hexahedron along its
-    main diagonal (Kuhn split); interior nodes are jittered by a uniform fraction
-    ``jitter`` of the grid step in every parametric direction.  Boundary faces carry
-    the zones of ``BUMP_ZONES``.  Cells: 6 nx ny nz.
-    """
-    rng = np.random.default_rng(seed)
-    Lx, Ly, Lz = L
-    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
-    xi, eta, zeta = i / nx, j / ny, k / nz
-    interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
-    if jitter:
-        for a, n in ((xi, nx), (eta, ny), (zeta, nz)):
-            a += np.where(interior, rng.uniform(-jitter / n, jitter / n, size=a.shape), 0.0)
-    x = -Lx / 2 + Lx * xi
-    h = bump_height(x, amp)
-    y = h + eta * (Ly - h)
-    z = Lz * zeta
-    nid = lambda a, b, c: (a * (ny + 1) + b) * (nz + 1) + c
-    coords = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
-    ci, cj, ck = [a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")]
-    tets = []
+def _kuhn_offsets():
+    """Vertex offsets of the 6 tetrahedra of a unit hexahedron split along its main diagonal."""
+    out = []
     for perm in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
         off = np.zeros((4, 3), dtype=np.int64)
         off[1, perm[0]] = 1
         off[2] = off[1]
         off[2, perm[1]] = 1
         off[3] = 1
-        tets.append(np.stack([nid(ci + o[0], cj + o[1], ck + o[2]) for o in off], axis=1))
+        out.append(off)
+    return out
+
+
+def bump_channel_tet(nx=160, ny=80, nz=26, jitter=0.05, seed=0x1234, amp=0.05, L=(4.0, 1.0, 0.5), periodic_z=False):
+    """Channel [-2,2] x [0,1] x [0,0.5] over the bump y = amp exp(-25 x^2), in tetrahedra.
+
+    A structured nx x ny x nz hexahedral grid whose vertical lines follow the bump
+    (y = h(x) + eta (1 - h(x))) is split into 6 tetrahedra per hexahedron along its
+    main diagonal (Kuhn split); interior nodes are jittered by a uniform fraction
+    ``jitter`` of the grid step in every parametric direction.  Boundary faces carry
+    the zones of ``BUMP_ZONES``; with ``periodic_z`` the two side planes are joined
+    periodically instead (translation Lz) and carry no zone.  Cells: 6 nx ny nz.
+    """
+    rng = np.random.default_rng(seed)
+    Lx, Ly, Lz = L
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    xi, eta, zeta = i / nx, j / ny, k / nz
+    kin = (k > 0) & (k < nz) if not periodic_z else (k < nz)
+    interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & kin
+    if jitter:
+        for a, n in ((xi, nx), (eta, ny), (zeta, nz)):
+            a += np.where(interior, rng.uniform(-jitter / n, jitter / n, size=a.shape), 0.0)
+    if periodic_z:  # the k = nz plane is the image of k = 0
+        for a in (xi, eta, zeta):
+            a[:, :, nz] = a[:, :, 0]
+        zeta[:, :, nz] += 1.0
+    x = -Lx / 2 + Lx * xi
+    h = bump_height(x, amp)
+    y = h + eta * (Ly - h)
+    z = Lz * zeta
+    nz_id = nz if periodic_z else nz + 1
+    nid = lambda a, b, c: (a * (ny + 1) + b) * nz_id + (c % nz_id)
+    sel = np.s_[:, :, :nz_id]
+    coords = np.stack([x[sel].ravel(), y[sel].ravel(), z[sel].ravel()], axis=1)
+    ci, cj, ck = [a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")]
+    tets = [np.stack([nid(ci + o[0], cj + o[1], ck + o[2]) for o in off], axis=1) for off in _kuhn_offsets()]
     c2n = np.stack(tets, axis=1).reshape(-1, 4).astype(np.int64)  # 6 tets of one hexahedron are consecutive
-    X = coords[c2n]
+    csh = np.zeros((c2n.shape[0], 4, 3))
+    if periodic_z:  # vertices on the k = nz plane are images of k = 0, shifted by Lz
+        kk = np.stack([np.stack([ck + o[2] for o in off6], axis=1) for off6 in _kuhn_offsets()], axis=1).reshape(-1, 4)
+        csh[:, :, 2] = np.where(kk >= nz, Lz, 0.0)
+    X = coords[c2n] + csh
     vol6 = np.einsum("ij,ij->i", np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0]), X[:, 3] - X[:, 0])
     neg = vol6 < 0
     c2n[neg, 1], c2n[neg, 2] = c2n[neg, 2].copy(), c2n[neg, 1].copy()
-    csh = np.zeros((c2n.shape[0], 4, 3))
+    csh[neg, 1], csh[neg, 2] = csh[neg, 2].copy(), csh[neg, 1].copy()
     f2n, fsh, f2c, fps, c2f, fz = _build_faces(TET4, c2n, csh)
     bnd = f2c[:, 1] < 0
-    I, J, K = i.ravel(), j.ravel(), k.ravel()
+    I, J, K = i[sel].ravel(), j[sel].ravel(), k[sel].ravel()
     fn = f2n[bnd]
     zone = np.zeros(fn.shape[0], dtype=np.int32)
-    for nm, test in (("inflow", I == 0), ("outflow", I == nx), ("bump", J == 0), ("top", J == ny), ("side0", K == 0), ("side1", K == nz)):
+    tests = [("inflow", I == 0), ("outflow", I == nx), ("bump", J == 0), ("top", J == ny)]
+    if not periodic_z:
+        tests += [("side0", K == 0), ("side1", K == nz)]
+    for nm, test in tests:
         zone[np.all(test[fn], axis=1)] = BUMP_ZONES[nm]
     if np.any(zone == 0):
         raise RuntimeError("unclassified boundary face")

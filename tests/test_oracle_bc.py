@@ -22,6 +22,18 @@ def test_bump_mesh_is_valid():
     assert set(np.unique(m.face_zone[bnd])) == set(M.BUMP_ZONES.values()) and np.all(m.face_zone[~bnd] == 0)
 
 
+def test_bump_mesh_with_periodic_sides():
+    m = M.bump_channel_tet(8, 4, 3, periodic_z=True)
+    X = m.cell_coords()
+    v6 = np.einsum("ij,ij->i", np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0]), X[:, 3] - X[:, 0])
+    x = np.linspace(-2, 2, 9)
+    assert v6.min() > 0 and abs(v6.sum() / 6 - (2.0 - np.trapezoid(M.bump_height(x), x) * 0.5)) < 1e-12
+    bnd = m.face2cell[:, 1] < 0
+    assert set(np.unique(m.face_zone[bnd])) == {1, 2, 3, 4}
+    per = np.abs(m.face_pshift[:, 2]) > 0
+    assert np.allclose(np.abs(m.face_pshift[per, 2]), 0.5) and per.sum() == 2 * 8 * 4
+
+
 @pytest.mark.parametrize("p", [1, 2])
 def test_freestream_is_preserved_in_a_flat_channel(p):
     m = M.bump_channel_tet(6, 3, 2, amp=0.0)
