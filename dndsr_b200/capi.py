@@ -83,6 +83,7 @@ SIGNATURES = {
     "dndsb_eval_solve_linear": [_P, _P, _d, _P, _d, _P, _P, _P, _P],
     "dndsb_vr_set_boundary": [_P, _i, _I32, _D, _i, _d, _d],
     "dndsb_eval_set_bc": [_P, _i, _I32, _D],
+    "dndsb_eval_set_wall_distance": [_P, _D],
     "dndsb_vr_iter_vjp": [_P, _P, _P, _P, _i, _P, _P, _P],
     "dndsb_vr_iter_jvp": [_P, _P, _P, _P, _P, _i, _P, _P],
     "dndsb_eval_rhs_vjp": [_P, _P, _P, _P, _P, _P, _P],

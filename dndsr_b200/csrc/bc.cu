@@ -8,6 +8,7 @@
 #include "solver.cuh"
 #include "basis_eval.cuh"
 #include "bc.cuh"
+#include "sa.cuh"
 
 namespace dndsb
 {
@@ -53,7 +54,7 @@ DNDSB_GLOBAL void k_vr_bc(MeshD m, GeomD g, VRD vr, const TC *__restrict__ AAInv
                     UL[v] = a;
                 }
                 compress_rec<NV>(uc, UL, ULf);
-                if (!bc_value<NV>(vr.bnd, zone, ULf, n, UB))
+                if (!bc_value_fix<NV>(vr.bnd, zone, ULf, n, UB))
                     for (int v = 0; v < NV; v++)
                         UB[v] = ULf[v];
                 real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q] * w0 * w0;
@@ -90,7 +91,7 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
                            const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1;
-    const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
+    const real gamma = s.gamma;
     DNDSB_KERNEL_LOOP(ii, m.nBndFace)
     {
         int64_t f = m.bndFace[ii];
@@ -135,7 +136,7 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
                 for (int d = 0; d < 3; d++)
                     GL[d * NV + v] = ga[d];
             }
-            if (!bc_value<NV>(vr.bnd, zone, UL, n, UR))
+            if (!bc_value_fix<NV>(vr.bnd, zone, UL, n, UR))
                 for (int v = 0; v < NV; v++)
                     UR[v] = UL[v];
             real Fv[NV];
@@ -154,17 +155,15 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
                     for (int v = 0; v < NV; v++)
                         GM[d * NV + v] = GL[d * NV + v] + iD * (n[d] * (UR[v] - UL[v]));
                 grad_cons2prim<NV>(UM, GM, GP, gamma);
-                real pM, a2M, HM;
-                gas_thermal(UM[4], UM[0], (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) / (UM[0] * UM[0]), gamma, pM, a2M, HM);
-                real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
-                real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
                 if (!slip)
-                    viscous_flux<NV>(UM, GP, n, type == BC_WALL, gamma, mu, cp * mu / s.prGas, cp, Fv);
+                    point_viscous_flux<NV>(s, UM, GP, n, type == BC_WALL, Fv);
             }
             real F[NV], l0, l1, l4;
             for (int v = 0; v < NV; v++)
                 F[v] = 0;
             bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+            if (NV == 6)
+                F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
             for (int v = 0; v < NV; v++)
                 fluxEs[v] -= (F[v] - Fv[v]) * JW;

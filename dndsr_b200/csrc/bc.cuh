@@ -127,6 +127,19 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const T *UL, const real *n,
     return false;
 }
 
+// the ghost state at a Gauss point with fixUL (USE_FIX_ZERO_SA_NUT_AT_WALL,
+// EulerEvaluator_EvaluateDt.hxx:2291-2296): on wall types the SA variable of both the inner
+// state (modified in place) and the ghost is set to zero
+template <int NV, typename T>
+DNDSB_HD bool bc_value_fix(const BoundaryD &b, int zone, T *UL, const real *n, T *UR)
+{
+    bool ok = bc_value<NV>(b, zone, UL, n, UR);
+    if (ok && NV > 5 && (b.type[zone] == BC_WALL || b.type[zone] == BC_WALL_ISOTHERMAL))
+        for (int j = 5; j < NV; j++)
+            UL[j] = UR[j] = T(0.0);
+    return ok;
+}
+
 // CompressRecPart: the cell mean replaces a reconstructed value with rho < 0 or e < 0
 template <int NV, typename T>
 DNDSB_HD void compress_rec(const T *um, const T *U, T *out)

@@ -302,7 +302,7 @@ extern "C"
         GeomD &g = v->g;
         for (void *p : {(void *)g.vol, (void *)g.cellBary, (void *)g.cellCent, (void *)g.cellScale, (void *)g.cellJDet, (void *)g.cellPP,
                         (void *)g.smoothRatio, (void *)g.faceArea, (void *)g.faceCent, (void *)g.faceJDet, (void *)g.facePP, (void *)g.faceNorm,
-                        (void *)g.faceMeanNorm, (void *)g.cellQw, (void *)g.faceQw, (void *)v->vr.baseMoment, (void *)v->vr.faceWeight,
+                        (void *)g.faceMeanNorm, (void *)g.cellQw, (void *)g.faceQw, (void *)g.hMax, (void *)v->vr.baseMoment, (void *)v->vr.faceWeight,
                         (void *)v->vr.faceL, (void *)v->vr.AAInvB, (void *)v->vr.AInvb, (void *)v->vr.matA, (void *)v->vr.AAInvB32,
                         (void *)v->vr.AInvb32, (void *)v->errWord, (void *)v->vr.bnd.type, (void *)v->vr.bnd.val})
             dev_free(p);
@@ -363,6 +363,7 @@ extern "C"
         else if (n == "cellJDet") src = g.cellJDet, cnt = m.nCell * g.nGc;
         else if (n == "cellPP") src = g.cellPP, cnt = m.nCell * g.nGc * 3;
         else if (n == "smoothRatio") src = g.smoothRatio, cnt = m.nCell;
+        else if (n == "cellHMax") src = g.hMax, cnt = m.nCell;
         else if (n == "faceArea") src = g.faceArea, cnt = m.nFace;
         else if (n == "faceCent") src = g.faceCent, cnt = m.nFace * 3;
         else if (n == "faceJDet") src = g.faceJDet, cnt = m.nFace * g.nGf;
@@ -489,11 +490,15 @@ extern "C"
         rc |= dev_alloc((void **)&e->e.faceFlux, sizeof(real) * std::max(m.nFace, m.nCell) * s->nVars);
         rc |= dev_alloc((void **)&e->e.redBuf, sizeof(real) * kRedBufLen);
         rc |= dev_alloc((void **)&e->e.errWord, sizeof(int));
+        if (s->nVars == 6)
+            rc |= dev_alloc((void **)&e->e.jSource, sizeof(real) * m.nCell * 6);
         if (rc)
         {
             dndsb_eval_destroy(e);
             return cuda_fail("dndsb_eval_create");
         }
+        if (e->e.jSource)
+            cudaMemset(e->e.jSource, 0, sizeof(real) * m.nCell * 6);
         if (fast_geometry(m, vr->g, vr->vr, e->e, 0) != ST_OK)
         {
             dndsb_eval_destroy(e);
@@ -515,13 +520,28 @@ extern "C"
         return DNDSB_OK;
     }
 
+    int dndsb_eval_set_wall_distance(dndsb_eval *e, const double *dHost)
+    {
+        if (!e || !dHost)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_wall_distance: null argument");
+        const MeshD &m = e->vr->mesh->d;
+        int64_t n = m.nCell * (int64_t)e->vr->g.nGc;
+        if (n <= 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_wall_distance: construct the reconstruction first");
+        dev_free(e->e.dWall);
+        e->e.dWall = nullptr;
+        if (upload(&e->e.dWall, dHost, n))
+            return cuda_fail("dndsb_eval_set_wall_distance");
+        return DNDSB_OK;
+    }
+
     int dndsb_eval_destroy(dndsb_eval *e)
     {
         if (!e)
             return DNDSB_OK;
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
-                        (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf})
+                        (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -552,6 +572,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: VR not constructed");
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (e->e.s.nVars == 6 && !e->e.dWall)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
         return status_msg(eval_rhs(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, u, uRec, rhs, nullptr, S(stream)), "dndsb_eval_evaluate_rhs");
     }
 
@@ -663,6 +685,7 @@ extern "C"
         else if (n == "lambdaFaceVis") src = e->e.lambdaFaceVis, cnt = m.nFace;
         else if (n == "deltaLambdaCell") src = e->e.deltaLambdaCell, cnt = m.nCell;
         else if (n == "faceFlux") src = e->e.faceFlux, cnt = m.nFace * e->e.s.nVars;
+        else if (n == "jSource" && e->e.jSource) src = e->e.jSource, cnt = m.nCell * e->e.s.nVars;
         else
             return fail(DNDSB_E_BADARG, "dndsb_eval_get_array: unknown name " + n);
         if (len)

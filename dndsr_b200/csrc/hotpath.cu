@@ -3,6 +3,7 @@
 // SGS sweeps and the LU-SGS matrix-vector product.
 #include "solver.cuh"
 #include "basis_eval.cuh"
+#include "sa.cuh"
 
 namespace dndsb
 {
@@ -166,16 +167,14 @@ DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const r
                     for (int v = 0; v < NV; v++)
                         GM[d * NV + v] = (GR[d * NV + v] + GL[d * NV + v]) * 0.5 + iD * (n[d] * (UR[v] - UL[v]));
                 grad_cons2prim<NV>(UM, GM, GP, gamma);
-                real pM, a2M, HM;
-                gas_thermal(UM[4], UM[0], (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) / (UM[0] * UM[0]), gamma, pM, a2M, HM);
-                real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
-                real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
-                viscous_flux<NV>(UM, GP, n, false, gamma, mu, cp * mu / s.prGas, cp, Fv);
+                point_viscous_flux<NV>(s, UM, GP, n, false, Fv);
             }
-            real F[5], l0, l1, l4;
+            real F[NV], l0, l1, l4;
             bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+            if (NV == 6)
+                F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
-            for (int v = 0; v < 5; v++)
+            for (int v = 0; v < NV; v++)
                 fluxEs[v] -= (F[v] - Fv[v]) * JW;
         }
         if (bad || !finite5(fluxEs, NV))
@@ -247,6 +246,8 @@ DNDSB_GLOBAL void k_dt_face(MeshD m, GeomD g, EulerSettingsD s, const real *__re
         real lamC = dmax(aL + fabs(vnL), aR + fabs(vnR));
         real T = pM / ((gamma - 1) / gamma * cp * uM[0]);
         real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, uM[0], T);
+        if (NV == 6)
+            mu += sa_mu_tur(uM, s.muGas, mu);
         real lamVis = mu / uM[0] * dmax(4. / 3., gamma / s.prGas);
         real area = g.faceArea[f];
         real vis = lamVis * area * (1. / g.vol[c0] + 1. / volR);
@@ -280,8 +281,9 @@ DNDSB_GLOBAL void k_dt_cell(MeshD m, GeomD g, const real *__restrict__ lamFace, 
 // LU-SGS (EulerEvaluator.hxx:37-159 init, :550-693 UpdateSGS, :175-274 MatrixVec)
 // scalar Jacobian, inviscid flux-increment Jacobian EulerEvaluator.hpp:1100-1158
 // ---------------------------------------------------------------------------
+// nd = 1: one diagonal per cell; nd = nv (SA model): fp plus alphaDiag JSource per variable
 DNDSB_GLOBAL void k_lusgs_init(MeshD m, GeomD g, const real *__restrict__ lamFace, const real *__restrict__ dTau, real dt, real alphaDiag,
-                               real *jdiag)
+                               const real *__restrict__ jSource, int nd, real *jdiag)
 {
     DNDSB_KERNEL_LOOP(c, m.nCell)
     {
@@ -292,7 +294,8 @@ DNDSB_GLOBAL void k_lusgs_init(MeshD m, GeomD g, const real *__restrict__ lamFac
             int64_t f = m.cell2face[c * m.nf + k] >> 1;
             fp += (0.5 * alphaDiag) * g.faceArea[f] * lamFace[f] * iv;
         }
-        jdiag[c] = fp;
+        for (int v = 0; v < nd; v++)
+            jdiag[c * nd + v] = fp + (nd > 1 ? alphaDiag * jSource[c * nd + v] : 0.0);
     }
 }
 
@@ -351,9 +354,9 @@ DNDSB_GLOBAL void k_sgs_color(MeshD m, GeomD g, real gamma, const real *__restri
             for (int v = 0; v < NV; v++)
                 buf[v] -= w * dF[v];
         }
-        real id = 1.0 / jdiag[c];
         for (int v = 0; v < NV; v++)
         {
+            real id = 1.0 / jdiag[NV == 6 ? c * NV + v : c];
             real nv = buf[v] * id;
             absInc[c * NV + v] = fabs(nv - uIncNew[c * NV + v]);
             uIncNew[c * NV + v] = nv;
@@ -387,7 +390,7 @@ DNDSB_GLOBAL void k_matvec(MeshD m, GeomD g, real gamma, const real *__restrict_
                 buf[v] -= w * dF[v];
         }
         for (int v = 0; v < NV; v++)
-            AuInc[c * NV + v] = jdiag[c] * uInc[c * NV + v] - buf[v];
+            AuInc[c * NV + v] = jdiag[NV == 6 ? c * NV + v : c] * uInc[c * NV + v] - buf[v];
     }
 }
 
@@ -429,6 +432,56 @@ DNDSB_GLOBAL void k_init_field(MeshD m, GeomD g, real gamma, int kind, real chi,
         }
         for (int v = 0; v < NV; v++)
             u[c * NV + v] = um[v] / g.vol[c];
+    }
+}
+
+// EvaluateRHS.hxx:665-801 for the SA model: the source at the cell Gauss points (state and
+// conservative gradient from the reconstruction), integrated and divided by the volume, added to
+// rhs; the mode-1 diagonal Jacobian gives JSource.  The NS source is zero.
+template <int DIM, int P>
+DNDSB_GLOBAL void k_sa_source(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec,
+                              const real *__restrict__ dWall, real *rhs, real *jSource)
+{
+    constexpr int NV = 6, NDOF = ndof_of<DIM>(P), R = NDOF - 1;
+    const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
+    DNDSB_KERNEL_LOOP(c, m.nCell)
+    {
+        real S = 0, J = 0;
+        real hMax = g.hMax[c];
+        for (int q = 0; q < g.nGc; q++)
+        {
+            real T[(DIM + 1) * NDOF];
+            cell_basis<DIM, NDOF>(&g.cellCent[c * 3], &g.cellScale[c * 3], &vr.baseMoment[c * NDOF], vr.s.anisotropicLengths,
+                                  &g.cellPP[(c * g.nGc + q) * 3], DIM + 1, T);
+            real U[NV], G[3 * NV];
+            for (int v = 0; v < NV; v++)
+            {
+                real a = u[c * NV + v];
+                real ga[3] = {0, 0, 0};
+                for (int j = 0; j < R; j++)
+                {
+                    real x = uRec[(c * R + j) * NV + v];
+                    a += T[1 + j] * x;
+                    for (int d = 0; d < DIM; d++)
+                        ga[d] += T[(1 + d) * NDOF + 1 + j] * x;
+                }
+                U[v] = a;
+                for (int d = 0; d < 3; d++)
+                    G[d * NV + v] = ga[d];
+            }
+            real pM, a2M, HM;
+            gas_thermal(U[4], U[0], (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / (U[0] * U[0]), gamma, pM, a2M, HM);
+            real Tm = pM / ((gamma - 1) / gamma * cp * U[0]);
+            real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, U[0], Tm);
+            real d = dmin(dWall[c * g.nGc + q], pow(kVeryLarge, 1. / 6.));
+            real lLES = dmin(hMax * kVeryLarge, dmax(d, hMax));
+            real JW = g.cellJDet[c * g.nGc + q] * g.cellQw[q];
+            S += sa_source(U, G, s.muGas, mu, d, lLES, hMax, 0) * JW;
+            J += sa_source(U, G, s.muGas, mu, d, lLES, hMax, 1) * JW;
+        }
+        rhs[c * NV + 5] += S / g.vol[c];
+        for (int v = 0; v < NV; v++)
+            jSource[c * NV + v] = v == 5 ? J / g.vol[c] : 0.0;
     }
 }
 
@@ -518,43 +571,73 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
     real *ff = faceFlux ? faceFlux : ev.faceFlux;
     dev_zero(ev.errWord, sizeof(int), st);
     int nv = ev.s.nVars;
-    if (nv != 5)
+    if (nv != 5 && nv != 6)
         return ST_UNSUPPORTED;
-    int frc = rhs_face_fast(m, g, vr, ev, u, uRec, ff, st);
+    int frc = nv == 5 ? rhs_face_fast(m, g, vr, ev, u, uRec, ff, st) : ST_UNSUPPORTED;
     if (frc == ST_CUDA)
         return ST_CUDA;
-    if (frc == ST_OK)
+    if (frc != ST_OK)
     {
-        int brc = rhs_bc(m, g, vr, ev, u, uRec, ff, st);
-        if (brc != ST_OK)
-            return brc;
-        DNDSB_LAUNCH(k_rhs_gather<5>, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ff, rhs);
-        return check(st, ev.errWord, true);
-    }
-#define DNDSB_RF(D, PP) DNDSB_LAUNCH((k_rhs_face<D, PP, 5>), m.nFace, 128, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord)
-    if (m.dim == 2)
-    {
-        if (vr.P == 1)
-            DNDSB_RF(2, 1);
-        else if (vr.P == 2)
-            DNDSB_RF(2, 2);
+#define DNDSB_RF(D, PP, NVV) DNDSB_LAUNCH((k_rhs_face<D, PP, NVV>), m.nFace, 128, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord)
+#define DNDSB_RF_P(D, NVV)        \
+    do                            \
+    {                             \
+        if (vr.P == 1)            \
+            DNDSB_RF(D, 1, NVV);  \
+        else if (vr.P == 2)       \
+            DNDSB_RF(D, 2, NVV);  \
+        else                      \
+            DNDSB_RF(D, 3, NVV);  \
+    } while (0)
+        if (m.dim == 2)
+        {
+            if (nv == 5)
+                DNDSB_RF_P(2, 5);
+            else
+                DNDSB_RF_P(2, 6);
+        }
         else
-            DNDSB_RF(2, 3);
-    }
-    else
-    {
-        if (vr.P == 1)
-            DNDSB_RF(3, 1);
-        else if (vr.P == 2)
-            DNDSB_RF(3, 2);
-        else
-            DNDSB_RF(3, 3);
-    }
+        {
+            if (nv == 5)
+                DNDSB_RF_P(3, 5);
+            else
+                DNDSB_RF_P(3, 6);
+        }
+#undef DNDSB_RF_P
 #undef DNDSB_RF
+    }
     int brc = rhs_bc(m, g, vr, ev, u, uRec, ff, st);
     if (brc != ST_OK)
         return brc;
-    DNDSB_LAUNCH(k_rhs_gather<5>, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ff, rhs);
+    if (nv == 5)
+        DNDSB_LAUNCH(k_rhs_gather<5>, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ff, rhs);
+    else
+    {
+        DNDSB_LAUNCH(k_rhs_gather<6>, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ff, rhs);
+        // SA source (EvaluateRHS.hxx:665-801) and its Jacobian diagonal JSource
+        if (!ev.dWall)
+            return ST_BADARG;
+#define DNDSB_SAS(D, PP) DNDSB_LAUNCH((k_sa_source<D, PP>), m.nCell, 64, st, m, g, vr, ev.s, u, uRec, ev.dWall, rhs, ev.jSource)
+        if (m.dim == 2)
+        {
+            if (vr.P == 1)
+                DNDSB_SAS(2, 1);
+            else if (vr.P == 2)
+                DNDSB_SAS(2, 2);
+            else
+                DNDSB_SAS(2, 3);
+        }
+        else
+        {
+            if (vr.P == 1)
+                DNDSB_SAS(3, 1);
+            else if (vr.P == 2)
+                DNDSB_SAS(3, 2);
+            else
+                DNDSB_SAS(3, 3);
+        }
+#undef DNDSB_SAS
+    }
     return check(st, ev.errWord, true);
 }
 
@@ -584,7 +667,10 @@ int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, 
 
 int lusgs_init(const MeshD &m, const GeomD &g, EvalD &ev, const real *dTau, real dt, real alphaDiag, real *jdiag, cudaStream_t st)
 {
-    DNDSB_LAUNCH(k_lusgs_init, m.nCell, 256, st, m, g, ev.lambdaFace, dTau, dt, alphaDiag, jdiag);
+    int nd = ev.s.nVars == 6 ? 6 : 1;
+    if (nd > 1 && !ev.jSource)
+        return ST_BADARG;
+    DNDSB_LAUNCH(k_lusgs_init, m.nCell, 256, st, m, g, ev.lambdaFace, dTau, dt, alphaDiag, ev.jSource, nd, jdiag);
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 

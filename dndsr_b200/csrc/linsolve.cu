@@ -46,10 +46,14 @@ struct Vec4<double>
 // ---------------------------------------------------------------------------
 // operator build: LUSGSMatrixInit (EulerEvaluator.hxx:37-159) + packing
 // ---------------------------------------------------------------------------
+// JD: diagonals per cell (1, or NV with the SA source Jacobian)
+template <typename T, int NV>
+constexpr int jd_of() { return NV == 6 ? NV : 1; }
+
 template <typename T, int NV>
 DNDSB_GLOBAL void k_sgsop_build(MeshD m, GeomD g, const real *__restrict__ lamFace, const real *__restrict__ dTau, real dt, real alphaDiag,
-                                const real *__restrict__ u, const int32_t *__restrict__ cellPos, int32_t *nbrPos,
-                                typename Vec4<T>::type *op, T *jd, T *uT)
+                                const real *__restrict__ u, const real *__restrict__ jSource, const int32_t *__restrict__ cellPos,
+                                int32_t *nbrPos, typename Vec4<T>::type *op, T *jd, T *uT)
 {
     DNDSB_KERNEL_LOOP(p, m.nCell)
     {
@@ -73,7 +77,9 @@ DNDSB_GLOBAL void k_sgsop_build(MeshD m, GeomD g, const real *__restrict__ lamFa
             int o = m.cellNbr[c * m.nf + k];
             nbrPos[p * m.nf + k] = o < 0 ? -1 : cellPos[o];
         }
-        jd[p] = (T)fp;
+        constexpr int JD = jd_of<T, NV>();
+        for (int v = 0; v < JD; v++)
+            jd[p * JD + v] = (T)(fp + (JD > 1 ? alphaDiag * jSource[c * NV + v] : 0.0));
         for (int v = 0; v < NV; v++)
             uT[p * NV + v] = (T)u[c * NV + v];
     }
@@ -169,9 +175,9 @@ DNDSB_GLOBAL void k_sgs_pos(int64_t pBeg, int64_t pEnd, const int32_t *__restric
             for (int v = 0; v < NV; v++)
                 buf[v] -= dF[v];
         }
-        T id = T(1) / jd[p];
+        constexpr int JD = jd_of<T, NV>();
         for (int v = 0; v < NV; v++)
-            xNew[p * NV + v] = buf[v] * id;
+            xNew[p * NV + v] = buf[v] * (T(1) / jd[p * JD + (JD > 1 ? v : 0)]);
     }
 }
 
@@ -197,8 +203,9 @@ DNDSB_GLOBAL void k_matvec_pos(int64_t n, const int32_t *__restrict__ nbrPos, co
             for (int v = 0; v < NV; v++)
                 buf[v] -= dF[v];
         }
+        constexpr int JD = jd_of<T, NV>();
         for (int v = 0; v < NV; v++)
-            Ax[p * NV + v] = jd[p] * x[p * NV + v] - buf[v];
+            Ax[p * NV + v] = jd[p * JD + (JD > 1 ? v : 0)] * x[p * NV + v] - buf[v];
     }
 }
 
@@ -359,7 +366,7 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv)
     int64_t n = m.nCell * nv;
     bool ok = dev_alloc((void **)&w->cellPos, sizeof(int32_t) * m.nCell) == cudaSuccess &&
               dev_alloc((void **)&w->nbrPos, sizeof(int32_t) * m.nCell * m.nf) == cudaSuccess &&
-              dev_alloc(&w->op, 4 * es * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->jd, es * m.nCell) == cudaSuccess &&
+              dev_alloc(&w->op, 4 * es * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->jd, es * m.nCell * (nv == 6 ? 6 : 1)) == cudaSuccess &&
               dev_alloc(&w->uT, es * n) == cudaSuccess && dev_alloc(&w->rhsT, es * n) == cudaSuccess &&
               dev_alloc(&w->x, es * n) == cudaSuccess && dev_alloc(&w->tmp, es * n) == cudaSuccess &&
               dev_alloc(&w->tmp2, es * n) == cudaSuccess && dev_alloc(&w->MLb, es * n) == cudaSuccess &&
@@ -507,7 +514,9 @@ int run(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &
     auto kbuild = k_sgsop_build<T, NV>;
     auto kgather = k_gather_T<T, NV>;
     auto kscatter = k_scatter_T<T, NV>;
-    DNDSB_LAUNCH(kbuild, m.nCell, 128, cs, m, g, ev.lambdaFace, dTau, dt, alphaDiag, u, w.cellPos, w.nbrPos, (T4 *)w.op,
+    if (NV == 6 && !ev.jSource)
+        return ST_BADARG;
+    DNDSB_LAUNCH(kbuild, m.nCell, 128, cs, m, g, ev.lambdaFace, dTau, dt, alphaDiag, u, ev.jSource, w.cellPos, w.nbrPos, (T4 *)w.op,
                  (T *)w.jd, (T *)w.uT);
     DNDSB_LAUNCH(kgather, m.nCell, 256, cs, m.nCell, m.colorCells, rhs, (T *)w.rhsT);
     Solve<T, NV, NF> S{m, w, ls, (T)ev.s.gamma, cs};

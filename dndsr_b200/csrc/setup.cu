@@ -33,6 +33,75 @@ DNDSB_D void load_face_coords(const MeshD &m, int64_t f, real *cs)
 
 // FiniteVolume.cpp:22-330: volume (order-6 rule), barycentre, centre,
 // Jacobian determinants and points of the intOrder rule, aligned half box
+// FiniteVolume.cpp:288-335 cellMajorHBox with FiniteVolume.hpp:387-393 GetCellMaxLenScale: twice the
+// largest vertex extent along the principal axes of the cell's inertia tensor (integrated at
+// INT_ORDER_MAX).  Principal axes by cyclic Jacobi rotations; a fully isotropic tensor keeps the
+// coordinate axes, as the reference's diagonal perturbation does.
+DNDSB_D real cell_major_length(const MeshD &m, const real *cs, const real *bary, real vol)
+{
+    real A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    PtGeo pg;
+    real p[3], w;
+    int nMax = quad_n(m.cellType, kIntOrderMax);
+    for (int q = 0; q < nMax; q++)
+    {
+        quad_point(m.cellType, kIntOrderMax, q, p, w);
+        pt_geo(m.cellType, cs, p, pg);
+        real J = cell_jdet(m.dim, pg);
+        real x[3] = {pg.x[0] - bary[0], pg.x[1] - bary[1], pg.x[2] - bary[2]};
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                A[a][b] += x[a] * x[b] * J * w;
+    }
+    const int n = m.dim;
+    real nrm = 0;
+    for (int a = 0; a < n; a++)
+        for (int b = 0; b < n; b++)
+            A[a][b] /= vol, nrm += A[a][b] * A[a][b];
+    real V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int sweep = 0; sweep < 50; sweep++)
+    {
+        real off = 0;
+        for (int a = 0; a < n; a++)
+            for (int b = a + 1; b < n; b++)
+                off += A[a][b] * A[a][b];
+        if (off <= 1e-34 * nrm)
+            break;
+        for (int a = 0; a < n; a++)
+            for (int b = a + 1; b < n; b++)
+            {
+                if (A[a][b] == 0)
+                    continue;
+                real th = (A[b][b] - A[a][a]) / (2 * A[a][b]);
+                real t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
+                real c = 1 / sqrt(t * t + 1), s = t * c;
+                for (int k = 0; k < 3; k++)
+                {
+                    real x = A[k][a], y = A[k][b];
+                    A[k][a] = c * x - s * y, A[k][b] = s * x + c * y;
+                }
+                for (int k = 0; k < 3; k++)
+                {
+                    real x = A[a][k], y = A[b][k];
+                    A[a][k] = c * x - s * y, A[b][k] = s * x + c * y;
+                }
+                for (int k = 0; k < 3; k++)
+                {
+                    real x = V[k][a], y = V[k][b];
+                    V[k][a] = c * x - s * y, V[k][b] = s * x + c * y;
+                }
+            }
+    }
+    real h = 0;
+    for (int k = 0; k < m.nvert; k++)
+    {
+        real x[3] = {cs[k * 3] - bary[0], cs[k * 3 + 1] - bary[1], cs[k * 3 + 2] - bary[2]};
+        for (int a = 0; a < n; a++)
+            h = dmax(h, fabs(V[0][a] * x[0] + V[1][a] * x[1] + V[2][a] * x[2]));
+    }
+    return 2 * h;
+}
+
 DNDSB_GLOBAL void k_cell_metrics(MeshD m, int intOrder, GeomD g)
 {
     DNDSB_KERNEL_LOOP(c, m.nCell)
@@ -78,6 +147,7 @@ DNDSB_GLOBAL void k_cell_metrics(MeshD m, int intOrder, GeomD g)
         }
         if (m.dim == 2)
             g.cellScale[c * 3 + 2] = 1;
+        g.hMax[c] = cell_major_length(m, cs, &g.cellBary[c * 3], v);
     }
 }
 
@@ -471,6 +541,7 @@ int geom_construct(const MeshD &m, const VRSettingsD &s, GeomD &g, cudaStream_t 
     rc |= alloc_real(&g.cellJDet, m.nCell * g.nGc);
     rc |= alloc_real(&g.cellPP, m.nCell * g.nGc * 3);
     rc |= alloc_real(&g.smoothRatio, m.nCell);
+    rc |= alloc_real(&g.hMax, m.nCell);
     rc |= alloc_real(&g.faceArea, m.nFace);
     rc |= alloc_real(&g.faceCent, m.nFace * 3);
     rc |= alloc_real(&g.faceJDet, m.nFace * g.nGf);

@@ -106,6 +106,7 @@ struct GeomD
          *smoothRatio = nullptr;
     real *faceArea = nullptr, *faceCent = nullptr, *faceJDet = nullptr, *facePP = nullptr, *faceNorm = nullptr, *faceMeanNorm = nullptr;
     real *cellQw = nullptr, *faceQw = nullptr; // quadrature weights of the cell / face rule at intOrder
+    real *hMax = nullptr; // [nCell] largest extent along the inertia principal axes (GetCellMaxLenScale)
 };
 
 struct VRD
@@ -139,6 +140,8 @@ struct EvalD
     real *cellPar = nullptr;  // [nCell][6]: centre, 1/L
     real *redBuf = nullptr;   // scratch for reductions
     real *adjBuf = nullptr;   // scratch of the derivative kernels [nFace][2][(R+1) nv], allocated on first use
+    real *dWall = nullptr;    // SA: wall distance at the cell Gauss points [nCell][nGc]
+    real *jSource = nullptr;  // SA: source-term Jacobian diagonal of the last RHS [nCell][nv]
     int *errWord = nullptr;   // device error word
 };
 

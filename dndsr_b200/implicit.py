@@ -214,7 +214,7 @@ class ImplicitSolver:
         self.uRec = vr.BuildURec(nv)
         self.uRecNew = vr.BuildURec(nv)
         dev = self.uRec.device
-        self.jd = torch.zeros(nc, dtype=torch.float64, device=dev)
+        self.jd = torch.zeros((nc, nv) if nv == 6 else (nc,), dtype=torch.float64, device=dev)
         self.tmp = torch.zeros((nc, nv), dtype=torch.float64, device=dev)
         self.gmres = GMRES(cfg.nGmresSpace, self.tmp) if cfg.gmresCode else None
         self.resBase = None

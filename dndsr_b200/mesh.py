@@ -300,6 +300,64 @@ def freestream(mach, gamma=1.4, rho=1.0, p=1.0, direction=(1.0, 0.0, 0.0)):
     return np.array([rho, rho * v[0], rho * v[1], rho * v[2], p / (gamma - 1) + 0.5 * rho * v @ v])
 
 
+# boundary zones of the flat-plate mesh and their EulerBC.hpp types (BCFar 1, BCWall 2, BCSym 9); the top is a
+# symmetry plane: a far-field face there has u.n = 0, where the characteristic switch is decided by rounding
+PLATE_ZONES = {"inflow": 1, "outflow": 2, "plate": 3, "upstream": 4, "top": 5}
+PLATE_BC_TYPES = {1: 1, 2: 1, 3: 2, 4: 9, 5: 9}
+
+
+def flat_plate_hex(nx=120, ny=80, nz=4, x0=-0.25, length=1.0, y1=5e-6, growth=1.1, lz=0.05, jitter=0.02, seed=0x1234, nx_up=None):
+    """Stretched hexahedral boundary-layer mesh over a flat plate on y = 0, 0 <= x <= length.
+
+    x in [x0, length] (``nx_up`` cells upstream of the leading edge, the rest on the plate), y from
+    0 with first spacing ``y1`` and geometric ``growth`` (ny cells), z periodic over ``lz``
+    (nz cells).  Interior nodes are jittered tangentially (x and z) by a uniform fraction
+    ``jitter`` of the local spacing.  Zones: ``PLATE_ZONES``.  Cells: nx ny nz.
+    """
+    if nz < 3:
+        raise ValueError("the periodic z direction needs nz >= 3 cells")
+    rng = np.random.default_rng(seed)
+    nx_up = max(1, int(round(nx * (-x0) / (length - x0)))) if nx_up is None else nx_up
+    xs = np.concatenate([np.linspace(x0, 0.0, nx_up + 1)[:-1], np.linspace(0.0, length, nx - nx_up + 1)])
+    ys = np.concatenate([[0.0], y1 * np.cumsum(growth ** np.arange(ny))])
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz), indexing="ij")
+    x, y, z = xs[i].astype(float), ys[j].astype(float), (k * lz / nz).astype(float)
+    if jitter:
+        interior = (i > 0) & (i < nx) & (j > 0) & (j < ny)
+        hx = np.diff(xs).min()
+        x += np.where(interior, rng.uniform(-jitter, jitter, size=x.shape) * hx, 0.0)
+        z += np.where(j > 0, rng.uniform(-jitter, jitter, size=z.shape) * lz / nz, 0.0) * (j < ny)
+    nid = lambda a, b, c: (a * (ny + 1) + b) * nz + (c % nz)
+    coords = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    ci, cj, ck = [a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")]
+    corners = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    c2n = np.stack([nid(ci + a, cj + b, ck + c) for a, b, c in corners], axis=1).astype(np.int64)
+    csh = np.zeros((ci.size, 8, 3))
+    for q, (a, b, c) in enumerate(corners):
+        csh[:, q, 2] = np.where(ck + c >= nz, lz, 0.0)
+    f2n, fsh, f2c, fps, c2f, fz = _build_faces(HEX8, c2n, csh)
+    bnd = f2c[:, 1] < 0
+    I, J = i.ravel(), j.ravel()
+    fn = f2n[bnd]
+    zone = np.zeros(fn.shape[0], dtype=np.int32)
+    onx = np.all(J[fn] == 0, axis=1)
+    upstream = np.all(I[fn] <= nx_up, axis=1)
+    for nm, test in (("inflow", np.all(I[fn] == 0, axis=1)), ("outflow", np.all(I[fn] == nx, axis=1)), ("plate", onx & ~upstream),
+                     ("upstream", onx & upstream), ("top", np.all(J[fn] == ny, axis=1))):
+        zone[test] = PLATE_ZONES[nm]
+    if np.any(zone == 0):
+        raise RuntimeError("unclassified boundary face")
+    fz[bnd] = zone
+    return Mesh(3, HEX8, coords, c2n, csh, f2n, fsh, f2c, fz, fps, c2f, QUAD4)
+
+
+def plate_wall_distance(points):
+    """Distance to the plate segment {0 <= x, y = 0}: y over the plate, the distance to the leading
+    edge upstream of it.  ``points`` is (..., 3)."""
+    x, y = points[..., 0], points[..., 1]
+    return np.where(x >= 0, np.abs(y), np.sqrt(x * x + y * y))
+
+
 def greedy_colors(mesh):
     """First-fit colouring of the cell adjacency graph in cell order."""
     nbr = np.where(mesh.face2cell[mesh.cell2face, 0] == np.arange(mesh.n_cell)[:, None],

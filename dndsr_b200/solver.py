@@ -218,6 +218,11 @@ class EulerEvaluator(Handle):
         self._bc = (t, v)
         capi.call("dndsb_eval_set_bc", self.h, len(t), t.ctypes.data_as(capi._I32), capi.dptr(v))
 
+    def SetWallDistance(self, d):
+        """dWall of the SA model at every cell Gauss point, [nCell][nGc] host array."""
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        capi.call("dndsb_eval_set_wall_distance", self.h, capi.dptr(d))
+
     def InitializeUDOF(self, u, kind, chi=5.0):
         capi.call("dndsb_eval_initialize_udof", self.h, kind, float(chi), _ptr(u, "u"), _stream())
 
@@ -250,6 +255,11 @@ class EulerEvaluator(Handle):
         capi.call("dndsb_eval_rhs_jvp", self.h, _ptr(du, "du"), _ptr(duRec, "duRec"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(out, "dRhs"),
                   _stream())
         return out
+
+    def BuildJDiag(self):
+        """Diagonal array of LUSGSMatrixInit: [nCell] (one value per cell), or [nCell][nVars] for the SA model."""
+        n = self.vr.mesh.n_cell
+        return torch.zeros((n, self.nVars) if self.nVars == 6 else (n,), dtype=torch.float64, device="cuda")
 
     def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag):
         capi.call("dndsb_eval_lusgs_matrix_init", self.h, _ptr(dTau, "dTau"), float(dt), float(alphaDiag), _ptr(jdiag, "jdiag"), _stream())

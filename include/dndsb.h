@@ -152,6 +152,10 @@ int dndsb_eval_destroy(dndsb_eval *ev);
  * dndsb_vr_set_boundary, with nVars, gamma and Rgas of the evaluator; it also becomes the
  * reconstruction's FBoundary (EulerSolver.hxx:163-175). */
 int dndsb_eval_set_bc(dndsb_eval *ev, int nZone, const int32_t *type, const double *value);
+/* The SA model's wall distance dWall (EulerEvaluator.hpp dWall, one value per cell Gauss point,
+ * [nCell][nGc] in the order of the reconstruction's cell quadrature, host array).  Needed before the
+ * first RHS of a 6-variable (NS_SA) evaluator. */
+int dndsb_eval_set_wall_distance(dndsb_eval *ev, const double *dHost);
 /* InitializeUDOF special initialisers, EulerEvaluator.hxx:1039-1143:
  * kind 2 = isentropic vortex of strength chi, 3 = Taylor-Green vortex (M0 = 0.1) */
 int dndsb_eval_initialize_udof(dndsb_eval *ev, int kind, double chi, double *u, void *stream);
@@ -159,9 +163,13 @@ int dndsb_eval_initialize_udof(dndsb_eval *ev, int kind, double chi, double *u, 
 int dndsb_eval_evaluate_dt(dndsb_eval *ev, const double *u, double CFL, double MaxDt, int useLocalDt, double *dt, double *dtMinHost,
                            void *stream);
 /* EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, ...), EulerEvaluator_EvaluateRHS.hxx:55-818
- * (no limiter: uRecUnlim == uRec; source term ignored) */
+ * (no limiter: uRecUnlim == uRec).  The NS source is zero; with 6 variables (NS_SA) the SA source
+ * is integrated at the cell Gauss points and JSource (the source Jacobian diagonal) is kept for
+ * the next lusgs_matrix_init. */
 int dndsb_eval_evaluate_rhs(dndsb_eval *ev, double *rhs, const double *u, const double *uRec, void *stream);
-/* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, 0, t), EulerEvaluator.hxx:37-159 (scalar Jacobian) */
+/* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, 0, t), EulerEvaluator.hxx:37-159 (scalar Jacobian).
+ * jdiag holds one value per cell for 5 variables, and nVars values per cell for the SA model
+ * (the shared diagonal plus alphaDiag times JSource of the last RHS). */
 int dndsb_eval_lusgs_matrix_init(dndsb_eval *ev, const double *dTau, double dt, double alphaDiag, double *jdiag, void *stream);
 /* UpdateSGS(alphaDiag, t, rhs, u, uInc, uIncNew, JDiag, forward, gsUpdate, sumInc, uIncIsZero),
  * EulerEvaluator.hxx:550-693, swept colour by colour; sumIncHost [nVars] may be NULL */

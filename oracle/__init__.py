@@ -79,6 +79,7 @@ def _declare(L):
     L.orc_get.argtypes = [_V, ctypes.c_char_p, _D]
     L.orc_set_delta_lambda.argtypes = [_V, _D]
     L.orc_set_bc.argtypes = [_V, ctypes.c_int, _I, _D, ctypes.c_int]
+    L.orc_set_wall_dist.argtypes = [_V, _D]
     L.orc_init_field.argtypes = [_V, ctypes.c_int, ctypes.c_double, _D]
     L.orc_vr_iter.argtypes = [_V, _D, _D, _D, ctypes.c_int, ctypes.c_int]
     L.orc_eval_dt.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D]
@@ -187,6 +188,12 @@ class Oracle:
         self._bc = (t, v)
         lib().orc_set_bc(self.h, len(t), t.ctypes.data_as(_I), _p(v), self.nv)
 
+    def set_wall_distance(self, d):
+        """Wall distance at every cell Gauss point, [nCell][nGc] (the SA model's dWall)."""
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        self._dwall = d
+        lib().orc_set_wall_dist(self.h, _p(d))
+
     def init_field(self, kind, chi=5.0):
         u = np.zeros((self.mesh.n_cell, self.nv))
         lib().orc_init_field(self.h, kind, chi, _p(u))
@@ -218,9 +225,9 @@ class Oracle:
 
     def lusgs_init(self, dTau, dt, alphaDiag):
         dTau = _f64(dTau)
-        jd = np.zeros(self.mesh.n_cell)
+        jd = np.zeros(self.mesh.n_cell * (self.nv if self.nv >= 6 else 1))
         lib().orc_lusgs_init(self.h, _p(dTau), dt, alphaDiag, _p(jd))
-        return jd
+        return jd if self.nv < 6 else jd.reshape(self.mesh.n_cell, self.nv)
 
     def update_sgs(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False):
         rhs, u, uInc, jdiag = _f64(rhs), _f64(u), _f64(uInc), _f64(jdiag)

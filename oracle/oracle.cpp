@@ -866,6 +866,9 @@ struct Oracle
     std::vector<real> AAInvB, AInvb, matA;
     // evaluator state (EulerEvaluator.hpp lambdaFace*, deltaLambda*)
     std::vector<real> lambdaFace, lambdaFaceC, lambdaFaceVis, lambdaFace0, deltaLambdaFace, deltaLambdaCell;
+    // SA model (nVars = 6): wall distance per cell Gauss point, major length scale per cell,
+    // and the source-term Jacobian diagonal of the last RHS
+    std::vector<real> dWall, cellHMax, jSource;
     // boundary table indexed by face zone (EulerBC.hpp:35-48 types; value = far / inflow state or wall temperature)
     std::vector<int> bcType;
     std::vector<real> bcVal; // [zone][8]
@@ -905,9 +908,81 @@ struct Oracle
     }
 
     // FiniteVolume.cpp:22-330 + VariationalReconstruction.cpp:10-43
+    // FiniteVolume.cpp:288-335 cellMajorHBox and FiniteVolume.hpp:387-393 GetCellMaxLenScale: the
+    // largest half extent of the cell's vertices along the principal axes of its inertia tensor
+    // (integrated at INT_ORDER_MAX), times 2.  Principal axes by cyclic Jacobi rotations.
+    real majorLength(long c, const real *cc) const
+    {
+        real I[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int g = 0; g < quadNPoints(cellType, INT_ORDER_MAX); g++)
+        {
+            real p[3], w;
+            quadPoint(cellType, INT_ORDER_MAX, g, p, w);
+            PointGeo pg = pointGeo(cellType, cc, p);
+            real J = cellJacDet(dim, pg);
+            real x[3] = {pg.x[0] - cellBary[c * 3], pg.x[1] - cellBary[c * 3 + 1], pg.x[2] - cellBary[c * 3 + 2]};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    I[a][b] += x[a] * x[b] * J * w;
+        }
+        int n = dim;
+        real nrm = 0;
+        for (int a = 0; a < n; a++)
+            for (int b = 0; b < n; b++)
+                I[a][b] /= vol[c], nrm += I[a][b] * I[a][b];
+        nrm = std::sqrt(nrm);
+        real V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        real A[3][3];
+        std::memcpy(A, I, sizeof(A));
+        for (int sweep = 0; sweep < 50; sweep++)
+        {
+            real off = 0;
+            for (int a = 0; a < n; a++)
+                for (int b = a + 1; b < n; b++)
+                    off += A[a][b] * A[a][b];
+            if (off <= 1e-34 * nrm * nrm)
+                break;
+            for (int a = 0; a < n; a++)
+                for (int b = a + 1; b < n; b++)
+                {
+                    if (A[a][b] == 0)
+                        continue;
+                    real th = (A[b][b] - A[a][a]) / (2 * A[a][b]);
+                    real t = (th >= 0 ? 1.0 : -1.0) / (std::abs(th) + std::sqrt(th * th + 1));
+                    real cs = 1 / std::sqrt(t * t + 1), sn = t * cs;
+                    for (int k = 0; k < n; k++)
+                    {
+                        real x = A[k][a], y = A[k][b];
+                        A[k][a] = cs * x - sn * y, A[k][b] = sn * x + cs * y;
+                    }
+                    for (int k = 0; k < n; k++)
+                    {
+                        real x = A[a][k], y = A[b][k];
+                        A[a][k] = cs * x - sn * y, A[b][k] = sn * x + cs * y;
+                    }
+                    for (int k = 0; k < n; k++)
+                    {
+                        real x = V[k][a], y = V[k][b];
+                        V[k][a] = cs * x - sn * y, V[k][b] = sn * x + cs * y;
+                    }
+                }
+        }
+        // degenerate inertia (eigenvalue ratio below 1 + smallReal): the reference perturbs the
+        // diagonal and keeps the coordinate axes, which is what the identity start gives here
+        real h = 0;
+        for (int k = 0; k < nvert; k++)
+        {
+            real x[3] = {cc[k * 3] - cellBary[c * 3], cc[k * 3 + 1] - cellBary[c * 3 + 1], cc[k * 3 + 2] - cellBary[c * 3 + 2]};
+            for (int a = 0; a < n; a++)
+                h = std::max(h, std::abs(V[0][a] * x[0] + V[1][a] * x[1] + V[2][a] * x[2]));
+        }
+        return h * 2;
+    }
+
     void constructMetrics()
     {
         vol.assign(nCell, 0);
+        cellHMax.assign(nCell, 0);
         cellBary.assign(nCell * 3, 0);
         cellCent.assign(nCell * 3, 0);
         cellHBox.assign(nCell * 3, 0);
@@ -960,6 +1035,7 @@ struct Oracle
             }
             if (dim == 2)
                 cellHBox[c * 3 + 2] = 1;
+            cellHMax[c] = majorLength(c, cc);
         }
         nGf = quadNPoints(faceType, vs.intOrder);
         faceArea.assign(nFace, 0);
@@ -1343,6 +1419,24 @@ struct Oracle
     // 4 BCWallIsothermal, 5 BCOut, 6 BCOutP, 7 BCIn, 9 BCSym.  Returns false for an unsupported type.
     bool bcValue(int type, int zone, const real *UL, const real *n, real *UR) const
     {
+        real ULc[8];
+        std::copy(UL, UL + es.nVars, ULc);
+        return bcValueFix(type, zone, ULc, n, UR, false);
+    }
+
+    // fixUL (USE_FIX_ZERO_SA_NUT_AT_WALL, EvaluateDt.hxx:2291-2296): on wall types the SA variable of
+    // both the inner state UL (modified) and the ghost is set to zero
+    bool bcValueFix(int type, int zone, real *UL, const real *n, real *UR, bool fixUL) const
+    {
+        bool ok = bcValueRaw(type, zone, UL, n, UR);
+        if (ok && fixUL && (type == 2 || type == 4))
+            for (int j = 5; j < es.nVars; j++)
+                UL[j] = UR[j] = 0;
+        return ok;
+    }
+
+    bool bcValueRaw(int type, int zone, const real *UL, const real *n, real *UR) const
+    {
         int nv = es.nVars;
         real g = es.gamma;
         const real *far = &bcVal[zone * 8];
@@ -1453,7 +1547,7 @@ struct Oracle
                 UL[v] = u[c * nv + v] + a;
             }
             compressRec(u + c * nv, UL, ULf);
-            if (!bcValue(type, faceZone[f], ULf, n, UB))
+            if (!bcValueFix(type, faceZone[f], ULf, n, UB, true))
                 std::copy(ULf, ULf + nv, UB);
             real JW = faceJDet[f * nGf + g] * w * w0 * w0;
             for (int i = 0; i < R; i++)
@@ -1579,6 +1673,7 @@ struct Oracle
             real lambdaConvection = std::max(aL + std::abs(veloNL - vgN), aR + std::abs(veloNR - vgN));
             real T = pMean / ((gamma - 1) / gamma * cp() * uMean[0]);
             real muf = muEff(uMean.data(), T);
+            muf += muTurSA(uMean.data(), muf);
             real lamVis = muf / uMean[0] * std::max(4. / 3., gamma / es.prGas);
             real area = faceArea[f];
             real volR = c1 >= 0 ? vol[c1] : vol[c0];
@@ -1609,6 +1704,200 @@ struct Oracle
         if (!useLocalDt)
             for (long c = 0; c < nCell; c++)
                 dt[c] = mn;
+    }
+
+    // EulerEvaluator.hpp:791-833 getMuTur (SA, negative-model smoothing of chi)
+    real muTurSA(const real *U, real muf) const
+    {
+        if (es.nVars < 6)
+            return 0;
+        const real cnu1 = 7.1;
+        real Chi = U[5] * es.muGas / muf;
+        if (Chi < 10)
+            Chi = 0.05 * std::log(1 + std::exp(20 * Chi));
+        real Chi3 = Chi * Chi * Chi;
+        real fnu1 = Chi3 / (Chi3 + cnu1 * cnu1 * cnu1);
+        return muf * std::max(Chi * fnu1, 0.0);
+    }
+
+    // fluxFace viscous part at one point (EvaluateDt.hxx:1167-1209) with the SA terms of
+    // visFluxTurVariable (EulerEvaluator.hpp:835-877): mu + mu_t, heat conduction with Pr_t = 0.9,
+    // and the nuTilde diffusion flux
+    void pointViscousFlux(const real *UM, const real *GMP, const real *n, bool adiabatic, real *vis) const
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        real velo2 = (sqr(UM[1]) + sqr(UM[2]) + sqr(UM[3])) / sqr(UM[0]);
+        real pM, aM, HM;
+        idealGasThermal(UM[4], UM[0], velo2, gamma, pM, aM, HM);
+        real Tm = pM / ((gamma - 1) / gamma * cp() * UM[0]);
+        real mufPhy = muEff(UM, Tm);
+        real muTur = muTurSA(UM, mufPhy);
+        real muf = mufPhy + muTur;
+        real k = cp() * muTur / 0.9 + cp() * mufPhy / es.prGas;
+        viscousFlux(nv, UM, GMP, n, adiabatic, gamma, muf, k, cp(), vis);
+        if (nv >= 6)
+        {
+            const real sigma = 2.0 / 3.0, cn1 = 16.0;
+            real fn = 1;
+            if (UM[5] < 0)
+            {
+                real Chi = UM[5] * es.muGas / mufPhy;
+                fn = (cn1 + Chi * Chi * Chi) / (cn1 - Chi * Chi * Chi);
+            }
+            vis[5] = (GMP[0 * nv + 5] * n[0] + GMP[1 * nv + 5] * n[1] + GMP[2 * nv + 5] * n[2]) * (mufPhy + UM[5] * es.muGas * fn) / sigma;
+        }
+    }
+
+    // passive-scalar upwind flux of the SA variable (EvaluateDt.hxx:1413-1425), with the
+    // Riemann solver's lam123 as the dissipation speed (ransEigScheme 0)
+    void scalarConvectiveFlux(const real *UL, const real *UR, const real *n, real lam123, real *F) const
+    {
+        for (int j = 5; j < es.nVars; j++)
+        {
+            real vnL = (UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2]) / UL[0];
+            real vnR = (UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2]) / UR[0];
+            F[j] = ((vnL * UL[j] + vnR * UR[j]) - (UR[j] - UL[j]) * lam123) * 0.5;
+        }
+    }
+
+    // RANS_ke.hpp:985-1195 GetSource_SA with the settings defaults (SADESMode 1, rotation
+    // correction on, SAVersion 0) and the compiled options USE_NS_SA_NEGATIVE_MODEL and
+    // SA_USE_FT2_TERM; mode 0 source, mode 1 diagonal Jacobian.  G is the conservative gradient [3][nv].
+    real saSource(const real *U, const real *G, real mufPhy, real d, real lLES, real hMax, int mode) const
+    {
+        const int nv = es.nVars;
+        const real muRef = es.muGas;
+        const real cb1 = 0.1355, cb2 = 0.622, sigma = 2.0 / 3.0, cnu1 = 7.1, cnu2 = 0.7, cnu3 = 0.9, cw2 = 0.3, cw3 = 2,
+                   kappa = 0.41, rlim = 10, cn1 = 16.0;
+        const real cw1 = cb1 / sqr(kappa) + (1 + cb2) / sigma;
+        const real ct3 = 1.2, ct4 = 0.5;
+        real nuh = U[5] * muRef / U[0];
+        real Chi = U[5] * muRef / mufPhy;
+        real Chi3 = Chi * Chi * Chi;
+        real fnu1 = Chi3 / (Chi3 + cnu1 * cnu1 * cnu1);
+        real fnu2 = 1 - Chi / (1 + Chi * fnu1);
+        real velo[3] = {U[1] / U[0], U[2] / U[0], U[3] / U[0]};
+        real diffRho[3], diffNu[3], diffU[3][3];
+        for (int i = 0; i < 3; i++)
+        {
+            diffRho[i] = G[i * nv + 0];
+            diffNu[i] = (G[i * nv + 5] * muRef - nuh * diffRho[i]) / U[0];
+            for (int j = 0; j < 3; j++)
+                diffU[i][j] = (G[i * nv + 1 + j] - diffRho[i] * velo[j]) / U[0];
+        }
+        real om2 = 0, ss2 = 0, du2 = 0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+            {
+                real o = 0.5 * (diffU[j][i] - diffU[i][j]);
+                real sij = diffU[i][j] + diffU[j][i];
+                om2 += o * o, ss2 += sij * sij, du2 += diffU[i][j] * diffU[i][j];
+            }
+        real S = std::sqrt(om2) * std::sqrt(2.0);
+        real SS = std::sqrt(ss2) * (1. / std::sqrt(2.0));
+        real SRotCor = 2.0 * std::min(0.0, S - SS);
+        real diffUNorm = std::sqrt(du2);
+        real ft2 = ct3 * std::exp(-ct4 * sqr(Chi));
+        real lDES = d;
+        {
+            real lRANS = d, fwStar = .424;
+            real nuTur = mufPhy / U[0] * std::max(Chi * fnu1, 0.0);
+            real nufPhy = mufPhy / U[0];
+            real den = sqr(kappa) * sqr(d) * std::max(smallReal, diffUNorm);
+            real rd = (nuTur + nufPhy) / den;
+            real fd = 1. - std::tanh(std::pow(8 * rd, 3));
+            real psiSqr = Chi <= 0 ? 100.0
+                                   : std::min(100.0, (1 - cb1 / (cw1 * sqr(kappa) * fwStar) * (ft2 + (1 - ft2) * fnu2)) /
+                                                         (fnu1 * std::max(smallReal, 1 - ft2)));
+            real psi = std::sqrt(std::max(psiSqr, 1.0));
+            lDES = lRANS - fd * std::max(0., lRANS - lLES * psi);
+            // IDDES (SADESMode 1)
+            real alphaIDDES = 0.25 - d / hMax;
+            real fB = std::min(2 * std::exp(-9. * sqr(alphaIDDES)), 1.0);
+            const real cl = 3.55, ct = 1.63;
+            real rdt = nuTur / den, rdl = nufPhy / den;
+            real ftt = std::tanh(std::pow(sqr(ct) * rdt, 3));
+            real flt = sqr(sqr(cl) * rdl);
+            real fl = std::tanh(sqr(sqr(flt)) * flt);
+            real fe1 = 2. * std::exp(-(alphaIDDES >= 0 ? 11.09 : 9.0) * sqr(alphaIDDES));
+            real fe2 = 1. - std::max(ftt, fl);
+            real fe = std::max(fe1 - 1., 0.) * psi * fe2;
+            real fdTilde = std::max(fB, std::tanh(std::pow(8 * rdt, 3)));
+            real lIDDES = fdTilde * (1 + fe) * lRANS + (1 - fdTilde) * lLES * psi;
+            lDES = std::max(lLES * smallReal, lIDDES);
+        }
+        d = lDES;
+        real Sbar = nuh / (sqr(kappa) * sqr(d)) * fnu2;
+        real Sh = Sbar < -cnu2 * S ? S + S * (sqr(cnu2) * S + cnu3 * Sbar) / ((cnu3 - 2 * cnu2) * S - Sbar) : S + Sbar;
+        real r = std::min(nuh / (Sh * sqr(kappa * d) + verySmallReal), rlim);
+        real g = r + cw2 * (std::pow(r, 6) - r);
+        real fw = g * std::pow((1 + std::pow(cw3, 6)) / (std::pow(g, 6) + std::pow(cw3, 6)), 1. / 6.);
+        real D = (cw1 * fw - cb1 / sqr(kappa) * ft2) * sqr(nuh / lDES);
+        real P = cb1 * (1 - ft2) * (Sh + SRotCor) * nuh;
+        real fn = 1;
+        if (U[5] < 0)
+        {
+            real Chi_ = U[5] * muRef / mufPhy;
+            fn = (cn1 + std::pow(Chi_, 3)) / (cn1 - std::pow(Chi_, 3));
+            D = -cw1 * sqr(nuh / lDES);
+            P = cb1 * (1 - ct3) * std::abs(S + SRotCor) * nuh;
+        }
+        real dd = diffRho[0] * diffNu[0] + diffRho[1] * diffNu[1] + diffRho[2] * diffNu[2];
+        real nn = diffNu[0] * diffNu[0] + diffNu[1] * diffNu[1] + diffNu[2] * diffNu[2];
+        if (mode == 0)
+            return U[0] * (P - D + nn * cb2 / sigma) / muRef - (U[5] * fn * muRef + mufPhy) / (U[0] * sigma) * dd / muRef;
+        return -std::min(U[0] * (std::min(P, 0.0) * 1 - D * 2) / muRef / (std::abs(U[5]) + verySmallReal), -verySmallReal);
+    }
+
+    // EvaluateRHS.hxx:665-801 source integration (SA only; the NS source is zero) and the
+    // source-term Jacobian diagonal JSource, both cell means
+    void addSource(const real *u, const real *uRec, real *rhs)
+    {
+        int nv = es.nVars;
+        jSource.assign(nCell * nv, 0.0);
+        if (nv < 6)
+            return;
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            std::vector<real> T((dim + 1) * NDOF);
+            real S = 0, J = 0;
+            for (int g = 0; g < nGc; g++)
+            {
+                real pq[3], w;
+                quadPoint(cellType, vs.intOrder, g, pq, w);
+                diffBase(c, &cellPP[(c * nGc + g) * 3], T.data(), dim + 1, true);
+                real U[8], G[3 * 8] = {0};
+                for (int v = 0; v < nv; v++)
+                {
+                    real a = u[c * nv + v];
+                    for (int j = 0; j < R; j++)
+                        a += T[1 + j] * uRec[(c * R + j) * nv + v];
+                    U[v] = a;
+                    for (int d = 0; d < dim; d++)
+                    {
+                        real ga = 0;
+                        for (int j = 0; j < R; j++)
+                            ga += T[(1 + d) * NDOF + 1 + j] * uRec[(c * R + j) * nv + v];
+                        G[d * nv + v] = ga;
+                    }
+                }
+                real velo2 = (sqr(U[1]) + sqr(U[2]) + sqr(U[3])) / sqr(U[0]);
+                real pM, aM, HM;
+                idealGasThermal(U[4], U[0], velo2, es.gamma, pM, aM, HM);
+                real Tm = pM / ((es.gamma - 1) / es.gamma * cp() * U[0]);
+                real muf = muEff(U, Tm);
+                real d = std::min(dWall.empty() ? veryLargeReal : dWall[c * nGc + g], std::pow(veryLargeReal, 1. / 6.));
+                real hMax = cellHMax[c];
+                real lLES = std::min(hMax * veryLargeReal, std::max(d * 1.0, hMax * 1.0));
+                real JW = cellJDet[c * nGc + g] * w;
+                S += saSource(U, G, muf, d, lLES, hMax, 0) * JW;
+                J += saSource(U, G, muf, d, lLES, hMax, 1) * JW;
+            }
+            rhs[c * nv + 5] += S / vol[c];
+            jSource[c * nv + 5] = J / vol[c];
+        }
     }
 
     // EulerEvaluator_EvaluateRHS.hxx:171-562 for a boundary face (f2c[1] == UnInitIndex): ghost
@@ -1655,7 +1944,7 @@ struct Oracle
                     GL[d * nv + v] = ga;
                 }
             }
-            if (!bcValue(type, zone, UL, n, UR))
+            if (!bcValueFix(type, zone, UL, n, UR, true))
                 std::copy(UL, UL + nv, UR);
             real dc[3] = {faceCent[f * 3 + 0] - cellBary[c0 * 3 + 0], faceCent[f * 3 + 1] - cellBary[c0 * 3 + 1],
                           faceCent[f * 3 + 2] - cellBary[c0 * 3 + 2]};
@@ -1676,16 +1965,10 @@ struct Oracle
             gradCons2Prim(nv, UM, GM, GMP, gamma);
             real vis[8] = {0};
             if (!es.ignoreVis && !noVis)
-            {
-                real velo2 = (sqr(UM[1]) + sqr(UM[2]) + sqr(UM[3])) / sqr(UM[0]);
-                real pM, aM, HM;
-                idealGasThermal(UM[4], UM[0], velo2, gamma, pM, aM, HM);
-                real Tm = pM / ((gamma - 1) / gamma * cp() * UM[0]);
-                real muf = muEff(UM, Tm);
-                viscousFlux(nv, UM, GMP, n, type == 2, gamma, muf, cp() * muf / es.prGas, cp(), vis);
-            }
+                pointViscousFlux(UM, GMP, n, type == 2, vis);
             real F[8] = {0}, l0, l1, l4, vg[3] = {0, 0, 0};
             riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4);
+            scalarConvectiveFlux(UL, UR, n, l1, F);
             real JD = faceJDet[f * nGf + g];
             for (int v = 0; v < nv; v++)
                 fluxEs[v] += -(F[v] - vis[v]) * JD * w;
@@ -1767,18 +2050,11 @@ struct Oracle
                 gradCons2Prim(nv, UM, GM, GMP, gamma);
                 // fluxFace (EulerEvaluator_EvaluateDt.hxx:1084-1511)
                 real vis[8] = {0};
-                {
-                    real velo2 = (sqr(UM[1]) + sqr(UM[2]) + sqr(UM[3])) / sqr(UM[0]);
-                    real pM, aM, HM;
-                    idealGasThermal(UM[4], UM[0], velo2, gamma, pM, aM, HM);
-                    real Tm = pM / ((gamma - 1) / gamma * cp() * UM[0]);
-                    real muf = muEff(UM, Tm);
-                    real k = cp() * muf / es.prGas;
-                    if (!es.ignoreVis)
-                        viscousFlux(nv, UM, GMP, n, false, gamma, muf, k, cp(), vis);
-                }
+                if (!es.ignoreVis)
+                    pointViscousFlux(UM, GMP, n, false, vis);
                 real F[8] = {0}, l0, l1, l4, vg[3] = {0, 0, 0};
                 riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4);
+                scalarConvectiveFlux(UL, UR, n, l1, F);
                 real JD = faceJDet[f * nGf + g];
                 for (int v = 0; v < nv; v++)
                     fluxEs[v] += -(F[v] - vis[v]) * JD * w;
@@ -1800,6 +2076,7 @@ struct Oracle
                     rhs[c * nv + v] += sgn * faceFlux[f * nv + v] / vol[c];
             }
         }
+        addSource(u, uRec, rhs);
         if (faceFluxOut)
             std::copy(faceFlux.begin(), faceFlux.end(), faceFluxOut);
     }
@@ -1807,6 +2084,8 @@ struct Oracle
     // EulerEvaluator.hxx:37-159 LUSGSMatrixInit, scalar Jacobian, source ignored
     void lusgsInit(const real *dTau, real dt, real alphaDiag, real *jdiag) const
     {
+        // the SA model keeps one diagonal per variable (JDiag.getDiag plus alphaDiag JSource, :139-153)
+        int nv = es.nVars, nd = nv >= 6 ? nv : 1;
         for (long c = 0; c < nCell; c++)
         {
             real fp = 1.0 / dTau[c] + 1.0 / dt;
@@ -1815,7 +2094,8 @@ struct Oracle
                 long f = cell2face[c * nf + k];
                 fp += (0.5 * alphaDiag) * faceArea[f] * lambdaFace[f] / vol[c];
             }
-            jdiag[c] = fp;
+            for (int v = 0; v < nd; v++)
+                jdiag[c * nd + v] = fp + (nd > 1 && !jSource.empty() ? alphaDiag * jSource[c * nv + v] : 0.0);
         }
     }
 
@@ -1879,7 +2159,7 @@ struct Oracle
             for (int v = 0; v < nv; v++)
             {
                 real old = uIncNew[c * nv + v];
-                uIncNew[c * nv + v] = buf[v] / jdiag[c];
+                uIncNew[c * nv + v] = buf[v] / jdiag[nv >= 6 ? c * nv + v : c];
                 sumInc[v] += std::abs(uIncNew[c * nv + v] - old);
             }
         }
@@ -1909,7 +2189,7 @@ struct Oracle
                     buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
             }
             for (int v = 0; v < nv; v++)
-                AuInc[c * nv + v] = jdiag[c] * uInc[c * nv + v] - buf[v];
+                AuInc[c * nv + v] = jdiag[nv >= 6 ? c * nv + v : c] * uInc[c * nv + v] - buf[v];
         }
     }
 
@@ -1989,6 +2269,13 @@ extern "C"
     }
     void orc_destroy(void *h) { delete (Oracle *)h; }
 
+    // wall distance at the cell Gauss points [nCell][nGc] (the SA model's dWall)
+    void orc_set_wall_dist(void *h, const double *d)
+    {
+        Oracle *o = (Oracle *)h;
+        o->dWall.assign(d, d + o->nCell * o->nGc);
+    }
+
     // boundary table per face zone (zone 0 = interior): EulerBC.hpp:35-48 type codes, values [nZone][nVars]
     void orc_set_bc(void *h, int nZone, const int *type, const double *value, int nv)
     {
@@ -2028,6 +2315,8 @@ extern "C"
         else if (n == "smoothRatio") v = &o->smoothRatio;
         else if (n == "faceArea") v = &o->faceArea;
         else if (n == "cellPP") v = &o->cellPP;
+        else if (n == "cellHMax") v = &o->cellHMax;
+        else if (n == "jSource") v = &o->jSource;
         else if (n == "faceCent") v = &o->faceCent;
         else if (n == "faceJDet") v = &o->faceJDet;
         else if (n == "facePP") v = &o->facePP;

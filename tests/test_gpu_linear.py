@@ -49,7 +49,7 @@ def _init(o, kind):
 
 
 def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, jacobi, sgsIter, k, nIter, meanScale=None):
-    jd = torch.zeros(u.shape[0], dtype=torch.float64)
+    jd = torch.zeros((u.shape[0], 6) if u.shape[1] == 6 else (u.shape[0],), dtype=torch.float64)
     oe.LUSGSMatrixInit(jd, dTau, dt, alpha)
     tmp = torch.zeros_like(rhs)
 
@@ -64,7 +64,7 @@ def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, jacobi, sgsIter, k, nIte
         for _ in range(1 + sgsIter):
             pair(rhs, x)
     if code:
-        s2 = torch.ones(5, dtype=torch.float64) if meanScale is None else torch.tensor([1 / (m + 1e-200) ** 2 for m in meanScale])
+        s2 = torch.ones(u.shape[1], dtype=torch.float64) if meanScale is None else torch.tensor([1 / (m + 1e-200) ** 2 for m in meanScale])
         g = I.GMRES(k, x)
 
         def FML(v, Mv):
