@@ -372,6 +372,10 @@ int dispatch_ng(int nG, const MeshD &m, const GeomD &g, const VRD &vr, const Eva
             return launch_rhs_fast<DIM, P, 5, 4>(m, g, vr, ev, u, uRec, ff, st);
         if (nG == 7)
             return launch_rhs_fast<DIM, P, 5, 7>(m, g, vr, ev, u, uRec, ff, st);
+        if (nG == 3)
+            return launch_rhs_fast<DIM, P, 5, 3>(m, g, vr, ev, u, uRec, ff, st);
+        if (nG == 6)
+            return launch_rhs_fast<DIM, P, 5, 6>(m, g, vr, ev, u, uRec, ff, st);
     }
     else
     {

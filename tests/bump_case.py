@@ -23,12 +23,12 @@ def bump_bc(far, outflow_type=1):
     return types, vals, w
 
 
-def bump_oracle(m, p, rs="Roe", mu=0.0, ignoreVis=1, mach=0.8, outflow_type=1):
+def bump_oracle(m, p, rs="Roe", mu=0.0, ignoreVis=1, mach=0.8, outflow_type=1, intOrder=5):
     far = M.freestream(mach)
     types, vals, w = bump_bc(far, outflow_type)
     es = dict(nVars=5, rsType=oracle.RS[rs], rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=mu, prGas=0.72, TRef=273.15,
               CSutherland=110.4, muModel=0, ignoreVis=ignoreVis)
-    o = oracle.Oracle(m, dict(VR_HQM, maxOrder=p), es)
+    o = oracle.Oracle(m, dict(VR_HQM, maxOrder=p, intOrder=intOrder), es)
     assert o.construct(w) == 0
     o.set_bc(types, vals)
     return o, far, types, vals, w

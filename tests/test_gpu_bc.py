@@ -13,23 +13,24 @@ from tests.util import VR_HQM_PY, relerr
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
-CASES = [("p1-Roe-euler", 1, "Roe", 0.0, 1, 1), ("p2-Roe-euler", 2, "Roe", 0.0, 1, 1), ("p2-HLLEP-ns-bcout", 2, "HLLEP", 1e-3, 0, 5),
-         ("p3-RoeM1-euler", 3, "Roe_M1", 0.0, 1, 1)]
+CASES = [("p1-Roe-euler", 1, "Roe", 0.0, 1, 1, 5), ("p2-Roe-euler", 2, "Roe", 0.0, 1, 1, 5),
+         ("p2-HLLEP-ns-bcout", 2, "HLLEP", 1e-3, 0, 5, 5), ("p3-RoeM1-euler", 3, "Roe_M1", 0.0, 1, 1, 5),
+         ("p1-Roe-euler-int2", 1, "Roe", 0.0, 1, 1, 2)]
 
 
-def _setup(p, rs, mu, ignoreVis, outflow):
+def _setup(p, rs, mu, ignoreVis, outflow, intOrder=5):
     from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
     m = M.renumber_by_color(M.bump_channel_tet(6, 4, 2))
-    o, far, types, vals, w = bump_oracle(m, p, rs, mu, ignoreVis, outflow_type=outflow)
-    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p)).construct(w)
+    o, far, types, vals, w = bump_oracle(m, p, rs, mu, ignoreVis, outflow_type=outflow, intOrder=intOrder)
+    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p, intOrder=intOrder)).construct(w)
     ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType=rs, muGas=mu, muModel=0, ignoreVis=bool(ignoreVis)))
     ev.SetBC(types, vals)
     return m, o, vr, ev, far
 
 
-@pytest.mark.parametrize("name,p,rs,mu,iv,outflow", CASES, ids=[c[0] for c in CASES])
-def test_boundary_operators(name, p, rs, mu, iv, outflow):
-    m, o, vr, ev, far = _setup(p, rs, mu, iv, outflow)
+@pytest.mark.parametrize("name,p,rs,mu,iv,outflow,intOrder", CASES, ids=[c[0] for c in CASES])
+def test_boundary_operators(name, p, rs, mu, iv, outflow, intOrder):
+    m, o, vr, ev, far = _setup(p, rs, mu, iv, outflow, intOrder)
     for nm in ["faceWeight", "matrixA", "matrixAAInvB", "vectorAInvB"]:
         assert relerr(vr.get(nm), o.get(nm)) < TOL, nm
     u0, uRec0 = perturbed_state(m, far, R=o.R)
