@@ -201,6 +201,56 @@ def run_steady(args):
                     "transonic case; both precisions follow the same residual history"}
 
 
+def run_adjoint_cost(args):
+    """Cost of the residual VJP against one primal RHS (inviscid bump, the derivative configuration):
+    CUDA-event times of EvaluateRHS, EvaluateRHSVJP, one VR sweep and its VJP."""
+    import torch
+    from dndsr_b200 import mesh as M
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction, euler_bc_dir_weights
+    nx, ny, nz = args.adjoint_mesh
+    mesh = M.bump_channel_tet(nx, ny, nz, periodic_z=True)
+    far = M.freestream(0.8)
+    types = np.zeros(7, np.int32)
+    vals = np.zeros((7, 5))
+    for z in (1, 2, 3, 4):
+        types[z], vals[z] = M.BUMP_BC_TYPES[z], far
+    out = {}
+    for p in (1, 2):
+        vr = VariationalReconstruction(mesh, dict(maxOrder=p, intOrder=4, dirWeightScheme="HQM_OPT", geomWeightScheme="HQM_SD",
+                                                  geomWeightBias=1.0)).construct(euler_bc_dir_weights(types))
+        ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType="Roe", muGas=0.0, ignoreVis=True))
+        ev.SetBC(types, vals)
+        u = vr.BuildUDof(5)
+        u[:] = torch.tensor(far, device="cuda")
+        uRec, uNew = vr.BuildURec(5), vr.BuildURec(5)
+        dt = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            vr.DoReconstructionIter(uRec, uNew, u, putIntoNew=False)
+        ev.EvaluateDt(dt, u, 1.0)
+        rhs = torch.zeros_like(u)
+        w = torch.randn(u.shape, dtype=torch.float64, device="cuda")
+        cot = torch.randn(uRec.shape, dtype=torch.float64, device="cuda")
+
+        def timed(fn, n=10):
+            fn()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(n):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / n
+
+        t_rhs = timed(lambda: ev.EvaluateRHS(rhs, u, uRec))
+        t_vjp = timed(lambda: ev.EvaluateRHSVJP(w, u, uRec))
+        t_vr = timed(lambda: vr.DoReconstructionIter(uRec, uNew, u, putIntoNew=True))
+        t_vrvjp = timed(lambda: vr.DoReconstructionIterVJP(cot, uRec, u))
+        out[f"p{p}"] = {"ms_rhs": t_rhs, "ms_rhs_vjp": t_vjp, "vjp_over_rhs": t_vjp / t_rhs, "ms_vr_sweep": t_vr, "ms_vr_sweep_vjp": t_vrvjp,
+                        "residual_vjp_over_primal": (t_vjp + t_vrvjp) / (t_rhs + t_vr)}
+    return {"workload": f"inviscid bump, {mesh.n_cell} tets, Roe, intOrder 4; VJP with respect to u and uRec (state)", **out}
+
+
 def n_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -341,6 +391,7 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clk.summary()}
     if world == 1 and not args.no_steady:
         line["steady"] = run_steady(args)
+        line["adjoint_cost"] = run_adjoint_cost(args)
     if world == 1 and not args.no_cpu_baseline:
         v, steps, el, cells = cpu_baseline_oracle(args.sample_n, p, args.sample_seconds, n_cores())
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": n_cores(), "kind": "port",
@@ -363,6 +414,7 @@ def main():
     ap.add_argument("--no-steady", action="store_true")
     ap.add_argument("--steady-mesh", type=int, nargs=3, default=(160, 80, 26))
     ap.add_argument("--steady-iters", type=int, default=100)
+    ap.add_argument("--adjoint-mesh", type=int, nargs=3, default=(80, 40, 13))
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

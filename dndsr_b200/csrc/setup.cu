@@ -515,6 +515,24 @@ DNDSB_GLOBAL void k_vr_coeff(MeshD m, GeomD g, VRD vr, int *err)
     }
 }
 
+// [cell][face k][row i][R+1]: row i of A^-1 B_k followed by (A^-1 b_k)_i
+DNDSB_GLOBAL void k_pack_sweep(int64_t nCell, int nf, int R, const real *__restrict__ AAInvB, const real *__restrict__ AInvb, real *out,
+                               float *out32)
+{
+    const int64_t per = (int64_t)nf * R * (R + 1);
+    DNDSB_KERNEL_LOOP(e, nCell * per)
+    {
+        int64_t c = e / per;
+        int r = (int)(e - c * per);
+        int k = r / (R * (R + 1));
+        int rem = r - k * R * (R + 1);
+        int i = rem / (R + 1), j = rem - i * (R + 1);
+        real v = j < R ? AAInvB[((c * (nf + 1) + 1 + k) * R + i) * R + j] : AInvb[(c * nf + k) * R + i];
+        out[e] = v;
+        out32[e] = (float)v;
+    }
+}
+
 DNDSB_GLOBAL void k_to_f32(int64_t n, const real *a, float *b)
 {
     DNDSB_KERNEL_LOOP(i, n)
@@ -647,6 +665,17 @@ int vr_construct_rec_coeff(const MeshD &m, const GeomD &g, VRD &vr, int *errWord
 #undef DNDSB_RC
     DNDSB_LAUNCH(k_to_f32, nA, 256, st, nA, vr.AAInvB, vr.AAInvB32);
     DNDSB_LAUNCH(k_to_f32, nb, 256, st, nb, vr.AInvb, vr.AInvb32);
+    {
+        int64_t nS = m.nCell * m.nf * R * (R + 1);
+        dev_free(vr.sweepCoef), dev_free(vr.sweepCoef32);
+        vr.sweepCoef = nullptr, vr.sweepCoef32 = nullptr;
+        if (alloc_real(&vr.sweepCoef, nS) || dev_alloc((void **)&vr.sweepCoef32, sizeof(float) * nS) != cudaSuccess)
+            return ST_CUDA;
+        DNDSB_LAUNCH(k_pack_sweep, nS, 256, st, m.nCell, m.nf, R, vr.AAInvB, vr.AInvb, vr.sweepCoef, vr.sweepCoef32);
+        if (!vr.sweepErr && dev_alloc((void **)&vr.sweepErr, sizeof(int)) != cudaSuccess)
+            return ST_CUDA;
+        dev_zero(vr.sweepErr, sizeof(int), st);
+    }
     int e = 0;
     d2h(&e, errWord, sizeof(int), st);
     if (dev_sync(st) != cudaSuccess || last_error() != cudaSuccess)

@@ -116,7 +116,12 @@ struct VRD
     real *baseMoment = nullptr, *faceWeight = nullptr, *faceL = nullptr;
     real *AAInvB = nullptr, *AInvb = nullptr, *matA = nullptr;
     float *AAInvB32 = nullptr, *AInvb32 = nullptr;
-    BoundaryD bnd; // boundary values for the BC faces of the sweep
+    // the sweep's coefficients packed per cell as [nf][R][R+1] (row i of A^-1 B_k, then (A^-1 b_k)_i):
+    // one contiguous, 16-byte aligned range per cell, staged into shared memory by bulk async copies
+    real *sweepCoef = nullptr;
+    float *sweepCoef32 = nullptr;
+    int *sweepErr = nullptr; // device word: a bulk copy that did not complete in time
+    BoundaryD bnd;           // boundary values for the BC faces of the sweep
 };
 
 struct EulerSettingsD
