@@ -304,7 +304,7 @@ extern "C"
                         (void *)g.smoothRatio, (void *)g.faceArea, (void *)g.faceCent, (void *)g.faceJDet, (void *)g.facePP, (void *)g.faceNorm,
                         (void *)g.faceMeanNorm, (void *)g.cellQw, (void *)g.faceQw, (void *)g.hMax, (void *)v->vr.baseMoment, (void *)v->vr.faceWeight,
                         (void *)v->vr.faceL, (void *)v->vr.AAInvB, (void *)v->vr.AInvb, (void *)v->vr.matA, (void *)v->vr.AAInvB32,
-                        (void *)v->vr.AInvb32, (void *)v->vr.sweepCoef, (void *)v->vr.sweepCoef32, (void *)v->vr.sweepErr, (void *)v->errWord, (void *)v->vr.bnd.type, (void *)v->vr.bnd.val})
+                        (void *)v->vr.AInvb32, (void *)v->vr.sweepCoef, (void *)v->vr.sweepCoef32, (void *)v->errWord, (void *)v->vr.bnd.type, (void *)v->vr.bnd.val})
             dev_free(p);
         delete v;
         return DNDSB_OK;
@@ -364,18 +364,6 @@ extern "C"
         else if (n == "cellPP") src = g.cellPP, cnt = m.nCell * g.nGc * 3;
         else if (n == "smoothRatio") src = g.smoothRatio, cnt = m.nCell;
         else if (n == "cellHMax") src = g.hMax, cnt = m.nCell;
-        else if (n == "sweepStatus")
-        {
-            // 1 when a bulk coefficient copy of the sweep did not complete within its bounded wait
-            int e = 0;
-            if (r.sweepErr && cudaMemcpy(&e, r.sweepErr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-                return cuda_fail("dndsb_vr_get_array");
-            if (len)
-                *len = 1;
-            if (hostOut)
-                hostOut[0] = e;
-            return DNDSB_OK;
-        }
         else if (n == "faceArea") src = g.faceArea, cnt = m.nFace;
         else if (n == "faceCent") src = g.faceCent, cnt = m.nFace * 3;
         else if (n == "faceJDet") src = g.faceJDet, cnt = m.nFace * g.nGf;

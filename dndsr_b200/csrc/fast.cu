@@ -270,13 +270,15 @@ DNDSB_GLOBAL void k_cell_par(int64_t nCell, int aniso, const real *__restrict__ 
 }
 
 // VR Jacobi sweep, R threads per cell (VariationalReconstruction_Reconstruction.hxx:485-615).
-// No barriers: the neighbour rows are read through L1 (the R threads of a cell
-// share each row), and the next face's coefficient row is loaded while the
-// current one is applied, so every thread keeps a full row of HBM loads in flight.
+// Coefficients come from the packed, transposed stream coefT[cell][face][j][i] (j < R: A^-1 B
+// entry (i, j); j = R: A^-1 b entry i), so for each j the R threads of a cell read R consecutive
+// values (one or two L1 lines per cell instead of a strided row each).  The neighbour's uRec
+// block and mean are read as broadcasts: the R threads of a cell share each line through L1.
+// No barriers; the next face's coefficients are loaded while the current face is applied.
 template <int R, int NV, typename TC>
-__global__ void __launch_bounds__(32 * R) k_vr_jacobi_fast(int64_t nCell, int nf, const int32_t *__restrict__ nbr, const TC *__restrict__ AAInvB,
-                                                           const TC *__restrict__ AInvb, const real *__restrict__ uRec, real *__restrict__ uRecNew,
-                                                           const real *__restrict__ u, real relax, int recordInc, int uRecIsZero)
+__global__ void __launch_bounds__(32 * R, 2) k_vr_jacobi_fast(int64_t nCell, int nf, const int32_t *__restrict__ nbr, const TC *__restrict__ coefT,
+                                                           const real *__restrict__ uRec, real *__restrict__ uRecNew, const real *__restrict__ u,
+                                                           real relax, int recordInc, int uRecIsZero)
 {
     const int tid = threadIdx.x;
     const int cl = tid / R, i = tid - cl * R;
@@ -293,26 +295,26 @@ __global__ void __launch_bounds__(32 * R) k_vr_jacobi_fast(int64_t nCell, int nf
     }
     const real sgn = recordInc ? -1.0 : relax;
     const bool useRec = !(recordInc && uRecIsZero);
-    const TC *Mbase = AAInvB + ((c * (nf + 1) + 1) * R + i) * R; // row i of block 1 + k is Mbase + k R^2
-    TC Mcur[R], Mnext[R];
+    const TC *cb = coefT + c * nf * (R + 1) * R + i; // entry (face k, j) at cb[(k (R+1) + j) R]
+    TC Mcur[R + 1], Mnext[R + 1];
 #pragma unroll
-    for (int j = 0; j < R; j++)
-        Mcur[j] = useRec ? Mbase[j] : TC(0);
+    for (int j = 0; j <= R; j++)
+        Mcur[j] = (useRec || j == R) ? cb[j * R] : TC(0);
     for (int k = 0; k < nf; k++)
     {
         if (k + 1 < nf)
         {
 #pragma unroll
-            for (int j = 0; j < R; j++)
-                Mnext[j] = useRec ? Mbase[(k + 1) * R * R + j] : TC(0);
+            for (int j = 0; j <= R; j++)
+                Mnext[j] = (useRec || j == R) ? cb[((k + 1) * (R + 1) + j) * R] : TC(0);
         }
         int o = nbr[c * nf + k];
         if (o >= 0)
         {
-            real bi = (real)AInvb[(c * nf + k) * R + i];
+            real t[NV];
             const real *rr = uRec + (int64_t)o * R * NV;
             const real *uo = u + (int64_t)o * NV;
-            real t[NV];
+            const real bi = (real)Mcur[R];
 #pragma unroll
             for (int v = 0; v < NV; v++)
                 t[v] = bi * (uo[v] - ui[v]);
@@ -321,7 +323,7 @@ __global__ void __launch_bounds__(32 * R) k_vr_jacobi_fast(int64_t nCell, int nf
 #pragma unroll
                 for (int j = 0; j < R; j++)
                 {
-                    real mij = (real)Mcur[j];
+                    const real mij = (real)Mcur[j];
 #pragma unroll
                     for (int v = 0; v < NV; v++)
                         t[v] += mij * rr[j * NV + v];
@@ -332,169 +334,12 @@ __global__ void __launch_bounds__(32 * R) k_vr_jacobi_fast(int64_t nCell, int nf
                 acc[v] += sgn * t[v];
         }
 #pragma unroll
-        for (int j = 0; j < R; j++)
+        for (int j = 0; j <= R; j++)
             Mcur[j] = Mnext[j];
     }
 #pragma unroll
     for (int v = 0; v < NV; v++)
         uRecNew[(c * R + i) * NV + v] = acc[v];
-}
-
-// VR Jacobi sweep with the coefficient stream staged by bulk async copies (the Blackwell TMA
-// engine, untiled form): each block owns G consecutive cells at a time; one thread issues a single
-// cp.async.bulk of their packed [G][nf][R][R+1] coefficients into shared memory and an mbarrier
-// counts the bytes in; meanwhile every thread loads its own row of uRec and u.  R threads per
-// cell then apply the rows from shared memory (neighbour reconstructions through L1/L2).  Several
-// resident blocks per SM keep several copies in flight.  The wait on the mbarrier is bounded:
-// when it runs out the block records an error and returns after a second bounded wait.
-DNDSB_D uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-DNDSB_D bool mbar_wait(uint32_t mb, uint32_t phase, int limit)
-{
-    for (int it = 0; it < limit; it++)
-    {
-        uint32_t ok;
-        asm volatile("{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n selp.b32 %0, 1, 0, P1;\n}\n"
-                     : "=r"(ok)
-                     : "r"(mb), "r"(phase)
-                     : "memory");
-        if (ok)
-            return true;
-    }
-    return false;
-}
-
-template <int R, int NV, typename TC, int G>
-__global__ void __launch_bounds__(G * R) k_vr_jacobi_bulk(int64_t nCell, int nf, const int32_t *__restrict__ nbr, const TC *__restrict__ coef,
-                                                          const real *__restrict__ uRec, real *__restrict__ uRecNew, const real *__restrict__ u,
-                                                          real relax, int recordInc, int uRecIsZero, int *err)
-{
-    extern __shared__ __align__(128) unsigned char smraw[];
-    __shared__ __align__(8) unsigned long long mbar;
-    const TC *sc = (const TC *)smraw;
-    const int tid = threadIdx.x, cl = tid / R, i = tid - cl * R;
-    const int per = nf * R * (R + 1);
-    const uint32_t bytesPerCell = (uint32_t)(per * sizeof(TC));
-    const uint32_t mb = smem_addr(&mbar), sdst = smem_addr(smraw);
-    if (tid == 0)
-    {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb), "r"(1) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    __syncthreads();
-    const real sgn = recordInc ? -1.0 : relax;
-    const bool useRec = !(recordInc && uRecIsZero);
-    uint32_t phase = 0;
-    for (int64_t grp = blockIdx.x; grp * G < nCell; grp += gridDim.x)
-    {
-        const int64_t c0 = grp * G;
-        const int n = (int)(nCell - c0 < G ? nCell - c0 : G);
-        if (tid == 0)
-        {
-            const uint32_t bytes = (uint32_t)n * bytesPerCell;
-            const TC *src = coef + c0 * per;
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb), "r"(bytes) : "memory");
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(sdst), "l"(src),
-                         "r"(bytes), "r"(mb)
-                         : "memory");
-        }
-        const int64_t c = c0 + cl;
-        const bool act = cl < n;
-        real acc[NV], ui[NV];
-        int on[8];
-        if (act)
-        {
-#pragma unroll
-            for (int v = 0; v < NV; v++)
-            {
-                real x = uRec[(c * R + i) * NV + v];
-                acc[v] = recordInc ? (uRecIsZero ? 0.0 : x) : x * (1 - relax);
-                ui[v] = u[c * NV + v];
-            }
-            for (int k = 0; k < nf; k++)
-                on[k] = nbr[c * nf + k];
-        }
-        // every thread waits (bounded), then the block decides together whether the copy landed
-        bool landed = mbar_wait(mb, phase, 1 << 22);
-        if (!__syncthreads_and(landed))
-        {
-            if (tid == 0)
-                atomicOr(err, 1);
-            mbar_wait(mb, phase, 1 << 22); // let a late copy finish before the block's shared memory is released
-            return;
-        }
-        phase ^= 1;
-        if (act)
-        {
-            for (int k = 0; k < nf; k++)
-            {
-                int o = on[k];
-                if (o < 0)
-                    continue;
-                const TC *row = sc + (cl * nf + k) * R * (R + 1) + i * (R + 1);
-                real bi = (real)row[R];
-                const real *rr = uRec + (int64_t)o * R * NV;
-                const real *uo = u + (int64_t)o * NV;
-                real t[NV];
-#pragma unroll
-                for (int v = 0; v < NV; v++)
-                    t[v] = bi * (uo[v] - ui[v]);
-                if (useRec)
-                {
-#pragma unroll
-                    for (int j = 0; j < R; j++)
-                    {
-                        real mij = (real)row[j];
-#pragma unroll
-                        for (int v = 0; v < NV; v++)
-                            t[v] += mij * rr[j * NV + v];
-                    }
-                }
-#pragma unroll
-                for (int v = 0; v < NV; v++)
-                    acc[v] += sgn * t[v];
-            }
-#pragma unroll
-            for (int v = 0; v < NV; v++)
-                uRecNew[(c * R + i) * NV + v] = acc[v];
-        }
-        __syncthreads(); // every row read before the next copy lands
-    }
-}
-
-template <int R, typename TC>
-constexpr int bulk_group() { return R <= 3 ? 64 : R <= 5 ? 32 : R <= 9 ? 16 : 8; }
-
-template <int R, typename TC>
-int launch_vr_bulk(const MeshD &m, const VRD &vr, const TC *coef, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
-                   cudaStream_t st)
-{
-    constexpr int G = bulk_group<R, TC>();
-    const size_t cellBytes = (size_t)m.nf * R * (R + 1) * sizeof(TC);
-    if (cellBytes % 16 != 0 || m.nf > 8 || !coef || !vr.sweepErr)
-        return ST_UNSUPPORTED;
-    const size_t smem = cellBytes * G;
-    if (smem > 200 * 1024)
-        return ST_UNSUPPORTED;
-    static unsigned long long attrSet = 0; // one bit per device
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 64 && !((attrSet >> dev) & 1ULL))
-    {
-        if (cudaFuncSetAttribute(k_vr_jacobi_bulk<R, 5, TC, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return ST_CUDA;
-        attrSet |= 1ULL << dev;
-    }
-    int64_t groups = (m.nCell + G - 1) / G;
-    int perSM = (int)((220 * 1024) / (smem + 1024));
-    perSM = perSM < 1 ? 1 : perSM > 8 ? 8 : perSM;
-    int64_t grid = 148LL * perSM;
-    if (grid > groups)
-        grid = groups;
-    k_vr_jacobi_bulk<R, 5, TC, G><<<(unsigned)grid, G * R, smem, st>>>(m.nCell, m.nf, m.cellNbr, coef, uRec, uRecNew, u, vr.s.jacobiRelax,
-                                                                       recordInc, uRecIsZero, vr.sweepErr);
-    return ST_OK;
 }
 
 template <int DIM, int P, int NV, int NG>
@@ -581,24 +426,18 @@ int rhs_face_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev
 int vr_iter_fast(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
                  int useFP32, cudaStream_t st)
 {
-    if (nv != 5 || m.nf > 6)
+    if (nv != 5 || !vr.sweepCoef)
         return ST_UNSUPPORTED;
     unsigned nb = (unsigned)((m.nCell + 31) / 32);
     real relax = vr.s.jacobiRelax;
 #define DNDSB_VRF(RR)                                                                                                                       \
     do                                                                                                                                      \
     {                                                                                                                                       \
-        int brc = useFP32 ? launch_vr_bulk<RR, float>(m, vr, vr.sweepCoef32, uRec, uRecNew, u, recordInc, uRecIsZero, st)               \
-                          : launch_vr_bulk<RR, real>(m, vr, vr.sweepCoef, uRec, uRecNew, u, recordInc, uRecIsZero, st);                   \
-        if (brc == ST_CUDA)                                                                                                                 \
-            return ST_CUDA;                                                                                                                 \
-        if (brc == ST_OK)                                                                                                                   \
-            break;                                                                                                                          \
         if (useFP32)                                                                                                                        \
-            k_vr_jacobi_fast<RR, 5, float><<<nb, 32 * RR, 0, st>>>(m.nCell, m.nf, m.cellNbr, vr.AAInvB32, vr.AInvb32, uRec, uRecNew, u, relax, \
+            k_vr_jacobi_fast<RR, 5, float><<<nb, 32 * RR, 0, st>>>(m.nCell, m.nf, m.cellNbr, vr.sweepCoef32, uRec, uRecNew, u, relax,      \
                                                                    recordInc, uRecIsZero);                                                  \
         else                                                                                                                                \
-            k_vr_jacobi_fast<RR, 5, real><<<nb, 32 * RR, 0, st>>>(m.nCell, m.nf, m.cellNbr, vr.AAInvB, vr.AInvb, uRec, uRecNew, u, relax,    \
+            k_vr_jacobi_fast<RR, 5, real><<<nb, 32 * RR, 0, st>>>(m.nCell, m.nf, m.cellNbr, vr.sweepCoef, uRec, uRecNew, u, relax,         \
                                                                   recordInc, uRecIsZero);                                                   \
     } while (0)
     switch (vr.R)
@@ -614,9 +453,6 @@ int vr_iter_fast(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *
         break;
     case 9:
         DNDSB_VRF(9);
-        break;
-    case 19:
-        DNDSB_VRF(19);
         break;
     default:
         return ST_UNSUPPORTED;

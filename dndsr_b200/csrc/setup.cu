@@ -515,7 +515,7 @@ DNDSB_GLOBAL void k_vr_coeff(MeshD m, GeomD g, VRD vr, int *err)
     }
 }
 
-// [cell][face k][row i][R+1]: row i of A^-1 B_k followed by (A^-1 b_k)_i
+// packed sweep coefficients [cell][face k][j][i]: entry (i, j) of A^-1 B_k for j < R, (A^-1 b_k)_i for j = R
 DNDSB_GLOBAL void k_pack_sweep(int64_t nCell, int nf, int R, const real *__restrict__ AAInvB, const real *__restrict__ AInvb, real *out,
                                float *out32)
 {
@@ -524,9 +524,10 @@ DNDSB_GLOBAL void k_pack_sweep(int64_t nCell, int nf, int R, const real *__restr
     {
         int64_t c = e / per;
         int r = (int)(e - c * per);
+        // layout [cell][face k][j][i]: j < R is column j of A^-1 B_k, j = R is A^-1 b_k
         int k = r / (R * (R + 1));
         int rem = r - k * R * (R + 1);
-        int i = rem / (R + 1), j = rem - i * (R + 1);
+        int j = rem / R, i = rem - j * R;
         real v = j < R ? AAInvB[((c * (nf + 1) + 1 + k) * R + i) * R + j] : AInvb[(c * nf + k) * R + i];
         out[e] = v;
         out32[e] = (float)v;
@@ -672,9 +673,6 @@ int vr_construct_rec_coeff(const MeshD &m, const GeomD &g, VRD &vr, int *errWord
         if (alloc_real(&vr.sweepCoef, nS) || dev_alloc((void **)&vr.sweepCoef32, sizeof(float) * nS) != cudaSuccess)
             return ST_CUDA;
         DNDSB_LAUNCH(k_pack_sweep, nS, 256, st, m.nCell, m.nf, R, vr.AAInvB, vr.AInvb, vr.sweepCoef, vr.sweepCoef32);
-        if (!vr.sweepErr && dev_alloc((void **)&vr.sweepErr, sizeof(int)) != cudaSuccess)
-            return ST_CUDA;
-        dev_zero(vr.sweepErr, sizeof(int), st);
     }
     int e = 0;
     d2h(&e, errWord, sizeof(int), st);

@@ -120,7 +120,6 @@ struct VRD
     // one contiguous, 16-byte aligned range per cell, staged into shared memory by bulk async copies
     real *sweepCoef = nullptr;
     float *sweepCoef32 = nullptr;
-    int *sweepErr = nullptr; // device word: a bulk copy that did not complete in time
     BoundaryD bnd;           // boundary values for the BC faces of the sweep
 };
 
