@@ -287,7 +287,7 @@ DNDSB_GLOBAL void k_gmres_lsq(int k, const real *H, real *sc)
 
 // x += sum_i y_i v_i over the valid columns
 template <typename T>
-DNDSB_GLOBAL void k_gmres_update(int64_t n, int k, const T *__restrict__ V, const real *__restrict__ sc, T *x)
+DNDSB_GLOBAL void k_gmres_update(int64_t n, int64_t ld, int k, const T *__restrict__ V, const real *__restrict__ sc, T *x)
 {
     int nv = (int)sc[2];
     if (nv > k)
@@ -296,7 +296,7 @@ DNDSB_GLOBAL void k_gmres_update(int64_t n, int k, const T *__restrict__ V, cons
     {
         real acc = (real)x[i];
         for (int jj = 0; jj < nv; jj++)
-            acc += sc[kScY + jj] * (real)V[jj * n + i];
+            acc += sc[kScY + jj] * (real)V[jj * ld + i];
         x[i] = (T)acc;
     }
 }
@@ -370,11 +370,12 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv)
               dev_alloc(&w->uT, es * n) == cudaSuccess && dev_alloc(&w->rhsT, es * n) == cudaSuccess &&
               dev_alloc(&w->x, es * n) == cudaSuccess && dev_alloc(&w->tmp, es * n) == cudaSuccess &&
               dev_alloc(&w->tmp2, es * n) == cudaSuccess && dev_alloc(&w->MLb, es * n) == cudaSuccess &&
-              dev_alloc(&w->V, es * n * (k + 1)) == cudaSuccess &&
+              dev_alloc(&w->V, es * krylov_ld(n) * (k + 1)) == cudaSuccess &&
               dev_alloc((void **)&w->H, sizeof(real) * (k + 1) * (k > 0 ? k : 1)) == cudaSuccess &&
               dev_alloc((void **)&w->sc, sizeof(real) * (kScY + 40)) == cudaSuccess &&
               dev_alloc((void **)&w->s2, sizeof(real) * 8) == cudaSuccess &&
               dev_alloc((void **)&w->red, sizeof(real) * kRedBufLenK) == cudaSuccess;
+    ok = ok && dev_zero(w->V, es * krylov_ld(n) * (k + 1), nullptr) == cudaSuccess; // the column pads stay zero
     if (!ok || stream_create(&w->cs) != cudaSuccess || event_create(&w->evIn) != cudaSuccess || event_create(&w->evOut) != cudaSuccess)
     {
         linws_free(w);
@@ -402,7 +403,8 @@ struct Solve
     cudaStream_t st;
     int64_t n() const { return m.nCell * NV; }
     using T4 = typename Vec4<T>::type;
-    T *V(int i) const { return (T *)w.V + (int64_t)i * n(); }
+    int64_t ld() const { return krylov_ld(n()); }
+    T *V(int i) const { return (T *)w.V + (int64_t)i * ld(); }
 
     // one colour sweep over all classes; result in xNew
     void sweep(const T *rhs, const T *xOld, T *xNew, bool forward, bool gs, bool zeroIn) const
@@ -489,12 +491,12 @@ struct Solve
                 FML(tmp, V(j + 1));
                 real *hcol = w.H + (int64_t)j * (k + 1);
                 // classical Gram-Schmidt: h = V^T w, w -= V h, h[j+1] = |w|
-                krylov_mdot(prec(), nn, NV, j + 1, w.V, V(j + 1), w.s2, w.red, hcol, st);
-                krylov_maxpy_norm(prec(), nn, NV, j + 1, w.V, hcol, V(j + 1), w.s2, w.red, hcol + j + 1, st);
+                krylov_mdot(prec(), nn, ld(), NV, j + 1, w.V, V(j + 1), w.s2, w.red, hcol, st);
+                krylov_maxpy_norm(prec(), nn, ld(), NV, j + 1, w.V, hcol, V(j + 1), w.s2, w.red, hcol + j + 1, st);
                 DNDSB_LAUNCH(k_gmres_next<T>, nn, 256, st, nn, V(j + 1), hcol, j, w.sc);
             }
             DNDSB_LAUNCH(k_gmres_lsq, 1, 32, st, k, w.H, w.sc);
-            DNDSB_LAUNCH(k_gmres_update<T>, nn, 256, st, nn, k, (const T *)w.V, w.sc, x);
+            DNDSB_LAUNCH(k_gmres_update<T>, nn, 256, st, nn, ld(), k, (const T *)w.V, w.sc, x);
             xZero = false;
         }
     }

@@ -112,52 +112,197 @@ DNDSB_D void block_sum4(real (*sh)[kRedBlock], real a0, real a1, real a2, real a
     }
 }
 
-// partial[block][col] = sum_i V[col][i] * w[i] * s2[i % NV] over the block's chunk
-template <typename T, int NV>
-DNDSB_GLOBAL void k_kmdot(int64_t n, int ncol, const T *__restrict__ V, const T *__restrict__ w, const real *__restrict__ s2, real *partial)
+// Quads of 4 consecutive elements, loaded as one 16-byte (float) or two 16-byte (double) loads.
+template <typename T>
+struct Quad;
+template <>
+struct Quad<float>
 {
-    __shared__ real sh[4][kRedBlock];
-    int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-    int64_t b0 = blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
-    for (int c0 = 0; c0 < ncol; c0 += 4)
+    static DNDSB_D void load(const float *p, real (&o)[4])
     {
-        real a[4] = {0, 0, 0, 0};
-        for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
+        float4 v = *(const float4 *)p;
+        o[0] = v.x, o[1] = v.y, o[2] = v.z, o[3] = v.w;
+    }
+    // stores x rounded to float and returns the stored values
+    static DNDSB_D void store(float *p, const real (&x)[4], real (&r)[4])
+    {
+        float4 v = make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
+        *(float4 *)p = v;
+        r[0] = v.x, r[1] = v.y, r[2] = v.z, r[3] = v.w;
+    }
+};
+template <>
+struct Quad<double>
+{
+    static DNDSB_D void load(const double *p, real (&o)[4])
+    {
+        double2 a = ((const double2 *)p)[0], b = ((const double2 *)p)[1];
+        o[0] = a.x, o[1] = a.y, o[2] = b.x, o[3] = b.y;
+    }
+    static DNDSB_D void store(double *p, const real (&x)[4], real (&r)[4])
+    {
+        ((double2 *)p)[0] = make_double2(x[0], x[1]);
+        ((double2 *)p)[1] = make_double2(x[2], x[3]);
+        r[0] = x[0], r[1] = x[1], r[2] = x[2], r[3] = x[3];
+    }
+};
+
+// sum over the block in a fixed order: xor-shuffle tree inside each warp (lane 0's value is
+// used), then the warps in index order by one thread; valid in thread 0 (and for column k in
+// thread k of the multi-column form below)
+DNDSB_D real warp_sum(real x)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+constexpr int kKG = 8; // columns per pass of the multi-dot
+
+// partial[block][col] = sum_i V[col][i] w[i] s2[i % NV] over the block's chunk of quads.  Columns are
+// ld apart (ld a multiple of 4, the pad beyond n zero); all columns of a pass share one read of w.
+template <typename T, int NV>
+DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmdot(int64_t n, int64_t ld, int ncol, const T *__restrict__ V, const T *__restrict__ w,
+                                                       const real *__restrict__ s2, real *partial)
+{
+    __shared__ real sh[kKG][kRedBlock / 32];
+    __shared__ real ss[8];
+    if (threadIdx.x < NV)
+        ss[threadIdx.x] = s2[threadIdx.x];
+    __syncthreads();
+    const int64_t nq = (n + 3) >> 2, cq = (nq + gridDim.x - 1) / gridDim.x;
+    const int64_t q0 = blockIdx.x * cq, q1 = q0 + cq < nq ? q0 + cq : nq;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int c0 = 0; c0 < ncol; c0 += kKG)
+    {
+        real a[kKG];
+#pragma unroll
+        for (int k = 0; k < kKG; k++)
+            a[k] = 0;
+        // r = (4 q) % NV, advanced incrementally with q
+        const int dr = (int)((4 * (int64_t)blockDim.x) % NV);
+        int r = (int)((4 * (q0 + threadIdx.x)) % NV);
+        const T *Vc = V + (int64_t)c0 * ld;
+        for (int64_t q = q0 + threadIdx.x; q < q1; q += blockDim.x)
         {
-            real wi = (real)w[i] * s2[i % NV];
-            for (int q = 0; q < 4; q++)
-                if (c0 + q < ncol)
-                    a[q] += (real)V[(int64_t)(c0 + q) * n + i] * wi;
+            real wv[4];
+            Quad<T>::load(w + 4 * q, wv);
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                wv[e] *= ss[r + e < NV ? r + e : r + e - NV];
+            r += dr;
+            r = r >= NV ? r - NV : r;
+            const T *pv = Vc + 4 * q;
+#pragma unroll
+            for (int k = 0; k < kKG; k++)
+                if (c0 + k < ncol)
+                {
+                    real v[4];
+                    Quad<T>::load(pv + k * ld, v);
+                    a[k] += v[0] * wv[0] + v[1] * wv[1] + v[2] * wv[2] + v[3] * wv[3];
+                }
         }
-        block_sum4(sh, a[0], a[1], a[2], a[3]);
-        if (threadIdx.x == 0)
-            for (int q = 0; q < 4 && c0 + q < ncol; q++)
-                partial[blockIdx.x * ncol + c0 + q] = sh[q][0];
+#pragma unroll
+        for (int k = 0; k < kKG; k++)
+        {
+            real x = warp_sum(a[k]);
+            if (lane == 0)
+                sh[k][wid] = x;
+        }
+        __syncthreads();
+        if (threadIdx.x < kKG && c0 + (int)threadIdx.x < ncol)
+        {
+            real t = 0;
+            for (int q = 0; q < nw; q++)
+                t += sh[threadIdx.x][q];
+            partial[blockIdx.x * ncol + c0 + threadIdx.x] = t;
+        }
         __syncthreads();
     }
 }
 
-// w -= sum_c h[c] V[c]; partial[block] = sum_i w_i^2 s2[i % NV] of the stored w
+// w -= sum_c h[c] V[c] (columns subtracted in index order); partial[block] = sum_i w_i^2 s2[i % NV]
+// of the stored w.  w is column ncol of the same basis (not read through V).
 template <typename T, int NV>
-DNDSB_GLOBAL void k_kmaxpy_norm(int64_t n, int ncol, const T *__restrict__ V, const real *__restrict__ h, T *w, const real *__restrict__ s2,
-                                real *partial)
+DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmaxpy_norm(int64_t n, int64_t ld, int ncol, const T *__restrict__ V, const real *__restrict__ h,
+                                                             T *w, const real *__restrict__ s2, real *partial)
 {
-    __shared__ real sh[4][kRedBlock];
-    __shared__ real hs[33];
+    __shared__ real hs[32];
+    __shared__ real ss[8];
+    __shared__ real sh[kRedBlock / 32];
     if (threadIdx.x < ncol)
         hs[threadIdx.x] = h[threadIdx.x];
+    if (threadIdx.x < NV)
+        ss[threadIdx.x] = s2[threadIdx.x];
     __syncthreads();
+    const int64_t nq = (n + 3) >> 2, cq = (nq + gridDim.x - 1) / gridDim.x;
+    const int64_t q0 = blockIdx.x * cq, q1 = q0 + cq < nq ? q0 + cq : nq;
+    real a = 0;
+    const int dr = (int)((4 * (int64_t)blockDim.x) % NV);
+    int r = (int)((4 * (q0 + threadIdx.x)) % NV);
+    for (int64_t q = q0 + threadIdx.x; q < q1; q += blockDim.x)
+    {
+        real x[4];
+        Quad<T>::load(w + 4 * q, x);
+        int c = 0;
+        for (; c + 4 <= ncol; c += 4)
+        {
+            real v[4][4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                Quad<T>::load(V + (int64_t)(c + k) * ld + 4 * q, v[k]);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+            {
+                const real hc = hs[c + k];
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    x[e] -= hc * v[k][e];
+            }
+        }
+        for (; c < ncol; c++)
+        {
+            real v[4];
+            Quad<T>::load(V + (int64_t)c * ld + 4 * q, v);
+            const real hc = hs[c];
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                x[e] -= hc * v[e];
+        }
+        real xr[4];
+        Quad<T>::store(w + 4 * q, x, xr);
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            a += xr[e] * xr[e] * ss[r + e < NV ? r + e : r + e - NV];
+        r += dr;
+        r = r >= NV ? r - NV : r;
+    }
+    const real x = warp_sum(a);
+    if ((threadIdx.x & 31) == 0)
+        sh[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        real t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++)
+            t += sh[q];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// partial[block] = sum_i x_i^2 s2[i % NV] (any length, any alignment)
+template <typename T, int NV>
+DNDSB_GLOBAL void k_knorm2(int64_t n, const T *__restrict__ x, const real *__restrict__ s2, real *partial)
+{
+    __shared__ real sh[4][kRedBlock];
     int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
     int64_t b0 = blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
     real a = 0;
     for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
     {
-        real x = (real)w[i];
-        for (int c = 0; c < ncol; c++)
-            x -= hs[c] * (real)V[(int64_t)c * n + i];
-        T xt = (T)x;
-        w[i] = xt;
-        a += (real)xt * (real)xt * s2[i % NV];
+        real d = (real)x[i];
+        a += d * d * s2[i % NV];
     }
     block_sum4(sh, a, 0, 0, 0);
     if (threadIdx.x == 0)
@@ -206,16 +351,23 @@ DNDSB_GLOBAL void k_kfinal(int nb, int ncol, const real *__restrict__ partial, r
 }
 
 template <typename T, int NV>
-void kmdot(int64_t n, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st)
+void kmdot(int64_t n, int64_t ld, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st)
 {
-    k_kmdot<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ncol, (const T *)V, (const T *)w, s2, red);
+    k_kmdot<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, (const T *)w, s2, red);
     k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, ncol, red, out, 0);
 }
 
 template <typename T, int NV>
-void kmaxpy(int64_t n, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm, cudaStream_t st)
+void kmaxpy(int64_t n, int64_t ld, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm, cudaStream_t st)
 {
-    k_kmaxpy_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ncol, (const T *)V, h, (T *)w, s2, red);
+    k_kmaxpy_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, h, (T *)w, s2, red);
+    k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+}
+
+template <typename T, int NV>
+void knorm(int64_t n, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st)
+{
+    k_knorm2<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, s2, red);
     k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
 }
 
@@ -224,12 +376,6 @@ void kdiff(int64_t n, const void *x, const void *y, const real *s2, real *red, r
 {
     k_kdiff_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, (const T *)y, s2, red);
     k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
-}
-
-DNDSB_GLOBAL void k_ksqrt(real *x)
-{
-    if (threadIdx.x == 0)
-        *x = sqrt(*x);
 }
 
 #define DNDSB_KDISPATCH(FN, ...)                      \
@@ -246,22 +392,22 @@ DNDSB_GLOBAL void k_ksqrt(real *x)
     } while (0)
 } // namespace
 
-void krylov_mdot(int prec, int64_t n, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st)
+// V: ncol columns ld apart (ld a multiple of 4, 16-byte aligned, zero beyond n); w: a column of the same storage
+void krylov_mdot(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out,
+                 cudaStream_t st)
 {
-    DNDSB_KDISPATCH(kmdot, n, ncol, V, w, s2, red, out, st);
+    DNDSB_KDISPATCH(kmdot, n, ld, ncol, V, w, s2, red, out, st);
 }
 
-void krylov_maxpy_norm(int prec, int64_t n, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm,
-                       cudaStream_t st)
+void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red,
+                       real *outNorm, cudaStream_t st)
 {
-    DNDSB_KDISPATCH(kmaxpy, n, ncol, V, h, w, s2, red, outNorm, st);
+    DNDSB_KDISPATCH(kmaxpy, n, ld, ncol, V, h, w, s2, red, outNorm, st);
 }
 
 void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st)
 {
-    // |x| = sqrt(x . x): the dot with itself, then the root on the device
-    DNDSB_KDISPATCH(kmdot, n, 1, x, x, s2, red, outNorm, st);
-    k_ksqrt<<<1, 1, 0, st>>>(outNorm);
+    DNDSB_KDISPATCH(knorm, n, x, s2, red, outNorm, st);
 }
 
 void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st)

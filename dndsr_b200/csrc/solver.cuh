@@ -216,9 +216,12 @@ int linear_solve(const MeshD &m, const GeomD &g, EvalD &ev, LinWs *&ws, const Li
                  const real *u, const real *rhs, real *xInc, cudaStream_t st);
 void linws_free(LinWs *w);
 // prec 0: double vectors, 1: float vectors; nv 5 or 6; FP64 accumulation, deterministic
-void krylov_mdot(int prec, int64_t n, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st);
-void krylov_maxpy_norm(int prec, int64_t n, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm,
-                       cudaStream_t st);
+// Krylov basis columns are ld apart: ld = n rounded up to a multiple of 4, storage 16-byte aligned, pad zero
+inline int64_t krylov_ld(int64_t n) { return (n + 3) & ~(int64_t)3; }
+void krylov_mdot(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out,
+                 cudaStream_t st);
+void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red,
+                       real *outNorm, cudaStream_t st);
 void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st);
 void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st);
 } // namespace dndsb
