@@ -633,6 +633,35 @@ extern "C"
                           "dndsb_eval_lusgs_matrix_vec");
     }
 
+    int dndsb_eval_lusgs_matrix_vec_t(dndsb_eval *e, double alphaDiag, const double *u, const double *y, const double *jdiag, double *ATy,
+                                      void *stream)
+    {
+        if (!e || !u || !y || !jdiag || !ATy || y == ATy)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_vec_t: null or aliased argument");
+        return status_msg(lusgs_matvec_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, y, jdiag, ATy, S(stream)),
+                          "dndsb_eval_lusgs_matrix_vec_t");
+    }
+
+    int dndsb_eval_update_sgs_t(dndsb_eval *e, double alphaDiag, const double *b, const double *u, const double *y, double *yNew,
+                                const double *jdiag, int forward, int gsUpdate, void *stream)
+    {
+        if (!e || !b || !u || !y || !yNew || !jdiag)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: null argument");
+        if (y == yNew)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: y and yNew must differ");
+        return status_msg(update_sgs_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate, S(stream)),
+                          "dndsb_eval_update_sgs_t");
+    }
+
+    int dndsb_eval_pressure_force(dndsb_eval *e, int zone, const double *dir, const double *u, const double *uRec, double *Jhost, double *dJdu,
+                                  double *dJduRec, void *stream)
+    {
+        if (!e || !dir || !u || !uRec || !Jhost)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_pressure_force: null argument");
+        return status_msg(pressure_force(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, zone, dir, u, uRec, Jhost, dJdu, dJduRec, S(stream)),
+                          "dndsb_eval_pressure_force");
+    }
+
     int dndsb_eval_solve_linear(dndsb_eval *e, const dndsb_linear_settings *ls, double alphaDiag, const double *dTau, double dt,
                                 const double *u, const double *rhs, double *xInc, void *stream)
     {

@@ -167,6 +167,13 @@ int update_sgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const 
 int lusgs_matvec(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jdiag,
                  real *AuInc, cudaStream_t st);
 int init_field(const MeshD &m, const GeomD &g, const EvalD &ev, int kind, real chi, real *u, cudaStream_t st);
+// adjoint building blocks (adjoint_ops.cu)
+int lusgs_matvec_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *y, const real *jdiag, real *ATy,
+                   cudaStream_t st);
+int update_sgs_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *b, const real *u, const real *y, real *yNew,
+                 const real *jdiag, int forward, int gsUpdate, cudaStream_t st);
+int pressure_force(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, int zone, const real *dir, const real *u, const real *uRec,
+                   real *Jhost, real *gU, real *gRec, cudaStream_t st);
 int vr_swap(int64_t n, real *a, real *b, cudaStream_t st);
 // tuned kernels (fast.cu); ST_UNSUPPORTED means "use the generic kernel"
 int fast_geometry(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, cudaStream_t st);

@@ -275,6 +275,26 @@ class EulerEvaluator(Handle):
         capi.call("dndsb_eval_lusgs_matrix_vec", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(uInc, "uInc"), _ptr(jdiag, "jdiag"),
                   _ptr(AuInc, "AuInc"), _stream())
 
+    def LUSGSMatrixVecT(self, alphaDiag, u, y, jdiag, ATy):
+        """ATy = A^T y for the operator A of LUSGSMatrixVec (same lambdaFace, jdiag, alphaDiag)."""
+        capi.call("dndsb_eval_lusgs_matrix_vec_t", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(y, "y"), _ptr(jdiag, "jdiag"),
+                  _ptr(ATy, "ATy"), _stream())
+
+    def UpdateSGST(self, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate=True):
+        """One Gauss-Seidel sweep on A^T y = b (the transpose of UpdateSGS), colour by colour."""
+        capi.call("dndsb_eval_update_sgs_t", self.h, float(alphaDiag), _ptr(b, "b"), _ptr(u, "u"), _ptr(y, "y"), _ptr(yNew, "yNew"),
+                  _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), _stream())
+
+    def PressureForce(self, zone, direction, u, uRec, grad=False):
+        """Pressure force along direction on boundary zone; with grad also (dJ/du, dJ/duRec) as device tensors."""
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        J = np.zeros(1)
+        gU = torch.empty_like(u) if grad else None
+        gR = torch.empty_like(uRec) if grad else None
+        capi.call("dndsb_eval_pressure_force", self.h, int(zone), capi.dptr(d), _ptr(u, "u"), _ptr(uRec, "uRec"), capi.dptr(J),
+                  _ptr(gU, "dJdu") if grad else None, _ptr(gR, "dJduRec") if grad else None, _stream())
+        return (float(J[0]), gU, gR) if grad else float(J[0])
+
     def SolveLinear(self, alphaDiag, dTau, dt, u, rhs, xInc, gmresCode=0, jacobiCode=1, sgsIter=0, nGmresSpace=5, nGmresIter=1,
                     precision="fp64", meanScale=None, useGraph=True):
         """EulerSolver::solveLinear with LUSGSMatrixInit (EulerSolver.hxx:1407-1579, EulerEvaluator.hxx:37-159):

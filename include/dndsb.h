@@ -186,6 +186,22 @@ int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *
 int dndsb_eval_rhs_vjp(dndsb_eval *ev, const double *w, const double *u, const double *uRec, double *du, double *duRec, void *stream);
 int dndsb_eval_rhs_jvp(dndsb_eval *ev, const double *du, const double *duRec, const double *u, const double *uRec, double *dRhs, void *stream);
 
+/* Adjoint building blocks (no reference counterpart; they transpose the operators above).
+ * lusgs_matrix_vec_t: ATy = A^T y for the operator A of dndsb_eval_lusgs_matrix_vec (same lambdaFace,
+ * jdiag and alphaDiag).  update_sgs_t: one Gauss-Seidel sweep on A^T y = b, colour by colour (forward:
+ * colours ascending, new values of earlier colours when gsUpdate), y and yNew distinct; a forward then
+ * a backward sweep is the symmetric Gauss-Seidel preconditioner of A^T. */
+int dndsb_eval_lusgs_matrix_vec_t(dndsb_eval *ev, double alphaDiag, const double *u, const double *y, const double *jdiag, double *ATy,
+                                  void *stream);
+int dndsb_eval_update_sgs_t(dndsb_eval *ev, double alphaDiag, const double *b, const double *u, const double *y, double *yNew,
+                            const double *jdiag, int forward, int gsUpdate, void *stream);
+/* Pressure force along dir[3] on the boundary faces of zone:
+ *   J = sum_f sum_g |J|_g w_g p(U_L(x_g)) (n_g . dir),  U_L = u + phi . uRec of the face's cell,
+ * returned in *Jhost; dJdu [nCell][nVars] and dJduRec [nCell][R][nVars] (device, either may be NULL)
+ * receive its gradient, zero away from the zone. */
+int dndsb_eval_pressure_force(dndsb_eval *ev, int zone, const double *dir, const double *u, const double *uRec, double *Jhost, double *dJdu,
+                              double *dJduRec, void *stream);
+
 /* Linear-solver controls, EulerSolver.hpp linearSolverControl (fields of the same names) plus the
  * precision of the solve.  meanScale: the GMRES dot weights of EulerSolver.hxx:1518-1540
  * (dot(a, b) = sum a_v b_v / (meanScale_v + 1e-200)^2); entries <= 0 count as 1. */

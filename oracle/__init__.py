@@ -87,6 +87,10 @@ def _declare(L):
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_update_sgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
     L.orc_lusgs_matvec.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D]
+    L.orc_lusgs_matvec_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D]
+    L.orc_update_sgs_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
+    L.orc_pressure_force.argtypes = [_V, ctypes.c_int, _D, _D, _D, _D, _D]
+    L.orc_pressure_force.restype = ctypes.c_double
     L.orc_riemann.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                               ctypes.c_double, _D, _D]
     L.orc_viscous_flux.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -242,6 +246,29 @@ class Oracle:
         out = np.zeros_like(uInc)
         lib().orc_lusgs_matvec(self.h, alphaDiag, _p(u), _p(uInc), _p(jdiag), _p(out))
         return out
+
+    def lusgs_matvec_t(self, alphaDiag, u, y, jdiag):
+        """Transpose of lusgs_matvec applied to y."""
+        u, y, jdiag = _f64(u), _f64(y), _f64(jdiag)
+        out = np.zeros_like(y)
+        lib().orc_lusgs_matvec_t(self.h, alphaDiag, _p(u), _p(y), _p(jdiag), _p(out))
+        return out
+
+    def update_sgs_t(self, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate=True):
+        """One Gauss-Seidel sweep on the transposed LU-SGS system, natural cell order."""
+        b, u, y, jdiag = _f64(b), _f64(u), _f64(y), _f64(jdiag)
+        out = np.array(yNew, dtype=np.float64, copy=True, order="C")
+        lib().orc_update_sgs_t(self.h, alphaDiag, _p(b), _p(u), _p(y), _p(out), _p(jdiag), int(forward), int(gsUpdate))
+        return out
+
+    def pressure_force(self, zone, direction, u, uRec, grad=False):
+        """Pressure force along direction on boundary zone; with grad, also (dJ/du, dJ/duRec)."""
+        u, uRec = _f64(u), _f64(uRec)
+        d = _f64(np.asarray(direction, dtype=np.float64))
+        gU = np.zeros_like(u) if grad else None
+        gR = np.zeros_like(uRec) if grad else None
+        J = lib().orc_pressure_force(self.h, int(zone), _p(d), _p(u), _p(uRec), _p(gU) if grad else None, _p(gR) if grad else None)
+        return (J, gU, gR) if grad else J
 
     def cell_point_values(self, u, uRec):
         u, uRec = _f64(u), _f64(uRec)

@@ -2193,6 +2193,155 @@ struct Oracle
         }
     }
 
+    // transpose of fluxJacTimesDu: out = (dF/dU at U along n, minus lambda I)^T y, written as the reverse
+    // sweep of the same statements (adjoint LU-SGS operator, no reference counterpart)
+    void fluxJacTransposeTimes(const real *U, const real n[3], const real *y, real lambdaMain, real *out) const
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        real ir = 1.0 / U[0];
+        real velo[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
+        real p, H, asqr;
+        idealGasThermal(U[4], U[0], dot3(velo, velo), gamma, p, asqr, H);
+        real vn = dot3(velo, n);
+        for (int j = 0; j < nv; j++)
+            out[j] = -lambdaMain * y[j] + vn * (j >= 1 ? y[j] : 0.0);
+        real bvn = 0, bp = 0;
+        for (int d = 0; d < 3; d++)
+        {
+            out[1 + d] += n[d] * y[0];
+            bvn += U[1 + d] * y[1 + d];
+            bp += n[d] * y[1 + d];
+        }
+        bp += vn * y[4];
+        bvn += (U[4] + p) * y[4];
+        for (int j = 5; j < nv; j++)
+            bvn += U[j] * y[j];
+        out[4] += (gamma - 1) * bp;
+        for (int d = 0; d < 3; d++)
+        {
+            real bv = n[d] * bvn - 0.5 * (gamma - 1) * U[1 + d] * bp;
+            out[1 + d] += -0.5 * (gamma - 1) * velo[d] * bp + ir * bv;
+            out[0] += -U[1 + d] * ir * ir * bv;
+        }
+    }
+
+    // transpose of LUSGSMatrixVec: (A^T y)_q = D_q y_q + sum_c w_cq (J_q(n_cq) - lambda)^T y_c with
+    // w_cq = alpha A_f / (2 V_c) and n_cq the normal out of the neighbour c
+    void lusgsMatVecT(real alphaDiag, const real *u, const real *y, const real *jdiag, real *ATy) const
+    {
+        int nv = es.nVars;
+#pragma omp parallel for schedule(static)
+        for (long q = 0; q < nCell; q++)
+        {
+            real buf[8] = {0};
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[q * nf + k];
+                long c = otherOf(q, f);
+                if (c < 0)
+                    continue;
+                int side = sideOf(q, f);
+                real n[3];
+                for (int d = 0; d < 3; d++)
+                    n[d] = -faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+                real t[8];
+                fluxJacTransposeTimes(u + q * nv, n, y + c * nv, lambdaFace[f], t);
+                for (int v = 0; v < nv; v++)
+                    buf[v] += (0.5 * alphaDiag) * faceArea[f] / vol[c] * t[v];
+            }
+            for (int v = 0; v < nv; v++)
+                ATy[q * nv + v] = jdiag[nv >= 6 ? q * nv + v : q] * y[q * nv + v] + buf[v];
+        }
+    }
+
+    // one Gauss-Seidel sweep on A^T y = b, sequential in natural cell order (the transposed UpdateSGS)
+    void updateSGST(real alphaDiag, const real *b, const real *u, const real *y, real *yNew, const real *jdiag, bool forward, bool gsUpdate) const
+    {
+        int nv = es.nVars;
+        for (long s = 0; s < nCell; s++)
+        {
+            long q = forward ? s : nCell - 1 - s;
+            real buf[8];
+            for (int v = 0; v < nv; v++)
+                buf[v] = b[q * nv + v];
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[q * nf + k];
+                long c = otherOf(q, f);
+                if (c < 0 || c == q)
+                    continue;
+                bool useNew = gsUpdate && (forward ? (c < q) : (c > q));
+                int side = sideOf(q, f);
+                real n[3];
+                for (int d = 0; d < 3; d++)
+                    n[d] = -faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+                real t[8];
+                fluxJacTransposeTimes(u + q * nv, n, (useNew ? yNew : y) + c * nv, lambdaFace[f], t);
+                for (int v = 0; v < nv; v++)
+                    buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * t[v];
+            }
+            for (int v = 0; v < nv; v++)
+                yNew[q * nv + v] = buf[v] / jdiag[nv >= 6 ? q * nv + v : q];
+        }
+    }
+
+    // Pressure force along dir on the boundary faces of one zone:
+    //   J = sum_f sum_g |J|_g w_g p(U_L(x_g)) (n_g . dir),  U_L = u + phi . uRec of the face's cell
+    // (the reconstructed state the boundary flux starts from, boundaryFaceFlux above), with its gradient
+    // with respect to u and uRec (objective of the adjoint, no reference counterpart)
+    real pressureForce(int zone, const real *dir, const real *u, const real *uRec, real *gU, real *gRec) const
+    {
+        int nv = es.nVars;
+        real gamma = es.gamma;
+        std::vector<real> T0(4 * NDOF);
+        real J = 0;
+        if (gU)
+            std::fill(gU, gU + nCell * nv, 0.0);
+        if (gRec)
+            std::fill(gRec, gRec + nCell * R * nv, 0.0);
+        for (long f = 0; f < nFace; f++)
+        {
+            if (face2cell[f * 2 + 1] >= 0 || faceZone[f] != zone)
+                continue;
+            long c0 = face2cell[f * 2 + 0];
+            for (int g = 0; g < nGf; g++)
+            {
+                real pq[3], w;
+                quadPoint(faceType, vs.intOrder, g, pq, w);
+                const real *n = &faceNorm[(f * nGf + g) * 3];
+                const real *p0 = &facePP[(f * nGf + g) * 3];
+                diffBase(c0, p0, T0.data(), 1, true);
+                real UL[8];
+                for (int v = 0; v < nv; v++)
+                {
+                    real a = 0;
+                    for (int j = 0; j < R; j++)
+                        a += T0[1 + j] * uRec[(c0 * R + j) * nv + v];
+                    UL[v] = u[c0 * nv + v] + a;
+                }
+                real vel[3] = {UL[1] / UL[0], UL[2] / UL[0], UL[3] / UL[0]};
+                real p = (gamma - 1) * (UL[4] - 0.5 * UL[0] * dot3(vel, vel));
+                real wt = faceJDet[f * nGf + g] * w * dot3(n, dir);
+                J += wt * p;
+                real dp[8] = {0};
+                dp[0] = (gamma - 1) * 0.5 * dot3(vel, vel);
+                for (int d = 0; d < 3; d++)
+                    dp[1 + d] = -(gamma - 1) * vel[d];
+                dp[4] = gamma - 1;
+                for (int v = 0; v < nv; v++)
+                {
+                    if (gU)
+                        gU[c0 * nv + v] += wt * dp[v];
+                    if (gRec)
+                        for (int j = 0; j < R; j++)
+                            gRec[(c0 * R + j) * nv + v] += wt * T0[1 + j] * dp[v];
+                }
+            }
+        }
+        return J;
+    }
+
     // EulerEvaluator.hxx:1039-1143 InitializeUDOF: 2 = isentropic vortex (chi given), 3 = Taylor-Green (M0 = 0.1)
     void initField(int kind, real chi, real *u) const
     {
@@ -2376,6 +2525,22 @@ extern "C"
     void orc_lusgs_matvec(void *h, double alphaDiag, const double *u, const double *uInc, const double *jdiag, double *AuInc)
     {
         ((Oracle *)h)->lusgsMatVec(alphaDiag, u, uInc, jdiag, AuInc);
+    }
+
+    void orc_lusgs_matvec_t(void *h, double alphaDiag, const double *u, const double *y, const double *jdiag, double *ATy)
+    {
+        ((Oracle *)h)->lusgsMatVecT(alphaDiag, u, y, jdiag, ATy);
+    }
+
+    void orc_update_sgs_t(void *h, double alphaDiag, const double *b, const double *u, const double *y, double *yNew, const double *jdiag,
+                          int forward, int gsUpdate)
+    {
+        ((Oracle *)h)->updateSGST(alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate);
+    }
+
+    double orc_pressure_force(void *h, int zone, const double *dir, const double *u, const double *uRec, double *gU, double *gRec)
+    {
+        return ((Oracle *)h)->pressureForce(zone, dir, u, uRec, gU, gRec);
     }
 
     // single Riemann flux evaluation (Gas.hpp:1434 dispatcher), 5 conservative variables
