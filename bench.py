@@ -290,7 +290,41 @@ def run_adjoint_cost(args):
                         "residual_vjp_over_primal": (t_vjp + t_vrvjp) / (t_rhs + t_vr)}
         if p == 1:
             out["adjoint_solve_p1"] = adjoint_solve(vr, ev, u, uRec, far, mesh, t_rhs + t_vr)
-    return {"workload": f"inviscid bump, {mesh.n_cell} tets, Roe, intOrder 4; VJP with respect to u and uRec (state)", **out}
+    out["tgv_viscous"] = tgv_vjp_cost(args)
+    return {"workload": f"inviscid bump, {mesh.n_cell} tets, Roe, intOrder 4; VJP with respect to u and uRec (state); "
+                        f"tgv_viscous: the TGV workload ({args.n}^3, p={args.p}, HLLE+ and viscous flux)", **out}
+
+
+def tgv_vjp_cost(args):
+    """CUDA-event times of EvaluateRHS and of its VJP (inviscid and viscous parts) on the TGV workload."""
+    import torch
+    from dndsr_b200 import mesh as M
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    mesh = M.tgv_mesh(args.n)
+    vr = VariationalReconstruction(mesh, dict(VR_SETTINGS, maxOrder=args.p)).construct()
+    ev = EulerEvaluator(vr, EULER_SETTINGS)
+    u, uRec, tmp = vr.BuildUDof(5), vr.BuildURec(5), vr.BuildURec(5)
+    ev.InitializeUDOF(u, 3)
+    vr.DoReconstructionIter(uRec, tmp, u, putIntoNew=False)
+    dt = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dt, u, 1.0)
+    rhs = torch.zeros_like(u)
+    w = torch.randn(u.shape, dtype=torch.float64, device="cuda")
+
+    def timed(fn, n=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    t_rhs = timed(lambda: ev.EvaluateRHS(rhs, u, uRec))
+    t_vjp = timed(lambda: ev.EvaluateRHSVJP(w, u, uRec))
+    return {"ms_rhs": t_rhs, "ms_rhs_vjp": t_vjp, "vjp_over_rhs": t_vjp / t_rhs}
 
 
 def adjoint_solve(vr, ev, u, uRec, far, mesh, ms_primal):

@@ -10,7 +10,8 @@
 // a scratch array and gathered per cell in a fixed order (no atomics on data),
 // and the transposed VR sweep gathers A^-1 B blocks of the neighbours through
 // the face-slot map.  The entropy-fix scale deltaLambdaCell is held fixed.
-// The viscous flux is not differentiated yet (ignoreVis is required).
+// The viscous flux derivative is added by adjoint_visc.cu (boundary zones without a viscous
+// flux only).
 #include "solver.cuh"
 #include "basis_eval.cuh"
 #include "bc.cuh"
@@ -477,6 +478,12 @@ int rhs_vjp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const r
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1, W = (R + 1) * NV;
     auto kf = k_rhs_vjp_face<DIM, P>;
     DNDSB_LAUNCH(kf, m.nFace, 64, st, m, g, vr, ev.s, w, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord);
+    if (!ev.s.ignoreVis)
+    {
+        int rc = rhs_vjp_visc(m, g, vr, ev, w, u, uRec, ev.adjBuf, st);
+        if (rc != ST_OK)
+            return rc;
+    }
     auto kg = k_adj_gather<W>;
     DNDSB_LAUNCH(kg, m.nCell, 128, st, m.nCell, m.nf, m.cell2face, ev.adjBuf, du, duRec);
     return ST_OK;
@@ -488,6 +495,12 @@ int rhs_jvp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const r
 {
     auto kf = k_rhs_jvp_face<DIM, P>;
     DNDSB_LAUNCH(kf, m.nFace, 64, st, m, g, vr, ev.s, du, duRec, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord);
+    if (!ev.s.ignoreVis)
+    {
+        int rc = rhs_jvp_visc(m, g, vr, ev, du, duRec, u, uRec, ev.adjBuf, st);
+        if (rc != ST_OK)
+            return rc;
+    }
     DNDSB_LAUNCH(k_flux_gather, m.nCell, 256, st, m.nCell, m.nf, m.cell2face, g.vol, ev.adjBuf, dRhs);
     return ST_OK;
 }
@@ -530,7 +543,7 @@ int vr_jvp_dp(const MeshD &m, const GeomD &g, const VRD &vr, const real *dRec, c
 int rhs_vjp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *w, const real *u, const real *uRec, real *du, real *duRec,
             cudaStream_t st)
 {
-    if (ev.s.nVars != NV || !ev.s.ignoreVis)
+    if (ev.s.nVars != NV || (!ev.s.ignoreVis && !vr.bnd.viscFree))
         return ST_UNSUPPORTED;
     if (ensure_adj(m, vr, ev) != ST_OK)
         return ST_CUDA;
@@ -550,7 +563,7 @@ int rhs_vjp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real
 int rhs_jvp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *du, const real *duRec, const real *u, const real *uRec,
             real *dRhs, cudaStream_t st)
 {
-    if (ev.s.nVars != NV || !ev.s.ignoreVis)
+    if (ev.s.nVars != NV || (!ev.s.ignoreVis && !vr.bnd.viscFree))
         return ST_UNSUPPORTED;
     if (ensure_adj(m, vr, ev) != ST_OK)
         return ST_CUDA;

@@ -440,6 +440,9 @@ extern "C"
         if (nZone > 0 && (upload(&b.type, ty.data(), nZone) || upload(&b.val, val.data(), (int64_t)nZone * 8)))
             return cuda_fail("dndsb_vr_set_boundary");
         b.nZone = nZone, b.gamma = gamma, b.Rgas = Rgas;
+        b.viscFree = true;
+        for (int32_t z : m->bndZoneHost)
+            b.viscFree = b.viscFree && (type[z] == BC_FAR || type[z] == BC_OUT || type[z] == BC_WALL_INVIS || type[z] == BC_SYM);
         v->bndNVars = nVars;
         return DNDSB_OK;
     }

@@ -729,19 +729,19 @@ DNDSB_HD bool riemann_flux(int rs, const T *UL, const T *UR, const T *ULm, const
 }
 
 // Gas.hpp:1677-1698 GradientCons2Prim_IdealGas; G and GP are [3][NV]
-template <int NV>
-DNDSB_HD void grad_cons2prim(const real *U, const real *G, real *GP, real gamma)
+template <int NV, typename T>
+DNDSB_HD void grad_cons2prim(const T *U, const T *G, T *GP, real gamma)
 {
-    real ir = 1.0 / U[0];
-    real v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
+    T ir = 1.0 / U[0];
+    T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
     for (int r = 0; r < 3; r++)
     {
-        const real *g = G + r * NV;
-        real *gp = GP + r * NV;
+        const T *g = G + r * NV;
+        T *gp = GP + r * NV;
         gp[0] = g[0];
         for (int j = 0; j < 3; j++)
             gp[1 + j] = (U[0] * g[1 + j] - g[0] * U[1 + j]) * ir * ir;
-        real s = g[1] * v[0] + g[2] * v[1] + g[3] * v[2] + gp[1] * U[1] + gp[2] * U[2] + gp[3] * U[3];
+        T s = g[1] * v[0] + g[2] * v[1] + g[3] * v[2] + gp[1] * U[1] + gp[2] * U[2] + gp[3] * U[3];
         gp[4] = (gamma - 1) * (g[4] - 0.5 * s);
         for (int j = 5; j < NV; j++)
             gp[j] = (g[j] - g[0] * U[j] * ir) * ir;
@@ -749,31 +749,31 @@ DNDSB_HD void grad_cons2prim(const real *U, const real *G, real *GP, real gamma)
 }
 
 // Gas.hpp:1594-1655 ViscousFlux_IdealGas without QCR; GP is the primitive gradient [3][NV]
-template <int NV>
-DNDSB_HD void viscous_flux(const real *U, const real *GP, const real *n, bool adiabatic, real gamma, real mu, real k, real Cp, real *Fv)
+template <int NV, typename T>
+DNDSB_HD void viscous_flux(const T *U, const T *GP, const real *n, bool adiabatic, real gamma, T mu, T k, real Cp, T *Fv)
 {
-    real ir = 1.0 / U[0];
-    real v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
-    real p = (gamma - 1) * (U[4] - U[0] * 0.5 * dot3(v, v));
-    real cT = gamma / ((gamma - 1) * Cp * U[0] * U[0]);
-    real gT[3];
+    T ir = 1.0 / U[0];
+    T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
+    T p = (gamma - 1) * (U[4] - U[0] * 0.5 * dot3s(v, v));
+    T cT = gamma / ((gamma - 1) * Cp * U[0] * U[0]);
+    T gT[3];
     for (int i = 0; i < 3; i++)
         gT[i] = cT * (U[0] * GP[i * NV + 4] - p * GP[i * NV + 0]);
     if (adiabatic)
     {
-        real gn = dot3(gT, n);
+        T gn = dot3v(gT, n);
         for (int i = 0; i < 3; i++)
             gT[i] -= gn * n[i];
     }
-    real tr = GP[0 * NV + 1] + GP[1 * NV + 2] + GP[2 * NV + 3];
-    real lm = -2.0 / 3.0 * mu * tr;
-    real e = 0;
+    T tr = GP[0 * NV + 1] + GP[1 * NV + 2] + GP[2 * NV + 3];
+    T lm = -2.0 / 3.0 * mu * tr;
+    T e = 0;
     for (int i = 0; i < 3; i++)
     {
-        real fi = 0, si = 0;
+        T fi = 0, si = 0;
         for (int j = 0; j < 3; j++)
         {
-            real s = (GP[i * NV + 1 + j] + GP[j * NV + 1 + i]) * mu + (i == j ? lm : 0.0);
+            T s = (GP[i * NV + 1 + j] + GP[j * NV + 1 + i]) * mu + (i == j ? lm : T(0.0));
             fi += s * n[j];
             si += s * v[j];
         }
@@ -785,14 +785,15 @@ DNDSB_HD void viscous_flux(const real *U, const real *GP, const real *n, bool ad
 }
 
 // EulerEvaluator.hpp:751-789 muEff: 0 constant, 1 Sutherland, 2 proportional to density
-DNDSB_HD real mu_eff(int model, real muGas, real TRef, real CSuth, real rho, real T)
+template <typename T>
+DNDSB_HD T mu_eff(int model, real muGas, real TRef, real CSuth, T rho, T Temp)
 {
     if (model == 0)
-        return muGas;
+        return T(muGas);
     if (model == 1)
     {
-        real TRel = T / TRef;
-        return muGas * TRel * sqrt(TRel) * (TRef + CSuth) / (T + CSuth);
+        T TRel = Temp / TRef;
+        return muGas * TRel * sqrt(TRel) * (TRef + CSuth) / (Temp + CSuth);
     }
     return muGas * rho;
 }

@@ -82,6 +82,7 @@ struct BoundaryD
     int32_t *type = nullptr; // [nZone], 0 for zones without a boundary condition
     real *val = nullptr;     // [nZone][8]: far-field / inflow state, or wall temperature
     real gamma = 1.4, Rgas = 1;
+    bool viscFree = true;    // host: every used boundary zone carries no viscous flux (far-field, outflow, slip wall, symmetry)
 };
 
 struct VRSettingsD
@@ -167,6 +168,12 @@ int update_sgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const 
 int lusgs_matvec(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jdiag,
                  real *AuInc, cudaStream_t st);
 int init_field(const MeshD &m, const GeomD &g, const EvalD &ev, int kind, real chi, real *u, cudaStream_t st);
+// viscous part of the residual derivatives (adjoint_visc.cu): added to the inviscid face
+// cotangents [nFace][2][(R+1) nv] / face flux derivatives [nFace][nv] before their gathers
+int rhs_vjp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec, real *faceAdj,
+                 cudaStream_t st);
+int rhs_jvp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *du, const real *duRec, const real *u,
+                 const real *uRec, real *ffd, cudaStream_t st);
 // adjoint building blocks (adjoint_ops.cu)
 int lusgs_matvec_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *y, const real *jdiag, real *ATy,
                    cudaStream_t st);

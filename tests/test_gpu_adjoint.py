@@ -7,6 +7,8 @@
   (JVP) and reverse (VJP) kernels, at 1e-12 relative;
 * torch.autograd through two VR sweeps and the RHS, against finite differences
   of the same composition on the oracle.
+Inviscid cases on the bump channel and the vortex meshes; Navier-Stokes cases (constant
+viscosity and Sutherland's law) on the periodic hex box.
 The entropy-fix scale is held fixed (the oracle's EvaluateDt is called once at the
 base state).  Riemann solvers with kinks at the tested states (Roe_M1's |u| fix, HLLC's
 wave-speed branches) are left to the dual-consistency check.
@@ -22,7 +24,8 @@ from tests.util import VR_HQM_PY, oracle_for
 pytestmark = pytest.mark.gpu
 
 CASES = [("bump-tet-p2-Roe", "bump", 2, "Roe"), ("bump-tet-p1-HLLEP", "bump", 1, "HLLEP"), ("iv-tri-p2-HLLEP", "iv", 2, "HLLEP"),
-         ("iv-quad-p3-Roe", "ivq", 3, "Roe")]
+         ("iv-quad-p3-Roe", "ivq", 3, "Roe"), ("tgv-hex-p2-HLLEP-viscous", "tgv", 2, "HLLEP"),
+         ("tgv-hex-p1-Roe-sutherland", "tgvs", 1, "Roe")]
 
 
 def _setup(case, p, rs):
@@ -34,6 +37,15 @@ def _setup(case, p, rs):
         ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType=rs, muGas=0.0, ignoreVis=True))
         ev.SetBC(types, vals)
         u0, uRec0 = perturbed_state(m, far, R=o.R)
+    elif case in ("tgv", "tgvs"):
+        # Navier-Stokes on the periodic hex box: constant viscosity, or Sutherland's law
+        mu, model = (0.02, 0) if case == "tgv" else (0.05, 1)
+        m = M.tgv_mesh(4)
+        o = oracle_for(m, p, rs, mu=mu, muModel=model, ignoreVis=0)
+        vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p)).construct()
+        ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType=rs, muGas=mu, muModel=model))
+        u0 = o.init_field(3)
+        uRec0 = np.random.default_rng(3).normal(size=(m.n_cell, o.R, 5)) * 0.01 * np.abs(u0).mean(0)
     else:
         m = M.iv_mesh(8) if case == "iv" else M.periodic_quad_2d(7, jitter=0.1)
         o = oracle_for(m, p, rs, mu=0.0, ignoreVis=1)
@@ -108,13 +120,16 @@ def test_autograd_through_sweeps_and_rhs():
         assert abs(adj - fd) < 1e-6 * abs(fd)
 
 
-def test_viscous_vjp_is_reported_unsupported():
+def test_viscous_wall_vjp_is_reported_unsupported():
     from dndsr_b200.capi import DndsbError
     from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
-    m = M.tgv_mesh(3)
-    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1)).construct()
+    m = M.bump_channel_tet(4, 2, 2)
+    o, far, types, vals, w = bump_oracle(m, 1, "Roe", 0.0, 1)
+    types[M.BUMP_ZONES["bump"]] = 2  # BCWall: a viscous flux on boundary faces, not differentiated
+    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1)).construct(w)
     ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType="Roe", muGas=1e-3, muModel=0))
+    ev.SetBC(types, vals)
     u, uRec = vr.BuildUDof(5), vr.BuildURec(5)
-    ev.InitializeUDOF(u, 3)
+    u[:] = torch.tensor(far, device="cuda")
     with pytest.raises(DndsbError):
         ev.EvaluateRHSVJP(torch.ones_like(u), u, uRec)
