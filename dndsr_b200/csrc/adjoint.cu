@@ -40,12 +40,15 @@ DNDSB_D void recon_value(const real *T, const real *u, const real *rec, real *U)
 // cotangent of one interior or boundary face: faceAdj[f][side][(R+1)][NV], entry 0 = d/du, 1+j = d/duRec_j
 template <int DIM, int P>
 DNDSB_GLOBAL void k_rhs_vjp_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ w, const real *__restrict__ u,
-                                 const real *__restrict__ uRec, const real *__restrict__ dLamCell, real *__restrict__ faceAdj, int *err)
+                                 const real *__restrict__ uRec, const real *__restrict__ dLamCell, real *__restrict__ faceAdj, int *err,
+                                 int boundaryOnly)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1, W = (R + 1) * NV;
     const real gamma = s.gamma;
-    DNDSB_KERNEL_LOOP(f, m.nFace)
+    // boundaryOnly: the boundary faces of the list m.bndFace (the reverse-mode Roe kernel writes the others)
+    DNDSB_KERNEL_LOOP(ii, boundaryOnly ? m.nBndFace : m.nFace)
     {
+        const int64_t f = boundaryOnly ? (int64_t)m.bndFace[ii] : ii;
         int64_t c0 = m.face2cell[f * 2], c1 = m.face2cell[f * 2 + 1];
         bool bnd = c1 < 0;
         int zone = m.faceZone[f];
@@ -477,7 +480,14 @@ int rhs_vjp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const r
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1, W = (R + 1) * NV;
     auto kf = k_rhs_vjp_face<DIM, P>;
-    DNDSB_LAUNCH(kf, m.nFace, 64, st, m, g, vr, ev.s, w, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord);
+    const int roe = roe_scheme_of(ev.s.rsType) >= 0;
+    DNDSB_LAUNCH(kf, roe ? m.nBndFace : m.nFace, 64, st, m, g, vr, ev.s, w, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord, roe);
+    if (roe)
+    {
+        int rc = rhs_vjp_roe_interior(m, g, vr, ev, w, u, uRec, ev.adjBuf, st);
+        if (rc != ST_OK)
+            return rc;
+    }
     if (!ev.s.ignoreVis)
     {
         int rc = rhs_vjp_visc(m, g, vr, ev, w, u, uRec, ev.adjBuf, st);

@@ -12,42 +12,12 @@
 // One thread per cell (per boundary cell for the objective); fixed loop orders, no atomics on data.
 #include "solver.cuh"
 #include "basis_eval.cuh"
+#include "flux_t.cuh"
 
 namespace dndsb
 {
 namespace
 {
-// out = (J(U; n) - lambda I)^T y: the reverse sweep of flux_jac_du's statements
-template <int NV>
-DNDSB_D void flux_jac_du_t(const real *U, const real *n, const real *y, real lam, real gamma, real *out)
-{
-    real ir = 1.0 / U[0];
-    real v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
-    real p, a2, H;
-    gas_thermal(U[4], U[0], dot3(v, v), gamma, p, a2, H);
-    real vn = dot3(v, n);
-    for (int j = 0; j < NV; j++)
-        out[j] = -lam * y[j] + (j >= 1 ? vn * y[j] : 0.0);
-    real bvn = 0, bp = 0;
-    for (int d = 0; d < 3; d++)
-    {
-        out[1 + d] += n[d] * y[0];
-        bvn += U[1 + d] * y[1 + d];
-        bp += n[d] * y[1 + d];
-    }
-    bp += vn * y[4];
-    bvn += (U[4] + p) * y[4];
-    for (int j = 5; j < NV; j++)
-        bvn += U[j] * y[j];
-    out[4] += (gamma - 1) * bp;
-    for (int d = 0; d < 3; d++)
-    {
-        real bv = n[d] * bvn - 0.5 * (gamma - 1) * U[1 + d] * bp;
-        out[1 + d] += -0.5 * (gamma - 1) * v[d] * bp + ir * bv;
-        out[0] += -U[1 + d] * ir * ir * bv;
-    }
-}
-
 // contribution of neighbour slot k (neighbour c, possibly q itself across a periodic face) to (A^T y)_q:
 // w_cq (J(u_q; n_cq) - lambda)^T y_c, with n_cq the normal out of c and w_cq = alpha A_f / (2 V_c)
 template <int NV>

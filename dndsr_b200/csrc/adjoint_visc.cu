@@ -4,9 +4,10 @@
 //   Fv(U_M, grad U_M),  U_M = (U_L + U_R) / 2,
 //   grad U_M = (grad U_L + grad U_R) / 2 + (U_R - U_L) (x) n / d_GRP,
 // with grad U = D1 phi . uRec of each side and the flux of Gas.hpp:1594-1655 on the primitive
-// gradient (Gas.hpp:1677-1698).  Fv depends on the 20 numbers (U_M, grad U_M); one Dual<20> pass
-// per Gauss point gives their cotangents, which the chain above carries to (u, uRec) of both
-// cells (VJP), and a Dual<1> pass gives the directional derivative (JVP).  Both add to the
+// gradient (Gas.hpp:1677-1698).  Fv depends on the 20 numbers (U_M, grad U_M).  Their cotangents
+// (VJP): one Dual<5> pass for U_M at fixed gradient, and for grad U_M the transposes of the two
+// maps that are linear in it (conservative -> primitive gradient, primitive gradient -> flux);
+// the chain above carries them to (u, uRec) of both cells.  The JVP is one Dual<1> pass.  Both add to the
 // inviscid face arrays before their per-cell gathers.  Boundary faces carry no viscous flux in
 // the zone types allowed here (far-field, outflow, slip wall, symmetry).
 #include "solver.cuh"
@@ -17,7 +18,7 @@ namespace dndsb
 namespace
 {
 constexpr int NV = 5;
-using D20 = Dual<20>;
+using D5 = Dual<5>;
 using D1 = Dual<1>;
 
 // the 5-variable branch of point_viscous_flux (sa.cuh), on any scalar type
@@ -30,6 +31,60 @@ DNDSB_D void visc_flux_t(const EulerSettingsD &s, const T *UM, const T *GP, cons
     T Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
     T mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
     viscous_flux<NV>(UM, GP, n, false, gamma, mu, cp * mu / s.prGas, cp, Fv);
+}
+
+// GMbar = (d Fv / d grad U_M)^T Fvbar at fixed U_M: Fv is linear in the primitive gradient GP
+// (viscous_flux) and GP is linear in the conservative gradient (grad_cons2prim), so the cotangent
+// is the transpose of those two linear maps, statement by statement in reverse
+DNDSB_D void visc_grad_transpose(const EulerSettingsD &s, const real *UM, const real *n, const real *Fvbar, real *GMbar)
+{
+    const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
+    real pM, a2M, HM;
+    gas_thermal(UM[4], UM[0], (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) / (UM[0] * UM[0]), gamma, pM, a2M, HM);
+    real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
+    real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
+    real k = cp * mu / s.prGas;
+    real ir = 1.0 / UM[0];
+    real v[3] = {UM[1] * ir, UM[2] * ir, UM[3] * ir};
+    real p = (gamma - 1) * (UM[4] - UM[0] * 0.5 * dot3(v, v));
+    real cT = gamma / ((gamma - 1) * cp * UM[0] * UM[0]);
+    // viscous_flux: Fv[1+i] = sum_j s_ij n_j, Fv[4] = sum_i (sum_j s_ij v_j + k gT_i) n_i
+    real GPb[3 * NV];
+    for (int i = 0; i < 3 * NV; i++)
+        GPb[i] = 0;
+    real lmb = 0;
+    for (int i = 0; i < 3; i++)
+    {
+        real gTb = Fvbar[4] * k * n[i];
+        GPb[i * NV + 4] += cT * UM[0] * gTb;
+        GPb[i * NV + 0] += -cT * p * gTb;
+        for (int j = 0; j < 3; j++)
+        {
+            real sb = Fvbar[1 + i] * n[j] + Fvbar[4] * n[i] * v[j];
+            GPb[i * NV + 1 + j] += mu * sb;
+            GPb[j * NV + 1 + i] += mu * sb;
+            if (i == j)
+                lmb += sb;
+        }
+    }
+    real trb = -2.0 / 3.0 * mu * lmb;
+    for (int i = 0; i < 3; i++)
+        GPb[i * NV + 1 + i] += trb;
+    // grad_cons2prim per direction r
+    for (int r = 0; r < 3; r++)
+    {
+        const real *gpb = GPb + r * NV;
+        real *gb = GMbar + r * NV;
+        real sbar = -0.5 * (gamma - 1) * gpb[4];
+        gb[4] = (gamma - 1) * gpb[4];
+        gb[0] = gpb[0];
+        for (int j = 0; j < 3; j++)
+        {
+            real gpj = gpb[1 + j] + sbar * UM[1 + j];
+            gb[1 + j] = sbar * v[j] + UM[0] * ir * ir * gpj;
+            gb[0] += -UM[1 + j] * ir * ir * gpj;
+        }
+    }
 }
 
 // geometry of one interior face shared by its Gauss points
@@ -108,24 +163,33 @@ DNDSB_GLOBAL void k_rhs_vjp_visc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
             real T0[(DIM + 1) * NDOF], T1[(DIM + 1) * NDOF], UL[NV], UR[NV], GL[3 * NV], GR[3 * NV], iD;
             const real *n;
             visc_point<DIM, P>(m, g, vr, F, f, q, u, uRec, T0, T1, UL, UR, GL, GR, iD, n);
-            D20 UM[NV], GM[3 * NV], GP[3 * NV], Fv[NV];
+            // the face flux is -(F - Fv) |J| w: the cotangent of Fv is +|J| w gbar.  bar[0..4]: the
+            // cotangent of U_M (one Dual<5> pass at fixed grad U_M); bar[5..19]: of grad U_M
+            // (transposed linear maps at fixed U_M)
+            real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
+            real UMr[NV], GMr[3 * NV], Fvbar[NV], bar[20];
             for (int v = 0; v < NV; v++)
-                UM[v] = D20::var(0.5 * (UL[v] + UR[v]), v);
+                UMr[v] = 0.5 * (UL[v] + UR[v]), Fvbar[v] = JW * gbar[v];
             for (int d = 0; d < 3; d++)
                 for (int v = 0; v < NV; v++)
-                    GM[d * NV + v] = D20::var((GR[d * NV + v] + GL[d * NV + v]) * 0.5 + iD * (n[d] * (UR[v] - UL[v])), NV + d * NV + v);
-            grad_cons2prim<NV>(UM, GM, GP, gamma);
-            visc_flux_t(s, UM, GP, n, Fv);
-            // the face flux is -(F - Fv) |J| w: the cotangent of Fv is +|J| w gbar
-            real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
-            real bar[20];
-            for (int i = 0; i < 20; i++)
+                    GMr[d * NV + v] = (GR[d * NV + v] + GL[d * NV + v]) * 0.5 + iD * (n[d] * (UR[v] - UL[v]));
             {
-                real a = 0;
-                for (int k = 0; k < NV; k++)
-                    a += Fv[k].d[i] * gbar[k];
-                bar[i] = a * JW;
+                D5 UM[NV], GM[3 * NV], GP[3 * NV], Fv[NV];
+                for (int v = 0; v < NV; v++)
+                    UM[v] = D5::var(UMr[v], v);
+                for (int i = 0; i < 3 * NV; i++)
+                    GM[i] = D5(GMr[i]);
+                grad_cons2prim<NV>(UM, GM, GP, gamma);
+                visc_flux_t(s, UM, GP, n, Fv);
+                for (int i = 0; i < NV; i++)
+                {
+                    real a = 0;
+                    for (int k = 0; k < NV; k++)
+                        a += Fv[k].d[i] * Fvbar[k];
+                    bar[i] = a;
+                }
             }
+            visc_grad_transpose(s, UMr, n, Fvbar, bar + NV);
             for (int v = 0; v < NV; v++)
             {
                 real nG = 0;

@@ -174,6 +174,10 @@ int rhs_vjp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev,
                  cudaStream_t st);
 int rhs_jvp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *du, const real *duRec, const real *u,
                  const real *uRec, real *ffd, cudaStream_t st);
+// reverse-mode interior-face derivative of the Roe-family fluxes (adjoint_roe.cu)
+int roe_scheme_of(int rsType);
+int rhs_vjp_roe_interior(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec,
+                         real *faceAdj, cudaStream_t st);
 // adjoint building blocks (adjoint_ops.cu)
 int lusgs_matvec_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *y, const real *jdiag, real *ATy,
                    cudaStream_t st);
