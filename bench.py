@@ -143,8 +143,8 @@ def cpu_baseline_oracle(n_sample, p, seconds, threads=None):
 
 def run_steady(args):
     """Steady transonic bump (the mixed-precision configuration): FP64 vs FP32 linear solve inside the FP64
-    defect correction, the same number of pseudo-iterations each; wall time per iteration, their ratio,
-    the residual drop reached and the state difference."""
+    defect correction, the same number of pseudo-iterations each (after a two-iteration warm-up per
+    precision); wall time per iteration, their ratio, the residual drop reached and the state difference."""
     import torch
     from dndsr_b200 import implicit as I
     from dndsr_b200 import mesh as M
@@ -164,6 +164,10 @@ def run_steady(args):
     out, comp = {}, {}
     for prec in ("fp64", "fp32"):
         u = vr.BuildUDof(5)
+        # warm-up (linear-solver workspace, CUDA graph capture) on a throw-away state
+        u[:] = torch.tensor(far, device="cuda")
+        I.ImplicitSolver(vr, ev, I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=2, nTimeStepInternalMin=2,
+                                                CFL=200.0, gmresCode=1, nGmresSpace=30, linear_precision=prec)).run(u)
         u[:] = torch.tensor(far, device="cuda")
         cfg = I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=args.steady_iters, nTimeStepInternalMin=args.steady_iters,
                              CFL=200.0, gmresCode=1, nGmresSpace=30, nGmresIter=1, sgsIter=0, rhsThresholdInternal=1e-10,
@@ -239,6 +243,69 @@ def run_dual_time(args):
             "inner_iterations_fp64": a[2], "inner_iterations_mixed": b[2], "iterations_per_stage_fp64": a[4],
             "worst_final_drop_fp64": a[3], "worst_final_drop_mixed": b[3],
             "state_rel_diff": float((a[0] - b[0]).abs().max() / a[0].abs().max())}
+
+
+def run_sa_plate(args):
+    """The SA flat-plate workload at full size: Re_L 5e6, Mach 0.2, nuTilde_inf = 3 nu, stretched hexahedra
+    (first cell 5e-6, growth 1.1), VR degree 1, Roe, 6 variables (NS_SA with the IDDES length scale and the
+    analytic wall distance).  Reported: VR sweep + EvaluateRHS throughput (CUDA events) and BDF1 pseudo
+    iterations (CFL 50, GMRES(30) with one SGS pair) with the FP64 and the FP32 linear solve, each after a
+    two-iteration warm-up."""
+    import torch
+    from dndsr_b200 import implicit as I
+    from dndsr_b200 import mesh as M
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    nx, ny, nz = args.sa_mesh
+    mesh = M.flat_plate_hex(nx, ny, nz, y1=5e-6, growth=1.1)
+    far5 = M.freestream(0.2)
+    mu = np.linalg.norm(far5[1:4]) / far5[0] / 5e6
+    far = np.concatenate([far5, [3.0 * far5[0]]])
+    types, vals = np.zeros(6, np.int32), np.zeros((6, 6))
+    w = np.ones((6, 4))
+    for z, tp in M.PLATE_BC_TYPES.items():
+        types[z], vals[z], w[z] = tp, far, (1, 0, 0, 0)
+    vr = VariationalReconstruction(mesh, dict(maxOrder=1, intOrder=3, dirWeightScheme="HQM_OPT", geomWeightScheme="HQM_SD",
+                                              geomWeightBias=1.0)).construct(w)
+    ev = EulerEvaluator(vr, dict(nVars=6, riemannSolverType="Roe", muGas=mu, muModel=0, prGas=0.72))
+    ev.SetBC(types, vals)
+    ev.SetWallDistance(M.plate_wall_distance(vr.get("cellPP").reshape(mesh.n_cell, -1, 3)))
+    u = vr.BuildUDof(6)
+    u[:] = torch.tensor(far, device="cuda")
+    uRec, tmp, rhs = vr.BuildURec(6), vr.BuildURec(6), torch.zeros_like(u)
+    dt = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dt, u, 1.0)
+    vr.DoReconstructionIter(uRec, tmp, u, putIntoNew=False)
+    ev.EvaluateRHS(rhs, u, uRec)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(5):
+        vr.DoReconstructionIter(uRec, tmp, u, putIntoNew=False)
+        ev.EvaluateRHS(rhs, u, uRec)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / 5
+    out = {"workload": f"SA flat plate, {mesh.n_cell} hex ({nx}x{ny}x{nz}), Re_L 5e6, Mach 0.2, VR degree 1, Roe, 6 variables",
+           "ms_vr_sweep_plus_rhs": ms, "mcell_rhs_per_s": mesh.n_cell / ms / 1e3}
+    res = {}
+    for prec in ("fp64", "fp32"):
+        u[:] = torch.tensor(far, device="cuda")
+        I.ImplicitSolver(vr, ev, I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=2, nTimeStepInternalMin=2,
+                                                CFL=50.0, gmresCode=1, nGmresSpace=30, linear_precision=prec)).run(u)
+        u[:] = torch.tensor(far, device="cuda")
+        cfg = I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=args.sa_iters, nTimeStepInternalMin=args.sa_iters,
+                             CFL=50.0, gmresCode=1, nGmresSpace=30, nGmresIter=1, sgsIter=0, rhsThresholdInternal=1e-9, linear_precision=prec)
+        solver = I.ImplicitSolver(vr, ev, cfg)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solver.run(u)
+        torch.cuda.synchronize()
+        res[prec] = (u.clone(), time.perf_counter() - t0, len(cfg.res_history), cfg.res_history[-1][2])
+    a64, a32 = res["fp64"], res["fp32"]
+    out.update({"iterations": a64[2], "fp64_ms_per_iter": 1e3 * a64[1] / a64[2], "mixed_ms_per_iter": 1e3 * a32[1] / a32[2],
+                "mixed_over_fp64_time": a32[1] / a64[1], "residual_drop_fp64": a64[3], "residual_drop_mixed": a32[3],
+                "state_rel_diff": float((a64[0] - a32[0]).abs().max() / a64[0].abs().max())})
+    return out
 
 
 def run_adjoint_cost(args):
@@ -497,6 +564,8 @@ def run_ours(args, rank, world, local_rank):
         line["time_to_1e-10"] = run_dual_time(args)
         line["steady"] = run_steady(args)
         line["adjoint_cost"] = run_adjoint_cost(args)
+        if not args.no_sa:
+            line["sa_plate"] = run_sa_plate(args)
     if world == 1 and not args.no_cpu_baseline:
         v, steps, el, cells = cpu_baseline_oracle(args.sample_n, p, args.sample_seconds, n_cores())
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": n_cores(), "kind": "port",
@@ -520,6 +589,9 @@ def main():
     ap.add_argument("--steady-mesh", type=int, nargs=3, default=(160, 80, 26))
     ap.add_argument("--steady-iters", type=int, default=100)
     ap.add_argument("--adjoint-mesh", type=int, nargs=3, default=(80, 40, 13))
+    ap.add_argument("--no-sa", action="store_true")
+    ap.add_argument("--sa-mesh", type=int, nargs=3, default=(300, 100, 100))
+    ap.add_argument("--sa-iters", type=int, default=30)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

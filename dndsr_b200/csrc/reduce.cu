@@ -327,55 +327,51 @@ DNDSB_GLOBAL void k_kdiff_norm(int64_t n, const T *__restrict__ x, const T *__re
         partial[blockIdx.x] = sh[0][0];
 }
 
-// out[col] = sum over blocks (fixed tree), optionally its square root
+// out[col] = sum over blocks, optionally its square root: one warp per column (columns strided over
+// the warps), each lane summing a fixed stride of the partials, then a fixed xor-shuffle tree
 DNDSB_GLOBAL void k_kfinal(int nb, int ncol, const real *__restrict__ partial, real *out, int takeSqrt)
 {
-    __shared__ real sh[kRedBlock];
-    for (int col = 0; col < ncol; col++)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int col = wid; col < ncol; col += nw)
     {
         real a = 0;
-        for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        for (int i = lane; i < nb; i += 32)
             a += partial[i * ncol + col];
-        sh[threadIdx.x] = a;
-        __syncthreads();
-        for (int st = blockDim.x / 2; st > 0; st >>= 1)
-        {
-            if (threadIdx.x < st)
-                sh[threadIdx.x] += sh[threadIdx.x + st];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0)
-            out[col] = takeSqrt ? sqrt(sh[0]) : sh[0];
-        __syncthreads();
+        a = warp_sum(a);
+        if (lane == 0)
+            out[col] = takeSqrt ? sqrt(a) : a;
     }
 }
+
+// block size of the final pass: one warp per column, at most 32 warps
+inline int kfinal_threads(int ncol) { return 32 * (ncol < 1 ? 1 : ncol > 32 ? 32 : ncol); }
 
 template <typename T, int NV>
 void kmdot(int64_t n, int64_t ld, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st)
 {
     k_kmdot<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, (const T *)w, s2, red);
-    k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, ncol, red, out, 0);
+    k_kfinal<<<1, kfinal_threads(ncol), 0, st>>>(kRedBlocks, ncol, red, out, 0);
 }
 
 template <typename T, int NV>
 void kmaxpy(int64_t n, int64_t ld, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm, cudaStream_t st)
 {
     k_kmaxpy_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, h, (T *)w, s2, red);
-    k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+    k_kfinal<<<1, 32, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
 }
 
 template <typename T, int NV>
 void knorm(int64_t n, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st)
 {
     k_knorm2<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, s2, red);
-    k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+    k_kfinal<<<1, 32, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
 }
 
 template <typename T, int NV>
 void kdiff(int64_t n, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st)
 {
     k_kdiff_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, (const T *)y, s2, red);
-    k_kfinal<<<1, kRedBlock, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+    k_kfinal<<<1, 32, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
 }
 
 #define DNDSB_KDISPATCH(FN, ...)                      \
