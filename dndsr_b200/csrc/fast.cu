@@ -15,6 +15,7 @@
 // in shared memory face by face.
 #include "solver.cuh"
 #include "basis_eval.cuh"
+#include "sa.cuh"
 
 namespace dndsb
 {
@@ -188,7 +189,10 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
         real UL[NV], UR[NV], G[3 * NV];
         recon_point<DIM, P, NV, false>(sCell + fl * CS, p0, UL, G);
         recon_point<DIM, P, NV, true>(sCell + (32 + fl) * CS, p1, UR, G);
-        real Fv[5] = {0, 0, 0, 0, 0};
+        real Fv[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+            Fv[v] = 0;
         if (!s.ignoreVis)
         {
             real distGRP = fd->gbase;
@@ -204,20 +208,27 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
                 for (int v = 0; v < NV; v++)
                     G[d * NV + v] = G[d * NV + v] * 0.5 + iD * (n[d] * (UR[v] - UL[v]));
             grad_cons2prim<NV>(UM, G, GP, gamma);
-            real irho = 1.0 / UM[0];
-            real pM = (gamma - 1) * (UM[4] - 0.5 * (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) * irho);
-            real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
-            real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
-            viscous_flux<NV>(UM, GP, n, false, gamma, mu, cp * mu / s.prGas, cp, Fv);
+            if (NV == 5)
+            {
+                real irho = 1.0 / UM[0];
+                real pM = (gamma - 1) * (UM[4] - 0.5 * (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) * irho);
+                real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
+                real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
+                viscous_flux<NV>(UM, GP, n, false, gamma, mu, cp * mu / s.prGas, cp, Fv);
+            }
+            else // SA: eddy viscosity in the momentum/energy fluxes and the nuTilde diffusion flux
+                point_viscous_flux<NV>(s, UM, GP, n, false, Fv);
         }
-        real F[5], l0, l1, l4;
+        real F[NV], l0, l1, l4;
         bool ok = riemann_flux_pre(s.rsType, UL, UR, fd->r, n, gamma, fd->dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+        if (NV == 6)
+            F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
 #pragma unroll
-        for (int v = 0; v < 5; v++)
+        for (int v = 0; v < NV; v++)
             out[v] = -(F[v] - Fv[v]) * JW;
         bool fin = true;
 #pragma unroll
-        for (int v = 0; v < 5; v++)
+        for (int v = 0; v < NV; v++)
             fin = fin && isfinite(out[v]);
         if (!ok || !fin)
             atomicOr(err, !ok ? (int)DE_NONPHYSICAL : (int)DE_NONFINITE);
@@ -406,8 +417,19 @@ int fast_geometry(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, cuda
 // returns ST_UNSUPPORTED when no tuned instantiation exists (the caller then uses the generic kernel)
 int rhs_face_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st)
 {
-    if (!ev.facePt || ev.s.nVars != 5)
+    if (!ev.facePt || (ev.s.nVars != 5 && ev.s.nVars != 6))
         return ST_UNSUPPORTED;
+    if (ev.s.nVars == 6)
+    {
+        // the SA model: hexahedral meshes at degree 1 (quadrilateral faces, 4 or 9 points)
+        if (m.dim != 3 || vr.P != 1)
+            return ST_UNSUPPORTED;
+        if (g.nGf == 4)
+            return launch_rhs_fast<3, 1, 6, 4>(m, g, vr, ev, u, uRec, ff, st);
+        if (g.nGf == 9)
+            return launch_rhs_fast<3, 1, 6, 9>(m, g, vr, ev, u, uRec, ff, st);
+        return ST_UNSUPPORTED;
+    }
     if (m.dim == 2)
     {
         if (vr.P == 1)

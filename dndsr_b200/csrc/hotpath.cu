@@ -573,7 +573,7 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
     int nv = ev.s.nVars;
     if (nv != 5 && nv != 6)
         return ST_UNSUPPORTED;
-    int frc = nv == 5 ? rhs_face_fast(m, g, vr, ev, u, uRec, ff, st) : ST_UNSUPPORTED;
+    int frc = rhs_face_fast(m, g, vr, ev, u, uRec, ff, st);
     if (frc == ST_CUDA)
         return ST_CUDA;
     if (frc != ST_OK)

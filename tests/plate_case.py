@@ -27,12 +27,12 @@ def plate_bc(far):
     return types, vals, w
 
 
-def plate_oracle(m, p, rs="Roe"):
+def plate_oracle(m, p, rs="Roe", intOrder=5):
     far, mu = plate_state()
     types, vals, w = plate_bc(far)
     es = dict(nVars=6, rsType=oracle.RS[rs], rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=mu, prGas=0.72, TRef=273.15,
               CSutherland=110.4, muModel=0, ignoreVis=0)
-    o = oracle.Oracle(m, dict(VR_HQM, maxOrder=p), es)
+    o = oracle.Oracle(m, dict(VR_HQM, maxOrder=p, intOrder=intOrder), es)
     assert o.construct(w) == 0
     o.set_bc(types, vals)
     o.set_wall_distance(M.plate_wall_distance(o.get("cellPP").reshape(m.n_cell, -1, 3)))

@@ -18,20 +18,21 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def _setup(p, rs):
+def _setup(p, rs, intOrder=5):
     from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
     m = M.renumber_by_color(M.flat_plate_hex(12, 10, 3, y1=1e-3, growth=1.3))
-    o, far, mu, types, vals, w = plate_oracle(m, p, rs)
-    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p)).construct(w)
+    o, far, mu, types, vals, w = plate_oracle(m, p, rs, intOrder)
+    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p, intOrder=intOrder)).construct(w)
     ev = EulerEvaluator(vr, dict(nVars=6, riemannSolverType=rs, muGas=mu, muModel=0, prGas=0.72))
     ev.SetBC(types, vals)
     ev.SetWallDistance(M.plate_wall_distance(vr.get("cellPP").reshape(m.n_cell, -1, 3)))
     return m, o, vr, ev, far
 
 
-@pytest.mark.parametrize("p,rs", [(1, "Roe"), (2, "HLLEP")])
-def test_sa_operators(p, rs):
-    m, o, vr, ev, far = _setup(p, rs)
+# p=1 runs the tuned face kernel (4 and 9 points per quadrilateral face); p=2 the generic one
+@pytest.mark.parametrize("p,rs,io", [(1, "Roe", 5), (1, "Roe", 3), (2, "HLLEP", 5)])
+def test_sa_operators(p, rs, io):
+    m, o, vr, ev, far = _setup(p, rs, io)
     assert relerr(vr.get("cellHMax"), o.get("cellHMax")) < TOL
     u0, uRec0 = plate_perturbed(m, far, R=o.R)
     u, uRec = torch.tensor(u0, device="cuda"), torch.tensor(uRec0, device="cuda")
