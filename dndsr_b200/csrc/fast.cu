@@ -448,8 +448,22 @@ int rhs_face_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev
 int vr_iter_fast(const MeshD &m, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc, int uRecIsZero,
                  int useFP32, cudaStream_t st)
 {
-    if (nv != 5 || !vr.sweepCoef)
+    if ((nv != 5 && nv != 6) || !vr.sweepCoef)
         return ST_UNSUPPORTED;
+    if (nv == 6)
+    {
+        // the SA model at degree 1 in 3-D (R = 3)
+        if (vr.R != 3)
+            return ST_UNSUPPORTED;
+        unsigned nb6 = (unsigned)((m.nCell + 31) / 32);
+        if (useFP32)
+            k_vr_jacobi_fast<3, 6, float><<<nb6, 32 * 3, 0, st>>>(m.nCell, m.nf, m.cellNbr, vr.sweepCoef32, uRec, uRecNew, u, vr.s.jacobiRelax,
+                                                                 recordInc, uRecIsZero);
+        else
+            k_vr_jacobi_fast<3, 6, real><<<nb6, 32 * 3, 0, st>>>(m.nCell, m.nf, m.cellNbr, vr.sweepCoef, uRec, uRecNew, u, vr.s.jacobiRelax,
+                                                                recordInc, uRecIsZero);
+        return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+    }
     unsigned nb = (unsigned)((m.nCell + 31) / 32);
     real relax = vr.s.jacobiRelax;
 #define DNDSB_VRF(RR)                                                                                                                       \
