@@ -91,9 +91,11 @@ DNDSB_D void recon_point(const real *cell, const real *p, real *U, real *G)
     }
 }
 
-// resident blocks per SM the register budget is sized for (about 18 warps per SM)
+// resident blocks per SM the register budget is sized for (about 27 warps per SM: at 9 points per
+// face, 3 blocks of 288 threads with 72 registers each and some spilling beat 2 blocks with 96 by
+// 18 % on the TGV workload at 64^3)
 #ifndef DNDSB_RHS_WARPS_PER_SM
-#define DNDSB_RHS_WARPS_PER_SM 18
+#define DNDSB_RHS_WARPS_PER_SM 27
 #endif
 template <int NG>
 constexpr int min_blocks() { return (DNDSB_RHS_WARPS_PER_SM / NG) > 0 ? (DNDSB_RHS_WARPS_PER_SM / NG) : 1; }
