@@ -1,4 +1,4 @@
-// Reverse-mode derivative of the interior-face Roe-family fluxes (Roe and Roe_M1..M8).
+// Reverse-mode derivative of the interior-face Roe-family fluxes (Roe and Roe_M1..M8) and of HLLE+.
 //
 // RoeFlux_IdealGas_HartenYee (Gas.hpp:1038-1126) with the Roe averages r of the two cell means
 // (Gas.hpp:229-259) is
@@ -14,6 +14,8 @@
 //     cotangents of the Roe-average fields, and one Dual<10> evaluation of the averages per face
 //     carries those to the means; the other schemes take the eigenvalues and D (U_R - U_L) in
 //     Dual<10> per Gauss point.
+// HLLEPFlux_IdealGas (Gas.hpp:601-714) mixes the point states into its wave-speed bounds, so it is
+// reversed as a whole (hllep_rev), with the same per-face Dual<10> Roe averages for the means.
 // This replaces two 10-wide forward passes through the whole flux.  Boundary faces keep the
 // generic derivative kernel (ghost states).
 #include "solver.cuh"
@@ -25,6 +27,7 @@ namespace dndsb
 namespace
 {
 constexpr int NV = 5;
+constexpr int kHLLEP = 100; // flux mode of HLLE+ (Roe schemes use their eigScheme 0..8)
 using D10 = Dual<10>;
 
 template <typename T>
@@ -221,6 +224,138 @@ DNDSB_D void roe0_diss_rev(const real *incU, const real *n, const RoeAvg &r, rea
     }
 }
 
+// reverse of the wave strength a1 of roe_waves (Gas.hpp:1098-1109) with respect to incU and the Roe
+// averages: adds a1b d a1/d(incU, r) to incUb, rb (and d a1 / d vRoe0 to vNb)
+DNDSB_D void roe_a1_rev(const real *incU, const real *n, const RoeAvg &r, real gamma, real a1b, real *incUb, RoeBar &rb, real &vNb)
+{
+    real vN = dot3(r.v, n);
+    real incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
+    real a23[3] = {incU[1] - incU[0] * r.v[0], incU[2] - incU[0] * r.v[1], incU[3] - incU[0] * r.v[2]};
+    real a23n = dot3(a23, n);
+    real a23T[3];
+    for (int d = 0; d < 3; d++)
+        a23T[d] = a23[d] - n[d] * a23n;
+    real incU4b = incU[4] - dot3(a23T, r.v);
+    real X = incU[0] * (r.H - vN * vN) + vN * incU123N - incU4b;
+    real a1 = (gamma - 1) / r.asqr * X;
+    real Xb = (gamma - 1) / r.asqr * a1b;
+    rb.asqr += -a1 / r.asqr * a1b;
+    incUb[0] += (r.H - vN * vN) * Xb;
+    rb.H += incU[0] * Xb;
+    vNb += (-2 * vN * incU[0] + incU123N) * Xb;
+    real incU123Nb = vN * Xb;
+    real incU4bb = -Xb;
+    incUb[4] += incU4bb;
+    real a23nb = 0, a23b[3];
+    for (int d = 0; d < 3; d++)
+    {
+        real a23Tb = -r.v[d] * incU4bb;
+        rb.v[d] += -a23T[d] * incU4bb;
+        a23b[d] = a23Tb;
+        a23nb -= n[d] * a23Tb;
+    }
+    for (int d = 0; d < 3; d++)
+    {
+        a23b[d] += n[d] * a23nb;
+        incUb[1 + d] += a23b[d] + n[d] * incU123Nb;
+        incUb[0] += -r.v[d] * a23b[d];
+        rb.v[d] += -incU[0] * a23b[d];
+    }
+}
+
+// d(a^2)/dU of the ideal gas (a^2 = gamma p / rho) times ab, added to Ub
+DNDSB_D void asqr_rev(const real *U, real gamma, real ab, real *Ub)
+{
+    real ir = 1.0 / U[0];
+    real m2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+    real p = (gamma - 1) * (U[4] - 0.5 * m2 * ir);
+    real dpdr = (gamma - 1) * 0.5 * m2 * ir * ir;
+    Ub[0] += ab * gamma * (dpdr * U[0] - p) * ir * ir;
+    for (int d = 0; d < 3; d++)
+        Ub[1 + d] += ab * gamma * ir * (-(gamma - 1) * U[1 + d] * ir);
+    Ub[4] += ab * gamma * ir * (gamma - 1);
+}
+
+// HLLEPFlux_IdealGas (Gas.hpp:601-714) reversed: given Fbar, the cotangents of U_L, U_R (ULb, URb,
+// set) and of the Roe-average fields (rb, accumulated); branch choices (min/max/|.|) follow the
+// primal values, |x| at 0 takes the slope of x >= 0
+DNDSB_D void hllep_rev(const real *UL, const real *UR, const real *n, const RoeAvg &r, real gamma, real dLambda, real fixScale,
+                       const real *Fbar, real *ULb, real *URb, RoeBar &rb)
+{
+    real FL[5], FR[5], pL, pR, aL2, aR2;
+    phys_flux(UL, n, gamma, FL, pL, aL2);
+    phys_flux(UR, n, gamma, FR, pR, aR2);
+    real vRoe0 = dot3(r.v, n), vLm0 = dot3(r.vL, n), vRm0 = dot3(r.vR, n);
+    real incU[5];
+    for (int i = 0; i < 5; i++)
+        incU[i] = UR[i] - UL[i];
+    RoeWavesT<real> w;
+    roe_waves(incU, n, r, gamma, w);
+    real sL = sqrt(aL2), sR = sqrt(aR2);
+    real x1 = vRoe0 - r.a, x2 = vLm0 - sL, y1 = vRoe0 + r.a, y2 = vRm0 + sR;
+    real SL = dmin(x1, x2), SR = dmax(y1, y2);
+    real Mx = dmax(fabs(vRoe0), dLambda * fixScale);
+    real dfix = r.a / (r.a + Mx);
+    real SP = dmax(SR, 0.0), SM = dmin(SL, 0.0);
+    real div = SP - SM;
+    div = div + (div >= 0 ? 1 : -1) * kVerySmall;
+    real id = 1.0 / div;
+    real rv1[5] = {1.0, r.v[0], r.v[1], r.v[2], 0.5 * r.vsqr};
+    real P = SP * SM * id;
+    // F_i = (SP FL_i - SM FR_i) id + P X_i,  X_i = incU_i - dfix rv1_i a1
+    real FLb[5], FRb[5], incUb[5], sumFrv = 0, G = 0, sumFX = 0, sumFFL = 0, sumFFR = 0;
+    for (int i = 0; i < 5; i++)
+    {
+        real Xi = incU[i] - dfix * rv1[i] * w.a1;
+        FLb[i] = SP * id * Fbar[i];
+        FRb[i] = -SM * id * Fbar[i];
+        incUb[i] = P * Fbar[i];
+        sumFrv += Fbar[i] * rv1[i];
+        sumFX += Fbar[i] * Xi;
+        sumFFL += Fbar[i] * FL[i];
+        sumFFR += Fbar[i] * FR[i];
+        G += Fbar[i] * ((SP * FL[i] - SM * FR[i]) + SP * SM * Xi);
+    }
+    real a1b = -P * dfix * sumFrv;
+    real dfixb = -P * w.a1 * sumFrv;
+    for (int d = 0; d < 3; d++)
+        rb.v[d] += -P * dfix * w.a1 * Fbar[1 + d];
+    rb.vsqr += -P * dfix * w.a1 * Fbar[4] * 0.5;
+    real SPb = sumFFL * id + SM * id * sumFX - id * id * G;
+    real SMb = -sumFFR * id + SP * id * sumFX + id * id * G;
+    real SRb = SR > 0.0 ? SPb : 0.0;
+    real SLb = SL < 0.0 ? SMb : 0.0;
+    real vNb = 0, vLm0b = 0, vRm0b = 0, aL2b = 0, aR2b = 0;
+    if (x1 < x2)
+        vNb += SLb, rb.a -= SLb;
+    else
+        vLm0b += SLb, aL2b += -SLb * 0.5 / sL;
+    if (y1 > y2)
+        vNb += SRb, rb.a += SRb;
+    else
+        vRm0b += SRb, aR2b += SRb * 0.5 / sR;
+    // dfix = a / (a + Mx), Mx = max(|vRoe0|, dLambda fixScale)
+    real den = r.a + Mx;
+    rb.a += dfixb * Mx / (den * den);
+    real Mxb = -dfixb * r.a / (den * den);
+    if (fabs(vRoe0) > dLambda * fixScale)
+        vNb += Mxb * (vRoe0 >= 0 ? 1.0 : -1.0);
+    roe_a1_rev(incU, n, r, gamma, a1b, incUb, rb, vNb);
+    // point states: physical fluxes, sound speeds, jump
+    flux_jac_du_t<NV>(UL, n, FLb, 0.0, gamma, ULb);
+    flux_jac_du_t<NV>(UR, n, FRb, 0.0, gamma, URb);
+    asqr_rev(UL, gamma, aL2b, ULb);
+    asqr_rev(UR, gamma, aR2b, URb);
+    for (int i = 0; i < 5; i++)
+        ULb[i] -= incUb[i], URb[i] += incUb[i];
+    for (int d = 0; d < 3; d++)
+    {
+        rb.v[d] += n[d] * vNb;
+        rb.vL[d] += n[d] * vLm0b;
+        rb.vR[d] += n[d] * vRm0b;
+    }
+}
+
 template <int DIM, int P>
 DNDSB_GLOBAL void k_rhs_vjp_face_roe(MeshD m, GeomD g, VRD vr, EulerSettingsD s, int es, const real *__restrict__ w, const real *__restrict__ u,
                                      const real *__restrict__ uRec, const real *__restrict__ dLamCell, real *__restrict__ faceAdj, int *err)
@@ -280,6 +415,22 @@ DNDSB_GLOBAL void k_rhs_vjp_face_roe(MeshD m, GeomD g, VRD vr, EulerSettingsD s,
                 UL[v] = a, UR[v] = b, incU[v] = b - a;
             }
             bad |= !(UL[0] > 0 && UR[0] > 0);
+            if (es == kHLLEP)
+            {
+                real ULbar[NV], URbar[NV];
+                hllep_rev(UL, UR, n, r, gamma, dLambda, s.rsFixScale, Fbar, ULbar, URbar, rbar);
+                for (int v = 0; v < NV; v++)
+                {
+                    acc0[v] += ULbar[v];
+                    acc1[v] += URbar[v];
+                    for (int j = 0; j < R; j++)
+                    {
+                        acc0[NV + j * NV + v] += T0[1 + j] * ULbar[v];
+                        acc1[NV + j * NV + v] += T1[1 + j] * URbar[v];
+                    }
+                }
+                continue;
+            }
             if (es == 0)
             {
                 // plain Roe: one reverse sweep gives D^T incFb and the Roe-average cotangents
@@ -346,7 +497,7 @@ DNDSB_GLOBAL void k_rhs_vjp_face_roe(MeshD m, GeomD g, VRD vr, EulerSettingsD s,
                 }
             }
         }
-        if (es == 0)
+        if (es == 0 || es == kHLLEP)
         {
             // Roe-average cotangents -> cell means through the per-face Dual<10> averages
             for (int i = 0; i < 2 * NV; i++)
@@ -368,8 +519,13 @@ DNDSB_GLOBAL void k_rhs_vjp_face_roe(MeshD m, GeomD g, VRD vr, EulerSettingsD s,
 }
 } // namespace
 
-// the Roe-family scheme index (eigScheme 0..8) of a Riemann-solver code, or -1
-int roe_scheme_of(int rsType) { return rsType == RS_Roe ? 0 : (rsType >= RS_Roe_M1 && rsType <= RS_Roe_M8) ? rsType - 10 : -1; }
+// the reverse-mode flux of a Riemann-solver code: the Roe eigScheme 0..8, kHLLEP, or -1 (forward mode)
+int roe_scheme_of(int rsType)
+{
+    if (rsType == RS_HLLEP)
+        return kHLLEP;
+    return rsType == RS_Roe ? 0 : (rsType >= RS_Roe_M1 && rsType <= RS_Roe_M8) ? rsType - 10 : -1;
+}
 
 int rhs_vjp_roe_interior(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec,
                          real *faceAdj, cudaStream_t st)
