@@ -397,7 +397,8 @@ def tgv_vjp_cost(args):
 def adjoint_solve(vr, ev, u, uRec, far, mesh, ms_primal):
     """Adjoint of the pressure drag on the bump for the coupled (EvaluateRHS, VR sweep) residual of one
     implicit Euler step (dt = 5 local CFL-1 steps) at a smooth non-uniform state: GMRES(40) preconditioned
-    by the transposed LU-SGS pair and a 4-term Neumann series of the transposed sweep, to a 1e-10 drop."""
+    by the transposed LU-SGS pair (FP64, then on FP32 vectors) and a 4-term Neumann series of the
+    transposed sweep, to a 1e-10 drop."""
     import torch
     from dndsr_b200 import mesh as M
     from dndsr_b200.adjoint import SteadyAdjoint
@@ -411,15 +412,20 @@ def adjoint_solve(vr, ev, u, uRec, far, mesh, ms_primal):
         vr.DoReconstructionIter(ur, tmp, us, putIntoNew=False)
     dTau = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
     ev.EvaluateDt(dTau, us, 1.0)
-    adj = SteadyAdjoint(vr, ev, us, ur, cfl=5.0, dt=5.0 * float(dTau.max()))
     J, gU, gR = ev.PressureForce(M.BUMP_ZONES["bump"], (1.0, 0.0, 0.0), us, ur, grad=True)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    psi, lam, hist = adj.solve_adjoint(gU, gR, restart=40, max_restarts=40, rtol=1e-10)
-    torch.cuda.synchronize()
-    el = time.perf_counter() - t0
-    return {"objective": "pressure drag on the bump", "J": J, "gmres_iterations": len(hist) - 1, "final_drop": hist[-1], "seconds": el,
-            "solve_over_one_residual": 1e3 * el / ms_primal}
+    out = {"objective": "pressure drag on the bump", "J": J}
+    for prec in ("fp64", "fp32"):
+        adj = SteadyAdjoint(vr, ev, us, ur, cfl=5.0, dt=5.0 * float(dTau.max()), precision=prec)
+        adj.solve_adjoint(gU, gR, restart=40, max_restarts=1, rtol=1e-10)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        psi, lam, hist = adj.solve_adjoint(gU, gR, restart=40, max_restarts=40, rtol=1e-10)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        key = "" if prec == "fp64" else "_fp32_preconditioner"
+        out.update({"gmres_iterations" + key: len(hist) - 1, "final_drop" + key: hist[-1], "seconds" + key: el,
+                    "solve_over_one_residual" + key: 1e3 * el / ms_primal})
+    return out
 
 
 def n_cores():

@@ -20,7 +20,8 @@ reproduces as <g, d> (dual consistency).
 Both systems are solved by right-preconditioned restarted GMRES on the device.  The u block
 is preconditioned by the scalar-Jacobian LU-SGS pair (primal) or its transpose (adjoint),
 the operator of LUSGSMatrixInit/UpdateSGS (EulerEvaluator.hxx:37-159, 550-693) at a pseudo
-time step of CFL ``cfl``; the uRec block by a truncated Neumann series of the sweep,
+time step of CFL ``cfl`` (the transposed sweeps optionally on FP32 vectors, ``precision="fp32"``,
+inside the FP64 Krylov iteration); the uRec block by a truncated Neumann series of the sweep,
 -(I + M + ... + M^k), M = dS/duRec.
 """
 from __future__ import annotations
@@ -98,9 +99,11 @@ def gmres(op, prec, b, restart=30, max_restarts=100, rtol=1e-10):
 class SteadyAdjoint:
     """The coupled steady residual linearised at (u, uRec); see the module docstring."""
 
-    def __init__(self, vr, ev, u, uRec, cfl=5.0, alphaDiag=1.0, n_neumann=4, dt=math.inf):
+    def __init__(self, vr, ev, u, uRec, cfl=5.0, alphaDiag=1.0, n_neumann=4, dt=math.inf, precision="fp64"):
         self.vr, self.ev, self.u, self.uRec = vr, ev, u.contiguous(), uRec.contiguous()
         self.alphaDiag, self.n_neumann = alphaDiag, n_neumann
+        # "fp32": the transposed LU-SGS preconditioner sweeps FP32 vectors (the operator stays FP64)
+        self.pdt = torch.float32 if precision == "fp32" else torch.float64
         # dt < inf: the residual of one implicit Euler step, R_u - (u - u_n) / dt (its Jacobian gains -I / dt)
         self.idt = 0.0 if math.isinf(dt) else 1.0 / dt
         n = u.shape[0]
@@ -129,14 +132,17 @@ class SteadyAdjoint:
     # preconditioners: u block -(LU-SGS pair) ~ (dR_u/du)^-1, uRec block -(I + M + ... + M^k) ~ (M - I)^-1
     def _sgs_pair(self, r, transposed):
         ev, a, jd = self.ev, self.alphaDiag, self.jd
+        if transposed:
+            rp = r.to(self.pdt).contiguous()
+            z0 = torch.zeros_like(rp)
+            z1, z2 = torch.empty_like(rp), torch.empty_like(rp)
+            ev.UpdateSGST(a, rp, self.u, z0, z1, jd, True)
+            ev.UpdateSGST(a, rp, self.u, z1, z2, jd, False)
+            return z2.to(r.dtype)
         z0 = torch.zeros_like(r)
         z1, z2 = torch.empty_like(r), torch.empty_like(r)
-        if transposed:
-            ev.UpdateSGST(a, r, self.u, z0, z1, jd, True)
-            ev.UpdateSGST(a, r, self.u, z1, z2, jd, False)
-        else:
-            ev.UpdateSGS(a, r, self.u, z0, z1, jd, True, want_sum=False)
-            ev.UpdateSGS(a, r, self.u, z1, z2, jd, False, want_sum=False)
+        ev.UpdateSGS(a, r, self.u, z0, z1, jd, True, want_sum=False)
+        ev.UpdateSGS(a, r, self.u, z1, z2, jd, False, want_sum=False)
         return z2
 
     def _neumann(self, r, transposed):

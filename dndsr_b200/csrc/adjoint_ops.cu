@@ -59,17 +59,19 @@ DNDSB_GLOBAL void k_matvec_t(MeshD m, GeomD g, real gamma, const real *__restric
     }
 }
 
-template <int NV>
+// TY: the precision of b, y and yNew (the transposed sweep as an FP32 preconditioner reads and writes
+// float vectors; the operator coefficients come from the FP64 state and are applied in FP64)
+template <int NV, typename TY>
 DNDSB_GLOBAL void k_sgs_color_t(MeshD m, GeomD g, real gamma, const real *__restrict__ lamFace, const int32_t *__restrict__ cellColor,
-                                int64_t cBeg, int64_t cEnd, int color, real alphaDiag, const real *__restrict__ b, const real *__restrict__ u,
-                                const real *__restrict__ y, real *yNew, const real *__restrict__ jdiag, int forward, int gsUpdate)
+                                int64_t cBeg, int64_t cEnd, int color, real alphaDiag, const TY *__restrict__ b, const real *__restrict__ u,
+                                const TY *__restrict__ y, TY *yNew, const real *__restrict__ jdiag, int forward, int gsUpdate)
 {
     DNDSB_KERNEL_LOOP(ii, cEnd - cBeg)
     {
         int64_t q = m.colorCells[cBeg + ii];
         real buf[NV];
         for (int v = 0; v < NV; v++)
-            buf[v] = b[q * NV + v];
+            buf[v] = (real)b[q * NV + v];
         for (int k = 0; k < m.nf; k++)
         {
             int o = m.cellNbr[q * m.nf + k];
@@ -77,13 +79,16 @@ DNDSB_GLOBAL void k_sgs_color_t(MeshD m, GeomD g, real gamma, const real *__rest
                 continue;
             int oc = cellColor[o];
             bool useNew = gsUpdate && (forward ? oc < color : oc > color);
-            real t[NV];
-            neighbour_term_t<NV>(m, g, gamma, lamFace, alphaDiag, q, k, o, u, (useNew ? yNew : y) + (int64_t)o * NV, t);
+            const TY *src = (useNew ? yNew : y) + (int64_t)o * NV;
+            real yo[NV], t[NV];
+            for (int v = 0; v < NV; v++)
+                yo[v] = (real)src[v];
+            neighbour_term_t<NV>(m, g, gamma, lamFace, alphaDiag, q, k, o, u, yo, t);
             for (int v = 0; v < NV; v++)
                 buf[v] -= t[v];
         }
         for (int v = 0; v < NV; v++)
-            yNew[q * NV + v] = buf[v] / jdiag[NV == 6 ? q * NV + v : q];
+            yNew[q * NV + v] = (TY)(buf[v] / jdiag[NV == 6 ? q * NV + v : q]);
     }
 }
 
@@ -186,22 +191,28 @@ int lusgs_matvec_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, co
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
-int update_sgs_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *b, const real *u, const real *y, real *yNew,
-                 const real *jdiag, int forward, int gsUpdate, cudaStream_t st)
+int update_sgs_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const void *b, const real *u, const void *y, void *yNew,
+                 const real *jdiag, int forward, int gsUpdate, int fp32, cudaStream_t st)
 {
     int nv = ev.s.nVars;
     for (int ci = 0; ci < m.nColor; ci++)
     {
         int col = forward ? ci : m.nColor - 1 - ci;
         int64_t bb = m.colorStart[col], e = m.colorStart[col + 1];
-        if (nv == 5)
-            DNDSB_LAUNCH(k_sgs_color_t<5>, e - bb, 128, st, m, g, ev.s.gamma, ev.lambdaFace, m.cellColor, bb, e, col, alphaDiag, b, u, y, yNew,
-                         jdiag, forward, gsUpdate);
+#define DNDSB_SGST(NVV, TY)                                                                                                               \
+    DNDSB_LAUNCH((k_sgs_color_t<NVV, TY>), e - bb, 128, st, m, g, ev.s.gamma, ev.lambdaFace, m.cellColor, bb, e, col, alphaDiag, (const TY *)b, u, \
+                 (const TY *)y, (TY *)yNew, jdiag, forward, gsUpdate)
+        if (nv == 5 && !fp32)
+            DNDSB_SGST(5, real);
+        else if (nv == 5)
+            DNDSB_SGST(5, float);
+        else if (nv == 6 && !fp32)
+            DNDSB_SGST(6, real);
         else if (nv == 6)
-            DNDSB_LAUNCH(k_sgs_color_t<6>, e - bb, 128, st, m, g, ev.s.gamma, ev.lambdaFace, m.cellColor, bb, e, col, alphaDiag, b, u, y, yNew,
-                         jdiag, forward, gsUpdate);
+            DNDSB_SGST(6, float);
         else
             return ST_UNSUPPORTED;
+#undef DNDSB_SGST
     }
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }

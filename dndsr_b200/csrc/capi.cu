@@ -645,14 +645,14 @@ extern "C"
                           "dndsb_eval_lusgs_matrix_vec_t");
     }
 
-    int dndsb_eval_update_sgs_t(dndsb_eval *e, double alphaDiag, const double *b, const double *u, const double *y, double *yNew,
-                                const double *jdiag, int forward, int gsUpdate, void *stream)
+    int dndsb_eval_update_sgs_t(dndsb_eval *e, double alphaDiag, const void *b, const double *u, const void *y, void *yNew,
+                                const double *jdiag, int forward, int gsUpdate, int precision, void *stream)
     {
-        if (!e || !b || !u || !y || !yNew || !jdiag)
-            return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: null argument");
+        if (!e || !b || !u || !y || !yNew || !jdiag || precision < 0 || precision > 1)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: null argument or bad precision");
         if (y == yNew)
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: y and yNew must differ");
-        return status_msg(update_sgs_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate, S(stream)),
+        return status_msg(update_sgs_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate, precision, S(stream)),
                           "dndsb_eval_update_sgs_t");
     }
 

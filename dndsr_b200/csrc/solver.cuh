@@ -181,8 +181,8 @@ int rhs_vjp_roe_interior(const MeshD &m, const GeomD &g, const VRD &vr, const Ev
 // adjoint building blocks (adjoint_ops.cu)
 int lusgs_matvec_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *y, const real *jdiag, real *ATy,
                    cudaStream_t st);
-int update_sgs_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *b, const real *u, const real *y, real *yNew,
-                 const real *jdiag, int forward, int gsUpdate, cudaStream_t st);
+int update_sgs_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const void *b, const real *u, const void *y, void *yNew,
+                 const real *jdiag, int forward, int gsUpdate, int fp32, cudaStream_t st);
 int pressure_force(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, int zone, const real *dir, const real *u, const real *uRec,
                    real *Jhost, real *gU, real *gRec, cudaStream_t st);
 int vr_swap(int64_t n, real *a, real *b, cudaStream_t st);

@@ -55,9 +55,10 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def _ptr(t: torch.Tensor, nm="tensor"):
-    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
-        raise ValueError(f"{nm} must be a contiguous float64 CUDA tensor")
+def _ptr(t: torch.Tensor, nm="tensor", fp32=False):
+    dt = torch.float32 if fp32 else torch.float64
+    if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
+        raise ValueError(f"{nm} must be a contiguous {'float32' if fp32 else 'float64'} CUDA tensor")
     return ctypes.c_void_p(t.data_ptr())
 
 
@@ -281,9 +282,13 @@ class EulerEvaluator(Handle):
                   _ptr(ATy, "ATy"), _stream())
 
     def UpdateSGST(self, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate=True):
-        """One Gauss-Seidel sweep on A^T y = b (the transpose of UpdateSGS), colour by colour."""
-        capi.call("dndsb_eval_update_sgs_t", self.h, float(alphaDiag), _ptr(b, "b"), _ptr(u, "u"), _ptr(y, "y"), _ptr(yNew, "yNew"),
-                  _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), _stream())
+        """One Gauss-Seidel sweep on A^T y = b (the transpose of UpdateSGS), colour by colour; b, y and
+        yNew are all float64 or all float32 (the FP32 preconditioner)."""
+        fp32 = b.dtype == torch.float32
+        if any((t.dtype == torch.float32) != fp32 for t in (y, yNew)):
+            raise TypeError("UpdateSGST: b, y and yNew must share one precision")
+        capi.call("dndsb_eval_update_sgs_t", self.h, float(alphaDiag), _ptr(b, "b", fp32), _ptr(u, "u"), _ptr(y, "y", fp32),
+                  _ptr(yNew, "yNew", fp32), _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), int(fp32), _stream())
 
     def PressureForce(self, zone, direction, u, uRec, grad=False):
         """Pressure force along direction on boundary zone; with grad also (dJ/du, dJ/duRec) as device tensors."""

@@ -190,11 +190,12 @@ int dndsb_eval_rhs_jvp(dndsb_eval *ev, const double *du, const double *duRec, co
  * lusgs_matrix_vec_t: ATy = A^T y for the operator A of dndsb_eval_lusgs_matrix_vec (same lambdaFace,
  * jdiag and alphaDiag).  update_sgs_t: one Gauss-Seidel sweep on A^T y = b, colour by colour (forward:
  * colours ascending, new values of earlier colours when gsUpdate), y and yNew distinct; a forward then
- * a backward sweep is the symmetric Gauss-Seidel preconditioner of A^T. */
+ * a backward sweep is the symmetric Gauss-Seidel preconditioner of A^T.  precision 0: b, y, yNew are
+ * double; 1: float (the FP32 preconditioner; the operator is applied in FP64 from the FP64 state). */
 int dndsb_eval_lusgs_matrix_vec_t(dndsb_eval *ev, double alphaDiag, const double *u, const double *y, const double *jdiag, double *ATy,
                                   void *stream);
-int dndsb_eval_update_sgs_t(dndsb_eval *ev, double alphaDiag, const double *b, const double *u, const double *y, double *yNew,
-                            const double *jdiag, int forward, int gsUpdate, void *stream);
+int dndsb_eval_update_sgs_t(dndsb_eval *ev, double alphaDiag, const void *b, const double *u, const void *y, void *yNew,
+                            const double *jdiag, int forward, int gsUpdate, int precision, void *stream);
 /* Pressure force along dir[3] on the boundary faces of zone:
  *   J = sum_f sum_g |J|_g w_g p(U_L(x_g)) (n_g . dir),  U_L = u + phi . uRec of the face's cell,
  * returned in *Jhost; dJdu [nCell][nVars] and dJduRec [nCell][R][nVars] (device, either may be NULL)

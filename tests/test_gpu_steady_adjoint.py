@@ -66,6 +66,10 @@ def test_transposed_lusgs_and_pressure_force_parity(p):
         ev.UpdateSGST(1.0, torch.tensor(b0, device="cuda"), u, y, yn, jd, forward)
         ref = o.update_sgs_t(1.0, b0, u0, y0, y0, jd0, forward)
         assert relerr(yn.cpu().numpy(), ref) < 1e-12
+        # the FP32 sweep (float vectors, FP64 operator) of the adjoint preconditioner
+        yn32 = torch.empty_like(y, dtype=torch.float32)
+        ev.UpdateSGST(1.0, torch.tensor(b0, device="cuda", dtype=torch.float32), u, y.float(), yn32, jd, forward)
+        assert relerr(yn32.double().cpu().numpy(), ref) < 1e-6
     J, gU, gR = ev.PressureForce(BUMP, DRAG, u, uRec, grad=True)
     J0, gU0, gR0 = o.pressure_force(BUMP, DRAG, u0, uRec0, grad=True)
     assert abs(J - J0) < 1e-12 * abs(J0)
@@ -92,6 +96,10 @@ def test_coupled_adjoint_and_tangent_solves_agree(p):
     J, gU, gR = ev.PressureForce(BUMP, DRAG, u, uRec, grad=True)
     psi, lam, h_adj = adj.solve_adjoint(gU, gR, restart=40, max_restarts=60, rtol=1e-10)
     assert h_adj[-1] < 1e-10
+    # FP32 transposed LU-SGS inside the FP64 Krylov iteration reaches the same adjoint
+    adj32 = SteadyAdjoint(vr, ev, u, uRec, cfl=5.0, dt=5.0 * float(dTau.max()), precision="fp32")
+    psi32, lam32, h32 = adj32.solve_adjoint(gU, gR, restart=40, max_restarts=60, rtol=1e-10)
+    assert h32[-1] < 1e-10 and relerr(psi32.cpu().numpy(), psi.cpu().numpy()) < 1e-8
     sU = torch.tensor(rng.normal(size=u0.shape), device="cuda")
     sR = torch.zeros_like(uRec)
     du, dRec, h_tan = adj.solve_tangent(sU, sR, restart=40, max_restarts=60, rtol=1e-10)
