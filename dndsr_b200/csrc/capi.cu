@@ -482,6 +482,7 @@ extern "C"
         d.nVars = s->nVars, d.rsType = s->rsType, d.rsFixScale = s->rsFixScale, d.rsIncFScale = s->rsIncFScale;
         d.gamma = s->gamma, d.Rgas = s->Rgas, d.muGas = s->muGas, d.prGas = s->prGas, d.TRef = s->TRef, d.CSutherland = s->CSutherland;
         d.muModel = s->muModel, d.ignoreVis = s->ignoreVis;
+        d.derive();
         const MeshD &m = vr->mesh->d;
         int rc = 0;
         rc |= dev_alloc((void **)&e->e.lambdaFace, sizeof(real) * m.nFace);

@@ -441,8 +441,9 @@ template <typename T>
 DNDSB_HD void gas_thermal(T E, T rho, T vSqr, real gamma, T &p, T &asqr, T &H)
 {
     p = (gamma - 1) * (E - rho * 0.5 * vSqr);
-    asqr = gamma * p / rho;
-    H = (E + p) / rho;
+    T ir = 1.0 / rho;
+    asqr = gamma * p * ir;
+    H = (E + p) * ir;
 }
 
 enum RSType : int
@@ -474,6 +475,7 @@ struct RoeAvgT
 {
     T vL[3], vR[3], aL, aR, pLm, pRm;
     T v[3], vsqr, H, asqr, a, rho;
+    T gOverA2, inv2a; // (gamma - 1) / asqr and 1 / (2 a), shared by the Gauss points of a face
 };
 using RoeAvg = RoeAvgT<real>;
 
@@ -496,6 +498,8 @@ DNDSB_HD void roe_average(const T *ULm, const T *URm, real gamma, RoeAvgT<T> &r)
     r.asqr = (gamma - 1) * (r.H - 0.5 * r.vsqr);
     r.rho = sL * sR;
     r.a = sqrt(r.asqr);
+    r.gOverA2 = (gamma - 1) / r.asqr;
+    r.inv2a = 0.5 / r.a;
 }
 
 // physical flux through n (no grid velocity): Gas.hpp:390-397
@@ -504,8 +508,8 @@ DNDSB_HD void phys_flux(const T *U, const real *n, real gamma, T F[5], T &p, T &
 {
     T ir = 1.0 / U[0];
     T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
-    T H;
-    gas_thermal(U[4], U[0], dot3s(v, v), gamma, p, asqr, H);
+    p = (gamma - 1) * (U[4] - U[0] * 0.5 * dot3s(v, v));
+    asqr = gamma * p * ir;
     T vn = dot3v(v, n);
     F[0] = U[0] * vn;
     F[1] = U[1] * vn + p * n[0];
@@ -531,8 +535,8 @@ DNDSB_HD void roe_waves(const T *incU, const real *n, const RoeAvgT<T> &r, real 
     for (int d = 0; d < 3; d++)
         w.a23T[d] = a23[d] - n[d] * a23n;
     T incU4b = incU[4] - dot3s(w.a23T, r.v);
-    w.a1 = (gamma - 1) / r.asqr * (incU[0] * (r.H - w.vRoeN * w.vRoeN) + w.vRoeN * incU123N - incU4b);
-    w.a0 = (incU[0] * (w.vRoeN + r.a) - incU123N - r.a * w.a1) / (2 * r.a);
+    w.a1 = r.gOverA2 * (incU[0] * (r.H - w.vRoeN * w.vRoeN) + w.vRoeN * incU123N - incU4b);
+    w.a0 = (incU[0] * (w.vRoeN + r.a) - incU123N - r.a * w.a1) * r.inv2a;
     w.a4 = incU[0] - (w.a0 + w.a1);
 }
 
@@ -728,11 +732,10 @@ DNDSB_HD bool riemann_flux(int rs, const T *UL, const T *UR, const T *ULm, const
     return riemann_flux_pre(rs, UL, UR, r, n, gamma, dLambda, fixScale, incFScale, F, lam0, lam123, lam4);
 }
 
-// Gas.hpp:1677-1698 GradientCons2Prim_IdealGas; G and GP are [3][NV]
+// Gas.hpp:1677-1698 GradientCons2Prim_IdealGas; G and GP are [3][NV]; ir = 1 / U[0]
 template <int NV, typename T>
-DNDSB_HD void grad_cons2prim(const T *U, const T *G, T *GP, real gamma)
+DNDSB_HD void grad_cons2prim_ir(const T *U, const T &ir, const T *G, T *GP, real gamma)
 {
-    T ir = 1.0 / U[0];
     T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
     for (int r = 0; r < 3; r++)
     {
@@ -748,14 +751,21 @@ DNDSB_HD void grad_cons2prim(const T *U, const T *G, T *GP, real gamma)
     }
 }
 
-// Gas.hpp:1594-1655 ViscousFlux_IdealGas without QCR; GP is the primitive gradient [3][NV]
 template <int NV, typename T>
-DNDSB_HD void viscous_flux(const T *U, const T *GP, const real *n, bool adiabatic, real gamma, T mu, T k, real Cp, T *Fv)
+DNDSB_HD void grad_cons2prim(const T *U, const T *G, T *GP, real gamma)
 {
     T ir = 1.0 / U[0];
+    grad_cons2prim_ir<NV>(U, ir, G, GP, gamma);
+}
+
+// Gas.hpp:1594-1655 ViscousFlux_IdealGas without QCR; GP is the primitive gradient [3][NV];
+// ir = 1 / U[0], kT = gamma / ((gamma - 1) Cp)
+template <int NV, typename T>
+DNDSB_HD void viscous_flux_ir(const T *U, const T &ir, const T *GP, const real *n, bool adiabatic, real gamma, T mu, T k, real kT, T *Fv)
+{
     T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
     T p = (gamma - 1) * (U[4] - U[0] * 0.5 * dot3s(v, v));
-    T cT = gamma / ((gamma - 1) * Cp * U[0] * U[0]);
+    T cT = kT * ir * ir;
     T gT[3];
     for (int i = 0; i < 3; i++)
         gT[i] = cT * (U[0] * GP[i * NV + 4] - p * GP[i * NV + 0]);
@@ -782,6 +792,13 @@ DNDSB_HD void viscous_flux(const T *U, const T *GP, const real *n, bool adiabati
     }
     Fv[0] = 0;
     Fv[4] = e;
+}
+
+template <int NV, typename T>
+DNDSB_HD void viscous_flux(const T *U, const T *GP, const real *n, bool adiabatic, real gamma, T mu, T k, real Cp, T *Fv)
+{
+    T ir = 1.0 / U[0];
+    viscous_flux_ir<NV>(U, ir, GP, n, adiabatic, gamma, mu, k, gamma / ((gamma - 1) * Cp), Fv);
 }
 
 // EulerEvaluator.hpp:751-789 muEff: 0 constant, 1 Sutherland, 2 proportional to density

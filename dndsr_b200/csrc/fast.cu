@@ -39,7 +39,7 @@ struct Layout
     static constexpr int CS = (OM + NDOF) | 1; // odd stride: lanes of a warp (different faces) hit different banks
 };
 
-// per-face data shared by the Gauss points of a face (27 doubles: an odd stride in shared memory)
+// per-face data shared by the Gauss points of a face (29 doubles: an odd stride in shared memory)
 struct FaceData
 {
     RoeAvg r;       // Roe averages of the two cell means
@@ -49,7 +49,7 @@ struct FaceData
     real shift[3];  // periodic translation into side 1's frame
     real pad;       // keeps the stride odd
 };
-static_assert(sizeof(FaceData) == 27 * sizeof(real), "FaceData layout");
+static_assert(sizeof(FaceData) == 29 * sizeof(real), "FaceData layout");
 
 // u + phi . uRec and the gradient D1 phi . uRec of one cell at point p (VariationalReconstruction.hpp:378-442 rows 0..dim)
 template <int DIM, int P, int NV, bool ACC>
@@ -209,14 +209,14 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
 #pragma unroll
                 for (int v = 0; v < NV; v++)
                     G[d * NV + v] = G[d * NV + v] * 0.5 + iD * (n[d] * (UR[v] - UL[v]));
-            grad_cons2prim<NV>(UM, G, GP, gamma);
+            real irho = 1.0 / UM[0]; // the one reciprocal density of the viscous flux
+            grad_cons2prim_ir<NV>(UM, irho, G, GP, gamma);
             if (NV == 5)
             {
-                real irho = 1.0 / UM[0];
                 real pM = (gamma - 1) * (UM[4] - 0.5 * (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) * irho);
-                real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
+                real Tm = pM * irho * s.kT;
                 real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
-                viscous_flux<NV>(UM, GP, n, false, gamma, mu, cp * mu / s.prGas, cp, Fv);
+                viscous_flux_ir<NV>(UM, irho, GP, n, false, gamma, mu, cp * mu * s.iPr, s.kT, Fv);
             }
             else // SA: eddy viscosity in the momentum/energy fluxes and the nuTilde diffusion flux
                 point_viscous_flux<NV>(s, UM, GP, n, false, Fv);

@@ -132,7 +132,9 @@ struct EulerSettingsD
     real gamma = 1.4, Rgas = 1, muGas = 1, prGas = 0.72, TRef = 273.15, CSutherland = 110.4;
     int muModel = 1;
     int ignoreVis = 0;
+    real kT = 0, iPr = 0; // host-derived: gamma / ((gamma - 1) cp) (T = p kT / rho), 1 / prGas
     real cp() const { return Rgas * gamma / (gamma - 1); }
+    void derive() { kT = gamma / ((gamma - 1) * cp()), iPr = 1.0 / prGas; }
 };
 
 struct EvalD
