@@ -5,27 +5,29 @@ import oracle
 from dndsr_b200 import mesh as M
 from tests.util import VR_HQM
 
-# EulerEvaluator.hpp:138-152: Dirichlet-type VR weights {1,0,0,0} on far-field, walls and
-# symmetry; zero weight on supersonic outflow (BCOut); interior zones keep 1
+# EulerEvaluator.hpp:138-152: Dirichlet-type VR weights {1,0,0,0} on far-field, walls, symmetry
+# and inflow (the default below); zero weight on supersonic outflow (BCOut); interior zones keep 1
 BC_DIR_WEIGHT = {1: (1, 0, 0, 0), 3: (1, 0, 0, 0), 9: (1, 0, 0, 0), 5: (0, 0, 0, 0)}
 
 
-def bump_bc(far, outflow_type=1):
+def bump_bc(far, outflow_type=1, inflow_type=1, wall_type=3):
     types = np.zeros(7, np.int32)
     vals = np.zeros((7, len(far)))
     for z, tp in M.BUMP_BC_TYPES.items():
         types[z] = tp
         vals[z] = far
     types[M.BUMP_ZONES["outflow"]] = outflow_type
+    types[M.BUMP_ZONES["inflow"]] = inflow_type
+    types[M.BUMP_ZONES["bump"]] = wall_type  # an isothermal wall (4) takes its temperature from value[0]
     w = np.ones((7, 4))
     for z in range(1, 7):
-        w[z] = BC_DIR_WEIGHT[int(types[z])]
+        w[z] = BC_DIR_WEIGHT.get(int(types[z]), (1, 0, 0, 0))
     return types, vals, w
 
 
-def bump_oracle(m, p, rs="Roe", mu=0.0, ignoreVis=1, mach=0.8, outflow_type=1, intOrder=5):
+def bump_oracle(m, p, rs="Roe", mu=0.0, ignoreVis=1, mach=0.8, outflow_type=1, intOrder=5, inflow_type=1, wall_type=3):
     far = M.freestream(mach)
-    types, vals, w = bump_bc(far, outflow_type)
+    types, vals, w = bump_bc(far, outflow_type, inflow_type, wall_type)
     es = dict(nVars=5, rsType=oracle.RS[rs], rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=mu, prGas=0.72, TRef=273.15,
               CSutherland=110.4, muModel=0, ignoreVis=ignoreVis)
     o = oracle.Oracle(m, dict(VR_HQM, maxOrder=p, intOrder=intOrder), es)

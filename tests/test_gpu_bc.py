@@ -1,5 +1,6 @@
 """Boundary faces on the GPU against the oracle: the bump channel with far-field,
-slip-wall, symmetry and outflow zones (setup arrays, VR sweeps with GetBoundaryRHS,
+slip-wall, symmetry and outflow zones, and viscous cases with inflow, pressure-outflow,
+no-slip and isothermal walls (setup arrays, VR sweeps with GetBoundaryRHS,
 local time step, right-hand side, LU-SGS operators and the native linear solve).
 Tolerance 1e-12 relative for FP64 operators."""
 import numpy as np
@@ -13,24 +14,28 @@ from tests.util import VR_HQM_PY, relerr
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
-CASES = [("p1-Roe-euler", 1, "Roe", 0.0, 1, 1, 5), ("p2-Roe-euler", 2, "Roe", 0.0, 1, 1, 5),
-         ("p2-HLLEP-ns-bcout", 2, "HLLEP", 1e-3, 0, 5, 5), ("p3-RoeM1-euler", 3, "Roe_M1", 0.0, 1, 1, 5),
-         ("p1-Roe-euler-int2", 1, "Roe", 0.0, 1, 1, 2)]
+# (name, p, Riemann solver, mu, ignoreVis, outflow type, intOrder, inflow type, bump-wall type)
+CASES = [("p1-Roe-euler", 1, "Roe", 0.0, 1, 1, 5, 1, 3), ("p2-Roe-euler", 2, "Roe", 0.0, 1, 1, 5, 1, 3),
+         ("p2-HLLEP-ns-bcout", 2, "HLLEP", 1e-3, 0, 5, 5, 1, 3), ("p3-RoeM1-euler", 3, "Roe_M1", 0.0, 1, 1, 5, 1, 3),
+         ("p1-Roe-euler-int2", 1, "Roe", 0.0, 1, 1, 2, 1, 3),
+         # viscous boundary fluxes: BCIn inflow, BCOutP pressure outflow, BCWallIsothermal / BCWall no-slip bump
+         ("p1-Roe-ns-in-outp-isothermal", 1, "Roe", 1e-3, 0, 6, 5, 7, 4), ("p2-HLLEP-ns-in-outp-wall", 2, "HLLEP", 1e-3, 0, 6, 5, 7, 2)]
 
 
-def _setup(p, rs, mu, ignoreVis, outflow, intOrder=5):
+def _setup(p, rs, mu, ignoreVis, outflow, intOrder=5, inflow=1, wall=3):
     from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
     m = M.renumber_by_color(M.bump_channel_tet(6, 4, 2))
-    o, far, types, vals, w = bump_oracle(m, p, rs, mu, ignoreVis, outflow_type=outflow, intOrder=intOrder)
+    o, far, types, vals, w = bump_oracle(m, p, rs, mu, ignoreVis, outflow_type=outflow, intOrder=intOrder, inflow_type=inflow,
+                                         wall_type=wall)
     vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p, intOrder=intOrder)).construct(w)
     ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType=rs, muGas=mu, muModel=0, ignoreVis=bool(ignoreVis)))
     ev.SetBC(types, vals)
     return m, o, vr, ev, far
 
 
-@pytest.mark.parametrize("name,p,rs,mu,iv,outflow,intOrder", CASES, ids=[c[0] for c in CASES])
-def test_boundary_operators(name, p, rs, mu, iv, outflow, intOrder):
-    m, o, vr, ev, far = _setup(p, rs, mu, iv, outflow, intOrder)
+@pytest.mark.parametrize("name,p,rs,mu,iv,outflow,intOrder,inflow,wall", CASES, ids=[c[0] for c in CASES])
+def test_boundary_operators(name, p, rs, mu, iv, outflow, intOrder, inflow, wall):
+    m, o, vr, ev, far = _setup(p, rs, mu, iv, outflow, intOrder, inflow, wall)
     for nm in ["faceWeight", "matrixA", "matrixAAInvB", "vectorAInvB"]:
         assert relerr(vr.get(nm), o.get(nm)) < TOL, nm
     u0, uRec0 = perturbed_state(m, far, R=o.R)
