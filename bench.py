@@ -41,10 +41,10 @@ B_VR = 8 * (6 * 81 + 6 * 9) + 8 * (2 * 9 * 5 + 5)
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per cell of one k_rhs_face_fast launch (the face kernel: 97% of EvaluateRHS; the per-cell
 # gather adds ~4% more bytes), from the ncu capture of the same workload at 48^3 (dram__bytes_read.sum +
-# dram__bytes_write.sum = 268.0 MB for 110,592 cells); traffic grows in proportion to cells and faces, so
+# dram__bytes_write.sum = 273.1 MB for 110,592 cells); traffic grows in proportion to cells and faces, so
 # a 64^3 launch is scaled by the cell count
-RHS_TRAFFIC_PER_CELL = 268.0e6 / 48 ** 3
-RHS_FP64_PIPE_PCT = 31.4  # sm__pipe_fp64_cycles_active of the same capture
+RHS_TRAFFIC_PER_CELL = 273.1e6 / 48 ** 3
+RHS_FP64_PIPE_PCT = 30.5  # sm__pipe_fp64_cycles_active of the same capture
 # the reference's published TGV throughput for this path: 71.8 M cell-iterations/s on 10,240 CPU ranks
 REF_PUBLISHED_MCIPS = 71.8
 
