@@ -118,6 +118,9 @@ struct Quad;
 template <>
 struct Quad<float>
 {
+    using raw = float4;
+    static DNDSB_D raw load_raw(const float *p) { return *(const float4 *)p; }
+    static DNDSB_D real dot(const raw &v, const real (&w)[4]) { return (real)v.x * w[0] + (real)v.y * w[1] + (real)v.z * w[2] + (real)v.w * w[3]; }
     static DNDSB_D void load(const float *p, real (&o)[4])
     {
         float4 v = *(const float4 *)p;
@@ -134,6 +137,12 @@ struct Quad<float>
 template <>
 struct Quad<double>
 {
+    struct raw
+    {
+        double2 a, b;
+    };
+    static DNDSB_D raw load_raw(const double *p) { return raw{((const double2 *)p)[0], ((const double2 *)p)[1]}; }
+    static DNDSB_D real dot(const raw &v, const real (&w)[4]) { return v.a.x * w[0] + v.a.y * w[1] + v.b.x * w[2] + v.b.y * w[3]; }
     static DNDSB_D void load(const double *p, real (&o)[4])
     {
         double2 a = ((const double2 *)p)[0], b = ((const double2 *)p)[1];
@@ -194,14 +203,28 @@ DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmdot(int64_t n, int64_t ld,
             r += dr;
             r = r >= NV ? r - NV : r;
             const T *pv = Vc + 4 * q;
+            if (c0 + kKG <= ncol)
+            {
+                // a full group: every load issued (in its storage type) before the first use
+                typename Quad<T>::raw v[kKG];
 #pragma unroll
-            for (int k = 0; k < kKG; k++)
-                if (c0 + k < ncol)
-                {
-                    real v[4];
-                    Quad<T>::load(pv + k * ld, v);
-                    a[k] += v[0] * wv[0] + v[1] * wv[1] + v[2] * wv[2] + v[3] * wv[3];
-                }
+                for (int k = 0; k < kKG; k++)
+                    v[k] = Quad<T>::load_raw(pv + k * ld);
+#pragma unroll
+                for (int k = 0; k < kKG; k++)
+                    a[k] += Quad<T>::dot(v[k], wv);
+            }
+            else
+            {
+#pragma unroll
+                for (int k = 0; k < kKG; k++)
+                    if (c0 + k < ncol)
+                    {
+                        real v[4];
+                        Quad<T>::load(pv + k * ld, v);
+                        a[k] += v[0] * wv[0] + v[1] * wv[1] + v[2] * wv[2] + v[3] * wv[3];
+                    }
+            }
         }
 #pragma unroll
         for (int k = 0; k < kKG; k++)
