@@ -91,6 +91,10 @@ SIGNATURES = {
     "dndsb_vr_iter_jvp": [_P, _P, _P, _P, _P, _i, _P, _P],
     "dndsb_eval_rhs_vjp": [_P, _P, _P, _P, _P, _P, _P],
     "dndsb_eval_rhs_jvp": [_P, _P, _P, _P, _P, _P, _P],
+    "dndsb_vr_iter_vjp_coords": [_P, _P, _P, _P, _i, _P, _P],
+    "dndsb_vr_iter_jvp_coords": [_P, _P, _P, _P, _i, _P, _P],
+    "dndsb_eval_rhs_vjp_coords": [_P, _P, _P, _P, _P, _P],
+    "dndsb_eval_rhs_jvp_coords": [_P, _P, _P, _P, _P, _P],
     "dndsb_eval_get_array": [_P, ctypes.c_char_p, _D, _l, _I64],
     "dndsb_eval_set_delta_lambda": [_P, _P, _P],
     "dndsb_eval_evaluate_rhs_noalloc": [_P, _P, _P, _P, _P],

@@ -33,8 +33,9 @@ DNDSB_HD void bc_prim2cons(const T *P, T *U, real gamma)
 
 // ghost state UR of the boundary zone for the inner state UL and outward unit normal n;
 // false for a zone without a supported boundary type
-template <int NV, typename T>
-DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const T *UL, const real *n, T *UR)
+// n: real, or dual numbers of the same kind as T for derivatives with respect to the face geometry
+template <int NV, typename T, typename TN>
+DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const T *UL, const TN *n, T *UR)
 {
     if (zone < 0 || zone >= b.nZone)
         return false;
@@ -130,8 +131,8 @@ DNDSB_HD bool bc_value(const BoundaryD &b, int zone, const T *UL, const real *n,
 // the ghost state at a Gauss point with fixUL (USE_FIX_ZERO_SA_NUT_AT_WALL,
 // EulerEvaluator_EvaluateDt.hxx:2291-2296): on wall types the SA variable of both the inner
 // state (modified in place) and the ghost is set to zero
-template <int NV, typename T>
-DNDSB_HD bool bc_value_fix(const BoundaryD &b, int zone, T *UL, const real *n, T *UR)
+template <int NV, typename T, typename TN>
+DNDSB_HD bool bc_value_fix(const BoundaryD &b, int zone, T *UL, const TN *n, T *UR)
 {
     bool ok = bc_value<NV>(b, zone, UL, n, UR);
     if (ok && NV > 5 && (b.type[zone] == BC_WALL || b.type[zone] == BC_WALL_ISOTHERMAL))

@@ -24,6 +24,7 @@ struct dndsb_vr
     dndsb_mesh *mesh = nullptr;
     GeomD g;
     VRD vr;
+    CoordAdjWs coordWs; // node-coordinate derivatives: patches and shares, built on first use
     int *errWord = nullptr;
     bool metrics = false, base = false, coeff = false;
     int bndNVars = 0; // number of variables of the boundary table's values
@@ -306,6 +307,7 @@ extern "C"
                         (void *)v->vr.faceL, (void *)v->vr.AAInvB, (void *)v->vr.AInvb, (void *)v->vr.matA, (void *)v->vr.AAInvB32,
                         (void *)v->vr.AInvb32, (void *)v->vr.sweepCoef, (void *)v->vr.sweepCoef32, (void *)v->errWord, (void *)v->vr.bnd.type, (void *)v->vr.bnd.val})
             dev_free(p);
+        coords_ws_free(v->coordWs);
         delete v;
         return DNDSB_OK;
     }
@@ -458,6 +460,38 @@ extern "C"
         return status_msg(vr_vjp(v->mesh->d, v->g, v->vr, nVars, cot, uRec, u, vRec, vU, S(stream)), "dndsb_vr_iter_vjp");
     }
 
+    int dndsb_vr_iter_vjp_coords(dndsb_vr *v, const double *cot, const double *uRec, const double *u, int nVars, double *dX, void *stream)
+    {
+        if (!v || !cot || !uRec || !u || !dX)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp_coords: null argument");
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp_coords: call construct_rec_coeff first");
+        if (v->mesh->nBndFace > 0 && v->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp_coords: the mesh has boundary faces; set their boundary table first");
+        if (nVars != 5)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp_coords: needs nVars = 5");
+        int rc = coords_vjp(v->mesh->d, v->g, v->vr, nullptr, nullptr, v->coordWs, nullptr, cot, u, uRec, dX, v->errWord, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_vjp_coords: VR degree 1-2 in 3-D, 1-3 in 2-D");
+        return status_msg(rc, "dndsb_vr_iter_vjp_coords");
+    }
+
+    int dndsb_vr_iter_jvp_coords(dndsb_vr *v, const double *dX, const double *uRec, const double *u, int nVars, double *dRecNew, void *stream)
+    {
+        if (!v || !dX || !uRec || !u || !dRecNew)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: null argument");
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: call construct_rec_coeff first");
+        if (v->mesh->nBndFace > 0 && v->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: the mesh has boundary faces; set their boundary table first");
+        if (nVars != 5)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: needs nVars = 5");
+        int rc = coords_jvp(v->mesh->d, v->g, v->vr, nullptr, nullptr, dX, u, uRec, nullptr, dRecNew, v->errWord, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: VR degree 1-2 in 3-D, 1-3 in 2-D");
+        return status_msg(rc, "dndsb_vr_iter_jvp_coords");
+    }
+
     int dndsb_vr_iter_jvp(dndsb_vr *v, const double *dRec, const double *du, const double *uRec, const double *u, int nVars, double *dRecNew,
                           void *stream)
     {
@@ -593,6 +627,36 @@ extern "C"
         if (rc == ST_UNSUPPORTED)
             return fail(rc, "dndsb_eval_rhs_vjp: needs nVars = 5 and ignoreVis (the viscous flux is not differentiated yet)");
         return status_msg(rc, "dndsb_eval_rhs_vjp");
+    }
+
+    int dndsb_eval_rhs_vjp_coords(dndsb_eval *e, const double *w, const double *u, const double *uRec, double *dX, void *stream)
+    {
+        if (!e || !w || !u || !uRec || !dX)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp_coords: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp_coords: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        dndsb_vr *v = e->vr;
+        int rc = coords_vjp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, v->coordWs, w, nullptr, u, uRec, dX, e->e.errWord, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(rc, "dndsb_eval_rhs_vjp_coords: needs nVars = 5, ignoreVis, and VR degree 1-2 in 3-D, 1-3 in 2-D");
+        return status_msg(rc, "dndsb_eval_rhs_vjp_coords");
+    }
+
+    int dndsb_eval_rhs_jvp_coords(dndsb_eval *e, const double *dX, const double *u, const double *uRec, double *dRhs, void *stream)
+    {
+        if (!e || !dX || !u || !uRec || !dRhs)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp_coords: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp_coords: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        dndsb_vr *v = e->vr;
+        int rc = coords_jvp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, dX, u, uRec, dRhs, nullptr, e->e.errWord, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(rc, "dndsb_eval_rhs_jvp_coords: needs nVars = 5, ignoreVis, and VR degree 1-2 in 3-D, 1-3 in 2-D");
+        return status_msg(rc, "dndsb_eval_rhs_jvp_coords");
     }
 
     int dndsb_eval_rhs_jvp(dndsb_eval *e, const double *du, const double *duRec, const double *u, const double *uRec, double *dRhs, void *stream)

@@ -244,13 +244,18 @@ DNDSB_HD void quad_point(int elem, int order, int i, real p[3], real &w)
 // ---------------------------------------------------------------------------
 DNDSB_HD int elem_nnode(int e) { return e == E_LINE2 ? 2 : e == E_TRI3 ? 3 : e == E_HEX8 ? 8 : 4; }
 
-struct PtGeo
+// point and Jacobian of an element map; templated on the coordinate type (real, or dual numbers
+// for derivatives with respect to the node coordinates)
+template <typename T>
+struct PtGeoT
 {
-    real x[3];
-    real J[3][3]; // J[r][c] = d x_r / d xi_c
+    T x[3];
+    T J[3][3]; // J[r][c] = d x_r / d xi_c
 };
+using PtGeo = PtGeoT<real>;
 
-DNDSB_HD void pt_geo(int e, const real *cs /*nn x 3*/, const real p[3], PtGeo &g)
+template <typename T>
+DNDSB_HD void pt_geo(int e, const T *cs /*nn x 3*/, const real p[3], PtGeoT<T> &g)
 {
     real N[8], dN[3][8];
     int nn = elem_nnode(e);
@@ -297,10 +302,10 @@ DNDSB_HD void pt_geo(int e, const real *cs /*nn x 3*/, const real p[3], PtGeo &g
     }
     for (int r = 0; r < 3; r++)
     {
-        real s = 0, j0 = 0, j1 = 0, j2 = 0;
+        T s = 0, j0 = 0, j1 = 0, j2 = 0;
         for (int i = 0; i < nn; i++)
         {
-            real c = cs[i * 3 + r];
+            const T &c = cs[i * 3 + r];
             s += c * N[i], j0 += c * dN[0][i], j1 += c * dN[1][i], j2 += c * dN[2][i];
         }
         g.x[r] = s, g.J[r][0] = j0, g.J[r][1] = j1, g.J[r][2] = j2;
@@ -308,33 +313,35 @@ DNDSB_HD void pt_geo(int e, const real *cs /*nn x 3*/, const real p[3], PtGeo &g
 }
 
 // Geom/Quadrature.hpp:480-490 (cell) and :500-511 with Geom/Geometric.hpp:113-128 (face)
-DNDSB_HD real cell_jdet(int dim, const PtGeo &g)
+template <typename T>
+DNDSB_HD T cell_jdet(int dim, const PtGeoT<T> &g)
 {
     if (dim == 2)
     {
-        real c2 = g.J[0][0] * g.J[1][1] - g.J[1][0] * g.J[0][1];
-        real c0 = g.J[1][0] * g.J[2][1] - g.J[2][0] * g.J[1][1];
-        real c1 = g.J[2][0] * g.J[0][1] - g.J[0][0] * g.J[2][1];
+        T c2 = g.J[0][0] * g.J[1][1] - g.J[1][0] * g.J[0][1];
+        T c0 = g.J[1][0] * g.J[2][1] - g.J[2][0] * g.J[1][1];
+        T c1 = g.J[2][0] * g.J[0][1] - g.J[0][0] * g.J[2][1];
         return sqrt(c0 * c0 + c1 * c1 + c2 * c2);
     }
-    const real(*J)[3] = g.J;
+    const T(*J)[3] = g.J;
     return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
            J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
 }
 
 // returns |J| of the face map and writes the (unnormalised) normal
-DNDSB_HD real face_jdet_normal(int dim, const PtGeo &g, real n[3])
+template <typename T>
+DNDSB_HD T face_jdet_normal(int dim, const PtGeoT<T> &g, T n[3])
 {
     if (dim == 2)
     {
         n[0] = g.J[1][0], n[1] = -g.J[0][0], n[2] = 0;
         return sqrt(g.J[0][0] * g.J[0][0] + g.J[1][0] * g.J[1][0] + g.J[2][0] * g.J[2][0]);
     }
-    real a[3] = {g.J[0][0], g.J[1][0], g.J[2][0]}, b[3] = {g.J[0][1], g.J[1][1], g.J[2][1]};
+    T a[3] = {g.J[0][0], g.J[1][0], g.J[2][0]}, b[3] = {g.J[0][1], g.J[1][1], g.J[2][1]};
     n[0] = a[1] * b[2] - a[2] * b[1];
     n[1] = a[2] * b[0] - a[0] * b[2];
     n[2] = a[0] * b[1] - a[1] * b[0];
-    return sqrt(dot3(n, n));
+    return sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -401,9 +408,10 @@ DNDSB_HD real falling(int p, int d)
     return r;
 }
 
-DNDSB_HD real ipow(real x, int e)
+template <typename T>
+DNDSB_HD T ipow(const T &x, int e)
 {
-    real r = 1;
+    T r = 1;
     for (int i = 0; i < e; i++)
         r *= x;
     return r;
@@ -411,20 +419,25 @@ DNDSB_HD real ipow(real x, int e)
 
 // Diff table of the basis at scaled offset (x,y,z) = (p - cent) / L with
 // scales L; rows [0, rows), columns [0, NDOF).  Column 0 is the constant.
-template <int DIM, int NDOF>
-DNDSB_HD void basis_table(real *T, int rows, real x, real y, real z, const real L[3])
+template <int DIM, int NDOF, typename S>
+DNDSB_HD void basis_table(S *T, int rows, const S &x, const S &y, const S &z, const S L[3])
 {
     for (int r = 0; r < rows; r++)
     {
         int d[3];
         Basis<DIM>::exps(r, d);
-        real lscale = ipow(L[0], d[0]) * ipow(L[1], d[1]) * (DIM == 3 ? ipow(L[2], d[2]) : 1.0);
+        S lscale = ipow(L[0], d[0]) * ipow(L[1], d[1]);
+        if (DIM == 3)
+            lscale = lscale * ipow(L[2], d[2]);
         for (int k = 0; k < NDOF; k++)
         {
             int e[3];
             Basis<DIM>::exps(k, e);
             real c = falling(e[0], d[0]) * falling(e[1], d[1]) * falling(e[2], d[2]);
-            T[r * NDOF + k] = c == 0 ? 0.0 : c * ipow(x, e[0] - d[0]) * ipow(y, e[1] - d[1]) * ipow(z, e[2] - d[2]) / lscale;
+            if (c == 0)
+                T[r * NDOF + k] = 0.0;
+            else
+                T[r * NDOF + k] = c * ipow(x, e[0] - d[0]) * ipow(y, e[1] - d[1]) * ipow(z, e[2] - d[2]) / lscale;
         }
     }
 }
@@ -465,8 +478,8 @@ enum RSType : int
 template <typename T>
 DNDSB_HD real sign_tol(const T &a, const T &tol) { return a > tol ? 1 : (a < -tol ? -1 : 0); }
 
-template <typename T>
-DNDSB_HD T dot3v(const T *a, const real *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+template <typename T, typename TN>
+DNDSB_HD T dot3v(const T *a, const TN *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 template <typename T>
 DNDSB_HD T dot3s(const T *a, const T *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
@@ -503,8 +516,9 @@ DNDSB_HD void roe_average(const T *ULm, const T *URm, real gamma, RoeAvgT<T> &r)
 }
 
 // physical flux through n (no grid velocity): Gas.hpp:390-397
-template <typename T>
-DNDSB_HD void phys_flux(const T *U, const real *n, real gamma, T F[5], T &p, T &asqr)
+// n: real, or dual numbers of the same kind as T for derivatives with respect to the face geometry
+template <typename T, typename TN>
+DNDSB_HD void phys_flux(const T *U, const TN *n, real gamma, T F[5], T &p, T &asqr)
 {
     T ir = 1.0 / U[0];
     T v[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
@@ -525,8 +539,8 @@ struct RoeWavesT
     T a0, a1, a4, a23T[3], vRoeN;
 };
 
-template <typename T>
-DNDSB_HD void roe_waves(const T *incU, const real *n, const RoeAvgT<T> &r, real gamma, RoeWavesT<T> &w)
+template <typename T, typename TN>
+DNDSB_HD void roe_waves(const T *incU, const TN *n, const RoeAvgT<T> &r, real gamma, RoeWavesT<T> &w)
 {
     w.vRoeN = dot3v(r.v, n);
     T incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
@@ -541,8 +555,8 @@ DNDSB_HD void roe_waves(const T *incU, const real *n, const RoeAvgT<T> &r, real 
 }
 
 // |A| dU assembled from wave strengths times eigenvalues (Gas.hpp:1110-1124)
-template <typename T>
-DNDSB_HD void roe_dissipation(const RoeWavesT<T> &w, const real *n, const RoeAvgT<T> &r, const T &l0, const T &l123, const T &l4, T incF[5])
+template <typename T, typename TN>
+DNDSB_HD void roe_dissipation(const RoeWavesT<T> &w, const TN *n, const RoeAvgT<T> &r, const T &l0, const T &l123, const T &l4, T incF[5])
 {
     T a0 = w.a0 * l0, a1 = w.a1 * l123, a4 = w.a4 * l4;
     T t[3] = {w.a23T[0] * l123, w.a23T[1] * l123, w.a23T[2] * l123};
@@ -624,8 +638,8 @@ DNDSB_HD void roe_entropy_fix(int es, const T &aL, const T &aR, const T &aAve, c
 // Returns false when a state is non-physical (the caller records an error).
 // The Roe averages r come from the cell-mean states (Gas.hpp:229-259) and are
 // shared by all Gauss points of a face.
-template <typename T>
-DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T> &r, const real *n, real gamma, real dLambda, real fixScale,
+template <typename T, typename TN>
+DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T> &r, const TN *n, real gamma, real dLambda, real fixScale,
                                real incFScale, T F[5], T &lam0, T &lam123, T &lam4)
 {
     T FL[5], FR[5], pL, pR, aL2, aR2;
@@ -723,8 +737,8 @@ DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T
     return ok;
 }
 
-template <typename T>
-DNDSB_HD bool riemann_flux(int rs, const T *UL, const T *UR, const T *ULm, const T *URm, const real *n, real gamma, real dLambda,
+template <typename T, typename TN>
+DNDSB_HD bool riemann_flux(int rs, const T *UL, const T *UR, const T *ULm, const T *URm, const TN *n, real gamma, real dLambda,
                            real fixScale, real incFScale, T F[5], T &lam0, T &lam123, T &lam4)
 {
     RoeAvgT<T> r;

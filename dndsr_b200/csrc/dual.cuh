@@ -11,6 +11,7 @@ namespace dndsb
 {
 // keep the plain-real overloads visible next to the Dual ones below
 using ::fabs;
+using ::pow;
 using ::isfinite;
 using ::sqrt;
 
@@ -177,6 +178,17 @@ DNDSB_HD Dual<N> sqrt(const Dual<N> &a)
 }
 template <int N>
 DNDSB_HD Dual<N> fabs(const Dual<N> &a) { return a.v >= 0 ? a : -a; }
+// a^e for a real exponent: d(a^e) = e a^(e-1) da (zero derivative at a = 0)
+template <int N>
+DNDSB_HD Dual<N> pow(const Dual<N> &a, real e)
+{
+    Dual<N> r;
+    r.v = ::pow(a.v, e);
+    real s = a.v != 0 ? e * r.v / a.v : 0.0;
+    for (int i = 0; i < N; i++)
+        r.d[i] = s * a.d[i];
+    return r;
+}
 template <int N>
 DNDSB_HD bool isfinite(const Dual<N> &a) { return ::isfinite(a.v); }
 

@@ -373,44 +373,6 @@ DNDSB_D void functional_acc(const real *w2L /*per order*/, int maxOrd, const rea
     }
 }
 
-// Gauss-Jordan inverse with partial pivoting; false if singular
-template <int N>
-DNDSB_D bool invert_gj(real *A, real *Ai)
-{
-    for (int i = 0; i < N; i++)
-        for (int j = 0; j < N; j++)
-            Ai[i * N + j] = i == j ? 1.0 : 0.0;
-    for (int c = 0; c < N; c++)
-    {
-        int piv = c;
-        for (int r = c + 1; r < N; r++)
-            if (fabs(A[r * N + c]) > fabs(A[piv * N + c]))
-                piv = r;
-        if (A[piv * N + c] == 0)
-            return false;
-        if (piv != c)
-            for (int j = 0; j < N; j++)
-            {
-                real t = A[piv * N + j];
-                A[piv * N + j] = A[c * N + j], A[c * N + j] = t;
-                t = Ai[piv * N + j];
-                Ai[piv * N + j] = Ai[c * N + j], Ai[c * N + j] = t;
-            }
-        real id = 1.0 / A[c * N + c];
-        for (int j = 0; j < N; j++)
-            A[c * N + j] *= id, Ai[c * N + j] *= id;
-        for (int r = 0; r < N; r++)
-            if (r != c)
-            {
-                real fct = A[r * N + c];
-                if (fct != 0)
-                    for (int j = 0; j < N; j++)
-                        A[r * N + j] -= fct * A[c * N + j], Ai[r * N + j] -= fct * Ai[c * N + j];
-            }
-    }
-    return true;
-}
-
 template <int DIM, int P>
 DNDSB_D void face_w2L(const VRD &vr, int64_t f, real *w2L)
 {

@@ -210,6 +210,21 @@ int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const
 // ---- derivatives (adjoint.cu): VJP / JVP of EvaluateRHS and of one VR Jacobi sweep ----
 // deltaLambdaCell (the entropy-fix scale of the last EvaluateDt) is held fixed, as between the
 // reference's EvaluateDt and EvaluateRHS calls
+// ---- derivatives with respect to the node coordinates (adjoint_geom.cu) ----
+struct CoordAdjWs
+{
+    int maxSlot = 0;
+    int32_t *patch = nullptr;                 // [nCell][maxSlot] patch nodes of each cell, -1 padded
+    int64_t *start = nullptr, *ent = nullptr; // node -> (cell, slot) entries, CSR in entry order
+    real *share = nullptr;                    // [nCell][maxSlot][3]
+};
+int coords_ws_build(const MeshD &m, CoordAdjWs &ws);
+void coords_ws_free(CoordAdjWs &ws);
+// s == nullptr: the VR sweep only (w unused); otherwise EvaluateRHS (w) and/or the sweep (cot)
+int coords_vjp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, CoordAdjWs &ws, const real *w,
+               const real *cot, const real *u, const real *uRec, real *dX, int *errWord, cudaStream_t st);
+int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, const real *dX, const real *u,
+               const real *uRec, real *dRhs, real *dRec, int *errWord, cudaStream_t st);
 int rhs_vjp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *w, const real *u, const real *uRec, real *du, real *duRec,
             cudaStream_t st);
 int rhs_jvp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *du, const real *duRec, const real *u, const real *uRec,

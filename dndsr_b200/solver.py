@@ -187,6 +187,21 @@ class VariationalReconstruction(Handle):
                   _ptr(out, "dRecNew"), _stream())
         return out
 
+    def DoReconstructionIterVJPCoords(self, cot, uRec, u):
+        """(dS/dX)^T cot for one Jacobi sweep uRecNew = S(uRec, u; X), X the node coordinates
+        [nNode][3]: the geometry, basis moments, weights and A^-1 B / A^-1 b are differentiated."""
+        dX = torch.empty((self.mesh.n_node, 3), dtype=torch.float64, device="cuda")
+        capi.call("dndsb_vr_iter_vjp_coords", self.h, _ptr(cot, "cot"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1], _ptr(dX, "dX"),
+                  _stream())
+        return dX
+
+    def DoReconstructionIterJVPCoords(self, dX, uRec, u):
+        """dS/dX dX for one Jacobi sweep along the node displacement dX [nNode][3]."""
+        out = torch.empty_like(uRec)
+        capi.call("dndsb_vr_iter_jvp_coords", self.h, _ptr(dX, "dX"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1], _ptr(out, "dRecNew"),
+                  _stream())
+        return out
+
 
 class EulerEvaluator(Handle):
     """Euler::EulerEvaluator<model> on the GPU (models NS / NS_3D with 5 variables)."""
@@ -255,6 +270,19 @@ class EulerEvaluator(Handle):
         out = torch.empty_like(u)
         capi.call("dndsb_eval_rhs_jvp", self.h, _ptr(du, "du"), _ptr(duRec, "duRec"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(out, "dRhs"),
                   _stream())
+        return out
+
+    def EvaluateRHSVJPCoords(self, w, u, uRec):
+        """(dR/dX)^T w of EvaluateRHS with respect to the node coordinates X [nNode][3] (u, uRec
+        and deltaLambdaCell held fixed)."""
+        dX = torch.empty((self.vr.mesh.n_node, 3), dtype=torch.float64, device="cuda")
+        capi.call("dndsb_eval_rhs_vjp_coords", self.h, _ptr(w, "w"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dX"), _stream())
+        return dX
+
+    def EvaluateRHSJVPCoords(self, dX, u, uRec):
+        """dR/dX dX of EvaluateRHS along the node displacement dX [nNode][3]."""
+        out = torch.empty_like(u)
+        capi.call("dndsb_eval_rhs_jvp_coords", self.h, _ptr(dX, "dX"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(out, "dRhs"), _stream())
         return out
 
     def BuildJDiag(self):

@@ -144,6 +144,14 @@ int dndsb_vr_set_boundary(dndsb_vr *vr, int nZone, const int32_t *type, const do
 int dndsb_vr_iter_vjp(dndsb_vr *vr, const double *cot, const double *uRec, const double *u, int nVars, double *vRec, double *vU, void *stream);
 int dndsb_vr_iter_jvp(dndsb_vr *vr, const double *dRec, const double *du, const double *uRec, const double *u, int nVars, double *dRecNew,
                       void *stream);
+/* Derivatives of the same sweep with respect to the mesh node coordinates X [nNode][3] (uRec and u
+ * held fixed): the cell metrics and basis moments (FiniteVolume.cpp:22-648,
+ * VariationalReconstruction.cpp:56-498), the face weights and A^-1 B / A^-1 b (:507-872) and the
+ * boundary term are recomputed per cell in dual numbers.  vjp: cot [nCell][R][5] -> dX = (dS/dX)^T cot;
+ * jvp: dX -> dRecNew = dS/dX dX.  5 variables; VR degree 1-2 in 3-D, 1-3 in 2-D.  The first call
+ * builds the per-cell node patches (a device-to-host copy of the topology, then device buffers). */
+int dndsb_vr_iter_vjp_coords(dndsb_vr *vr, const double *cot, const double *uRec, const double *u, int nVars, double *dX, void *stream);
+int dndsb_vr_iter_jvp_coords(dndsb_vr *vr, const double *dX, const double *uRec, const double *u, int nVars, double *dRecNew, void *stream);
 
 /* ---- Euler evaluator: EulerEvaluator.hpp:76-1980 ---- */
 int dndsb_eval_create(dndsb_eval **out, dndsb_vr *vr, const dndsb_euler_settings *s);
@@ -185,6 +193,12 @@ int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *
  * reference has no hand-written adjoint of this path (its Python package differentiates nothing). */
 int dndsb_eval_rhs_vjp(dndsb_eval *ev, const double *w, const double *u, const double *uRec, double *du, double *duRec, void *stream);
 int dndsb_eval_rhs_jvp(dndsb_eval *ev, const double *du, const double *duRec, const double *u, const double *uRec, double *dRhs, void *stream);
+/* Derivatives of EvaluateRHS with respect to the mesh node coordinates X [nNode][3] (u, uRec and
+ * deltaLambdaCell held fixed; geometry, basis and face points, normals and Jacobians recomputed per
+ * cell in dual numbers): vjp: w [nCell][5] -> dX = (dR/dX)^T w; jvp: dX -> dRhs.  Inviscid
+ * (ignoreVis) 5-variable models; VR degree 1-2 in 3-D, 1-3 in 2-D. */
+int dndsb_eval_rhs_vjp_coords(dndsb_eval *ev, const double *w, const double *u, const double *uRec, double *dX, void *stream);
+int dndsb_eval_rhs_jvp_coords(dndsb_eval *ev, const double *dX, const double *u, const double *uRec, double *dRhs, void *stream);
 
 /* Adjoint building blocks (no reference counterpart; they transpose the operators above).
  * lusgs_matrix_vec_t: ATy = A^T y for the operator A of dndsb_eval_lusgs_matrix_vec (same lambdaFace,

@@ -2466,6 +2466,7 @@ extern "C"
         else if (n == "cellPP") v = &o->cellPP;
         else if (n == "cellHMax") v = &o->cellHMax;
         else if (n == "jSource") v = &o->jSource;
+        else if (n == "deltaLambdaCell") v = &o->deltaLambdaCell;
         else if (n == "faceCent") v = &o->faceCent;
         else if (n == "faceJDet") v = &o->faceJDet;
         else if (n == "facePP") v = &o->facePP;
