@@ -167,6 +167,15 @@ class SteadyAdjoint:
         x, hist = gmres(self.op_T, self.prec_T, (gU.contiguous(), gRec.contiguous()), **kw)
         return x[0], x[1], hist
 
+    def shape_gradient(self, psi, lam, dJdX=None):
+        """dJ/dX for the node coordinates X [nNode][3] at the converged state: the residuals R(u, uRec; X)
+        stay zero, so dJ/dX = dJ/dX|_state - psi^T dR_u/dX - lam^T dS/dX (the time term of the implicit
+        step and -uRec do not depend on X).  dJdX: the objective's own derivative (e.g.
+        ``ev.PressureForceCoords``), or None for an objective of the state only."""
+        g = self.ev.EvaluateRHSVJPCoords(psi.contiguous(), self.u, self.uRec)
+        g = g + self.vr.DoReconstructionIterVJPCoords(lam.contiguous(), self.uRec, self.u)
+        return -g if dJdX is None else dJdX - g
+
     def solve_tangent(self, sU, sRec, **kw):
         """(du, dRec) with A (du, dRec) = -(sU, sRec): the state response to a residual source."""
         x, hist = gmres(self.op, self.prec, (-sU.contiguous(), -sRec.contiguous()), **kw)

@@ -8,6 +8,8 @@ namespace dndsb
 {
 extern template void coords_vjp_launch<2>(const MeshD &, const GeomD &, const VRD &, const EulerSettingsD &, const real *, const real *,
                                           const real *, const real *, const real *, const CoordAdjWs &, int *, cudaStream_t);
+extern template void pressure_force_coords_launch<2>(const MeshD &, const GeomD &, const VRD &, real, int, const real *, const real *,
+                                                     const real *, const CoordAdjWs &, cudaStream_t);
 extern template void coords_jvp_launch<2>(const MeshD &, const GeomD &, const VRD &, const EulerSettingsD &, const real *, const real *,
                                           const real *, const real *, real *, real *, int *, cudaStream_t);
 
@@ -131,6 +133,25 @@ int coords_vjp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSetting
         coords_vjp_launch<3>(m, g, vr, es, dLamCell, u, uRec, w, cot, ws, errWord, st);
     DNDSB_LAUNCH(k_node_gather, m.nNode, 256, st, m.nNode, ws.start, ws.ent, ws.share, dX);
     return geo_status(st, errWord);
+}
+
+int pressure_force_coords(const MeshD &m, const GeomD &g, const VRD &vr, real gamma, int zone, const real *dir, const real *u, const real *uRec,
+                          CoordAdjWs &ws, real *dX, cudaStream_t st)
+{
+    if (!geo_supported(m, vr))
+        return ST_UNSUPPORTED;
+    int rc = coords_ws_build(m, ws);
+    if (rc != ST_OK)
+        return rc;
+    dev_zero(ws.share, sizeof(real) * 3 * m.nCell * ws.maxSlot, st);
+    if (m.dim == 2)
+        pressure_force_coords_launch<2>(m, g, vr, gamma, zone, dir, u, uRec, ws, st);
+    else
+        pressure_force_coords_launch<3>(m, g, vr, gamma, zone, dir, u, uRec, ws, st);
+    DNDSB_LAUNCH(k_node_gather, m.nNode, 256, st, m.nNode, ws.start, ws.ent, ws.share, dX);
+    if (last_error() != cudaSuccess || dev_sync(st) != cudaSuccess)
+        return ST_CUDA;
+    return ST_OK;
 }
 
 int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, const real *dX, const real *u,

@@ -563,7 +563,87 @@ DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_jvp(MeshD m, GeomD g, VR
             atomicOr(err, (int)DE_NONPHYSICAL);
     }
 }
+// Share of one (boundary cell, cell vertex) in the derivative of the pressure force
+// J = sum over the zone's faces and points of p(U) (n . dir) |J| w (k_pressure_force) with respect to
+// the vertex coordinates: the cell's basis and its faces' geometry depend on its own nodes only.
+// Written into the patch slot of that node in the cell's own patch (a node met twice in a cell, as
+// periodic images, is seeded once).
+template <int DIM, int P>
+DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_pressure_force_coords(MeshD m, GeomD g, VRD vr, real gamma, int zone, real d0, real d1, real d2,
+                                                                       const real *__restrict__ u, const real *__restrict__ uRec,
+                                                                       const int32_t *__restrict__ patch, int maxSlot, real *__restrict__ share)
+{
+    constexpr int NV = 5, NDOF = ndof_of<DIM>(P), R = NDOF - 1;
+    DNDSB_KERNEL_LOOP(e, m.nBndCell * m.nvert)
+    {
+        const int64_t ii = e / m.nvert;
+        const int v = (int)(e - ii * m.nvert);
+        const int64_t c = m.bndCell[ii];
+        const int32_t node = m.cell2node[c * m.nvert + v];
+        bool dup = false;
+        for (int v2 = 0; v2 < v; v2++)
+            dup = dup || m.cell2node[c * m.nvert + v2] == node;
+        int slot = 0;
+        while (slot < maxSlot && patch[c * maxSlot + slot] != node)
+            slot++;
+        if (dup || slot == maxSlot)
+            continue;
+        SeedNode sd{node};
+        const bool aniso = vr.s.anisotropicLengths;
+        CellG<Dual<3>, NDOF> gc;
+        bool any = false;
+        Dual<3> J = 0.0;
+        for (int k = 0; k < m.nf; k++)
+        {
+            if (m.cellNbr[c * m.nf + k] >= 0)
+                continue;
+            const int64_t f = m.cell2face[c * m.nf + k] >> 1;
+            if (m.faceZone[f] != zone)
+                continue;
+            if (!any)
+                cell_geo<DIM, NDOF>(m, vr.s.intOrder, g.nGc, aniso, c, sd, gc);
+            any = true;
+            FaceG<Dual<3>> fg;
+            face_geo(m, vr.s.intOrder, g.nGf, f, sd, fg);
+            for (int q = 0; q < g.nGf; q++)
+            {
+                Dual<3> pp[3], nrm[3], JW, T0[NDOF];
+                face_point(m, vr.s.intOrder, fg, q, g.faceQw[q], pp, nrm, JW);
+                cell_basis<DIM, NDOF>(gc.cent, gc.scale, gc.moment, aniso, pp, 1, T0);
+                Dual<3> UL[NV];
+                for (int w = 0; w < NV; w++)
+                {
+                    Dual<3> a = 0.0;
+                    for (int j = 0; j < R; j++)
+                        a += T0[1 + j] * uRec[(c * R + j) * NV + w];
+                    UL[w] = u[c * NV + w] + a;
+                }
+                Dual<3> vel[3] = {UL[1] / UL[0], UL[2] / UL[0], UL[3] / UL[0]};
+                Dual<3> pr = (gamma - 1) * (UL[4] - 0.5 * UL[0] * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]));
+                Dual<3> wt = JW * (nrm[0] * d0 + nrm[1] * d1 + nrm[2] * d2);
+                J += wt * pr;
+            }
+        }
+        for (int d = 0; d < 3; d++)
+            share[(c * maxSlot + slot) * 3 + d] = J.d[d];
+    }
+}
 } // namespace
+
+template <int DIM>
+void pressure_force_coords_launch(const MeshD &m, const GeomD &g, const VRD &vr, real gamma, int zone, const real *dir, const real *u,
+                                  const real *uRec, const CoordAdjWs &ws, cudaStream_t st)
+{
+    constexpr int PTop = DIM == 2 ? 3 : 2;
+    const int64_t n = m.nBndCell * m.nvert;
+    if (vr.P == 1)
+        DNDSB_LAUNCH((k_pressure_force_coords<DIM, 1>), n, kGeoBlock, st, m, g, vr, gamma, zone, dir[0], dir[1], dir[2], u, uRec, ws.patch, ws.maxSlot, ws.share);
+    else if (vr.P == 2)
+        DNDSB_LAUNCH((k_pressure_force_coords<DIM, 2>), n, kGeoBlock, st, m, g, vr, gamma, zone, dir[0], dir[1], dir[2], u, uRec, ws.patch, ws.maxSlot, ws.share);
+    else
+        DNDSB_LAUNCH((k_pressure_force_coords<DIM, PTop>), n, kGeoBlock, st, m, g, vr, gamma, zone, dir[0], dir[1], dir[2], u, uRec, ws.patch,
+                     ws.maxSlot, ws.share);
+}
 
 // launches for one dimension; P = 1, 2 (and 3 in 2-D)
 template <int DIM>

@@ -721,6 +721,22 @@ extern "C"
                           "dndsb_eval_update_sgs_t");
     }
 
+    int dndsb_eval_pressure_force_coords(dndsb_eval *e, int zone, const double *dir, const double *u, const double *uRec, double *dJdX,
+                                         void *stream)
+    {
+        if (!e || !dir || !u || !uRec || !dJdX)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_pressure_force_coords: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_pressure_force_coords: VR not constructed");
+        if (e->e.s.nVars != 5)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_pressure_force_coords: needs nVars = 5");
+        dndsb_vr *v = e->vr;
+        int rc = pressure_force_coords(v->mesh->d, v->g, v->vr, e->e.s.gamma, zone, dir, u, uRec, v->coordWs, dJdX, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_pressure_force_coords: VR degree 1-2 in 3-D, 1-3 in 2-D");
+        return status_msg(rc, "dndsb_eval_pressure_force_coords");
+    }
+
     int dndsb_eval_pressure_force(dndsb_eval *e, int zone, const double *dir, const double *u, const double *uRec, double *Jhost, double *dJdu,
                                   double *dJduRec, void *stream)
     {

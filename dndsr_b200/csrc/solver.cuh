@@ -225,6 +225,9 @@ int coords_vjp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSetting
                const real *cot, const real *u, const real *uRec, real *dX, int *errWord, cudaStream_t st);
 int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, const real *dX, const real *u,
                const real *uRec, real *dRhs, real *dRec, int *errWord, cudaStream_t st);
+// d/dX of the pressure force of one boundary zone along dir (pressure_force's objective)
+int pressure_force_coords(const MeshD &m, const GeomD &g, const VRD &vr, real gamma, int zone, const real *dir, const real *u, const real *uRec,
+                          CoordAdjWs &ws, real *dX, cudaStream_t st);
 int rhs_vjp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *w, const real *u, const real *uRec, real *du, real *duRec,
             cudaStream_t st);
 int rhs_jvp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *du, const real *duRec, const real *u, const real *uRec,

@@ -328,6 +328,14 @@ class EulerEvaluator(Handle):
                   _ptr(gU, "dJdu") if grad else None, _ptr(gR, "dJduRec") if grad else None, _stream())
         return (float(J[0]), gU, gR) if grad else float(J[0])
 
+    def PressureForceCoords(self, zone, direction, u, uRec):
+        """Derivative of PressureForce with respect to the node coordinates [nNode][3] (u, uRec held fixed)."""
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        dX = torch.empty((self.vr.mesh.n_node, 3), dtype=torch.float64, device="cuda")
+        capi.call("dndsb_eval_pressure_force_coords", self.h, int(zone), capi.dptr(d), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dJdX"),
+                  _stream())
+        return dX
+
     def SolveLinear(self, alphaDiag, dTau, dt, u, rhs, xInc, gmresCode=0, jacobiCode=1, sgsIter=0, nGmresSpace=5, nGmresIter=1,
                     precision="fp64", meanScale=None, useGraph=True):
         """EulerSolver::solveLinear with LUSGSMatrixInit (EulerSolver.hxx:1407-1579, EulerEvaluator.hxx:37-159):

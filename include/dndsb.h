@@ -216,6 +216,11 @@ int dndsb_eval_update_sgs_t(dndsb_eval *ev, double alphaDiag, const void *b, con
  * receive its gradient, zero away from the zone. */
 int dndsb_eval_pressure_force(dndsb_eval *ev, int zone, const double *dir, const double *u, const double *uRec, double *Jhost, double *dJdu,
                               double *dJduRec, void *stream);
+/* Derivative of the same objective with respect to the mesh node coordinates X [nNode][3] (u and uRec
+ * held fixed): the cell's basis and the face points, normals and Jacobians differentiated.  With the
+ * adjoint (psi, lam) of the coupled residual, the shape gradient is
+ * dJ/dX = dJdX - dndsb_eval_rhs_vjp_coords(psi) - dndsb_vr_iter_vjp_coords(lam). */
+int dndsb_eval_pressure_force_coords(dndsb_eval *ev, int zone, const double *dir, const double *u, const double *uRec, double *dJdX, void *stream);
 
 /* Linear-solver controls, EulerSolver.hpp linearSolverControl (fields of the same names) plus the
  * precision of the solve.  meanScale: the GMRES dot weights of EulerSolver.hxx:1518-1540

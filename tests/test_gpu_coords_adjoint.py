@@ -136,3 +136,46 @@ def test_coordinate_derivatives_unsupported_cases_fail_loudly():
     uRec = torch.zeros((m.n_cell, vr.R, 5), dtype=torch.float64, device="cuda")
     with pytest.raises(capi.DndsbError):
         ev.EvaluateRHSVJPCoords(torch.ones_like(u), u, uRec)
+
+
+BUMP = M.BUMP_ZONES["bump"]
+DRAG = np.array([1.0, 0.0, 0.0])
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_pressure_force_coordinate_derivative_against_finite_differences(p):
+    m, o, vr, ev, u0, uRec0, u, uRec, X, at, scale, sv = _setup("bump", p, "Roe")
+    dX = ev.PressureForceCoords(BUMP, DRAG, u, uRec).cpu().numpy()
+    assert np.abs(dX).max() > 0
+    rng = np.random.default_rng(29)
+    h = 1e-5
+    worst = 0.0
+    for _ in range(64):
+        V = rng.normal(size=X.shape) * scale
+        fd = (at(X + h * V).pressure_force(BUMP, DRAG, u0, uRec0) - at(X - h * V).pressure_force(BUMP, DRAG, u0, uRec0)) / (2 * h)
+        worst = max(worst, abs(float((dX * V).sum()) - fd) / abs(fd))
+    assert worst < 1e-6, worst
+
+
+def test_shape_gradient_of_the_pressure_drag_against_the_tangent_response():
+    """dJ/dX = dJ/dX|_state - psi^T dR_u/dX - lam^T dS/dX from one adjoint solve against
+    <dJ/dX|_state, v> + <g, d>, with d the tangent response A d = -(dR/dX) v, in 3 directions."""
+    from dndsr_b200.adjoint import SteadyAdjoint
+    m, o, vr, ev, u0, uRec0, u, uRec, X, at, scale, sv = _setup("bump", 1, "Roe")
+    dTau = torch.zeros(m.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dTau, u, 1.0)
+    adj = SteadyAdjoint(vr, ev, u, uRec, cfl=5.0, dt=5.0 * float(dTau.max()))
+    J, gU, gR = ev.PressureForce(BUMP, DRAG, u, uRec, grad=True)
+    psi, lam, h_adj = adj.solve_adjoint(gU, gR, restart=40, max_restarts=60, rtol=1e-11)
+    assert h_adj[-1] < 1e-11
+    dJdX = ev.PressureForceCoords(BUMP, DRAG, u, uRec)
+    G = adj.shape_gradient(psi, lam, dJdX)
+    rng = np.random.default_rng(31)
+    for _ in range(3):
+        V = torch.tensor(rng.normal(size=X.shape) * scale, device="cuda")
+        sU = ev.EvaluateRHSJVPCoords(V, u, uRec)
+        sR = vr.DoReconstructionIterJVPCoords(V, uRec, u)
+        du, dRec, h_tan = adj.solve_tangent(sU, sR, restart=40, max_restarts=60, rtol=1e-11)
+        assert h_tan[-1] < 1e-11
+        tangent = float((dJdX * V).sum() + (gU * du).sum() + (gR * dRec).sum())
+        assert abs(float((G * V).sum()) - tangent) < 1e-8 * abs(tangent)
