@@ -83,6 +83,9 @@ SIGNATURES = {
     "dndsb_eval_update_sgs_t": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _P],
     "dndsb_eval_pressure_force": [_P, _i, _D, _P, _P, _D, _P, _P, _P],
     "dndsb_eval_pressure_force_coords": [_P, _i, _D, _P, _P, _P, _P],
+    "dndsb_eval_cell_rhs_alpha": [_P, _P, _P, _P, _d, _d, _d, _i, _d, _i, _i, _P, _P, _P],
+    "dndsb_eval_cell_rhs_alpha_expansion": [_P, _P, _P, _P, _d, _d, _d, _P],
+    "dndsb_eval_add_fixed_increment": [_P, _P, _P, _d, _d, _d, _i, _P, _P],
     "dndsb_eval_evaluate_norm": [_P, _P, _i, _i, _D, _P],
     "dndsb_eval_solve_linear": [_P, _P, _d, _P, _d, _P, _P, _P, _P],
     "dndsb_vr_set_boundary": [_P, _i, _I32, _D, _i, _d, _d],

@@ -721,6 +721,41 @@ extern "C"
                           "dndsb_eval_update_sgs_t");
     }
 
+    int dndsb_eval_cell_rhs_alpha(dndsb_eval *e, const double *u, const double *res, double *alpha, double refRho, double refP, double relax,
+                                  int compress, double compressPower, int ppEpsIsRelaxed, int flag, int64_t *nLimHost, double *alphaMinHost,
+                                  void *stream)
+    {
+        if (!e || !u || !res || !alpha)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_cell_rhs_alpha: null argument");
+        if (!(refRho > 0 && refP > 0))
+            return fail(DNDSB_E_BADARG, "dndsb_eval_cell_rhs_alpha: refRho and refP must be positive");
+        if (ppEpsIsRelaxed && !(relax < 1))
+            return fail(DNDSB_E_BADARG, "dndsb_eval_cell_rhs_alpha: relaxed floors need relax < 1");
+        int rc = cell_rhs_alpha(e->vr->mesh->d, e->e, u, res, alpha, refRho, refP, relax, compress, compressPower, ppEpsIsRelaxed, flag, nLimHost,
+                                alphaMinHost, S(stream));
+        return status_msg(rc, "dndsb_eval_cell_rhs_alpha");
+    }
+
+    int dndsb_eval_cell_rhs_alpha_expansion(dndsb_eval *e, const double *u, const double *res, double *alpha, double refRho, double refP,
+                                            double alphaMin, void *stream)
+    {
+        if (!e || !u || !res || !alpha)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_cell_rhs_alpha_expansion: null argument");
+        return status_msg(cell_rhs_alpha_expansion(e->vr->mesh->d, e->e, u, res, alpha, refRho, refP, alphaMin, S(stream)),
+                          "dndsb_eval_cell_rhs_alpha_expansion");
+    }
+
+    int dndsb_eval_add_fixed_increment(dndsb_eval *e, double *u, const double *inc, double alpha, double refRho, double refP, int ppEpsIsRelaxed,
+                                       double *alphaFixMinHost, void *stream)
+    {
+        if (!e || !u || !inc)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_add_fixed_increment: null argument");
+        if (!(refRho > 0 && refP > 0))
+            return fail(DNDSB_E_BADARG, "dndsb_eval_add_fixed_increment: refRho and refP must be positive");
+        return status_msg(add_fixed_increment(e->vr->mesh->d, e->e, u, inc, alpha, refRho, refP, ppEpsIsRelaxed, alphaFixMinHost, S(stream)),
+                          "dndsb_eval_add_fixed_increment");
+    }
+
     int dndsb_eval_pressure_force_coords(dndsb_eval *e, int zone, const double *dir, const double *u, const double *uRec, double *dJdX,
                                          void *stream)
     {

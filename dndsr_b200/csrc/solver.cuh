@@ -210,6 +210,14 @@ int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const
 // ---- derivatives (adjoint.cu): VJP / JVP of EvaluateRHS and of one VR Jacobi sweep ----
 // deltaLambdaCell (the entropy-fix scale of the last EvaluateDt) is held fixed, as between the
 // reference's EvaluateDt and EvaluateRHS calls
+// ---- positivity-preserving increment limiting (positivity.cu) ----
+int cell_rhs_alpha(const MeshD &m, EvalD &ev, const real *u, const real *res, real *alpha, real refRho, real refP, real relax, int compress,
+                   real compressPower, int ppEpsIsRelaxed, int flag, int64_t *nLim, real *alphaMin, cudaStream_t st);
+int cell_rhs_alpha_expansion(const MeshD &m, EvalD &ev, const real *u, const real *res, real *alpha, real refRho, real refP, real alphaMin,
+                             cudaStream_t st);
+int add_fixed_increment(const MeshD &m, EvalD &ev, real *u, const real *inc, real alpha, real refRho, real refP, int ppEpsIsRelaxed,
+                        real *alphaFixMin, cudaStream_t st);
+
 // ---- derivatives with respect to the node coordinates (adjoint_geom.cu) ----
 struct CoordAdjWs
 {

@@ -201,6 +201,12 @@ class SolverConfig:
     vr_precision: str = "fp64"       # coefficient precision of the VR sweeps
     native_linear: bool = True       # one device call per linear solve (dndsb_eval_solve_linear) when the evaluator has it
     meanScale: tuple = ()            # GMRES dot weights (gmresScale), empty = ones
+    # positivity-preserving increments (timeMarchControl.incrementPPRelax, uRecAlphaCompressPower,
+    # ppEpsIsRelaxed); the floors scale with the far-field state, empty = plain u += alpha inc
+    farFieldStaticValue: tuple = ()
+    incrementPPRelax: float = 0.9
+    uRecAlphaCompressPower: float = 1.0
+    ppEpsIsRelaxed: bool = False
     res_history: list = field(default_factory=list)
 
 
@@ -221,6 +227,15 @@ class ImplicitSolver:
         self.CFLNow = cfg.CFL
         self.n_rhs = 0
         self.n_sgs = 0
+        self.pp = None
+        if cfg.farFieldStaticValue:
+            far = [float(x) for x in cfg.farFieldStaticValue]
+            gamma = float(ev.settings["gamma"])
+            rho = far[0]
+            self.pp = (rho, (gamma - 1) * (far[4] - 0.5 * (far[1] ** 2 + far[2] ** 2 + far[3] ** 2) / rho))
+            self.alphaPP = torch.ones(nc, dtype=torch.float64, device=dev)
+            self.incPP = torch.zeros((nc, nv), dtype=torch.float64, device=dev)
+            self.nLimInc, self.alphaMinInc = 0, 1.0
 
     # EulerSolver.hxx:147-672 (VR sweeps then EvaluateRHS)
     def frhs(self, crhs, cx, dtau, it, ct):
@@ -234,9 +249,17 @@ class ImplicitSolver:
         self.ev.EvaluateDt(dtau, cx, self.CFLNow, 1e100, self.cfg.useLocalDt)
         dtau.mul_(1.0 / alphaDiag)
 
-    # EulerSolver.hxx:696-738 without the positivity limiting (AddFixedIncrement with alpha = 1)
+    # EulerSolver.hxx:696-738: EvaluateCellRHSAlpha, then AddFixedIncrement of alphaPP * inc (with a
+    # far-field state); without one, u += alpha inc
     def fincrement(self, cx, cxInc, alpha):
-        cx.add_(cxInc, alpha=alpha)
+        if self.pp is None:
+            cx.add_(cxInc, alpha=alpha)
+            return
+        cfg, (refRho, refP) = self.cfg, self.pp
+        self.nLimInc, self.alphaMinInc = self.ev.EvaluateCellRHSAlpha(cx, cxInc, self.alphaPP, refRho, refP, cfg.incrementPPRelax, 2,
+                                                                     cfg.uRecAlphaCompressPower, cfg.ppEpsIsRelaxed, 0)
+        torch.mul(cxInc, self.alphaPP[:, None], out=self.incPP)
+        self.ev.AddFixedIncrement(cx, self.incPP, alpha, refRho, refP, cfg.ppEpsIsRelaxed)
 
     def _sgs_pair(self, alphaDiag, rhs, cx, xinc):
         """doPrecondition, EulerSolver.hxx:1605-1635: forward then backward sweep."""

@@ -328,6 +328,30 @@ class EulerEvaluator(Handle):
                   _ptr(gU, "dJdu") if grad else None, _ptr(gR, "dJduRec") if grad else None, _stream())
         return (float(J[0]), gU, gR) if grad else float(J[0])
 
+    # positivity-preserving increment limiting (EulerSolver.hxx:696-738)
+    def EvaluateCellRHSAlpha(self, u, res, alpha, refRho, refP, relax=0.9, compress=2, compressPower=1.0, ppEpsIsRelaxed=False, flag=0):
+        """EulerEvaluator.hxx:1938-2062: alpha [nCell] (written in place) so that u + alpha res keeps the
+        relaxed density and pressure floors; returns (nLim, alphaMin).  refRho, refP: far-field density
+        and pressure (refUPrim); flag 1 = MIN_IF_NOT_ONE, 2 = MIN_ALL."""
+        n, amin = ctypes.c_int64(), ctypes.c_double()
+        capi.call("dndsb_eval_cell_rhs_alpha", self.h, _ptr(u, "u"), _ptr(res, "res"), _ptr(alpha, "alpha"), float(refRho), float(refP),
+                  float(relax), int(compress), float(compressPower), int(bool(ppEpsIsRelaxed)), int(flag), ctypes.addressof(n),
+                  ctypes.addressof(amin), _stream())
+        return int(n.value), float(amin.value)
+
+    def EvaluateCellRHSAlphaExpansion(self, u, res, alpha, refRho, refP, alphaMin):
+        """EulerEvaluator.hxx:2064-2140: alpha = alphaMin where u + res leaves the floors."""
+        capi.call("dndsb_eval_cell_rhs_alpha_expansion", self.h, _ptr(u, "u"), _ptr(res, "res"), _ptr(alpha, "alpha"), float(refRho),
+                  float(refP), float(alphaMin), _stream())
+
+    def AddFixedIncrement(self, u, inc, alpha, refRho, refP, ppEpsIsRelaxed=False):
+        """EulerEvaluator.hpp:1795-1857: u += CompressInc(u, alpha inc) in place; returns the smallest
+        density-increment ratio the compression applied."""
+        amin = ctypes.c_double()
+        capi.call("dndsb_eval_add_fixed_increment", self.h, _ptr(u, "u"), _ptr(inc, "inc"), float(alpha), float(refRho), float(refP),
+                  int(bool(ppEpsIsRelaxed)), ctypes.addressof(amin), _stream())
+        return float(amin.value)
+
     def PressureForceCoords(self, zone, direction, u, uRec):
         """Derivative of PressureForce with respect to the node coordinates [nNode][3] (u, uRec held fixed)."""
         d = np.ascontiguousarray(direction, dtype=np.float64)

@@ -186,6 +186,25 @@ int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, c
 /* LUSGSMatrixVec(alphaDiag, t, u, uInc, JDiag, AuInc), EulerEvaluator.hxx:175-274 */
 int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
                                 double *AuInc, void *stream);
+/* Positivity-preserving increment limiting of the implicit update (EulerSolver.hxx:696-738).
+ * refRho, refP: the reference's refUPrim(0), refUPrim(I4) (far-field density and pressure), which set
+ * the floors rhoEps = 1e-11 refRho, pEps = 1e-11 refP.  A state for which the reference asserts returns
+ * DNDSB_E_NONPHYSICAL.  Each call synchronises its stream to return its counts.
+ * cell_rhs_alpha: EvaluateCellRHSAlpha(u, uRec, uRecBeta, res, cellRHSAlpha, nLim, alphaMin, relax,
+ *   compress, flag) (EulerEvaluator.hxx:1938-2062; uRec and uRecBeta are not read there): alpha [nCell]
+ *   with u + alpha res inside the relaxed floors; flag 1 = MIN_IF_NOT_ONE, 2 = MIN_ALL; compressPower is
+ *   the settings' uRecAlphaCompressPower.  nLimHost, alphaMinHost may be NULL.
+ * cell_rhs_alpha_expansion: EvaluateCellRHSAlphaExpansion (EulerEvaluator.hxx:2064-2140).
+ * add_fixed_increment: AddFixedIncrement(cx, cxInc, alpha) (EulerEvaluator.hpp:1795-1857),
+ *   u += CompressInc(u, alpha inc); alphaFixMinHost (may be NULL) = the smallest density-increment ratio. */
+int dndsb_eval_cell_rhs_alpha(dndsb_eval *ev, const double *u, const double *res, double *alpha, double refRho, double refP, double relax,
+                              int compress, double compressPower, int ppEpsIsRelaxed, int flag, int64_t *nLimHost, double *alphaMinHost,
+                              void *stream);
+int dndsb_eval_cell_rhs_alpha_expansion(dndsb_eval *ev, const double *u, const double *res, double *alpha, double refRho, double refP,
+                                        double alphaMin, void *stream);
+int dndsb_eval_add_fixed_increment(dndsb_eval *ev, double *u, const double *inc, double alpha, double refRho, double refP, int ppEpsIsRelaxed,
+                                   double *alphaFixMinHost, void *stream);
+
 /* Derivatives of EvaluateRHS (EulerEvaluator_EvaluateRHS.hxx:55-818) with respect to the cell
  * means u and the reconstruction uRec, at the deltaLambdaCell of the last evaluate_dt (held
  * fixed): vjp: w [nCell][5] -> du = (dR/du)^T w, duRec = (dR/duRec)^T w; jvp: (du, duRec) -> dRhs.

@@ -91,6 +91,13 @@ def _declare(L):
     L.orc_update_sgs_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
     L.orc_pressure_force.argtypes = [_V, ctypes.c_int, _D, _D, _D, _D, _D]
     L.orc_pressure_force.restype = ctypes.c_double
+    L.orc_cell_rhs_alpha.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_long), _D]
+    L.orc_cell_rhs_alpha_expansion.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double]
+    L.orc_add_fixed_increment.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int, _D]
     L.orc_riemann.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                               ctypes.c_double, _D, _D]
     L.orc_viscous_flux.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -122,6 +129,34 @@ def riemann(rs, UL, UR, n, gamma=1.4, ULm=None, URm=None, dLambda=0.0, fixScale=
     code = RS[rs] if isinstance(rs, str) else int(rs)
     lib().orc_riemann(code, _p(UL), _p(UR), _p(ULm), _p(URm), _p(n), gamma, dLambda, fixScale, incFScale, _p(F), _p(lam))
     return F, lam
+
+
+def cell_rhs_alpha(u, res, refRho, refP, gamma=1.4, relax=0.9, compress=2, compressPower=1.0, ppEpsIsRelaxed=False, flag=0):
+    """EvaluateCellRHSAlpha (EulerEvaluator.hxx:1938-2062): (alpha per cell, nLim, alphaMin, assertion_failed)."""
+    u, res = _f64(u), _f64(res)
+    alpha = np.zeros(u.shape[0])
+    n = ctypes.c_long()
+    amin = np.zeros(1)
+    bad = lib().orc_cell_rhs_alpha(u.shape[0], u.shape[1], gamma, _p(u), _p(res), _p(alpha), refRho, refP, relax, int(compress),
+                                   compressPower, int(ppEpsIsRelaxed), int(flag), ctypes.byref(n), _p(amin))
+    return alpha, int(n.value), float(amin[0]), bool(bad)
+
+
+def cell_rhs_alpha_expansion(u, res, alpha, refRho, refP, alphaMin, gamma=1.4):
+    """EvaluateCellRHSAlphaExpansion (EulerEvaluator.hxx:2064-2140) on a copy of alpha."""
+    u, res = _f64(u), _f64(res)
+    a = _f64(alpha).copy()
+    lib().orc_cell_rhs_alpha_expansion(u.shape[0], u.shape[1], gamma, _p(u), _p(res), _p(a), refRho, refP, alphaMin)
+    return a
+
+
+def add_fixed_increment(u, inc, alpha, refRho, refP, gamma=1.4, ppEpsIsRelaxed=False):
+    """AddFixedIncrement (EulerEvaluator.hpp:1795-1857) on a copy of u: (u_new, alpha_fix_min, assertion_failed)."""
+    un, inc = _f64(u).copy(), _f64(inc)
+    amin = np.zeros(1)
+    bad = lib().orc_add_fixed_increment(un.shape[0], un.shape[1], gamma, _p(un), _p(inc), float(alpha), refRho, refP,
+                                        int(ppEpsIsRelaxed), _p(amin))
+    return un, float(amin[0]), bool(bad)
 
 
 def viscous_flux(U, gradU, n, gamma, mu, k, Cp, adiabatic=False):

@@ -2594,3 +2594,221 @@ extern "C"
         }
     }
 }
+
+// ---------------------------------------------------------------------------
+// Positivity-preserving increment limiting (5 conservative variables, the SA variable 6th).
+// ---------------------------------------------------------------------------
+namespace
+{
+const double kPPSmall = 1e-10, kPPVerySmall = 1e-200;
+
+double ppRhoE(const double *u) { return u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]; }
+
+// Gas.hpp:1750-1860 IdealGasGetCompressionRatioPressure, scheme 0 (quadratic in alpha, then decay)
+double ppCompressionRatio(const double *u, const double *inc, double newRhoE, bool &bad)
+{
+    const double safety = 1 - 1e-5;
+    double r[5], un[5];
+    for (int i = 0; i < 5; i++)
+        r[i] = inc[i], un[i] = u[i] + inc[i];
+    double m2 = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+    double rhoEOld = u[4] - m2 / (u[0] + kPPVerySmall) * 0.5;
+    newRhoE = std::max(kPPSmall * rhoEOld, newRhoE);
+    double rhoENew = un[4] - (un[1] * un[1] + un[2] * un[2] + un[3] * un[3]) / (un[0] + kPPVerySmall) * 0.5;
+    double alpha = (rhoEOld - newRhoE) / std::max(-rhoENew + rhoEOld, kPPVerySmall);
+    if (rhoENew > rhoEOld)
+        alpha = 1;
+    alpha = std::max(std::min(alpha, 1.), 0.);
+    double c0 = 2 * u[4] * u[0] - m2 - 2 * u[0] * newRhoE;
+    double c1 = 2 * u[4] * r[0] + 2 * u[0] * r[4] - 2 * (u[1] * r[1] + u[2] * r[2] + u[3] * r[3]) - 2 * r[0] * newRhoE;
+    double c2 = 2 * r[4] * r[0] - (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+    c2 += (c2 >= 0 ? 1 : -1) * kPPVerySmall;
+    double dC = c1 * c1 - 4 * c0 * c2;
+    if (dC <= -c0 * c0 * kPPSmall)
+        bad = true;
+    dC = std::max(0., dC);
+    double aL = (-std::sqrt(dC) - c1) / (2 * c2);
+    if (std::abs(c2) < 1e-10 * c0)
+        alpha = std::abs(c1) < 1e-10 * c0 ? 0 : std::min(-c0 / c1, 1.);
+    else
+        alpha = std::min(aL, 1.);
+    alpha = std::max(0., alpha) * safety;
+    if (alpha < kPPSmall)
+        alpha = 0;
+    for (int i = 0; i < 5; i++)
+        r[i] *= alpha;
+    int it = 0;
+    for (; it < 1000; it++)
+    {
+        double s[3] = {u[1] + r[1], u[2] + r[2], u[3] + r[3]};
+        double ek = 0.5 * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) / (u[0] + r[0] + kPPVerySmall);
+        if (r[4] + u[4] - ek < newRhoE)
+        {
+            for (int i = 0; i < 5; i++)
+                r[i] *= 1 - 1e-2;
+            alpha *= 1 - 1e-2;
+        }
+        else
+            break;
+    }
+    if (it >= 1000)
+        bad = true;
+    return alpha;
+}
+
+// EulerEvaluator.hpp:1645-1773 CompressInc
+void ppCompressInc(int nv, double gamma, const double *u, const double *inc, double rhoEps, double pEps, double *ret, bool &bad)
+{
+    for (int i = 0; i < nv; i++)
+        ret[i] = inc[i];
+    if (!(u[0] > 0))
+        bad = true;
+    if (u[0] + ret[0] <= rhoEps)
+    {
+        double f = (rhoEps - u[0]) / (ret[0] - kPPVerySmall);
+        for (int i = 0; i < nv; i++)
+            ret[i] *= f;
+    }
+    double rhoEint = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / (u[0] + kPPVerySmall);
+    if (!(rhoEint > 0))
+        bad = true;
+    auto ekOf = [&]()
+    {
+        double s[3] = {u[1] + ret[1], u[2] + ret[2], u[3] + ret[3]};
+        return 0.5 * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) / (u[0] + ret[0] + kPPVerySmall);
+    };
+    double rhoEintNew = u[4] + ret[4] - ekOf();
+    if (rhoEintNew <= pEps)
+    {
+        double e = pEps / (gamma - 1);
+        double m2 = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+        double c0 = 2 * u[4] * u[0] - m2 - 2 * u[0] * e;
+        double c1 = 2 * u[4] * ret[0] + 2 * u[0] * ret[4] - 2 * (u[1] * ret[1] + u[2] * ret[2] + u[3] * ret[3]) - 2 * ret[0] * e;
+        double c2 = 2 * ret[4] * ret[0] - (ret[1] * ret[1] + ret[2] * ret[2] + ret[3] * ret[3]);
+        double dC = c1 * c1 - 4 * c0 * c2;
+        if (!(dC > 0))
+            bad = true;
+        double alpha = std::max(0., std::min((-std::sqrt(std::max(dC, 0.)) - c1) / (2 * c2), 1.));
+        for (int i = 0; i < nv; i++)
+            ret[i] *= alpha * 0.99;
+        for (int it = 0; it < 1000; it++)
+        {
+            if (ret[4] + u[4] - ekOf() < e)
+                for (int i = 0; i < nv; i++)
+                    ret[i] *= 1 - 1e-1;
+            else
+                break;
+        }
+        if (ret[4] + u[4] - ekOf() < e * 0.5)
+            bad = true;
+    }
+    if (nv > 5 && u[5] + ret[5] < 0)
+    {
+        if (u[5] < 0)
+            bad = true;
+        double nu = std::max(1e-6, u[5] * std::exp(ret[5] / (u[5] + 1e-6)));
+        ret[5] = nu - u[5];
+    }
+}
+} // namespace
+
+extern "C"
+{
+    // EulerEvaluator.hxx:1938-2062 EvaluateCellRHSAlpha (refRho, refP = refUPrim(0), refUPrim(I4));
+    // returns 1 when an assertion of the reference would fire
+    int orc_cell_rhs_alpha(long nCell, int nv, double gamma, const double *u, const double *res, double *alpha, double refRho, double refP,
+                           double relax, int compress, double compressPower, int ppEpsIsRelaxed, int flag, long *nLimOut,
+                           double *alphaMinOut)
+    {
+        double rhoEps = kPPSmall * refRho * 1e-1, pEps = kPPSmall * refP * 1e-1;
+        const double safety = 1 - 1e-5;
+        if (ppEpsIsRelaxed)
+            pEps *= 0, rhoEps *= 0;
+        long nLim = 0;
+        double aMin = 1;
+        bool bad = false;
+        for (long c = 0; c < nCell; c++)
+        {
+            const double *uc = u + c * nv;
+            double inc[5];
+            for (int i = 0; i < 5; i++)
+                inc[i] = res[c * nv + i];
+            if (!(uc[0] >= rhoEps))
+                bad = true;
+            double aRho = 1, relRho = rhoEps * relax + uc[0] * (1 - relax);
+            if (inc[0] < 0)
+                aRho = std::min(1.0, (uc[0] - relRho) / (-inc[0] - kPPSmall * inc[0]));
+            if (!(aRho >= 0 && aRho <= 1))
+                bad = true;
+            double un[5];
+            for (int i = 0; i < 5; i++)
+                inc[i] *= aRho, un[i] = uc[i] + inc[i];
+            double pNew = ppRhoE(un) * (gamma - 1), pOld = ppRhoE(uc) * (gamma - 1);
+            double relP = pEps;
+            if (pNew < pOld)
+                relP = pEps + (pOld - pEps) * (1 - relax);
+            double aP = 1;
+            if (pNew < relP)
+                aP = std::min(aP, ppCompressionRatio(uc, inc, relP / (gamma - 1), bad));
+            double a = aRho * aP;
+            if (a < 1)
+            {
+                a = std::pow(a, compress * (int)std::round(compressPower));
+                nLim++;
+                a *= safety;
+                aMin = std::min(aMin, a);
+            }
+            alpha[c] = a;
+        }
+        if (flag & 1)
+            for (long c = 0; c < nCell; c++)
+                if (alpha[c] < 1)
+                    alpha[c] = aMin;
+        if (flag & 2)
+            for (long c = 0; c < nCell; c++)
+                alpha[c] = aMin;
+        *nLimOut = nLim, *alphaMinOut = aMin;
+        return bad ? 1 : 0;
+    }
+
+    // EulerEvaluator.hxx:2064-2140 EvaluateCellRHSAlphaExpansion
+    void orc_cell_rhs_alpha_expansion(long nCell, int nv, double gamma, const double *u, const double *res, double *alpha, double refRho,
+                                      double refP, double alphaMin)
+    {
+        double rhoEps = kPPSmall * refRho * 1e-1, pEps = kPPSmall * refP * 1e-1;
+        for (long c = 0; c < nCell; c++)
+        {
+            double un[5];
+            for (int i = 0; i < 5; i++)
+                un[i] = u[c * nv + i] + res[c * nv + i];
+            if (ppRhoE(un) * (gamma - 1) < pEps || un[0] < rhoEps)
+                alpha[c] = alphaMin;
+        }
+    }
+
+    // EulerEvaluator.hpp:1795-1857 AddFixedIncrement: u += CompressInc(u, alpha inc)
+    int orc_add_fixed_increment(long nCell, int nv, double gamma, double *u, const double *inc, double alpha, double refRho, double refP,
+                                int ppEpsIsRelaxed, double *alphaFixMinOut)
+    {
+        double rhoEps = kPPSmall * refRho * 1e-1, pEps = kPPSmall * refP * 1e-1;
+        if (ppEpsIsRelaxed)
+            pEps *= kPPVerySmall, rhoEps *= kPPVerySmall;
+        double fixMin = 1;
+        bool bad = false;
+        for (long c = 0; c < nCell; c++)
+        {
+            double a[8], comp[8];
+            for (int i = 0; i < nv; i++)
+                a[i] = inc[c * nv + i] * alpha;
+            ppCompressInc(nv, gamma, u + c * nv, a, rhoEps, pEps, comp, bad);
+            double na = std::abs(comp[0]) / std::abs(a[0]);
+            if (std::abs(a[0]) < kPPVerySmall)
+                na = 1.;
+            fixMin = std::min(fixMin, na);
+            for (int i = 0; i < nv; i++)
+                u[c * nv + i] += comp[i];
+        }
+        *alphaFixMinOut = fixMin;
+        return bad ? 1 : 0;
+    }
+}
