@@ -172,8 +172,7 @@ class SteadyAdjoint:
         stay zero, so dJ/dX = dJ/dX|_state - psi^T dR_u/dX - lam^T dS/dX (the time term of the implicit
         step and -uRec do not depend on X).  dJdX: the objective's own derivative (e.g.
         ``ev.PressureForceCoords``), or None for an objective of the state only."""
-        g = self.ev.EvaluateRHSVJPCoords(psi.contiguous(), self.u, self.uRec)
-        g = g + self.vr.DoReconstructionIterVJPCoords(lam.contiguous(), self.uRec, self.u)
+        g = self.ev.ResidualVJPCoords(psi.contiguous(), lam.contiguous(), self.u, self.uRec)
         return -g if dJdX is None else dJdX - g
 
     def solve_tangent(self, sU, sRec, **kw):

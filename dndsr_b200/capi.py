@@ -83,6 +83,8 @@ SIGNATURES = {
     "dndsb_eval_update_sgs_t": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _P],
     "dndsb_eval_pressure_force": [_P, _i, _D, _P, _P, _D, _P, _P, _P],
     "dndsb_eval_pressure_force_coords": [_P, _i, _D, _P, _P, _P, _P],
+    "dndsb_vr_smooth_indicator": [_P, _P, _P, _i, _P, _P],
+    "dndsb_eval_limiter_wbap_c": [_P, _P, _P, _P, _P, _d, _d, _i, _P],
     "dndsb_eval_cell_rhs_alpha": [_P, _P, _P, _P, _d, _d, _d, _i, _d, _i, _i, _P, _P, _P],
     "dndsb_eval_cell_rhs_alpha_expansion": [_P, _P, _P, _P, _d, _d, _d, _P],
     "dndsb_eval_add_fixed_increment": [_P, _P, _P, _d, _d, _d, _i, _P, _P],
@@ -99,6 +101,7 @@ SIGNATURES = {
     "dndsb_vr_iter_jvp_coords": [_P, _P, _P, _P, _i, _P, _P],
     "dndsb_eval_rhs_vjp_coords": [_P, _P, _P, _P, _P, _P],
     "dndsb_eval_rhs_jvp_coords": [_P, _P, _P, _P, _P, _P],
+    "dndsb_eval_residual_vjp_coords": [_P, _P, _P, _P, _P, _P, _P],
     "dndsb_eval_get_array": [_P, ctypes.c_char_p, _D, _l, _I64],
     "dndsb_eval_set_delta_lambda": [_P, _P, _P],
     "dndsb_eval_evaluate_rhs_noalloc": [_P, _P, _P, _P, _P],

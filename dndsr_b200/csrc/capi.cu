@@ -25,6 +25,7 @@ struct dndsb_vr
     GeomD g;
     VRD vr;
     CoordAdjWs coordWs; // node-coordinate derivatives: patches and shares, built on first use
+    real *limSec = nullptr; // WBAP limiter: matrixSecondary per interior face [nFace][2][R][R], built on first use
     int *errWord = nullptr;
     bool metrics = false, base = false, coeff = false;
     int bndNVars = 0; // number of variables of the boundary table's values
@@ -308,6 +309,7 @@ extern "C"
                         (void *)v->vr.AInvb32, (void *)v->vr.sweepCoef, (void *)v->vr.sweepCoef32, (void *)v->errWord, (void *)v->vr.bnd.type, (void *)v->vr.bnd.val})
             dev_free(p);
         coords_ws_free(v->coordWs);
+        dev_free(v->limSec);
         delete v;
         return DNDSB_OK;
     }
@@ -644,6 +646,22 @@ extern "C"
         return status_msg(rc, "dndsb_eval_rhs_vjp_coords");
     }
 
+    int dndsb_eval_residual_vjp_coords(dndsb_eval *e, const double *w, const double *cot, const double *u, const double *uRec, double *dX,
+                                       void *stream)
+    {
+        if (!e || !w || !cot || !u || !uRec || !dX)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_residual_vjp_coords: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_residual_vjp_coords: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_residual_vjp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        dndsb_vr *v = e->vr;
+        int rc = coords_vjp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, v->coordWs, w, cot, u, uRec, dX, e->e.errWord, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(rc, "dndsb_eval_residual_vjp_coords: needs nVars = 5, ignoreVis, and VR degree 1-2 in 3-D, 1-3 in 2-D");
+        return status_msg(rc, "dndsb_eval_residual_vjp_coords");
+    }
+
     int dndsb_eval_rhs_jvp_coords(dndsb_eval *e, const double *dX, const double *u, const double *uRec, double *dRhs, void *stream)
     {
         if (!e || !dX || !u || !uRec || !dRhs)
@@ -719,6 +737,37 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: y and yNew must differ");
         return status_msg(update_sgs_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate, precision, S(stream)),
                           "dndsb_eval_update_sgs_t");
+    }
+
+    int dndsb_vr_smooth_indicator(dndsb_vr *v, const double *u, const double *uRec, int nVars, double *si, void *stream)
+    {
+        if (!v || !u || !uRec || !si)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_smooth_indicator: null argument");
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_smooth_indicator: call construct_rec_coeff first");
+        int rc = smooth_indicator(v->mesh->d, v->g, v->vr, nVars, u, uRec, si, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(DNDSB_E_BADARG, "dndsb_vr_smooth_indicator: 3-D meshes, VR degree 1-2, 5 or 6 variables");
+        return status_msg(rc, "dndsb_vr_smooth_indicator");
+    }
+
+    int dndsb_eval_limiter_wbap_c(dndsb_eval *e, const double *u, const double *uRec, const double *si, double *uRecNew, double smoothThreshold,
+                                  double nStd, int ifAll, void *stream)
+    {
+        if (!e || !u || !uRec || !si || !uRecNew || uRec == uRecNew)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_limiter_wbap_c: null argument, or uRecNew aliases uRec");
+        dndsb_vr *v = e->vr;
+        if (!v->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_limiter_wbap_c: VR not constructed");
+        int rc = lim_secondary_build(v->mesh->d, v->g, v->vr, &v->limSec, v->errWord, S(stream));
+        if (rc == ST_OK)
+            rc = limiter_wbap_c(v->mesh->d, v->g, v->vr, v->limSec, e->e.s.nVars, e->e.s.gamma, u, uRec, si, uRecNew, smoothThreshold, nStd, ifAll,
+                                S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_limiter_wbap_c: 3-D meshes, VR degree 1-2, 5 or 6 variables");
+        if (rc == ST_NONFINITE)
+            return fail(rc, "dndsb_eval_limiter_wbap_c: a face-centre derivative basis is singular");
+        return status_msg(rc, "dndsb_eval_limiter_wbap_c");
     }
 
     int dndsb_eval_cell_rhs_alpha(dndsb_eval *e, const double *u, const double *res, double *alpha, double refRho, double refP, double relax,

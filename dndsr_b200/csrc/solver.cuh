@@ -210,6 +210,12 @@ int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const
 // ---- derivatives (adjoint.cu): VJP / JVP of EvaluateRHS and of one VR Jacobi sweep ----
 // deltaLambdaCell (the entropy-fix scale of the last EvaluateDt) is held fixed, as between the
 // reference's EvaluateDt and EvaluateRHS calls
+// ---- WBAP_C limiter (limiter.cu; 3-D, VR degree 1-2) ----
+int lim_secondary_build(const MeshD &m, const GeomD &g, const VRD &vr, real **sec, int *errWord, cudaStream_t st);
+int smooth_indicator(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *u, const real *uRec, real *si, cudaStream_t st);
+int limiter_wbap_c(const MeshD &m, const GeomD &g, const VRD &vr, const real *sec, int nv, real gamma, const real *u, const real *uRec,
+                   const real *si, real *uRecNew, real threshold, real nStd, int ifAll, cudaStream_t st);
+
 // ---- positivity-preserving increment limiting (positivity.cu) ----
 int cell_rhs_alpha(const MeshD &m, EvalD &ev, const real *u, const real *res, real *alpha, real refRho, real refP, real relax, int compress,
                    real compressPower, int ppEpsIsRelaxed, int flag, int64_t *nLim, real *alphaMin, cudaStream_t st);

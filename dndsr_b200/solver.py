@@ -187,6 +187,12 @@ class VariationalReconstruction(Handle):
                   _ptr(out, "dRecNew"), _stream())
         return out
 
+    def DoCalculateSmoothIndicator(self, u, uRec):
+        """VariationalReconstruction_LimiterProcedure.hxx:40-108 (procedure 0, density and energy): si [nCell]."""
+        si = torch.empty(self.mesh.n_cell, dtype=torch.float64, device="cuda")
+        capi.call("dndsb_vr_smooth_indicator", self.h, _ptr(u, "u"), _ptr(uRec, "uRec"), u.shape[1], _ptr(si, "si"), _stream())
+        return si
+
     def DoReconstructionIterVJPCoords(self, cot, uRec, u):
         """(dS/dX)^T cot for one Jacobi sweep uRecNew = S(uRec, u; X), X the node coordinates
         [nNode][3]: the geometry, basis moments, weights and A^-1 B / A^-1 b are differentiated."""
@@ -279,6 +285,13 @@ class EulerEvaluator(Handle):
         capi.call("dndsb_eval_rhs_vjp_coords", self.h, _ptr(w, "w"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dX"), _stream())
         return dX
 
+    def ResidualVJPCoords(self, w, cot, u, uRec):
+        """(dR/dX)^T w + (dS/dX)^T cot in one pass (S: one VR sweep of this evaluator's reconstruction)."""
+        dX = torch.empty((self.vr.mesh.n_node, 3), dtype=torch.float64, device="cuda")
+        capi.call("dndsb_eval_residual_vjp_coords", self.h, _ptr(w, "w"), _ptr(cot, "cot"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dX"),
+                  _stream())
+        return dX
+
     def EvaluateRHSJVPCoords(self, dX, u, uRec):
         """dR/dX dX of EvaluateRHS along the node displacement dX [nNode][3]."""
         out = torch.empty_like(u)
@@ -327,6 +340,12 @@ class EulerEvaluator(Handle):
         capi.call("dndsb_eval_pressure_force", self.h, int(zone), capi.dptr(d), _ptr(u, "u"), _ptr(uRec, "uRec"), capi.dptr(J),
                   _ptr(gU, "dJdu") if grad else None, _ptr(gR, "dJduRec") if grad else None, _stream())
         return (float(J[0]), gU, gR) if grad else float(J[0])
+
+    def DoLimiterWBAP_C(self, u, uRec, si, uRecNew, smoothThreshold=0.01, WBAP_nStd=10.0, ifAll=False):
+        """VariationalReconstruction_LimiterProcedure.hxx:188-334 with the characteristic projections of
+        EulerSolver.hxx:466-505: the limited reconstruction into uRecNew (putIntoNew)."""
+        capi.call("dndsb_eval_limiter_wbap_c", self.h, _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(si, "si"), _ptr(uRecNew, "uRecNew"),
+                  float(smoothThreshold), float(WBAP_nStd), int(bool(ifAll)), _stream())
 
     # positivity-preserving increment limiting (EulerSolver.hxx:696-738)
     def EvaluateCellRHSAlpha(self, u, res, alpha, refRho, refP, relax=0.9, compress=2, compressPower=1.0, ppEpsIsRelaxed=False, flag=0):

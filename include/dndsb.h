@@ -186,6 +186,18 @@ int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, c
 /* LUSGSMatrixVec(alphaDiag, t, u, uInc, JDiag, AuInc), EulerEvaluator.hxx:175-274 */
 int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
                                 double *AuInc, void *stream);
+/* WBAP_C limiter of the reconstruction (EulerSolver.hxx:455-556: smoothIndicatorProcedure 0,
+ * limiterProcedure 1, limiterBiwayAlter 0, normWBAP false); 3-D meshes, VR degree 1-2, 5 or 6 variables.
+ * smooth_indicator: DoCalculateSmoothIndicator(si, uRec, u, {0, I4})
+ *   (VariationalReconstruction_LimiterProcedure.hxx:40-108), si [nCell].
+ * limiter_wbap_c: DoLimiterWBAP_C(u, uRec, uRecNew, ..., si, ifAll, FM, FMI, putIntoNew = true)
+ *   (VariationalReconstruction_LimiterProcedure.hxx:188-334) with the characteristic projections FM/FMI
+ *   of EulerSolver.hxx:466-505 (the evaluator's gamma); cells with si < smoothThreshold are copied unless
+ *   ifAll.  The first call builds matrixSecondary (VariationalReconstruction.cpp:840-866) on the device. */
+int dndsb_vr_smooth_indicator(dndsb_vr *vr, const double *u, const double *uRec, int nVars, double *si, void *stream);
+int dndsb_eval_limiter_wbap_c(dndsb_eval *ev, const double *u, const double *uRec, const double *si, double *uRecNew, double smoothThreshold,
+                              double nStd, int ifAll, void *stream);
+
 /* Positivity-preserving increment limiting of the implicit update (EulerSolver.hxx:696-738).
  * refRho, refP: the reference's refUPrim(0), refUPrim(I4) (far-field density and pressure), which set
  * the floors rhoEps = 1e-11 refRho, pEps = 1e-11 refP.  A state for which the reference asserts returns
@@ -218,6 +230,10 @@ int dndsb_eval_rhs_jvp(dndsb_eval *ev, const double *du, const double *duRec, co
  * (ignoreVis) 5-variable models; VR degree 1-2 in 3-D, 1-3 in 2-D. */
 int dndsb_eval_rhs_vjp_coords(dndsb_eval *ev, const double *w, const double *u, const double *uRec, double *dX, void *stream);
 int dndsb_eval_rhs_jvp_coords(dndsb_eval *ev, const double *dX, const double *u, const double *uRec, double *dRhs, void *stream);
+/* Both at once, sharing the per-cell recomputation: dX = (dR/dX)^T w + (dS/dX)^T cot, S the VR sweep of the
+ * evaluator's reconstruction (the coupled residual's coordinate VJP). */
+int dndsb_eval_residual_vjp_coords(dndsb_eval *ev, const double *w, const double *cot, const double *u, const double *uRec, double *dX,
+                                   void *stream);
 
 /* Adjoint building blocks (no reference counterpart; they transpose the operators above).
  * lusgs_matrix_vec_t: ATy = A^T y for the operator A of dndsb_eval_lusgs_matrix_vec (same lambdaFace,

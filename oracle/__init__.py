@@ -91,6 +91,8 @@ def _declare(L):
     L.orc_update_sgs_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
     L.orc_pressure_force.argtypes = [_V, ctypes.c_int, _D, _D, _D, _D, _D]
     L.orc_pressure_force.restype = ctypes.c_double
+    L.orc_smooth_indicator.argtypes = [_V, _D, _D, _D]
+    L.orc_limiter_wbap_c.argtypes = [_V, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double]
     L.orc_cell_rhs_alpha.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_long), _D]
@@ -304,6 +306,21 @@ class Oracle:
         gR = np.zeros_like(uRec) if grad else None
         J = lib().orc_pressure_force(self.h, int(zone), _p(d), _p(u), _p(uRec), _p(gU) if grad else None, _p(gR) if grad else None)
         return (J, gU, gR) if grad else J
+
+    def smooth_indicator(self, u, uRec):
+        """DoCalculateSmoothIndicator (procedure 0, density and energy), one value per cell."""
+        u, uRec = _f64(u), _f64(uRec)
+        si = np.zeros(self.mesh.n_cell)
+        lib().orc_smooth_indicator(self.h, _p(u), _p(uRec), _p(si))
+        return si
+
+    def limiter_wbap_c(self, u, uRec, si, smoothThreshold=0.01, WBAP_nStd=10.0, ifAll=False, gamma=1.4):
+        """DoLimiterWBAP_C (WBAP-L2 biway and multiway, characteristic variables): the limited uRec."""
+        u, uRec, si = _f64(u), _f64(uRec), _f64(si)
+        out = np.zeros_like(uRec)
+        bad = lib().orc_limiter_wbap_c(self.h, _p(u), _p(uRec), _p(si), _p(out), smoothThreshold, WBAP_nStd, int(ifAll), gamma)
+        assert bad == 0, "singular derivative basis at a face centre"
+        return out
 
     def cell_point_values(self, u, uRec):
         u, uRec = _f64(u), _f64(uRec)

@@ -2812,3 +2812,306 @@ extern "C"
         return bad ? 1 : 0;
     }
 }
+
+// ---------------------------------------------------------------------------
+// WBAP_C limiter (3-D, 5 or 6 variables): DoCalculateSmoothIndicator (procedure 0) and DoLimiterWBAP_C
+// with the WBAP-L2 biway (limiterBiwayAlter 0) and multiway (normWBAP false) functions, in the
+// characteristic variables of EulerSolver.hxx:455-556.
+// ---------------------------------------------------------------------------
+namespace
+{
+// solve A X = B, A n x n (row-major, overwritten), B n x m (overwritten by X); Gauss-Jordan, partial pivoting
+bool ocSolve(int n, int m, double *A, double *B)
+{
+    for (int c = 0; c < n; c++)
+    {
+        int piv = c;
+        for (int r = c + 1; r < n; r++)
+            if (std::abs(A[r * n + c]) > std::abs(A[piv * n + c]))
+                piv = r;
+        if (A[piv * n + c] == 0)
+            return false;
+        if (piv != c)
+        {
+            for (int j = 0; j < n; j++)
+                std::swap(A[piv * n + j], A[c * n + j]);
+            for (int j = 0; j < m; j++)
+                std::swap(B[piv * m + j], B[c * m + j]);
+        }
+        double id = 1.0 / A[c * n + c];
+        for (int j = 0; j < n; j++)
+            A[c * n + j] *= id;
+        for (int j = 0; j < m; j++)
+            B[c * m + j] *= id;
+        for (int r = 0; r < n; r++)
+            if (r != c && A[r * n + c] != 0)
+            {
+                double f = A[r * n + c];
+                for (int j = 0; j < n; j++)
+                    A[r * n + j] -= f * A[c * n + j];
+                for (int j = 0; j < m; j++)
+                    B[r * m + j] -= f * B[c * m + j];
+            }
+    }
+    return true;
+}
+
+// Geometric.hpp:135-160 NormBuildLocalBaseV (3-D): columns n, t1, t2
+void ocNormBase(const double *n, double B[3][3])
+{
+    double t[3];
+    if (std::abs(n[2]) < 0.9) // -(n x e_z)
+        t[0] = -(n[1] * 1 - n[2] * 0), t[1] = -(n[2] * 0 - n[0] * 1), t[2] = -(n[0] * 0 - n[1] * 0);
+    else // -(n x e_y)
+        t[0] = -(n[1] * 0 - n[2] * 1), t[1] = -(n[2] * 0 - n[0] * 0), t[2] = -(n[0] * 1 - n[1] * 0);
+    double tn = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    for (int d = 0; d < 3; d++)
+        t[d] /= tn;
+    double s[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
+    double sn = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (int d = 0; d < 3; d++)
+        B[d][0] = n[d], B[d][1] = t[d], B[d][2] = s[d] / sn;
+}
+
+// Gas.hpp:120-200 Euler eigenvectors of the state UC (5 conservative), right (R) and left (L)
+void ocEigen(const double *UC, double gamma, double Rv[5][5], double Lv[5][5])
+{
+    double v[3] = {UC[1] / UC[0], UC[2] / UC[0], UC[3] / UC[0]};
+    double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    double p = (gamma - 1) * (UC[4] - 0.5 * UC[0] * vsq);
+    double a2 = gamma * p / UC[0], a = std::sqrt(a2), H = (UC[4] + p) / UC[0];
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++)
+            Rv[i][j] = Lv[i][j] = 0;
+    Rv[0][0] = Rv[0][1] = Rv[0][4] = 1;
+    Rv[2][2] = Rv[3][3] = 1;
+    for (int d = 0; d < 3; d++)
+        Rv[1 + d][0] = v[d], Rv[1 + d][1] = v[d], Rv[1 + d][4] = v[d];
+    Rv[1][0] -= a, Rv[1][4] += a;
+    Rv[4][0] = H - v[0] * a, Rv[4][4] = H + v[0] * a, Rv[4][1] = 0.5 * vsq;
+    Rv[4][2] = v[1], Rv[4][3] = v[2];
+    const double gb = gamma - 1;
+    Lv[0][0] = H + a / gb * (v[0] - a), Lv[0][1] = -v[0] - a / gb, Lv[0][2] = -v[1], Lv[0][3] = -v[2], Lv[0][4] = 1;
+    Lv[1][0] = -2 * H + 4 / gb * a2, Lv[1][1] = 2 * v[0], Lv[1][2] = 2 * v[1], Lv[1][3] = 2 * v[2], Lv[1][4] = -2;
+    Lv[2][0] = v[1] * (-2 * a2 / gb), Lv[3][0] = v[2] * (-2 * a2 / gb);
+    Lv[2][2] = Lv[3][3] = 2 * a2 / gb;
+    Lv[4][0] = H - a / gb * (v[0] + a), Lv[4][1] = -v[0] + a / gb, Lv[4][2] = -v[1], Lv[4][3] = -v[2], Lv[4][4] = 1;
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++)
+            Lv[i][j] *= gb / (2 * a2);
+}
+
+// EulerSolver.hxx:466-505 fML / fMR: rows of `data` (one per DOF, nv values) to characteristic
+// variables (left) or back (right), in the face's normal-aligned frame
+void ocCharTransform(const double *uL, const double *uR, const double *n, double gamma, bool toChar, int rows, int nv, double *data)
+{
+    double UC[5], B[3][3];
+    for (int i = 0; i < 5; i++)
+        UC[i] = (uL[i] + uR[i]) * 0.5;
+    ocNormBase(n, B);
+    double m[3] = {UC[1], UC[2], UC[3]};
+    for (int d = 0; d < 3; d++)
+        UC[1 + d] = B[0][d] * m[0] + B[1][d] * m[1] + B[2][d] * m[2];
+    double Rv[5][5], Lv[5][5], M[5][5];
+    ocEigen(UC, gamma, Rv, Lv);
+    if (toChar) // M = L; M(:, 1..3) = M(:, 1..3) B^T
+        for (int i = 0; i < 5; i++)
+        {
+            M[i][0] = Lv[i][0], M[i][4] = Lv[i][4];
+            for (int d = 0; d < 3; d++)
+                M[i][1 + d] = Lv[i][1] * B[d][0] + Lv[i][2] * B[d][1] + Lv[i][3] * B[d][2];
+        }
+    else // M = R; M(1..3, :) = B M(1..3, :)
+        for (int j = 0; j < 5; j++)
+        {
+            M[0][j] = Rv[0][j], M[4][j] = Rv[4][j];
+            for (int d = 0; d < 3; d++)
+                M[1 + d][j] = B[d][0] * Rv[1][j] + B[d][1] * Rv[2][j] + B[d][2] * Rv[3][j];
+        }
+    for (int r = 0; r < rows; r++)
+    {
+        double x[5], y[5];
+        for (int i = 0; i < 5; i++)
+            x[i] = data[r * nv + i];
+        for (int i = 0; i < 5; i++)
+        {
+            y[i] = 0;
+            for (int j = 0; j < 5; j++)
+                y[i] += M[i][j] * x[j];
+        }
+        for (int i = 0; i < 5; i++)
+            data[r * nv + i] = y[i];
+    }
+}
+
+double ocSign(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+const double kPDiP = 1e-50; // verySmallReal^(1/4)
+} // namespace
+
+extern "C"
+{
+    // VariationalReconstruction_LimiterProcedure.hxx:40-108 DoCalculateSmoothIndicator, varsSee {0, 4}
+    void orc_smooth_indicator(void *h, const double *u, const double *uRec, double *si)
+    {
+        Oracle *o = (Oracle *)h;
+        const int nv = o->es.nVars, NDOF = o->NDOF, R = o->R;
+        std::vector<double> T(NDOF * NDOF);
+        const int vs[2] = {0, 4};
+        for (long c = 0; c < o->nCell; c++)
+        {
+            double S[2][2] = {{0, 0}, {0, 0}};
+            for (int k = 0; k < o->nf; k++)
+            {
+                long fp = o->cell2face[c * o->nf + k], f = fp;
+                long other = o->otherOf(c, f);
+                if (other < 0)
+                    continue;
+                double val[2][20 * 2], jmp[20 * 2], avg[20 * 2];
+                for (int side = 0; side < 2; side++)
+                {
+                    long cc = side == 0 ? c : other;
+                    int sd = o->face2cell[f * 2] == cc ? 0 : 1;
+                    double p[3];
+                    for (int d = 0; d < 3; d++)
+                        p[d] = o->faceCent[f * 3 + d] + (sd ? o->facePShift[f * 3 + d] : 0.0);
+                    o->diffBase(cc, p, T.data(), NDOF, true);
+                    for (int r = 0; r < NDOF; r++)
+                        for (int q = 0; q < 2; q++)
+                        {
+                            double a = 0;
+                            for (int j = 0; j < R; j++)
+                                a += T[r * NDOF + 1 + j] * uRec[(cc * R + j) * nv + vs[q]];
+                            if (r == 0)
+                                a += u[cc * nv + vs[q]];
+                            val[side][r * 2 + q] = a;
+                        }
+                }
+                for (int i = 0; i < NDOF * 2; i++)
+                    avg[i] = (val[0][i] + val[1][i]) * 0.5, jmp[i] = (val[0][i] - val[1][i]) * 0.5;
+                double IJ[4], IS[4];
+                o->faceFunctional(f, jmp, 2, jmp, 2, NDOF, IJ);
+                o->faceFunctional(f, avg, 2, avg, 2, NDOF, IS);
+                for (int q = 0; q < 2; q++)
+                    S[q][0] += IJ[q * 2 + q] * o->faceArea[f], S[q][1] += IS[q * 2 + q] * o->faceArea[f];
+            }
+            double sm = 0;
+            for (int q = 0; q < 2; q++)
+                sm = std::max(sm, std::abs(S[q][0] / (S[q][1] + 1e-200)));
+            si[c] = std::sqrt(sm) * o->vs.maxOrder * o->vs.maxOrder;
+        }
+    }
+
+    // VariationalReconstruction_LimiterProcedure.hxx:188-334 DoLimiterWBAP_C (putIntoNew), with
+    // VariationalReconstruction.cpp:840-866 matrixSecondary and Limiters.hpp:361-470 WBAP-L2
+    int orc_limiter_wbap_c(void *h, const double *u, const double *uRec, const double *si, double *uRecNew, double threshold, double nStd,
+                           int ifAll, double gamma)
+    {
+        Oracle *o = (Oracle *)h;
+        const int nv = o->es.nVars, NDOF = o->NDOF, R = o->R, P = o->vs.maxOrder;
+        // matrixSecondary per interior face: [0] = DiffI^-1 DiffJ (for side 0), [1] = DiffJ^-1 DiffI (side 1)
+        std::vector<double> sec((size_t)o->nFace * 2 * R * R, 0.0), T(NDOF * NDOF);
+        for (long f = 0; f < o->nFace; f++)
+        {
+            long cL = o->face2cell[f * 2], cR = o->face2cell[f * 2 + 1];
+            if (cR < 0)
+                continue;
+            std::vector<double> DI(R * R), DJ(R * R);
+            double p[3];
+            for (int d = 0; d < 3; d++)
+                p[d] = o->faceCent[f * 3 + d];
+            o->diffBase(cL, p, T.data(), NDOF, true);
+            for (int r = 0; r < R; r++)
+                for (int j = 0; j < R; j++)
+                    DI[r * R + j] = T[(r + 1) * NDOF + 1 + j];
+            for (int d = 0; d < 3; d++)
+                p[d] += o->facePShift[f * 3 + d];
+            o->diffBase(cR, p, T.data(), NDOF, true);
+            for (int r = 0; r < R; r++)
+                for (int j = 0; j < R; j++)
+                    DJ[r * R + j] = T[(r + 1) * NDOF + 1 + j];
+            std::vector<double> A = DI, X = DJ;
+            if (!ocSolve(R, R, A.data(), X.data()))
+                return 1;
+            std::copy(X.begin(), X.end(), sec.begin() + (size_t)f * 2 * R * R);
+            A = DJ, X = DI;
+            if (!ocSolve(R, R, A.data(), X.data()))
+                return 1;
+            std::copy(X.begin(), X.end(), sec.begin() + ((size_t)f * 2 + 1) * R * R);
+        }
+        const int st3[5] = {0, 1, 4, 10, 20};
+        for (long c = 0; c < o->nCell; c++)
+        {
+            double *out = uRecNew + c * R * nv;
+            const double *rc = uRec + c * R * nv;
+            if (!ifAll && si[c] < threshold)
+            {
+                std::copy(rc, rc + R * nv, out);
+                continue;
+            }
+            std::vector<double> uFaces((size_t)o->nf * R * nv, 0.0);
+            for (int cp = P; cp >= 1; cp--)
+            {
+                const int ls = st3[cp] - 1, le = st3[cp + 1] - 2, nr = le - ls + 1;
+                std::vector<std::vector<double>> others;
+                others.emplace_back(rc + ls * nv, rc + (le + 1) * nv);
+                for (int k = 0; k < o->nf; k++)
+                {
+                    long f = o->cell2face[c * o->nf + k];
+                    long oc = o->otherOf(c, f);
+                    if (oc < 0)
+                        continue;
+                    int side = o->face2cell[f * 2] == c ? 0 : 1;
+                    const double *Mt = &sec[((size_t)f * 2 + side) * R * R], *Mo = &sec[((size_t)f * 2 + 1 - side) * R * R];
+                    std::vector<double> uoo(uRec + oc * R * nv, uRec + (oc + 1) * R * nv);
+                    double *uf = &uFaces[(size_t)k * R * nv];
+                    for (int i = le + 1; i < R; i++)
+                        for (int v = 0; v < nv; v++)
+                        {
+                            double a = 0;
+                            for (int j = le + 1; j < R; j++)
+                                a += Mo[i * R + j] * uf[j * nv + v];
+                            uoo[i * nv + v] = a;
+                        }
+                    std::vector<double> oin(nr * nv), tin(rc + ls * nv, rc + (le + 1) * nv);
+                    for (int i = 0; i < nr; i++)
+                        for (int v = 0; v < nv; v++)
+                        {
+                            double a = 0;
+                            for (int j = 0; j < R; j++)
+                                a += Mt[(ls + i) * R + j] * uoo[j * nv + v];
+                            oin[i * nv + v] = a;
+                        }
+                    const double *uL = side == 0 ? u + c * nv : u + oc * nv, *uR = side == 0 ? u + oc * nv : u + c * nv;
+                    const double *n = &o->faceMeanNorm[f * 3];
+                    ocCharTransform(uL, uR, n, gamma, true, nr, nv, oin.data());
+                    ocCharTransform(uL, uR, n, gamma, true, nr, nv, tin.data());
+                    std::vector<double> lim(nr * nv);
+                    for (int i = 0; i < nr * nv; i++)
+                    {
+                        double u1 = tin[i], u2 = oin[i];
+                        double fr = u1 / (std::abs(u2) + kPDiP) * ocSign(u2);
+                        double t1 = fr * fr * fr, t2 = (fr * fr) * (fr * fr);
+                        lim[i] = u1 * (1 + t1) / (1 + t2) * std::abs(ocSign(u2));
+                    }
+                    ocCharTransform(uL, uR, n, gamma, false, nr, nv, lim.data());
+                    for (int i = 0; i < nr * nv; i++)
+                        uf[ls * nv + i] = lim[i];
+                    others.push_back(lim);
+                }
+                for (int i = 0; i < nr * nv; i++)
+                {
+                    double up = 0, down = 0, cent = others[0][i];
+                    for (size_t q = 1; q < others.size(); q++)
+                    {
+                        double ti = others[0][i] / (std::abs(others[q][i]) + kPDiP) * ocSign(others[q][i]);
+                        down += (ti * ti) * (ti * ti);
+                        up += ti * ti * ti;
+                        cent *= std::abs(ocSign(others[q][i]));
+                    }
+                    out[ls * nv + i] = cent * (up + nStd) / (down + nStd);
+                }
+            }
+        }
+        return 0;
+    }
+}

@@ -27,7 +27,7 @@ import torch
 import oracle
 from dndsr_b200 import mesh as M
 from tests.bump_case import bump_oracle, perturbed_state
-from tests.util import VR_HQM, VR_HQM_PY
+from tests.util import VR_HQM, VR_HQM_PY, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -122,6 +122,12 @@ def test_vr_sweep_coordinate_vjp_against_finite_differences_and_jvp(name, case, 
         assert abs(adj - fd) < 1e-6 * abs(fd), (adj, fd)
         jv = vr.DoReconstructionIterJVPCoords(torch.tensor(V, device="cuda"), uRec, u).cpu().numpy()
         assert abs(float((C * jv).sum()) - adj) <= 1e-12 * max(abs(adj), np.abs(C * jv).sum() * 1e-3)
+    # the one-pass coupled VJP is the sum of the two
+    W = rng.normal(size=u0.shape)
+    Ct, Wt = torch.tensor(C, device="cuda"), torch.tensor(W, device="cuda")
+    both = ev.ResidualVJPCoords(Wt, Ct, u, uRec).cpu().numpy()
+    apart = (ev.EvaluateRHSVJPCoords(Wt, u, uRec) + vr.DoReconstructionIterVJPCoords(Ct, uRec, u)).cpu().numpy()
+    assert relerr(both, apart) < 1e-13
 
 
 def test_coordinate_derivatives_unsupported_cases_fail_loudly():
