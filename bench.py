@@ -357,6 +357,17 @@ def run_adjoint_cost(args):
         t_xr = timed(lambda: ev.EvaluateRHSVJPCoords(w, u, uRec), n=3)
         t_xv = timed(lambda: vr.DoReconstructionIterVJPCoords(cot, uRec, u), n=3)
         t_xb = timed(lambda: ev.ResidualVJPCoords(w, cot, u, uRec), n=3)
+        # the limiter step (every cell limited) and the positivity-preserving increment, against one residual
+        si = vr.DoCalculateSmoothIndicator(u, uRec)
+        uLim = torch.empty_like(uRec)
+        t_si = timed(lambda: vr.DoCalculateSmoothIndicator(u, uRec))
+        t_lim = timed(lambda: ev.DoLimiterWBAP_C(u, uRec, si, uLim, 0.01, 10.0, True))
+        inc = torch.randn(u.shape, dtype=torch.float64, device="cuda") * 1e-2 * u.abs()
+        alphaPP, uInc = torch.ones(mesh.n_cell, dtype=torch.float64, device="cuda"), u.clone()
+        t_alpha = timed(lambda: ev.EvaluateCellRHSAlpha(u, inc, alphaPP, far[0], 1.0, 0.9))
+        t_fix = timed(lambda: ev.AddFixedIncrement(uInc, inc, 1e-6, far[0], 1.0))
+        limiter = {"ms_smooth_indicator": t_si, "ms_wbap_limiter_all_cells": t_lim, "ms_cell_rhs_alpha": t_alpha,
+                   "ms_add_fixed_increment": t_fix, "limiter_over_residual": (t_si + t_lim) / (t_rhs + t_vr)}
         V = torch.randn((mesh.n_node, 3), dtype=torch.float64, device="cuda") * 1e-3
         a_r = float((ev.EvaluateRHSVJPCoords(w, u, uRec) * V).sum())
         b_r = float((w * ev.EvaluateRHSJVPCoords(V, u, uRec)).sum())
@@ -367,7 +378,7 @@ def run_adjoint_cost(args):
                         "ms_vr_sweep_vjp_coords": t_xv, "ms_residual_vjp_coords_one_pass": t_xb,
                         "coords_vjp_over_primal": t_xb / (t_rhs + t_vr),
                         "coords_dual_consistency_rhs": abs(a_r - b_r) / max(abs(a_r), 1e-300),
-                        "coords_dual_consistency_sweep": abs(a_v - b_v) / max(abs(a_v), 1e-300)}
+                        "coords_dual_consistency_sweep": abs(a_v - b_v) / max(abs(a_v), 1e-300), **limiter}
         if p == 1:
             out["adjoint_solve_p1"] = adjoint_solve(vr, ev, u, uRec, far, mesh, t_rhs + t_vr)
     out["tgv_viscous"] = tgv_vjp_cost(args)
