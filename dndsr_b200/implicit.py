@@ -203,6 +203,12 @@ class SolverConfig:
     meanScale: tuple = ()            # GMRES dot weights (gmresScale), empty = ones
     # positivity-preserving increments (timeMarchControl.incrementPPRelax, uRecAlphaCompressPower,
     # ppEpsIsRelaxed); the floors scale with the far-field state, empty = plain u += alpha inc
+    # limiterControl (EulerSolver.hxx:455-580): WBAP_C after the VR sweeps, the RHS from the limited
+    # reconstruction (inviscid evaluators: their face values are all the reference takes from it)
+    useLimiter: bool = False
+    smoothThreshold: float = 0.01
+    WBAP_nStd: float = 10.0
+    preserveLimited: bool = False
     farFieldStaticValue: tuple = ()
     incrementPPRelax: float = 0.9
     uRecAlphaCompressPower: float = 1.0
@@ -227,6 +233,11 @@ class ImplicitSolver:
         self.CFLNow = cfg.CFL
         self.n_rhs = 0
         self.n_sgs = 0
+        self.uRecLim = None
+        if cfg.useLimiter:
+            if not bool(ev.settings.get("ignoreVis", False)):
+                raise NotImplementedError("useLimiter: the limited / unlimited reconstruction pair of a viscous RHS is not built")
+            self.uRecLim = vr.BuildURec(nv)
         self.pp = None
         if cfg.farFieldStaticValue:
             far = [float(x) for x in cfg.farFieldStaticValue]
@@ -241,7 +252,14 @@ class ImplicitSolver:
     def frhs(self, crhs, cx, dtau, it, ct):
         for _ in range(self.cfg.nInternalRecStep):
             self.vr.DoReconstructionIter(self.uRec, self.uRecNew, cx, putIntoNew=False, precision=self.cfg.vr_precision)
-        self.ev.EvaluateRHS(crhs, cx, self.uRec)
+        if self.uRecLim is not None:
+            si = self.vr.DoCalculateSmoothIndicator(cx, self.uRec)
+            self.ev.DoLimiterWBAP_C(cx, self.uRec, si, self.uRecLim, self.cfg.smoothThreshold, self.cfg.WBAP_nStd, False)
+            if self.cfg.preserveLimited:
+                self.uRec.copy_(self.uRecLim)
+            self.ev.EvaluateRHS(crhs, cx, self.uRecLim)
+        else:
+            self.ev.EvaluateRHS(crhs, cx, self.uRec)
         self.n_rhs += 1
 
     # EulerSolver.hxx:674-694

@@ -65,3 +65,22 @@ def test_linear_field_is_left_unchanged_on_the_device():
     ev.DoLimiterWBAP_C(u, uRec, si, out, 0.01, 10.0, True)
     assert float(si.max()) < 1e-12
     assert relerr(out.cpu().numpy(), uRec0) < 1e-13
+
+
+def test_implicit_solver_with_the_limiter():
+    """useLimiter in the implicit solver: with a threshold no cell reaches, the run equals the
+    unlimited one bit for bit; with every cell limited it stays finite and differs."""
+    from dndsr_b200 import implicit as I
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    m = M.tgv_mesh(6)
+    runs = []
+    for lim, thr in ((False, 0.01), (True, 1e30), (True, 0.0)):
+        vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1)).construct()
+        ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType="HLLEP", muGas=0.0, ignoreVis=True))
+        u = vr.BuildUDof(5)
+        ev.InitializeUDOF(u, 3)
+        cfg = I.SolverConfig(odeCode=0, dtImplicit=0.05, nTimeStep=2, nTimeStepInternal=4, useLimiter=lim, smoothThreshold=thr)
+        I.ImplicitSolver(vr, ev, cfg).run(u)
+        runs.append(u.cpu().numpy())
+    assert np.array_equal(runs[0], runs[1])
+    assert np.isfinite(runs[2]).all() and not np.array_equal(runs[0], runs[2])
