@@ -138,7 +138,34 @@ def cpu_baseline_oracle(n_sample, p, seconds, threads=None):
         el = time.perf_counter() - t0
         if el > seconds:
             break
+    cpu_baseline_oracle.per_operator = _cpu_per_operator(o, u, uRec, m.n_cell)
     return m.n_cell * steps / el / 1e6, steps, el, m.n_cell
+
+
+def _cpu_per_operator(o, u, uRec, n_cell, reps=5, warm=2):
+    """Median CPU times of the oracle's operators on the sample (after warm-up): the VR sweep (a1),
+    EvaluateRHS (a9) and one forward + backward SGS sweep pair (a14)."""
+    dTau, _ = o.eval_dt(u, 5.0)
+    jd = o.lusgs_init(dTau, 1e100, 1.0)
+    rhs = o.eval_rhs(u, uRec)
+    z, t1, t2 = np.zeros_like(u), np.zeros_like(u), np.zeros_like(u)
+
+    def sgs_pair():
+        o.update_sgs(1.0, rhs, u, z, t1, jd, True)
+        o.update_sgs(1.0, rhs, u, t1, t2, jd, False)
+
+    ops = {"vr_sweep": lambda: o.vr_iter(uRec, u), "evaluate_rhs": lambda: o.eval_rhs(u, uRec), "sgs_pair": sgs_pair}
+    out = {}
+    for name, fn in ops.items():
+        ts = []
+        for i in range(warm + reps):
+            t0 = time.perf_counter()
+            fn()
+            if i >= warm:
+                ts.append(time.perf_counter() - t0)
+        ms = float(np.median(ts)) * 1e3
+        out[name] = {"ms": ms, "mcell_per_s": n_cell / ms / 1e3}
+    return out
 
 
 def run_steady(args):
@@ -632,7 +659,9 @@ def run_ours(args, rank, world, local_rank):
         v, steps, el, cells = cpu_baseline_oracle(args.sample_n, p, args.sample_seconds, n_cores())
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": n_cores(), "kind": "port",
                                 "sample": f"oracle port, OpenMP: {steps} steps of VR sweep + EvaluateRHS on TGV {args.sample_n}^3 "
-                                          f"({cells} cells, same settings) in {el:.1f} s"}
+                                          f"({cells} cells, same settings) in {el:.1f} s",
+                                "per_operator": {"sample": f"TGV {args.sample_n}^3, median of 5 after 2 warm-ups",
+                                                 **cpu_baseline_oracle.per_operator}}
     print(json.dumps(line), flush=True)
 
 
