@@ -11,7 +11,8 @@ extern template void coords_vjp_launch<2>(const MeshD &, const GeomD &, const VR
 extern template void pressure_force_coords_launch<2>(const MeshD &, const GeomD &, const VRD &, real, int, const real *, const real *,
                                                      const real *, const CoordAdjWs &, cudaStream_t);
 extern template void coords_jvp_launch<2>(const MeshD &, const GeomD &, const VRD &, const EulerSettingsD &, const real *, const real *,
-                                          const real *, const real *, real *, real *, int *, cudaStream_t);
+                                   const real *, const real *, real *, real *, int *, const real *, cudaStream_t);
+extern template void coords_lanes_launch<2>(const MeshD &, const GeomD &, const VRD &, real *, cudaStream_t);
 
 namespace
 {
@@ -111,9 +112,28 @@ int coords_ws_build(const MeshD &m, CoordAdjWs &ws)
     return ST_OK;
 }
 
+// the cell geometry lanes (value and derivatives with respect to the cell's own vertices); without
+// the memory for them the kernels recompute the geometry of each cell they need
+void coords_lanes_build(const MeshD &m, const GeomD &g, const VRD &vr, CoordAdjWs &ws, cudaStream_t st)
+{
+    if (ws.lanes || ws.noLanes)
+        return;
+    const size_t n = (size_t)m.nCell * (10 + vr.NDOF) * (1 + 3 * m.nvert);
+    if (dev_alloc((void **)&ws.lanes, sizeof(real) * n) != cudaSuccess)
+    {
+        (void)last_error();
+        ws.lanes = nullptr, ws.noLanes = true;
+        return;
+    }
+    if (m.dim == 2)
+        coords_lanes_launch<2>(m, g, vr, ws.lanes, st);
+    else
+        coords_lanes_launch<3>(m, g, vr, ws.lanes, st);
+}
+
 void coords_ws_free(CoordAdjWs &ws)
 {
-    dev_free(ws.patch), dev_free(ws.start), dev_free(ws.ent), dev_free(ws.share);
+    dev_free(ws.patch), dev_free(ws.start), dev_free(ws.ent), dev_free(ws.share), dev_free(ws.lanes);
     ws = CoordAdjWs();
 }
 
@@ -125,6 +145,7 @@ int coords_vjp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSetting
     int rc = coords_ws_build(m, ws);
     if (rc != ST_OK)
         return rc;
+    coords_lanes_build(m, g, vr, ws, st);
     const EulerSettingsD es = s ? *s : EulerSettingsD();
     dev_zero(errWord, sizeof(int), st);
     if (m.dim == 2)
@@ -154,17 +175,18 @@ int pressure_force_coords(const MeshD &m, const GeomD &g, const VRD &vr, real ga
     return ST_OK;
 }
 
-int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, const real *dX, const real *u,
-               const real *uRec, real *dRhs, real *dRec, int *errWord, cudaStream_t st)
+int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, CoordAdjWs &ws, const real *dX,
+               const real *u, const real *uRec, real *dRhs, real *dRec, int *errWord, cudaStream_t st)
 {
     if (!geo_supported(m, vr) || (s && (s->nVars != 5 || !s->ignoreVis)))
         return ST_UNSUPPORTED;
+    coords_lanes_build(m, g, vr, ws, st);
     const EulerSettingsD es = s ? *s : EulerSettingsD();
     dev_zero(errWord, sizeof(int), st);
     if (m.dim == 2)
-        coords_jvp_launch<2>(m, g, vr, es, dLamCell, dX, u, uRec, dRhs, dRec, errWord, st);
+        coords_jvp_launch<2>(m, g, vr, es, dLamCell, dX, u, uRec, dRhs, dRec, errWord, ws.lanes, st);
     else
-        coords_jvp_launch<3>(m, g, vr, es, dLamCell, dX, u, uRec, dRhs, dRec, errWord, st);
+        coords_jvp_launch<3>(m, g, vr, es, dLamCell, dX, u, uRec, dRhs, dRec, errWord, ws.lanes, st);
     return geo_status(st, errWord);
 }
 } // namespace dndsb

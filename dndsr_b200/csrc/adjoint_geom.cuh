@@ -62,7 +62,49 @@ template <typename T, int NDOF>
 struct CellG
 {
     T vol, bary[3], cent[3], scale[3], moment[NDOF];
+    static constexpr int kFields = 10 + NDOF;
+    DNDSB_D T *fields() { return &vol; }
 };
+
+// Cell geometry from the per-mesh cache: [field][lane], lane 0 the value, lane 1 + 3 v + d its derivative
+// with respect to coordinate d of the cell's vertex v (the first vertex of a node carries all of it)
+template <int NDOF>
+DNDSB_D void lanes_load(const real *cg, const MeshD &m, int64_t c, const SeedNode &sd, CellG<Dual<3>, NDOF> &o)
+{
+    const int L = 1 + 3 * m.nvert;
+    Dual<3> *f = o.fields();
+    for (int i = 0; i < CellG<Dual<3>, NDOF>::kFields; i++)
+        f[i] = Dual<3>(cg[i * L]);
+    for (int v = 0; v < m.nvert; v++)
+        if (m.cell2node[c * m.nvert + v] == sd.node)
+            for (int i = 0; i < CellG<Dual<3>, NDOF>::kFields; i++)
+                for (int d = 0; d < 3; d++)
+                    f[i].d[d] += cg[i * L + 1 + 3 * v + d];
+}
+
+template <int NDOF>
+DNDSB_D void lanes_load(const real *cg, const MeshD &m, int64_t c, const SeedDir &sd, CellG<Dual<1>, NDOF> &o)
+{
+    const int L = 1 + 3 * m.nvert;
+    Dual<1> *f = o.fields();
+    real dx[3 * kGeoMaxVert];
+    for (int v = 0; v < m.nvert; v++)
+        for (int d = 0; d < 3; d++)
+            dx[v * 3 + d] = sd.dX[(int64_t)m.cell2node[c * m.nvert + v] * 3 + d];
+    for (int i = 0; i < CellG<Dual<1>, NDOF>::kFields; i++)
+    {
+        real a = 0;
+        for (int l = 0; l < 3 * m.nvert; l++)
+            a += cg[i * L + 1 + l] * dx[l];
+        f[i] = Dual<1>(cg[i * L]);
+        f[i].d[0] = a;
+    }
+}
+
+// geometry of cell c: from the cache when there is one, else recomputed
+template <int DIM, int NDOF, typename T, typename Seed>
+DNDSB_D void cell_geo_or_lanes(const real *lanes, const MeshD &m, int intOrder, int nGc, bool aniso, int64_t c, const Seed &sd,
+                               CellG<T, NDOF> &o);
 
 template <typename T>
 struct FaceG
@@ -130,6 +172,16 @@ DNDSB_D void cell_geo(const MeshD &m, int intOrder, int nGc, bool aniso, int64_t
     }
     for (int k = 0; k < NDOF; k++)
         o.moment[k] = acc[k] / acc[0];
+}
+
+template <int DIM, int NDOF, typename T, typename Seed>
+DNDSB_D void cell_geo_or_lanes(const real *lanes, const MeshD &m, int intOrder, int nGc, bool aniso, int64_t c, const Seed &sd,
+                               CellG<T, NDOF> &o)
+{
+    if (lanes)
+        lanes_load<NDOF>(lanes + c * (int64_t)CellG<T, NDOF>::kFields * (1 + 3 * m.nvert), m, c, sd, o);
+    else
+        cell_geo<DIM, NDOF>(m, intOrder, nGc, aniso, c, sd, o);
 }
 
 // face area, mean normal and centre (FiniteVolume.cpp:352-543, as k_face_metrics)
@@ -286,13 +338,14 @@ DNDSB_D bool invert_t(const Dual<N> *A, Dual<N> *Ai)
 // with B_k uRec_k and b_k (u_k - u_c) accumulated point by point instead of stored.
 template <int DIM, int P, typename T, typename Seed>
 DNDSB_D void cell_local(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD &s, const real *dLamCell, const real *u,
-                        const real *uRec, int64_t c, const Seed &sd, bool wantRhs, bool wantRec, T *rhs, T *S, int &bad)
+                        const real *uRec, int64_t c, const Seed &sd, bool wantRhs, bool wantRec, T *rhs, T *S, int &bad,
+                        const real *lanes)
 {
     constexpr int NV = 5, NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     const int intOrder = vr.s.intOrder;
     const bool aniso = vr.s.anisotropicLengths;
     CellG<T, NDOF> gc, go;
-    cell_geo<DIM, NDOF>(m, intOrder, g.nGc, aniso, c, sd, gc);
+    cell_geo_or_lanes<DIM, NDOF>(lanes, m, intOrder, g.nGc, aniso, c, sd, gc);
     T A[R * R], Sacc[R * NV], flux[NV];
     for (int i = 0; i < R * R; i++)
         A[i] = 0.0;
@@ -313,7 +366,7 @@ DNDSB_D void cell_local(const MeshD &m, const GeomD &g, const VRD &vr, const Eul
         FaceG<T> fg;
         face_geo(m, intOrder, g.nGf, f, sd, fg);
         if (o >= 0)
-            cell_geo<DIM, NDOF>(m, intOrder, g.nGc, aniso, o, sd, go);
+            cell_geo_or_lanes<DIM, NDOF>(lanes, m, intOrder, g.nGc, aniso, o, sd, go);
         const CellG<T, NDOF> &g0 = side ? go : gc, &g1 = side ? gc : go;
         T w2L[P + 1], w0;
         face_weights<DIM, P>(m, vr, f, fg, g0.bary, o >= 0 ? g1.bary : nullptr, g0.scale, o >= 0 ? g1.scale : nullptr, w2L, w0);
@@ -509,7 +562,7 @@ template <int DIM, int P>
 DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_vjp(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ dLamCell,
                                                             const real *__restrict__ u, const real *__restrict__ uRec, const real *__restrict__ w,
                                                             const real *__restrict__ cot, real relax, const int32_t *__restrict__ patch,
-                                                            int maxSlot, real *__restrict__ share, int *err)
+                                                            int maxSlot, real *__restrict__ share, int *err, const real *__restrict__ lanes)
 {
     constexpr int NV = 5, NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     DNDSB_KERNEL_LOOP(e, m.nCell * maxSlot)
@@ -522,7 +575,7 @@ DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_vjp(MeshD m, GeomD g, VR
             SeedNode sd{node};
             Dual<3> rhs[NV], S[R * NV];
             int bad = 0;
-            cell_local<DIM, P>(m, g, vr, s, dLamCell, u, uRec, c, sd, w != nullptr, cot != nullptr, rhs, S, bad);
+            cell_local<DIM, P>(m, g, vr, s, dLamCell, u, uRec, c, sd, w != nullptr, cot != nullptr, rhs, S, bad, lanes);
             Dual<3> acc = 0.0;
             if (w)
                 for (int v = 0; v < NV; v++)
@@ -544,7 +597,8 @@ DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_vjp(MeshD m, GeomD g, VR
 template <int DIM, int P>
 DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_jvp(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ dLamCell,
                                                             const real *__restrict__ u, const real *__restrict__ uRec, const real *__restrict__ dX,
-                                                            real relax, real *__restrict__ dRhs, real *__restrict__ dRec, int *err)
+                                                            real relax, real *__restrict__ dRhs, real *__restrict__ dRec, int *err,
+                                                            const real *__restrict__ lanes)
 {
     constexpr int NV = 5, NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     DNDSB_KERNEL_LOOP(c, m.nCell)
@@ -552,7 +606,7 @@ DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_jvp(MeshD m, GeomD g, VR
         SeedDir sd{dX};
         Dual<1> rhs[NV], S[R * NV];
         int bad = 0;
-        cell_local<DIM, P>(m, g, vr, s, dLamCell, u, uRec, c, sd, dRhs != nullptr, dRec != nullptr, rhs, S, bad);
+        cell_local<DIM, P>(m, g, vr, s, dLamCell, u, uRec, c, sd, dRhs != nullptr, dRec != nullptr, rhs, S, bad, lanes);
         if (dRhs)
             for (int v = 0; v < NV; v++)
                 dRhs[c * NV + v] = rhs[v].d[0];
@@ -563,6 +617,34 @@ DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_coords_jvp(MeshD m, GeomD g, VR
             atomicOr(err, (int)DE_NONPHYSICAL);
     }
 }
+// the per-mesh cache of cell geometry lanes: one thread per (cell, vertex), that vertex's node seeded
+template <int DIM, int P>
+DNDSB_GLOBAL void __launch_bounds__(kGeoBlock) k_cell_lanes(MeshD m, GeomD g, VRD vr, real *__restrict__ lanes)
+{
+    constexpr int NDOF = ndof_of<DIM>(P), NF = CellG<real, NDOF>::kFields;
+    const int L = 1 + 3 * m.nvert;
+    DNDSB_KERNEL_LOOP(e, m.nCell * m.nvert)
+    {
+        const int64_t c = e / m.nvert;
+        const int v = (int)(e - c * m.nvert);
+        const int32_t node = m.cell2node[c * m.nvert + v];
+        bool dup = false;
+        for (int v2 = 0; v2 < v; v2++)
+            dup = dup || m.cell2node[c * m.nvert + v2] == node;
+        CellG<Dual<3>, NDOF> o;
+        cell_geo<DIM, NDOF>(m, vr.s.intOrder, g.nGc, vr.s.anisotropicLengths, c, SeedNode{node}, o);
+        real *cg = lanes + c * (int64_t)NF * L;
+        const Dual<3> *f = o.fields();
+        for (int i = 0; i < NF; i++)
+        {
+            if (v == 0)
+                cg[i * L] = f[i].v;
+            for (int d = 0; d < 3; d++)
+                cg[i * L + 1 + 3 * v + d] = dup ? 0.0 : f[i].d[d];
+        }
+    }
+}
+
 // Share of one (boundary cell, cell vertex) in the derivative of the pressure force
 // J = sum over the zone's faces and points of p(U) (n . dir) |J| w (k_pressure_force) with respect to
 // the vertex coordinates: the cell's basis and its faces' geometry depend on its own nodes only.
@@ -654,25 +736,40 @@ void coords_vjp_launch(const MeshD &m, const GeomD &g, const VRD &vr, const Eule
     const int64_t n = m.nCell * ws.maxSlot;
     const real relax = vr.s.jacobiRelax;
     if (vr.P == 1)
-        DNDSB_LAUNCH((k_coords_vjp<DIM, 1>), n, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, w, cot, relax, ws.patch, ws.maxSlot, ws.share, err);
+        DNDSB_LAUNCH((k_coords_vjp<DIM, 1>), n, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, w, cot, relax, ws.patch, ws.maxSlot, ws.share, err,
+                     ws.lanes);
     else if (vr.P == 2)
-        DNDSB_LAUNCH((k_coords_vjp<DIM, 2>), n, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, w, cot, relax, ws.patch, ws.maxSlot, ws.share, err);
+        DNDSB_LAUNCH((k_coords_vjp<DIM, 2>), n, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, w, cot, relax, ws.patch, ws.maxSlot, ws.share, err,
+                     ws.lanes);
     else
         DNDSB_LAUNCH((k_coords_vjp<DIM, PTop>), n, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, w, cot, relax, ws.patch, ws.maxSlot, ws.share,
-                     err);
+                     err, ws.lanes);
 }
 
 template <int DIM>
 void coords_jvp_launch(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD &es, const real *dLamCell, const real *dX, const real *u,
-                       const real *uRec, real *dRhs, real *dRec, int *err, cudaStream_t st)
+                       const real *uRec, real *dRhs, real *dRec, int *err, const real *lanes, cudaStream_t st)
 {
     constexpr int PTop = DIM == 2 ? 3 : 2;
     const real relax = vr.s.jacobiRelax;
     if (vr.P == 1)
-        DNDSB_LAUNCH((k_coords_jvp<DIM, 1>), m.nCell, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, dX, relax, dRhs, dRec, err);
+        DNDSB_LAUNCH((k_coords_jvp<DIM, 1>), m.nCell, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, dX, relax, dRhs, dRec, err, lanes);
     else if (vr.P == 2)
-        DNDSB_LAUNCH((k_coords_jvp<DIM, 2>), m.nCell, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, dX, relax, dRhs, dRec, err);
+        DNDSB_LAUNCH((k_coords_jvp<DIM, 2>), m.nCell, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, dX, relax, dRhs, dRec, err, lanes);
     else
-        DNDSB_LAUNCH((k_coords_jvp<DIM, PTop>), m.nCell, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, dX, relax, dRhs, dRec, err);
+        DNDSB_LAUNCH((k_coords_jvp<DIM, PTop>), m.nCell, kGeoBlock, st, m, g, vr, es, dLamCell, u, uRec, dX, relax, dRhs, dRec, err, lanes);
+}
+
+template <int DIM>
+void coords_lanes_launch(const MeshD &m, const GeomD &g, const VRD &vr, real *lanes, cudaStream_t st)
+{
+    constexpr int PTop = DIM == 2 ? 3 : 2;
+    const int64_t n = m.nCell * m.nvert;
+    if (vr.P == 1)
+        DNDSB_LAUNCH((k_cell_lanes<DIM, 1>), n, kGeoBlock, st, m, g, vr, lanes);
+    else if (vr.P == 2)
+        DNDSB_LAUNCH((k_cell_lanes<DIM, 2>), n, kGeoBlock, st, m, g, vr, lanes);
+    else
+        DNDSB_LAUNCH((k_cell_lanes<DIM, PTop>), n, kGeoBlock, st, m, g, vr, lanes);
 }
 } // namespace dndsb

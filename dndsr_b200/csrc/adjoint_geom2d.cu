@@ -9,6 +9,7 @@ template void coords_vjp_launch<2>(const MeshD &, const GeomD &, const VRD &, co
                                    const real *, const real *, const CoordAdjWs &, int *, cudaStream_t);
 template void pressure_force_coords_launch<2>(const MeshD &, const GeomD &, const VRD &, real, int, const real *, const real *, const real *,
                                               const CoordAdjWs &, cudaStream_t);
-template void coords_jvp_launch<2>(const MeshD &, const GeomD &, const VRD &, const EulerSettingsD &, const real *, const real *, const real *,
-                                   const real *, real *, real *, int *, cudaStream_t);
+template void coords_jvp_launch<2>(const MeshD &, const GeomD &, const VRD &, const EulerSettingsD &, const real *, const real *,
+                                   const real *, const real *, real *, real *, int *, const real *, cudaStream_t);
+template void coords_lanes_launch<2>(const MeshD &, const GeomD &, const VRD &, real *, cudaStream_t);
 } // namespace dndsb

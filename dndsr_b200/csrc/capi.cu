@@ -488,7 +488,7 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: the mesh has boundary faces; set their boundary table first");
         if (nVars != 5)
             return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: needs nVars = 5");
-        int rc = coords_jvp(v->mesh->d, v->g, v->vr, nullptr, nullptr, dX, u, uRec, nullptr, dRecNew, v->errWord, S(stream));
+        int rc = coords_jvp(v->mesh->d, v->g, v->vr, nullptr, nullptr, v->coordWs, dX, u, uRec, nullptr, dRecNew, v->errWord, S(stream));
         if (rc == ST_UNSUPPORTED)
             return fail(DNDSB_E_BADARG, "dndsb_vr_iter_jvp_coords: VR degree 1-2 in 3-D, 1-3 in 2-D");
         return status_msg(rc, "dndsb_vr_iter_jvp_coords");
@@ -671,7 +671,7 @@ extern "C"
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
         dndsb_vr *v = e->vr;
-        int rc = coords_jvp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, dX, u, uRec, dRhs, nullptr, e->e.errWord, S(stream));
+        int rc = coords_jvp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, v->coordWs, dX, u, uRec, dRhs, nullptr, e->e.errWord, S(stream));
         if (rc == ST_UNSUPPORTED)
             return fail(rc, "dndsb_eval_rhs_jvp_coords: needs nVars = 5, ignoreVis, and VR degree 1-2 in 3-D, 1-3 in 2-D");
         return status_msg(rc, "dndsb_eval_rhs_jvp_coords");

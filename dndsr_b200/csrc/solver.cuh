@@ -231,14 +231,16 @@ struct CoordAdjWs
     int32_t *patch = nullptr;                 // [nCell][maxSlot] patch nodes of each cell, -1 padded
     int64_t *start = nullptr, *ent = nullptr; // node -> (cell, slot) entries, CSR in entry order
     real *share = nullptr;                    // [nCell][maxSlot][3]
+    real *lanes = nullptr;                    // [nCell][10 + NDOF][1 + 3 nvert] cell geometry and its vertex derivatives
+    bool noLanes = false;                     // no memory for the lanes: geometry recomputed per use
 };
 int coords_ws_build(const MeshD &m, CoordAdjWs &ws);
 void coords_ws_free(CoordAdjWs &ws);
 // s == nullptr: the VR sweep only (w unused); otherwise EvaluateRHS (w) and/or the sweep (cot)
 int coords_vjp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, CoordAdjWs &ws, const real *w,
                const real *cot, const real *u, const real *uRec, real *dX, int *errWord, cudaStream_t st);
-int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, const real *dX, const real *u,
-               const real *uRec, real *dRhs, real *dRec, int *errWord, cudaStream_t st);
+int coords_jvp(const MeshD &m, const GeomD &g, const VRD &vr, const EulerSettingsD *s, const real *dLamCell, CoordAdjWs &ws, const real *dX,
+               const real *u, const real *uRec, real *dRhs, real *dRec, int *errWord, cudaStream_t st);
 // d/dX of the pressure force of one boundary zone along dir (pressure_force's objective)
 int pressure_force_coords(const MeshD &m, const GeomD &g, const VRD &vr, real gamma, int zone, const real *dir, const real *u, const real *uRec,
                           CoordAdjWs &ws, real *dX, cudaStream_t st);
