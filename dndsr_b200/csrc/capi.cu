@@ -26,6 +26,7 @@ struct dndsb_vr
     VRD vr;
     CoordAdjWs coordWs; // node-coordinate derivatives: patches and shares, built on first use
     real *limSec = nullptr; // WBAP limiter: matrixSecondary per interior face [nFace][2][R][R], built on first use
+    real *siFace = nullptr; // smooth indicator: per-face terms [nFace][4], allocated on first use
     int *errWord = nullptr;
     bool metrics = false, base = false, coeff = false;
     int bndNVars = 0; // number of variables of the boundary table's values
@@ -310,6 +311,7 @@ extern "C"
             dev_free(p);
         coords_ws_free(v->coordWs);
         dev_free(v->limSec);
+        dev_free(v->siFace);
         delete v;
         return DNDSB_OK;
     }
@@ -745,7 +747,7 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_vr_smooth_indicator: null argument");
         if (!v->coeff)
             return fail(DNDSB_E_BADARG, "dndsb_vr_smooth_indicator: call construct_rec_coeff first");
-        int rc = smooth_indicator(v->mesh->d, v->g, v->vr, nVars, u, uRec, si, S(stream));
+        int rc = smooth_indicator(v->mesh->d, v->g, v->vr, nVars, u, uRec, &v->siFace, si, S(stream));
         if (rc == ST_UNSUPPORTED)
             return fail(DNDSB_E_BADARG, "dndsb_vr_smooth_indicator: 3-D meshes, VR degree 1-2, 5 or 6 variables");
         return status_msg(rc, "dndsb_vr_smooth_indicator");

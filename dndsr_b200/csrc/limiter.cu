@@ -3,7 +3,8 @@
 //   k_lim_secondary     VariationalReconstruction.cpp:840-866 matrixSecondary: per interior face the
 //                       maps between the two cells' derivative bases at the face centre
 //                       (DiffI^-1 DiffJ and DiffJ^-1 DiffI), built once per reconstruction;
-//   k_smooth_indicator  VariationalReconstruction_LimiterProcedure.hxx:40-108 (density and energy);
+//   k_smooth_face/_gather  VariationalReconstruction_LimiterProcedure.hxx:40-108 (density and energy),
+//                       each interior face's terms once, then summed per cell;
 //   k_limiter_wbap_c    VariationalReconstruction_LimiterProcedure.hxx:188-334 with the WBAP-L2 biway
 //                       and multiway functions (Limiters.hpp:361-470) in the characteristic variables of
 //                       the face (Gas.hpp:120-200 eigenvectors, Geometric.hpp:135-160 normal frame).
@@ -78,59 +79,75 @@ DNDSB_D void lim_w2L(const VRD &vr, int64_t f, real *w2L)
     }
 }
 
+// per interior face: the jump and mean functionals of density and energy at the face centre, times
+// the face area (the terms both cells of the face add); boundary faces contribute nothing
 template <int P>
-DNDSB_GLOBAL void k_smooth_indicator(MeshD m, GeomD g, VRD vr, int nv, const real *__restrict__ u, const real *__restrict__ uRec,
-                                     real *__restrict__ si)
+DNDSB_GLOBAL void k_smooth_face(MeshD m, GeomD g, VRD vr, int nv, const real *__restrict__ u, const real *__restrict__ uRec,
+                                real *__restrict__ faceTerm)
 {
     constexpr int NDOF = ndof_of<3>(P), R = NDOF - 1;
     const int vs[2] = {0, 4};
+    DNDSB_KERNEL_LOOP(f, m.nFace)
+    {
+        const int c1 = m.face2cell[f * 2 + 1];
+        real *out = faceTerm + f * 4;
+        if (c1 < 0)
+        {
+            for (int i = 0; i < 4; i++)
+                out[i] = 0;
+            continue;
+        }
+        real val[2][NDOF * 2];
+        for (int sd = 0; sd < 2; sd++)
+        {
+            const int64_t cc = m.face2cell[f * 2 + sd];
+            real p[3], T[NDOF * NDOF];
+            for (int d = 0; d < 3; d++)
+                p[d] = g.faceCent[f * 3 + d] + (sd ? m.facePShift[f * 3 + d] : 0.0);
+            cell_basis<3, NDOF>(&g.cellCent[cc * 3], &g.cellScale[cc * 3], &vr.baseMoment[cc * NDOF], vr.s.anisotropicLengths, p, NDOF, T);
+            for (int r = 0; r < NDOF; r++)
+                for (int q = 0; q < 2; q++)
+                {
+                    real a = 0;
+                    for (int j = 0; j < R; j++)
+                        a += T[r * NDOF + 1 + j] * uRec[(cc * R + j) * nv + vs[q]];
+                    if (r == 0)
+                        a += u[cc * nv + vs[q]];
+                    val[sd][r * 2 + q] = a;
+                }
+        }
+        real w2L[P + 1];
+        lim_w2L<P>(vr, f, w2L);
+        real IJ[2] = {0, 0}, IS[2] = {0, 0};
+        for (int ob = P; ob >= 0; ob--)
+            for (int kk = Basis<3>::order_start(ob); kk < Basis<3>::order_start(ob + 1); kk++)
+                for (int q = 0; q < 2; q++)
+                {
+                    const real jm = (val[0][kk * 2 + q] - val[1][kk * 2 + q]) * 0.5, av = (val[0][kk * 2 + q] + val[1][kk * 2 + q]) * 0.5;
+                    IJ[q] += jm * jm * Basis<3>::ncomb(kk) * w2L[ob];
+                    IS[q] += av * av * Basis<3>::ncomb(kk) * w2L[ob];
+                }
+        for (int q = 0; q < 2; q++)
+            out[q] = IJ[q] * g.faceArea[f], out[2 + q] = IS[q] * g.faceArea[f];
+    }
+}
+
+// per cell: the sums over its faces, si = sqrt(max over the two variables of IJ / IS) maxOrder^2
+DNDSB_GLOBAL void k_smooth_gather(MeshD m, int maxOrder, const real *__restrict__ faceTerm, real *__restrict__ si)
+{
     DNDSB_KERNEL_LOOP(c, m.nCell)
     {
-        real S[2][2] = {{0, 0}, {0, 0}};
+        real S[4] = {0, 0, 0, 0};
         for (int k = 0; k < m.nf; k++)
         {
-            const int o = m.cellNbr[c * m.nf + k];
-            if (o < 0)
-                continue;
             const int64_t f = m.cell2face[c * m.nf + k] >> 1;
-            real val[2][NDOF * 2];
-            for (int s = 0; s < 2; s++)
-            {
-                const int64_t cc = s == 0 ? c : o;
-                const int sd = m.face2cell[f * 2] == cc ? 0 : 1;
-                real p[3], T[NDOF * NDOF];
-                for (int d = 0; d < 3; d++)
-                    p[d] = g.faceCent[f * 3 + d] + (sd ? m.facePShift[f * 3 + d] : 0.0);
-                cell_basis<3, NDOF>(&g.cellCent[cc * 3], &g.cellScale[cc * 3], &vr.baseMoment[cc * NDOF], vr.s.anisotropicLengths, p, NDOF, T);
-                for (int r = 0; r < NDOF; r++)
-                    for (int q = 0; q < 2; q++)
-                    {
-                        real a = 0;
-                        for (int j = 0; j < R; j++)
-                            a += T[r * NDOF + 1 + j] * uRec[(cc * R + j) * nv + vs[q]];
-                        if (r == 0)
-                            a += u[cc * nv + vs[q]];
-                        val[s][r * 2 + q] = a;
-                    }
-            }
-            real w2L[P + 1];
-            lim_w2L<P>(vr, f, w2L);
-            real IJ[2] = {0, 0}, IS[2] = {0, 0};
-            for (int ob = P; ob >= 0; ob--)
-                for (int kk = Basis<3>::order_start(ob); kk < Basis<3>::order_start(ob + 1); kk++)
-                    for (int q = 0; q < 2; q++)
-                    {
-                        const real jm = (val[0][kk * 2 + q] - val[1][kk * 2 + q]) * 0.5, av = (val[0][kk * 2 + q] + val[1][kk * 2 + q]) * 0.5;
-                        IJ[q] += jm * jm * Basis<3>::ncomb(kk) * w2L[ob];
-                        IS[q] += av * av * Basis<3>::ncomb(kk) * w2L[ob];
-                    }
-            for (int q = 0; q < 2; q++)
-                S[q][0] += IJ[q] * g.faceArea[f], S[q][1] += IS[q] * g.faceArea[f];
+            for (int i = 0; i < 4; i++)
+                S[i] += faceTerm[f * 4 + i];
         }
         real sm = 0;
         for (int q = 0; q < 2; q++)
-            sm = fmax(sm, fabs(S[q][0] / (S[q][1] + kVerySmall)));
-        si[c] = sqrt(sm) * (real)(vr.s.maxOrder * vr.s.maxOrder);
+            sm = fmax(sm, fabs(S[q] / (S[2 + q] + kVerySmall)));
+        si[c] = sqrt(sm) * (real)(maxOrder * maxOrder);
     }
 }
 
@@ -342,14 +359,18 @@ int lim_secondary_build(const MeshD &m, const GeomD &g, const VRD &vr, real **se
     return ST_OK;
 }
 
-int smooth_indicator(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *u, const real *uRec, real *si, cudaStream_t st)
+int smooth_indicator(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *u, const real *uRec, real **faceTerm, real *si,
+                     cudaStream_t st)
 {
     if (m.dim != 3 || vr.P < 1 || vr.P > 2 || (nv != 5 && nv != 6))
         return ST_UNSUPPORTED;
+    if (!*faceTerm && dev_alloc((void **)faceTerm, sizeof(real) * 4 * m.nFace) != cudaSuccess)
+        return ST_CUDA;
     if (vr.P == 1)
-        DNDSB_LAUNCH(k_smooth_indicator<1>, m.nCell, 128, st, m, g, vr, nv, u, uRec, si);
+        DNDSB_LAUNCH(k_smooth_face<1>, m.nFace, 128, st, m, g, vr, nv, u, uRec, *faceTerm);
     else
-        DNDSB_LAUNCH(k_smooth_indicator<2>, m.nCell, 128, st, m, g, vr, nv, u, uRec, si);
+        DNDSB_LAUNCH(k_smooth_face<2>, m.nFace, 128, st, m, g, vr, nv, u, uRec, *faceTerm);
+    DNDSB_LAUNCH(k_smooth_gather, m.nCell, 256, st, m, vr.s.maxOrder, *faceTerm, si);
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 

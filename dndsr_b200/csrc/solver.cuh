@@ -212,7 +212,9 @@ int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const
 // reference's EvaluateDt and EvaluateRHS calls
 // ---- WBAP_C limiter (limiter.cu; 3-D, VR degree 1-2) ----
 int lim_secondary_build(const MeshD &m, const GeomD &g, const VRD &vr, real **sec, int *errWord, cudaStream_t st);
-int smooth_indicator(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *u, const real *uRec, real *si, cudaStream_t st);
+// faceTerm: [nFace][4] scratch, allocated on first use
+int smooth_indicator(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *u, const real *uRec, real **faceTerm, real *si,
+                     cudaStream_t st);
 int limiter_wbap_c(const MeshD &m, const GeomD &g, const VRD &vr, const real *sec, int nv, real gamma, const real *u, const real *uRec,
                    const real *si, real *uRecNew, real threshold, real nStd, int ifAll, cudaStream_t st);
 
