@@ -650,10 +650,14 @@ def run_ours(args, rank, world, local_rank):
                            "vr_GBps": B_VR * nc / (t_vr * 1e-3) / 1e9, "rhs_GBps": B_RHS * nc / (t_rhs * 1e-3) / 1e9},
             "clocks": clk.summary()}
     if world == 1 and not args.no_steady:
-        line["time_to_1e-10"] = run_dual_time(args)
-        line["steady"] = run_steady(args)
-        line["adjoint_cost"] = run_adjoint_cost(args)
-        if not args.no_sa:
+        blocks = set(args.blocks.split(","))
+        if "time_to_1e-10" in blocks:
+            line["time_to_1e-10"] = run_dual_time(args)
+        if "steady" in blocks:
+            line["steady"] = run_steady(args)
+        if "adjoint_cost" in blocks:
+            line["adjoint_cost"] = run_adjoint_cost(args)
+        if not args.no_sa and "sa_plate" in blocks:
             line["sa_plate"] = run_sa_plate(args)
     if world == 1 and not args.no_cpu_baseline:
         v, steps, el, cells = cpu_baseline_oracle(args.sample_n, p, args.sample_seconds, n_cores())
@@ -681,6 +685,8 @@ def main():
     ap.add_argument("--steady-iters", type=int, default=100)
     ap.add_argument("--adjoint-mesh", type=int, nargs=3, default=(80, 40, 13))
     ap.add_argument("--no-sa", action="store_true")
+    # the extra measurement blocks after the headline, comma separated (a subset for profiling runs)
+    ap.add_argument("--blocks", default="time_to_1e-10,steady,adjoint_cost,sa_plate")
     ap.add_argument("--sa-mesh", type=int, nargs=3, default=(300, 100, 100))
     ap.add_argument("--sa-iters", type=int, default=30)
     args = ap.parse_args()
