@@ -5,7 +5,7 @@
 //   grad U_M = (grad U_L + grad U_R) / 2 + (U_R - U_L) (x) n / d_GRP,
 // with grad U = D1 phi . uRec of each side and the flux of Gas.hpp:1594-1655 on the primitive
 // gradient (Gas.hpp:1677-1698).  Fv depends on the 20 numbers (U_M, grad U_M).  Their cotangents
-// (VJP): one Dual<5> pass for U_M at fixed gradient, and for grad U_M the transposes of the two
+// (VJP): five Dual<1> passes for U_M at fixed gradient, and for grad U_M the transposes of the two
 // maps that are linear in it (conservative -> primitive gradient, primitive gradient -> flux);
 // the chain above carries them to (u, uRec) of both cells.  The JVP is one Dual<1> pass.  Both add to the
 // inviscid face arrays before their per-cell gathers.  Boundary faces carry no viscous flux in
@@ -18,7 +18,6 @@ namespace dndsb
 namespace
 {
 constexpr int NV = 5;
-using D5 = Dual<5>;
 using D1 = Dual<1>;
 
 // the 5-variable branch of point_viscous_flux (sa.cuh), on any scalar type
@@ -164,7 +163,7 @@ DNDSB_GLOBAL void k_rhs_vjp_visc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
             const real *n;
             visc_point<DIM, P>(m, g, vr, F, f, q, u, uRec, T0, T1, UL, UR, GL, GR, iD, n);
             // the face flux is -(F - Fv) |J| w: the cotangent of Fv is +|J| w gbar.  bar[0..4]: the
-            // cotangent of U_M (one Dual<5> pass at fixed grad U_M); bar[5..19]: of grad U_M
+            // cotangent of U_M (Dual<1> passes at fixed grad U_M); bar[5..19]: of grad U_M
             // (transposed linear maps at fixed U_M)
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
             real UMr[NV], GMr[3 * NV], Fvbar[NV], bar[20];
@@ -173,21 +172,22 @@ DNDSB_GLOBAL void k_rhs_vjp_visc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
             for (int d = 0; d < 3; d++)
                 for (int v = 0; v < NV; v++)
                     GMr[d * NV + v] = (GR[d * NV + v] + GL[d * NV + v]) * 0.5 + iD * (n[d] * (UR[v] - UL[v]));
+            // one Dual<1> pass per component of U_M: a fifth of the dual state of one Dual<5> pass, which
+            // spilled to local memory (the flux is cheap next to that traffic)
+#pragma unroll 1
+            for (int i = 0; i < NV; i++)
             {
-                D5 UM[NV], GM[3 * NV], GP[3 * NV], Fv[NV];
+                D1 UM[NV], GM[3 * NV], GP[3 * NV], Fv[NV];
                 for (int v = 0; v < NV; v++)
-                    UM[v] = D5::var(UMr[v], v);
-                for (int i = 0; i < 3 * NV; i++)
-                    GM[i] = D5(GMr[i]);
+                    UM[v] = D1::var(UMr[v], v == i ? 0 : -1);
+                for (int k = 0; k < 3 * NV; k++)
+                    GM[k] = D1(GMr[k]);
                 grad_cons2prim<NV>(UM, GM, GP, gamma);
                 visc_flux_t(s, UM, GP, n, Fv);
-                for (int i = 0; i < NV; i++)
-                {
-                    real a = 0;
-                    for (int k = 0; k < NV; k++)
-                        a += Fv[k].d[i] * Fvbar[k];
-                    bar[i] = a;
-                }
+                real a = 0;
+                for (int k = 0; k < NV; k++)
+                    a += Fv[k].d[0] * Fvbar[k];
+                bar[i] = a;
             }
             visc_grad_transpose(s, UMr, n, Fvbar, bar + NV);
             for (int v = 0; v < NV; v++)
