@@ -153,7 +153,11 @@ DNDSB_GLOBAL void k_rhs_vjp_visc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
         if (m.face2cell[f * 2 + 1] < 0)
             continue;
         ViscFace F = visc_face(m, g, f);
-        real *o0 = faceAdj + (f * 2) * W, *o1 = faceAdj + (f * 2 + 1) * W;
+        real *o0g = faceAdj + (f * 2) * W, *o1g = faceAdj + (f * 2 + 1) * W;
+        // the face's two cotangent rows accumulated over its Gauss points, stored once
+        real o0[W], o1[W];
+        for (int i = 0; i < W; i++)
+            o0[i] = o0g[i], o1[i] = o1g[i];
         real gbar[NV];
         for (int v = 0; v < NV; v++)
             gbar[v] = w[F.c0 * NV + v] / g.vol[F.c0] - w[F.c1 * NV + v] / g.vol[F.c1];
@@ -212,6 +216,8 @@ DNDSB_GLOBAL void k_rhs_vjp_visc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
                 }
             }
         }
+        for (int i = 0; i < W; i++)
+            o0g[i] = o0[i], o1g[i] = o1[i];
     }
 }
 
