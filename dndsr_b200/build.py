@@ -29,6 +29,13 @@ def up_to_date():
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
+def _headers_mtime():
+    d = os.path.join(HERE, "csrc")
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    hs = [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".cuh", ".h"))] + [os.path.join(inc, f) for f in os.listdir(inc)]
+    return max(os.path.getmtime(p) for p in hs)
+
+
 def build(force=False, verbose=False, jobs=None):
     if not force and up_to_date():
         return LIB
@@ -36,9 +43,13 @@ def build(force=False, verbose=False, jobs=None):
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
+    th = _headers_mtime()
     for s in sources():
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         objs.append(o)
+        # an object is reused when it is newer than its source and every header (headers are shared)
+        if not force and not verbose and os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(s), th):
+            continue
         cmd = [NVCC, *FLAGS, "-c", s, "-o", o]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

@@ -40,6 +40,7 @@ class EulerSettings(ctypes.Structure):
         ("nVars", ctypes.c_int), ("rsType", ctypes.c_int), ("rsFixScale", ctypes.c_double), ("rsIncFScale", ctypes.c_double),
         ("gamma", ctypes.c_double), ("Rgas", ctypes.c_double), ("muGas", ctypes.c_double), ("prGas", ctypes.c_double),
         ("TRef", ctypes.c_double), ("CSutherland", ctypes.c_double), ("muModel", ctypes.c_int), ("ignoreVis", ctypes.c_int),
+        ("rsMeanValueEig", ctypes.c_int),
     ]
 
 
@@ -79,6 +80,9 @@ SIGNATURES = {
     "dndsb_eval_lusgs_matrix_init": [_P, _P, _d, _d, _P, _P],
     "dndsb_eval_update_sgs": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _D, _P],
     "dndsb_eval_lusgs_matrix_vec": [_P, _d, _P, _P, _P, _P, _P],
+    "dndsb_eval_update_lusgs_forward": [_P, _d, _P, _P, _P, _P, _P, _P],
+    "dndsb_eval_update_lusgs_backward": [_P, _d, _P, _P, _P, _P, _P, _P],
+    "dndsb_eval_fix_umax_filter": [_P, _P, _P],
     "dndsb_eval_lusgs_matrix_vec_t": [_P, _d, _P, _P, _P, _P, _P],
     "dndsb_eval_update_sgs_t": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _P],
     "dndsb_eval_pressure_force": [_P, _i, _D, _P, _P, _D, _P, _P, _P],

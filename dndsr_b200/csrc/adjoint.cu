@@ -49,6 +49,7 @@ DNDSB_GLOBAL void k_rhs_vjp_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
     DNDSB_KERNEL_LOOP(ii, boundaryOnly ? m.nBndFace : m.nFace)
     {
         const int64_t f = boundaryOnly ? (int64_t)m.bndFace[ii] : ii;
+        const real *nMV = s.rsMeanValueEig ? &g.faceMeanNorm[f * 3] : nullptr; // batched mean-value eigenvalues
         int64_t c0 = m.face2cell[f * 2], c1 = m.face2cell[f * 2 + 1];
         bool bnd = c1 < 0;
         int zone = m.faceZone[f];
@@ -90,14 +91,14 @@ DNDSB_GLOBAL void k_rhs_vjp_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
                 D10 ULd[NV], URd[NV], ULmd[NV], URmd[NV];
                 for (int v = 0; v < NV; v++)
                     ULd[v] = D10::var(UL[v], v), URd[v] = D10::var(UR[v], 5 + v), ULmd[v] = D10(ULm[v]), URmd[v] = D10(URm[v]);
-                bad |= !riemann_flux(s.rsType, ULd, URd, ULmd, URmd, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+                bad |= !riemann_flux(s.rsType, ULd, URd, ULmd, URmd, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4, nMV);
                 for (int v = 0; v < NV; v++)
                     for (int i = 0; i < NV; i++)
                         ULbar[i] += F[v].d[i] * Fbar[v], URbar[i] += F[v].d[5 + i] * Fbar[v];
                 // pass 2: cell means ULm (0..4), URm (5..9) through the Roe averages
                 for (int v = 0; v < NV; v++)
                     ULd[v] = D10(UL[v]), URd[v] = D10(UR[v]), ULmd[v] = D10::var(ULm[v], v), URmd[v] = D10::var(URm[v], 5 + v);
-                bad |= !riemann_flux(s.rsType, ULd, URd, ULmd, URmd, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+                bad |= !riemann_flux(s.rsType, ULd, URd, ULmd, URmd, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4, nMV);
                 for (int v = 0; v < NV; v++)
                     for (int i = 0; i < NV; i++)
                         ULmbar[i] += F[v].d[i] * Fbar[v], URmbar[i] += F[v].d[5 + i] * Fbar[v];
@@ -114,7 +115,7 @@ DNDSB_GLOBAL void k_rhs_vjp_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
                 if (!bc_value<NV>(vr.bnd, zone, ULmd, &g.faceMeanNorm[f * 3], URmd))
                     for (int v = 0; v < NV; v++)
                         URmd[v] = ULmd[v];
-                bad |= !riemann_flux(s.rsType, ULd, URd, ULmd, URmd, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+                bad |= !riemann_flux(s.rsType, ULd, URd, ULmd, URmd, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4, nMV);
                 for (int v = 0; v < NV; v++)
                     for (int i = 0; i < NV; i++)
                         ULbar[i] += F[v].d[i] * Fbar[v], ULmbar[i] += F[v].d[5 + i] * Fbar[v];
@@ -172,6 +173,7 @@ DNDSB_GLOBAL void k_rhs_jvp_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
     const real gamma = s.gamma;
     DNDSB_KERNEL_LOOP(f, m.nFace)
     {
+        const real *nMV = s.rsMeanValueEig ? &g.faceMeanNorm[f * 3] : nullptr; // batched mean-value eigenvalues
         int64_t c0 = m.face2cell[f * 2], c1 = m.face2cell[f * 2 + 1];
         bool bnd = c1 < 0;
         int zone = m.faceZone[f];
@@ -236,7 +238,7 @@ DNDSB_GLOBAL void k_rhs_jvp_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
                 }
             }
             D1 F[NV], l0, l1, l4;
-            bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+            bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4, nMV);
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
             for (int v = 0; v < NV; v++)
                 acc[v] -= F[v].d[0] * JW;
@@ -480,7 +482,9 @@ int rhs_vjp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const r
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1, W = (R + 1) * NV;
     auto kf = k_rhs_vjp_face<DIM, P>;
-    const int roe = roe_scheme_of(ev.s.rsType) >= 0;
+    // the hand-reversed Roe kernel takes the point-normal eigenvalues; the batched mean-value variant
+    // (rsMeanValueEig with Roe_M1..M5) runs through the forward-mode face kernel on every face
+    const int roe = roe_scheme_of(ev.s.rsType) >= 0 && !(ev.s.rsMeanValueEig && ev.s.rsType >= RS_Roe_M1 && ev.s.rsType <= RS_Roe_M1 + 4);
     DNDSB_LAUNCH(kf, roe ? m.nBndFace : m.nFace, 64, st, m, g, vr, ev.s, w, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord, roe);
     if (roe)
     {

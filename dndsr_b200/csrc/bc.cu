@@ -161,7 +161,8 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
             real F[NV], l0, l1, l4;
             for (int v = 0; v < NV; v++)
                 F[v] = 0;
-            bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+            bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4,
+                                 s.rsMeanValueEig ? &g.faceMeanNorm[f * 3] : nullptr);
             if (NV == 6)
                 F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];

@@ -81,6 +81,9 @@ int status_msg(int rc, const char *where)
 }
 
 cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+// the batched mean-value Roe flux (rsMeanValueEig with Roe_M1..M5, Gas.hpp:1272-1408)
+bool mean_value_roe(const EulerSettingsD &s) { return s.rsMeanValueEig && s.rsType >= RS_Roe_M1 && s.rsType <= RS_Roe_M1 + 4; }
 } // namespace
 
 namespace dndsb
@@ -520,6 +523,7 @@ extern "C"
         d.nVars = s->nVars, d.rsType = s->rsType, d.rsFixScale = s->rsFixScale, d.rsIncFScale = s->rsIncFScale;
         d.gamma = s->gamma, d.Rgas = s->Rgas, d.muGas = s->muGas, d.prGas = s->prGas, d.TRef = s->TRef, d.CSutherland = s->CSutherland;
         d.muModel = s->muModel, d.ignoreVis = s->ignoreVis;
+        d.rsMeanValueEig = s->rsMeanValueEig;
         d.derive();
         const MeshD &m = vr->mesh->d;
         int rc = 0;
@@ -641,6 +645,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp_coords: VR not constructed");
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (mean_value_roe(e->e.s))
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_rhs_vjp_coords: rsMeanValueEig with Roe_M1..M5 is differentiated with respect to the state only");
         dndsb_vr *v = e->vr;
         int rc = coords_vjp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, v->coordWs, w, nullptr, u, uRec, dX, e->e.errWord, S(stream));
         if (rc == ST_UNSUPPORTED)
@@ -657,6 +663,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_residual_vjp_coords: VR not constructed");
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_residual_vjp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (mean_value_roe(e->e.s))
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_residual_vjp_coords: rsMeanValueEig with Roe_M1..M5 is differentiated with respect to the state only");
         dndsb_vr *v = e->vr;
         int rc = coords_vjp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, v->coordWs, w, cot, u, uRec, dX, e->e.errWord, S(stream));
         if (rc == ST_UNSUPPORTED)
@@ -672,6 +680,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp_coords: VR not constructed");
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp_coords: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (mean_value_roe(e->e.s))
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_rhs_jvp_coords: rsMeanValueEig with Roe_M1..M5 is differentiated with respect to the state only");
         dndsb_vr *v = e->vr;
         int rc = coords_jvp(v->mesh->d, v->g, v->vr, &e->e.s, e->e.deltaLambdaCell, v->coordWs, dX, u, uRec, dRhs, nullptr, e->e.errWord, S(stream));
         if (rc == ST_UNSUPPORTED)
@@ -710,6 +720,32 @@ extern "C"
         return status_msg(update_sgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate, uIncIsZero,
                                      sumIncHost, S(stream)),
                           "dndsb_eval_update_sgs");
+    }
+
+    int dndsb_eval_update_lusgs_forward(dndsb_eval *e, double alphaDiag, const double *rhs, const double *u, const double *uInc,
+                                        const double *jdiag, double *uIncNew, void *stream)
+    {
+        if (!e || !rhs || !u || !uInc || !jdiag || !uIncNew)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_lusgs_forward: null argument");
+        return status_msg(update_lusgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, 1, S(stream)),
+                          "dndsb_eval_update_lusgs_forward");
+    }
+
+    int dndsb_eval_update_lusgs_backward(dndsb_eval *e, double alphaDiag, const double *rhs, const double *u, const double *uInc,
+                                         const double *jdiag, double *uIncNew, void *stream)
+    {
+        if (!e || !rhs || !u || !uInc || !jdiag || !uIncNew)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_update_lusgs_backward: null argument");
+        return status_msg(update_lusgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, 0, S(stream)),
+                          "dndsb_eval_update_lusgs_backward");
+    }
+
+    int dndsb_eval_fix_umax_filter(dndsb_eval *e, double *u, void *stream)
+    {
+        (void)stream;
+        if (!e || !u)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_fix_umax_filter: null argument");
+        return DNDSB_OK; // EulerEvaluator.hxx:1318-1323 returns before touching u
     }
 
     int dndsb_eval_lusgs_matrix_vec(dndsb_eval *e, double alphaDiag, const double *u, const double *uInc, const double *jdiag,

@@ -539,10 +539,12 @@ struct RoeWavesT
     T a0, a1, a4, a23T[3], vRoeN;
 };
 
+// nE: normal of the Roe normal velocity (the point normal n, or the face's mean normal for the
+// batched mean-value eigenvalues of Gas.hpp:1272-1408)
 template <typename T, typename TN>
-DNDSB_HD void roe_waves(const T *incU, const TN *n, const RoeAvgT<T> &r, real gamma, RoeWavesT<T> &w)
+DNDSB_HD void roe_waves(const T *incU, const TN *n, const RoeAvgT<T> &r, real gamma, RoeWavesT<T> &w, const TN *nE = nullptr)
 {
-    w.vRoeN = dot3v(r.v, n);
+    w.vRoeN = dot3v(r.v, nE ? nE : n);
     T incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
     T a23[3] = {incU[1] - incU[0] * r.v[0], incU[2] - incU[0] * r.v[1], incU[3] - incU[0] * r.v[2]};
     T a23n = dot3v(a23, n);
@@ -638,17 +640,22 @@ DNDSB_HD void roe_entropy_fix(int es, const T &aL, const T &aR, const T &aAve, c
 // Returns false when a state is non-physical (the caller records an error).
 // The Roe averages r come from the cell-mean states (Gas.hpp:229-259) and are
 // shared by all Gauss points of a face.
+// nMean (may be null): the face's mean normal, given when the settings ask for the batched
+// mean-value eigenvalues (rsMeanValueEig != 0 with Roe_M1..Roe_M5, EulerEvaluator_EvaluateDt.hxx:1259-1270):
+// RoeFlux_IdealGas_HartenYee_Batch (Gas.hpp:1272-1408) then takes the eigenvalues, the entropy fix
+// and the Roe normal velocity along it, the physical fluxes and jump projections along n.
 template <typename T, typename TN>
 DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T> &r, const TN *n, real gamma, real dLambda, real fixScale,
-                               real incFScale, T F[5], T &lam0, T &lam123, T &lam4)
+                               real incFScale, T F[5], T &lam0, T &lam123, T &lam4, const TN *nMean = nullptr)
 {
     T FL[5], FR[5], pL, pR, aL2, aR2;
     phys_flux(UL, n, gamma, FL, pL, aL2);
     phys_flux(UR, n, gamma, FR, pR, aR2);
     bool ok = UL[0] > 0 && UR[0] > 0 && r.asqr > 0;
-    T vRoe0 = dot3v(r.v, n);
+    const TN *nE = (nMean && rs >= RS_Roe_M1 && rs <= RS_Roe_M1 + 4) ? nMean : n;
+    T vRoe0 = dot3v(r.v, nE);
     lam0 = fabs(vRoe0 - r.a), lam123 = fabs(vRoe0), lam4 = fabs(vRoe0 + r.a);
-    T vLm0 = dot3v(r.vL, n), vRm0 = dot3v(r.vR, n);
+    T vLm0 = dot3v(r.vL, nE), vRm0 = dot3v(r.vR, nE);
     T incU[5];
     for (int i = 0; i < 5; i++)
         incU[i] = UR[i] - UL[i];
@@ -729,7 +736,7 @@ DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T
     T VAve = sqrt(r.vsqr);
     roe_entropy_fix(es, r.aL, r.aR, r.a, vLm0, vRm0, vRoe0, VAve, dLambda, fixScale, incFScale, lam0, lam123, lam4);
     RoeWavesT<T> w;
-    roe_waves(incU, n, r, gamma, w);
+    roe_waves(incU, n, r, gamma, w, nE);
     T incF[5];
     roe_dissipation(w, n, r, lam0, lam123, lam4, incF);
     for (int i = 0; i < 5; i++)
@@ -739,11 +746,11 @@ DNDSB_HD bool riemann_flux_pre(int rs, const T *UL, const T *UR, const RoeAvgT<T
 
 template <typename T, typename TN>
 DNDSB_HD bool riemann_flux(int rs, const T *UL, const T *UR, const T *ULm, const T *URm, const TN *n, real gamma, real dLambda,
-                           real fixScale, real incFScale, T F[5], T &lam0, T &lam123, T &lam4)
+                           real fixScale, real incFScale, T F[5], T &lam0, T &lam123, T &lam4, const TN *nMean = nullptr)
 {
     RoeAvgT<T> r;
     roe_average(ULm, URm, gamma, r);
-    return riemann_flux_pre(rs, UL, UR, r, n, gamma, dLambda, fixScale, incFScale, F, lam0, lam123, lam4);
+    return riemann_flux_pre(rs, UL, UR, r, n, gamma, dLambda, fixScale, incFScale, F, lam0, lam123, lam4, nMean);
 }
 
 // Gas.hpp:1677-1698 GradientCons2Prim_IdealGas; G and GP are [3][NV]; ir = 1 / U[0]

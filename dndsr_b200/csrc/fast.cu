@@ -221,8 +221,11 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
             else // SA: eddy viscosity in the momentum/energy fluxes and the nuTilde diffusion flux
                 point_viscous_flux<NV>(s, UM, GP, n, false, Fv);
         }
-        real F[NV], l0, l1, l4;
-        bool ok = riemann_flux_pre(s.rsType, UL, UR, fd->r, n, gamma, fd->dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+        real F[NV], l0, l1, l4, nm[3];
+        if (s.rsMeanValueEig) // batched mean-value eigenvalues along the face's mean normal
+            nm[0] = g.faceMeanNorm[f * 3], nm[1] = g.faceMeanNorm[f * 3 + 1], nm[2] = g.faceMeanNorm[f * 3 + 2];
+        bool ok = riemann_flux_pre(s.rsType, UL, UR, fd->r, n, gamma, fd->dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4,
+                                   s.rsMeanValueEig ? (const real *)nm : nullptr);
         if (NV == 6)
             F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
 #pragma unroll

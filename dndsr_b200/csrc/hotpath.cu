@@ -170,7 +170,8 @@ DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const r
                 point_viscous_flux<NV>(s, UM, GP, n, false, Fv);
             }
             real F[NV], l0, l1, l4;
-            bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4);
+            bad |= !riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4,
+                                 s.rsMeanValueEig ? &g.faceMeanNorm[f * 3] : nullptr);
             if (NV == 6)
                 F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
@@ -360,6 +361,46 @@ DNDSB_GLOBAL void k_sgs_color(MeshD m, GeomD g, real gamma, const real *__restri
             real nv = buf[v] * id;
             absInc[c * NV + v] = fabs(nv - uIncNew[c * NV + v]);
             uIncNew[c * NV + v] = nv;
+        }
+    }
+}
+
+// UpdateLUSGSForward / UpdateLUSGSBackward (EulerEvaluator.hxx:376-529): forward
+//   uIncNew_c = D_c^-1 (rhs_c - sum_{o < c} (alpha/2)(A_f/V_c) dF(u_o; uInc_o)),
+// backward uIncNew_c += D_c^-1 (- sum_{o > c} of the same).  "Lower" and "upper" are cell indices,
+// as in the reference.  cells == nullptr: every cell of [cBeg, cEnd) in one launch (uInc distinct from
+// uIncNew, so the cells are independent); otherwise the cells of one colour (in-place sweep).
+template <int NV>
+DNDSB_GLOBAL void k_lusgs_sweep(MeshD m, GeomD g, real gamma, const real *__restrict__ lamFace, const int32_t *__restrict__ cells,
+                                int64_t cBeg, int64_t cEnd, real alphaDiag, const real *__restrict__ rhs, const real *__restrict__ u,
+                                const real *uInc, real *uIncNew, const real *__restrict__ jdiag, int forward)
+{
+    DNDSB_KERNEL_LOOP(ii, cEnd - cBeg)
+    {
+        int64_t c = cells ? (int64_t)cells[cBeg + ii] : cBeg + ii;
+        real buf[NV];
+        for (int v = 0; v < NV; v++)
+            buf[v] = forward ? rhs[c * NV + v] : 0.0;
+        real cf = 0.5 * alphaDiag / g.vol[c];
+        for (int k = 0; k < m.nf; k++)
+        {
+            int o = m.cellNbr[c * m.nf + k];
+            if (o < 0 || !(forward ? o < c : o > c))
+                continue;
+            int fp = m.cell2face[c * m.nf + k];
+            int64_t f = fp >> 1;
+            real sg = (fp & 1) ? -1.0 : 1.0;
+            real n[3] = {g.faceMeanNorm[f * 3] * sg, g.faceMeanNorm[f * 3 + 1] * sg, g.faceMeanNorm[f * 3 + 2] * sg};
+            real dF[NV];
+            flux_jac_du<NV>(u + (int64_t)o * NV, n, uInc + (int64_t)o * NV, lamFace[f], gamma, dF);
+            real w = cf * g.faceArea[f];
+            for (int v = 0; v < NV; v++)
+                buf[v] -= w * dF[v];
+        }
+        for (int v = 0; v < NV; v++)
+        {
+            real x = buf[v] / jdiag[NV == 6 ? c * NV + v : c];
+            uIncNew[c * NV + v] = forward ? x : uIncNew[c * NV + v] + x;
         }
     }
 }
@@ -699,6 +740,32 @@ int update_sgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const 
         if (dev_sync(st) != cudaSuccess)
             return ST_CUDA;
     }
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int update_lusgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc,
+                 real *uIncNew, const real *jdiag, int forward, cudaStream_t st)
+{
+    int nv = ev.s.nVars;
+    if (nv != 5 && nv != 6)
+        return ST_UNSUPPORTED;
+    auto launch = [&](const int32_t *cells, int64_t b, int64_t e)
+    {
+        if (nv == 5)
+            DNDSB_LAUNCH(k_lusgs_sweep<5>, e - b, 128, st, m, g, ev.s.gamma, ev.lambdaFace, cells, b, e, alphaDiag, rhs, u, uInc, uIncNew,
+                         jdiag, forward);
+        else
+            DNDSB_LAUNCH(k_lusgs_sweep<6>, e - b, 128, st, m, g, ev.s.gamma, ev.lambdaFace, cells, b, e, alphaDiag, rhs, u, uInc, uIncNew,
+                         jdiag, forward);
+    };
+    if (uInc != uIncNew)
+        launch(nullptr, 0, m.nCell);
+    else // in place: colour by colour, so a cell reads the new values of the neighbours swept before it
+        for (int ci = 0; ci < m.nColor; ci++)
+        {
+            int col = forward ? ci : m.nColor - 1 - ci;
+            launch(m.colorCells, m.colorStart[col], m.colorStart[col + 1]);
+        }
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 

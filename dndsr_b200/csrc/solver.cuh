@@ -132,6 +132,7 @@ struct EulerSettingsD
     real gamma = 1.4, Rgas = 1, muGas = 1, prGas = 0.72, TRef = 273.15, CSutherland = 110.4;
     int muModel = 1;
     int ignoreVis = 0;
+    int rsMeanValueEig = 0; // Roe_M1..M5 with the eigenvalues along the face's mean normal (Gas.hpp:1272-1408)
     real kT = 0, iPr = 0; // host-derived: gamma / ((gamma - 1) cp) (T = p kT / rho), 1 / prGas
     real cp() const { return Rgas * gamma / (gamma - 1); }
     void derive() { kT = gamma / ((gamma - 1) * cp()), iPr = 1.0 / prGas; }
@@ -169,6 +170,9 @@ int update_sgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const 
                real *uIncNew, const real *jdiag, int forward, int gsUpdate, int uIncIsZero, real *sumIncHost, cudaStream_t st);
 int lusgs_matvec(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jdiag,
                  real *AuInc, cudaStream_t st);
+// UpdateLUSGSForward / UpdateLUSGSBackward; uInc may equal uIncNew (in-place sweep over the colours)
+int update_lusgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc,
+                 real *uIncNew, const real *jdiag, int forward, cudaStream_t st);
 int init_field(const MeshD &m, const GeomD &g, const EvalD &ev, int kind, real chi, real *u, cudaStream_t st);
 // viscous part of the residual derivatives (adjoint_visc.cu): added to the inviscid face
 // cotangents [nFace][2][(R+1) nv] / face flux derivatives [nFace][nv] before their gathers

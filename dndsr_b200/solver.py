@@ -28,7 +28,7 @@ VR_DEFAULTS = dict(maxOrder=1, intOrder=1, jacobiRelax=1.0, SORInstead=False, an
                    scaleMultiplier=1.0, dirWeightScheme="Factorial", manualDirWeights=(1, 1, 0.5, 1.0 / 6), geomWeightScheme="GWNone",
                    geomWeightBias=0.0, geomWeightPower=0.5, geomWeightPower1=0.0, geomWeightPower2=0.0, bcWeight=1.0)
 EULER_DEFAULTS = dict(nVars=5, riemannSolverType="Roe", rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=1.0, prGas=0.72,
-                      TRef=273.15, CSutherland=110.4, muModel=1, ignoreVis=False)
+                      TRef=273.15, CSutherland=110.4, muModel=1, ignoreVis=False, rsMeanValueEig=0)
 
 
 # boundary condition codes, Euler/EulerBC.hpp:35-48
@@ -225,6 +225,7 @@ class EulerEvaluator(Handle):
         cs.rsFixScale, cs.rsIncFScale = float(s["rsFixScale"]), float(s["rsIncFScale"])
         cs.gamma, cs.Rgas, cs.muGas, cs.prGas = float(s["gamma"]), float(s["Rgas"]), float(s["muGas"]), float(s["prGas"])
         cs.TRef, cs.CSutherland, cs.muModel, cs.ignoreVis = float(s["TRef"]), float(s["CSutherland"]), int(s["muModel"]), int(bool(s["ignoreVis"]))
+        cs.rsMeanValueEig = int(s["rsMeanValueEig"])
         h = ctypes.c_void_p()
         capi.call("dndsb_eval_create", ctypes.byref(h), vr.h, ctypes.byref(cs))
         self.h = h
@@ -312,6 +313,21 @@ class EulerEvaluator(Handle):
                   _ptr(uIncNew, "uIncNew"), _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), int(uIncIsZero),
                   capi.dptr(s) if want_sum else None, _stream())
         return s
+
+    def UpdateLUSGSForward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
+        """EulerEvaluator.hxx:376-451: uIncNew = D^-1 (rhs - lower-neighbour flux increments of uInc).
+        uInc may be uIncNew itself (the in-place sweep of the reference's callers)."""
+        capi.call("dndsb_eval_update_lusgs_forward", self.h, float(alphaDiag), _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uInc, "uInc"),
+                  _ptr(jdiag, "jdiag"), _ptr(uIncNew, "uIncNew"), _stream())
+
+    def UpdateLUSGSBackward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
+        """EulerEvaluator.hxx:453-529: uIncNew += D^-1 (- upper-neighbour flux increments of uInc)."""
+        capi.call("dndsb_eval_update_lusgs_backward", self.h, float(alphaDiag), _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uInc, "uInc"),
+                  _ptr(jdiag, "jdiag"), _ptr(uIncNew, "uIncNew"), _stream())
+
+    def FixUMaxFilter(self, u):
+        """EulerEvaluator.hxx:1318-1323: the reference's filter returns without changing u."""
+        capi.call("dndsb_eval_fix_umax_filter", self.h, _ptr(u, "u"), _stream())
 
     def LUSGSMatrixVec(self, alphaDiag, u, uInc, jdiag, AuInc):
         capi.call("dndsb_eval_lusgs_matrix_vec", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(uInc, "uInc"), _ptr(jdiag, "jdiag"),

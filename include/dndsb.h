@@ -83,6 +83,9 @@ typedef struct dndsb_euler_settings
     double gamma, Rgas, muGas, prGas, TRef, CSutherland; /* idealGasProperty */
     int muModel;
     int ignoreVis; /* RHS_Ignore_Viscosity flag of EvaluateRHS */
+    int rsMeanValueEig; /* 1: Roe_M1..Roe_M5 take their eigenvalues, entropy fix and Roe normal velocity
+                           along the face's mean normal (the batched flux, EulerEvaluator_EvaluateDt.hxx:1259-1270,
+                           Gas.hpp:1272-1408); derivatives with respect to node coordinates then unsupported */
 } dndsb_euler_settings;
 
 /* ---- mesh (replaces Geom::UnstructuredMesh as input; src/Geom/Mesh/Mesh.hpp) ----
@@ -183,6 +186,19 @@ int dndsb_eval_lusgs_matrix_init(dndsb_eval *ev, const double *dTau, double dt, 
  * EulerEvaluator.hxx:550-693, swept colour by colour; sumIncHost [nVars] may be NULL */
 int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
                           const double *jdiag, int forward, int gsUpdate, int uIncIsZero, double *sumIncHost, void *stream);
+/* UpdateLUSGSForward / UpdateLUSGSBackward(alphaDiag, t, rhs, u, uInc, JDiag, uIncNew),
+ * EulerEvaluator.hxx:376-529: forward uIncNew_i = D_i^-1 (rhs_i - sum over neighbours j < i of
+ * (alphaDiag/2)(A_f/V_i) dF(u_j; uInc_j)); backward uIncNew_i += D_i^-1 (- the same sum over j > i).
+ * uInc may be the same array as uIncNew, as the reference's callers pass it: the sweep then runs
+ * colour by colour in place, which equals the reference's sequential sweep on a mesh numbered
+ * colour by colour (dndsb_mesh_colors).  With distinct arrays every cell is independent. */
+int dndsb_eval_update_lusgs_forward(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc,
+                                    const double *jdiag, double *uIncNew, void *stream);
+int dndsb_eval_update_lusgs_backward(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc,
+                                     const double *jdiag, double *uIncNew, void *stream);
+/* FixUMaxFilter(u), EulerEvaluator.hpp:591 / EulerEvaluator.hxx:1318-1323: the reference returns
+ * without touching u; kept so that callers of the reference's sequence port unchanged. */
+int dndsb_eval_fix_umax_filter(dndsb_eval *ev, double *u, void *stream);
 /* LUSGSMatrixVec(alphaDiag, t, u, uInc, JDiag, AuInc), EulerEvaluator.hxx:175-274 */
 int dndsb_eval_lusgs_matrix_vec(dndsb_eval *ev, double alphaDiag, const double *u, const double *uInc, const double *jdiag,
                                 double *AuInc, void *stream);

@@ -56,7 +56,7 @@ class EulerSettings(ctypes.Structure):
         ("rsFixScale", ctypes.c_double), ("rsIncFScale", ctypes.c_double),
         ("gamma", ctypes.c_double), ("Rgas", ctypes.c_double), ("muGas", ctypes.c_double),
         ("prGas", ctypes.c_double), ("TRef", ctypes.c_double), ("CSutherland", ctypes.c_double),
-        ("muModel", ctypes.c_int), ("ignoreVis", ctypes.c_int),
+        ("muModel", ctypes.c_int), ("ignoreVis", ctypes.c_int), ("rsMeanValueEig", ctypes.c_int),
     ]
 
 
@@ -86,6 +86,7 @@ def _declare(L):
     L.orc_eval_rhs.argtypes = [_V, _D, _D, _D, _D]
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_update_sgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
+    L.orc_update_lusgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int]
     L.orc_lusgs_matvec.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D]
     L.orc_lusgs_matvec_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D]
     L.orc_update_sgs_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
@@ -277,6 +278,15 @@ class Oracle:
         lib().orc_update_sgs(self.h, alphaDiag, _p(rhs), _p(u), _p(uInc), _p(out), _p(jdiag), int(forward), int(gsUpdate),
                              int(uIncIsZero), _p(s))
         return out, s
+
+    def update_lusgs(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, inplace=False):
+        """UpdateLUSGSForward / UpdateLUSGSBackward (EulerEvaluator.hxx:376-529) on a copy of uIncNew.
+        inplace: uInc is the same array as uIncNew (the copy), as the reference's callers pass it."""
+        rhs, u, jdiag = _f64(rhs), _f64(u), _f64(jdiag)
+        out = np.array(uIncNew, dtype=np.float64, copy=True, order="C")
+        src = out if inplace else _f64(uInc)
+        lib().orc_update_lusgs(self.h, alphaDiag, _p(rhs), _p(u), _p(src), _p(out), _p(jdiag), int(forward))
+        return out
 
     def lusgs_matvec(self, alphaDiag, u, uInc, jdiag):
         u, uInc, jdiag = _f64(u), _f64(uInc), _f64(jdiag)

@@ -520,8 +520,12 @@ static void roeEntropyFix(int eigScheme, real aL, real aR, real aAve, real uL, r
 }
 
 // Gas.hpp:1038-1126 RoeFlux_IdealGas_HartenYee
+// nE: the normal of the eigenvalues and of the Roe normal velocity.  The per-point flux passes nE = n; the
+// batched flux of Gas.hpp:1272-1408 (RoeFlux_IdealGas_HartenYee_Batch, rsMeanValueEig = 1) passes the face's
+// mean normal while the physical fluxes, the jump projections and the acoustic eigenvectors keep the point normal
 static void roeFlux(int eigScheme, const real *UL, const real *UR, const real *ULm, const real *URm, const real vg[3], const real n[3],
-                    real gamma, real F[5], real dLambda, real fixScale, real incFScale, real &lam0, real &lam123, real &lam4)
+                    const real nE[3], real gamma, real F[5], real dLambda, real fixScale, real incFScale, real &lam0, real &lam123,
+                    real &lam4)
 {
     real veloL[3], veloR[3];
     for (int d = 0; d < 3; d++)
@@ -533,7 +537,7 @@ static void roeFlux(int eigScheme, const real *UL, const real *UR, const real *U
     real FL[5], FR[5];
     inviscidFluxXY(UL, veloL, vg, n, pL, FL);
     inviscidFluxXY(UR, veloR, vg, n, pR, FR);
-    real veloRoeN = dot3(rp.veloRoe, n), vgN = dot3(vg, n);
+    real veloRoeN = dot3(rp.veloRoe, nE), vgN = dot3(vg, nE);
     real veloRoe0 = veloRoeN - vgN;
     lam0 = std::abs(veloRoe0 - rp.aRoe);
     lam123 = std::abs(veloRoe0);
@@ -541,7 +545,7 @@ static void roeFlux(int eigScheme, const real *UL, const real *UR, const real *U
     real dvL[3], dvR[3], dvRoe[3];
     for (int d = 0; d < 3; d++)
         dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d], dvRoe[d] = rp.veloRoe[d] - vg[d];
-    real veloLm0 = dot3(dvL, n), veloRm0 = dot3(dvR, n);
+    real veloLm0 = dot3(dvL, nE), veloRm0 = dot3(dvR, nE);
     if (eigScheme == 2)
     {
         lam0 = lam123 = lam4 = std::max(std::abs(veloLm0) + std::sqrt(rp.asqrLm), std::abs(veloRm0) + std::sqrt(rp.asqrRm));
@@ -736,13 +740,17 @@ enum RS
 };
 
 // Gas.hpp:1434-1490 InviscidFlux_IdealGas_Dispatcher
+// nMean: the face's mean normal when the settings ask for the batched mean-value eigenvalues
+// (EulerEvaluator_EvaluateDt.hxx:1259-1270: rsMeanValueEig != 0 and Roe_M1..Roe_M5), else nullptr
 static void riemann(int type, const real *UL, const real *UR, const real *ULm, const real *URm, const real vg[3], const real n[3], real gamma,
-                    real F[5], real dLambda, real fixScale, real incFScale, real &lam0, real &lam123, real &lam4)
+                    real F[5], real dLambda, real fixScale, real incFScale, real &lam0, real &lam123, real &lam4,
+                    const real *nMean = nullptr)
 {
+    const real *nE = (nMean && type >= 11 && type <= 15) ? nMean : n;
     if (type == RS_Roe)
-        roeFlux(0, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, incFScale, lam0, lam123, lam4);
+        roeFlux(0, UL, UR, ULm, URm, vg, n, n, gamma, F, dLambda, fixScale, incFScale, lam0, lam123, lam4);
     else if (type >= 11 && type <= 18)
-        roeFlux(type - 10, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, incFScale, lam0, lam123, lam4);
+        roeFlux(type - 10, UL, UR, ULm, URm, vg, n, nE, gamma, F, dLambda, fixScale, incFScale, lam0, lam123, lam4);
     else if (type == RS_HLLEP)
         hllepFlux(0, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, lam0, lam123, lam4);
     else if (type == RS_HLLEP_V1)
@@ -842,6 +850,7 @@ extern "C"
         double gamma, Rgas, muGas, prGas, TRef, CSutherland;
         int muModel;
         int ignoreVis;
+        int rsMeanValueEig; // EulerEvaluatorSettings.hpp:79: Roe_M1..M5 through the batched dispatcher
     };
 }
 
@@ -1967,7 +1976,8 @@ struct Oracle
             if (!es.ignoreVis && !noVis)
                 pointViscousFlux(UM, GMP, n, type == 2, vis);
             real F[8] = {0}, l0, l1, l4, vg[3] = {0, 0, 0};
-            riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4);
+            riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4,
+                    es.rsMeanValueEig ? &faceMeanNorm[f * 3] : nullptr);
             scalarConvectiveFlux(UL, UR, n, l1, F);
             real JD = faceJDet[f * nGf + g];
             for (int v = 0; v < nv; v++)
@@ -2053,7 +2063,8 @@ struct Oracle
                 if (!es.ignoreVis)
                     pointViscousFlux(UM, GMP, n, false, vis);
                 real F[8] = {0}, l0, l1, l4, vg[3] = {0, 0, 0};
-                riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4);
+                riemann(es.rsType, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, es.rsFixScale, es.rsIncFScale, l0, l1, l4,
+                        es.rsMeanValueEig ? &faceMeanNorm[f * 3] : nullptr);
                 scalarConvectiveFlux(UL, UR, n, l1, F);
                 real JD = faceJDet[f * nGf + g];
                 for (int v = 0; v < nv; v++)
@@ -2161,6 +2172,42 @@ struct Oracle
                 real old = uIncNew[c * nv + v];
                 uIncNew[c * nv + v] = buf[v] / jdiag[nv >= 6 ? c * nv + v : c];
                 sumInc[v] += std::abs(uIncNew[c * nv + v] - old);
+            }
+        }
+    }
+
+    // EulerEvaluator.hxx:376-529 UpdateLUSGSForward / UpdateLUSGSBackward (sequential, natural cell order).
+    // Forward: uIncNew_c = D_c^-1 (rhs_c - sum over lower neighbours of (alpha/2)(A_f/V_c) dF(uInc_o));
+    // backward: uIncNew_c += D_c^-1 (- sum over upper neighbours of the same).  uInc may alias uIncNew
+    // (the reference's callers pass one array), which turns the neighbour reads into Gauss-Seidel reads.
+    void updateLUSGS(real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew, const real *jdiag, bool forward) const
+    {
+        int nv = es.nVars;
+        for (long s = 0; s < nCell; s++)
+        {
+            long c = forward ? s : nCell - 1 - s;
+            real buf[8];
+            for (int v = 0; v < nv; v++)
+                buf[v] = forward ? rhs[c * nv + v] : 0.0;
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                long o = otherOf(c, f);
+                if (o < 0 || !(forward ? (o < c) : (o > c)))
+                    continue;
+                int side = sideOf(c, f);
+                real n[3];
+                for (int d = 0; d < 3; d++)
+                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+                real dF[8];
+                fluxJacTimesDu(u + o * nv, n, uInc + o * nv, lambdaFace[f], dF);
+                for (int v = 0; v < nv; v++)
+                    buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
+            }
+            for (int v = 0; v < nv; v++)
+            {
+                real x = buf[v] / jdiag[nv >= 6 ? c * nv + v : c];
+                uIncNew[c * nv + v] = forward ? x : uIncNew[c * nv + v] + x;
             }
         }
     }
@@ -2545,6 +2592,12 @@ extern "C"
     }
 
     // single Riemann flux evaluation (Gas.hpp:1434 dispatcher), 5 conservative variables
+    // uInc may equal uIncNew (in-place sweep, as the reference's callers use it)
+    void orc_update_lusgs(void *h, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
+                          const double *jdiag, int forward)
+    {
+        ((Oracle *)h)->updateLUSGS(alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward != 0);
+    }
     void orc_riemann(int type, const double *UL, const double *UR, const double *ULm, const double *URm, const double *n, double gamma,
                      double dLambda, double fixScale, double incFScale, double *F, double *lam)
     {

@@ -86,3 +86,73 @@ _CASES = [(key, c, ib) for key in _FUNCS for c in GOLD[key]["cases"] for ib in r
 def test_vr_iv10_golden(key, case, ib):
     err = _vr_error([10, 20, 40][ib], case["p"], case["weights"] == "HQM", _FUNCS[key])
     assert abs(err - case["golden"][ib]) <= GOLD[key]["rel_tol"] * case["golden"][ib]
+
+
+# ---- one Newton step of the evaluator pipeline (test_EulerEvaluator.cpp:120-330) ----
+from tests.newton_case import CASES as NEWTON_CASES, GAS, initial_state, norms  # noqa: E402
+
+
+def _newton_oracle(case, rsMeanValueEig=None):
+    m = case["mesh"]()
+    mve = case["rsMeanValueEig"] if rsMeanValueEig is None else rsMeanValueEig
+    es = dict(nVars=5, rsType=oracle.RS[case["rs"]], rsFixScale=1.0, rsIncFScale=1.0, ignoreVis=0, rsMeanValueEig=mve, **GAS)
+    o = oracle.Oracle(m, case["vr_oracle"], es)
+    assert o.construct() == 0
+    u = initial_state(case, o.get("cellBary").reshape(-1, 3), init_field=o.init_field)
+    dTau, _ = o.eval_dt(u, case["CFL"], 1e100, True)
+    rhs = o.eval_rhs(u, np.zeros((m.n_cell, o.R, 5)))
+    jd = o.lusgs_init(dTau, 1e100, 1.0)
+    x = np.zeros_like(u)
+    xn = o.update_lusgs(1.0, rhs, u, x, np.zeros_like(u), jd, forward=True)
+    xn = o.update_lusgs(1.0, rhs, u, x, xn, jd, forward=False)
+    return norms(rhs, xn, o.get("volume")), (o, u, rhs)
+
+
+@pytest.mark.parametrize("name", list(NEWTON_CASES))
+def test_newton_step_golden(name):
+    case = NEWTON_CASES[name]
+    (rhs_l1, inc_l2), _ = _newton_oracle(case)
+    g = case["gold"]
+    assert abs(rhs_l1 - g["rhsDensityL1"]) <= g["rel_tol"] * g["rhsDensityL1"]
+    assert abs(inc_l2 - g["incL2"]) <= g["rel_tol"] * g["incL2"]
+
+
+def test_mean_value_eig_straight_and_curved_faces():
+    # straight faces: the batched mean-value Roe flux equals the per-point one (one normal per face)
+    (a, _), (_, _, rhs1) = _newton_oracle(NEWTON_CASES["iv"], 1)
+    (b, _), (_, _, rhs0) = _newton_oracle(NEWTON_CASES["iv"], 0)
+    assert np.abs(rhs1 - rhs0).max() <= 1e-13 * np.abs(rhs0).max()
+    # warped hexahedra: per-point normals differ from the face mean, and so do the two fluxes
+    m = M.tgv_mesh(4)
+    out = []
+    for mve in (0, 1):
+        es = dict(nVars=5, rsType=oracle.RS["Roe_M1"], rsFixScale=1.0, rsIncFScale=1.0, ignoreVis=1, rsMeanValueEig=mve, gamma=1.4,
+                  Rgas=1.0, muGas=0.0, prGas=0.72, TRef=273.15, CSutherland=110.4, muModel=0)
+        o = oracle.Oracle(m, dict(NEWTON_CASES["iv"]["vr_oracle"], maxOrder=2, intOrder=5), es)
+        assert o.construct() == 0
+        u = o.init_field(3)
+        uRec = np.random.default_rng(3).normal(size=(m.n_cell, o.R, 5)) * 1e-2
+        o.eval_dt(u, 1.0)
+        out.append(o.eval_rhs(u, uRec))
+    d = np.abs(out[1] - out[0]).max() / np.abs(out[0]).max()
+    assert 1e-12 < d < 0.5
+
+
+def test_update_lusgs_inplace_is_gauss_seidel():
+    # uInc aliased with uIncNew: the forward sweep reads the new values of lower cells (sequential
+    # Gauss-Seidel); with a separate zero uInc it is D^-1 rhs (the Newton-step sequence above)
+    _, (o, u, rhs) = _newton_oracle(NEWTON_CASES["iv"])
+    dTau, _ = o.eval_dt(u, 100.0)
+    jd = o.lusgs_init(dTau, 1e100, 1.0)
+    zero = np.zeros_like(u)
+    jac = o.update_lusgs(1.0, rhs, u, zero, zero, jd, forward=True)
+    np.testing.assert_allclose(jac, rhs / jd[:, None], rtol=1e-14, atol=0)
+    gs = o.update_lusgs(1.0, rhs, u, None, zero, jd, forward=True, inplace=True)
+    # reference: an explicit sequential sweep with the matrix-vector operator's off-diagonal part
+    ref = np.zeros_like(u)
+    for c in range(u.shape[0]):
+        x = np.zeros_like(u)
+        x[:c] = ref[:c]
+        Ax = o.lusgs_matvec(1.0, u, x, jd)  # row c: sum_{o<c} w dF(x_o) (x_c = 0)
+        ref[c] = (rhs[c] - Ax[c]) / jd[c]
+    np.testing.assert_allclose(gs, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
