@@ -77,6 +77,9 @@ SIGNATURES = {
     "dndsb_eval_initialize_udof": [_P, _i, _d, _P, _P],
     "dndsb_eval_evaluate_dt": [_P, _P, _d, _d, _i, _P, _D, _P],
     "dndsb_eval_evaluate_rhs": [_P, _P, _P, _P, _P],
+    "dndsb_eval_evaluate_rhs_full": [_P, _P, _P, _P, _P, _P, _P, _P, _i, _d, ctypes.c_uint64, _P],
+    "dndsb_eval_set_deferred_errors": [_P, _i],
+    "dndsb_eval_check_errors": [_P, _P],
     "dndsb_eval_lusgs_matrix_init": [_P, _P, _d, _d, _P, _P],
     "dndsb_eval_update_sgs": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _D, _P],
     "dndsb_eval_lusgs_matrix_vec": [_P, _d, _P, _P, _P, _P, _P],

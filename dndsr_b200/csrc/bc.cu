@@ -88,7 +88,7 @@ DNDSB_GLOBAL void k_vr_bc(MeshD m, GeomD g, VRD vr, const TC *__restrict__ AAInv
 // viscous flux on slip, far-field and outflow faces (:423-430, EvaluateDt.hxx:1203-1207)
 template <int DIM, int P, int NV>
 DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec,
-                           const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
+                           const real *__restrict__ uRecG, const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     const real gamma = s.gamma;
@@ -98,7 +98,7 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
         int64_t c0 = m.face2cell[f * 2];
         int zone = m.faceZone[f];
         int type = zone >= 0 && zone < vr.bnd.nZone ? vr.bnd.type[zone] : 0;
-        const real *ULm = u + c0 * NV, *r0 = uRec + c0 * R * NV;
+        const real *ULm = u + c0 * NV, *r0 = uRec + c0 * R * NV, *q0 = uRecG + c0 * R * NV; // values, gradients
         real URm[NV];
         bool bad = false;
         if (!bc_value<NV>(vr.bnd, zone, ULm, &g.faceMeanNorm[f * 3], URm))
@@ -127,10 +127,10 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
                 real ga[3] = {0, 0, 0};
                 for (int j = 0; j < R; j++)
                 {
-                    real x0 = r0[j * NV + v];
+                    real x0 = r0[j * NV + v], y0 = q0[j * NV + v];
                     a += T0[1 + j] * x0;
                     for (int d = 0; d < DIM; d++)
-                        ga[d] += T0[(1 + d) * NDOF + 1 + j] * x0;
+                        ga[d] += T0[(1 + d) * NDOF + 1 + j] * y0;
                 }
                 UL[v] = a;
                 for (int d = 0; d < 3; d++)
@@ -215,26 +215,27 @@ int vr_bc_p(const MeshD &m, const GeomD &g, const VRD &vr, const real *uRec, rea
 }
 
 template <int DIM, int NV>
-int rhs_bc_p(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st)
+int rhs_bc_p(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, const real *uRecG, real *ff,
+             cudaStream_t st)
 {
     switch (vr.P)
     {
     case 1:
     {
         auto k = k_rhs_bc<DIM, 1, NV>;
-        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord);
+        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord);
         return ST_OK;
     }
     case 2:
     {
         auto k = k_rhs_bc<DIM, 2, NV>;
-        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord);
+        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord);
         return ST_OK;
     }
     case 3:
     {
         auto k = k_rhs_bc<DIM, 3, NV>;
-        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord);
+        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord);
         return ST_OK;
     }
     }
@@ -259,15 +260,16 @@ int vr_iter_bc(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
-int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st)
+int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, const real *uRecG, real *ff,
+           cudaStream_t st)
 {
     if (m.nBndFace == 0)
         return ST_OK;
     int rc = ST_UNSUPPORTED;
     if (ev.s.nVars == 5)
-        rc = m.dim == 2 ? rhs_bc_p<2, 5>(m, g, vr, ev, u, uRec, ff, st) : rhs_bc_p<3, 5>(m, g, vr, ev, u, uRec, ff, st);
+        rc = m.dim == 2 ? rhs_bc_p<2, 5>(m, g, vr, ev, u, uRec, uRecG, ff, st) : rhs_bc_p<3, 5>(m, g, vr, ev, u, uRec, uRecG, ff, st);
     else if (ev.s.nVars == 6)
-        rc = m.dim == 2 ? rhs_bc_p<2, 6>(m, g, vr, ev, u, uRec, ff, st) : rhs_bc_p<3, 6>(m, g, vr, ev, u, uRec, ff, st);
+        rc = m.dim == 2 ? rhs_bc_p<2, 6>(m, g, vr, ev, u, uRec, uRecG, ff, st) : rhs_bc_p<3, 6>(m, g, vr, ev, u, uRec, uRecG, ff, st);
     if (rc != ST_OK)
         return rc;
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;

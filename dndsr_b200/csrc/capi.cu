@@ -536,6 +536,8 @@ extern "C"
         rc |= dev_alloc((void **)&e->e.faceFlux, sizeof(real) * std::max(m.nFace, m.nCell) * s->nVars);
         rc |= dev_alloc((void **)&e->e.redBuf, sizeof(real) * kRedBufLen);
         rc |= dev_alloc((void **)&e->e.errWord, sizeof(int));
+        rc |= dev_alloc((void **)&e->e.errDeferred, sizeof(int));
+        rc |= dev_alloc((void **)&e->e.fluxWall, sizeof(real) * 8);
         if (s->nVars == 6)
             rc |= dev_alloc((void **)&e->e.jSource, sizeof(real) * m.nCell * 6);
         if (rc)
@@ -552,6 +554,8 @@ extern "C"
         }
         cudaMemset(e->e.deltaLambdaCell, 0, sizeof(real) * m.nCell);
         cudaMemset(e->e.lambdaFace, 0, sizeof(real) * m.nFace);
+        cudaMemset(e->e.errDeferred, 0, sizeof(int));
+        cudaMemset(e->e.fluxWall, 0, sizeof(real) * 8);
         *out = e;
         return DNDSB_OK;
     }
@@ -587,7 +591,8 @@ extern "C"
             return DNDSB_OK;
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
-                        (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource})
+                        (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource,
+                        (void *)e->e.errDeferred, (void *)e->e.fluxWall})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -621,6 +626,51 @@ extern "C"
         if (e->e.s.nVars == 6 && !e->e.dWall)
             return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
         return status_msg(eval_rhs(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, u, uRec, rhs, nullptr, S(stream)), "dndsb_eval_evaluate_rhs");
+    }
+
+    int dndsb_eval_evaluate_rhs_full(dndsb_eval *e, double *rhs, double *JSource, const double *u, const double *uRecUnlim, const double *uRec,
+                                     const double *uRecBeta, const double *cellRHSAlpha, int onlyOnHalfAlpha, double t, uint64_t flags,
+                                     void *stream)
+    {
+        (void)uRecBeta, (void)onlyOnHalfAlpha, (void)t; // not read by the reference's EvaluateRHS body either
+        if (!e || !rhs || !u || !uRecUnlim || !uRec)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs_full: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs_full: VR not constructed");
+        if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs_full: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (e->e.s.nVars == 6 && !e->e.dWall)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_evaluate_rhs_full: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
+        const uint64_t known = DNDSB_RHS_IGNORE_VISCOSITY | DNDSB_RHS_DONT_UPDATE_INTEGRATION | DNDSB_RHS_DONT_RECORD_BND_FLUX;
+        if (flags & ~known)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_evaluate_rhs_full: the direct second-order reconstruction flags are not supported");
+        return status_msg(eval_rhs_ex(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, u, uRecUnlim, uRec, cellRHSAlpha, (unsigned)flags, rhs, nullptr,
+                                      JSource, S(stream)),
+                          "dndsb_eval_evaluate_rhs_full");
+    }
+
+    int dndsb_eval_set_deferred_errors(dndsb_eval *e, int deferred)
+    {
+        if (!e)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_deferred_errors: null argument");
+        e->e.deferErr = deferred != 0;
+        return DNDSB_OK;
+    }
+
+    int dndsb_eval_check_errors(dndsb_eval *e, void *stream)
+    {
+        if (!e)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_check_errors: null argument");
+        int w = 0;
+        d2h(&w, e->e.errDeferred, sizeof(int), S(stream));
+        dev_zero(e->e.errDeferred, sizeof(int), S(stream));
+        if (dev_sync(S(stream)) != cudaSuccess)
+            return cuda_fail("dndsb_eval_check_errors");
+        if (w & DE_NONPHYSICAL)
+            return status_msg(ST_NONPHYSICAL, "dndsb_eval_check_errors");
+        if (w & DE_NONFINITE)
+            return status_msg(ST_NONFINITE, "dndsb_eval_check_errors");
+        return DNDSB_OK;
     }
 
     int dndsb_eval_rhs_vjp(dndsb_eval *e, const double *w, const double *u, const double *uRec, double *du, double *duRec, void *stream)
@@ -921,6 +971,7 @@ extern "C"
         else if (n == "deltaLambdaCell") src = e->e.deltaLambdaCell, cnt = m.nCell;
         else if (n == "faceFlux") src = e->e.faceFlux, cnt = m.nFace * e->e.s.nVars;
         else if (n == "jSource" && e->e.jSource) src = e->e.jSource, cnt = m.nCell * e->e.s.nVars;
+        else if (n == "fluxWallSum") src = e->e.fluxWall, cnt = e->e.s.nVars;
         else
             return fail(DNDSB_E_BADARG, "dndsb_eval_get_array: unknown name " + n);
         if (len)

@@ -95,8 +95,10 @@ DNDSB_GLOBAL void k_swap(int64_t n, real *a, real *b)
 // gather below divides by the volume.
 // ---------------------------------------------------------------------------
 template <int DIM, int P, int NV>
+// uRecG: the reconstruction the gradients come from (the reference's uRecUnlim, EvaluateRHS.hxx:264-327;
+// the same array as uRec when there is no limiter); point values come from uRec
 DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec,
-                             const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
+                             const real *__restrict__ uRecG, const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
@@ -114,6 +116,7 @@ DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const r
         }
         const real *ULm = u + (int64_t)c0 * NV, *URm = u + (int64_t)c1 * NV;
         const real *r0 = uRec + (int64_t)c0 * R * NV, *r1 = uRec + (int64_t)c1 * R * NV;
+        const real *q0 = uRecG + (int64_t)c0 * R * NV, *q1 = uRecG + (int64_t)c1 * R * NV;
         real dLambda = dmax(dLamCell[c0], dLamCell[c1]);
         real minVol = dmin(g.vol[c0], g.vol[c1]);
         real db[3];
@@ -143,10 +146,11 @@ DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const r
                 for (int j = 0; j < R; j++)
                 {
                     real x0 = r0[j * NV + v], x1 = r1[j * NV + v];
+                    real y0 = q0[j * NV + v], y1 = q1[j * NV + v];
                     a += T0[1 + j] * x0;
                     b += T1[1 + j] * x1;
                     for (int d = 0; d < DIM; d++)
-                        ga[d] += T0[(1 + d) * NDOF + 1 + j] * x0, gb[d] += T1[(1 + d) * NDOF + 1 + j] * x1;
+                        ga[d] += T0[(1 + d) * NDOF + 1 + j] * y0, gb[d] += T1[(1 + d) * NDOF + 1 + j] * y1;
                 }
                 UL[v] = a, UR[v] = b;
                 for (int d = 0; d < 3; d++)
@@ -480,8 +484,11 @@ DNDSB_GLOBAL void k_init_field(MeshD m, GeomD g, real gamma, int kind, real chi,
 // conservative gradient from the reconstruction), integrated and divided by the volume, added to
 // rhs; the mode-1 diagonal Jacobian gives JSource.  The NS source is zero.
 template <int DIM, int P>
+// values from uRec, gradients from uRecG (uRecUnlim); the integral times cellRHSAlpha / V (EvaluateRHS.hxx:790;
+// alpha == nullptr: 1), for the source and its Jacobian diagonal alike
 DNDSB_GLOBAL void k_sa_source(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec,
-                              const real *__restrict__ dWall, real *rhs, real *jSource)
+                              const real *__restrict__ uRecG, const real *__restrict__ alpha, const real *__restrict__ dWall, real *rhs,
+                              real *jSource)
 {
     constexpr int NV = 6, NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
@@ -501,10 +508,10 @@ DNDSB_GLOBAL void k_sa_source(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const 
                 real ga[3] = {0, 0, 0};
                 for (int j = 0; j < R; j++)
                 {
-                    real x = uRec[(c * R + j) * NV + v];
+                    real x = uRec[(c * R + j) * NV + v], y = uRecG[(c * R + j) * NV + v];
                     a += T[1 + j] * x;
                     for (int d = 0; d < DIM; d++)
-                        ga[d] += T[(1 + d) * NDOF + 1 + j] * x;
+                        ga[d] += T[(1 + d) * NDOF + 1 + j] * y;
                 }
                 U[v] = a;
                 for (int d = 0; d < 3; d++)
@@ -520,9 +527,10 @@ DNDSB_GLOBAL void k_sa_source(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const 
             S += sa_source(U, G, s.muGas, mu, d, lLES, hMax, 0) * JW;
             J += sa_source(U, G, s.muGas, mu, d, lLES, hMax, 1) * JW;
         }
-        rhs[c * NV + 5] += S / g.vol[c];
+        real sc = (alpha ? alpha[c] : 1.0) / g.vol[c];
+        rhs[c * NV + 5] += S * sc;
         for (int v = 0; v < NV; v++)
-            jSource[c * NV + v] = v == 5 ? J / g.vol[c] : 0.0;
+            jSource[c * NV + v] = v == 5 ? J * sc : 0.0;
     }
 }
 
@@ -606,20 +614,69 @@ int vr_swap(int64_t n, real *a, real *b, cudaStream_t st)
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
+// wall-flux integral of EvaluateRHS.hxx:599-607: minus the face fluxes of the BCWall / BCWallIsothermal faces
+// (and of BCWallInvis faces when muGas < 1e-99), summed over the boundary-face list in a fixed order (one
+// block: thread partial sums over a fixed stride, then a fixed tree)
+template <int NV>
+DNDSB_GLOBAL void k_wall_flux_sum(MeshD m, BoundaryD bnd, real muGas, const real *__restrict__ ff, real *out)
+{
+    __shared__ real sp[256][NV];
+    real acc[NV];
+    for (int v = 0; v < NV; v++)
+        acc[v] = 0;
+    for (int64_t ii = threadIdx.x; ii < m.nBndFace; ii += blockDim.x)
+    {
+        int64_t f = m.bndFace[ii];
+        int zone = m.faceZone[f];
+        int t = zone >= 0 && zone < bnd.nZone ? bnd.type[zone] : 0;
+        if (t == BC_WALL || t == BC_WALL_ISOTHERMAL || (t == BC_WALL_INVIS && muGas < 1e-99))
+            for (int v = 0; v < NV; v++)
+                acc[v] -= ff[f * NV + v];
+    }
+    for (int v = 0; v < NV; v++)
+        sp[threadIdx.x][v] = acc[v];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1)
+    {
+        if ((int)threadIdx.x < w)
+            for (int v = 0; v < NV; v++)
+                sp[threadIdx.x][v] += sp[threadIdx.x + w][v];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < NV; v++)
+            out[v] = sp[0][v];
+}
+
 int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *u, const real *uRec, real *rhs, real *faceFlux,
              cudaStream_t st)
 {
+    return eval_rhs_ex(m, g, vr, ev, u, uRec, uRec, nullptr, 0, rhs, faceFlux, nullptr, st);
+}
+
+int eval_rhs_ex(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *u, const real *uRecG, const real *uRec,
+                const real *alpha, unsigned flags, real *rhs, real *faceFlux, real *jSourceOut, cudaStream_t st)
+{
     real *ff = faceFlux ? faceFlux : ev.faceFlux;
-    dev_zero(ev.errWord, sizeof(int), st);
     int nv = ev.s.nVars;
     if (nv != 5 && nv != 6)
         return ST_UNSUPPORTED;
-    int frc = rhs_face_fast(m, g, vr, ev, u, uRec, ff, st);
+    // a per-call RHS_Ignore_Viscosity on top of the settings; in deferred mode the kernels OR into the
+    // evaluator's deferred error word, which only dndsb_eval_check_errors reads and clears
+    EvalD evc = ev;
+    if (flags & RHSF_IGNORE_VISCOSITY)
+        evc.s.ignoreVis = 1;
+    if (ev.deferErr)
+        evc.errWord = ev.errDeferred;
+    else
+        dev_zero(ev.errWord, sizeof(int), st);
+    const EulerSettingsD &s = evc.s;
+    int frc = uRecG == uRec ? rhs_face_fast(m, g, vr, evc, u, uRec, ff, st) : (int)ST_UNSUPPORTED;
     if (frc == ST_CUDA)
         return ST_CUDA;
     if (frc != ST_OK)
     {
-#define DNDSB_RF(D, PP, NVV) DNDSB_LAUNCH((k_rhs_face<D, PP, NVV>), m.nFace, 128, st, m, g, vr, ev.s, u, uRec, ev.deltaLambdaCell, ff, ev.errWord)
+#define DNDSB_RF(D, PP, NVV) DNDSB_LAUNCH((k_rhs_face<D, PP, NVV>), m.nFace, 128, st, m, g, vr, s, u, uRec, uRecG, ev.deltaLambdaCell, ff, evc.errWord)
 #define DNDSB_RF_P(D, NVV)        \
     do                            \
     {                             \
@@ -647,7 +704,7 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
 #undef DNDSB_RF_P
 #undef DNDSB_RF
     }
-    int brc = rhs_bc(m, g, vr, ev, u, uRec, ff, st);
+    int brc = rhs_bc(m, g, vr, evc, u, uRec, uRecG, ff, st);
     if (brc != ST_OK)
         return brc;
     if (nv == 5)
@@ -658,7 +715,7 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
         // SA source (EvaluateRHS.hxx:665-801) and its Jacobian diagonal JSource
         if (!ev.dWall)
             return ST_BADARG;
-#define DNDSB_SAS(D, PP) DNDSB_LAUNCH((k_sa_source<D, PP>), m.nCell, 64, st, m, g, vr, ev.s, u, uRec, ev.dWall, rhs, ev.jSource)
+#define DNDSB_SAS(D, PP) DNDSB_LAUNCH((k_sa_source<D, PP>), m.nCell, 64, st, m, g, vr, s, u, uRec, uRecG, alpha, ev.dWall, rhs, ev.jSource)
         if (m.dim == 2)
         {
             if (vr.P == 1)
@@ -679,7 +736,21 @@ int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const rea
         }
 #undef DNDSB_SAS
     }
-    return check(st, ev.errWord, true);
+    if (jSourceOut)
+    {
+        if (nv == 6)
+            d2d(jSourceOut, ev.jSource, sizeof(real) * m.nCell * 6, st);
+        else
+            dev_zero(jSourceOut, sizeof(real) * m.nCell * nv, st);
+    }
+    if (!(flags & RHSF_DONT_UPDATE_INTEGRATION) && m.nBndFace > 0 && ev.fluxWall)
+    {
+        if (nv == 5)
+            k_wall_flux_sum<5><<<1, 256, 0, st>>>(m, vr.bnd, s.muGas, ff, ev.fluxWall);
+        else
+            k_wall_flux_sum<6><<<1, 256, 0, st>>>(m, vr.bnd, s.muGas, ff, ev.fluxWall);
+    }
+    return check(st, evc.errWord, !ev.deferErr);
 }
 
 int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, real MaxDt, int useLocalDt, real *dt, real *dtMin,
@@ -694,6 +765,8 @@ int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, 
     else
         return ST_UNSUPPORTED;
     DNDSB_LAUNCH(k_dt_cell, m.nCell, 256, st, m, g, ev.lambdaFace, ev.deltaLambdaFace, CFL, MaxDt, dt, ev.deltaLambdaCell);
+    if (useLocalDt && !dtMin) // nothing to reduce and nothing to report: no host synchronisation
+        return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
     real *res = reduce_cols(1, m.nCell, 1, dt, nullptr, 0, ev.redBuf, st);
     real mn = 0;
     d2h(&mn, res, sizeof(real), st);

@@ -150,8 +150,16 @@ struct EvalD
     real *adjBuf = nullptr;   // scratch of the derivative kernels [nFace][2][(R+1) nv], allocated on first use
     real *dWall = nullptr;    // SA: wall distance at the cell Gauss points [nCell][nGc]
     real *jSource = nullptr;  // SA: source-term Jacobian diagonal of the last RHS [nCell][nv]
+    real *fluxWall = nullptr; // wall-flux integral of the last RHS [8] (EvaluateRHS.hxx:599-607 fluxWallSum)
     int *errWord = nullptr;   // device error word
+    int *errDeferred = nullptr; // error word of EvaluateRHS in deferred mode (read and cleared on request)
+    bool deferErr = false;    // EvaluateRHS skips its per-call read-back of the error word
 };
+
+// EvaluateRHS flags (EulerEvaluator.hpp:370-378 RHS_* values)
+constexpr unsigned RHSF_IGNORE_VISCOSITY = 1u << 0;
+constexpr unsigned RHSF_DONT_UPDATE_INTEGRATION = 1u << 1;
+constexpr unsigned RHSF_DONT_RECORD_BND_FLUX = 1u << 2;
 
 // ---- setup (setup.cu) ----
 int geom_construct(const MeshD &m, const VRSettingsD &s, GeomD &g, cudaStream_t st);
@@ -165,6 +173,11 @@ int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, 
             cudaStream_t st);
 int eval_rhs(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *u, const real *uRec, real *rhs, real *faceFlux,
              cudaStream_t st);
+// EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, uRecBeta, cellRHSAlpha, onlyOnHalfAlpha, t, flags):
+// uRecG = uRecUnlim (gradients), uRec (point values), alpha = cellRHSAlpha (nullptr: 1), flags RHSF_*,
+// jSourceOut [nCell][nv] (may be nullptr)
+int eval_rhs_ex(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *u, const real *uRecG, const real *uRec,
+                const real *alpha, unsigned flags, real *rhs, real *faceFlux, real *jSourceOut, cudaStream_t st);
 int lusgs_init(const MeshD &m, const GeomD &g, EvalD &ev, const real *dTau, real dt, real alphaDiag, real *jdiag, cudaStream_t st);
 int update_sgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc,
                real *uIncNew, const real *jdiag, int forward, int gsUpdate, int uIncIsZero, real *sumIncHost, cudaStream_t st);
@@ -209,7 +222,9 @@ real *reduce_cols(int op, int64_t n, int ncol, const real *x, const real *w, int
 int vr_iter_bc(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc,
                int uRecIsZero, int useFP32, cudaStream_t st);
 // writes the face flux of every boundary face
-int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, real *ff, cudaStream_t st);
+// uRecG: the reconstruction of the inner gradients (uRecUnlim)
+int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, const real *uRecG, real *ff,
+           cudaStream_t st);
 
 // ---- derivatives (adjoint.cu): VJP / JVP of EvaluateRHS and of one VR Jacobi sweep ----
 // deltaLambdaCell (the entropy-fix scale of the last EvaluateDt) is held fixed, as between the

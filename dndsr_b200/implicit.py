@@ -203,9 +203,11 @@ class SolverConfig:
     meanScale: tuple = ()            # GMRES dot weights (gmresScale), empty = ones
     # positivity-preserving increments (timeMarchControl.incrementPPRelax, uRecAlphaCompressPower,
     # ppEpsIsRelaxed); the floors scale with the far-field state, empty = plain u += alpha inc
-    # limiterControl (EulerSolver.hxx:455-580): WBAP_C after the VR sweeps, the RHS from the limited
-    # reconstruction (inviscid evaluators: their face values are all the reference takes from it)
+    # limiterControl (EulerSolver.hxx:455-580, EulerSolver.hpp:670 useViscousLimited): WBAP_C after the VR
+    # sweeps, the RHS with point values from the limited reconstruction and gradients from the limited
+    # (useViscousLimited) or unlimited one
     useLimiter: bool = False
+    useViscousLimited: bool = True
     smoothThreshold: float = 0.01
     WBAP_nStd: float = 10.0
     preserveLimited: bool = False
@@ -235,9 +237,12 @@ class ImplicitSolver:
         self.n_sgs = 0
         self.uRecLim = None
         if cfg.useLimiter:
-            if not bool(ev.settings.get("ignoreVis", False)):
-                raise NotImplementedError("useLimiter: the limited / unlimited reconstruction pair of a viscous RHS is not built")
             self.uRecLim = vr.BuildURec(nv)
+        # EvaluateRHS reports non-physical states once per pseudo-iteration (fstop reads the residual
+        # norm there anyway) instead of synchronising on every call
+        self.deferred = hasattr(ev, "SetDeferredErrors")
+        if self.deferred:
+            ev.SetDeferredErrors(True)
         self.pp = None
         if cfg.farFieldStaticValue:
             far = [float(x) for x in cfg.farFieldStaticValue]
@@ -257,14 +262,16 @@ class ImplicitSolver:
             self.ev.DoLimiterWBAP_C(cx, self.uRec, si, self.uRecLim, self.cfg.smoothThreshold, self.cfg.WBAP_nStd, False)
             if self.cfg.preserveLimited:
                 self.uRec.copy_(self.uRecLim)
-            self.ev.EvaluateRHS(crhs, cx, self.uRecLim)
+            # EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, ...) with uRecUnlim = the limited reconstruction
+            # (useViscousLimited, the default) or the unlimited one (EulerSolver.hxx:624-626)
+            self.ev.EvaluateRHS(crhs, cx, self.uRecLim, uRecUnlim=self.uRecLim if self.cfg.useViscousLimited else self.uRec)
         else:
             self.ev.EvaluateRHS(crhs, cx, self.uRec)
         self.n_rhs += 1
 
     # EulerSolver.hxx:674-694
     def fdtau(self, cx, dtau, alphaDiag):
-        self.ev.EvaluateDt(dtau, cx, self.CFLNow, 1e100, self.cfg.useLocalDt)
+        self.ev.EvaluateDt(dtau, cx, self.CFLNow, 1e100, self.cfg.useLocalDt, want_min=False)
         dtau.mul_(1.0 / alphaDiag)
 
     # EulerSolver.hxx:696-738: EvaluateCellRHSAlpha, then AddFixedIncrement of alphaPP * inc (with a
@@ -334,6 +341,8 @@ class ImplicitSolver:
     def fstop(self, it, res, stage):
         cfg = self.cfg
         nrm = np.asarray(self.ev.EvaluateNorm(res, cfg.normOrd, cfg.useVolWiseResidual), dtype=np.float64)
+        if self.deferred:
+            self.ev.CheckErrors()
         if it == 1 or self.resBase is None:
             self.resBase = np.zeros_like(nrm)
         self.resBase = np.maximum(self.resBase, nrm)

@@ -249,14 +249,41 @@ class EulerEvaluator(Handle):
     def InitializeUDOF(self, u, kind, chi=5.0):
         capi.call("dndsb_eval_initialize_udof", self.h, kind, float(chi), _ptr(u, "u"), _stream())
 
-    def EvaluateDt(self, dt, u, CFL, MaxDt=1e100, UseLocaldt=True):
+    def EvaluateDt(self, dt, u, CFL, MaxDt=1e100, UseLocaldt=True, want_min=True):
+        """Returns the global minimum of dt (want_min=False with UseLocaldt: no host synchronisation, None)."""
         mn = ctypes.c_double()
+        ask = want_min or not UseLocaldt
         capi.call("dndsb_eval_evaluate_dt", self.h, _ptr(u, "u"), float(CFL), float(MaxDt), int(UseLocaldt), _ptr(dt, "dt"),
-                  ctypes.byref(mn), _stream())
-        return mn.value
+                  ctypes.byref(mn) if ask else None, _stream())
+        return mn.value if ask else None
 
-    def EvaluateRHS(self, rhs, u, uRec):
-        capi.call("dndsb_eval_evaluate_rhs", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+    # EvaluateRHS flags, EulerEvaluator.hpp:370-378
+    RHS_No_Flags, RHS_Ignore_Viscosity, RHS_Dont_Update_Integration, RHS_Dont_Record_Bud_Flux = 0, 1, 2, 4
+
+    def EvaluateRHS(self, rhs, u, uRec, JSource=None, uRecUnlim=None, uRecBeta=None, cellRHSAlpha=None, onlyOnHalfAlpha=False, t=0.0,
+                    flags=0):
+        """EvaluateRHS (EulerEvaluator_EvaluateRHS.hxx:55-818).  The short form (rhs, u, uRec) evaluates with
+        the reconstruction uRec for values and gradients.  The keyword form is the reference's full
+        contract: uRecUnlim gives the gradients (uRec the limited point values), cellRHSAlpha scales the
+        SA source, JSource [nCell][nVars] receives the source Jacobian diagonal, flags are RHS_* bits;
+        uRecBeta, onlyOnHalfAlpha and t are accepted and not read, as in the reference's body."""
+        if JSource is None and uRecUnlim is None and cellRHSAlpha is None and flags == 0:
+            capi.call("dndsb_eval_evaluate_rhs", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+            return
+        capi.call("dndsb_eval_evaluate_rhs_full", self.h, _ptr(rhs, "rhs"), _ptr(JSource, "JSource") if JSource is not None else None,
+                  _ptr(u, "u"), _ptr(uRecUnlim if uRecUnlim is not None else uRec, "uRecUnlim"), _ptr(uRec, "uRec"),
+                  _ptr(uRecBeta, "uRecBeta") if uRecBeta is not None else None,
+                  _ptr(cellRHSAlpha, "cellRHSAlpha") if cellRHSAlpha is not None else None, int(bool(onlyOnHalfAlpha)), float(t),
+                  int(flags), _stream())
+
+    def SetDeferredErrors(self, deferred=True):
+        """EvaluateRHS stops reading its error word back on every call; CheckErrors reads it."""
+        capi.call("dndsb_eval_set_deferred_errors", self.h, int(bool(deferred)))
+
+    def CheckErrors(self):
+        """Reads and clears the deferred error word of EvaluateRHS (raises DndsbError on a non-physical or
+        non-finite state seen since the last check)."""
+        capi.call("dndsb_eval_check_errors", self.h, _stream())
 
     def EvaluateRHSNoAlloc(self, rhs, u, uRec):
         """EvaluateRHS without any device allocation: the face-flux scratch is a

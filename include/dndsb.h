@@ -170,7 +170,9 @@ int dndsb_eval_set_wall_distance(dndsb_eval *ev, const double *dHost);
 /* InitializeUDOF special initialisers, EulerEvaluator.hxx:1039-1143:
  * kind 2 = isentropic vortex of strength chi, 3 = Taylor-Green vortex (M0 = 0.1) */
 int dndsb_eval_initialize_udof(dndsb_eval *ev, int kind, double chi, double *u, void *stream);
-/* EvaluateDt(dt, u, uRec, CFL, dtMinall, MaxDt, UseLocaldt, t), EulerEvaluator_EvaluateDt.hxx:840-1048 */
+/* EvaluateDt(dt, u, uRec, CFL, dtMinall, MaxDt, UseLocaldt, t), EulerEvaluator_EvaluateDt.hxx:840-1048.
+ * dtMinHost receives the global minimum (one host synchronisation); with useLocalDt and dtMinHost NULL
+ * the call only launches. */
 int dndsb_eval_evaluate_dt(dndsb_eval *ev, const double *u, double CFL, double MaxDt, int useLocalDt, double *dt, double *dtMinHost,
                            void *stream);
 /* EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, ...), EulerEvaluator_EvaluateRHS.hxx:55-818
@@ -178,6 +180,30 @@ int dndsb_eval_evaluate_dt(dndsb_eval *ev, const double *u, double CFL, double M
  * is integrated at the cell Gauss points and JSource (the source Jacobian diagonal) is kept for
  * the next lusgs_matrix_init. */
 int dndsb_eval_evaluate_rhs(dndsb_eval *ev, double *rhs, const double *u, const double *uRec, void *stream);
+/* The full EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, uRecBeta, cellRHSAlpha, onlyOnHalfAlpha, t, flags),
+ * EulerEvaluator.hpp:399-409 / EulerEvaluator_EvaluateRHS.hxx:55-818: point values from uRec (the limited
+ * reconstruction), gradients of the viscous flux and of the SA source from uRecUnlim (may be the same
+ * array); the SA source and JSource are scaled by cellRHSAlpha [nCell] (NULL = 1, :790); JSource
+ * [nCell][nVars] (may be NULL) receives the source Jacobian diagonal (zero for 5 variables).  uRecBeta,
+ * onlyOnHalfAlpha and t are accepted and, as in the reference's body, not read (the supported boundary
+ * types are time independent).  flags: the reference's RHS_* bits (EulerEvaluator.hpp:370-378) below;
+ * the direct second-order reconstruction bits are rejected with DNDSB_E_UNSUPPORTED.  Unless
+ * RHS_Dont_Update_Integration is set, the wall-flux integral (:599-607, minus the summed face fluxes of
+ * BCWall, BCWallIsothermal and, when muGas < 1e-99, BCWallInvis faces) is kept as "fluxWallSum"
+ * (dndsb_eval_get_array). */
+#define DNDSB_RHS_IGNORE_VISCOSITY (1ull << 0)
+#define DNDSB_RHS_DONT_UPDATE_INTEGRATION (1ull << 1)
+#define DNDSB_RHS_DONT_RECORD_BND_FLUX (1ull << 2)
+int dndsb_eval_evaluate_rhs_full(dndsb_eval *ev, double *rhs, double *JSource, const double *u, const double *uRecUnlim, const double *uRec,
+                                 const double *uRecBeta, const double *cellRHSAlpha, int onlyOnHalfAlpha, double t, uint64_t flags,
+                                 void *stream);
+/* Error reporting of EvaluateRHS (no reference counterpart: the reference asserts inside its loops).
+ * By default each EvaluateRHS reads its device error word back and synchronises its stream, so that
+ * it returns DNDSB_E_NONPHYSICAL / DNDSB_E_NONFINITE itself.  With set_deferred_errors(ev, 1) it only
+ * launches: its kernels OR their findings into a deferred word, which check_errors reads, clears and
+ * reports (one synchronisation, e.g. once per pseudo-iteration where a residual norm is read anyway). */
+int dndsb_eval_set_deferred_errors(dndsb_eval *ev, int deferred);
+int dndsb_eval_check_errors(dndsb_eval *ev, void *stream);
 /* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, 0, t), EulerEvaluator.hxx:37-159 (scalar Jacobian).
  * jdiag holds one value per cell for 5 variables, and nVars values per cell for the SA model
  * (the shared diagonal plus alphaDiag times JSource of the last RHS). */

@@ -84,6 +84,7 @@ def _declare(L):
     L.orc_vr_iter.argtypes = [_V, _D, _D, _D, ctypes.c_int, ctypes.c_int]
     L.orc_eval_dt.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D]
     L.orc_eval_rhs.argtypes = [_V, _D, _D, _D, _D]
+    L.orc_eval_rhs_full.argtypes = [_V, _D, _D, _D, _D, _D, _D, _D]
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_update_sgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
     L.orc_update_lusgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int]
@@ -264,6 +265,17 @@ class Oracle:
         ff = np.zeros((self.mesh.n_face, self.nv)) if want_face_flux else None
         lib().orc_eval_rhs(self.h, _p(u), _p(uRec), _p(rhs), _p(ff) if ff is not None else None)
         return (rhs, ff) if want_face_flux else rhs
+
+    def eval_rhs_full(self, u, uRecUnlim, uRec, alpha=None):
+        """EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, uRecBeta, cellRHSAlpha, ...): face values from uRec,
+        gradients from uRecUnlim, SA source scaled by alpha.  Returns (rhs, JSource [nCell][nv], fluxWallSum [nv])."""
+        u, uU, uR = _f64(u), _f64(uRecUnlim), _f64(uRec)
+        rhs = np.zeros_like(u)
+        js = np.zeros_like(u)
+        fw = np.zeros(self.nv)
+        a = _f64(alpha) if alpha is not None else None
+        lib().orc_eval_rhs_full(self.h, _p(u), _p(uU), _p(uR), _p(a) if a is not None else None, _p(rhs), _p(js), _p(fw))
+        return rhs, js, fw
 
     def lusgs_init(self, dTau, dt, alphaDiag):
         dTau = _f64(dTau)

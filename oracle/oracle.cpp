@@ -1861,8 +1861,12 @@ struct Oracle
 
     // EvaluateRHS.hxx:665-801 source integration (SA only; the NS source is zero) and the
     // source-term Jacobian diagonal JSource, both cell means
-    void addSource(const real *u, const real *uRec, real *rhs)
+    // EvaluateRHS.hxx:677-801: values from uRec, gradients from uRecUnlim (uRecG), the integral scaled by
+    // cellRHSAlpha / V (alpha == nullptr: 1)
+    void addSource(const real *u, const real *uRec, real *rhs, const real *uRecG = nullptr, const real *alpha = nullptr)
     {
+        if (!uRecG)
+            uRecG = uRec;
         int nv = es.nVars;
         jSource.assign(nCell * nv, 0.0);
         if (nv < 6)
@@ -1888,7 +1892,7 @@ struct Oracle
                     {
                         real ga = 0;
                         for (int j = 0; j < R; j++)
-                            ga += T[(1 + d) * NDOF + 1 + j] * uRec[(c * R + j) * nv + v];
+                            ga += T[(1 + d) * NDOF + 1 + j] * uRecG[(c * R + j) * nv + v];
                         G[d * nv + v] = ga;
                     }
                 }
@@ -1904,8 +1908,9 @@ struct Oracle
                 S += saSource(U, G, muf, d, lLES, hMax, 0) * JW;
                 J += saSource(U, G, muf, d, lLES, hMax, 1) * JW;
             }
-            rhs[c * nv + 5] += S / vol[c];
-            jSource[c * nv + 5] = J / vol[c];
+            real a = alpha ? alpha[c] : 1.0;
+            rhs[c * nv + 5] += S * a / vol[c];
+            jSource[c * nv + 5] = J * a / vol[c];
         }
     }
 
@@ -1914,7 +1919,7 @@ struct Oracle
     // mean at the face centre (:198-210), gradient copied from the inside (:360-362), GRP
     // distance from the face centre (:363-386), viscous flux removed on slip, far-field and
     // outflow faces (:423-430, EvaluateDt.hxx:1203-1207)
-    void boundaryFaceFlux(long f, const real *u, const real *uRec, real *fluxEs) const
+    void boundaryFaceFlux(long f, const real *u, const real *uRec, real *fluxEs, const real *uRecG) const
     {
         int nv = es.nVars;
         real gamma = es.gamma;
@@ -1949,7 +1954,7 @@ struct Oracle
                 {
                     real ga = 0;
                     for (int j = 0; j < R; j++)
-                        ga += T0[(1 + d) * NDOF + 1 + j] * uRec[(c0 * R + j) * nv + v];
+                        ga += T0[(1 + d) * NDOF + 1 + j] * uRecG[(c0 * R + j) * nv + v];
                     GL[d * nv + v] = ga;
                 }
             }
@@ -1988,8 +1993,15 @@ struct Oracle
     // EulerEvaluator_EvaluateRHS.hxx:55-818 EvaluateRHS with the flux of
     // EulerEvaluator_EvaluateDt.hxx:1084-1511 fluxFace (interior/periodic faces,
     // no limiter, source term ignored, no grid velocity)
-    void evaluateRHS(const real *u, const real *uRec, real *rhs, real *faceFluxOut)
+    // uRecG: the unlimited reconstruction the gradients come from (EvaluateRHS.hxx:264-327, uRecUnlim;
+    // nullptr: uRec); alpha: cellRHSAlpha of the source term (nullptr: 1); fluxWall (may be nullptr): the
+    // wall-flux integral of :599-607, minus the face fluxes of BCWall / BCWallIsothermal faces (and of
+    // BCWallInvis faces when muGas < 1e-99), summed in face order
+    void evaluateRHS(const real *u, const real *uRec, real *rhs, real *faceFluxOut, const real *uRecG = nullptr, const real *alpha = nullptr,
+                     real *fluxWall = nullptr)
     {
+        if (!uRecG)
+            uRecG = uRec;
         int nv = es.nVars;
         real gamma = es.gamma;
         std::vector<real> faceFlux(nFace * nv, 0.0);
@@ -2001,7 +2013,7 @@ struct Oracle
             long c0 = face2cell[f * 2 + 0], c1 = face2cell[f * 2 + 1];
             if (c1 < 0)
             {
-                boundaryFaceFlux(f, u, uRec, &faceFlux[f * nv]);
+                boundaryFaceFlux(f, u, uRec, &faceFlux[f * nv], uRecG);
                 continue;
             }
             std::vector<real> T0(4 * NDOF), T1(4 * NDOF);
@@ -2035,8 +2047,8 @@ struct Oracle
                         real ga = 0, gb = 0;
                         for (int j = 0; j < R; j++)
                         {
-                            ga += T0[(1 + d) * NDOF + 1 + j] * uRec[(c0 * R + j) * nv + v];
-                            gb += T1[(1 + d) * NDOF + 1 + j] * uRec[(c1 * R + j) * nv + v];
+                            ga += T0[(1 + d) * NDOF + 1 + j] * uRecG[(c0 * R + j) * nv + v];
+                            gb += T1[(1 + d) * NDOF + 1 + j] * uRecG[(c1 * R + j) * nv + v];
                         }
                         GL[d * nv + v] = ga, GR[d * nv + v] = gb;
                     }
@@ -2087,9 +2099,23 @@ struct Oracle
                     rhs[c * nv + v] += sgn * faceFlux[f * nv + v] / vol[c];
             }
         }
-        addSource(u, uRec, rhs);
+        addSource(u, uRec, rhs, uRecG, alpha);
         if (faceFluxOut)
             std::copy(faceFlux.begin(), faceFlux.end(), faceFluxOut);
+        if (fluxWall)
+        {
+            for (int v = 0; v < nv; v++)
+                fluxWall[v] = 0;
+            for (long f = 0; f < nFace; f++)
+            {
+                if (face2cell[f * 2 + 1] >= 0)
+                    continue;
+                int t = zoneType(f);
+                if (t == 2 || t == 4 || (t == 3 && es.muGas < 1e-99))
+                    for (int v = 0; v < nv; v++)
+                        fluxWall[v] -= faceFlux[f * nv + v];
+            }
+        }
     }
 
     // EulerEvaluator.hxx:37-159 LUSGSMatrixInit, scalar Jacobian, source ignored
@@ -2557,6 +2583,16 @@ extern "C"
     void orc_eval_rhs(void *h, const double *u, const double *uRec, double *rhs, double *faceFlux)
     {
         ((Oracle *)h)->evaluateRHS(u, uRec, rhs, faceFlux);
+    }
+    // EvaluateRHS(rhs, JSource, u, uRecUnlim, uRec, uRecBeta, cellRHSAlpha, ...): jSource (may be null)
+    // receives the source Jacobian diagonal [nCell][nv], fluxWall (may be null) the wall-flux integral [nv]
+    void orc_eval_rhs_full(void *h, const double *u, const double *uRecUnlim, const double *uRec, const double *alpha, double *rhs,
+                           double *jSource, double *fluxWall)
+    {
+        Oracle *o = (Oracle *)h;
+        o->evaluateRHS(u, uRec, rhs, nullptr, uRecUnlim, alpha, fluxWall);
+        if (jSource)
+            std::copy(o->jSource.begin(), o->jSource.end(), jSource);
     }
 
     void orc_lusgs_init(void *h, const double *dTau, double dt, double alphaDiag, double *jdiag)

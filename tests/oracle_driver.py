@@ -34,10 +34,13 @@ class OracleEval:
         self.o, self.nVars = o, o.nv
         self.vol = o.get("volume")
 
-    def EvaluateRHS(self, rhs, u, uRec):
-        rhs.copy_(torch.tensor(self.o.eval_rhs(u.numpy(), uRec.numpy())))
+    def EvaluateRHS(self, rhs, u, uRec, uRecUnlim=None):
+        if uRecUnlim is None:
+            rhs.copy_(torch.tensor(self.o.eval_rhs(u.numpy(), uRec.numpy())))
+        else:
+            rhs.copy_(torch.tensor(self.o.eval_rhs_full(u.numpy(), uRecUnlim.numpy(), uRec.numpy())[0]))
 
-    def EvaluateDt(self, dt, u, CFL, MaxDt=1e100, UseLocaldt=True):
+    def EvaluateDt(self, dt, u, CFL, MaxDt=1e100, UseLocaldt=True, want_min=True):
         d, mn = self.o.eval_dt(u.numpy(), CFL, MaxDt, UseLocaldt)
         dt.copy_(torch.tensor(d))
         return mn
