@@ -36,8 +36,29 @@ def _headers_mtime():
     return max(os.path.getmtime(p) for p in hs)
 
 
+def _ext_path():
+    import sysconfig
+    return os.path.join(HERE, "_C" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_pybind(force=False):
+    """The pybind11 module dndsr_b200/_C (host C++ over the C-ABI), linked to libdndsb.so by an $ORIGIN rpath."""
+    import sysconfig
+    import pybind11
+    src = os.path.join(HERE, "csrc", "pybind.cpp")
+    out = _ext_path()
+    hdr = os.path.join(os.path.dirname(HERE), "include", "dndsb.h")
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(src), os.path.getmtime(hdr), os.path.getmtime(LIB)):
+        return out
+    cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden", "-I", pybind11.get_include(), "-I",
+           sysconfig.get_paths()["include"], src, "-o", out, "-L", HERE, "-ldndsb", "-Wl,-rpath,$ORIGIN"]
+    subprocess.check_call(cmd)
+    return out
+
+
 def build(force=False, verbose=False, jobs=None):
     if not force and up_to_date():
+        build_pybind()
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -64,6 +85,7 @@ def build(force=False, verbose=False, jobs=None):
     if failed:
         raise RuntimeError("nvcc failed")
     subprocess.check_call([NVCC, *FLAGS, "-shared", "-o", LIB, *objs, "-lcudart"])
+    build_pybind(force=True)
     return LIB
 
 

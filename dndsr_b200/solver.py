@@ -4,17 +4,16 @@ Class and method names follow CFV::VariationalReconstruction
 (src/CFV/VariationalReconstruction.hpp:108-1114, bound in
 src/CFV/VariationalReconstruction_bind.hpp:19-145) and
 Euler::EulerEvaluator (src/Euler/EulerEvaluator.hpp:76-1980).  State arrays
-are caller-owned contiguous float64 CUDA tensors; every call goes through the
-C-ABI of include/dndsb.h on torch's current stream.
+are caller-owned contiguous float64 CUDA tensors.  Every call goes through the
+pybind11 module ``dndsr_b200._C`` (csrc/pybind.cpp), which calls the C-ABI of
+include/dndsb.h on torch's current stream; this layer adds the reference's
+setting names and defaults and allocates result tensors.
 """
 from __future__ import annotations
-
-import ctypes
 
 import numpy as np
 import torch
 
-from . import capi
 from .mesh import Mesh
 
 # reference setting names -> C struct codes
@@ -51,59 +50,37 @@ def euler_bc_dir_weights(types, maxOrder=3):
     return w
 
 
-def _stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+def _C():
+    """The pybind11 module; there is no CPU path, so a host without a CUDA device is refused here."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("dndsr_b200 needs a CUDA device; there is no CPU path")
+    from . import build as _b
+    if not _b.up_to_date():
+        raise ImportError("dndsr_b200/libdndsb.so is missing or stale: run dndsr_b200/build.py (nvcc, sm_100a)")
+    from . import _C as mod
+    return mod
 
 
-def _ptr(t: torch.Tensor, nm="tensor", fp32=False):
-    dt = torch.float32 if fp32 else torch.float64
-    if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
-        raise ValueError(f"{nm} must be a contiguous {'float32' if fp32 else 'float64'} CUDA tensor")
-    return ctypes.c_void_p(t.data_ptr())
-
-
-class Handle:
-    _destroy = None
-
-    def __del__(self):
-        h = getattr(self, "h", None)
-        if h and self._destroy:
-            try:
-                capi.load(require_device=False)
-                getattr(capi._lib, self._destroy)(h)
-            except Exception:
-                pass
-            self.h = None
-
-
-class DeviceMesh(Handle):
+class DeviceMesh:
     """Uploads a :class:`dndsr_b200.mesh.Mesh` (replaces Geom::UnstructuredMesh as the VR input)."""
-    _destroy = "dndsb_mesh_destroy"
 
     def __init__(self, mesh: Mesh):
-        capi.load()
+        C = _C()
         self.mesh = mesh
         a = mesh.arrays()
-        self._keep = a
-        h = ctypes.c_void_p()
-        D = capi.dptr
-        I64 = lambda x: x.ctypes.data_as(capi._I64)
-        capi.call("dndsb_mesh_create", ctypes.byref(h), mesh.dim, mesh.cell_type, mesh.face_type, mesh.n_node, D(a["coords"]), mesh.n_cell,
-                  a["cell2node"].shape[1], I64(a["cell2node"]), D(a["cell_shift"]), mesh.n_face, a["face2node"].shape[1],
-                  I64(a["face2node"]), D(a["face_shift"]), I64(a["face2cell"]), a["face_zone"].ctypes.data_as(capi._I32), D(a["face_pshift"]),
-                  a["cell2face"].shape[1], I64(a["cell2face"]))
-        self.h = h
+        self._c = C.Mesh(mesh.dim, mesh.cell_type, mesh.face_type, a["coords"], a["cell2node"], a["cell_shift"], a["face2node"],
+                         a["face_shift"], a["face2cell"], a["face_zone"], a["face_pshift"], a["cell2face"])
 
     def colors(self):
-        n = ctypes.c_int()
-        col = np.zeros(self.mesh.n_cell, dtype=np.int32)
-        capi.call("dndsb_mesh_colors", self.h, ctypes.byref(n), col.ctypes.data_as(capi._I32))
-        return n.value, col
+        return self._c.colors()
 
 
-class VariationalReconstruction(Handle):
+def _code(table, x):
+    return table[x] if isinstance(x, str) else int(x)
+
+
+class VariationalReconstruction:
     """CFV::VariationalReconstruction<dim> on the GPU."""
-    _destroy = "dndsb_vr_destroy"
 
     def __init__(self, mesh, settings: dict | None = None):
         self.dmesh = mesh if isinstance(mesh, DeviceMesh) else DeviceMesh(mesh)
@@ -111,38 +88,25 @@ class VariationalReconstruction(Handle):
         s = dict(VR_DEFAULTS)
         s.update(settings or {})
         self.settings = s
-        cs = capi.VRSettings()
-        cs.maxOrder, cs.intOrder, cs.jacobiRelax = int(s["maxOrder"]), int(s["intOrder"]), float(s["jacobiRelax"])
-        cs.SORInstead, cs.anisotropicLengths = int(bool(s["SORInstead"])), int(bool(s["anisotropicLengths"]))
-        cs.scaleType = _SCALE[s["scaleType"]] if isinstance(s["scaleType"], str) else int(s["scaleType"])
-        cs.scaleMultiplier = float(s["scaleMultiplier"])
-        cs.dirWeightScheme = _DIRW[s["dirWeightScheme"]] if isinstance(s["dirWeightScheme"], str) else int(s["dirWeightScheme"])
-        for i, x in enumerate(s["manualDirWeights"][:4]):
-            cs.manualDirWeights[i] = float(x)
-        cs.geomWeightScheme = _GEOMW[s["geomWeightScheme"]] if isinstance(s["geomWeightScheme"], str) else int(s["geomWeightScheme"])
-        cs.geomWeightBias, cs.geomWeightPower = float(s["geomWeightBias"]), float(s["geomWeightPower"])
-        cs.geomWeightPower1, cs.geomWeightPower2, cs.bcWeight = float(s["geomWeightPower1"]), float(s["geomWeightPower2"]), float(s["bcWeight"])
-        h = ctypes.c_void_p()
-        capi.call("dndsb_vr_create", ctypes.byref(h), self.dmesh.h, ctypes.byref(cs))
-        self.h = h
-        self._cs = cs
+        cs = dict(maxOrder=int(s["maxOrder"]), intOrder=int(s["intOrder"]), jacobiRelax=float(s["jacobiRelax"]),
+                  SORInstead=int(bool(s["SORInstead"])), anisotropicLengths=int(bool(s["anisotropicLengths"])),
+                  scaleType=_code(_SCALE, s["scaleType"]), scaleMultiplier=float(s["scaleMultiplier"]),
+                  dirWeightScheme=_code(_DIRW, s["dirWeightScheme"]), manualDirWeights=[float(x) for x in s["manualDirWeights"]][:4],
+                  geomWeightScheme=_code(_GEOMW, s["geomWeightScheme"]), geomWeightBias=float(s["geomWeightBias"]),
+                  geomWeightPower=float(s["geomWeightPower"]), geomWeightPower1=float(s["geomWeightPower1"]),
+                  geomWeightPower2=float(s["geomWeightPower2"]), bcWeight=float(s["bcWeight"]))
+        self._c = _C().VariationalReconstruction(self.dmesh._c, cs)
 
     # VariationalReconstruction.cpp:10-43, :56-498, :507-872
     def ConstructMetrics(self):
-        capi.call("dndsb_vr_construct_metrics", self.h)
+        self._c.ConstructMetrics()
 
     def ConstructBaseAndWeight(self, bc_dir_weight=None):
-        if bc_dir_weight is None:
-            capi.call("dndsb_vr_construct_base_and_weight", self.h, None, 0)
-        else:
-            w = np.ascontiguousarray(bc_dir_weight, dtype=np.float64).reshape(-1, 4)
-            capi.call("dndsb_vr_construct_base_and_weight", self.h, capi.dptr(w), w.shape[0])
+        self._c.ConstructBaseAndWeight(None if bc_dir_weight is None else np.ascontiguousarray(bc_dir_weight, dtype=np.float64).reshape(-1, 4))
 
     def ConstructRecCoeff(self):
-        capi.call("dndsb_vr_construct_rec_coeff", self.h)
-        out = np.zeros(4, dtype=np.int64)
-        capi.call("dndsb_vr_sizes", self.h, out.ctypes.data_as(capi._I64))
-        self.NDOF, self.R, self.nGf, self.nGc = [int(x) for x in out]
+        self._c.ConstructRecCoeff()
+        self.NDOF, self.R, self.nGf, self.nGc = [int(x) for x in self._c.sizes()]
 
     def construct(self, bc_dir_weight=None):
         self.ConstructMetrics()
@@ -151,11 +115,7 @@ class VariationalReconstruction(Handle):
         return self
 
     def get(self, name):
-        n = ctypes.c_int64()
-        capi.call("dndsb_vr_get_array", self.h, name.encode(), None, 0, ctypes.byref(n))
-        out = np.zeros(n.value)
-        capi.call("dndsb_vr_get_array", self.h, name.encode(), capi.dptr(out), n.value, ctypes.byref(n))
-        return out
+        return self._c.get(name)
 
     # VariationalReconstruction.hpp:920-1000 BuildURec / FiniteVolume BuildUDof
     def BuildURec(self, nVars):
@@ -166,71 +126,60 @@ class VariationalReconstruction(Handle):
 
     def DoReconstructionIter(self, uRec, uRecNew, u, putIntoNew=False, recordInc=False, uRecIsZero=False, precision="fp64"):
         """VariationalReconstruction_Reconstruction.hxx:485-615 (Jacobi sweep)."""
-        nv = u.shape[1]
-        capi.call("dndsb_vr_do_reconstruction_iter", self.h, _ptr(uRec, "uRec"), _ptr(uRecNew, "uRecNew"), _ptr(u, "u"), nv,
-                  int(putIntoNew), int(recordInc), int(uRecIsZero), 1 if precision == "fp32" else 0, _stream())
-
+        self._c.DoReconstructionIter(uRec, uRecNew, u, u.shape[1], bool(putIntoNew), bool(recordInc), bool(uRecIsZero),
+                                     1 if precision == "fp32" else 0)
 
     def DoReconstructionIterVJP(self, cot, uRec, u):
         """Vector-Jacobian product of one Jacobi sweep uRecNew = S(uRec, u): returns
         ((dS/duRec)^T cot, (dS/du)^T cot)."""
         vRec, vU = torch.empty_like(uRec), torch.empty_like(u)
-        capi.call("dndsb_vr_iter_vjp", self.h, _ptr(cot, "cot"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1], _ptr(vRec, "vRec"),
-                  _ptr(vU, "vU"), _stream())
+        self._c.DoReconstructionIterVJP(cot, uRec, u, u.shape[1], vRec, vU)
         return vRec, vU
 
     def DoReconstructionIterJVP(self, dRec, du, uRec, u):
         """Jacobian-vector product of one Jacobi sweep (DoReconstructionIterDiff with the
         linearised boundary term): dS/duRec dRec + dS/du du."""
         out = torch.empty_like(uRec)
-        capi.call("dndsb_vr_iter_jvp", self.h, _ptr(dRec, "dRec"), _ptr(du, "du"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1],
-                  _ptr(out, "dRecNew"), _stream())
+        self._c.DoReconstructionIterJVP(dRec, du, uRec, u, u.shape[1], out)
         return out
 
     def DoCalculateSmoothIndicator(self, u, uRec):
         """VariationalReconstruction_LimiterProcedure.hxx:40-108 (procedure 0, density and energy): si [nCell]."""
         si = torch.empty(self.mesh.n_cell, dtype=torch.float64, device="cuda")
-        capi.call("dndsb_vr_smooth_indicator", self.h, _ptr(u, "u"), _ptr(uRec, "uRec"), u.shape[1], _ptr(si, "si"), _stream())
+        self._c.DoCalculateSmoothIndicator(u, uRec, u.shape[1], si)
         return si
 
     def DoReconstructionIterVJPCoords(self, cot, uRec, u):
         """(dS/dX)^T cot for one Jacobi sweep uRecNew = S(uRec, u; X), X the node coordinates
         [nNode][3]: the geometry, basis moments, weights and A^-1 B / A^-1 b are differentiated."""
         dX = torch.empty((self.mesh.n_node, 3), dtype=torch.float64, device="cuda")
-        capi.call("dndsb_vr_iter_vjp_coords", self.h, _ptr(cot, "cot"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1], _ptr(dX, "dX"),
-                  _stream())
+        self._c.DoReconstructionIterVJPCoords(cot, uRec, u, u.shape[1], dX)
         return dX
 
     def DoReconstructionIterJVPCoords(self, dX, uRec, u):
         """dS/dX dX for one Jacobi sweep along the node displacement dX [nNode][3]."""
         out = torch.empty_like(uRec)
-        capi.call("dndsb_vr_iter_jvp_coords", self.h, _ptr(dX, "dX"), _ptr(uRec, "uRec"), _ptr(u, "u"), u.shape[1], _ptr(out, "dRecNew"),
-                  _stream())
+        self._c.DoReconstructionIterJVPCoords(dX, uRec, u, u.shape[1], out)
         return out
 
 
-class EulerEvaluator(Handle):
-    """Euler::EulerEvaluator<model> on the GPU (models NS / NS_3D with 5 variables)."""
-    _destroy = "dndsb_eval_destroy"
+class EulerEvaluator:
+    """Euler::EulerEvaluator<model> on the GPU (models NS / NS_3D with 5 variables, NS_SA with 6)."""
+
+    # EvaluateRHS flags, EulerEvaluator.hpp:370-378
+    RHS_No_Flags, RHS_Ignore_Viscosity, RHS_Dont_Update_Integration, RHS_Dont_Record_Bud_Flux = 0, 1, 2, 4
 
     def __init__(self, vr: VariationalReconstruction, settings: dict | None = None):
         self.vr = vr
         s = dict(EULER_DEFAULTS)
         s.update(settings or {})
         self.settings = s
-        cs = capi.EulerSettings()
-        cs.nVars = int(s["nVars"])
-        rs = s["riemannSolverType"]
-        cs.rsType = RS[rs] if isinstance(rs, str) else int(rs)
-        cs.rsFixScale, cs.rsIncFScale = float(s["rsFixScale"]), float(s["rsIncFScale"])
-        cs.gamma, cs.Rgas, cs.muGas, cs.prGas = float(s["gamma"]), float(s["Rgas"]), float(s["muGas"]), float(s["prGas"])
-        cs.TRef, cs.CSutherland, cs.muModel, cs.ignoreVis = float(s["TRef"]), float(s["CSutherland"]), int(s["muModel"]), int(bool(s["ignoreVis"]))
-        cs.rsMeanValueEig = int(s["rsMeanValueEig"])
-        h = ctypes.c_void_p()
-        capi.call("dndsb_eval_create", ctypes.byref(h), vr.h, ctypes.byref(cs))
-        self.h = h
-        self.nVars = cs.nVars
-        self._cs = cs
+        cs = dict(nVars=int(s["nVars"]), rsType=_code(RS, s["riemannSolverType"]), rsFixScale=float(s["rsFixScale"]),
+                  rsIncFScale=float(s["rsIncFScale"]), gamma=float(s["gamma"]), Rgas=float(s["Rgas"]), muGas=float(s["muGas"]),
+                  prGas=float(s["prGas"]), TRef=float(s["TRef"]), CSutherland=float(s["CSutherland"]), muModel=int(s["muModel"]),
+                  ignoreVis=int(bool(s["ignoreVis"])), rsMeanValueEig=int(s["rsMeanValueEig"]))
+        self._c = _C().EulerEvaluator(vr._c, cs)
+        self.nVars = cs["nVars"]
 
     def SetBC(self, types, values):
         """BoundaryHandler of the evaluator (Euler/EulerBC.hpp) as a per-zone table: types[zone]
@@ -239,26 +188,18 @@ class EulerEvaluator(Handle):
         t = np.array([BC[x] if isinstance(x, str) else int(x) for x in types], dtype=np.int32)
         v = np.ascontiguousarray(values, dtype=np.float64).reshape(len(t), self.nVars)
         self._bc = (t, v)
-        capi.call("dndsb_eval_set_bc", self.h, len(t), t.ctypes.data_as(capi._I32), capi.dptr(v))
+        self._c.SetBC(t, v)
 
     def SetWallDistance(self, d):
         """dWall of the SA model at every cell Gauss point, [nCell][nGc] host array."""
-        d = np.ascontiguousarray(d, dtype=np.float64)
-        capi.call("dndsb_eval_set_wall_distance", self.h, capi.dptr(d))
+        self._c.SetWallDistance(np.ascontiguousarray(d, dtype=np.float64))
 
     def InitializeUDOF(self, u, kind, chi=5.0):
-        capi.call("dndsb_eval_initialize_udof", self.h, kind, float(chi), _ptr(u, "u"), _stream())
+        self._c.InitializeUDOF(u, int(kind), float(chi))
 
     def EvaluateDt(self, dt, u, CFL, MaxDt=1e100, UseLocaldt=True, want_min=True):
         """Returns the global minimum of dt (want_min=False with UseLocaldt: no host synchronisation, None)."""
-        mn = ctypes.c_double()
-        ask = want_min or not UseLocaldt
-        capi.call("dndsb_eval_evaluate_dt", self.h, _ptr(u, "u"), float(CFL), float(MaxDt), int(UseLocaldt), _ptr(dt, "dt"),
-                  ctypes.byref(mn) if ask else None, _stream())
-        return mn.value if ask else None
-
-    # EvaluateRHS flags, EulerEvaluator.hpp:370-378
-    RHS_No_Flags, RHS_Ignore_Viscosity, RHS_Dont_Update_Integration, RHS_Dont_Record_Bud_Flux = 0, 1, 2, 4
+        return self._c.EvaluateDt(dt, u, float(CFL), float(MaxDt), bool(UseLocaldt), bool(want_min))
 
     def EvaluateRHS(self, rhs, u, uRec, JSource=None, uRecUnlim=None, uRecBeta=None, cellRHSAlpha=None, onlyOnHalfAlpha=False, t=0.0,
                     flags=0):
@@ -268,62 +209,56 @@ class EulerEvaluator(Handle):
         SA source, JSource [nCell][nVars] receives the source Jacobian diagonal, flags are RHS_* bits;
         uRecBeta, onlyOnHalfAlpha and t are accepted and not read, as in the reference's body."""
         if JSource is None and uRecUnlim is None and cellRHSAlpha is None and flags == 0:
-            capi.call("dndsb_eval_evaluate_rhs", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+            self._c.EvaluateRHS(rhs, u, uRec)
             return
-        capi.call("dndsb_eval_evaluate_rhs_full", self.h, _ptr(rhs, "rhs"), _ptr(JSource, "JSource") if JSource is not None else None,
-                  _ptr(u, "u"), _ptr(uRecUnlim if uRecUnlim is not None else uRec, "uRecUnlim"), _ptr(uRec, "uRec"),
-                  _ptr(uRecBeta, "uRecBeta") if uRecBeta is not None else None,
-                  _ptr(cellRHSAlpha, "cellRHSAlpha") if cellRHSAlpha is not None else None, int(bool(onlyOnHalfAlpha)), float(t),
-                  int(flags), _stream())
+        self._c.EvaluateRHSFull(rhs, JSource, u, uRecUnlim if uRecUnlim is not None else uRec, uRec, uRecBeta, cellRHSAlpha,
+                                bool(onlyOnHalfAlpha), float(t), int(flags))
 
     def SetDeferredErrors(self, deferred=True):
         """EvaluateRHS stops reading its error word back on every call; CheckErrors reads it."""
-        capi.call("dndsb_eval_set_deferred_errors", self.h, int(bool(deferred)))
+        self._c.SetDeferredErrors(bool(deferred))
 
     def CheckErrors(self):
         """Reads and clears the deferred error word of EvaluateRHS (raises DndsbError on a non-physical or
         non-finite state seen since the last check)."""
-        capi.call("dndsb_eval_check_errors", self.h, _stream())
+        self._c.CheckErrors()
 
     def EvaluateRHSNoAlloc(self, rhs, u, uRec):
         """EvaluateRHS without any device allocation: the face-flux scratch is a
         static 8 MiB device array (nFace * nVars <= capi.NOALLOC_SCRATCH_DOUBLES).
         For callers that cannot allocate device memory when they evaluate a
         residual; calls that overlap on the same GPU share the array and race."""
-        capi.call("dndsb_eval_evaluate_rhs_noalloc", self.h, _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uRec, "uRec"), _stream())
+        self._c.EvaluateRHSNoAlloc(rhs, u, uRec)
 
     def EvaluateRHSVJP(self, w, u, uRec):
         """(dR/du)^T w and (dR/duRec)^T w of EvaluateRHS at (u, uRec), deltaLambdaCell held fixed."""
         du, duRec = torch.empty_like(u), torch.empty_like(uRec)
-        capi.call("dndsb_eval_rhs_vjp", self.h, _ptr(w, "w"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(du, "du"), _ptr(duRec, "duRec"),
-                  _stream())
+        self._c.EvaluateRHSVJP(w, u, uRec, du, duRec)
         return du, duRec
 
     def EvaluateRHSJVP(self, du, duRec, u, uRec):
         """dR/du du + dR/duRec duRec of EvaluateRHS at (u, uRec), deltaLambdaCell held fixed."""
         out = torch.empty_like(u)
-        capi.call("dndsb_eval_rhs_jvp", self.h, _ptr(du, "du"), _ptr(duRec, "duRec"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(out, "dRhs"),
-                  _stream())
+        self._c.EvaluateRHSJVP(du, duRec, u, uRec, out)
         return out
 
     def EvaluateRHSVJPCoords(self, w, u, uRec):
         """(dR/dX)^T w of EvaluateRHS with respect to the node coordinates X [nNode][3] (u, uRec
         and deltaLambdaCell held fixed)."""
         dX = torch.empty((self.vr.mesh.n_node, 3), dtype=torch.float64, device="cuda")
-        capi.call("dndsb_eval_rhs_vjp_coords", self.h, _ptr(w, "w"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dX"), _stream())
+        self._c.EvaluateRHSVJPCoords(w, u, uRec, dX)
         return dX
 
     def ResidualVJPCoords(self, w, cot, u, uRec):
         """(dR/dX)^T w + (dS/dX)^T cot in one pass (S: one VR sweep of this evaluator's reconstruction)."""
         dX = torch.empty((self.vr.mesh.n_node, 3), dtype=torch.float64, device="cuda")
-        capi.call("dndsb_eval_residual_vjp_coords", self.h, _ptr(w, "w"), _ptr(cot, "cot"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dX"),
-                  _stream())
+        self._c.ResidualVJPCoords(w, cot, u, uRec, dX)
         return dX
 
     def EvaluateRHSJVPCoords(self, dX, u, uRec):
         """dR/dX dX of EvaluateRHS along the node displacement dX [nNode][3]."""
         out = torch.empty_like(u)
-        capi.call("dndsb_eval_rhs_jvp_coords", self.h, _ptr(dX, "dX"), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(out, "dRhs"), _stream())
+        self._c.EvaluateRHSJVPCoords(dX, u, uRec, out)
         return out
 
     def BuildJDiag(self):
@@ -332,38 +267,31 @@ class EulerEvaluator(Handle):
         return torch.zeros((n, self.nVars) if self.nVars == 6 else (n,), dtype=torch.float64, device="cuda")
 
     def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag):
-        capi.call("dndsb_eval_lusgs_matrix_init", self.h, _ptr(dTau, "dTau"), float(dt), float(alphaDiag), _ptr(jdiag, "jdiag"), _stream())
+        self._c.LUSGSMatrixInit(jdiag, dTau, float(dt), float(alphaDiag))
 
     def UpdateSGS(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False, want_sum=True):
-        s = np.zeros(self.nVars)
-        capi.call("dndsb_eval_update_sgs", self.h, float(alphaDiag), _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uInc, "uInc"),
-                  _ptr(uIncNew, "uIncNew"), _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), int(uIncIsZero),
-                  capi.dptr(s) if want_sum else None, _stream())
-        return s
+        s = self._c.UpdateSGS(float(alphaDiag), rhs, u, uInc, uIncNew, jdiag, bool(forward), bool(gsUpdate), bool(uIncIsZero), bool(want_sum))
+        return s if want_sum else np.zeros(self.nVars)
 
     def UpdateLUSGSForward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
         """EulerEvaluator.hxx:376-451: uIncNew = D^-1 (rhs - lower-neighbour flux increments of uInc).
         uInc may be uIncNew itself (the in-place sweep of the reference's callers)."""
-        capi.call("dndsb_eval_update_lusgs_forward", self.h, float(alphaDiag), _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uInc, "uInc"),
-                  _ptr(jdiag, "jdiag"), _ptr(uIncNew, "uIncNew"), _stream())
+        self._c.UpdateLUSGSForward(float(alphaDiag), rhs, u, uInc, jdiag, uIncNew)
 
     def UpdateLUSGSBackward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
         """EulerEvaluator.hxx:453-529: uIncNew += D^-1 (- upper-neighbour flux increments of uInc)."""
-        capi.call("dndsb_eval_update_lusgs_backward", self.h, float(alphaDiag), _ptr(rhs, "rhs"), _ptr(u, "u"), _ptr(uInc, "uInc"),
-                  _ptr(jdiag, "jdiag"), _ptr(uIncNew, "uIncNew"), _stream())
+        self._c.UpdateLUSGSBackward(float(alphaDiag), rhs, u, uInc, jdiag, uIncNew)
 
     def FixUMaxFilter(self, u):
         """EulerEvaluator.hxx:1318-1323: the reference's filter returns without changing u."""
-        capi.call("dndsb_eval_fix_umax_filter", self.h, _ptr(u, "u"), _stream())
+        self._c.FixUMaxFilter(u)
 
     def LUSGSMatrixVec(self, alphaDiag, u, uInc, jdiag, AuInc):
-        capi.call("dndsb_eval_lusgs_matrix_vec", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(uInc, "uInc"), _ptr(jdiag, "jdiag"),
-                  _ptr(AuInc, "AuInc"), _stream())
+        self._c.LUSGSMatrixVec(float(alphaDiag), u, uInc, jdiag, AuInc)
 
     def LUSGSMatrixVecT(self, alphaDiag, u, y, jdiag, ATy):
         """ATy = A^T y for the operator A of LUSGSMatrixVec (same lambdaFace, jdiag, alphaDiag)."""
-        capi.call("dndsb_eval_lusgs_matrix_vec_t", self.h, float(alphaDiag), _ptr(u, "u"), _ptr(y, "y"), _ptr(jdiag, "jdiag"),
-                  _ptr(ATy, "ATy"), _stream())
+        self._c.LUSGSMatrixVecT(float(alphaDiag), u, y, jdiag, ATy)
 
     def UpdateSGST(self, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate=True):
         """One Gauss-Seidel sweep on A^T y = b (the transpose of UpdateSGS), colour by colour; b, y and
@@ -371,55 +299,43 @@ class EulerEvaluator(Handle):
         fp32 = b.dtype == torch.float32
         if any((t.dtype == torch.float32) != fp32 for t in (y, yNew)):
             raise TypeError("UpdateSGST: b, y and yNew must share one precision")
-        capi.call("dndsb_eval_update_sgs_t", self.h, float(alphaDiag), _ptr(b, "b", fp32), _ptr(u, "u"), _ptr(y, "y", fp32),
-                  _ptr(yNew, "yNew", fp32), _ptr(jdiag, "jdiag"), int(forward), int(gsUpdate), int(fp32), _stream())
+        self._c.UpdateSGST(float(alphaDiag), b, u, y, yNew, jdiag, bool(forward), bool(gsUpdate), bool(fp32))
 
     def PressureForce(self, zone, direction, u, uRec, grad=False):
         """Pressure force along direction on boundary zone; with grad also (dJ/du, dJ/duRec) as device tensors."""
         d = np.ascontiguousarray(direction, dtype=np.float64)
-        J = np.zeros(1)
         gU = torch.empty_like(u) if grad else None
         gR = torch.empty_like(uRec) if grad else None
-        capi.call("dndsb_eval_pressure_force", self.h, int(zone), capi.dptr(d), _ptr(u, "u"), _ptr(uRec, "uRec"), capi.dptr(J),
-                  _ptr(gU, "dJdu") if grad else None, _ptr(gR, "dJduRec") if grad else None, _stream())
-        return (float(J[0]), gU, gR) if grad else float(J[0])
+        J = self._c.PressureForce(int(zone), d, u, uRec, gU, gR)
+        return (J, gU, gR) if grad else J
 
     def DoLimiterWBAP_C(self, u, uRec, si, uRecNew, smoothThreshold=0.01, WBAP_nStd=10.0, ifAll=False):
         """VariationalReconstruction_LimiterProcedure.hxx:188-334 with the characteristic projections of
         EulerSolver.hxx:466-505: the limited reconstruction into uRecNew (putIntoNew)."""
-        capi.call("dndsb_eval_limiter_wbap_c", self.h, _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(si, "si"), _ptr(uRecNew, "uRecNew"),
-                  float(smoothThreshold), float(WBAP_nStd), int(bool(ifAll)), _stream())
+        self._c.DoLimiterWBAP_C(u, uRec, si, uRecNew, float(smoothThreshold), float(WBAP_nStd), bool(ifAll))
 
     # positivity-preserving increment limiting (EulerSolver.hxx:696-738)
     def EvaluateCellRHSAlpha(self, u, res, alpha, refRho, refP, relax=0.9, compress=2, compressPower=1.0, ppEpsIsRelaxed=False, flag=0):
         """EulerEvaluator.hxx:1938-2062: alpha [nCell] (written in place) so that u + alpha res keeps the
         relaxed density and pressure floors; returns (nLim, alphaMin).  refRho, refP: far-field density
         and pressure (refUPrim); flag 1 = MIN_IF_NOT_ONE, 2 = MIN_ALL."""
-        n, amin = ctypes.c_int64(), ctypes.c_double()
-        capi.call("dndsb_eval_cell_rhs_alpha", self.h, _ptr(u, "u"), _ptr(res, "res"), _ptr(alpha, "alpha"), float(refRho), float(refP),
-                  float(relax), int(compress), float(compressPower), int(bool(ppEpsIsRelaxed)), int(flag), ctypes.addressof(n),
-                  ctypes.addressof(amin), _stream())
-        return int(n.value), float(amin.value)
+        n, amin = self._c.EvaluateCellRHSAlpha(u, res, alpha, float(refRho), float(refP), float(relax), int(compress), float(compressPower),
+                                               bool(ppEpsIsRelaxed), int(flag))
+        return int(n), float(amin)
 
     def EvaluateCellRHSAlphaExpansion(self, u, res, alpha, refRho, refP, alphaMin):
         """EulerEvaluator.hxx:2064-2140: alpha = alphaMin where u + res leaves the floors."""
-        capi.call("dndsb_eval_cell_rhs_alpha_expansion", self.h, _ptr(u, "u"), _ptr(res, "res"), _ptr(alpha, "alpha"), float(refRho),
-                  float(refP), float(alphaMin), _stream())
+        self._c.EvaluateCellRHSAlphaExpansion(u, res, alpha, float(refRho), float(refP), float(alphaMin))
 
     def AddFixedIncrement(self, u, inc, alpha, refRho, refP, ppEpsIsRelaxed=False):
         """EulerEvaluator.hpp:1795-1857: u += CompressInc(u, alpha inc) in place; returns the smallest
         density-increment ratio the compression applied."""
-        amin = ctypes.c_double()
-        capi.call("dndsb_eval_add_fixed_increment", self.h, _ptr(u, "u"), _ptr(inc, "inc"), float(alpha), float(refRho), float(refP),
-                  int(bool(ppEpsIsRelaxed)), ctypes.addressof(amin), _stream())
-        return float(amin.value)
+        return float(self._c.AddFixedIncrement(u, inc, float(alpha), float(refRho), float(refP), bool(ppEpsIsRelaxed)))
 
     def PressureForceCoords(self, zone, direction, u, uRec):
         """Derivative of PressureForce with respect to the node coordinates [nNode][3] (u, uRec held fixed)."""
-        d = np.ascontiguousarray(direction, dtype=np.float64)
         dX = torch.empty((self.vr.mesh.n_node, 3), dtype=torch.float64, device="cuda")
-        capi.call("dndsb_eval_pressure_force_coords", self.h, int(zone), capi.dptr(d), _ptr(u, "u"), _ptr(uRec, "uRec"), _ptr(dX, "dJdX"),
-                  _stream())
+        self._c.PressureForceCoords(int(zone), np.ascontiguousarray(direction, dtype=np.float64), u, uRec, dX)
         return dX
 
     def SolveLinear(self, alphaDiag, dTau, dt, u, rhs, xInc, gmresCode=0, jacobiCode=1, sgsIter=0, nGmresSpace=5, nGmresIter=1,
@@ -427,27 +343,16 @@ class EulerEvaluator(Handle):
         """EulerSolver::solveLinear with LUSGSMatrixInit (EulerSolver.hxx:1407-1579, EulerEvaluator.hxx:37-159):
         xInc = M^-1 rhs by LU-SGS pairs (gmresCode 0), GMRES preconditioned by SGS pairs (1), or both (2),
         in FP64 or FP32; all on the device, no host synchronisation."""
-        ls = capi.LinearSettings()
-        ls.gmresCode, ls.jacobiCode, ls.sgsIter = int(gmresCode), int(jacobiCode), int(sgsIter)
-        ls.nGmresSpace, ls.nGmresIter = int(nGmresSpace), int(nGmresIter)
-        ls.precision = 1 if precision == "fp32" else 0
-        ls.useGraph = int(bool(useGraph))
-        for i, x in enumerate(meanScale if meanScale is not None else []):
-            ls.meanScale[i] = float(x)
-        capi.call("dndsb_eval_solve_linear", self.h, ctypes.byref(ls), float(alphaDiag), _ptr(dTau, "dTau"), float(dt), _ptr(u, "u"),
-                  _ptr(rhs, "rhs"), _ptr(xInc, "xInc"), _stream())
+        ls = dict(gmresCode=int(gmresCode), jacobiCode=int(jacobiCode), sgsIter=int(sgsIter), nGmresSpace=int(nGmresSpace),
+                  nGmresIter=int(nGmresIter), precision=1 if precision == "fp32" else 0, useGraph=int(bool(useGraph)),
+                  meanScale=[float(x) for x in (meanScale if meanScale is not None else [])])
+        self._c.SolveLinear(ls, float(alphaDiag), dTau, float(dt), u, rhs, xInc)
 
     def EvaluateNorm(self, x, P=1, volWise=True):
-        out = np.zeros(self.nVars)
-        capi.call("dndsb_eval_evaluate_norm", self.h, _ptr(x, "x"), int(P), int(volWise), capi.dptr(out), _stream())
-        return out
+        return self._c.EvaluateNorm(x, int(P), bool(volWise))
 
     def get(self, name):
-        n = ctypes.c_int64()
-        capi.call("dndsb_eval_get_array", self.h, name.encode(), None, 0, ctypes.byref(n))
-        out = np.zeros(n.value)
-        capi.call("dndsb_eval_get_array", self.h, name.encode(), capi.dptr(out), n.value, ctypes.byref(n))
-        return out
+        return self._c.get(name)
 
     def SetDeltaLambda(self, dl):
-        capi.call("dndsb_eval_set_delta_lambda", self.h, _ptr(dl, "deltaLambdaCell"), _stream())
+        self._c.SetDeltaLambda(dl)
