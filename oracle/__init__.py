@@ -15,7 +15,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_CNT_PATH = os.path.join(_HERE, "liboracle_opcount.so")
 _lib = None
+_cnt = None
 
 
 def build():
@@ -24,15 +26,30 @@ def build():
     subprocess.check_call(["make", "-s", "-f", os.path.join("oracle", "Makefile")], cwd=root)
 
 
+def _load(path):
+    src = os.path.join(_HERE, "oracle.cpp")
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        build()
+    L = ctypes.CDLL(path)
+    _declare(L)
+    return L
+
+
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(_HERE, "oracle.cpp")
-        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
-            build()
-        _lib = ctypes.CDLL(_LIB_PATH)
-        _declare(_lib)
+        _lib = _load(_LIB_PATH)
     return _lib
+
+
+def opcount_lib():
+    """The op-counting build (oracle/opcount.hpp): same entry points, every floating-point operation counted."""
+    global _cnt
+    if _cnt is None:
+        _cnt = _load(_CNT_PATH)
+        _cnt.orc_opcount_reset.argtypes = []
+        _cnt.orc_opcount_get.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+    return _cnt
 
 
 class VRSettings(ctypes.Structure):
@@ -66,7 +83,24 @@ _I = ctypes.POINTER(ctypes.c_int)
 _V = ctypes.c_void_p
 
 
+def _optional_decls():
+    # entry points of the limiter and positivity restatements (the op-counting build leaves them out)
+    return {
+        "orc_smooth_indicator": [_V, _D, _D, _D],
+        "orc_limiter_wbap_c": [_V, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double],
+        "orc_cell_rhs_alpha": [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_long), _D],
+        "orc_cell_rhs_alpha_expansion": [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double],
+        "orc_add_fixed_increment": [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, _D],
+    }
+
+
 def _declare(L):
+    for name, args in _optional_decls().items():  # absent from the op-counting build
+        if hasattr(L, name):
+            getattr(L, name).argtypes = args
     L.orc_create.restype = _V
     L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, _D, ctypes.c_long, ctypes.c_int, _L, _D,
                              ctypes.c_long, ctypes.c_int, _L, _D, _L, _I, _D, ctypes.c_int, _L,
@@ -93,15 +127,6 @@ def _declare(L):
     L.orc_update_sgs_t.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int]
     L.orc_pressure_force.argtypes = [_V, ctypes.c_int, _D, _D, _D, _D, _D]
     L.orc_pressure_force.restype = ctypes.c_double
-    L.orc_smooth_indicator.argtypes = [_V, _D, _D, _D]
-    L.orc_limiter_wbap_c.argtypes = [_V, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double]
-    L.orc_cell_rhs_alpha.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
-                                     ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
-                                     ctypes.POINTER(ctypes.c_long), _D]
-    L.orc_cell_rhs_alpha_expansion.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double,
-                                               ctypes.c_double, ctypes.c_double]
-    L.orc_add_fixed_increment.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
-                                          ctypes.c_double, ctypes.c_int, _D]
     L.orc_riemann.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                               ctypes.c_double, _D, _D]
     L.orc_viscous_flux.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -173,9 +198,11 @@ def viscous_flux(U, gradU, n, gamma, mu, k, Cp, adiabatic=False):
 class Oracle:
     """One mesh + VR + evaluator instance of the CPU restatement."""
 
-    def __init__(self, mesh, vr: dict, euler: dict):
+    def __init__(self, mesh, vr: dict, euler: dict, opcount=False):
+        """opcount: run on the op-counting build (oracle/opcount.hpp), single-threaded; see op_counts()."""
         self.mesh = mesh
-        L = lib()
+        L = opcount_lib() if opcount else lib()
+        self.L = L
         a = mesh.arrays()
         self._keep = a
         vs = VRSettings()
@@ -201,26 +228,35 @@ class Oracle:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().orc_destroy(self.h)
+            self.L.orc_destroy(self.h)
             self.h = None
+
+    def op_counts(self, reset=False):
+        """Operations counted by the op-counting build since the last reset:
+        dict(add, mul, div, sqrt, fn) (fn: exp / pow / log / trigonometric calls)."""
+        out = np.zeros(5, dtype=np.uint64)
+        self.L.orc_opcount_get(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+        if reset:
+            self.L.orc_opcount_reset()
+        return dict(zip(("add", "mul", "div", "sqrt", "fn"), [int(x) for x in out]))
 
     def construct(self, bc_dir_weight=None):
         if bc_dir_weight is None:
-            bad = lib().orc_construct(self.h, None, 0)
+            bad = self.L.orc_construct(self.h, None, 0)
         else:
             w = _f64(bc_dir_weight)
-            bad = lib().orc_construct(self.h, _p(w), w.shape[0])
+            bad = self.L.orc_construct(self.h, _p(w), w.shape[0])
         out = np.zeros(4, dtype=np.int64)
-        lib().orc_sizes(self.h, _p(out, _L))
+        self.L.orc_sizes(self.h, _p(out, _L))
         self.NDOF, self.R, self.nGf, self.nGc = [int(x) for x in out]
         return bad
 
     def get(self, name):
-        n = lib().orc_get(self.h, name.encode(), None)
+        n = self.L.orc_get(self.h, name.encode(), None)
         if n < 0:
             raise KeyError(name)
         out = np.zeros(n)
-        lib().orc_get(self.h, name.encode(), _p(out))
+        self.L.orc_get(self.h, name.encode(), _p(out))
         return out
 
     def set_bc(self, types, values):
@@ -229,41 +265,41 @@ class Oracle:
         t = np.ascontiguousarray(types, dtype=np.int32)
         v = np.ascontiguousarray(values, dtype=np.float64).reshape(len(t), self.nv)
         self._bc = (t, v)
-        lib().orc_set_bc(self.h, len(t), t.ctypes.data_as(_I), _p(v), self.nv)
+        self.L.orc_set_bc(self.h, len(t), t.ctypes.data_as(_I), _p(v), self.nv)
 
     def set_wall_distance(self, d):
         """Wall distance at every cell Gauss point, [nCell][nGc] (the SA model's dWall)."""
         d = np.ascontiguousarray(d, dtype=np.float64)
         self._dwall = d
-        lib().orc_set_wall_dist(self.h, _p(d))
+        self.L.orc_set_wall_dist(self.h, _p(d))
 
     def init_field(self, kind, chi=5.0):
         u = np.zeros((self.mesh.n_cell, self.nv))
-        lib().orc_init_field(self.h, kind, chi, _p(u))
+        self.L.orc_init_field(self.h, kind, chi, _p(u))
         return u
 
     def vr_iter(self, uRec, u, recordInc=False, uRecIsZero=False):
         uRec, u = _f64(uRec), _f64(u)
         out = np.zeros_like(uRec)
-        lib().orc_vr_iter(self.h, _p(uRec), _p(out), _p(u), int(recordInc), int(uRecIsZero))
+        self.L.orc_vr_iter(self.h, _p(uRec), _p(out), _p(u), int(recordInc), int(uRecIsZero))
         return out
 
     def eval_dt(self, u, CFL, MaxDt=1e100, useLocalDt=True):
         u = _f64(u)
         dt = np.zeros(self.mesh.n_cell)
         mn = np.zeros(1)
-        lib().orc_eval_dt(self.h, _p(u), CFL, MaxDt, int(useLocalDt), _p(dt), _p(mn))
+        self.L.orc_eval_dt(self.h, _p(u), CFL, MaxDt, int(useLocalDt), _p(dt), _p(mn))
         return dt, float(mn[0])
 
     def set_delta_lambda(self, dl):
         dl = _f64(dl)
-        lib().orc_set_delta_lambda(self.h, _p(dl))
+        self.L.orc_set_delta_lambda(self.h, _p(dl))
 
     def eval_rhs(self, u, uRec, want_face_flux=False):
         u, uRec = _f64(u), _f64(uRec)
         rhs = np.zeros_like(u)
         ff = np.zeros((self.mesh.n_face, self.nv)) if want_face_flux else None
-        lib().orc_eval_rhs(self.h, _p(u), _p(uRec), _p(rhs), _p(ff) if ff is not None else None)
+        self.L.orc_eval_rhs(self.h, _p(u), _p(uRec), _p(rhs), _p(ff) if ff is not None else None)
         return (rhs, ff) if want_face_flux else rhs
 
     def eval_rhs_full(self, u, uRecUnlim, uRec, alpha=None):
@@ -274,20 +310,20 @@ class Oracle:
         js = np.zeros_like(u)
         fw = np.zeros(self.nv)
         a = _f64(alpha) if alpha is not None else None
-        lib().orc_eval_rhs_full(self.h, _p(u), _p(uU), _p(uR), _p(a) if a is not None else None, _p(rhs), _p(js), _p(fw))
+        self.L.orc_eval_rhs_full(self.h, _p(u), _p(uU), _p(uR), _p(a) if a is not None else None, _p(rhs), _p(js), _p(fw))
         return rhs, js, fw
 
     def lusgs_init(self, dTau, dt, alphaDiag):
         dTau = _f64(dTau)
         jd = np.zeros(self.mesh.n_cell * (self.nv if self.nv >= 6 else 1))
-        lib().orc_lusgs_init(self.h, _p(dTau), dt, alphaDiag, _p(jd))
+        self.L.orc_lusgs_init(self.h, _p(dTau), dt, alphaDiag, _p(jd))
         return jd if self.nv < 6 else jd.reshape(self.mesh.n_cell, self.nv)
 
     def update_sgs(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False):
         rhs, u, uInc, jdiag = _f64(rhs), _f64(u), _f64(uInc), _f64(jdiag)
         out = np.array(uIncNew, dtype=np.float64, copy=True, order="C")
         s = np.zeros(self.nv)
-        lib().orc_update_sgs(self.h, alphaDiag, _p(rhs), _p(u), _p(uInc), _p(out), _p(jdiag), int(forward), int(gsUpdate),
+        self.L.orc_update_sgs(self.h, alphaDiag, _p(rhs), _p(u), _p(uInc), _p(out), _p(jdiag), int(forward), int(gsUpdate),
                              int(uIncIsZero), _p(s))
         return out, s
 
@@ -297,27 +333,27 @@ class Oracle:
         rhs, u, jdiag = _f64(rhs), _f64(u), _f64(jdiag)
         out = np.array(uIncNew, dtype=np.float64, copy=True, order="C")
         src = out if inplace else _f64(uInc)
-        lib().orc_update_lusgs(self.h, alphaDiag, _p(rhs), _p(u), _p(src), _p(out), _p(jdiag), int(forward))
+        self.L.orc_update_lusgs(self.h, alphaDiag, _p(rhs), _p(u), _p(src), _p(out), _p(jdiag), int(forward))
         return out
 
     def lusgs_matvec(self, alphaDiag, u, uInc, jdiag):
         u, uInc, jdiag = _f64(u), _f64(uInc), _f64(jdiag)
         out = np.zeros_like(uInc)
-        lib().orc_lusgs_matvec(self.h, alphaDiag, _p(u), _p(uInc), _p(jdiag), _p(out))
+        self.L.orc_lusgs_matvec(self.h, alphaDiag, _p(u), _p(uInc), _p(jdiag), _p(out))
         return out
 
     def lusgs_matvec_t(self, alphaDiag, u, y, jdiag):
         """Transpose of lusgs_matvec applied to y."""
         u, y, jdiag = _f64(u), _f64(y), _f64(jdiag)
         out = np.zeros_like(y)
-        lib().orc_lusgs_matvec_t(self.h, alphaDiag, _p(u), _p(y), _p(jdiag), _p(out))
+        self.L.orc_lusgs_matvec_t(self.h, alphaDiag, _p(u), _p(y), _p(jdiag), _p(out))
         return out
 
     def update_sgs_t(self, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate=True):
         """One Gauss-Seidel sweep on the transposed LU-SGS system, natural cell order."""
         b, u, y, jdiag = _f64(b), _f64(u), _f64(y), _f64(jdiag)
         out = np.array(yNew, dtype=np.float64, copy=True, order="C")
-        lib().orc_update_sgs_t(self.h, alphaDiag, _p(b), _p(u), _p(y), _p(out), _p(jdiag), int(forward), int(gsUpdate))
+        self.L.orc_update_sgs_t(self.h, alphaDiag, _p(b), _p(u), _p(y), _p(out), _p(jdiag), int(forward), int(gsUpdate))
         return out
 
     def pressure_force(self, zone, direction, u, uRec, grad=False):
@@ -326,31 +362,31 @@ class Oracle:
         d = _f64(np.asarray(direction, dtype=np.float64))
         gU = np.zeros_like(u) if grad else None
         gR = np.zeros_like(uRec) if grad else None
-        J = lib().orc_pressure_force(self.h, int(zone), _p(d), _p(u), _p(uRec), _p(gU) if grad else None, _p(gR) if grad else None)
+        J = self.L.orc_pressure_force(self.h, int(zone), _p(d), _p(u), _p(uRec), _p(gU) if grad else None, _p(gR) if grad else None)
         return (J, gU, gR) if grad else J
 
     def smooth_indicator(self, u, uRec):
         """DoCalculateSmoothIndicator (procedure 0, density and energy), one value per cell."""
         u, uRec = _f64(u), _f64(uRec)
         si = np.zeros(self.mesh.n_cell)
-        lib().orc_smooth_indicator(self.h, _p(u), _p(uRec), _p(si))
+        self.L.orc_smooth_indicator(self.h, _p(u), _p(uRec), _p(si))
         return si
 
     def limiter_wbap_c(self, u, uRec, si, smoothThreshold=0.01, WBAP_nStd=10.0, ifAll=False, gamma=1.4):
         """DoLimiterWBAP_C (WBAP-L2 biway and multiway, characteristic variables): the limited uRec."""
         u, uRec, si = _f64(u), _f64(uRec), _f64(si)
         out = np.zeros_like(uRec)
-        bad = lib().orc_limiter_wbap_c(self.h, _p(u), _p(uRec), _p(si), _p(out), smoothThreshold, WBAP_nStd, int(ifAll), gamma)
+        bad = self.L.orc_limiter_wbap_c(self.h, _p(u), _p(uRec), _p(si), _p(out), smoothThreshold, WBAP_nStd, int(ifAll), gamma)
         assert bad == 0, "singular derivative basis at a face centre"
         return out
 
     def cell_point_values(self, u, uRec):
         u, uRec = _f64(u), _f64(uRec)
         out = np.zeros((self.mesh.n_cell, self.nGc, self.nv))
-        lib().orc_cell_point_values(self.h, _p(u), _p(uRec), _p(out))
+        self.L.orc_cell_point_values(self.h, _p(u), _p(uRec), _p(out))
         return out
 
     def cell_quad_weights(self):
         w = np.zeros(self.nGc)
-        lib().orc_cell_quad_weights(self.h, _p(w))
+        self.L.orc_cell_quad_weights(self.h, _p(w))
         return w

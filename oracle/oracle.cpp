@@ -21,9 +21,31 @@
 #include <string>
 #include <vector>
 
+#ifdef ORC_OPCOUNT
+#include "opcount.hpp"
+#endif
+
 namespace orc
 {
+#ifdef ORC_OPCOUNT
+using real = orc_cnt::R; // the op-counting build (oracle/opcount.hpp)
+#else
 using real = double;
+#endif
+// unqualified math calls: the std overloads for double, the counting ones (found by argument-dependent
+// lookup) in the op-counting build
+using std::abs;
+using std::cos;
+using std::exp;
+using std::floor;
+using std::log;
+using std::max;
+using std::min;
+using std::pow;
+using std::round;
+using std::sin;
+using std::sqrt;
+using std::tanh;
 constexpr real verySmallReal = 1e-200; // DNDS/Defines.hpp:199
 constexpr real smallReal = 1e-10;      // DNDS/Defines.hpp:201
 constexpr real veryLargeReal = 3e200;  // DNDS/Defines.hpp:195
@@ -303,7 +325,7 @@ static void cross(const real a[3], const real b[3], real c[3])
     c[1] = a[2] * b[0] - a[0] * b[2];
     c[2] = a[0] * b[1] - a[1] * b[0];
 }
-static real norm3(const real a[3]) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+static real norm3(const real a[3]) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
 static real dot3(const real a[3], const real b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 // Geom/Quadrature.hpp:480-490
@@ -413,15 +435,15 @@ static RoePre roePreamble(const real *ULm, const real *URm, real gamma)
     r.vsqrRm = dot3(r.veloRm, r.veloRm);
     idealGasThermal(ULm[4], ULm[0], r.vsqrLm, gamma, r.pLm, r.asqrLm, r.HLm);
     idealGasThermal(URm[4], URm[0], r.vsqrRm, gamma, r.pRm, r.asqrRm, r.HRm);
-    r.sqrtRhoLm = std::sqrt(ULm[0]);
-    r.sqrtRhoRm = std::sqrt(URm[0]);
+    r.sqrtRhoLm = sqrt(ULm[0]);
+    r.sqrtRhoRm = sqrt(URm[0]);
     for (int d = 0; d < 3; d++)
         r.veloRoe[d] = (r.sqrtRhoLm * r.veloLm[d] + r.sqrtRhoRm * r.veloRm[d]) / (r.sqrtRhoLm + r.sqrtRhoRm);
     r.vsqrRoe = dot3(r.veloRoe, r.veloRoe);
     r.HRoe = (r.sqrtRhoLm * r.HLm + r.sqrtRhoRm * r.HRm) / (r.sqrtRhoLm + r.sqrtRhoRm);
     r.asqrRoe = (gamma - 1) * (r.HRoe - 0.5 * r.vsqrRoe);
     r.rhoRoe = r.sqrtRhoLm * r.sqrtRhoRm;
-    r.aRoe = std::sqrt(r.asqrRoe);
+    r.aRoe = sqrt(r.asqrRoe);
     return r;
 }
 
@@ -448,7 +470,7 @@ static void roeEntropyFix(int eigScheme, real aL, real aR, real aAve, real uL, r
     {
         auto Flim = [=](real v, real lam, real lamL, real lamR)
         {
-            const real thresH = std::max({0., lam - lamL, lamR - lam}) * scaleHartenYee;
+            const real thresH = max({real(0.), lam - lamL, lamR - lam}) * scaleHartenYee;
             if (v < thresH)
                 return (sqr(v) / thresH + thresH) * 0.5;
             return v;
@@ -460,54 +482,54 @@ static void roeEntropyFix(int eigScheme, real aL, real aR, real aAve, real uL, r
     else if (eigScheme == 1)
     {
         const real aLm = aL * incFScaleA, aRm = aR * incFScaleA;
-        const real uLm = signTol(uL, aLm * smallReal) * std::max(std::abs(uL) * incFScale, aLm * scaleLD);
-        const real uRm = signTol(uR, aRm * smallReal) * std::max(std::abs(uR) * incFScale, aRm * scaleLD);
-        lam0 = std::max(std::abs(uLm - aLm), std::abs(uRm - aRm));
-        lam123 = std::max(std::abs(uLm), std::abs(uRm));
-        lam4 = std::max(std::abs(uLm + aLm), std::abs(uRm + aRm));
+        const real uLm = signTol(uL, aLm * smallReal) * max(abs(uL) * incFScale, aLm * scaleLD);
+        const real uRm = signTol(uR, aRm * smallReal) * max(abs(uR) * incFScale, aRm * scaleLD);
+        lam0 = max(abs(uLm - aLm), abs(uRm - aRm));
+        lam123 = max(abs(uLm), abs(uRm));
+        lam4 = max(abs(uLm + aLm), abs(uRm + aRm));
     }
     else if (eigScheme == 3)
     {
-        const real LDthreshold = std::abs(uAve) / scaleLD;
-        const real aRoeStar = std::min(LDthreshold, aAve * incFScaleA);
-        lam0 = std::abs(uAve * incFScale - aRoeStar);
-        lam4 = std::abs(uAve * incFScale + aRoeStar);
+        const real LDthreshold = abs(uAve) / scaleLD;
+        const real aRoeStar = min(LDthreshold, aAve * incFScaleA);
+        lam0 = abs(uAve * incFScale - aRoeStar);
+        lam4 = abs(uAve * incFScale + aRoeStar);
     }
     else if (eigScheme == 4)
     {
-        const real uStar = signTol(uAve, aAve * smallReal) * std::max(aAve * scaleLD, std::abs(uAve) * incFScale);
-        lam0 = std::abs(uStar - aAve * incFScaleA);
-        lam123 = std::abs(uStar);
-        lam4 = std::abs(uStar + aAve * incFScaleA);
+        const real uStar = signTol(uAve, aAve * smallReal) * max(aAve * scaleLD, abs(uAve) * incFScale);
+        lam0 = abs(uStar - aAve * incFScaleA);
+        lam123 = abs(uStar);
+        lam4 = abs(uStar + aAve * incFScaleA);
     }
     else if (eigScheme == 5)
     {
         const real vL = uL * incFScale, vR = uR * incFScale;
-        const real aLm = std::min(aL * incFScaleA, std::abs(vL) / scaleLD);
-        const real aRm = std::min(aR * incFScaleA, std::abs(vR) / scaleLD);
-        lam0 = std::max(std::abs(vL - aLm), std::abs(vR - aRm));
-        lam123 = std::max(std::abs(vL), std::abs(vR));
-        lam4 = std::max(std::abs(vL + aLm), std::abs(vR + aRm));
+        const real aLm = min(aL * incFScaleA, abs(vL) / scaleLD);
+        const real aRm = min(aR * incFScaleA, abs(vR) / scaleLD);
+        lam0 = max(abs(vL - aLm), abs(vR - aRm));
+        lam123 = max(abs(vL), abs(vR));
+        lam4 = max(abs(vL + aLm), abs(vR + aRm));
     }
     else if (eigScheme == 6)
     {
-        lam0 = std::max(std::abs(uAve * incFScale - aAve * incFScaleA), dLambda * scaleHFix);
-        lam4 = std::max(std::abs(uAve * incFScale + aAve * incFScaleA), dLambda * scaleHFix);
-        lam123 = std::max(std::abs(uAve * incFScale), dLambda * scaleHFix);
+        lam0 = max(abs(uAve * incFScale - aAve * incFScaleA), dLambda * scaleHFix);
+        lam4 = max(abs(uAve * incFScale + aAve * incFScaleA), dLambda * scaleHFix);
+        lam123 = max(abs(uAve * incFScale), dLambda * scaleHFix);
     }
     else if (eigScheme == 7 || eigScheme == 8)
     {
         if (eigScheme == 7)
         {
-            lam0 *= std::abs(uAve * incFScale - aAve * incFScaleA);
-            lam4 *= std::abs(uAve * incFScale + aAve * incFScaleA);
-            lam123 *= std::abs(uAve * incFScale);
+            lam0 *= abs(uAve * incFScale - aAve * incFScaleA);
+            lam4 *= abs(uAve * incFScale + aAve * incFScaleA);
+            lam123 *= abs(uAve * incFScale);
         }
         else
         {
-            lam0 = std::max(std::abs(uAve * incFScale - aAve * incFScaleA), dLambda * scaleHFix);
-            lam4 = std::max(std::abs(uAve * incFScale + aAve * incFScaleA), dLambda * scaleHFix);
-            lam123 = std::max(std::abs(uAve * incFScale), dLambda * scaleHFix);
+            lam0 = max(abs(uAve * incFScale - aAve * incFScaleA), dLambda * scaleHFix);
+            lam4 = max(abs(uAve * incFScale + aAve * incFScaleA), dLambda * scaleHFix);
+            lam123 = max(abs(uAve * incFScale), dLambda * scaleHFix);
         }
         const real th = scaleHartenYee * (VAve + aAve), thS = sqr(th);
         if (lam0 < th)
@@ -539,21 +561,21 @@ static void roeFlux(int eigScheme, const real *UL, const real *UR, const real *U
     inviscidFluxXY(UR, veloR, vg, n, pR, FR);
     real veloRoeN = dot3(rp.veloRoe, nE), vgN = dot3(vg, nE);
     real veloRoe0 = veloRoeN - vgN;
-    lam0 = std::abs(veloRoe0 - rp.aRoe);
-    lam123 = std::abs(veloRoe0);
-    lam4 = std::abs(veloRoe0 + rp.aRoe);
+    lam0 = abs(veloRoe0 - rp.aRoe);
+    lam123 = abs(veloRoe0);
+    lam4 = abs(veloRoe0 + rp.aRoe);
     real dvL[3], dvR[3], dvRoe[3];
     for (int d = 0; d < 3; d++)
         dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d], dvRoe[d] = rp.veloRoe[d] - vg[d];
     real veloLm0 = dot3(dvL, nE), veloRm0 = dot3(dvR, nE);
     if (eigScheme == 2)
     {
-        lam0 = lam123 = lam4 = std::max(std::abs(veloLm0) + std::sqrt(rp.asqrLm), std::abs(veloRm0) + std::sqrt(rp.asqrRm));
+        lam0 = lam123 = lam4 = max(abs(veloLm0) + sqrt(rp.asqrLm), abs(veloRm0) + sqrt(rp.asqrRm));
         for (int i = 0; i < 5; i++)
             F[i] = (FL[i] + FR[i]) * 0.5 - 0.5 * lam0 * (UR[i] - UL[i]);
         return;
     }
-    roeEntropyFix(eigScheme, std::sqrt(rp.asqrLm), std::sqrt(rp.asqrRm), rp.aRoe, veloLm0, veloRm0, veloRoe0,
+    roeEntropyFix(eigScheme, sqrt(rp.asqrLm), sqrt(rp.asqrRm), rp.aRoe, veloLm0, veloRm0, veloRoe0,
                   norm3(dvL), norm3(dvR), norm3(dvRoe), dLambda, fixScale, incFScale, lam0, lam123, lam4);
     real incU[5];
     for (int i = 0; i < 5; i++)
@@ -600,9 +622,9 @@ static void hllepFlux(int type, const real *UL, const real *UR, const real *ULm,
     inviscidFluxXY(UR, veloR, vg, n, pR, FR);
     real veloRoeN = dot3(rp.veloRoe, n), vgN = dot3(vg, n);
     real veloRoe0 = veloRoeN - vgN;
-    lam0 = std::abs(veloRoe0 - rp.aRoe);
-    lam123 = std::abs(veloRoe0);
-    lam4 = std::abs(veloRoe0 + rp.aRoe);
+    lam0 = abs(veloRoe0 - rp.aRoe);
+    lam123 = abs(veloRoe0);
+    lam4 = abs(veloRoe0 + rp.aRoe);
     real dvL[3], dvR[3];
     for (int d = 0; d < 3; d++)
         dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d];
@@ -622,11 +644,11 @@ static void hllepFlux(int type, const real *UL, const real *UR, const real *ULm,
     real alpha1 = (gamma - 1) / rp.asqrRoe * (incU[0] * (rp.HRoe - veloRoeN * veloRoeN) + veloRoeN * incU123N - incU4b);
     real alpha0 = (incU[0] * (veloRoeN + rp.aRoe) - incU123N - rp.aRoe * alpha1) / (2 * rp.aRoe);
     real alpha4 = incU[0] - (alpha0 + alpha1);
-    real SL = std::min(veloRoe0 - rp.aRoe, veloLm0 - std::sqrt(asqrL));
-    real SR = std::max(veloRoe0 + rp.aRoe, veloRm0 + std::sqrt(asqrR));
-    real UU = std::abs(veloRoe0);
-    real dfix = rp.aRoe / (rp.aRoe + std::max(UU, dLambda * fixScale));
-    real SP = std::max(SR, 0.0), SM = std::min(SL, 0.0);
+    real SL = min(veloRoe0 - rp.aRoe, veloLm0 - sqrt(asqrL));
+    real SR = max(veloRoe0 + rp.aRoe, veloRm0 + sqrt(asqrR));
+    real UU = abs(veloRoe0);
+    real dfix = rp.aRoe / (rp.aRoe + max(UU, dLambda * fixScale));
+    real SP = max(SR, 0.0), SM = min(SL, 0.0);
     if (type != 1)
     {
         real ReV1[5] = {1, rp.veloRoe[0], rp.veloRoe[1], rp.veloRoe[2], rp.vsqrRoe * 0.5};
@@ -641,7 +663,7 @@ static void hllepFlux(int type, const real *UL, const real *UR, const real *ULm,
         lam123 = ((SP + SM) * (veloRoe0)-2.0 * (1.0 - delta1) * (SP * SM)) / (SP - SM);
         lam4 = ((SP + SM) * (veloRoe0 + rp.aRoe) - 2.0 * (1.0 - delta2) * (SP * SM)) / (SP - SM);
         lam0 = ((SP + SM) * (veloRoe0 - rp.aRoe) - 2.0 * (1.0 - delta3) * (SP * SM)) / (SP - SM);
-        lam123 = std::abs(lam123), lam0 = std::abs(lam0), lam4 = std::abs(lam4);
+        lam123 = abs(lam123), lam0 = abs(lam0), lam4 = abs(lam4);
         alpha0 *= lam0;
         alpha1 *= lam123;
         for (int d = 0; d < 3; d++)
@@ -673,24 +695,24 @@ static void hllcFlux(const real *UL, const real *UR, const real *ULm, const real
     inviscidFluxXY(UR, veloR, vg, n, pR, FR);
     real veloRoeN = dot3(rp.veloRoe, n), vgN = dot3(vg, n);
     real veloRoe0 = veloRoeN - vgN;
-    lam0 = std::abs(veloRoe0 - rp.aRoe);
-    lam123 = std::abs(veloRoe0);
-    lam4 = std::abs(veloRoe0 + rp.aRoe);
+    lam0 = abs(veloRoe0 - rp.aRoe);
+    lam123 = abs(veloRoe0);
+    lam4 = abs(veloRoe0 + rp.aRoe);
     real dvL[3], dvR[3];
     for (int d = 0; d < 3; d++)
         dvL[d] = rp.veloLm[d] - vg[d], dvR[d] = rp.veloRm[d] - vg[d];
     real veloLm0 = dot3(dvL, n), veloRm0 = dot3(dvR, n);
     auto HLLCq = [&](real p, real pS)
     {
-        real q = std::sqrt(1 + (gamma + 1) / 2 / gamma * (pS / p - 1));
+        real q = sqrt(1 + (gamma + 1) / 2 / gamma * (pS / p - 1));
         if (pS <= p)
             q = 1;
         return q;
     };
     real pS = 0.5 * (rp.pLm + rp.pRm) - 0.5 * (veloLm0 - veloRm0) * rp.rhoRoe * rp.aRoe;
-    pS = std::max(0.0, pS);
-    real SL = veloLm0 - std::sqrt(rp.asqrLm) * HLLCq(rp.pLm, pS);
-    real SR = veloRm0 + std::sqrt(rp.asqrRm) * HLLCq(rp.pRm, pS);
+    pS = max(0.0, pS);
+    real SL = veloLm0 - sqrt(rp.asqrLm) * HLLCq(rp.pLm, pS);
+    real SR = veloRm0 + sqrt(rp.asqrRm) * HLLCq(rp.pRm, pS);
     (void)dLambda;
     if (0 <= SL)
     {
@@ -705,13 +727,13 @@ static void hllcFlux(const real *UL, const real *UR, const real *ULm, const real
     real SS = 0;
     real div = (UL[0] * (SL - veloLm0) - UR[0] * (SR - veloRm0));
     real ULn = UL[1] * n[0] + UL[2] * n[1] + UL[3] * n[2], URn = UR[1] * n[0] + UR[2] * n[1] + UR[3] * n[2];
-    if (std::abs(div) > verySmallReal)
+    if (abs(div) > verySmallReal)
         SS = (pR - pL + (ULn - vgN * UL[0]) * (SL - veloLm0) - (URn - vgN * UR[0]) * (SR - veloRm0)) / div;
     real DS[5] = {0, n[0], n[1], n[2], SS};
     if (SS >= 0)
     {
         real dv = SL - SS;
-        if (std::abs(dv) < verySmallReal)
+        if (abs(dv) < verySmallReal)
             std::copy(FL, FL + 5, F);
         else
             for (int i = 0; i < 5; i++)
@@ -720,7 +742,7 @@ static void hllcFlux(const real *UL, const real *UR, const real *ULm, const real
     else
     {
         real dv = SR - SS;
-        if (std::abs(dv) < verySmallReal)
+        if (abs(dv) < verySmallReal)
             std::copy(FR, FR + 5, F);
         else
             for (int i = 0; i < 5; i++)
@@ -939,7 +961,7 @@ struct Oracle
         for (int a = 0; a < n; a++)
             for (int b = 0; b < n; b++)
                 I[a][b] /= vol[c], nrm += I[a][b] * I[a][b];
-        nrm = std::sqrt(nrm);
+        nrm = sqrt(nrm);
         real V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
         real A[3][3];
         std::memcpy(A, I, sizeof(A));
@@ -957,8 +979,8 @@ struct Oracle
                     if (A[a][b] == 0)
                         continue;
                     real th = (A[b][b] - A[a][a]) / (2 * A[a][b]);
-                    real t = (th >= 0 ? 1.0 : -1.0) / (std::abs(th) + std::sqrt(th * th + 1));
-                    real cs = 1 / std::sqrt(t * t + 1), sn = t * cs;
+                    real t = (th >= 0 ? 1.0 : -1.0) / (abs(th) + sqrt(th * th + 1));
+                    real cs = 1 / sqrt(t * t + 1), sn = t * cs;
                     for (int k = 0; k < n; k++)
                     {
                         real x = A[k][a], y = A[k][b];
@@ -983,7 +1005,7 @@ struct Oracle
         {
             real x[3] = {cc[k * 3] - cellBary[c * 3], cc[k * 3 + 1] - cellBary[c * 3 + 1], cc[k * 3 + 2] - cellBary[c * 3 + 2]};
             for (int a = 0; a < n; a++)
-                h = std::max(h, std::abs(V[0][a] * x[0] + V[1][a] * x[1] + V[2][a] * x[2]));
+                h = max(h, abs(V[0][a] * x[0] + V[1][a] * x[1] + V[2][a] * x[2]));
         }
         return h * 2;
     }
@@ -1039,7 +1061,7 @@ struct Oracle
             {
                 real m = 0;
                 for (int k = 0; k < nvert; k++)
-                    m = std::max(m, std::abs(cc[k * 3 + d] - cellBary[c * 3 + d]));
+                    m = max(m, abs(cc[k * 3 + d] - cellBary[c * 3 + d]));
                 cellHBox[c * 3 + d] = m;
             }
             if (dim == 2)
@@ -1108,7 +1130,7 @@ struct Oracle
                 }
                 sum += nAdj * 1 * cur[c];
                 sum /= nAdj * 2;
-                nxt[c] = std::min(cur[c], sum);
+                nxt[c] = min(cur[c], sum);
             }
             cur = nxt;
         }
@@ -1124,9 +1146,9 @@ struct Oracle
         if (!vs.anisotropicLengths)
         {
             if (dim == 2)
-                s[0] = s[1] = std::max(s[0], s[1]);
+                s[0] = s[1] = max(s[0], s[1]);
             else
-                s[0] = s[1] = s[2] = std::max({s[0], s[1], s[2]});
+                s[0] = s[1] = s[2] = max({s[0], s[1], s[2]});
         }
         real x = (p[0] - cellCent[c * 3 + 0]) / s[0], y = (p[1] - cellCent[c * 3 + 1]) / s[1], z = (p[2] - cellCent[c * 3 + 2]) / s[2];
         polyFill(dim, T, x, y, z, s[0], s[1], s[2], rows, NDOF);
@@ -1146,14 +1168,14 @@ struct Oracle
             real s = 0;
             for (int d = 0; d < dim; d++)
                 s += fl[d] * fl[d];
-            faceL = std::sqrt(s / dim);
+            faceL = sqrt(s / dim);
         }
         else
         {
             real s = 0;
             for (int d = 0; d < dim; d++)
                 s += fl[d] * fl[d];
-            faceL = std::sqrt(s);
+            faceL = sqrt(s);
         }
         faceL *= vs.scaleMultiplier;
         for (int i = 0; i < nI * nJ; i++)
@@ -1254,9 +1276,9 @@ struct Oracle
             real wg = 1;
             real dn = norm3(dv);
             if (vs.geomWeightScheme == 1)
-                wg = vs.geomWeightBias + std::pow(std::pow(faceArea[f], 1. / real(dim - 1)) / dn, vs.geomWeightPower * 0.5);
+                wg = vs.geomWeightBias + pow(pow(faceArea[f], 1. / real(dim - 1)) / dn, vs.geomWeightPower * 0.5);
             if (vs.geomWeightScheme == 2)
-                wg = vs.geomWeightBias + std::pow(faceArea[f], vs.geomWeightPower1 * 0.5) * std::pow(dn, vs.geomWeightPower2 * 0.5);
+                wg = vs.geomWeightBias + pow(faceArea[f], vs.geomWeightPower1 * 0.5) * pow(dn, vs.geomWeightPower2 * 0.5);
             real wd[4] = {0, 0, 0, 0};
             if (vs.dirWeightScheme == 0)
                 for (int p = 0; p <= P; p++)
@@ -1294,7 +1316,7 @@ struct Oracle
         {
             int piv = col;
             for (int r = col + 1; r < n; r++)
-                if (std::abs(M[r * 2 * n + col]) > std::abs(M[piv * 2 * n + col]))
+                if (abs(M[r * 2 * n + col]) > abs(M[piv * 2 * n + col]))
                     piv = r;
             if (M[piv * 2 * n + col] == 0)
                 return false;
@@ -1459,7 +1481,7 @@ struct Oracle
             real vsqr = (sqr(UL[1]) + sqr(UL[2]) + sqr(UL[3])) / sqr(UL[0]);
             real p, asqr, H;
             idealGasThermal(UL[4], UL[0], vsqr, g, p, asqr, H);
-            real a = std::sqrt(asqr);
+            real a = sqrt(asqr);
             if (un - a > 0)
                 std::copy(UL, UL + nv, UR);
             else if (un > 0)
@@ -1632,7 +1654,7 @@ struct Oracle
         case 1:
         {
             real TRel = T / es.TRef;
-            return es.muGas * TRel * std::sqrt(TRel) * (es.TRef + es.CSutherland) / (T + es.CSutherland);
+            return es.muGas * TRel * sqrt(TRel) * (es.TRef + es.CSutherland) / (T + es.CSutherland);
         }
         case 2:
             return es.muGas * U[0];
@@ -1678,20 +1700,20 @@ struct Oracle
             real veloNMean = 0.5 * dot3(vsum, n);
             real veloNL = dot3(vL, n), veloNR = dot3(vR, n), vgN = 0;
             real pMean = (pL + pR) * 0.5;
-            real aL = std::sqrt(asqrL), aR = std::sqrt(asqrR);
-            real lambdaConvection = std::max(aL + std::abs(veloNL - vgN), aR + std::abs(veloNR - vgN));
+            real aL = sqrt(asqrL), aR = sqrt(asqrR);
+            real lambdaConvection = max(aL + abs(veloNL - vgN), aR + abs(veloNR - vgN));
             real T = pMean / ((gamma - 1) / gamma * cp() * uMean[0]);
             real muf = muEff(uMean.data(), T);
             muf += muTurSA(uMean.data(), muf);
-            real lamVis = muf / uMean[0] * std::max(4. / 3., gamma / es.prGas);
+            real lamVis = muf / uMean[0] * max(4. / 3., gamma / es.prGas);
             real area = faceArea[f];
             real volR = c1 >= 0 ? vol[c1] : vol[c0];
             lambdaFace[f] = lambdaConvection + lamVis * area * (1. / vol[c0] + 1. / volR);
-            lambdaFaceC[f] = std::abs(veloNMean - vgN) + lamVis * area * (1. / vol[c0] + 1. / volR);
+            lambdaFaceC[f] = abs(veloNMean - vgN) + lamVis * area * (1. / vol[c0] + 1. / volR);
             lambdaFaceVis[f] = lamVis * area * (1. / vol[c0] + 1. / volR);
             lambdaFace0[f] = lambdaConvection;
             real dvn = veloNR - veloNL;
-            deltaLambdaFace[f] = std::max({std::abs(dvn + aR - aL), std::abs(dvn - aR + aL), std::abs(aL - aR)});
+            deltaLambdaFace[f] = max({abs(dvn + aR - aL), abs(dvn - aR + aL), abs(aL - aR)});
         }
         real mn = veryLargeReal;
         for (long c = 0; c < nCell; c++)
@@ -1702,11 +1724,11 @@ struct Oracle
                 long f = cell2face[c * nf + k];
                 lc += lambdaFace[f] * faceArea[f];
             }
-            dt[c] = std::min(CFL * vol[c] * smoothRatio[c] / (lc + 1e-100), MaxDt);
-            mn = std::min(mn, dt[c]);
+            dt[c] = min(CFL * vol[c] * smoothRatio[c] / (lc + 1e-100), MaxDt);
+            mn = min(mn, dt[c]);
             real dl = 0;
             for (int k = 0; k < nf; k++)
-                dl = std::max(dl, deltaLambdaFace[cell2face[c * nf + k]]);
+                dl = max(dl, deltaLambdaFace[cell2face[c * nf + k]]);
             deltaLambdaCell[c] = dl;
         }
         *dtMin = mn;
@@ -1723,10 +1745,10 @@ struct Oracle
         const real cnu1 = 7.1;
         real Chi = U[5] * es.muGas / muf;
         if (Chi < 10)
-            Chi = 0.05 * std::log(1 + std::exp(20 * Chi));
+            Chi = 0.05 * log(1 + exp(20 * Chi));
         real Chi3 = Chi * Chi * Chi;
         real fnu1 = Chi3 / (Chi3 + cnu1 * cnu1 * cnu1);
-        return muf * std::max(Chi * fnu1, 0.0);
+        return muf * max(Chi * fnu1, 0.0);
     }
 
     // fluxFace viscous part at one point (EvaluateDt.hxx:1167-1209) with the SA terms of
@@ -1803,60 +1825,60 @@ struct Oracle
                 real sij = diffU[i][j] + diffU[j][i];
                 om2 += o * o, ss2 += sij * sij, du2 += diffU[i][j] * diffU[i][j];
             }
-        real S = std::sqrt(om2) * std::sqrt(2.0);
-        real SS = std::sqrt(ss2) * (1. / std::sqrt(2.0));
-        real SRotCor = 2.0 * std::min(0.0, S - SS);
-        real diffUNorm = std::sqrt(du2);
-        real ft2 = ct3 * std::exp(-ct4 * sqr(Chi));
+        real S = sqrt(om2) * sqrt(2.0);
+        real SS = sqrt(ss2) * (1. / sqrt(2.0));
+        real SRotCor = 2.0 * min(0.0, S - SS);
+        real diffUNorm = sqrt(du2);
+        real ft2 = ct3 * exp(-ct4 * sqr(Chi));
         real lDES = d;
         {
             real lRANS = d, fwStar = .424;
-            real nuTur = mufPhy / U[0] * std::max(Chi * fnu1, 0.0);
+            real nuTur = mufPhy / U[0] * max(Chi * fnu1, 0.0);
             real nufPhy = mufPhy / U[0];
-            real den = sqr(kappa) * sqr(d) * std::max(smallReal, diffUNorm);
+            real den = sqr(kappa) * sqr(d) * max(smallReal, diffUNorm);
             real rd = (nuTur + nufPhy) / den;
-            real fd = 1. - std::tanh(std::pow(8 * rd, 3));
+            real fd = 1. - tanh(pow(8 * rd, 3));
             real psiSqr = Chi <= 0 ? 100.0
-                                   : std::min(100.0, (1 - cb1 / (cw1 * sqr(kappa) * fwStar) * (ft2 + (1 - ft2) * fnu2)) /
-                                                         (fnu1 * std::max(smallReal, 1 - ft2)));
-            real psi = std::sqrt(std::max(psiSqr, 1.0));
-            lDES = lRANS - fd * std::max(0., lRANS - lLES * psi);
+                                   : min(100.0, (1 - cb1 / (cw1 * sqr(kappa) * fwStar) * (ft2 + (1 - ft2) * fnu2)) /
+                                                         (fnu1 * max(smallReal, 1 - ft2)));
+            real psi = sqrt(max(psiSqr, 1.0));
+            lDES = lRANS - fd * max(0., lRANS - lLES * psi);
             // IDDES (SADESMode 1)
             real alphaIDDES = 0.25 - d / hMax;
-            real fB = std::min(2 * std::exp(-9. * sqr(alphaIDDES)), 1.0);
+            real fB = min(2 * exp(-9. * sqr(alphaIDDES)), 1.0);
             const real cl = 3.55, ct = 1.63;
             real rdt = nuTur / den, rdl = nufPhy / den;
-            real ftt = std::tanh(std::pow(sqr(ct) * rdt, 3));
+            real ftt = tanh(pow(sqr(ct) * rdt, 3));
             real flt = sqr(sqr(cl) * rdl);
-            real fl = std::tanh(sqr(sqr(flt)) * flt);
-            real fe1 = 2. * std::exp(-(alphaIDDES >= 0 ? 11.09 : 9.0) * sqr(alphaIDDES));
-            real fe2 = 1. - std::max(ftt, fl);
-            real fe = std::max(fe1 - 1., 0.) * psi * fe2;
-            real fdTilde = std::max(fB, std::tanh(std::pow(8 * rdt, 3)));
+            real fl = tanh(sqr(sqr(flt)) * flt);
+            real fe1 = 2. * exp(-(alphaIDDES >= 0 ? 11.09 : 9.0) * sqr(alphaIDDES));
+            real fe2 = 1. - max(ftt, fl);
+            real fe = max(fe1 - 1., 0.) * psi * fe2;
+            real fdTilde = max(fB, tanh(pow(8 * rdt, 3)));
             real lIDDES = fdTilde * (1 + fe) * lRANS + (1 - fdTilde) * lLES * psi;
-            lDES = std::max(lLES * smallReal, lIDDES);
+            lDES = max(lLES * smallReal, lIDDES);
         }
         d = lDES;
         real Sbar = nuh / (sqr(kappa) * sqr(d)) * fnu2;
         real Sh = Sbar < -cnu2 * S ? S + S * (sqr(cnu2) * S + cnu3 * Sbar) / ((cnu3 - 2 * cnu2) * S - Sbar) : S + Sbar;
-        real r = std::min(nuh / (Sh * sqr(kappa * d) + verySmallReal), rlim);
-        real g = r + cw2 * (std::pow(r, 6) - r);
-        real fw = g * std::pow((1 + std::pow(cw3, 6)) / (std::pow(g, 6) + std::pow(cw3, 6)), 1. / 6.);
+        real r = min(nuh / (Sh * sqr(kappa * d) + verySmallReal), rlim);
+        real g = r + cw2 * (pow(r, 6) - r);
+        real fw = g * pow((1 + pow(cw3, 6)) / (pow(g, 6) + pow(cw3, 6)), 1. / 6.);
         real D = (cw1 * fw - cb1 / sqr(kappa) * ft2) * sqr(nuh / lDES);
         real P = cb1 * (1 - ft2) * (Sh + SRotCor) * nuh;
         real fn = 1;
         if (U[5] < 0)
         {
             real Chi_ = U[5] * muRef / mufPhy;
-            fn = (cn1 + std::pow(Chi_, 3)) / (cn1 - std::pow(Chi_, 3));
+            fn = (cn1 + pow(Chi_, 3)) / (cn1 - pow(Chi_, 3));
             D = -cw1 * sqr(nuh / lDES);
-            P = cb1 * (1 - ct3) * std::abs(S + SRotCor) * nuh;
+            P = cb1 * (1 - ct3) * abs(S + SRotCor) * nuh;
         }
         real dd = diffRho[0] * diffNu[0] + diffRho[1] * diffNu[1] + diffRho[2] * diffNu[2];
         real nn = diffNu[0] * diffNu[0] + diffNu[1] * diffNu[1] + diffNu[2] * diffNu[2];
         if (mode == 0)
             return U[0] * (P - D + nn * cb2 / sigma) / muRef - (U[5] * fn * muRef + mufPhy) / (U[0] * sigma) * dd / muRef;
-        return -std::min(U[0] * (std::min(P, 0.0) * 1 - D * 2) / muRef / (std::abs(U[5]) + verySmallReal), -verySmallReal);
+        return -min(U[0] * (min(P, 0.0) * 1 - D * 2) / muRef / (abs(U[5]) + verySmallReal), -verySmallReal);
     }
 
     // EvaluateRHS.hxx:665-801 source integration (SA only; the NS source is zero) and the
@@ -1901,9 +1923,9 @@ struct Oracle
                 idealGasThermal(U[4], U[0], velo2, es.gamma, pM, aM, HM);
                 real Tm = pM / ((es.gamma - 1) / es.gamma * cp() * U[0]);
                 real muf = muEff(U, Tm);
-                real d = std::min(dWall.empty() ? veryLargeReal : dWall[c * nGc + g], std::pow(veryLargeReal, 1. / 6.));
+                real d = min(dWall.empty() ? veryLargeReal : dWall[c * nGc + g], pow(veryLargeReal, 1. / 6.));
                 real hMax = cellHMax[c];
-                real lLES = std::min(hMax * veryLargeReal, std::max(d * 1.0, hMax * 1.0));
+                real lLES = min(hMax * veryLargeReal, max(d * 1.0, hMax * 1.0));
                 real JW = cellJDet[c * nGc + g] * w;
                 S += saSource(U, G, muf, d, lLES, hMax, 0) * JW;
                 J += saSource(U, G, muf, d, lLES, hMax, 1) * JW;
@@ -1962,9 +1984,9 @@ struct Oracle
                 std::copy(UL, UL + nv, UR);
             real dc[3] = {faceCent[f * 3 + 0] - cellBary[c0 * 3 + 0], faceCent[f * 3 + 1] - cellBary[c0 * 3 + 1],
                           faceCent[f * 3 + 2] - cellBary[c0 * 3 + 2]};
-            real distBaryPerp = std::abs(dot3(dc, n)) * 2.;
+            real distBaryPerp = abs(dot3(dc, n)) * 2.;
             real distGRP = vol[c0] / faceArea[f] * 2;
-            distGRP = std::max(std::min(distBaryPerp, distGRP * 2), distGRP * 0.25);
+            distGRP = max(min(distBaryPerp, distGRP * 2), distGRP * 0.25);
             if (type == 3 || type == 9)
                 distGRP += veryLargeReal;
             real UM[8], GM[3 * 8], GMP[3 * 8];
@@ -2019,7 +2041,7 @@ struct Oracle
             std::vector<real> T0(4 * NDOF), T1(4 * NDOF);
             real fluxEs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             const real *ULm = u + c0 * nv, *URm = u + c1 * nv;
-            real dLambda = std::max(deltaLambdaCell[c0], deltaLambdaCell[c1]);
+            real dLambda = max(deltaLambdaCell[c0], deltaLambdaCell[c1]);
             for (int g = 0; g < nGf; g++)
             {
                 real pq[3], w;
@@ -2053,13 +2075,13 @@ struct Oracle
                         GL[d * nv + v] = ga, GR[d * nv + v] = gb;
                     }
                 }
-                real minVol = std::min(vol[c0], vol[c1]);
+                real minVol = min(vol[c0], vol[c1]);
                 real b1[3];
                 otherBary(c0, f, b1);
                 real db[3] = {b1[0] - cellBary[c0 * 3 + 0], b1[1] - cellBary[c0 * 3 + 1], b1[2] - cellBary[c0 * 3 + 2]};
-                real distBaryPerp = std::abs(dot3(db, n));
+                real distBaryPerp = abs(dot3(db, n));
                 real distGRP = minVol / faceArea[f] * 2;
-                distGRP = std::max(std::min(distBaryPerp, distGRP * 2), distGRP * 0.25);
+                distGRP = max(min(distBaryPerp, distGRP * 2), distGRP * 0.25);
                 real UM[8], GM[3 * 8], GMP[3 * 8];
                 for (int v = 0; v < nv; v++)
                     UM[v] = 0.5 * (UL[v] + UR[v]);
@@ -2197,7 +2219,7 @@ struct Oracle
             {
                 real old = uIncNew[c * nv + v];
                 uIncNew[c * nv + v] = buf[v] / jdiag[nv >= 6 ? c * nv + v : c];
-                sumInc[v] += std::abs(uIncNew[c * nv + v] - old);
+                sumInc[v] += abs(uIncNew[c * nv + v] - old);
             }
         }
     }
@@ -2433,22 +2455,22 @@ struct Oracle
                 {
                     // SpecialFields.hpp:42-77 IsentropicVortex10 at t = 0
                     real xyc = 5;
-                    real px = x[0] - std::floor(x[0] / 10) * 10, py = x[1] - std::floor(x[1] / 10) * 10;
-                    real r = std::sqrt(sqr(px - xyc) + sqr(py - xyc));
-                    real dT = -(gamma - 1) / (8 * gamma * sqr(pi)) * sqr(chi) * std::exp(1 - sqr(r));
-                    real dux = chi / 2 / pi * std::exp((1 - sqr(r)) / 2) * -(py - xyc);
-                    real duy = chi / 2 / pi * std::exp((1 - sqr(r)) / 2) * +(px - xyc);
+                    real px = x[0] - floor(x[0] / 10) * 10, py = x[1] - floor(x[1] / 10) * 10;
+                    real r = sqrt(sqr(px - xyc) + sqr(py - xyc));
+                    real dT = -(gamma - 1) / (8 * gamma * sqr(pi)) * sqr(chi) * exp(1 - sqr(r));
+                    real dux = chi / 2 / pi * exp((1 - sqr(r)) / 2) * -(py - xyc);
+                    real duy = chi / 2 / pi * exp((1 - sqr(r)) / 2) * +(px - xyc);
                     real T = dT + 1, ux = dux + 1, uy = duy + 1;
-                    real rho = std::pow(T, 1 / (gamma - 1));
+                    real rho = pow(T, 1 / (gamma - 1));
                     real p = T * rho;
                     inc[0] = rho, inc[1] = rho * ux, inc[2] = rho * uy, inc[4] = 0.5 * (sqr(ux) + sqr(uy)) * rho + p / (gamma - 1);
                 }
                 else
                 {
                     real M0 = 0.1;
-                    real ux = std::sin(x[0]) * std::cos(x[1]) * std::cos(x[2]);
-                    real uy = -std::cos(x[0]) * std::sin(x[1]) * std::cos(x[2]);
-                    real p = 1. / (gamma * sqr(M0)) + 1. / 16 * ((std::cos(2 * x[0]) + std::cos(2 * x[1])) * (2 + std::cos(2 * x[2])));
+                    real ux = sin(x[0]) * cos(x[1]) * cos(x[2]);
+                    real uy = -cos(x[0]) * sin(x[1]) * cos(x[2]);
+                    real p = 1. / (gamma * sqr(M0)) + 1. / 16 * ((cos(2 * x[0]) + cos(2 * x[1])) * (2 + cos(2 * x[2])));
                     real rho = gamma * sqr(M0) * p;
                     inc[0] = rho, inc[1] = rho * ux, inc[2] = rho * uy, inc[4] = 0.5 * (sqr(ux) + sqr(uy)) * rho + p / (gamma - 1);
                 }
@@ -2464,6 +2486,11 @@ struct Oracle
 
 using namespace orc;
 
+#ifdef ORC_OPCOUNT
+// the counting build: the same entry points with the counting scalar in place of double (one double in
+// a struct: the same calling convention, so the ctypes binding is unchanged)
+#define double real
+#endif
 extern "C"
 {
     void *orc_create(int dim, int cellType, int faceType, long nNode, const double *coords, long nCell, int nvert, const long *cell2node,
@@ -2683,6 +2710,19 @@ extern "C"
         }
     }
 }
+#ifdef ORC_OPCOUNT
+#undef double
+extern "C"
+{
+    // counts of the operations since the last reset: {add/sub, mul, div, sqrt, exp/pow/log/trig calls}
+    void orc_opcount_reset() { orc_cnt::ctr() = orc_cnt::Counter{}; }
+    void orc_opcount_get(uint64_t *out)
+    {
+        const orc_cnt::Counter &c = orc_cnt::ctr();
+        out[0] = c.add, out[1] = c.mul, out[2] = c.div, out[3] = c.sqrt, out[4] = c.fn;
+    }
+}
+#else
 
 // ---------------------------------------------------------------------------
 // Positivity-preserving increment limiting (5 conservative variables, the SA variable 6th).
@@ -2702,12 +2742,12 @@ double ppCompressionRatio(const double *u, const double *inc, double newRhoE, bo
         r[i] = inc[i], un[i] = u[i] + inc[i];
     double m2 = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
     double rhoEOld = u[4] - m2 / (u[0] + kPPVerySmall) * 0.5;
-    newRhoE = std::max(kPPSmall * rhoEOld, newRhoE);
+    newRhoE = max(kPPSmall * rhoEOld, newRhoE);
     double rhoENew = un[4] - (un[1] * un[1] + un[2] * un[2] + un[3] * un[3]) / (un[0] + kPPVerySmall) * 0.5;
-    double alpha = (rhoEOld - newRhoE) / std::max(-rhoENew + rhoEOld, kPPVerySmall);
+    double alpha = (rhoEOld - newRhoE) / max(-rhoENew + rhoEOld, kPPVerySmall);
     if (rhoENew > rhoEOld)
         alpha = 1;
-    alpha = std::max(std::min(alpha, 1.), 0.);
+    alpha = max(min(alpha, 1.), 0.);
     double c0 = 2 * u[4] * u[0] - m2 - 2 * u[0] * newRhoE;
     double c1 = 2 * u[4] * r[0] + 2 * u[0] * r[4] - 2 * (u[1] * r[1] + u[2] * r[2] + u[3] * r[3]) - 2 * r[0] * newRhoE;
     double c2 = 2 * r[4] * r[0] - (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
@@ -2715,13 +2755,13 @@ double ppCompressionRatio(const double *u, const double *inc, double newRhoE, bo
     double dC = c1 * c1 - 4 * c0 * c2;
     if (dC <= -c0 * c0 * kPPSmall)
         bad = true;
-    dC = std::max(0., dC);
-    double aL = (-std::sqrt(dC) - c1) / (2 * c2);
-    if (std::abs(c2) < 1e-10 * c0)
-        alpha = std::abs(c1) < 1e-10 * c0 ? 0 : std::min(-c0 / c1, 1.);
+    dC = max(0., dC);
+    double aL = (-sqrt(dC) - c1) / (2 * c2);
+    if (abs(c2) < 1e-10 * c0)
+        alpha = abs(c1) < 1e-10 * c0 ? 0 : min(-c0 / c1, 1.);
     else
-        alpha = std::min(aL, 1.);
-    alpha = std::max(0., alpha) * safety;
+        alpha = min(aL, 1.);
+    alpha = max(0., alpha) * safety;
     if (alpha < kPPSmall)
         alpha = 0;
     for (int i = 0; i < 5; i++)
@@ -2777,7 +2817,7 @@ void ppCompressInc(int nv, double gamma, const double *u, const double *inc, dou
         double dC = c1 * c1 - 4 * c0 * c2;
         if (!(dC > 0))
             bad = true;
-        double alpha = std::max(0., std::min((-std::sqrt(std::max(dC, 0.)) - c1) / (2 * c2), 1.));
+        double alpha = max(0., min((-sqrt(max(dC, 0.)) - c1) / (2 * c2), 1.));
         for (int i = 0; i < nv; i++)
             ret[i] *= alpha * 0.99;
         for (int it = 0; it < 1000; it++)
@@ -2795,7 +2835,7 @@ void ppCompressInc(int nv, double gamma, const double *u, const double *inc, dou
     {
         if (u[5] < 0)
             bad = true;
-        double nu = std::max(1e-6, u[5] * std::exp(ret[5] / (u[5] + 1e-6)));
+        double nu = max(1e-6, u[5] * exp(ret[5] / (u[5] + 1e-6)));
         ret[5] = nu - u[5];
     }
 }
@@ -2826,7 +2866,7 @@ extern "C"
                 bad = true;
             double aRho = 1, relRho = rhoEps * relax + uc[0] * (1 - relax);
             if (inc[0] < 0)
-                aRho = std::min(1.0, (uc[0] - relRho) / (-inc[0] - kPPSmall * inc[0]));
+                aRho = min(1.0, (uc[0] - relRho) / (-inc[0] - kPPSmall * inc[0]));
             if (!(aRho >= 0 && aRho <= 1))
                 bad = true;
             double un[5];
@@ -2838,14 +2878,14 @@ extern "C"
                 relP = pEps + (pOld - pEps) * (1 - relax);
             double aP = 1;
             if (pNew < relP)
-                aP = std::min(aP, ppCompressionRatio(uc, inc, relP / (gamma - 1), bad));
+                aP = min(aP, ppCompressionRatio(uc, inc, relP / (gamma - 1), bad));
             double a = aRho * aP;
             if (a < 1)
             {
-                a = std::pow(a, compress * (int)std::round(compressPower));
+                a = pow(a, compress * (int)round(compressPower));
                 nLim++;
                 a *= safety;
-                aMin = std::min(aMin, a);
+                aMin = min(aMin, a);
             }
             alpha[c] = a;
         }
@@ -2890,10 +2930,10 @@ extern "C"
             for (int i = 0; i < nv; i++)
                 a[i] = inc[c * nv + i] * alpha;
             ppCompressInc(nv, gamma, u + c * nv, a, rhoEps, pEps, comp, bad);
-            double na = std::abs(comp[0]) / std::abs(a[0]);
-            if (std::abs(a[0]) < kPPVerySmall)
+            double na = abs(comp[0]) / abs(a[0]);
+            if (abs(a[0]) < kPPVerySmall)
                 na = 1.;
-            fixMin = std::min(fixMin, na);
+            fixMin = min(fixMin, na);
             for (int i = 0; i < nv; i++)
                 u[c * nv + i] += comp[i];
         }
@@ -2916,7 +2956,7 @@ bool ocSolve(int n, int m, double *A, double *B)
     {
         int piv = c;
         for (int r = c + 1; r < n; r++)
-            if (std::abs(A[r * n + c]) > std::abs(A[piv * n + c]))
+            if (abs(A[r * n + c]) > abs(A[piv * n + c]))
                 piv = r;
         if (A[piv * n + c] == 0)
             return false;
@@ -2949,15 +2989,15 @@ bool ocSolve(int n, int m, double *A, double *B)
 void ocNormBase(const double *n, double B[3][3])
 {
     double t[3];
-    if (std::abs(n[2]) < 0.9) // -(n x e_z)
+    if (abs(n[2]) < 0.9) // -(n x e_z)
         t[0] = -(n[1] * 1 - n[2] * 0), t[1] = -(n[2] * 0 - n[0] * 1), t[2] = -(n[0] * 0 - n[1] * 0);
     else // -(n x e_y)
         t[0] = -(n[1] * 0 - n[2] * 1), t[1] = -(n[2] * 0 - n[0] * 0), t[2] = -(n[0] * 1 - n[1] * 0);
-    double tn = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    double tn = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
     for (int d = 0; d < 3; d++)
         t[d] /= tn;
     double s[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
-    double sn = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    double sn = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
     for (int d = 0; d < 3; d++)
         B[d][0] = n[d], B[d][1] = t[d], B[d][2] = s[d] / sn;
 }
@@ -2968,7 +3008,7 @@ void ocEigen(const double *UC, double gamma, double Rv[5][5], double Lv[5][5])
     double v[3] = {UC[1] / UC[0], UC[2] / UC[0], UC[3] / UC[0]};
     double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     double p = (gamma - 1) * (UC[4] - 0.5 * UC[0] * vsq);
-    double a2 = gamma * p / UC[0], a = std::sqrt(a2), H = (UC[4] + p) / UC[0];
+    double a2 = gamma * p / UC[0], a = sqrt(a2), H = (UC[4] + p) / UC[0];
     for (int i = 0; i < 5; i++)
         for (int j = 0; j < 5; j++)
             Rv[i][j] = Lv[i][j] = 0;
@@ -3085,8 +3125,8 @@ extern "C"
             }
             double sm = 0;
             for (int q = 0; q < 2; q++)
-                sm = std::max(sm, std::abs(S[q][0] / (S[q][1] + 1e-200)));
-            si[c] = std::sqrt(sm) * o->vs.maxOrder * o->vs.maxOrder;
+                sm = max(sm, abs(S[q][0] / (S[q][1] + 1e-200)));
+            si[c] = sqrt(sm) * o->vs.maxOrder * o->vs.maxOrder;
         }
     }
 
@@ -3178,9 +3218,9 @@ extern "C"
                     for (int i = 0; i < nr * nv; i++)
                     {
                         double u1 = tin[i], u2 = oin[i];
-                        double fr = u1 / (std::abs(u2) + kPDiP) * ocSign(u2);
+                        double fr = u1 / (abs(u2) + kPDiP) * ocSign(u2);
                         double t1 = fr * fr * fr, t2 = (fr * fr) * (fr * fr);
-                        lim[i] = u1 * (1 + t1) / (1 + t2) * std::abs(ocSign(u2));
+                        lim[i] = u1 * (1 + t1) / (1 + t2) * abs(ocSign(u2));
                     }
                     ocCharTransform(uL, uR, n, gamma, false, nr, nv, lim.data());
                     for (int i = 0; i < nr * nv; i++)
@@ -3192,10 +3232,10 @@ extern "C"
                     double up = 0, down = 0, cent = others[0][i];
                     for (size_t q = 1; q < others.size(); q++)
                     {
-                        double ti = others[0][i] / (std::abs(others[q][i]) + kPDiP) * ocSign(others[q][i]);
+                        double ti = others[0][i] / (abs(others[q][i]) + kPDiP) * ocSign(others[q][i]);
                         down += (ti * ti) * (ti * ti);
                         up += ti * ti * ti;
-                        cent *= std::abs(ocSign(others[q][i]));
+                        cent *= abs(ocSign(others[q][i]));
                     }
                     out[ls * nv + i] = cent * (up + nStd) / (down + nStd);
                 }
@@ -3204,3 +3244,5 @@ extern "C"
         return 0;
     }
 }
+
+#endif // ORC_OPCOUNT
