@@ -45,6 +45,10 @@ FALLBACK_HBM_GBS = 6650.0
 # a 64^3 launch is scaled by the cell count
 RHS_TRAFFIC_PER_CELL = 273.1e6 / 48 ** 3
 RHS_FP64_PIPE_PCT = 30.5  # sm__pipe_fp64_cycles_active of the same capture
+# algorithmic flops per cell (F_alg), counted by the op-counting build of the oracle on this workload
+# (python -m oracle.falg: +, -, *, / and sqrt one each; profiles/falg_tgv_p2.md)
+F_RHS = {2: 50067.0, 1: 30303.0}
+F_VR = {2: 6300.0, 1: 1020.0}
 # the reference's published TGV throughput for this path: 71.8 M cell-iterations/s on 10,240 CPU ranks
 REF_PUBLISHED_MCIPS = 71.8
 
@@ -66,6 +70,27 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def fp64_peak_tflops(dev):
+    """FP64 throughput of cuBLAS DGEMM (8192^3, best of 5 after a warm-up) on this GPU: the measured FP64 peak the
+    FP64-pipe fraction of the RHS is quoted against (MEASURED_PEAKS.json carries no FP64 figure)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = a @ b
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b, out=c)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return best
 
 
 class ClockSampler:
@@ -635,6 +660,14 @@ def run_ours(args, rank, world, local_rank):
     hbm, src = peaks()
     dom_name, dom_t, dom_b = ("vr_jacobi_sweep", t_vr, B_VR) if t_vr >= t_rhs else ("evaluate_rhs", t_rhs, B_RHS)
     achieved = dom_b * nc / (dom_t * 1e-3) / 1e9
+    p64 = fp64_peak_tflops(dev)
+    f_dom = (F_VR if dom_name == "vr_jacobi_sweep" else F_RHS).get(p)
+    fp64 = None
+    if f_dom:
+        ach_tf = f_dom * nc / (dom_t * 1e-3) / 1e12
+        fp64 = {"falg_per_cell": f_dom, "falg_source": "op-counting build of the oracle (python -m oracle.falg)",
+                "achieved_tflops": ach_tf, "peak_tflops": p64, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                "frac": ach_tf / p64}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": value / REF_PUBLISHED_MCIPS, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(n, p), parallelism=f"replicas{world}" if world > 1 else "single GPU"),
@@ -643,9 +676,11 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback 6650 GB/s",
                          "traffic": RHS_TRAFFIC_PER_CELL * nc if dom_name == "evaluate_rhs" else None,
-                         "traffic_source": "ncu dram bytes of k_rhs_face_fast at 48^3 (profiles/), scaled by cells",
+                         "traffic_source": "constant copied from the ncu capture of k_rhs_face_fast at 48^3 (profiles/), scaled by cells",
                          "fp64_pipe_pct": RHS_FP64_PIPE_PCT if dom_name == "evaluate_rhs" else None,
-                         "algorithmic_bytes_per_cell": dom_b},
+                         "fp64_pipe_pct_source": "constant copied from the same 48^3 ncu capture",
+                         "algorithmic_bytes_per_cell": dom_b,
+                         "fp64": fp64},
             "kernels_ms": {"vr_jacobi_sweep": t_vr, "evaluate_rhs": t_rhs,
                            "vr_GBps": B_VR * nc / (t_vr * 1e-3) / 1e9, "rhs_GBps": B_RHS * nc / (t_rhs * 1e-3) / 1e9},
             "clocks": clk.summary()}

@@ -182,10 +182,13 @@ DNDSB_GLOBAL void k_sgs_pos(int64_t pBeg, int64_t pEnd, const int32_t *__restric
 }
 
 // LUSGSMatrixVec (EulerEvaluator.hxx:175-274)
+// xs (may be null): a scale of x (the normalising factor of an unnormalised basis column): Ax = A (xs x)
 template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_matvec_pos(int64_t n, const int32_t *__restrict__ nbrPos, const typename Vec4<T>::type *__restrict__ op,
-                               const T *__restrict__ jd, const T *__restrict__ uT, const T *__restrict__ x, T *Ax, T gamma)
+                               const T *__restrict__ jd, const T *__restrict__ uT, const T *__restrict__ x, T *Ax, T gamma,
+                               const real *__restrict__ xs)
 {
+    const T sx = xs ? (T)*xs : T(1);
     DNDSB_KERNEL_LOOP(p, n)
     {
         T buf[NV];
@@ -205,7 +208,7 @@ DNDSB_GLOBAL void k_matvec_pos(int64_t n, const int32_t *__restrict__ nbrPos, co
         }
         constexpr int JD = jd_of<T, NV>();
         for (int v = 0; v < NV; v++)
-            Ax[p * NV + v] = jd[p * JD + (JD > 1 ? v : 0)] * x[p * NV + v] - buf[v];
+            Ax[p * NV + v] = sx * (jd[p * JD + (JD > 1 ? v : 0)] * x[p * NV + v] - buf[v]);
     }
 }
 
@@ -224,19 +227,6 @@ DNDSB_GLOBAL void k_gmres_v0(int64_t n, const T *__restrict__ w, const T *__rest
         real d = (wIsZero ? 0.0 : (real)w[i]) - (real)MLb[i];
         v0[i] = (T)(d * s);
     }
-}
-
-// v_{j+1} = w / h[j+1][j], or 0 after a breakdown; records the first breakdown
-template <typename T>
-DNDSB_GLOBAL void k_gmres_next(int64_t n, T *w, const real *hcol, int j, real *sc)
-{
-    real h = hcol[j + 1];
-    bool broken = !(h > sc[0] * 1e-32) || sc[2] <= j;
-    real s = broken ? 0.0 : 1.0 / h;
-    DNDSB_KERNEL_LOOP(i, n)
-    w[i] = (T)((real)w[i] * s);
-    if (broken && blockIdx.x == 0 && threadIdx.x == 0 && sc[2] > j)
-        sc[2] = j;
 }
 
 // least squares  min |beta e1 - H y|  by Givens rotations on the Hessenberg
@@ -285,9 +275,10 @@ DNDSB_GLOBAL void k_gmres_lsq(int k, const real *H, real *sc)
         sc[kScY + jj] = 0;
 }
 
-// x += sum_i y_i v_i over the valid columns
+// x += sum_i y_i v_i over the valid columns (v_i = colScale_i times the stored column)
 template <typename T>
-DNDSB_GLOBAL void k_gmres_update(int64_t n, int64_t ld, int k, const T *__restrict__ V, const real *__restrict__ sc, T *x)
+DNDSB_GLOBAL void k_gmres_update(int64_t n, int64_t ld, int k, const T *__restrict__ V, const real *__restrict__ sc,
+                                 const real *__restrict__ colScale, T *x)
 {
     int nv = (int)sc[2];
     if (nv > k)
@@ -296,15 +287,16 @@ DNDSB_GLOBAL void k_gmres_update(int64_t n, int64_t ld, int k, const T *__restri
     {
         real acc = (real)x[i];
         for (int jj = 0; jj < nv; jj++)
-            acc += sc[kScY + jj] * (real)V[jj * ld + i];
+            acc += sc[kScY + jj] * colScale[jj] * (real)V[jj * ld + i];
         x[i] = (T)acc;
     }
 }
 
-DNDSB_GLOBAL void k_gmres_reset(real *sc, int k)
+// a new Arnoldi cycle: k valid columns so far, the first column stored normalised
+DNDSB_GLOBAL void k_gmres_reset(real *sc, int k, real *colScale)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        sc[2] = k;
+        sc[2] = k, colScale[0] = 1.0;
 }
 
 DNDSB_GLOBAL void k_copy_scalar(const real *a, real *b)
@@ -323,6 +315,8 @@ struct LinWs
     void *op = nullptr, *jd = nullptr, *uT = nullptr, *rhsT = nullptr, *x = nullptr, *tmp = nullptr, *tmp2 = nullptr, *MLb = nullptr,
          *V = nullptr;
     real *H = nullptr, *sc = nullptr, *s2 = nullptr, *red = nullptr;
+    real *colScale = nullptr; // [33] normalising factors of the stored (unnormalised) Krylov columns
+    unsigned *cnt = nullptr;  // ticket counter of the one-launch reductions (zero between launches)
     cudaStream_t cs = nullptr;
     cudaEvent_t evIn = nullptr, evOut = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -335,7 +329,7 @@ void linws_free(LinWs *w)
     if (!w)
         return;
     for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
-                    (void *)w->sc, (void *)w->s2, (void *)w->red})
+                    (void *)w->sc, (void *)w->s2, (void *)w->red, (void *)w->colScale, (void *)w->cnt})
         dev_free(p);
     graph_free(w->graph);
     stream_free(w->cs);
@@ -374,8 +368,10 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv)
               dev_alloc((void **)&w->H, sizeof(real) * (k + 1) * (k > 0 ? k : 1)) == cudaSuccess &&
               dev_alloc((void **)&w->sc, sizeof(real) * (kScY + 40)) == cudaSuccess &&
               dev_alloc((void **)&w->s2, sizeof(real) * 8) == cudaSuccess &&
-              dev_alloc((void **)&w->red, sizeof(real) * kRedBufLenK) == cudaSuccess;
+              dev_alloc((void **)&w->red, sizeof(real) * kRedBufLenK) == cudaSuccess &&
+              dev_alloc((void **)&w->colScale, sizeof(real) * 33) == cudaSuccess && dev_alloc((void **)&w->cnt, sizeof(unsigned)) == cudaSuccess;
     ok = ok && dev_zero(w->V, es * krylov_ld(n) * (k + 1), nullptr) == cudaSuccess; // the column pads stay zero
+    ok = ok && dev_zero(w->cnt, sizeof(unsigned), nullptr) == cudaSuccess && dev_zero(w->colScale, sizeof(real) * 33, nullptr) == cudaSuccess;
     if (!ok || stream_create(&w->cs) != cudaSuccess || event_create(&w->evIn) != cudaSuccess || event_create(&w->evOut) != cudaSuccess)
     {
         linws_free(w);
@@ -441,11 +437,12 @@ struct Solve
             sgs_pair(b, MLx, i == 0);
     }
 
-    void FA(const T *x, T *Ax) const
+    // xs: the normalising factor of x when x is a stored Krylov column (nullptr: 1)
+    void FA(const T *x, T *Ax, const real *xs = nullptr) const
     {
         auto kern = k_matvec_pos<T, NV, NF>;
         DNDSB_LAUNCH(kern, m.nCell, 128, st, m.nCell, w.nbrPos, (const T4 *)w.op, (const T *)w.jd, (const T *)w.uT, x,
-                     Ax, gamma);
+                     Ax, gamma, xs);
     }
 
     void body() const
@@ -468,7 +465,7 @@ struct Solve
         int k = ls.nGmresSpace;
         T *MLb = (T *)w.MLb, *tmp = (T *)w.tmp;
         FML(b, MLb);
-        krylov_norm(prec(), nn, NV, MLb, w.s2, w.red, w.sc + 0, st); // scale
+        krylov_norm(prec(), nn, NV, MLb, w.s2, w.red, w.sc + 0, w.cnt, st); // scale
         for (int r = 0; r < ls.nGmresIter; r++)
         {
             // V0 = M (A x) - M b; beta = |V0|; V0 = -V0 / beta
@@ -481,22 +478,23 @@ struct Solve
             {
                 FA(x, tmp);
                 FML(tmp, V(0));
-                krylov_diff_norm(prec(), nn, NV, V(0), MLb, w.s2, w.red, w.sc + 1, st);
+                krylov_diff_norm(prec(), nn, NV, V(0), MLb, w.s2, w.red, w.sc + 1, w.cnt, st);
                 DNDSB_LAUNCH(k_gmres_v0<T>, nn, 256, st, nn, V(0), MLb, V(0), w.sc, 0);
             }
-            DNDSB_LAUNCH(k_gmres_reset, 1, 32, st, w.sc, k);
+            DNDSB_LAUNCH(k_gmres_reset, 1, 32, st, w.sc, k, w.colScale);
             for (int j = 0; j < k; j++)
             {
-                FA(V(j), tmp);
+                // the basis columns stay unnormalised: v_j = colScale[j] V(j), the factor applied by each reader
+                FA(V(j), tmp, w.colScale + j);
                 FML(tmp, V(j + 1));
                 real *hcol = w.H + (int64_t)j * (k + 1);
-                // classical Gram-Schmidt: h = V^T w, w -= V h, h[j+1] = |w|
-                krylov_mdot(prec(), nn, ld(), NV, j + 1, w.V, V(j + 1), w.s2, w.red, hcol, st);
-                krylov_maxpy_norm(prec(), nn, ld(), NV, j + 1, w.V, hcol, V(j + 1), w.s2, w.red, hcol + j + 1, st);
-                DNDSB_LAUNCH(k_gmres_next<T>, nn, 256, st, nn, V(j + 1), hcol, j, w.sc);
+                // classical Gram-Schmidt: h = V^T w, w -= V h, h[j+1] = |w|, colScale[j+1] = 1 / h[j+1]
+                krylov_mdot(prec(), nn, ld(), NV, j + 1, w.V, V(j + 1), w.s2, w.red, hcol, w.colScale, w.cnt, st);
+                krylov_maxpy_norm(prec(), nn, ld(), NV, j + 1, w.V, hcol, w.colScale, V(j + 1), w.s2, w.red, hcol + j + 1, w.cnt, w.sc, j,
+                                  w.colScale + j + 1, st);
             }
             DNDSB_LAUNCH(k_gmres_lsq, 1, 32, st, k, w.H, w.sc);
-            DNDSB_LAUNCH(k_gmres_update<T>, nn, 256, st, nn, ld(), k, (const T *)w.V, w.sc, x);
+            DNDSB_LAUNCH(k_gmres_update<T>, nn, 256, st, nn, ld(), k, (const T *)w.V, w.sc, w.colScale, x);
             xZero = false;
         }
     }

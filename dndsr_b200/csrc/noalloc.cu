@@ -16,6 +16,9 @@
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current); make that first call
 //    before any stream capture begins;
+//  * like dndsb_eval_evaluate_rhs, a call reads the device error word back and
+//    synchronises its stream before it returns, unless the evaluator reports
+//    its errors deferred (dndsb_eval_set_deferred_errors);
 //  * every call on a device shares the one array and leaves the last call's
 //    face fluxes in it; no entry has to start at zero because the face kernel
 //    writes every entry the gather kernel reads;
@@ -98,5 +101,9 @@ extern "C" int dndsb_eval_evaluate_rhs_noalloc(dndsb_eval *ev, double *rhs, cons
         return set_error(rc, "dndsb_eval_evaluate_rhs_noalloc: non-physical state (density or pressure <= 0)");
     if (rc == ST_NONFINITE)
         return set_error(rc, "dndsb_eval_evaluate_rhs_noalloc: non-finite value");
+    if (rc == ST_UNSUPPORTED)
+        return set_error(rc, "dndsb_eval_evaluate_rhs_noalloc: configuration not supported (nVars must be 5 or 6)");
+    if (rc == ST_BADARG)
+        return set_error(rc, "dndsb_eval_evaluate_rhs_noalloc: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
     return set_error(rc, std::string("dndsb_eval_evaluate_rhs_noalloc: ") + cudaGetErrorString(cudaGetLastError()));
 }

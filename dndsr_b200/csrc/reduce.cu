@@ -169,11 +169,50 @@ DNDSB_D real warp_sum(real x)
 
 constexpr int kKG = 8; // columns per pass of the multi-dot
 
+// Called by every block after it has written its partials [block][ncol]: the block that arrives last
+// (a ticket on *cnt, which it resets for the next launch) sums them per column in a fixed order (lanes
+// over a fixed stride of the blocks, then a fixed xor tree, lane 0's value), the order the separate
+// final pass used, so the result does not depend on which block finishes last.  out[col] = the sum
+// (its square root with takeSqrt) times colScale[col] (when given).  Returns true in that block
+// (uniformly over its threads).
+DNDSB_D bool last_block_final(int ncol, const real *partial, real *out, const real *colScale, int takeSqrt, unsigned *cnt)
+{
+    __shared__ unsigned ticket;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        ticket = atomicAdd(cnt, 1u);
+    __syncthreads();
+    if (ticket != gridDim.x - 1)
+        return false;
+    __threadfence();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int col = wid; col < ncol; col += nw)
+    {
+        real a = 0;
+        for (int i = lane; i < (int)gridDim.x; i += 32)
+            a += __ldcg(partial + (int64_t)i * ncol + col);
+        a = warp_sum(a);
+        if (lane == 0)
+        {
+            real r = takeSqrt ? sqrt(a) : a;
+            out[col] = colScale ? r * colScale[col] : r;
+        }
+    }
+    if (threadIdx.x == 0)
+        *cnt = 0;
+    __syncthreads();
+    return true;
+}
+
 // partial[block][col] = sum_i V[col][i] w[i] s2[i % NV] over the block's chunk of quads.  Columns are
 // ld apart (ld a multiple of 4, the pad beyond n zero); all columns of a pass share one read of w.
+// out[col] = partial sums reduced by the last block, times colScale[col] (the basis columns are stored
+// unnormalised; colScale holds their normalising factors)
 template <typename T, int NV>
 DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmdot(int64_t n, int64_t ld, int ncol, const T *__restrict__ V, const T *__restrict__ w,
-                                                       const real *__restrict__ s2, real *partial)
+                                                       const real *__restrict__ s2, real *partial, real *out, const real *colScale,
+                                                       unsigned *cnt)
 {
     __shared__ real sh[kKG][kRedBlock / 32];
     __shared__ real ss[8];
@@ -243,19 +282,24 @@ DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmdot(int64_t n, int64_t ld,
         }
         __syncthreads();
     }
+    last_block_final(ncol, partial, out, colScale, 0, cnt);
 }
 
-// w -= sum_c h[c] V[c] (columns subtracted in index order); partial[block] = sum_i w_i^2 s2[i % NV]
-// of the stored w.  w is column ncol of the same basis (not read through V).
+// w -= sum_c h[c] colScale[c] V[c] (columns subtracted in index order); the last block writes
+// *outNorm = sqrt(sum_i w_i^2 s2[i % NV]) of the stored w.  w is column ncol of the same basis (not read
+// through V).  With gsc (the GMRES scalars: [0] scale, [2] valid columns) it also sets the normalising
+// factor of the new column, *scaleNext = 1 / norm, or 0 at a breakdown (norm <= 1e-32 scale), which it
+// records in gsc[2] = j (GMRES_LeftPreconditioned::solve, Linear.hpp:100-108).
 template <typename T, int NV>
 DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmaxpy_norm(int64_t n, int64_t ld, int ncol, const T *__restrict__ V, const real *__restrict__ h,
-                                                             T *w, const real *__restrict__ s2, real *partial)
+                                                             const real *__restrict__ colScale, T *w, const real *__restrict__ s2, real *partial,
+                                                             real *outNorm, unsigned *cnt, real *gsc, int j, real *scaleNext)
 {
     __shared__ real hs[32];
     __shared__ real ss[8];
     __shared__ real sh[kRedBlock / 32];
     if (threadIdx.x < ncol)
-        hs[threadIdx.x] = h[threadIdx.x];
+        hs[threadIdx.x] = h[threadIdx.x] * (colScale ? colScale[threadIdx.x] : 1.0);
     if (threadIdx.x < NV)
         ss[threadIdx.x] = s2[threadIdx.x];
     __syncthreads();
@@ -312,11 +356,19 @@ DNDSB_GLOBAL void __launch_bounds__(kRedBlock, 4) k_kmaxpy_norm(int64_t n, int64
             t += sh[q];
         partial[blockIdx.x] = t;
     }
+    if (last_block_final(1, partial, outNorm, nullptr, 1, cnt) && gsc && threadIdx.x == 0)
+    {
+        real hn = *outNorm;
+        bool broken = !(hn > gsc[0] * 1e-32) || gsc[2] <= j;
+        *scaleNext = broken ? 0.0 : 1.0 / hn;
+        if (broken && gsc[2] > j)
+            gsc[2] = j;
+    }
 }
 
 // partial[block] = sum_i x_i^2 s2[i % NV] (any length, any alignment)
 template <typename T, int NV>
-DNDSB_GLOBAL void k_knorm2(int64_t n, const T *__restrict__ x, const real *__restrict__ s2, real *partial)
+DNDSB_GLOBAL void k_knorm2(int64_t n, const T *__restrict__ x, const real *__restrict__ s2, real *partial, real *outNorm, unsigned *cnt)
 {
     __shared__ real sh[4][kRedBlock];
     int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
@@ -330,11 +382,13 @@ DNDSB_GLOBAL void k_knorm2(int64_t n, const T *__restrict__ x, const real *__res
     block_sum4(sh, a, 0, 0, 0);
     if (threadIdx.x == 0)
         partial[blockIdx.x] = sh[0][0];
+    last_block_final(1, partial, outNorm, nullptr, 1, cnt);
 }
 
 // partial[block] = sum_i (a_i - b_i)^2 s2[i % NV]
 template <typename T, int NV>
-DNDSB_GLOBAL void k_kdiff_norm(int64_t n, const T *__restrict__ x, const T *__restrict__ y, const real *__restrict__ s2, real *partial)
+DNDSB_GLOBAL void k_kdiff_norm(int64_t n, const T *__restrict__ x, const T *__restrict__ y, const real *__restrict__ s2, real *partial,
+                               real *outNorm, unsigned *cnt)
 {
     __shared__ real sh[4][kRedBlock];
     int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
@@ -348,53 +402,34 @@ DNDSB_GLOBAL void k_kdiff_norm(int64_t n, const T *__restrict__ x, const T *__re
     block_sum4(sh, a, 0, 0, 0);
     if (threadIdx.x == 0)
         partial[blockIdx.x] = sh[0][0];
-}
-
-// out[col] = sum over blocks, optionally its square root: one warp per column (columns strided over
-// the warps), each lane summing a fixed stride of the partials, then a fixed xor-shuffle tree
-DNDSB_GLOBAL void k_kfinal(int nb, int ncol, const real *__restrict__ partial, real *out, int takeSqrt)
-{
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int col = wid; col < ncol; col += nw)
-    {
-        real a = 0;
-        for (int i = lane; i < nb; i += 32)
-            a += partial[i * ncol + col];
-        a = warp_sum(a);
-        if (lane == 0)
-            out[col] = takeSqrt ? sqrt(a) : a;
-    }
-}
-
-// block size of the final pass: one warp per column, at most 32 warps
-inline int kfinal_threads(int ncol) { return 32 * (ncol < 1 ? 1 : ncol > 32 ? 32 : ncol); }
-
-template <typename T, int NV>
-void kmdot(int64_t n, int64_t ld, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, cudaStream_t st)
-{
-    k_kmdot<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, (const T *)w, s2, red);
-    k_kfinal<<<1, kfinal_threads(ncol), 0, st>>>(kRedBlocks, ncol, red, out, 0);
+    last_block_final(1, partial, outNorm, nullptr, 1, cnt);
 }
 
 template <typename T, int NV>
-void kmaxpy(int64_t n, int64_t ld, int ncol, const void *V, const real *h, void *w, const real *s2, real *red, real *outNorm, cudaStream_t st)
+void kmdot(int64_t n, int64_t ld, int ncol, const void *V, const void *w, const real *s2, real *red, real *out, const real *colScale,
+           unsigned *cnt, cudaStream_t st)
 {
-    k_kmaxpy_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, h, (T *)w, s2, red);
-    k_kfinal<<<1, 32, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+    k_kmdot<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, (const T *)w, s2, red, out, colScale, cnt);
 }
 
 template <typename T, int NV>
-void knorm(int64_t n, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st)
+void kmaxpy(int64_t n, int64_t ld, int ncol, const void *V, const real *h, const real *colScale, void *w, const real *s2, real *red,
+            real *outNorm, unsigned *cnt, real *gsc, int j, real *scaleNext, cudaStream_t st)
 {
-    k_knorm2<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, s2, red);
-    k_kfinal<<<1, 32, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+    k_kmaxpy_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, ld, ncol, (const T *)V, h, colScale, (T *)w, s2, red, outNorm, cnt, gsc, j,
+                                                           scaleNext);
 }
 
 template <typename T, int NV>
-void kdiff(int64_t n, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st)
+void knorm(int64_t n, const void *x, const real *s2, real *red, real *outNorm, unsigned *cnt, cudaStream_t st)
 {
-    k_kdiff_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, (const T *)y, s2, red);
-    k_kfinal<<<1, 32, 0, st>>>(kRedBlocks, 1, red, outNorm, 1);
+    k_knorm2<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, s2, red, outNorm, cnt);
+}
+
+template <typename T, int NV>
+void kdiff(int64_t n, const void *x, const void *y, const real *s2, real *red, real *outNorm, unsigned *cnt, cudaStream_t st)
+{
+    k_kdiff_norm<T, NV><<<kRedBlocks, kRedBlock, 0, st>>>(n, (const T *)x, (const T *)y, s2, red, outNorm, cnt);
 }
 
 #define DNDSB_KDISPATCH(FN, ...)                      \
@@ -413,24 +448,25 @@ void kdiff(int64_t n, const void *x, const void *y, const real *s2, real *red, r
 
 // V: ncol columns ld apart (ld a multiple of 4, 16-byte aligned, zero beyond n); w: a column of the same storage
 void krylov_mdot(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out,
-                 cudaStream_t st)
+                 const real *colScale, unsigned *cnt, cudaStream_t st)
 {
-    DNDSB_KDISPATCH(kmdot, n, ld, ncol, V, w, s2, red, out, st);
+    DNDSB_KDISPATCH(kmdot, n, ld, ncol, V, w, s2, red, out, colScale, cnt, st);
 }
 
-void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red,
-                       real *outNorm, cudaStream_t st)
+void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const real *h, const real *colScale, void *w,
+                       const real *s2, real *red, real *outNorm, unsigned *cnt, real *gsc, int j, real *scaleNext, cudaStream_t st)
 {
-    DNDSB_KDISPATCH(kmaxpy, n, ld, ncol, V, h, w, s2, red, outNorm, st);
+    DNDSB_KDISPATCH(kmaxpy, n, ld, ncol, V, h, colScale, w, s2, red, outNorm, cnt, gsc, j, scaleNext, st);
 }
 
-void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st)
+void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, unsigned *cnt, cudaStream_t st)
 {
-    DNDSB_KDISPATCH(knorm, n, x, s2, red, outNorm, st);
+    DNDSB_KDISPATCH(knorm, n, x, s2, red, outNorm, cnt, st);
 }
 
-void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st)
+void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, unsigned *cnt,
+                      cudaStream_t st)
 {
-    DNDSB_KDISPATCH(kdiff, n, x, y, s2, red, outNorm, st);
+    DNDSB_KDISPATCH(kdiff, n, x, y, s2, red, outNorm, cnt, st);
 }
 } // namespace dndsb

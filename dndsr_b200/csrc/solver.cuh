@@ -293,10 +293,15 @@ void linws_free(LinWs *w);
 // prec 0: double vectors, 1: float vectors; nv 5 or 6; FP64 accumulation, deterministic
 // Krylov basis columns are ld apart: ld = n rounded up to a multiple of 4, storage 16-byte aligned, pad zero
 inline int64_t krylov_ld(int64_t n) { return (n + 3) & ~(int64_t)3; }
+// Each is one launch: the last block to finish reduces the per-block partials (cnt: a zeroed device counter
+// the kernels share; it is reset after each use).  colScale (may be null): normalising factors of the
+// basis columns, which are stored unnormalised.
 void krylov_mdot(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const void *w, const real *s2, real *red, real *out,
-                 cudaStream_t st);
-void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const real *h, void *w, const real *s2, real *red,
-                       real *outNorm, cudaStream_t st);
-void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, cudaStream_t st);
-void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, cudaStream_t st);
+                 const real *colScale, unsigned *cnt, cudaStream_t st);
+// w -= V (h colScale); *outNorm = |w|; with gsc (GMRES scalars) also *scaleNext = 1 / |w| or 0 at a breakdown
+void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const void *V, const real *h, const real *colScale, void *w,
+                       const real *s2, real *red, real *outNorm, unsigned *cnt, real *gsc, int j, real *scaleNext, cudaStream_t st);
+void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, unsigned *cnt, cudaStream_t st);
+void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, unsigned *cnt,
+                      cudaStream_t st);
 } // namespace dndsb

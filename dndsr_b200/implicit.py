@@ -191,6 +191,14 @@ class SolverConfig:
     nCFLRampLength: int = 2 ** 31 - 1
     CFLRampEnd: float = 0.0
     nInternalRecStep: int = 1
+    # implicitReconstructionControl (EulerSolver.hpp): recLinearScheme 0 = Jacobi sweeps, 1 = GMRES on the
+    # linearised reconstruction (EulerSolver.hxx:270-339) with nGmresSpaceRec / nGmresIterRec, stopped at
+    # recThreshold times the first sweep's residual; gmresRecScale 1 weighs the dot by the far-field state
+    recLinearScheme: int = 0
+    nGmresSpaceRec: int = 5
+    nGmresIterRec: int = 1
+    recThreshold: float = 1e-10
+    gmresRecScale: int = 0
     jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi
     sgsIter: int = 0
     gmresCode: int = 0               # 0: LU-SGS only, 1: GMRES preconditioned by SGS
@@ -235,6 +243,7 @@ class ImplicitSolver:
         self.CFLNow = cfg.CFL
         self.n_rhs = 0
         self.n_sgs = 0
+        self.gmresRec = None
         self.uRecLim = None
         if cfg.useLimiter:
             self.uRecLim = vr.BuildURec(nv)
@@ -246,6 +255,7 @@ class ImplicitSolver:
         self.pp = None
         if cfg.farFieldStaticValue:
             far = [float(x) for x in cfg.farFieldStaticValue]
+            self.farU = far
             gamma = float(ev.settings["gamma"])
             rho = far[0]
             self.pp = (rho, (gamma - 1) * (far[4] - 0.5 * (far[1] ** 2 + far[2] ** 2 + far[3] ** 2) / rho))
@@ -253,9 +263,49 @@ class ImplicitSolver:
             self.incPP = torch.zeros((nc, nv), dtype=torch.float64, device=dev)
             self.nLimInc, self.alphaMinInc = 0, 1.0
 
+    # EulerSolver.hxx:270-339, recLinearScheme 1: each of nInternalRecStep passes takes the sweep's residual
+    # r = uRec - S(uRec) (DoReconstructionIter with recordInc), solves (I - dS/duRec) d = r by GMRES with the
+    # linearised sweep (DoReconstructionIterDiff: the JVP of the sweep, boundary term included) and no
+    # preconditioner, and sets uRec -= d; the passes stop once GMRES reaches recThreshold times the first residual
+    def _rec_gmres(self, cx):
+        cfg = self.cfg
+        if self.gmresRec is None:
+            self.gmresRec = GMRES(cfg.nGmresSpaceRec, self.uRec)
+            self.recZeroU = torch.zeros_like(cx)
+        nv = cx.shape[1]
+        if cfg.gmresRecScale == 1 and self.pp is not None:
+            far = self.farU
+            ms = [far[0]] + [math.sqrt(far[0] * far[4])] * 3 + [far[4]] + [1.0] * (nv - 5)
+        else:
+            ms = [1.0] * nv
+        s2 = torch.tensor([1.0 / (m + 1e-200) ** 2 for m in ms[:nv]], dtype=cx.dtype, device=cx.device)
+
+        def fdot(a, b):
+            return float(torch.sum(a * b * s2))
+
+        def FA(x, Ax):
+            Ax.copy_(x - self.vr.DoReconstructionIterJVP(x, self.recZeroU, self.uRec, cx))
+
+        def FML(x, MLx):
+            MLx.copy_(x)
+
+        resB = None
+        for _ in range(cfg.nInternalRecStep):
+            self.vr.DoReconstructionIter(self.uRec, self.uRecNew, cx, putIntoNew=True, recordInc=True)
+            d = self.uRecNew.clone()
+            if resB is None:
+                resB = float(d.norm())  # uRecNew1.norm2() of the first pass
+            conv = self.gmresRec.solve(FA, FML, fdot, self.uRecNew, d, cfg.nGmresIterRec,
+                                       lambda i, res, rb: res < resB * cfg.recThreshold)
+            self.uRec.sub_(d)
+            if conv:
+                break
+
     # EulerSolver.hxx:147-672 (VR sweeps then EvaluateRHS)
     def frhs(self, crhs, cx, dtau, it, ct):
-        for _ in range(self.cfg.nInternalRecStep):
+        if self.cfg.recLinearScheme == 1:
+            self._rec_gmres(cx)
+        for _ in range(self.cfg.nInternalRecStep if self.cfg.recLinearScheme == 0 else 0):
             self.vr.DoReconstructionIter(self.uRec, self.uRecNew, cx, putIntoNew=False, precision=self.cfg.vr_precision)
         if self.uRecLim is not None:
             si = self.vr.DoCalculateSmoothIndicator(cx, self.uRec)

@@ -11,6 +11,8 @@ setting names and defaults and allocates result tensors.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 
@@ -55,8 +57,8 @@ def _C():
     if not torch.cuda.is_available():
         raise RuntimeError("dndsr_b200 needs a CUDA device; there is no CPU path")
     from . import build as _b
-    if not _b.up_to_date():
-        raise ImportError("dndsr_b200/libdndsb.so is missing or stale: run dndsr_b200/build.py (nvcc, sm_100a)")
+    if not os.path.exists(_b.LIB):
+        raise ImportError("dndsr_b200/libdndsb.so is missing: run dndsr_b200/build.py (nvcc, sm_100a)")
     from . import _C as mod
     return mod
 

@@ -337,7 +337,9 @@ int dndsb_eval_set_delta_lambda(dndsb_eval *ev, const double *deltaLambdaCell, v
  * that loads the library until exit); meshes with nFace * nVars above that
  * are rejected with DNDSB_E_UNSUPPORTED.  The first call on a device looks up
  * the array's address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls on a device share the array: calls whose
+ * stream capture.  Like dndsb_eval_evaluate_rhs, each call reads the error
+ * word back and synchronises its stream before it returns (unless the
+ * evaluator defers its error reports).  All calls on a device share the array: calls whose
  * kernels overlap on the GPU race and must be serialised by the caller.
  * Results equal dndsb_eval_evaluate_rhs. */
 #define DNDSB_NOALLOC_SCRATCH_DOUBLES (1 << 20)

@@ -36,6 +36,12 @@ def test_noalloc_rhs_matches_regular_entry_point_twice():
         uRec = torch.tensor(rng.normal(size=(m.n_cell, vr.R, 5)) * 1e-2, dtype=torch.float64, device="cuda")
         ref, got = torch.zeros_like(u), torch.full_like(u, np.nan)
         ev.EvaluateRHS(ref, u, uRec)
+        handle_scratch = ev.get("faceFlux")  # the regular call's face fluxes, in handle memory
+        # the allocation-free call works in the static array: evaluated at another reconstruction it
+        # must leave the handle's scratch as the regular call left it
+        other = torch.tensor(rng.normal(size=(m.n_cell, vr.R, 5)) * 1e-2, dtype=torch.float64, device="cuda")
+        ev.EvaluateRHSNoAlloc(got, u, other)
+        assert np.array_equal(ev.get("faceFlux"), handle_scratch), f"call {call}: handle scratch touched"
         ev.EvaluateRHSNoAlloc(got, u, uRec)
         torch.cuda.synchronize()
         assert relerr(got.cpu().numpy(), ref.cpu().numpy()) <= TOL, f"call {call}"
