@@ -17,7 +17,8 @@ the adjoint (psi, lam) solves A^T (psi, lam) = g; the derivative of J with respe
 source s added to the residuals is then -<(psi, lam), s>, which the tangent solve A d = -s
 reproduces as <g, d> (dual consistency).
 
-Both systems are solved by right-preconditioned restarted GMRES on the device.  The u block
+Both systems are solved by right-preconditioned restarted (flexible) GMRES whose Arnoldi process runs on
+the device through the native Krylov reductions (``gmres``).  The u block
 is preconditioned by the scalar-Jacobian LU-SGS pair (primal) or its transpose (adjoint),
 the operator of LUSGSMatrixInit/UpdateSGS (EulerEvaluator.hxx:37-159, 550-693) at a pseudo
 time step of CFL ``cfl`` (the transposed sweeps optionally on FP32 vectors, ``precision="fp32"``,
@@ -32,68 +33,92 @@ import numpy as np
 import torch
 
 
-def _dot(a, b):
-    return float(sum(torch.sum(x * y) for x, y in zip(a, b)))
+def _krylov():
+    from .solver import _C
+    return _C()
 
 
-def _axpy(alpha, x, y):
-    return tuple(yi + alpha * xi for xi, yi in zip(x, y))
+def gmres(op, prec, b, restart=30, max_restarts=100, rtol=1e-10, check_every=5, info=None):
+    """Right-preconditioned restarted flexible GMRES for op(x) = b on tuples of FP64 CUDA tensors; x = prec(z).
 
+    The Arnoldi process runs on the device through the library's Krylov primitives (classical Gram-Schmidt
+    with the deterministic one-launch reductions of the native linear solver, least squares by Givens
+    rotations in a one-thread kernel), the preconditioned columns z_j are kept (so the preconditioner may vary,
+    e.g. FP32 sweeps), and the host reads the least-squares residual only every ``check_every`` Arnoldi steps
+    and at each restart.  Returns x and the relative residual norms (the least-squares estimate after every
+    Arnoldi step, the true residual at every restart); ``info`` (a dict) receives the number of Arnoldi
+    steps and of restarts."""
+    C = _krylov()
+    shapes = [t.shape for t in b]
+    sizes = [t.numel() for t in b]
+    n, k = sum(sizes), int(restart)
+    dev = b[0].device
+    f64 = dict(dtype=torch.float64, device=dev)
+    ld = C.krylov_ld(n)
+    V = torch.zeros((k + 1, ld), **f64)
+    Z = torch.zeros((k, ld), **f64)
+    H = torch.zeros(k * (k + 1), **f64)
+    gsc = torch.zeros(8 + k, **f64)
+    cs = torch.zeros(k + 1, **f64)
+    ones = torch.ones(k + 1, **f64)
+    work = torch.zeros(C.krylov_work_bytes(), dtype=torch.uint8, device=dev)
+    res = torch.zeros(k, **f64)
+    x = torch.zeros(ld, **f64)
 
-def gmres(op, prec, b, restart=30, max_restarts=100, rtol=1e-10):
-    """Right-preconditioned restarted GMRES (modified Gram-Schmidt, Givens rotations) for
-    op(x) = b on tuples of device tensors; x = prec(z).  Returns x and the relative residual
-    norm after every Arnoldi step."""
-    bnorm = math.sqrt(_dot(b, b))
-    x = tuple(torch.zeros_like(t) for t in b)
+    def split(vec):
+        out, o = [], 0
+        for shp, sz in zip(shapes, sizes):
+            out.append(vec[o:o + sz].view(shp))
+            o += sz
+        return tuple(out)
+
+    def put(dst, parts):
+        for d, p in zip(split(dst), parts):
+            d.copy_(p)
+
+    bflat = torch.zeros(n, **f64)
+    put(bflat, b)
+    bnorm = float(torch.linalg.vector_norm(bflat))
     hist = [1.0]
     if bnorm == 0.0:
-        return x, hist
+        return split(x[:n]), hist
+    r = torch.empty(n, **f64)
+    steps = 0
     for outer in range(max_restarts):
-        r = b if outer == 0 else _axpy(-1.0, op(x), b)
-        beta = math.sqrt(_dot(r, r))
+        if info is not None:
+            info.update(arnoldi_steps=steps, restarts=outer)
+        if outer == 0:
+            r.copy_(bflat)
+        else:
+            put(r, op(split(x[:n])))
+            torch.sub(bflat, r, out=r)
+        C.krylov_start(r, V, gsc, cs, work, k)
         if outer > 0:
+            beta = float(gsc[1])
             hist.append(beta / bnorm)
-        if beta <= rtol * bnorm:
-            break
-        V = [tuple(t / beta for t in r)]
-        Z = []
-        H = np.zeros((restart + 1, restart))
-        cs, sn = np.zeros(restart), np.zeros(restart)
-        g = np.zeros(restart + 1)
-        g[0] = beta
-        k = 0
-        for j in range(restart):
-            z = prec(V[j])
-            Z.append(z)
-            w = op(z)
-            for i in range(j + 1):
-                H[i, j] = _dot(w, V[i])
-                w = _axpy(-H[i, j], V[i], w)
-            H[j + 1, j] = math.sqrt(_dot(w, w))
-            V.append(tuple(t / H[j + 1, j] for t in w) if H[j + 1, j] > 0 else w)
-            for i in range(j):
-                t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
-                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
-                H[i, j] = t
-            d = math.hypot(H[j, j], H[j + 1, j])
-            cs[j], sn[j] = H[j, j] / d, H[j + 1, j] / d
-            H[j, j], H[j + 1, j] = d, 0.0
-            g[j + 1] = -sn[j] * g[j]
-            g[j] = cs[j] * g[j]
-            k = j + 1
-            hist.append(abs(g[j + 1]) / bnorm)
-            if abs(g[j + 1]) <= rtol * bnorm:
+            if beta <= rtol * bnorm:
                 break
-        y = np.linalg.solve(np.triu(H[:k, :k]), g[:k])
-        for i in range(k):
-            x = _axpy(float(y[i]), Z[i], x)
-        if hist[-1] <= rtol:
-            r = _axpy(-1.0, op(x), b)
-            hist.append(math.sqrt(_dot(r, r)) / bnorm)
-            if hist[-1] <= rtol:
-                break
-    return x, hist
+        done, nread = False, 0
+        for j in range(k):
+            z = prec(split(V[j, :n] * cs[j]))
+            put(Z[j, :n], z)
+            put(V[j + 1, :n], op(z))
+            C.krylov_arnoldi(n, j, k, V, H, cs, gsc, res[j:j + 1], work)
+            steps += 1
+            if (j + 1) % check_every == 0 or j == k - 1:
+                est = res[nread:j + 1].cpu().numpy() / bnorm
+                hist.extend(float(e) for e in est)
+                nread = j + 1
+                if est[-1] <= rtol:
+                    done = True
+                    break
+        C.krylov_update(n, k, Z, gsc, ones, x)
+        if info is not None:
+            info.update(arnoldi_steps=steps, restarts=outer + 1)
+        if done and outer == max_restarts - 1:
+            put(r, op(split(x[:n])))
+            hist.append(float(torch.linalg.vector_norm(bflat - r)) / bnorm)
+    return tuple(t.clone() for t in split(x[:n])), hist
 
 
 class SteadyAdjoint:
@@ -163,7 +188,7 @@ class SteadyAdjoint:
         return -self._sgs_pair(r[0], True), -self._neumann(r[1], True)
 
     def solve_adjoint(self, gU, gRec, **kw):
-        """(psi, lam) with A^T (psi, lam) = (gU, gRec), and the GMRES history."""
+        """(psi, lam) with A^T (psi, lam) = (gU, gRec), and the GMRES history (keyword arguments: ``gmres``'s)."""
         x, hist = gmres(self.op_T, self.prec_T, (gU.contiguous(), gRec.contiguous()), **kw)
         return x[0], x[1], hist
 

@@ -104,6 +104,7 @@ SIGNATURES = {
     "dndsb_vr_iter_jvp": [_P, _P, _P, _P, _P, _i, _P, _P],
     "dndsb_eval_rhs_vjp": [_P, _P, _P, _P, _P, _P, _P],
     "dndsb_eval_rhs_jvp": [_P, _P, _P, _P, _P, _P, _P],
+    "dndsb_eval_wall_flux_vjp": [_P, _D, _P, _P, _P, _P, _P],
     "dndsb_vr_iter_vjp_coords": [_P, _P, _P, _P, _i, _P, _P],
     "dndsb_vr_iter_jvp_coords": [_P, _P, _P, _P, _i, _P, _P],
     "dndsb_eval_rhs_vjp_coords": [_P, _P, _P, _P, _P, _P],
@@ -112,9 +113,15 @@ SIGNATURES = {
     "dndsb_eval_get_array": [_P, ctypes.c_char_p, _D, _l, _I64],
     "dndsb_eval_set_delta_lambda": [_P, _P, _P],
     "dndsb_eval_evaluate_rhs_noalloc": [_P, _P, _P, _P, _P],
+    "dndsb_krylov_ld": [_l],
+    "dndsb_krylov_work_bytes": [],
+    "dndsb_krylov_start": [_i, _l, _i, _P, _P, _P, _P, _P, _P],
+    "dndsb_krylov_arnoldi": [_i, _l, _i, _i, _P, _P, _P, _P, _P, _P, _P],
+    "dndsb_krylov_update": [_i, _l, _i, _P, _P, _P, _P, _P],
     "dndsb_last_error": [],
     "dndsb_version": [],
 }
+_RESTYPES = {"dndsb_last_error": ctypes.c_char_p, "dndsb_krylov_ld": ctypes.c_int64, "dndsb_krylov_work_bytes": ctypes.c_size_t}
 
 _lib = None
 
@@ -129,7 +136,7 @@ def load(require_device=True):
         for name, args in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_char_p if name == "dndsb_last_error" else ctypes.c_int
+            fn.restype = _RESTYPES.get(name, ctypes.c_int)
         _lib = L
     if require_device:
         import torch

@@ -11,7 +11,8 @@
 // and the transposed VR sweep gathers A^-1 B blocks of the neighbours through
 // the face-slot map.  The entropy-fix scale deltaLambdaCell is held fixed.
 // The viscous flux derivative is added by adjoint_visc.cu (boundary zones without a viscous
-// flux only).
+// flux only); the SA model and viscous boundary zones go to the forward-mode kernels of
+// adjoint_generic.cu.
 #include "solver.cuh"
 #include "basis_eval.cuh"
 #include "bc.cuh"
@@ -529,10 +530,15 @@ int rhs_jvp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const r
 
 int ensure_adj(const MeshD &m, const VRD &vr, EvalD &ev)
 {
-    if (ev.adjBuf)
-        return ST_OK;
     size_t n = (size_t)m.nFace * 2 * (vr.R + 1) * NV;
-    return dev_alloc((void **)&ev.adjBuf, sizeof(real) * n) == cudaSuccess ? ST_OK : ST_CUDA;
+    if (ev.adjBuf && ev.adjBufLen >= n)
+        return ST_OK;
+    dev_free(ev.adjBuf);
+    ev.adjBuf = nullptr;
+    if (dev_alloc((void **)&ev.adjBuf, sizeof(real) * n) != cudaSuccess)
+        return ST_CUDA;
+    ev.adjBufLen = n;
+    return ST_OK;
 }
 
 template <int DIM, int P>
@@ -557,8 +563,9 @@ int vr_jvp_dp(const MeshD &m, const GeomD &g, const VRD &vr, const real *dRec, c
 int rhs_vjp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *w, const real *u, const real *uRec, real *du, real *duRec,
             cudaStream_t st)
 {
+    // the SA model and viscous boundary zones: the forward-mode kernels of adjoint_generic.cu
     if (ev.s.nVars != NV || (!ev.s.ignoreVis && !vr.bnd.viscFree))
-        return ST_UNSUPPORTED;
+        return rhs_vjp_generic(m, g, vr, ev, w, nullptr, u, uRec, du, duRec, st);
     if (ensure_adj(m, vr, ev) != ST_OK)
         return ST_CUDA;
     dev_zero(ev.errWord, sizeof(int), st);
@@ -578,7 +585,7 @@ int rhs_jvp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real
             real *dRhs, cudaStream_t st)
 {
     if (ev.s.nVars != NV || (!ev.s.ignoreVis && !vr.bnd.viscFree))
-        return ST_UNSUPPORTED;
+        return rhs_jvp_generic(m, g, vr, ev, du, duRec, u, uRec, dRhs, st);
     if (ensure_adj(m, vr, ev) != ST_OK)
         return ST_CUDA;
     dev_zero(ev.errWord, sizeof(int), st);
@@ -597,7 +604,7 @@ int vr_vjp(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *v,
            cudaStream_t st)
 {
     if (nv != NV)
-        return ST_UNSUPPORTED;
+        return vr_vjp_generic(m, g, vr, nv, v, uRec, u, vRec, vU, st);
     auto run = [&]() { DNDSB_DP_DISPATCH(vr_vjp_dp, m, g, vr, v, uRec, u, vRec, vU, st); };
     int rc = run();
     if (rc != ST_OK)
@@ -609,7 +616,7 @@ int vr_jvp(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *dR
            real *dRecNew, cudaStream_t st)
 {
     if (nv != NV)
-        return ST_UNSUPPORTED;
+        return vr_jvp_generic(m, g, vr, nv, dRec, du, uRec, u, dRecNew, st);
     auto run = [&]() { DNDSB_DP_DISPATCH(vr_jvp_dp, m, g, vr, dRec, du, uRec, u, dRecNew, st); };
     int rc = run();
     if (rc != ST_OK)

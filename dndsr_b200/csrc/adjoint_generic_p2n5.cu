@@ -1,0 +1,4 @@
+// Instantiation unit of the generic derivative kernels: 3-D, VR degree 2, 5 variables.
+#include "adjoint_generic.cuh"
+
+DNDSB_GEN_INSTANTIATE_RHS(2, 5)

@@ -538,6 +538,7 @@ extern "C"
         rc |= dev_alloc((void **)&e->e.errWord, sizeof(int));
         rc |= dev_alloc((void **)&e->e.errDeferred, sizeof(int));
         rc |= dev_alloc((void **)&e->e.fluxWall, sizeof(real) * 8);
+        rc |= dev_alloc((void **)&e->e.objDir, sizeof(real) * 8);
         if (s->nVars == 6)
             rc |= dev_alloc((void **)&e->e.jSource, sizeof(real) * m.nCell * 6);
         if (rc)
@@ -592,7 +593,7 @@ extern "C"
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
                         (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource,
-                        (void *)e->e.errDeferred, (void *)e->e.fluxWall})
+                        (void *)e->e.errDeferred, (void *)e->e.fluxWall, (void *)e->e.objDir})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -681,10 +682,30 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp: VR not constructed");
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (e->e.s.nVars == 6 && !e->e.dWall)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_vjp: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
         int rc = rhs_vjp(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, w, u, uRec, du, duRec, S(stream));
         if (rc == ST_UNSUPPORTED)
-            return fail(rc, "dndsb_eval_rhs_vjp: needs nVars = 5 and ignoreVis (the viscous flux is not differentiated yet)");
+            return fail(rc, "dndsb_eval_rhs_vjp: the SA model and viscous boundary zones are differentiated on 3-D meshes at VR degree 1-2");
         return status_msg(rc, "dndsb_eval_rhs_vjp");
+    }
+
+    int dndsb_eval_wall_flux_vjp(dndsb_eval *e, const double *dirHost, const double *u, const double *uRec, double *du, double *duRec,
+                                 void *stream)
+    {
+        if (!e || !dirHost || !u || !uRec || !du || !duRec)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_wall_flux_vjp: null argument");
+        if (!e->vr->coeff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_wall_flux_vjp: VR not constructed");
+        if (e->vr->mesh->nBndFace == 0 || e->vr->vr.bnd.nZone == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_wall_flux_vjp: the mesh has no boundary table");
+        if (e->e.s.nVars == 6 && !e->e.dWall)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_wall_flux_vjp: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
+        h2d(e->e.objDir, dirHost, sizeof(real) * e->e.s.nVars, S(stream));
+        int rc = rhs_vjp_generic(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, nullptr, e->e.objDir, u, uRec, du, duRec, S(stream));
+        if (rc == ST_UNSUPPORTED)
+            return fail(rc, "dndsb_eval_wall_flux_vjp: needs a 3-D mesh and VR degree 1-2");
+        return status_msg(rc, "dndsb_eval_wall_flux_vjp");
     }
 
     int dndsb_eval_rhs_vjp_coords(dndsb_eval *e, const double *w, const double *u, const double *uRec, double *dX, void *stream)
@@ -747,9 +768,11 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp: VR not constructed");
         if (e->vr->mesh->nBndFace > 0 && e->vr->vr.bnd.nZone == 0)
             return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp: the mesh has boundary faces; call dndsb_eval_set_bc first");
+        if (e->e.s.nVars == 6 && !e->e.dWall)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_rhs_jvp: the SA model needs the wall distance (dndsb_eval_set_wall_distance)");
         int rc = rhs_jvp(e->vr->mesh->d, e->vr->g, e->vr->vr, e->e, du, duRec, u, uRec, dRhs, S(stream));
         if (rc == ST_UNSUPPORTED)
-            return fail(rc, "dndsb_eval_rhs_jvp: needs nVars = 5 and ignoreVis (the viscous flux is not differentiated yet)");
+            return fail(rc, "dndsb_eval_rhs_jvp: the SA model and viscous boundary zones are differentiated on 3-D meshes at VR degree 1-2");
         return status_msg(rc, "dndsb_eval_rhs_jvp");
     }
 
@@ -936,6 +959,40 @@ extern "C"
         if (rc == ST_BADARG)
             return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..1, nGmresSpace 1..32, precision 0..1");
         return status_msg(rc, "dndsb_eval_solve_linear");
+    }
+
+    int64_t dndsb_krylov_ld(int64_t n) { return krylov_ld(n); }
+    size_t dndsb_krylov_work_bytes(void) { return krylov_work_bytes(); }
+
+    int dndsb_krylov_start(int precision, int64_t n, int k, const void *r, void *V, double *gsc, double *colScale, void *work, void *stream)
+    {
+        if (!r || !V || !gsc || !colScale || !work)
+            return fail(DNDSB_E_BADARG, "dndsb_krylov_start: null argument");
+        int rc = krylov_start(precision, n, k, r, V, gsc, colScale, work, S(stream));
+        if (rc == ST_BADARG)
+            return fail(DNDSB_E_BADARG, "dndsb_krylov_start: n > 0, 1 <= k <= 32, precision 0..1");
+        return status_msg(rc, "dndsb_krylov_start");
+    }
+
+    int dndsb_krylov_arnoldi(int precision, int64_t n, int j, int k, void *V, double *H, double *colScale, double *gsc, double *res, void *work,
+                             void *stream)
+    {
+        if (!V || !H || !colScale || !gsc || !work)
+            return fail(DNDSB_E_BADARG, "dndsb_krylov_arnoldi: null argument");
+        int rc = krylov_arnoldi(precision, n, j, k, V, H, colScale, gsc, res, work, S(stream));
+        if (rc == ST_BADARG)
+            return fail(DNDSB_E_BADARG, "dndsb_krylov_arnoldi: n > 0, 1 <= k <= 32, 0 <= j < k, precision 0..1");
+        return status_msg(rc, "dndsb_krylov_arnoldi");
+    }
+
+    int dndsb_krylov_update(int precision, int64_t n, int k, const void *V, const double *gsc, const double *colScale, void *x, void *stream)
+    {
+        if (!V || !gsc || !colScale || !x)
+            return fail(DNDSB_E_BADARG, "dndsb_krylov_update: null argument");
+        int rc = krylov_update(precision, n, k, V, gsc, colScale, x, S(stream));
+        if (rc == ST_BADARG)
+            return fail(DNDSB_E_BADARG, "dndsb_krylov_update: n > 0, 1 <= k <= 32, precision 0..1");
+        return status_msg(rc, "dndsb_krylov_update");
     }
 
     int dndsb_eval_evaluate_norm(dndsb_eval *e, const double *x, int P, int volWise, double *resHost, void *stream)

@@ -10,10 +10,13 @@
 namespace dndsb
 {
 // keep the plain-real overloads visible next to the Dual ones below
+using ::exp;
 using ::fabs;
-using ::pow;
 using ::isfinite;
+using ::log;
+using ::pow;
 using ::sqrt;
+using ::tanh;
 
 template <int N>
 struct Dual
@@ -191,11 +194,49 @@ DNDSB_HD Dual<N> pow(const Dual<N> &a, real e)
 }
 template <int N>
 DNDSB_HD bool isfinite(const Dual<N> &a) { return ::isfinite(a.v); }
+// the elementary functions of the SA model
+template <int N>
+DNDSB_HD Dual<N> exp(const Dual<N> &a)
+{
+    Dual<N> r;
+    r.v = ::exp(a.v);
+    for (int i = 0; i < N; i++)
+        r.d[i] = r.v * a.d[i];
+    return r;
+}
+template <int N>
+DNDSB_HD Dual<N> log(const Dual<N> &a)
+{
+    Dual<N> r;
+    r.v = ::log(a.v);
+    real s = 1.0 / a.v;
+    for (int i = 0; i < N; i++)
+        r.d[i] = s * a.d[i];
+    return r;
+}
+template <int N>
+DNDSB_HD Dual<N> tanh(const Dual<N> &a)
+{
+    Dual<N> r;
+    r.v = ::tanh(a.v);
+    real s = 1.0 - r.v * r.v;
+    for (int i = 0; i < N; i++)
+        r.d[i] = s * a.d[i];
+    return r;
+}
 
 template <int N>
 DNDSB_HD Dual<N> dmax(const Dual<N> &a, const Dual<N> &b) { return a.v > b.v ? a : b; }
 template <int N>
 DNDSB_HD Dual<N> dmin(const Dual<N> &a, const Dual<N> &b) { return a.v < b.v ? a : b; }
+template <int N>
+DNDSB_HD Dual<N> dmax(const Dual<N> &a, real b) { return a.v > b ? a : Dual<N>(b); }
+template <int N>
+DNDSB_HD Dual<N> dmax(real a, const Dual<N> &b) { return a > b.v ? Dual<N>(a) : b; }
+template <int N>
+DNDSB_HD Dual<N> dmin(const Dual<N> &a, real b) { return a.v < b ? a : Dual<N>(b); }
+template <int N>
+DNDSB_HD Dual<N> dmin(real a, const Dual<N> &b) { return a < b.v ? Dual<N>(a) : b; }
 
 // value of a real or a dual number
 DNDSB_HD real value_of(real x) { return x; }

@@ -230,14 +230,17 @@ DNDSB_GLOBAL void k_gmres_v0(int64_t n, const T *__restrict__ w, const T *__rest
 }
 
 // least squares  min |beta e1 - H y|  by Givens rotations on the Hessenberg
-// (HardEigen::EigenLeastSquareSolve on the (j+1) x j leading block)
-DNDSB_GLOBAL void k_gmres_lsq(int k, const real *H, real *sc)
+// (HardEigen::EigenLeastSquareSolve on the (j+1) x j leading block), over the valid columns and at most
+// ncolMax of them; res (may be null): the norm of the least-squares residual, |beta e1 - H y|
+DNDSB_GLOBAL void k_gmres_lsq(int k, const real *H, real *sc, int ncolMax, real *res)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0)
         return;
     int nv = (int)sc[2];
     if (nv > k)
         nv = k;
+    if (nv > ncolMax)
+        nv = ncolMax;
     real R[33 * 32];
     real gv[33];
     for (int i = 0; i <= nv; i++)
@@ -273,6 +276,8 @@ DNDSB_GLOBAL void k_gmres_lsq(int k, const real *H, real *sc)
     }
     for (int jj = nv; jj < k; jj++)
         sc[kScY + jj] = 0;
+    if (res)
+        *res = fabs(gv[nv]);
 }
 
 // x += sum_i y_i v_i over the valid columns (v_i = colScale_i times the stored column)
@@ -297,6 +302,21 @@ DNDSB_GLOBAL void k_gmres_reset(real *sc, int k, real *colScale)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         sc[2] = k, colScale[0] = 1.0;
+}
+
+// scalars of a caller-driven Arnoldi cycle: weights of the plain dot, k columns valid, column 0 stored normalised
+DNDSB_GLOBAL void k_krylov_begin(real *s2, unsigned *cnt, real *gsc, int k, real *colScale)
+{
+    if (blockIdx.x == 0 && threadIdx.x < 8)
+        s2[threadIdx.x] = 1.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *cnt = 0, gsc[2] = k, colScale[0] = 1.0;
+}
+
+DNDSB_GLOBAL void k_krylov_scale(real *gsc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        gsc[0] = gsc[1];
 }
 
 DNDSB_GLOBAL void k_copy_scalar(const real *a, real *b)
@@ -493,7 +513,7 @@ struct Solve
                 krylov_maxpy_norm(prec(), nn, ld(), NV, j + 1, w.V, hcol, w.colScale, V(j + 1), w.s2, w.red, hcol + j + 1, w.cnt, w.sc, j,
                                   w.colScale + j + 1, st);
             }
-            DNDSB_LAUNCH(k_gmres_lsq, 1, 32, st, k, w.H, w.sc);
+            DNDSB_LAUNCH(k_gmres_lsq, 1, 32, st, k, w.H, w.sc, k, (real *)nullptr);
             DNDSB_LAUNCH(k_gmres_update<T>, nn, 256, st, nn, ld(), k, (const T *)w.V, w.sc, w.colScale, x);
             xZero = false;
         }
@@ -589,5 +609,72 @@ int linear_solve(const MeshD &m, const GeomD &g, EvalD &ev, LinWs *&ws, const Li
         return ls.precision ? run_nf<float, 6>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
                             : run_nf<double, 6>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
     return ST_UNSUPPORTED;
+}
+
+// ---- caller-driven Arnoldi process: the same reductions for an operator applied outside the library ----
+// work: [red: kRedBufLenK doubles][s2: 8 doubles][cnt]
+size_t krylov_work_bytes() { return sizeof(real) * (kRedBufLenK + 8) + 64; }
+
+namespace
+{
+struct KWork
+{
+    real *red, *s2;
+    unsigned *cnt;
+    explicit KWork(void *w) : red((real *)w), s2((real *)w + kRedBufLenK), cnt((unsigned *)((real *)w + kRedBufLenK + 8)) {}
+};
+
+template <typename T>
+void kstart(int64_t n, int k, const void *r, void *V, real *gsc, real *colScale, void *work, cudaStream_t st)
+{
+    KWork kw(work);
+    const int prec = sizeof(T) == 4 ? 1 : 0;
+    DNDSB_LAUNCH(k_krylov_begin, 1, 32, st, kw.s2, kw.cnt, gsc, k, colScale);
+    krylov_norm(prec, n, 5, r, kw.s2, kw.red, gsc + 1, kw.cnt, st);
+    DNDSB_LAUNCH(k_krylov_scale, 1, 32, st, gsc);
+    DNDSB_LAUNCH(k_gmres_v0<T>, n, 256, st, n, (const T *)nullptr, (const T *)r, (T *)V, gsc, 1);
+}
+
+template <typename T>
+void kupdate(int64_t n, int k, const void *V, const real *gsc, const real *colScale, void *x, cudaStream_t st)
+{
+    DNDSB_LAUNCH(k_gmres_update<T>, n, 256, st, n, krylov_ld(n), k, (const T *)V, gsc, colScale, (T *)x);
+}
+} // namespace
+
+int krylov_start(int prec, int64_t n, int k, const void *r, void *V, real *gsc, real *colScale, void *work, cudaStream_t st)
+{
+    if (n <= 0 || k < 1 || k > 32 || prec < 0 || prec > 1)
+        return ST_BADARG;
+    if (prec)
+        kstart<float>(n, k, r, V, gsc, colScale, work, st);
+    else
+        kstart<double>(n, k, r, V, gsc, colScale, work, st);
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int krylov_arnoldi(int prec, int64_t n, int j, int k, void *V, real *H, real *colScale, real *gsc, real *res, void *work, cudaStream_t st)
+{
+    if (n <= 0 || k < 1 || k > 32 || j < 0 || j >= k || prec < 0 || prec > 1)
+        return ST_BADARG;
+    KWork kw(work);
+    const int64_t ld = krylov_ld(n);
+    real *hcol = H + (int64_t)j * (k + 1);
+    void *w = (char *)V + (int64_t)(j + 1) * ld * (prec ? 4 : 8);
+    krylov_mdot(prec, n, ld, 5, j + 1, V, w, kw.s2, kw.red, hcol, colScale, kw.cnt, st);
+    krylov_maxpy_norm(prec, n, ld, 5, j + 1, V, hcol, colScale, w, kw.s2, kw.red, hcol + j + 1, kw.cnt, gsc, j, colScale + j + 1, st);
+    DNDSB_LAUNCH(k_gmres_lsq, 1, 32, st, k, H, gsc, j + 1, res);
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int krylov_update(int prec, int64_t n, int k, const void *V, const real *gsc, const real *colScale, void *x, cudaStream_t st)
+{
+    if (n <= 0 || k < 1 || k > 32 || prec < 0 || prec > 1)
+        return ST_BADARG;
+    if (prec)
+        kupdate<float>(n, k, V, gsc, colScale, x, st);
+    else
+        kupdate<double>(n, k, V, gsc, colScale, x, st);
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 } // namespace dndsb

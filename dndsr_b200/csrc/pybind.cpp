@@ -52,6 +52,25 @@ void *dptr(const py::object &t, const char *name, bool fp32 = false, bool nullab
 double *dp(const py::object &t, const char *name) { return static_cast<double *>(dptr(t, name)); }
 double *dpn(const py::object &t, const char *name) { return static_cast<double *>(dptr(t, name, false, true)); }
 
+// data pointer of any contiguous CUDA tensor
+void *anyptr(const py::object &t, const char *name)
+{
+    if (t.is_none() || !py::hasattr(t, "data_ptr") || !t.attr("is_cuda").cast<bool>() || !t.attr("is_contiguous")().cast<bool>())
+        throw py::value_error(std::string(name) + " must be a contiguous CUDA tensor");
+    return reinterpret_cast<void *>(t.attr("data_ptr")().cast<uintptr_t>());
+}
+
+// 0 for a float64 tensor, 1 for float32
+int precision_of(const py::object &t)
+{
+    std::string d = py::str(t.attr("dtype")).cast<std::string>();
+    if (d == "torch.float64")
+        return 0;
+    if (d == "torch.float32")
+        return 1;
+    throw py::value_error("Krylov vectors must be float64 or float32");
+}
+
 void *stream()
 {
     static py::object cur = py::module_::import("torch").attr("cuda").attr("current_stream");
@@ -228,6 +247,10 @@ struct Eval
     {
         ck(dndsb_eval_rhs_vjp(h, dp(w, "w"), dp(u, "u"), dp(uRec, "uRec"), dp(du, "du"), dp(duRec, "duRec"), stream()));
     }
+    void WallFluxVJP(Arr<double> dir, py::object u, py::object uRec, py::object du, py::object duRec)
+    {
+        ck(dndsb_eval_wall_flux_vjp(h, dir.data(), dp(u, "u"), dp(uRec, "uRec"), dp(du, "du"), dp(duRec, "duRec"), stream()));
+    }
     void RhsJVP(py::object du, py::object duRec, py::object u, py::object uRec, py::object out)
     {
         ck(dndsb_eval_rhs_jvp(h, dp(du, "du"), dp(duRec, "duRec"), dp(u, "u"), dp(uRec, "uRec"), dp(out, "dRhs"), stream()));
@@ -352,6 +375,28 @@ PYBIND11_MODULE(_C, m)
     m.doc() = "B200 implementation of DNDSR's implicit residual path: mesh, variational reconstruction and Euler "
               "evaluator handles over the C-ABI of include/dndsb.h";
     m.def("version", &dndsb_version);
+    // device Krylov primitives of a caller-driven GMRES (include/dndsb.h); V [k+1][krylov_ld(n)] zero-filled
+    m.def("krylov_ld", &dndsb_krylov_ld);
+    m.def("krylov_work_bytes", &dndsb_krylov_work_bytes);
+    m.def("krylov_start",
+          [](py::object r, py::object V, py::object gsc, py::object colScale, py::object work, int k)
+          {
+              const int prec = precision_of(V);
+              ck(dndsb_krylov_start(prec, r.attr("numel")().cast<int64_t>(), k, dptr(r, "r", prec == 1), anyptr(V, "V"), dp(gsc, "gsc"),
+                                    dp(colScale, "colScale"), anyptr(work, "work"), stream()));
+          });
+    m.def("krylov_arnoldi",
+          [](int64_t n, int j, int k, py::object V, py::object H, py::object colScale, py::object gsc, py::object res, py::object work)
+          {
+              ck(dndsb_krylov_arnoldi(precision_of(V), n, j, k, anyptr(V, "V"), dp(H, "H"), dp(colScale, "colScale"), dp(gsc, "gsc"),
+                                      dpn(res, "res"), anyptr(work, "work"), stream()));
+          });
+    m.def("krylov_update",
+          [](int64_t n, int k, py::object V, py::object gsc, py::object colScale, py::object x)
+          {
+              const int prec = precision_of(V);
+              ck(dndsb_krylov_update(prec, n, k, anyptr(V, "V"), dp(gsc, "gsc"), dp(colScale, "colScale"), dptr(x, "x", prec == 1), stream()));
+          });
     py::class_<Mesh>(m, "Mesh")
         .def(py::init<int, int, int, Arr<double>, Arr<int64_t>, Arr<double>, Arr<int64_t>, Arr<double>, Arr<int64_t>, Arr<int32_t>,
                       Arr<double>, Arr<int64_t>>(),
@@ -391,6 +436,7 @@ PYBIND11_MODULE(_C, m)
         .def("CheckErrors", &Eval::CheckErrors)
         .def("EvaluateRHSVJP", &Eval::RhsVJP)
         .def("EvaluateRHSJVP", &Eval::RhsJVP)
+        .def("WallFluxVJP", &Eval::WallFluxVJP)
         .def("EvaluateRHSVJPCoords", &Eval::RhsVJPCoords)
         .def("ResidualVJPCoords", &Eval::ResidualVJPCoords)
         .def("EvaluateRHSJVPCoords", &Eval::RhsJVPCoords)

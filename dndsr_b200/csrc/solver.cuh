@@ -148,9 +148,11 @@ struct EvalD
     real *cellPar = nullptr;  // [nCell][6]: centre, 1/L
     real *redBuf = nullptr;   // scratch for reductions
     real *adjBuf = nullptr;   // scratch of the derivative kernels [nFace][2][(R+1) nv], allocated on first use
+    size_t adjBufLen = 0;     // its length in reals
     real *dWall = nullptr;    // SA: wall distance at the cell Gauss points [nCell][nGc]
     real *jSource = nullptr;  // SA: source-term Jacobian diagonal of the last RHS [nCell][nv]
     real *fluxWall = nullptr; // wall-flux integral of the last RHS [8] (EvaluateRHS.hxx:599-607 fluxWallSum)
+    real *objDir = nullptr;   // [8] direction of the wall-flux objective of dndsb_eval_wall_flux_vjp
     int *errWord = nullptr;   // device error word
     int *errDeferred = nullptr; // error word of EvaluateRHS in deferred mode (read and cleared on request)
     bool deferErr = false;    // EvaluateRHS skips its per-call read-back of the error word
@@ -273,6 +275,16 @@ int vr_vjp(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *v,
            cudaStream_t st);
 int vr_jvp(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *dRec, const real *du, const real *uRec, const real *u,
            real *dRecNew, cudaStream_t st);
+// forward-mode derivatives for the SA model and viscous boundary zones (adjoint_generic.cu; 3-D, VR degree 1-2);
+// rhs_vjp_generic with objDir != nullptr: the gradient of the wall-flux integral along objDir [nVars]
+int rhs_vjp_generic(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *w, const real *objDir, const real *u, const real *uRec,
+                    real *du, real *duRec, cudaStream_t st);
+int rhs_jvp_generic(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *du, const real *duRec, const real *u, const real *uRec,
+                    real *dRhs, cudaStream_t st);
+int vr_vjp_generic(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *v, const real *uRec, const real *u, real *vRec, real *vU,
+                   cudaStream_t st);
+int vr_jvp_generic(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *dRec, const real *du, const real *uRec, const real *u,
+                   real *dRecNew, cudaStream_t st);
 
 // ---- native linear solve (linsolve.cu) and its Krylov reductions (reduce.cu) ----
 struct LinSettings
@@ -304,4 +316,14 @@ void krylov_maxpy_norm(int prec, int64_t n, int64_t ld, int nv, int ncol, const 
 void krylov_norm(int prec, int64_t n, int nv, const void *x, const real *s2, real *red, real *outNorm, unsigned *cnt, cudaStream_t st);
 void krylov_diff_norm(int prec, int64_t n, int nv, const void *x, const void *y, const real *s2, real *red, real *outNorm, unsigned *cnt,
                       cudaStream_t st);
+// A caller-driven Arnoldi process (linsolve.cu): V holds k + 1 columns krylov_ld(n) apart (zero beyond n),
+// H k columns of k + 1, gsc the GMRES scalars ([0] breakdown scale, [1] beta, [2] valid columns, [8...] y),
+// work krylov_work_bytes() bytes zeroed before the first use.
+// start: beta = |r|, V0 = r / beta.  arnoldi: column j + 1 of V holds the operator applied to column j; it is
+// orthogonalised (H column j, colScale[j + 1]) and the least squares on j + 1 columns solved (y, *res = its
+// residual norm).  update: x += sum_i y_i colScale_i V_i.
+size_t krylov_work_bytes();
+int krylov_start(int prec, int64_t n, int k, const void *r, void *V, real *gsc, real *colScale, void *work, cudaStream_t st);
+int krylov_arnoldi(int prec, int64_t n, int j, int k, void *V, real *H, real *colScale, real *gsc, real *res, void *work, cudaStream_t st);
+int krylov_update(int prec, int64_t n, int k, const void *V, const real *gsc, const real *colScale, void *x, cudaStream_t st);
 } // namespace dndsb

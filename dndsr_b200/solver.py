@@ -238,6 +238,14 @@ class EulerEvaluator:
         self._c.EvaluateRHSVJP(w, u, uRec, du, duRec)
         return du, duRec
 
+    def WallFluxVJP(self, direction, u, uRec):
+        """(dJ/du, dJ/duRec) of the wall-flux integral J = direction . fluxWallSum (EvaluateRHS.hxx:599-607; the x
+        force on the walls for direction (0, 1, 0, 0, 0[, 0])), deltaLambdaCell held fixed.  J itself is
+        direction . get("fluxWallSum") after an EvaluateRHS at (u, uRec)."""
+        du, duRec = torch.empty_like(u), torch.empty_like(uRec)
+        self._c.WallFluxVJP(np.ascontiguousarray(direction, dtype=np.float64), u, uRec, du, duRec)
+        return du, duRec
+
     def EvaluateRHSJVP(self, du, duRec, u, uRec):
         """dR/du du + dR/duRec duRec of EvaluateRHS at (u, uRec), deltaLambdaCell held fixed."""
         out = torch.empty_like(u)

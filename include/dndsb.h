@@ -261,11 +261,22 @@ int dndsb_eval_add_fixed_increment(dndsb_eval *ev, double *u, const double *inc,
 
 /* Derivatives of EvaluateRHS (EulerEvaluator_EvaluateRHS.hxx:55-818) with respect to the cell
  * means u and the reconstruction uRec, at the deltaLambdaCell of the last evaluate_dt (held
- * fixed): vjp: w [nCell][5] -> du = (dR/du)^T w, duRec = (dR/duRec)^T w; jvp: (du, duRec) -> dRhs.
- * Inviscid (ignoreVis) 5-variable models; Gauss-point states are recomputed, not stored.  The
- * reference has no hand-written adjoint of this path (its Python package differentiates nothing). */
+ * fixed): vjp: w [nCell][nVars] -> du = (dR/du)^T w, duRec = (dR/duRec)^T w; jvp: (du, duRec) -> dRhs.
+ * Euler and Navier-Stokes (5 variables) through the inviscid, viscous and boundary fluxes; the SA
+ * model (6 variables: SA convective and diffusion fluxes, eddy viscosity, source term) and boundary
+ * zones with a viscous flux on 3-D meshes at VR degree 1-2.  Gauss-point states are recomputed, not
+ * stored.  The reference has no hand-written adjoint of this path (its Python package differentiates
+ * nothing). */
 int dndsb_eval_rhs_vjp(dndsb_eval *ev, const double *w, const double *u, const double *uRec, double *du, double *duRec, void *stream);
 int dndsb_eval_rhs_jvp(dndsb_eval *ev, const double *du, const double *duRec, const double *u, const double *uRec, double *dRhs, void *stream);
+/* Gradient of the wall-flux integral along dirHost [nVars] (host array): J = dir . fluxWallSum, the
+ * integral EvaluateRHS records (EulerEvaluator_EvaluateRHS.hxx:599-607: minus the face fluxes of the
+ * BCWall / BCWallIsothermal faces, and of BCWallInvis faces when muGas < 1e-99).  dir = (0, 1, 0, 0, 0 ...)
+ * gives the x force on the walls: pressure and skin friction, with the SA eddy viscosity for 6 variables.
+ * du [nCell][nVars], duRec [nCell][R][nVars] receive dJ/du, dJ/duRec (deltaLambdaCell held fixed).
+ * 3-D meshes, VR degree 1-2. */
+int dndsb_eval_wall_flux_vjp(dndsb_eval *ev, const double *dirHost, const double *u, const double *uRec, double *du, double *duRec,
+                             void *stream);
 /* Derivatives of EvaluateRHS with respect to the mesh node coordinates X [nNode][3] (u, uRec and
  * deltaLambdaCell held fixed; geometry, basis and face points, normals and Jacobians recomputed per
  * cell in dual numbers): vjp: w [nCell][5] -> dX = (dR/dX)^T w; jvp: dX -> dRhs.  Inviscid
@@ -344,6 +355,30 @@ int dndsb_eval_set_delta_lambda(dndsb_eval *ev, const double *deltaLambdaCell, v
  * Results equal dndsb_eval_evaluate_rhs. */
 #define DNDSB_NOALLOC_SCRATCH_DOUBLES (1 << 20)
 int dndsb_eval_evaluate_rhs_noalloc(dndsb_eval *ev, double *rhs, const double *u, const double *uRec, void *stream);
+
+/* Device Krylov primitives for a caller-driven, right-preconditioned restarted GMRES whose operator and
+ * preconditioner are applied outside the library (the adjoint and tangent solves of the coupled
+ * residual; no reference counterpart, the reference's GMRES_LeftPreconditioned::solve,
+ * Solver/Linear.hpp:46-133, takes its operator as a callback).  The same one-launch deterministic
+ * reductions as dndsb_eval_solve_linear's GMRES, FP64 accumulation; no call synchronises.
+ * precision 0: double vectors, 1: float vectors.  V: k + 1 columns (1 <= k <= 32) of
+ * dndsb_krylov_ld(n) elements, 16-byte aligned, zero beyond n; H: k columns of k + 1 doubles;
+ * colScale: k + 1 doubles (the normalising factors of the stored, unnormalised columns);
+ * gsc: 8 + k doubles ([1] beta, [2] valid columns, [8 ...] least-squares y); work:
+ * dndsb_krylov_work_bytes() bytes, zero-filled before its first use.  One cycle: start, then for
+ * j = 0 .. k-1 the caller writes A M (colScale[j] V_j) into column j + 1 and calls arnoldi, then
+ * update gives the correction t = V y to which the caller applies M. */
+int64_t dndsb_krylov_ld(int64_t n);
+size_t dndsb_krylov_work_bytes(void);
+/* beta = |r| (gsc[1]); column 0 = r / beta */
+int dndsb_krylov_start(int precision, int64_t n, int k, const void *r, void *V, double *gsc, double *colScale, void *work, void *stream);
+/* orthogonalises column j + 1 against columns 0..j (classical Gram-Schmidt: H column j, colScale[j + 1];
+ * a breakdown drops the column), then solves the least squares on j + 1 columns: y in gsc, *res = its
+ * residual norm (device) */
+int dndsb_krylov_arnoldi(int precision, int64_t n, int j, int k, void *V, double *H, double *colScale, double *gsc, double *res, void *work,
+                         void *stream);
+/* x += sum_i y_i colScale_i V_i over the columns of the last least squares */
+int dndsb_krylov_update(int precision, int64_t n, int k, const void *V, const double *gsc, const double *colScale, void *x, void *stream);
 
 const char *dndsb_last_error(void);
 int dndsb_version(void);

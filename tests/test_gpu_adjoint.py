@@ -120,16 +120,17 @@ def test_autograd_through_sweeps_and_rhs():
         assert abs(adj - fd) < 1e-6 * abs(fd)
 
 
-def test_viscous_wall_vjp_is_reported_unsupported():
+def test_sa_vjp_without_wall_distance_is_reported_unsupported():
     from dndsr_b200.capi import DndsbError
     from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
-    m = M.bump_channel_tet(4, 2, 2)
-    o, far, types, vals, w = bump_oracle(m, 1, "Roe", 0.0, 1)
-    types[M.BUMP_ZONES["bump"]] = 2  # BCWall: a viscous flux on boundary faces, not differentiated
+    from tests.plate_case import plate_bc, plate_state
+    m = M.flat_plate_hex(6, 4, 3, y1=1e-3, growth=1.3)
+    far, mu = plate_state()
+    types, vals, w = plate_bc(far)
     vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1)).construct(w)
-    ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType="Roe", muGas=1e-3, muModel=0))
-    ev.SetBC(types, vals)
-    u, uRec = vr.BuildUDof(5), vr.BuildURec(5)
+    ev = EulerEvaluator(vr, dict(nVars=6, riemannSolverType="Roe", muGas=mu, muModel=0, prGas=0.72))
+    ev.SetBC(types, vals)  # the SA source needs the wall distance, which was never set
+    u, uRec = vr.BuildUDof(6), vr.BuildURec(6)
     u[:] = torch.tensor(far, device="cuda")
     with pytest.raises(DndsbError):
         ev.EvaluateRHSVJP(torch.ones_like(u), u, uRec)
