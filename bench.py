@@ -501,7 +501,7 @@ def tgv_vjp_cost(args):
 
 def adjoint_solve(vr, ev, u, uRec, far, mesh, ms_primal):
     """Adjoint of the pressure drag on the bump for the coupled (EvaluateRHS, VR sweep) residual of one
-    implicit Euler step (dt = 5 local CFL-1 steps) at a smooth non-uniform state: GMRES(40) preconditioned
+    implicit Euler step (dt = 5 local CFL-1 steps) at a smooth non-uniform state: GMRES(32) preconditioned
     by the transposed LU-SGS pair (FP64, then on FP32 vectors) and a 4-term Neumann series of the
     transposed sweep, to a 1e-10 drop."""
     import torch
@@ -521,11 +521,11 @@ def adjoint_solve(vr, ev, u, uRec, far, mesh, ms_primal):
     out = {"objective": "pressure drag on the bump", "J": J}
     for prec in ("fp64", "fp32"):
         adj = SteadyAdjoint(vr, ev, us, ur, cfl=5.0, dt=5.0 * float(dTau.max()), precision=prec)
-        adj.solve_adjoint(gU, gR, restart=40, max_restarts=1, rtol=1e-10)  # warm-up
+        adj.solve_adjoint(gU, gR, restart=32, max_restarts=1, rtol=1e-10)  # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         info = {}
-        psi, lam, hist = adj.solve_adjoint(gU, gR, restart=40, max_restarts=40, rtol=1e-10, info=info)
+        psi, lam, hist = adj.solve_adjoint(gU, gR, restart=32, max_restarts=40, rtol=1e-10, info=info)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
         key = "" if prec == "fp64" else "_fp32_preconditioner"

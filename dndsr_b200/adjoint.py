@@ -48,6 +48,8 @@ def gmres(op, prec, b, restart=30, max_restarts=100, rtol=1e-10, check_every=5, 
     and at each restart.  Returns x and the relative residual norms (the least-squares estimate after every
     Arnoldi step, the true residual at every restart); ``info`` (a dict) receives the number of Arnoldi
     steps and of restarts."""
+    if not 1 <= int(restart) <= 32:
+        raise ValueError("gmres: restart must be 1..32 (the device Krylov reductions hold up to 33 columns)")
     C = _krylov()
     shapes = [t.shape for t in b]
     sizes = [t.numel() for t in b]

@@ -4,7 +4,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["setup.cu", "hotpath.cu", "fast.cu", "reduce.cu", "linsolve.cu", "bc.cu", "adjoint.cu", "adjoint_roe.cu", "adjoint_visc.cu", "adjoint_ops.cu", "adjoint_geom.cu", "adjoint_geom2d.cu", "adjoint_generic.cu", "adjoint_generic_p1n5.cu", "adjoint_generic_p1n6.cu", "adjoint_generic_p2n5.cu", "adjoint_generic_p2n6.cu", "positivity.cu", "limiter.cu", "capi.cu", "noalloc.cu"]
+SRC = ["setup.cu", "hotpath.cu", "fast.cu", "reduce.cu", "linsolve.cu", "bc.cu", "adjoint.cu", "adjoint_roe.cu", "adjoint_fast.cu", "adjoint_visc.cu", "adjoint_ops.cu", "adjoint_geom.cu", "adjoint_geom2d.cu", "adjoint_generic.cu", "adjoint_generic_p1n5.cu", "adjoint_generic_p1n6.cu", "adjoint_generic_p2n5.cu", "adjoint_generic_p2n6.cu", "positivity.cu", "limiter.cu", "capi.cu", "noalloc.cu"]
 LIB = os.path.join(HERE, "libdndsb.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -29,11 +29,19 @@ def up_to_date():
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
-def _headers_mtime():
-    d = os.path.join(HERE, "csrc")
-    inc = os.path.join(os.path.dirname(HERE), "include")
-    hs = [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".cuh", ".h"))] + [os.path.join(inc, f) for f in os.listdir(inc)]
-    return max(os.path.getmtime(p) for p in hs)
+def _includes_mtime(path, seen=None):
+    """Newest modification time of a source and of the local headers it includes, recursively."""
+    import re
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return 0.0
+    seen.add(path)
+    t = os.path.getmtime(path)
+    base = os.path.dirname(path)
+    with open(path) as fh:
+        for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', fh.read(), flags=re.M):
+            t = max(t, _includes_mtime(os.path.normpath(os.path.join(base, name)), seen))
+    return t
 
 
 def _ext_path():
@@ -64,12 +72,11 @@ def build(force=False, verbose=False, jobs=None):
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
-    th = _headers_mtime()
     for s in sources():
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         objs.append(o)
-        # an object is reused when it is newer than its source and every header (headers are shared)
-        if not force and not verbose and os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(s), th):
+        # an object is reused when it is newer than its source and every local header the source includes
+        if not force and not verbose and os.path.exists(o) and os.path.getmtime(o) >= _includes_mtime(s):
             continue
         cmd = [NVCC, *FLAGS, "-c", s, "-o", o]
         if verbose:

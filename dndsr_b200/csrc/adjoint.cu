@@ -487,13 +487,14 @@ int rhs_vjp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const r
     // (rsMeanValueEig with Roe_M1..M5) runs through the forward-mode face kernel on every face
     const int roe = roe_scheme_of(ev.s.rsType) >= 0 && !(ev.s.rsMeanValueEig && ev.s.rsType >= RS_Roe_M1 && ev.s.rsType <= RS_Roe_M1 + 4);
     DNDSB_LAUNCH(kf, roe ? m.nBndFace : m.nFace, 64, st, m, g, vr, ev.s, w, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord, roe);
+    bool viscDone = false;
     if (roe)
     {
-        int rc = rhs_vjp_roe_interior(m, g, vr, ev, w, u, uRec, ev.adjBuf, st);
+        int rc = rhs_vjp_roe_interior(m, g, vr, ev, w, u, uRec, ev.adjBuf, st, &viscDone);
         if (rc != ST_OK)
             return rc;
     }
-    if (!ev.s.ignoreVis)
+    if (!ev.s.ignoreVis && !viscDone)
     {
         int rc = rhs_vjp_visc(m, g, vr, ev, w, u, uRec, ev.adjBuf, st);
         if (rc != ST_OK)

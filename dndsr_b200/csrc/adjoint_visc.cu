@@ -12,6 +12,7 @@
 // the zone types allowed here (far-field, outflow, slip wall, symmetry).
 #include "solver.cuh"
 #include "basis_eval.cuh"
+#include "visc_rev.cuh"
 
 namespace dndsb
 {
@@ -19,72 +20,8 @@ namespace
 {
 constexpr int NV = 5;
 using D1 = Dual<1>;
-
-// the 5-variable branch of point_viscous_flux (sa.cuh), on any scalar type
-template <typename T>
-DNDSB_D void visc_flux_t(const EulerSettingsD &s, const T *UM, const T *GP, const real *n, T *Fv)
-{
-    const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
-    T pM, a2M, HM;
-    gas_thermal(UM[4], UM[0], (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) / (UM[0] * UM[0]), gamma, pM, a2M, HM);
-    T Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
-    T mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
-    viscous_flux<NV>(UM, GP, n, false, gamma, mu, cp * mu / s.prGas, cp, Fv);
-}
-
-// GMbar = (d Fv / d grad U_M)^T Fvbar at fixed U_M: Fv is linear in the primitive gradient GP
-// (viscous_flux) and GP is linear in the conservative gradient (grad_cons2prim), so the cotangent
-// is the transpose of those two linear maps, statement by statement in reverse
-DNDSB_D void visc_grad_transpose(const EulerSettingsD &s, const real *UM, const real *n, const real *Fvbar, real *GMbar)
-{
-    const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
-    real pM, a2M, HM;
-    gas_thermal(UM[4], UM[0], (UM[1] * UM[1] + UM[2] * UM[2] + UM[3] * UM[3]) / (UM[0] * UM[0]), gamma, pM, a2M, HM);
-    real Tm = pM / ((gamma - 1) / gamma * cp * UM[0]);
-    real mu = mu_eff(s.muModel, s.muGas, s.TRef, s.CSutherland, UM[0], Tm);
-    real k = cp * mu / s.prGas;
-    real ir = 1.0 / UM[0];
-    real v[3] = {UM[1] * ir, UM[2] * ir, UM[3] * ir};
-    real p = (gamma - 1) * (UM[4] - UM[0] * 0.5 * dot3(v, v));
-    real cT = gamma / ((gamma - 1) * cp * UM[0] * UM[0]);
-    // viscous_flux: Fv[1+i] = sum_j s_ij n_j, Fv[4] = sum_i (sum_j s_ij v_j + k gT_i) n_i
-    real GPb[3 * NV];
-    for (int i = 0; i < 3 * NV; i++)
-        GPb[i] = 0;
-    real lmb = 0;
-    for (int i = 0; i < 3; i++)
-    {
-        real gTb = Fvbar[4] * k * n[i];
-        GPb[i * NV + 4] += cT * UM[0] * gTb;
-        GPb[i * NV + 0] += -cT * p * gTb;
-        for (int j = 0; j < 3; j++)
-        {
-            real sb = Fvbar[1 + i] * n[j] + Fvbar[4] * n[i] * v[j];
-            GPb[i * NV + 1 + j] += mu * sb;
-            GPb[j * NV + 1 + i] += mu * sb;
-            if (i == j)
-                lmb += sb;
-        }
-    }
-    real trb = -2.0 / 3.0 * mu * lmb;
-    for (int i = 0; i < 3; i++)
-        GPb[i * NV + 1 + i] += trb;
-    // grad_cons2prim per direction r
-    for (int r = 0; r < 3; r++)
-    {
-        const real *gpb = GPb + r * NV;
-        real *gb = GMbar + r * NV;
-        real sbar = -0.5 * (gamma - 1) * gpb[4];
-        gb[4] = (gamma - 1) * gpb[4];
-        gb[0] = gpb[0];
-        for (int j = 0; j < 3; j++)
-        {
-            real gpj = gpb[1 + j] + sbar * UM[1 + j];
-            gb[1 + j] = sbar * v[j] + UM[0] * ir * ir * gpj;
-            gb[0] += -UM[1 + j] * ir * ir * gpj;
-        }
-    }
-}
+using visc_rev::visc_flux_t;
+using visc_rev::visc_point_bar;
 
 // geometry of one interior face shared by its Gauss points
 struct ViscFace
@@ -176,24 +113,7 @@ DNDSB_GLOBAL void k_rhs_vjp_visc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, con
             for (int d = 0; d < 3; d++)
                 for (int v = 0; v < NV; v++)
                     GMr[d * NV + v] = (GR[d * NV + v] + GL[d * NV + v]) * 0.5 + iD * (n[d] * (UR[v] - UL[v]));
-            // one Dual<1> pass per component of U_M: a fifth of the dual state of one Dual<5> pass, which
-            // spilled to local memory (the flux is cheap next to that traffic)
-#pragma unroll 1
-            for (int i = 0; i < NV; i++)
-            {
-                D1 UM[NV], GM[3 * NV], GP[3 * NV], Fv[NV];
-                for (int v = 0; v < NV; v++)
-                    UM[v] = D1::var(UMr[v], v == i ? 0 : -1);
-                for (int k = 0; k < 3 * NV; k++)
-                    GM[k] = D1(GMr[k]);
-                grad_cons2prim<NV>(UM, GM, GP, gamma);
-                visc_flux_t(s, UM, GP, n, Fv);
-                real a = 0;
-                for (int k = 0; k < NV; k++)
-                    a += Fv[k].d[0] * Fvbar[k];
-                bar[i] = a;
-            }
-            visc_grad_transpose(s, UMr, n, Fvbar, bar + NV);
+            visc_point_bar(s, UMr, GMr, n, Fvbar, bar);
             for (int v = 0; v < NV; v++)
             {
                 real nG = 0;

@@ -195,10 +195,15 @@ int rhs_vjp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev,
                  cudaStream_t st);
 int rhs_jvp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *du, const real *duRec, const real *u,
                  const real *uRec, real *ffd, cudaStream_t st);
-// reverse-mode interior-face derivative of the Roe-family fluxes (adjoint_roe.cu)
+// reverse-mode interior-face derivative of the Roe-family fluxes (adjoint_roe.cu); *viscDone: the viscous
+// flux's share was included (the Gauss-point-parallel kernel of plain Roe and HLLE+)
 int roe_scheme_of(int rsType);
+// the Gauss-point-parallel interior-face VJP of plain Roe (hllep false) or HLLE+ with the viscous flux
+// (adjoint_fast.cu); ST_UNSUPPORTED outside its instantiations
+int rhs_vjp_interior_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, bool hllep, const real *w, const real *u,
+                          const real *uRec, real *faceAdj, cudaStream_t st);
 int rhs_vjp_roe_interior(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec,
-                         real *faceAdj, cudaStream_t st);
+                         real *faceAdj, cudaStream_t st, bool *viscDone);
 // adjoint building blocks (adjoint_ops.cu)
 int lusgs_matvec_t(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *y, const real *jdiag, real *ATy,
                    cudaStream_t st);

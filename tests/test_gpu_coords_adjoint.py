@@ -172,7 +172,7 @@ def test_shape_gradient_of_the_pressure_drag_against_the_tangent_response():
     ev.EvaluateDt(dTau, u, 1.0)
     adj = SteadyAdjoint(vr, ev, u, uRec, cfl=5.0, dt=5.0 * float(dTau.max()))
     J, gU, gR = ev.PressureForce(BUMP, DRAG, u, uRec, grad=True)
-    psi, lam, h_adj = adj.solve_adjoint(gU, gR, restart=40, max_restarts=60, rtol=1e-11)
+    psi, lam, h_adj = adj.solve_adjoint(gU, gR, restart=32, max_restarts=60, rtol=1e-11)
     assert h_adj[-1] < 1e-11
     dJdX = ev.PressureForceCoords(BUMP, DRAG, u, uRec)
     G = adj.shape_gradient(psi, lam, dJdX)
@@ -181,7 +181,7 @@ def test_shape_gradient_of_the_pressure_drag_against_the_tangent_response():
         V = torch.tensor(rng.normal(size=X.shape) * scale, device="cuda")
         sU = ev.EvaluateRHSJVPCoords(V, u, uRec)
         sR = vr.DoReconstructionIterJVPCoords(V, uRec, u)
-        du, dRec, h_tan = adj.solve_tangent(sU, sR, restart=40, max_restarts=60, rtol=1e-11)
+        du, dRec, h_tan = adj.solve_tangent(sU, sR, restart=32, max_restarts=60, rtol=1e-11)
         assert h_tan[-1] < 1e-11
         tangent = float((dJdX * V).sum() + (gU * du).sum() + (gR * dRec).sum())
         assert abs(float((G * V).sum()) - tangent) < 1e-8 * abs(tangent)

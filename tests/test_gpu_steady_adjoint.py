@@ -94,15 +94,15 @@ def test_coupled_adjoint_and_tangent_solves_agree(p):
     assert abs(lhs - rhs) < 1e-12 * abs(rhs)
     # adjoint of the pressure force and the tangent response to a residual source
     J, gU, gR = ev.PressureForce(BUMP, DRAG, u, uRec, grad=True)
-    psi, lam, h_adj = adj.solve_adjoint(gU, gR, restart=40, max_restarts=60, rtol=1e-10)
+    psi, lam, h_adj = adj.solve_adjoint(gU, gR, restart=32, max_restarts=60, rtol=1e-10)
     assert h_adj[-1] < 1e-10
     # FP32 transposed LU-SGS inside the FP64 Krylov iteration reaches the same adjoint
     adj32 = SteadyAdjoint(vr, ev, u, uRec, cfl=5.0, dt=5.0 * float(dTau.max()), precision="fp32")
-    psi32, lam32, h32 = adj32.solve_adjoint(gU, gR, restart=40, max_restarts=60, rtol=1e-10)
+    psi32, lam32, h32 = adj32.solve_adjoint(gU, gR, restart=32, max_restarts=60, rtol=1e-10)
     assert h32[-1] < 1e-10 and relerr(psi32.cpu().numpy(), psi.cpu().numpy()) < 1e-8
     sU = torch.tensor(rng.normal(size=u0.shape), device="cuda")
     sR = torch.zeros_like(uRec)
-    du, dRec, h_tan = adj.solve_tangent(sU, sR, restart=40, max_restarts=60, rtol=1e-10)
+    du, dRec, h_tan = adj.solve_tangent(sU, sR, restart=32, max_restarts=60, rtol=1e-10)
     assert h_tan[-1] < 1e-10
     via_adjoint = -float((psi * sU).sum())
     via_tangent = float((gU * du).sum() + (gR * dRec).sum())
