@@ -216,7 +216,7 @@ def run_steady(args):
     """Wall time to a 1e-10 residual drop, mixed vs FP64, on the steady transonic bump (BCFar in/out, BCWallInvis
     floor/ceiling, BCSym sides, Mach 0.8, VR degree 1, Roe_M2): BDF1 dual time at CFL 200, GMRES(30) preconditioned
     by one SGS pair, FP64 or FP32 linear solve inside the FP64 defect correction, each precision from the free
-    stream after a two-iteration warm-up; plus the per-iteration cost on the ~2M-tet mesh."""
+    stream after a two-iteration warm-up; on the configuration's ~2M-tet mesh and on a 250k-tet one."""
     import torch
     from dndsr_b200 import implicit as I
 
@@ -235,54 +235,49 @@ def run_steady(args):
         torch.cuda.synchronize()
         return u, time.perf_counter() - t0, len(cfg.res_history), cfg.res_history[-1][2], solver
 
-    nx, ny, nz = args.steady_mesh
-    mesh, vr, ev, far = _bump_c3(nx, ny, nz)
-    out = {}
-    for prec in ("fp64", "fp32"):
-        out[prec] = solve(vr, ev, far, prec, args.steady_iters, 1e-10)
-    a, b = out["fp64"], out["fp32"]
-    # component times at the converged state (CUDA events, 5 calls each)
-    comp = {}
-    for prec in ("fp64", "fp32"):
-        s = out[prec][4]
-        u = out[prec][0]
-        rhs = torch.zeros_like(u)
-        dtau = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
-        xinc = torch.zeros_like(u)
-        s.fdtau(u, dtau, 1.0)
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        evs[0].record()
-        for _ in range(5):
-            s.frhs(rhs, u, dtau, 1, 1.0)
-        evs[1].record()
-        for _ in range(5):
-            s.fsolve(u, rhs, rhs, dtau, 1e100, 1.0, xinc, 1, 1.0)
-        evs[2].record()
-        torch.cuda.synchronize()
-        comp[prec] = (evs[0].elapsed_time(evs[1]) / 5, evs[1].elapsed_time(evs[2]) / 5)
-    res = {"workload": f"steady Euler over the bump, {mesh.n_cell} tets ({nx}x{ny}x{nz}x6), BCFar in/out, BCWallInvis floor/ceiling, "
-                       "BCSym sides, Mach 0.8, VR degree 1, Roe_M2, BDF1 dual time CFL 200, GMRES(30) preconditioned by one SGS pair; "
-                       "run to a 1e-10 density residual drop",
-           "converged_fp64": a[3] < 1e-10, "converged_mixed": b[3] < 1e-10,
-           "iterations_fp64": a[2], "iterations_mixed": b[2], "fp64_s": a[1], "mixed_s": b[1], "mixed_over_fp64_time": b[1] / a[1],
-           "fp64_ms_per_iter": 1e3 * a[1] / a[2], "mixed_ms_per_iter": 1e3 * b[1] / b[2],
-           "final_drop_fp64": a[3], "final_drop_mixed": b[3],
-           "state_rel_diff": float((a[0] - b[0]).abs().max() / a[0].abs().max()),
-           "ms_vr_sweep_plus_rhs": comp["fp64"][0], "ms_linear_solve_fp64": comp["fp64"][1], "ms_linear_solve_fp32": comp["fp32"][1]}
-    del out, vr, ev
-    torch.cuda.empty_cache()
-    # the ~2M-tet mesh of the configuration: per-iteration cost of both precisions over the first iterations
-    bx, by, bz = args.steady_big_mesh
-    mesh, vr, ev, far = _bump_c3(bx, by, bz)
-    big = {}
-    for prec in ("fp64", "fp32"):
-        u, el, it, drop, _ = solve(vr, ev, far, prec, args.steady_big_iters, 1e-30)
-        big[prec] = (el, it, drop, u)
-    res["large_mesh"] = {"cells": mesh.n_cell, "iterations": big["fp64"][1], "fp64_ms_per_iter": 1e3 * big["fp64"][0] / big["fp64"][1],
-                         "mixed_ms_per_iter": 1e3 * big["fp32"][0] / big["fp32"][1],
-                         "mixed_over_fp64_time": big["fp32"][0] / big["fp64"][0],
-                         "drop_fp64": big["fp64"][2], "drop_mixed": big["fp32"][2],
-                         "state_rel_diff": float((big["fp64"][3] - big["fp32"][3]).abs().max() / big["fp64"][3].abs().max())}
+    def measure(dims, iters):
+        nx, ny, nz = dims
+        mesh, vr, ev, far = _bump_c3(nx, ny, nz)
+        out = {}
+        for prec in ("fp64", "fp32"):
+            out[prec] = solve(vr, ev, far, prec, iters, 1e-10)
+        a, b = out["fp64"], out["fp32"]
+        # component times at the converged state (CUDA events, 5 calls each)
+        comp = {}
+        for prec in ("fp64", "fp32"):
+            s = out[prec][4]
+            u = out[prec][0]
+            rhs = torch.zeros_like(u)
+            dtau = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
+            xinc = torch.zeros_like(u)
+            s.fdtau(u, dtau, 1.0)
+            evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            evs[0].record()
+            for _ in range(5):
+                s.frhs(rhs, u, dtau, 1, 1.0)
+            evs[1].record()
+            for _ in range(5):
+                s.fsolve(u, rhs, rhs, dtau, 1e100, 1.0, xinc, 1, 1.0)
+            evs[2].record()
+            torch.cuda.synchronize()
+            comp[prec] = (evs[0].elapsed_time(evs[1]) / 5, evs[1].elapsed_time(evs[2]) / 5)
+        res = {"cells": mesh.n_cell, "mesh": f"{nx}x{ny}x{nz}x6 tets",
+               "converged_fp64": a[3] < 1e-10, "converged_mixed": b[3] < 1e-10,
+               "iterations_fp64": a[2], "iterations_mixed": b[2], "fp64_s": a[1], "mixed_s": b[1], "mixed_over_fp64_time": b[1] / a[1],
+               "fp64_ms_per_iter": 1e3 * a[1] / a[2], "mixed_ms_per_iter": 1e3 * b[1] / b[2],
+               "final_drop_fp64": a[3], "final_drop_mixed": b[3],
+               "state_rel_diff": float((a[0] - b[0]).abs().max() / a[0].abs().max()),
+               "ms_vr_sweep_plus_rhs": comp["fp64"][0], "ms_linear_solve_fp64": comp["fp64"][1], "ms_linear_solve_fp32": comp["fp32"][1]}
+        del out, vr, ev
+        torch.cuda.empty_cache()
+        return res
+
+    # the configuration's ~2M-tet mesh, then a 250k-tet one
+    res = {"workload": "steady Euler over the bump, BCFar in/out, BCWallInvis floor/ceiling, BCSym sides, Mach 0.8, VR degree 1, "
+                       "Roe_M2, BDF1 dual time CFL 200, GMRES(30) preconditioned by one SGS pair; each precision run from the free "
+                       "stream to a 1e-10 density residual drop",
+           **measure(args.steady_big_mesh, args.steady_big_iters)}
+    res["small_mesh"] = measure(args.steady_mesh, args.steady_iters)
     return res
 
 
@@ -386,6 +381,85 @@ def run_sa_plate(args):
     out.update({"iterations": a64[2], "fp64_ms_per_iter": 1e3 * a64[1] / a64[2], "mixed_ms_per_iter": 1e3 * a32[1] / a32[2],
                 "mixed_over_fp64_time": a32[1] / a64[1], "residual_drop_fp64": a64[3], "residual_drop_mixed": a32[3],
                 "state_rel_diff": float((a64[0] - a32[0]).abs().max() / a64[0].abs().max())})
+    del vr, ev, u, uRec, tmp, rhs, res, solver
+    torch.cuda.empty_cache()
+    out["adjoint"] = sa_adjoint(args)
+    return out
+
+
+def sa_adjoint(args):
+    """The skin-friction adjoint with the SA terms (the x force of the wall flux, pressure and friction,
+    EvaluateRHS.hxx:599-637) on a smaller plate (the same settings) after a bounded primal solve: CUDA-event
+    times of EvaluateRHS and its VJP (SA convective/diffusion fluxes, eddy viscosity, source; forward-mode
+    kernels), of the VR sweep and its VJP and of the objective gradient; then the adjoint of the coupled
+    residual of one implicit step (dt = 5 of the largest local steps) by the device GMRES(30) with the
+    transposed LU-SGS pair, bounded in restarts."""
+    import torch
+    from dndsr_b200 import implicit as I
+    from dndsr_b200 import mesh as M
+    from dndsr_b200.adjoint import SteadyAdjoint
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    nx, ny, nz = args.sa_adjoint_mesh
+    mesh = M.flat_plate_hex(nx, ny, nz, y1=5e-6, growth=1.1)
+    far5 = M.freestream(0.2)
+    mu = np.linalg.norm(far5[1:4]) / far5[0] / 5e6
+    far = np.concatenate([far5, [3.0 * far5[0]]])
+    types, vals = np.zeros(6, np.int32), np.zeros((6, 6))
+    w = np.ones((6, 4))
+    for z, tp in M.PLATE_BC_TYPES.items():
+        types[z], vals[z], w[z] = tp, far, (1, 0, 0, 0)
+    vr = VariationalReconstruction(mesh, dict(maxOrder=1, intOrder=3, dirWeightScheme="HQM_OPT", geomWeightScheme="HQM_SD",
+                                              geomWeightBias=1.0)).construct(w)
+    ev = EulerEvaluator(vr, dict(nVars=6, riemannSolverType="Roe", muGas=mu, muModel=0, prGas=0.72))
+    ev.SetBC(types, vals)
+    ev.SetWallDistance(M.plate_wall_distance(vr.get("cellPP").reshape(mesh.n_cell, -1, 3)))
+    u = vr.BuildUDof(6)
+    u[:] = torch.tensor(far, device="cuda")
+    cfg = I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=args.sa_adjoint_primal_iters,
+                         nTimeStepInternalMin=args.sa_adjoint_primal_iters, CFL=50.0, gmresCode=1, nGmresSpace=30, linear_precision="fp32")
+    solver = I.ImplicitSolver(vr, ev, cfg)
+    solver.run(u)
+    uRec = solver.uRec
+    d = np.zeros(6)
+    d[1] = 1.0
+    dTau = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dTau, u, 1.0)
+    rhs, tmp = torch.zeros_like(u), torch.empty_like(uRec)
+    W, C = torch.randn_like(u), torch.randn_like(uRec)
+
+    def timed(fn, n=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    t_rhs = timed(lambda: ev.EvaluateRHS(rhs, u, uRec))
+    t_vr = timed(lambda: vr.DoReconstructionIter(uRec, tmp, u, putIntoNew=True))
+    t_vjp = timed(lambda: ev.EvaluateRHSVJP(W, u, uRec))
+    t_vrvjp = timed(lambda: vr.DoReconstructionIterVJP(C, uRec, u))
+    t_obj = timed(lambda: ev.WallFluxVJP(d, u, uRec))
+    ev.EvaluateRHS(rhs, u, uRec, flags=0, JSource=torch.zeros_like(u))
+    J = float(d @ ev.get("fluxWallSum"))
+    gU, gR = ev.WallFluxVJP(d, u, uRec)
+    out = {"workload": f"SA flat plate, {mesh.n_cell} hex ({nx}x{ny}x{nz}), {args.sa_adjoint_primal_iters} primal BDF1 iterations at "
+                       "CFL 50 first; objective: x force of the wall flux (pressure and skin friction)",
+           "J": J, "primal_residual_drop": cfg.res_history[-1][2], "ms_rhs": t_rhs, "ms_vr_sweep": t_vr, "ms_rhs_vjp": t_vjp,
+           "ms_vr_sweep_vjp": t_vrvjp, "ms_objective_gradient": t_obj, "residual_vjp_over_primal": (t_vjp + t_vrvjp) / (t_rhs + t_vr)}
+    adj = SteadyAdjoint(vr, ev, u, uRec, cfl=5.0, dt=5.0 * float(dTau.max()), precision="fp32")
+    adj.solve_adjoint(gU, gR, restart=30, max_restarts=1, rtol=1e-10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    info = {}
+    psi, lam, hist = adj.solve_adjoint(gU, gR, restart=30, max_restarts=args.sa_adjoint_restarts, rtol=1e-8, info=info)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    out.update({"gmres_iterations": info["arnoldi_steps"], "adjoint_drop": hist[-1], "adjoint_s": el,
+                "adjoint_s_per_iteration": el / max(info["arnoldi_steps"], 1)})
     return out
 
 
@@ -761,10 +835,13 @@ def main():
     ap.add_argument("--sample-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-steady", action="store_true")
+    ap.add_argument("--sa-adjoint-mesh", type=int, nargs=3, default=(120, 80, 8))
+    ap.add_argument("--sa-adjoint-primal-iters", type=int, default=300)
+    ap.add_argument("--sa-adjoint-restarts", type=int, default=10)
     ap.add_argument("--steady-mesh", type=int, nargs=3, default=(80, 40, 13))
     ap.add_argument("--steady-iters", type=int, default=3000)
     ap.add_argument("--steady-big-mesh", type=int, nargs=3, default=(160, 80, 26))
-    ap.add_argument("--steady-big-iters", type=int, default=30)
+    ap.add_argument("--steady-big-iters", type=int, default=4000)
     ap.add_argument("--adjoint-mesh", type=int, nargs=3, default=(80, 40, 13))
     ap.add_argument("--no-sa", action="store_true")
     # the extra measurement blocks after the headline, comma separated (a subset for profiling runs)

@@ -9,8 +9,9 @@
 // and of the Roe-average fields (hand-written reverse sweeps of roe_rev.cuh and visc_rev.cuh).  Their
 // images in the cotangent rows of both cells' (u, uRec),
 //     row_j,v = sum_q [phi_j(p_q) Ub_q,v + sum_d dphi_j/dx_d(p_q) GMb_q,d,v],
-// are summed over the points in point order through shared memory, one reconstruction row of both sides
-// per round.  The Roe-average cotangents are summed the same way and carried to the two cell means by a
+// are summed over the points in point order through shared memory, all rows in one round (or half of them
+// per round where the shares would not fit).  The Roe-average cotangents are summed the same way and
+// carried to the two cell means by a
 // Dual<1> evaluation of the averages per mean component (one thread each).  The block's face records
 // [32][2][(R+1) NV] are assembled in shared memory and stored row-contiguously.
 #include "solver.cuh"
@@ -64,15 +65,18 @@ template <int DIM, int P, int NG, bool VISC>
 struct VjpRows
 {
     using Lt = Layout<DIM, P, NV>;
-    static constexpr int R = Lt::R, W = (R + 1) * NV, CH = 2 * NV;
+    static constexpr int R = Lt::R, W = (R + 1) * NV;
+    // reconstruction rows per round: all of them when the 32 faces' shares fit in 120 KB of shared memory,
+    // else half of them
+    static constexpr int ROWS = NG * 32 * (R + 1) * 2 * NV * 8 <= 120 * 1024 ? R + 1 : (R + 2) / 2;
+    static constexpr int CH = ROWS * 2 * NV > 15 ? ROWS * 2 * NV : 15; // values per point of one round
 
-    // one round per reconstruction row J: the point shares of both sides into sRed, summed over the points
-    // into the face records sOut
-    template <int J>
-    static DNDSB_D void round(const real *xs, const real *cell0, const real *cell1, const real *Ub0, const real *Ub1, const real *GMb, real *sRed,
-                              real *sOut, const int *sC, int64_t f0, int64_t nFace, int q, int fl, int tid, int nthr)
+    // the point shares of row J (both sides) into slot J - J0 of the round's buffer
+    template <int J, int J0>
+    static DNDSB_D void shares(const real *xs, const real *cell0, const real *cell1, const real *Ub0, const real *Ub1, const real *GMb, real *sRed,
+                               int q, int fl)
     {
-        if constexpr (J <= R)
+        if constexpr (J <= R && J < J0 + ROWS)
         {
 #pragma unroll
             for (int side = 0; side < 2; side++)
@@ -94,11 +98,25 @@ struct VjpRows
                         if (DIM == 3)
                             a += dz * GMb[2 * NV + v];
                     }
-                    sRed[((side * NV + v) * NG + q) * 32 + fl] = a;
+                    sRed[((((J - J0) * 2 + side) * NV + v) * NG + q) * 32 + fl] = a;
                 }
             }
+            shares<J + 1, J0>(xs, cell0, cell1, Ub0, Ub1, GMb, sRed, q, fl);
+        }
+    }
+
+    // rounds of ROWS rows: the shares into sRed, summed over the points in point order into the face records
+    // sOut (row 0, the cell means, adds to the Roe-average part already there)
+    template <int J0>
+    static DNDSB_D void rounds(const real *xs, const real *cell0, const real *cell1, const real *Ub0, const real *Ub1, const real *GMb, real *sRed,
+                               real *sOut, const int *sC, int64_t f0, int64_t nFace, int q, int fl, int tid, int nthr)
+    {
+        if constexpr (J0 <= R)
+        {
+            constexpr int nRow = R + 1 - J0 < ROWS ? R + 1 - J0 : ROWS;
+            shares<J0, J0>(xs, cell0, cell1, Ub0, Ub1, GMb, sRed, q, fl);
             __syncthreads();
-            for (int e = tid; e < 32 * CH; e += nthr)
+            for (int e = tid; e < 32 * nRow * 2 * NV; e += nthr)
             {
                 const int fi = e & 31, k = e >> 5;
                 if (f0 + fi < nFace && sC[32 + fi] >= 0)
@@ -107,12 +125,13 @@ struct VjpRows
 #pragma unroll
                     for (int qq = 0; qq < NG; qq++)
                         acc += sRed[(k * NG + qq) * 32 + fi];
-                    real &o = sOut[fi * 2 * W + (k / NV) * W + J * NV + k % NV];
-                    o = J == 0 ? o + acc : acc;
+                    const int row = J0 + k / (2 * NV), side = (k / NV) & 1, v = k % NV;
+                    real &o = sOut[fi * 2 * W + side * W + row * NV + v];
+                    o = row == 0 ? o + acc : acc;
                 }
             }
             __syncthreads();
-            round<J + 1>(xs, cell0, cell1, Ub0, Ub1, GMb, sRed, sOut, sC, f0, nFace, q, fl, tid, nthr);
+            rounds<J0 + ROWS>(xs, cell0, cell1, Ub0, Ub1, GMb, sRed, sOut, sC, f0, nFace, q, fl, tid, nthr);
         }
     }
 };
@@ -276,30 +295,24 @@ __global__ void __launch_bounds__(32 * NG, vjp_min_blocks<NG>())
                 GMb[i] = 0.5 * bar[NV + i];
         }
     }
-    // the Roe-average cotangents: 15 fields summed over the points of each face (two rounds)
+    // the Roe-average cotangents: 15 fields summed over the points of each face
     {
         const real rf[15] = {rb.v[0], rb.v[1], rb.v[2], rb.vL[0], rb.vL[1], rb.vL[2], rb.vR[0], rb.vR[1], rb.vR[2],
                              rb.aL, rb.aR, rb.vsqr, rb.H, rb.asqr, rb.a};
 #pragma unroll
-        for (int base = 0; base < 15; base += CH)
+        for (int k = 0; k < 15; k++)
+            sRed[(k * NG + q) * 32 + fl] = rf[k];
+        __syncthreads();
+        for (int e = tid; e < 32 * 15; e += nthr)
         {
+            const int fi = e & 31, k = e >> 5;
+            real acc = 0;
 #pragma unroll
-            for (int k = 0; k < CH; k++)
-                if (base + k < 15)
-                    sRed[(k * NG + q) * 32 + fl] = rf[base + k];
-            __syncthreads();
-            const int cnt = 15 - base < CH ? 15 - base : CH;
-            for (int e = tid; e < 32 * cnt; e += nthr)
-            {
-                const int fi = e & 31, k = e >> 5;
-                real acc = 0;
-#pragma unroll
-                for (int qq = 0; qq < NG; qq++)
-                    acc += sRed[(k * NG + qq) * 32 + fi];
-                sT[(base + k) * 32 + fi] = acc;
-            }
-            __syncthreads();
+            for (int qq = 0; qq < NG; qq++)
+                acc += sRed[(k * NG + qq) * 32 + fi];
+            sT[k * 32 + fi] = acc;
         }
+        __syncthreads();
     }
     // ... carried to the cell means: thread e -> face e % 32, mean component e / 32 (side (e / 32) / NV)
     for (int e = tid; e < 32 * 2 * NV; e += nthr)
@@ -325,7 +338,7 @@ __global__ void __launch_bounds__(32 * NG, vjp_min_blocks<NG>())
     }
     __syncthreads();
     // the rows: the cell means (row 0) and the reconstruction rows 1..R
-    Rows::template round<0>(xs, cell0, cell1, Ub0, Ub1, GMb, sRed, sOut, sC, f0, m.nFace, q, fl, tid, nthr);
+    Rows::template rounds<0>(xs, cell0, cell1, Ub0, Ub1, GMb, sRed, sOut, sC, f0, m.nFace, q, fl, tid, nthr);
     // interior faces' records (boundary faces keep what the boundary kernel stored)
     for (int e = tid; e < 32 * 2 * W; e += nthr)
     {
@@ -340,8 +353,9 @@ int launch_vjp_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &
                     const real *uRec, real *faceAdj, cudaStream_t st)
 {
     using Lt = Layout<DIM, P, NV>;
-    constexpr int W = (Lt::R + 1) * NV, CH = 2 * NV;
-    const size_t smem = sizeof(real) * (64 * Lt::CS + 32 * NV + 15 * 32 + CH * NG * 32 + 32 * 2 * W) + sizeof(FaceData) * 32;
+    constexpr int W = (Lt::R + 1) * NV, CH = VjpRows<DIM, P, NG, true>::CH;
+    constexpr size_t smem = sizeof(real) * (64 * Lt::CS + 32 * NV + 15 * 32 + CH * NG * 32 + 32 * 2 * W) + sizeof(FaceData) * 32;
+    static_assert(smem <= 227 * 1024, "shared memory of k_rhs_vjp_fast above the 227 KB a block may hold");
     auto kern = visc ? k_rhs_vjp_fast<DIM, P, NG, true> : k_rhs_vjp_fast<DIM, P, NG, false>;
     static unsigned long long attrSet[2] = {0, 0}; // per variant, one bit per device: dynamic shared memory limit raised
     int dev = 0;

@@ -29,15 +29,17 @@ namespace dndsb
 namespace
 {
 // F - Fv at one point of an interior face (the integrand of fluxEs, EvaluateRHS.hxx:369-525)
+// (parts: 1 the inviscid flux, 2 the viscous flux, 3 both; a pass whose seeds one part does not depend on
+// skips that part)
 template <int NV, typename T>
 DNDSB_D bool interior_point_flux(const EulerSettingsD &s, const T *UL, const T *UR, const T *ULm, const T *URm, const T *GL, const T *GR,
-                                 const real *n, const real *nMV, real distGRP, real dLambda, T *out)
+                                 const real *n, const real *nMV, real distGRP, real dLambda, T *out, int parts = 3)
 {
     const real gamma = s.gamma;
     T Fv[NV];
     for (int v = 0; v < NV; v++)
         Fv[v] = 0.0;
-    if (!s.ignoreVis)
+    if (!s.ignoreVis && (parts & 2))
     {
         real iD = 1.0 / distGRP;
         T UM[NV], GM[3 * NV], GP[3 * NV];
@@ -52,9 +54,13 @@ DNDSB_D bool interior_point_flux(const EulerSettingsD &s, const T *UL, const T *
     T F[NV], l0, l1, l4;
     for (int v = 0; v < NV; v++)
         F[v] = 0.0;
-    bool ok = riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4, nMV);
-    if (NV == 6)
-        F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
+    bool ok = true;
+    if (parts & 1)
+    {
+        ok = riemann_flux(s.rsType, UL, UR, ULm, URm, n, gamma, dLambda, s.rsFixScale, s.rsIncFScale, F, l0, l1, l4, nMV);
+        if (NV == 6)
+            F[NV - 1] = sa_convective_flux(UL, UR, n, l1);
+    }
     for (int v = 0; v < NV; v++)
         out[v] = F[v] - Fv[v];
     return ok;
@@ -244,8 +250,9 @@ DNDSB_GLOBAL void k_rhs_vjp_face_g(MeshD m, GeomD g, VRD vr, EulerSettingsD s, c
                     else
                         ga[d * NV + v].d[v] = 1, gb[d * NV + v].d[NV + v] = 1;
                 }
+                // on interior faces the means enter only the inviscid flux, the gradients only the viscous one
                 bool ok = bnd ? boundary_point_flux<NV>(s, vr.bnd, zone, type, a, am, &g.faceMeanNorm[f * 3], ga, n, nMV, distGRP, dLambda, out)
-                              : interior_point_flux<NV>(s, a, b, am, bm, ga, gb, n, nMV, distGRP, dLambda, out);
+                              : interior_point_flux<NV>(s, a, b, am, bm, ga, gb, n, nMV, distGRP, dLambda, out, pass == 0 ? 3 : pass == 1 ? 1 : 2);
                 bad |= !ok;
                 for (int i = 0; i < NV; i++)
                 {
