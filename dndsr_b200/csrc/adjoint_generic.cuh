@@ -161,7 +161,7 @@ DNDSB_D bool is_wall(int type, real muGas) { return type == BC_WALL || type == B
 template <int DIM, int P, int NV>
 DNDSB_GLOBAL void k_rhs_vjp_face_g(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ w, const real *__restrict__ objDir,
                                    const real *__restrict__ u, const real *__restrict__ uRec, const real *__restrict__ dLamCell,
-                                   real *__restrict__ faceAdj, int *err)
+                                   real *__restrict__ faceAdj, int *err, int bndOnly)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1, W = (R + 1) * NV;
     using DV = Dual<2 * NV>;
@@ -169,6 +169,8 @@ DNDSB_GLOBAL void k_rhs_vjp_face_g(MeshD m, GeomD g, VRD vr, EulerSettingsD s, c
     {
         const int64_t c0 = m.face2cell[f * 2], c1 = m.face2cell[f * 2 + 1];
         const bool bnd = c1 < 0;
+        if (bndOnly && !bnd)
+            continue; // the interior faces' records come from the Gauss-point-parallel kernel
         const int zone = m.faceZone[f], type = bnd ? zone_type(vr.bnd, zone) : 0;
         real *o0 = faceAdj + (f * 2) * W, *o1 = faceAdj + (f * 2 + 1) * W;
         for (int i = 0; i < W; i++)
@@ -747,8 +749,19 @@ int vjp_dp(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real 
            real *du, real *duRec, cudaStream_t st)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1, W = (R + 1) * NV;
+    // the SA model with plain Roe and the viscous flux: interior faces by the hand-reversed Gauss-point-parallel
+    // kernel, boundary faces here
+    int interiorDone = 0;
+    if (NV == 6 && !objDir)
+    {
+        int rc = rhs_vjp_interior_fast_sa(m, g, vr, ev, w, u, uRec, ev.adjBuf, st);
+        if (rc == ST_OK)
+            interiorDone = 1;
+        else if (rc != ST_UNSUPPORTED)
+            return rc;
+    }
     auto kf = k_rhs_vjp_face_g<DIM, P, NV>;
-    DNDSB_LAUNCH(kf, m.nFace, 64, st, m, g, vr, ev.s, w, objDir, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord);
+    DNDSB_LAUNCH(kf, m.nFace, 64, st, m, g, vr, ev.s, w, objDir, u, uRec, ev.deltaLambdaCell, ev.adjBuf, ev.errWord, interiorDone);
     auto kg = k_adj_gather_g<W, NV>;
     DNDSB_LAUNCH(kg, m.nCell, 128, st, m.nCell, m.nf, m.cell2face, ev.adjBuf, du, duRec);
     if (NV == 6 && !objDir)

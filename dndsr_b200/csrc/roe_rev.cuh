@@ -49,8 +49,10 @@ DNDSB_D void flim_rev(real v, real lam, real lamL, real lamR, real sHY, real ob,
 // Plain Roe (scheme 0): incF = D(r, n) incU.  Given incFb, adds the cotangents of incU (incUb, set)
 // and of the Roe-average fields (rb, accumulated), recomputing the forward intermediates of
 // roe_eigen / roe_waves / roe_dissipation statement by statement
+// (l123bIn: an extra cotangent of the fixed eigenvalue l123, which the SA convective flux also uses; l123Out,
+// when given, receives l123)
 DNDSB_D void roe0_diss_rev(const real *incU, const real *n, const RoeAvg &r, real gamma, real dLambda, real fixScale, real incFScale,
-                           const real *incFb, real *incUb, RoeBar &rb)
+                           const real *incFb, real *incUb, RoeBar &rb, real l123bIn = 0, real *l123Out = nullptr)
 {
     // forward: eigenvalues
     const real sHY = 0.05 * fixScale;
@@ -65,6 +67,8 @@ DNDSB_D void roe0_diss_rev(const real *incU, const real *n, const RoeAvg &r, rea
     real l0 = flim(in0, vN - r.a, vLm0 - r.aL, vRm0 - r.aR);
     real l123 = flim(in123, vN, vLm0, vRm0);
     real l4 = flim(in4, vN + r.a, vLm0 + r.aL, vRm0 + r.aR);
+    if (l123Out)
+        *l123Out = l123;
     // forward: waves
     real incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
     real a23[3] = {incU[1] - incU[0] * r.v[0], incU[2] - incU[0] * r.v[1], incU[3] - incU[0] * r.v[2]};
@@ -98,7 +102,7 @@ DNDSB_D void roe0_diss_rev(const real *incU, const real *n, const RoeAvg &r, rea
         rb.a += n[d] * (A4 - A0) * Fb[1 + d];
         rb.v[d] += t[d] * Fb[4] + (A0 + A4 + A1) * Fb[1 + d];
     }
-    real l0b = wa0 * A0b, l123b = wa1 * A1b, l4b = wa4 * A4b;
+    real l0b = wa0 * A0b, l123b = wa1 * A1b + l123bIn, l4b = wa4 * A4b;
     real wa0b = l0 * A0b, wa1b = l123 * A1b, wa4b = l4 * A4b;
     real a23Tb[3];
     for (int d = 0; d < 3; d++)

@@ -202,6 +202,9 @@ int roe_scheme_of(int rsType);
 // (adjoint_fast.cu); ST_UNSUPPORTED outside its instantiations
 int rhs_vjp_interior_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, bool hllep, const real *w, const real *u,
                           const real *uRec, real *faceAdj, cudaStream_t st);
+// the same for the SA model (adjoint_fast_sa.cu): 6 variables, plain Roe with the viscous flux, 3-D, VR degree 1-2
+int rhs_vjp_interior_fast_sa(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec,
+                             real *faceAdj, cudaStream_t st);
 int rhs_vjp_roe_interior(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec,
                          real *faceAdj, cudaStream_t st, bool *viscDone);
 // adjoint building blocks (adjoint_ops.cu)
