@@ -10,7 +10,13 @@ C1: isentropic vortex (strength 5) on periodic [0,10]^2, 64 x 64 quads split int
 C2: Taylor-Green vortex (Re 1600, Mach 0.1) on 24^3 jittered hexahedra, VR degree 2, HLLE+ with the
     compact viscous flux, ESDIRK4 (dt 0.05, 8 pseudo-iterations of one LU-SGS pair per stage) for 20
     steps: the kinetic-energy history E_k(t) and the dissipation rate -dE_k/dt, GPU against oracle (1e-8).
-Both runs take minutes on the oracle side (OpenMP on the host cores)."""
+C3 (reduced): the steady transonic bump of the steady configuration (BCFar in/out, BCWallInvis floor and
+    ceiling, BCSym sides, Mach 0.8, VR degree 1, Roe_M2) on 2,304 tetrahedra, BDF1 at CFL 200 with GMRES(30)
+    preconditioned by one LU-SGS pair, 4,000 pseudo-iterations from the free stream on each side (a residual
+    drop near 1e-10): the GPU's converged state against the oracle's (1e-8, the converged-state bound), the
+    GPU solving with its native FP64 and FP32 linear solves, the oracle with the restated GMRES on its own
+    operators.
+The runs take minutes on the oracle side (OpenMP on the host cores)."""
 import dataclasses
 
 import numpy as np
@@ -109,3 +115,29 @@ def test_c2_tgv_dissipation_history_matches_oracle():
     assert np.all(np.abs(rate_g - rate_o) <= 1e-8 * np.abs(rate_o).max())
     assert np.all(rate_g > 0)
     assert relerr(u.cpu().numpy(), u_o.numpy()) < 1e-8
+
+
+def test_c3_converged_state_matches_oracle():
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction, euler_bc_dir_weights
+    from tests.bump_case import bump_oracle
+    m = M.renumber_by_color(M.bump_channel_tet(16, 8, 3))
+    o, far, types, vals, w = bump_oracle(m, 1, "Roe_M2", 0.0, 1, intOrder=2)
+    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1, intOrder=2)).construct(euler_bc_dir_weights(types))
+    ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType="Roe_M2", muGas=0.0, ignoreVis=True))
+    ev.SetBC(types, vals)
+    kw = dict(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=4000, nTimeStepInternalMin=4000, CFL=200.0, gmresCode=1,
+              nGmresSpace=30, nGmresIter=1, sgsIter=0, rhsThresholdInternal=1e-10)
+    states = {}
+    for prec in ("fp64", "fp32"):
+        u = vr.BuildUDof(5)
+        u[:] = torch.tensor(far, device="cuda")
+        cfg = I.SolverConfig(**kw, linear_precision=prec)
+        I.ImplicitSolver(vr, ev, cfg).run(u)
+        assert cfg.res_history[-1][2] < 1e-9, (prec, cfg.res_history[-1])
+        states[prec] = u.cpu().numpy()
+    u_o = torch.tensor(np.tile(far, (m.n_cell, 1)))
+    cfg_o = I.SolverConfig(**kw, native_linear=False)
+    I.ImplicitSolver(OracleVR(o), OracleEval(o), cfg_o).run(u_o)
+    assert cfg_o.res_history[-1][2] < 1e-9, cfg_o.res_history[-1]
+    for prec, ug in states.items():
+        assert relerr(ug, u_o.numpy()) < 1e-8, (prec, relerr(ug, u_o.numpy()))
