@@ -406,6 +406,22 @@ class ImplicitSolver:
             self.CFLNow = cfg.CFL
         return stop
 
+    # restart (EulerSolver_PrintData.hxx:886-1073 PrintRestart / ReadRestart): the state u and the solver's
+    # running reconstruction, as a raw binary dump (dndsr_b200.checkpoint)
+    def save_state(self, path, u, **meta):
+        from .checkpoint import save_state
+        save_state(path, u, self.uRec, **meta)
+
+    def restore_state(self, path, u):
+        """Loads a dump into u and the running reconstruction; returns its metadata."""
+        from .checkpoint import load_state
+        a, b, meta = load_state(path, device=u.device)
+        if tuple(a.shape) != tuple(u.shape) or tuple(b.shape) != tuple(self.uRec.shape):
+            raise ValueError(f"restore_state: dump shapes {tuple(a.shape)}, {tuple(b.shape)} do not match the solver's")
+        u.copy_(a)
+        self.uRec.copy_(b)
+        return meta
+
     def run(self, u, n_steps=None, dt=None):
         cfg = self.cfg
         ode = ESDIRK(1 if cfg.odeCode == 0 else 0) if cfg.odeCode in (0, 101) else BDF1Stepper()
