@@ -39,6 +39,29 @@ struct FaceData
 static_assert(sizeof(FaceData) == 29 * sizeof(real), "FaceData layout");
 
 // u + phi . uRec and the gradient D1 phi . uRec of one cell at point p (VariationalReconstruction.hpp:378-442 rows 0..dim)
+// u + phi . uRec of one cell at point p, without the gradient
+template <int DIM, int P, int NV>
+DNDSB_D void recon_value(const real *cell, const real *p, real *U)
+{
+    using Lt = Layout<DIM, P, NV>;
+    const real *rec = cell, *uu = cell + Lt::OU, *cent = cell + Lt::OC, *iL = cell + Lt::OL, *mom = cell + Lt::OM;
+    real x = (p[0] - cent[0]) * iL[0], y = (p[1] - cent[1]) * iL[1], z = DIM == 3 ? (p[2] - cent[2]) * iL[2] : 0.0;
+    real px[4] = {1, x, x * x, x * x * x}, py[4] = {1, y, y * y, y * y * y}, pz[4] = {1, z, z * z, z * z * z};
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+        U[v] = uu[v];
+#pragma unroll
+    for (int k = 1; k < Lt::NDOF; k++)
+    {
+        const int c = mcode(DIM, k);
+        const real phi = px[c & 3] * py[(c >> 2) & 3] * pz[(c >> 4) & 3] - mom[k];
+        const real *r = rec + (k - 1) * NV;
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+            U[v] += phi * r[v];
+    }
+}
+
 template <int DIM, int P, int NV, bool ACC>
 DNDSB_D void recon_point(const real *cell, const real *p, real *U, real *G)
 {
