@@ -207,6 +207,10 @@ class SolverConfig:
     gmresScale: int = 0
     linear_precision: str = "fp64"   # "fp32": FP32 preconditioner / GMRES inside the FP64 defect correction
     vr_precision: str = "fp64"       # coefficient precision of the VR sweeps
+    # with vr_precision "fp32": the sweeps use FP32 coefficients only while the stage's relative residual is
+    # above vrFP64Below and FP64 ones from then on, so that the stage converges to the FP64 fixed point
+    # (0: FP32 throughout, whose fixed point differs by ~1e-7 relative)
+    vrFP64Below: float = 0.0
     native_linear: bool = True       # one device call per linear solve (dndsb_eval_solve_linear) when the evaluator has it
     meanScale: tuple = ()            # GMRES dot weights (gmresScale), empty = ones
     # positivity-preserving increments (timeMarchControl.incrementPPRelax, uRecAlphaCompressPower,
@@ -242,6 +246,7 @@ class ImplicitSolver:
         self.resBase = None
         self.CFLNow = cfg.CFL
         self.n_rhs = 0
+        self.vrPrec = cfg.vr_precision  # the sweeps' coefficient precision of the next pseudo-iteration
         self.n_sgs = 0
         self.gmresRec = None
         self.uRecLim = None
@@ -306,7 +311,7 @@ class ImplicitSolver:
         if self.cfg.recLinearScheme == 1:
             self._rec_gmres(cx)
         for _ in range(self.cfg.nInternalRecStep if self.cfg.recLinearScheme == 0 else 0):
-            self.vr.DoReconstructionIter(self.uRec, self.uRecNew, cx, putIntoNew=False, precision=self.cfg.vr_precision)
+            self.vr.DoReconstructionIter(self.uRec, self.uRecNew, cx, putIntoNew=False, precision=self.vrPrec)
         if self.uRecLim is not None:
             si = self.vr.DoCalculateSmoothIndicator(cx, self.uRec)
             self.ev.DoLimiterWBAP_C(cx, self.uRec, si, self.uRecLim, self.cfg.smoothThreshold, self.cfg.WBAP_nStd, False)
@@ -398,6 +403,12 @@ class ImplicitSolver:
         self.resBase = np.maximum(self.resBase, nrm)
         rel = nrm / (self.resBase + VERY_SMALL)
         stop = bool(rel[0] < cfg.rhsThresholdInternal) and it >= cfg.nTimeStepInternalMin
+        if cfg.vr_precision == "fp32" and cfg.vrFP64Below > 0:
+            # FP32 sweep coefficients far from convergence, FP64 ones below the threshold (latched for the stage)
+            if it == 1:
+                self.vrPrec = "fp32"
+            if rel[0] < cfg.vrFP64Below:
+                self.vrPrec = "fp64"
         cfg.res_history.append((stage, it, float(rel[0])))
         if cfg.nCFLRampStart <= it <= cfg.nCFLRampLength + cfg.nCFLRampStart:
             inter = (it - cfg.nCFLRampStart) / cfg.nCFLRampLength
