@@ -4,7 +4,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["setup.cu", "hotpath.cu", "fast.cu", "reduce.cu", "linsolve.cu", "bc.cu", "adjoint.cu", "adjoint_roe.cu", "adjoint_fast.cu", "adjoint_fast_sa.cu", "adjoint_visc.cu", "adjoint_ops.cu", "adjoint_geom.cu", "adjoint_geom2d.cu", "adjoint_generic.cu", "adjoint_generic_p1n5.cu", "adjoint_generic_p1n6.cu", "adjoint_generic_p2n5.cu", "adjoint_generic_p2n6.cu", "positivity.cu", "limiter.cu", "capi.cu", "noalloc.cu"]
+SRC = ["setup.cu", "hotpath.cu", "fast.cu", "reduce.cu", "linsolve.cu", "bc.cu", "adjoint.cu", "adjoint_roe.cu", "adjoint_fast.cu", "adjoint_fast_sa.cu", "adjoint_visc.cu", "adjoint_ops.cu", "adjoint_geom.cu", "adjoint_geom2d.cu", "adjoint_generic.cu", "adjoint_generic_p1n5.cu", "adjoint_generic_p1n6.cu", "adjoint_generic_p2n5.cu", "adjoint_generic_p2n6.cu", "positivity.cu", "limiter.cu", "capi.cu", "noalloc.cu", "roejac.cu"]
 LIB = os.path.join(HERE, "libdndsb.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

@@ -87,8 +87,10 @@ DNDSB_GLOBAL void k_vr_bc(MeshD m, GeomD g, VRD vr, const TC *__restrict__ AAInv
 // gradient on both sides (:360-362), GRP distance from the face centre (:363-386) and no
 // viscous flux on slip, far-field and outflow faces (:423-430, EvaluateDt.hxx:1203-1207)
 template <int DIM, int P, int NV>
+// lam (may be nullptr): [3][nFace] face integrals of the eigenvalues l0, l123, l4 divided by the area (useRoeJacobian)
 DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec,
-                           const real *__restrict__ uRecG, const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
+                           const real *__restrict__ uRecG, const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err,
+                           real *__restrict__ lam)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     const real gamma = s.gamma;
@@ -110,7 +112,7 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
         real dc[3];
         for (int d = 0; d < 3; d++)
             dc[d] = g.faceCent[f * 3 + d] - g.cellBary[c0 * 3 + d];
-        real fluxEs[NV];
+        real fluxEs[NV], lamEs[3] = {0, 0, 0};
         for (int v = 0; v < NV; v++)
             fluxEs[v] = 0;
         for (int q = 0; q < g.nGf; q++)
@@ -168,7 +170,11 @@ DNDSB_GLOBAL void k_rhs_bc(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const rea
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
             for (int v = 0; v < NV; v++)
                 fluxEs[v] -= (F[v] - Fv[v]) * JW;
+            lamEs[0] += l0 * JW, lamEs[1] += l1 * JW, lamEs[2] += l4 * JW;
         }
+        if (lam)
+            for (int i = 0; i < 3; i++)
+                lam[i * m.nFace + f] = lamEs[i] / g.faceArea[f];
         bool fin = true;
         for (int v = 0; v < NV; v++)
             fin = fin && isfinite(fluxEs[v]);
@@ -223,19 +229,22 @@ int rhs_bc_p(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, con
     case 1:
     {
         auto k = k_rhs_bc<DIM, 1, NV>;
-        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord);
+        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord,
+                     ev.jacMode == 2 ? ev.lambdaFace0 : nullptr);
         return ST_OK;
     }
     case 2:
     {
         auto k = k_rhs_bc<DIM, 2, NV>;
-        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord);
+        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord,
+                     ev.jacMode == 2 ? ev.lambdaFace0 : nullptr);
         return ST_OK;
     }
     case 3:
     {
         auto k = k_rhs_bc<DIM, 3, NV>;
-        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord);
+        DNDSB_LAUNCH(k, m.nBndFace, 64, st, m, g, vr, ev.s, u, uRec, uRecG, ev.deltaLambdaCell, ff, ev.errWord,
+                     ev.jacMode == 2 ? ev.lambdaFace0 : nullptr);
         return ST_OK;
     }
     }

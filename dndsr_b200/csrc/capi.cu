@@ -555,6 +555,7 @@ extern "C"
         }
         cudaMemset(e->e.deltaLambdaCell, 0, sizeof(real) * m.nCell);
         cudaMemset(e->e.lambdaFace, 0, sizeof(real) * m.nFace);
+        cudaMemset(e->e.lambdaConv, 0, sizeof(real) * m.nFace);
         cudaMemset(e->e.errDeferred, 0, sizeof(int));
         cudaMemset(e->e.fluxWall, 0, sizeof(real) * 8);
         *out = e;
@@ -593,7 +594,7 @@ extern "C"
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
                         (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource,
-                        (void *)e->e.errDeferred, (void *)e->e.fluxWall, (void *)e->e.objDir})
+                        (void *)e->e.errDeferred, (void *)e->e.fluxWall, (void *)e->e.objDir, (void *)e->e.lambdaFace0})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -776,11 +777,55 @@ extern "C"
         return status_msg(rc, "dndsb_eval_rhs_jvp");
     }
 
+    int dndsb_eval_set_jacobian_mode(dndsb_eval *e, int useScalarJacobian, int useRoeJacobian)
+    {
+        if (!e)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_jacobian_mode: null argument");
+        if (useScalarJacobian && useRoeJacobian) // EulerEvaluatorSettings.hpp:416-417
+            return fail(DNDSB_E_BADARG, "dndsb_eval_set_jacobian_mode: useScalarJacobian and useRoeJacobian are mutually exclusive");
+        if (useRoeJacobian && !e->e.lambdaFace0)
+        {
+            const MeshD &m = e->vr->mesh->d;
+            if (dev_alloc((void **)&e->e.lambdaFace0, sizeof(real) * 3 * m.nFace) != cudaSuccess)
+                return cuda_fail("dndsb_eval_set_jacobian_mode");
+            e->e.lambdaFace123 = e->e.lambdaFace0 + m.nFace, e->e.lambdaFace4 = e->e.lambdaFace0 + 2 * m.nFace;
+            // the convective speed of the last EvaluateDt until the next EvaluateRHS records the eigenvalues
+            for (real *l : {e->e.lambdaFace0, e->e.lambdaFace123, e->e.lambdaFace4})
+                if (cudaMemcpy(l, e->e.lambdaConv, sizeof(real) * m.nFace, cudaMemcpyDeviceToDevice) != cudaSuccess)
+                    return cuda_fail("dndsb_eval_set_jacobian_mode");
+        }
+        e->e.jacMode = useRoeJacobian ? 2 : (useScalarJacobian ? 0 : 1);
+        return DNDSB_OK;
+    }
+
     int dndsb_eval_lusgs_matrix_init(dndsb_eval *e, const double *dTau, double dt, double alphaDiag, double *jdiag, void *stream)
     {
         if (!e || !dTau || !jdiag)
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_init: null argument");
+        if (e->e.jacMode == 2)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_init: the Roe Jacobian needs u: use dndsb_eval_lusgs_matrix_init_full");
+        if (e->e.jacMode == 1)
+            return dndsb_eval_lusgs_matrix_init_full(e, dTau, dt, alphaDiag, nullptr, nullptr, 0, 0.0, jdiag, stream);
         return status_msg(lusgs_init(e->vr->mesh->d, e->vr->g, e->e, dTau, dt, alphaDiag, jdiag, S(stream)), "dndsb_eval_lusgs_matrix_init");
+    }
+
+    int dndsb_eval_lusgs_matrix_init_full(dndsb_eval *e, const double *dTau, double dt, double alphaDiag, const double *u, const double *uRec,
+                                          int jacobianCode, double t, double *jdiag, void *stream)
+    {
+        (void)uRec, (void)t; // read by neither the scalar nor the block branch of the reference (EulerEvaluator.hxx:37-159)
+        if (!e || !dTau || !jdiag || (e->e.jacMode == 2 && !u))
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_init_full: null argument");
+        if (jacobianCode != 0) // EulerEvaluator.hxx:49
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_init_full: jacobianCode must be 0");
+        const MeshD &m = e->vr->mesh->d;
+        if (e->e.jacMode == 0)
+            return status_msg(lusgs_init(m, e->vr->g, e->e, dTau, dt, alphaDiag, jdiag, S(stream)), "dndsb_eval_lusgs_matrix_init_full");
+        if (e->e.jacMode == 2 && m.nBndFace > 0 && !e->vr->vr.bnd.type)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_init_full: set the boundary table first");
+        int rc = lusgs_init_block(m, e->vr->g, e->vr->vr, e->e, dTau, dt, alphaDiag, u, jdiag, S(stream));
+        if (rc == ST_NONFINITE)
+            return fail(DNDSB_E_NONFINITE, "dndsb_eval_lusgs_matrix_init_full: singular or non-finite diagonal block");
+        return status_msg(rc, "dndsb_eval_lusgs_matrix_init_full");
     }
 
     int dndsb_eval_update_sgs(dndsb_eval *e, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
@@ -790,6 +835,10 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs: null argument");
         if (uInc == uIncNew)
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs: uInc and uIncNew must differ"); // EulerEvaluator.hxx:563
+        if (e->e.jacMode)
+            return status_msg(update_sgs_block(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate,
+                                               uIncIsZero, sumIncHost, S(stream)),
+                              "dndsb_eval_update_sgs");
         return status_msg(update_sgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate, uIncIsZero,
                                      sumIncHost, S(stream)),
                           "dndsb_eval_update_sgs");
@@ -800,6 +849,9 @@ extern "C"
     {
         if (!e || !rhs || !u || !uInc || !jdiag || !uIncNew)
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_lusgs_forward: null argument");
+        if (e->e.jacMode)
+            return status_msg(update_lusgs_block(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, 1, S(stream)),
+                              "dndsb_eval_update_lusgs_forward");
         return status_msg(update_lusgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, 1, S(stream)),
                           "dndsb_eval_update_lusgs_forward");
     }
@@ -809,6 +861,9 @@ extern "C"
     {
         if (!e || !rhs || !u || !uInc || !jdiag || !uIncNew)
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_lusgs_backward: null argument");
+        if (e->e.jacMode)
+            return status_msg(update_lusgs_block(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, 0, S(stream)),
+                              "dndsb_eval_update_lusgs_backward");
         return status_msg(update_lusgs(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, 0, S(stream)),
                           "dndsb_eval_update_lusgs_backward");
     }
@@ -826,6 +881,9 @@ extern "C"
     {
         if (!e || !u || !uInc || !jdiag || !AuInc)
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_vec: null argument");
+        if (e->e.jacMode)
+            return status_msg(lusgs_matvec_block(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, uInc, jdiag, AuInc, S(stream)),
+                              "dndsb_eval_lusgs_matrix_vec");
         return status_msg(lusgs_matvec(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, uInc, jdiag, AuInc, S(stream)),
                           "dndsb_eval_lusgs_matrix_vec");
     }
@@ -835,6 +893,8 @@ extern "C"
     {
         if (!e || !u || !y || !jdiag || !ATy || y == ATy)
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_vec_t: null or aliased argument");
+        if (e->e.jacMode)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_lusgs_matrix_vec_t: the transposed operators take the scalar Jacobian");
         return status_msg(lusgs_matvec_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, y, jdiag, ATy, S(stream)),
                           "dndsb_eval_lusgs_matrix_vec_t");
     }
@@ -846,6 +906,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: null argument or bad precision");
         if (y == yNew)
             return fail(DNDSB_E_BADARG, "dndsb_eval_update_sgs_t: y and yNew must differ");
+        if (e->e.jacMode)
+            return fail(DNDSB_E_UNSUPPORTED, "dndsb_eval_update_sgs_t: the transposed operators take the scalar Jacobian");
         return status_msg(update_sgs_t(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, b, u, y, yNew, jdiag, forward, gsUpdate, precision, S(stream)),
                           "dndsb_eval_update_sgs_t");
     }
@@ -955,7 +1017,7 @@ extern "C"
             double inv = 1.0 / (ms + 1e-200);
             s.scale2[v] = inv * inv;
         }
-        int rc = linear_solve(e->vr->mesh->d, e->vr->g, e->e, e->lin, s, alphaDiag, dTau, dt, u, rhs, xInc, S(stream));
+        int rc = linear_solve(e->vr->mesh->d, e->vr->g, e->vr->vr.bnd, e->e, e->lin, s, alphaDiag, dTau, dt, u, rhs, xInc, S(stream));
         if (rc == ST_BADARG)
             return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..1, nGmresSpace 1..32, precision 0..1");
         return status_msg(rc, "dndsb_eval_solve_linear");
@@ -1029,6 +1091,9 @@ extern "C"
         else if (n == "faceFlux") src = e->e.faceFlux, cnt = m.nFace * e->e.s.nVars;
         else if (n == "jSource" && e->e.jSource) src = e->e.jSource, cnt = m.nCell * e->e.s.nVars;
         else if (n == "fluxWallSum") src = e->e.fluxWall, cnt = e->e.s.nVars;
+        else if (n == "lambdaFace0" && e->e.lambdaFace0) src = e->e.lambdaFace0, cnt = m.nFace;
+        else if (n == "lambdaFace123" && e->e.lambdaFace0) src = e->e.lambdaFace123, cnt = m.nFace;
+        else if (n == "lambdaFace4" && e->e.lambdaFace0) src = e->e.lambdaFace4, cnt = m.nFace;
         else
             return fail(DNDSB_E_BADARG, "dndsb_eval_get_array: unknown name " + n);
         if (len)

@@ -37,11 +37,13 @@ constexpr int min_blocks() { return (DNDSB_RHS_WARPS_PER_SM / NG) > 0 ? (DNDSB_R
 // evaluators that ignore viscosity).  Splitting a viscous evaluation into an inviscid and a viscous launch
 // measured 1.63 ms against 0.94 ms for one MODE 0 launch on the TGV workload (the staging and the point
 // values done twice), so viscous evaluations stay in one launch.
-template <int DIM, int P, int NV, int NG, int MODE>
+// LAM: also record the face integrals of the Riemann eigenvalues divided by the area into lam [3][nFace]
+// (EvaluateRHS.hxx:527-545, for useRoeJacobian); a separate instantiation, so the default one is unchanged
+template <int DIM, int P, int NV, int NG, int MODE, bool LAM>
 __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
     k_rhs_face_fast(MeshD m, GeomD g, const real *__restrict__ facePt, const real *__restrict__ cellPar, const real *__restrict__ moment,
                     EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec, const real *__restrict__ dLamCell,
-                    real *__restrict__ faceFlux, int *err)
+                    real *__restrict__ faceFlux, int *err, real *__restrict__ lam)
 {
     using Lt = Layout<DIM, P, NV>;
     constexpr int CS = Lt::CS, R = Lt::R, NDOF = Lt::NDOF;
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
         }
     }
     __syncthreads();
-    real out[NV];
+    real out[NV], lw[3] = {0, 0, 0};
 #pragma unroll
     for (int v = 0; v < NV; v++)
         out[v] = 0;
@@ -183,6 +185,8 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
 #pragma unroll
         for (int v = 0; v < NV; v++)
             out[v] = -(F[v] - Fv[v]) * JW;
+        if constexpr (LAM)
+            lw[0] = l0 * JW, lw[1] = l1 * JW, lw[2] = l4 * JW;
         bool fin = true;
 #pragma unroll
         for (int v = 0; v < NV; v++)
@@ -206,6 +210,27 @@ __global__ void __launch_bounds__(32 * NG, min_blocks<NG>())
             for (int qq = 0; qq < NG; qq++)
                 acc += sFlux[(qq * 32 + fi) * NV + v];
             faceFlux[ff * NV + v] = acc;
+        }
+    }
+    if constexpr (LAM)
+    {
+        __syncthreads(); // sFlux is reused for the eigenvalues
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+            sFlux[(q * 32 + fl) * NV + i] = lw[i];
+        __syncthreads();
+        for (int e = tid; e < 32 * 3; e += blockDim.x)
+        {
+            int fi = e / 3, i = e - fi * 3;
+            int64_t ff = f0 + fi;
+            if (ff < m.nFace && sC[32 + fi] >= 0) // boundary faces are recorded by the boundary kernel
+            {
+                real acc = 0;
+#pragma unroll
+                for (int qq = 0; qq < NG; qq++)
+                    acc += sFlux[(qq * 32 + fi) * NV + i];
+                lam[i * m.nFace + ff] = acc / g.faceArea[ff];
+            }
         }
     }
 }
@@ -320,18 +345,33 @@ int launch_rhs_fast(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &
     cudaGetDevice(&dev);
     if (dev < 64 && !((attrSet >> dev) & 1ULL))
     {
-        if (cudaFuncSetAttribute(k_rhs_face_fast<DIM, P, NV, NG, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_rhs_face_fast<DIM, P, NV, NG, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        if (cudaFuncSetAttribute(k_rhs_face_fast<DIM, P, NV, NG, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_rhs_face_fast<DIM, P, NV, NG, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_rhs_face_fast<DIM, P, NV, NG, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_rhs_face_fast<DIM, P, NV, NG, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return ST_CUDA;
         attrSet |= 1ULL << dev;
     }
     unsigned nb = (unsigned)((m.nFace + 31) / 32);
+    real *lam = ev.jacMode == 2 ? ev.lambdaFace0 : nullptr;
+#define DNDSB_RFF(MODE, LAM)                                                                                                                  \
+    k_rhs_face_fast<DIM, P, NV, NG, MODE, LAM><<<nb, 32 * NG, smem, st>>>(m, g, ev.facePt, ev.cellPar, vr.baseMoment, ev.s, u, uRec,            \
+                                                                          ev.deltaLambdaCell, ff, ev.errWord, lam)
     if (ev.s.ignoreVis)
-        k_rhs_face_fast<DIM, P, NV, NG, 1><<<nb, 32 * NG, smem, st>>>(m, g, ev.facePt, ev.cellPar, vr.baseMoment, ev.s, u, uRec,
-                                                                     ev.deltaLambdaCell, ff, ev.errWord);
+    {
+        if (lam)
+            DNDSB_RFF(1, true);
+        else
+            DNDSB_RFF(1, false);
+    }
     else
-        k_rhs_face_fast<DIM, P, NV, NG, 0><<<nb, 32 * NG, smem, st>>>(m, g, ev.facePt, ev.cellPar, vr.baseMoment, ev.s, u, uRec,
-                                                                     ev.deltaLambdaCell, ff, ev.errWord);
+    {
+        if (lam)
+            DNDSB_RFF(0, true);
+        else
+            DNDSB_RFF(0, false);
+    }
+#undef DNDSB_RFF
     return ST_OK;
 }
 

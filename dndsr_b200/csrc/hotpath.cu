@@ -97,8 +97,11 @@ DNDSB_GLOBAL void k_swap(int64_t n, real *a, real *b)
 template <int DIM, int P, int NV>
 // uRecG: the reconstruction the gradients come from (the reference's uRecUnlim, EvaluateRHS.hxx:264-327;
 // the same array as uRec when there is no limiter); point values come from uRec
+// lam (may be nullptr): [3][nFace] face integrals of the Riemann eigenvalues l0, l123, l4 divided by the area
+// (EvaluateRHS.hxx:527-545, recorded for useRoeJacobian)
 DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const real *__restrict__ u, const real *__restrict__ uRec,
-                             const real *__restrict__ uRecG, const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err)
+                             const real *__restrict__ uRecG, const real *__restrict__ dLamCell, real *__restrict__ faceFlux, int *err,
+                             real *__restrict__ lam)
 {
     constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1;
     const real gamma = s.gamma, cp = s.Rgas * gamma / (gamma - 1);
@@ -124,6 +127,7 @@ DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const r
             db[d] = g.cellBary[c1 * 3 + d] - m.facePShift[f * 3 + d] - g.cellBary[c0 * 3 + d];
         real areaInv2 = 2.0 / g.faceArea[f];
         bool bad = false;
+        real lamEs[3] = {0, 0, 0};
         for (int q = 0; q < g.nGf; q++)
         {
             const real *n = &g.faceNorm[(f * g.nGf + q) * 3];
@@ -181,11 +185,15 @@ DNDSB_GLOBAL void k_rhs_face(MeshD m, GeomD g, VRD vr, EulerSettingsD s, const r
             real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q];
             for (int v = 0; v < NV; v++)
                 fluxEs[v] -= (F[v] - Fv[v]) * JW;
+            lamEs[0] += l0 * JW, lamEs[1] += l1 * JW, lamEs[2] += l4 * JW;
         }
         if (bad || !finite5(fluxEs, NV))
             atomicOr(err, bad ? (int)DE_NONPHYSICAL : (int)DE_NONFINITE);
         for (int v = 0; v < NV; v++)
             faceFlux[f * NV + v] = fluxEs[v];
+        if (lam)
+            for (int i = 0; i < 3; i++)
+                lam[i * m.nFace + f] = lamEs[i] / g.faceArea[f];
     }
 }
 
@@ -671,12 +679,14 @@ int eval_rhs_ex(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const 
     else
         dev_zero(ev.errWord, sizeof(int), st);
     const EulerSettingsD &s = evc.s;
+    real *lamOut = ev.jacMode == 2 ? ev.lambdaFace0 : nullptr; // [3][nFace]: lambdaFace0, 123, 4
     int frc = uRecG == uRec ? rhs_face_fast(m, g, vr, evc, u, uRec, ff, st) : (int)ST_UNSUPPORTED;
     if (frc == ST_CUDA)
         return ST_CUDA;
     if (frc != ST_OK)
     {
-#define DNDSB_RF(D, PP, NVV) DNDSB_LAUNCH((k_rhs_face<D, PP, NVV>), m.nFace, 128, st, m, g, vr, s, u, uRec, uRecG, ev.deltaLambdaCell, ff, evc.errWord)
+#define DNDSB_RF(D, PP, NVV) \
+    DNDSB_LAUNCH((k_rhs_face<D, PP, NVV>), m.nFace, 128, st, m, g, vr, s, u, uRec, uRecG, ev.deltaLambdaCell, ff, evc.errWord, lamOut)
 #define DNDSB_RF_P(D, NVV)        \
     do                            \
     {                             \
@@ -765,6 +775,9 @@ int eval_dt(const MeshD &m, const GeomD &g, EvalD &ev, const real *u, real CFL, 
     else
         return ST_UNSUPPORTED;
     DNDSB_LAUNCH(k_dt_cell, m.nCell, 256, st, m, g, ev.lambdaFace, ev.deltaLambdaFace, CFL, MaxDt, dt, ev.deltaLambdaCell);
+    if (ev.lambdaFace0) // lambdaFace0 = lambdaFace123 = lambdaFace4 = the convective speed (EvaluateDt.hxx:995-996)
+        for (real *l : {ev.lambdaFace0, ev.lambdaFace123, ev.lambdaFace4})
+            d2d(l, ev.lambdaConv, sizeof(real) * m.nFace, st);
     if (useLocalDt && !dtMin) // nothing to reduce and nothing to report: no host synchronisation
         return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
     real *res = reduce_cols(1, m.nCell, 1, dt, nullptr, 0, ev.redBuf, st);

@@ -21,10 +21,16 @@
 // both cases.  Reductions use a fixed partition and fixed trees, so results
 // are bitwise reproducible.
 //
+// Block mode (useScalarJacobian false, optionally useRoeJacobian): the operator is kept as dense blocks,
+// per position the diagonal block and its inverse, per (position, face slot) the off-diagonal block
+// (alpha/2)(A_f/V_c) dF/dU_o (the reference's fluxJacobian0_Right_Times_du_AsMatrix, the same blocks its
+// local LU assembles, EulerEvaluator.hxx:290-359), built in FP64 and stored in T.
+//
 // GMRES scalars (Hessenberg, norms, least-squares solution, breakdown index)
 // never leave the device: the whole solve is a fixed kernel sequence and is
 // captured once into a CUDA graph that later solves replay.
 #include "solver.cuh"
+#include "roejac.cuh"
 
 namespace dndsb
 {
@@ -212,6 +218,128 @@ DNDSB_GLOBAL void k_matvec_pos(int64_t n, const int32_t *__restrict__ nbrPos, co
     }
 }
 
+// block operator build: diagonal block + inverse [p][2][NV][NV], off-diagonal blocks [p][NF][NV][NV] (zero on boundaries)
+template <typename T, int NV>
+DNDSB_GLOBAL void k_sgsop_build_blk(MeshD m, GeomD g, BoundaryD bnd, EvalD ev, int roe, const real *__restrict__ dTau, real dt, real alphaDiag,
+                                    const real *__restrict__ u, const int32_t *__restrict__ cellPos, int32_t *nbrPos, T *opB, T *jdB, int *err)
+{
+    using namespace roej;
+    DNDSB_KERNEL_LOOP(p, m.nCell)
+    {
+        int64_t c = m.colorCells[p];
+        real B[NV * NV], Bi[NV * NV];
+        cell_block<NV>(m, g, bnd, ev, roe != 0, dTau, dt, alphaDiag, u, c, B);
+        if (!block_inv<NV>(B, Bi))
+        {
+            atomicOr(err, (int)DE_SINGULAR);
+            for (int i = 0; i < NV * NV; i++)
+                Bi[i] = 0;
+        }
+        T *jo = jdB + p * 2 * NV * NV;
+        for (int i = 0; i < NV * NV; i++)
+            jo[i] = (T)B[i], jo[NV * NV + i] = (T)Bi[i];
+        const real cf = 0.5 * alphaDiag / g.vol[c];
+        for (int k = 0; k < m.nf; k++)
+        {
+            int o = m.cellNbr[c * m.nf + k];
+            nbrPos[p * m.nf + k] = o < 0 ? -1 : cellPos[o];
+            T *ob = opB + (p * m.nf + k) * NV * NV;
+            if (o < 0)
+            {
+                for (int i = 0; i < NV * NV; i++)
+                    ob[i] = 0;
+                continue;
+            }
+            int pk = m.cell2face[c * m.nf + k];
+            int64_t f = pk >> 1;
+            int side = pk & 1;
+            real sg = side ? -1.0 : 1.0;
+            real n[3] = {g.faceMeanNorm[f * 3] * sg, g.faceMeanNorm[f * 3 + 1] * sg, g.faceMeanNorm[f * 3 + 2] * sg};
+            FaceLam L;
+            if (roe)
+                L = face_lam(ev, f, side);
+            else
+                L.main = ev.lambdaFace[f], L.l0 = L.l123 = L.l4 = L.vis = 0;
+            real w = cf * g.faceArea[f];
+            for (int i = 0; i < NV; i++)
+            {
+                real e[NV], col[NV];
+                for (int v = 0; v < NV; v++)
+                    e[v] = v == i ? 1.0 : 0.0;
+                nbr_inc<NV>(roe != 0, u + (int64_t)o * NV, u + c * NV, n, e, L, ev.s.gamma, col);
+                for (int v = 0; v < NV; v++)
+                    ob[v * NV + i] = (T)(w * col[v]);
+            }
+        }
+    }
+}
+
+// one colour class of a sweep with the block operator: x_p = D_p^-1 (rhs_p - sum_k O_pk x_q)
+template <typename T, int NV, int NF>
+DNDSB_GLOBAL void k_sgs_pos_blk(int64_t pBeg, int64_t pEnd, const int32_t *__restrict__ nbrPos, const T *__restrict__ opB, const T *__restrict__ jdB,
+                                const T *__restrict__ rhs, const T *__restrict__ xOld, T *xNew, int forward, int gsUpdate, int uIncIsZero)
+{
+    DNDSB_KERNEL_LOOP(ii, pEnd - pBeg)
+    {
+        int64_t p = pBeg + ii;
+        T buf[NV], x[NV];
+        for (int v = 0; v < NV; v++)
+            buf[v] = rhs[p * NV + v];
+#pragma unroll
+        for (int k = 0; k < NF; k++)
+        {
+            int q = nbrPos[p * NF + k];
+            if (q < 0 || q == p)
+                continue;
+            bool useNew = gsUpdate && (forward ? q < pBeg : q >= pEnd);
+            if (uIncIsZero && !useNew)
+                continue;
+            const T *dU = (useNew ? xNew : xOld) + (int64_t)q * NV;
+            const T *ob = opB + (p * NF + k) * NV * NV;
+            for (int r = 0; r < NV; r++)
+            {
+                T acc = 0;
+                for (int l = 0; l < NV; l++)
+                    acc += ob[r * NV + l] * dU[l];
+                buf[r] -= acc;
+            }
+        }
+        roej::block_mul<NV>(jdB + p * 2 * NV * NV + NV * NV, buf, x);
+        for (int v = 0; v < NV; v++)
+            xNew[p * NV + v] = x[v];
+    }
+}
+
+template <typename T, int NV, int NF>
+DNDSB_GLOBAL void k_matvec_pos_blk(int64_t n, const int32_t *__restrict__ nbrPos, const T *__restrict__ opB, const T *__restrict__ jdB,
+                                   const T *__restrict__ x, T *Ax, const real *__restrict__ xs)
+{
+    const T sx = xs ? (T)*xs : T(1);
+    DNDSB_KERNEL_LOOP(p, n)
+    {
+        T y[NV];
+        roej::block_mul<NV>(jdB + p * 2 * NV * NV, x + p * NV, y);
+#pragma unroll
+        for (int k = 0; k < NF; k++)
+        {
+            int q = nbrPos[p * NF + k];
+            if (q < 0)
+                continue;
+            const T *ob = opB + (p * NF + k) * NV * NV;
+            const T *xq = x + (int64_t)q * NV;
+            for (int r = 0; r < NV; r++)
+            {
+                T acc = 0;
+                for (int l = 0; l < NV; l++)
+                    acc += ob[r * NV + l] * xq[l];
+                y[r] += acc;
+            }
+        }
+        for (int v = 0; v < NV; v++)
+            Ax[p * NV + v] = sx * y[v];
+    }
+}
+
 // GMRES bookkeeping kernels on device scalars.  sc layout: [0] scale = |M b|,
 // [1] beta, [2] number of valid Arnoldi columns, [8 ...] least-squares y.
 constexpr int kScY = 8;
@@ -329,12 +457,13 @@ DNDSB_GLOBAL void k_copy_scalar(const real *a, real *b)
 // workspace owned by an evaluator handle
 struct LinWs
 {
-    int prec = -1, k = 0, nv = 0, nf = 0;
+    int prec = -1, k = 0, nv = 0, nf = 0, jacMode = 0;
     int64_t nCell = 0;
     int32_t *cellPos = nullptr, *nbrPos = nullptr;
     void *op = nullptr, *jd = nullptr, *uT = nullptr, *rhsT = nullptr, *x = nullptr, *tmp = nullptr, *tmp2 = nullptr, *MLb = nullptr,
          *V = nullptr;
     real *H = nullptr, *sc = nullptr, *s2 = nullptr, *red = nullptr;
+    void *opB = nullptr, *jdB = nullptr; // block mode: off-diagonal blocks [nCell][nf][nv][nv], diagonal blocks + inverses [nCell][2][nv][nv]
     real *colScale = nullptr; // [33] normalising factors of the stored (unnormalised) Krylov columns
     unsigned *cnt = nullptr;  // ticket counter of the one-launch reductions (zero between launches)
     cudaStream_t cs = nullptr;
@@ -348,7 +477,7 @@ void linws_free(LinWs *w)
 {
     if (!w)
         return;
-    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
+    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->opB, w->jdB, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
                     (void *)w->sc, (void *)w->s2, (void *)w->red, (void *)w->colScale, (void *)w->cnt})
         dev_free(p);
     graph_free(w->graph);
@@ -368,15 +497,18 @@ bool same_key(const LinSettings &a, const LinSettings &b)
     return true;
 }
 
-int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv)
+int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv, int jacMode)
 {
     int k = ls.gmresCode ? ls.nGmresSpace : 0;
     size_t es = ls.precision ? sizeof(float) : sizeof(double);
-    if (w && w->prec == ls.precision && w->k >= k && w->nv == nv && w->nCell == m.nCell)
+    if (w && w->prec == ls.precision && w->k >= k && w->nv == nv && w->nCell == m.nCell && (w->jacMode != 0) == (jacMode != 0))
+    {
+        w->jacMode = jacMode; // block with or without the Roe term: same storage, rebuilt by every solve
         return ST_OK;
+    }
     linws_free(w);
     w = new LinWs();
-    w->prec = ls.precision, w->k = k, w->nv = nv, w->nf = m.nf, w->nCell = m.nCell;
+    w->prec = ls.precision, w->k = k, w->nv = nv, w->nf = m.nf, w->nCell = m.nCell, w->jacMode = jacMode;
     int64_t n = m.nCell * nv;
     bool ok = dev_alloc((void **)&w->cellPos, sizeof(int32_t) * m.nCell) == cudaSuccess &&
               dev_alloc((void **)&w->nbrPos, sizeof(int32_t) * m.nCell * m.nf) == cudaSuccess &&
@@ -390,6 +522,8 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv)
               dev_alloc((void **)&w->s2, sizeof(real) * 8) == cudaSuccess &&
               dev_alloc((void **)&w->red, sizeof(real) * kRedBufLenK) == cudaSuccess &&
               dev_alloc((void **)&w->colScale, sizeof(real) * 33) == cudaSuccess && dev_alloc((void **)&w->cnt, sizeof(unsigned)) == cudaSuccess;
+    if (ok && jacMode)
+        ok = dev_alloc(&w->opB, es * nv * nv * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->jdB, es * 2 * nv * nv * m.nCell) == cudaSuccess;
     ok = ok && dev_zero(w->V, es * krylov_ld(n) * (k + 1), nullptr) == cudaSuccess; // the column pads stay zero
     ok = ok && dev_zero(w->cnt, sizeof(unsigned), nullptr) == cudaSuccess && dev_zero(w->colScale, sizeof(real) * 33, nullptr) == cudaSuccess;
     if (!ok || stream_create(&w->cs) != cudaSuccess || event_create(&w->evIn) != cudaSuccess || event_create(&w->evOut) != cudaSuccess)
@@ -425,6 +559,23 @@ struct Solve
     // one colour sweep over all classes; result in xNew
     void sweep(const T *rhs, const T *xOld, T *xNew, bool forward, bool gs, bool zeroIn) const
     {
+        if (w.jacMode)
+        {
+            auto kb = k_sgs_pos_blk<T, NV, NF>;
+            if (!gs)
+            {
+                DNDSB_LAUNCH(kb, m.nCell, 128, st, 0, m.nCell, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, rhs, xOld, xNew, (int)forward, 0,
+                             (int)zeroIn);
+                return;
+            }
+            for (int ci = 0; ci < m.nColor; ci++)
+            {
+                int col = forward ? ci : m.nColor - 1 - ci;
+                int64_t b = m.colorStart[col], e = m.colorStart[col + 1];
+                DNDSB_LAUNCH(kb, e - b, 128, st, b, e, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, rhs, xOld, xNew, (int)forward, 1, (int)zeroIn);
+            }
+            return;
+        }
         if (!gs)
         {
             auto kern = k_sgs_pos<T, NV, NF>;
@@ -460,6 +611,12 @@ struct Solve
     // xs: the normalising factor of x when x is a stored Krylov column (nullptr: 1)
     void FA(const T *x, T *Ax, const real *xs = nullptr) const
     {
+        if (w.jacMode)
+        {
+            auto kb = k_matvec_pos_blk<T, NV, NF>;
+            DNDSB_LAUNCH(kb, m.nCell, 128, st, m.nCell, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, x, Ax, xs);
+            return;
+        }
         auto kern = k_matvec_pos<T, NV, NF>;
         DNDSB_LAUNCH(kern, m.nCell, 128, st, m.nCell, w.nbrPos, (const T4 *)w.op, (const T *)w.jd, (const T *)w.uT, x,
                      Ax, gamma, xs);
@@ -522,8 +679,8 @@ struct Solve
 };
 
 template <typename T, int NV, int NF>
-int run(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
-        const real *u, const real *rhs, real *xInc, cudaStream_t st)
+int run(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs &w, const LinSettings &ls, real alphaDiag, const real *dTau,
+        real dt, const real *u, const real *rhs, real *xInc, cudaStream_t st)
 {
     using T4 = typename Vec4<T>::type;
     // the caller's stream -> the solver's stream
@@ -536,8 +693,17 @@ int run(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &
     auto kscatter = k_scatter_T<T, NV>;
     if (NV == 6 && !ev.jSource)
         return ST_BADARG;
-    DNDSB_LAUNCH(kbuild, m.nCell, 128, cs, m, g, ev.lambdaFace, dTau, dt, alphaDiag, u, ev.jSource, w.cellPos, w.nbrPos, (T4 *)w.op,
-                 (T *)w.jd, (T *)w.uT);
+    if (w.jacMode)
+    {
+        if (w.jacMode == 2 && (!ev.lambdaFace0 || (m.nBndFace > 0 && !bnd.type)))
+            return ST_BADARG;
+        auto kb = k_sgsop_build_blk<T, NV>;
+        DNDSB_LAUNCH(kb, m.nCell, 128, cs, m, g, bnd, ev, (int)(w.jacMode == 2), dTau, dt, alphaDiag, u, w.cellPos, w.nbrPos, (T *)w.opB,
+                     (T *)w.jdB, ev.errWord);
+    }
+    else
+        DNDSB_LAUNCH(kbuild, m.nCell, 128, cs, m, g, ev.lambdaFace, dTau, dt, alphaDiag, u, ev.jSource, w.cellPos, w.nbrPos, (T4 *)w.op,
+                     (T *)w.jd, (T *)w.uT);
     DNDSB_LAUNCH(kgather, m.nCell, 256, cs, m.nCell, m.colorCells, rhs, (T *)w.rhsT);
     Solve<T, NV, NF> S{m, w, ls, (T)ev.s.gamma, cs};
     if (ls.useGraph)
@@ -576,38 +742,38 @@ int run(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &
 }
 
 template <typename T, int NV>
-int run_nf(const MeshD &m, const GeomD &g, EvalD &ev, LinWs &w, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
-           const real *u, const real *rhs, real *xInc, cudaStream_t st)
+int run_nf(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs &w, const LinSettings &ls, real alphaDiag, const real *dTau,
+           real dt, const real *u, const real *rhs, real *xInc, cudaStream_t st)
 {
     switch (m.nf)
     {
     case 3:
-        return run<T, NV, 3>(m, g, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+        return run<T, NV, 3>(m, g, bnd, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
     case 4:
-        return run<T, NV, 4>(m, g, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+        return run<T, NV, 4>(m, g, bnd, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
     case 6:
-        return run<T, NV, 6>(m, g, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+        return run<T, NV, 6>(m, g, bnd, ev, w, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
     }
     return ST_UNSUPPORTED;
 }
 } // namespace
 
-int linear_solve(const MeshD &m, const GeomD &g, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
-                 const real *u, const real *rhs, real *xInc, cudaStream_t st)
+int linear_solve(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag,
+                 const real *dTau, real dt, const real *u, const real *rhs, real *xInc, cudaStream_t st)
 {
     if (ls.gmresCode < 0 || ls.gmresCode > 2 || ls.jacobiCode < 0 || ls.jacobiCode > 1 || ls.sgsIter < 0 || ls.nGmresIter < 0 ||
         (ls.gmresCode && (ls.nGmresSpace < 1 || ls.nGmresSpace > 32)) || ls.precision < 0 || ls.precision > 1)
         return ST_BADARG;
     int nv = ev.s.nVars;
-    int rc = ws_prepare(m, ws, ls, nv);
+    int rc = ws_prepare(m, ws, ls, nv, ev.jacMode);
     if (rc != ST_OK)
         return rc;
     if (nv == 5)
-        return ls.precision ? run_nf<float, 5>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
-                            : run_nf<double, 5>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+        return ls.precision ? run_nf<float, 5>(m, g, bnd, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
+                            : run_nf<double, 5>(m, g, bnd, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
     if (nv == 6)
-        return ls.precision ? run_nf<float, 6>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
-                            : run_nf<double, 6>(m, g, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
+        return ls.precision ? run_nf<float, 6>(m, g, bnd, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st)
+                            : run_nf<double, 6>(m, g, bnd, ev, *ws, ls, alphaDiag, dTau, dt, u, rhs, xInc, st);
     return ST_UNSUPPORTED;
 }
 

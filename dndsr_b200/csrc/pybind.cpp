@@ -272,6 +272,12 @@ struct Eval
     {
         ck(dndsb_eval_lusgs_matrix_init(h, dp(dTau, "dTau"), dt, alphaDiag, dp(jd, "jdiag"), stream()));
     }
+    void LUSGSMatrixInitFull(py::object jd, py::object dTau, double dt, double alphaDiag, py::object u, py::object uRec, int jacobianCode, double t)
+    {
+        ck(dndsb_eval_lusgs_matrix_init_full(h, dp(dTau, "dTau"), dt, alphaDiag, dpn(u, "u"), dpn(uRec, "uRec"), jacobianCode, t, dp(jd, "jdiag"),
+                                             stream()));
+    }
+    void SetJacobianMode(bool useScalarJacobian, bool useRoeJacobian) { ck(dndsb_eval_set_jacobian_mode(h, useScalarJacobian, useRoeJacobian)); }
     py::object UpdateSGS(double alphaDiag, py::object rhs, py::object u, py::object uInc, py::object uIncNew, py::object jd, bool forward,
                          bool gsUpdate, bool uIncIsZero, bool wantSum)
     {
@@ -441,6 +447,8 @@ PYBIND11_MODULE(_C, m)
         .def("ResidualVJPCoords", &Eval::ResidualVJPCoords)
         .def("EvaluateRHSJVPCoords", &Eval::RhsJVPCoords)
         .def("LUSGSMatrixInit", &Eval::LUSGSMatrixInit)
+        .def("LUSGSMatrixInitFull", &Eval::LUSGSMatrixInitFull)
+        .def("SetJacobianMode", &Eval::SetJacobianMode)
         .def("UpdateSGS", &Eval::UpdateSGS)
         .def("UpdateLUSGSForward", &Eval::UpdateLUSGSForward)
         .def("UpdateLUSGSBackward", &Eval::UpdateLUSGSBackward)

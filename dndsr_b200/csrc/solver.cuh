@@ -156,6 +156,12 @@ struct EvalD
     int *errWord = nullptr;   // device error word
     int *errDeferred = nullptr; // error word of EvaluateRHS in deferred mode (read and cleared on request)
     bool deferErr = false;    // EvaluateRHS skips its per-call read-back of the error word
+    // useScalarJacobian / useRoeJacobian (EulerEvaluatorSettings.hpp:53-54): 0 scalar diagonal, 1 block diagonal,
+    // 2 block diagonal with the Roe term (roejac.cuh); a block jdiag is [nCell][2][nv][nv] (block, inverse)
+    int jacMode = 0;
+    // EulerEvaluator.hpp:187-189, allocated for jacMode 2 as one [3][nFace] range: the convective speed after
+    // EvaluateDt, the face integrals of the Riemann eigenvalues divided by the area after EvaluateRHS
+    real *lambdaFace0 = nullptr, *lambdaFace123 = nullptr, *lambdaFace4 = nullptr;
 };
 
 // EvaluateRHS flags (EulerEvaluator.hpp:370-378 RHS_* values)
@@ -189,6 +195,15 @@ int lusgs_matvec(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, cons
 int update_lusgs(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc,
                  real *uIncNew, const real *jdiag, int forward, cudaStream_t st);
 int init_field(const MeshD &m, const GeomD &g, const EvalD &ev, int kind, real chi, real *u, cudaStream_t st);
+// block-mode LU-SGS operators (roejac.cu): jd [nCell][2][nv][nv]; the Roe term with ev.jacMode == 2
+int lusgs_init_block(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *dTau, real dt, real alphaDiag, const real *u,
+                     real *jd, cudaStream_t st);
+int update_sgs_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew,
+                     const real *jd, int forward, int gsUpdate, int uIncIsZero, real *sumIncHost, cudaStream_t st);
+int update_lusgs_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc,
+                       real *uIncNew, const real *jd, int forward, cudaStream_t st);
+int lusgs_matvec_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jd, real *AuInc,
+                       cudaStream_t st);
 // viscous part of the residual derivatives (adjoint_visc.cu): added to the inviscid face
 // cotangents [nFace][2][(R+1) nv] / face flux derivatives [nFace][nv] before their gathers
 int rhs_vjp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec, real *faceAdj,
@@ -307,8 +322,9 @@ struct LinSettings
     real scale2[8] = {1, 1, 1, 1, 1, 1, 1, 1}; // per-variable weights of the GMRES dot (meanScaleInv^2)
 };
 struct LinWs;
-int linear_solve(const MeshD &m, const GeomD &g, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag, const real *dTau, real dt,
-                 const real *u, const real *rhs, real *xInc, cudaStream_t st);
+// bnd: the boundary table (the ghost states of the Roe-term diagonal blocks)
+int linear_solve(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag,
+                 const real *dTau, real dt, const real *u, const real *rhs, real *xInc, cudaStream_t st);
 void linws_free(LinWs *w);
 // prec 0: double vectors, 1: float vectors; nv 5 or 6; FP64 accumulation, deterministic
 // Krylov basis columns are ld apart: ld = n rounded up to a multiple of 4, storage 16-byte aligned, pad zero

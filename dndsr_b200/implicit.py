@@ -240,7 +240,9 @@ class ImplicitSolver:
         self.uRec = vr.BuildURec(nv)
         self.uRecNew = vr.BuildURec(nv)
         dev = self.uRec.device
-        self.jd = torch.zeros((nc, nv) if nv == 6 else (nc,), dtype=torch.float64, device=dev)
+        # the evaluator's JDiag layout (scalar, per-variable for SA, or blocks with useScalarJacobian false)
+        self.jd = ev.BuildJDiag() if hasattr(ev, "BuildJDiag") else torch.zeros((nc, nv) if nv == 6 else (nc,), dtype=torch.float64,
+                                                                               device=dev)
         self.tmp = torch.zeros((nc, nv), dtype=torch.float64, device=dev)
         self.gmres = GMRES(cfg.nGmresSpace, self.tmp) if cfg.gmresCode else None
         self.resBase = None
@@ -361,7 +363,7 @@ class ImplicitSolver:
             return
         if cfg.linear_precision != "fp64":
             raise ValueError("an FP32 linear solve needs the device evaluator (native_linear)")
-        self.ev.LUSGSMatrixInit(self.jd, dtau, dt, alphaDiag)
+        self.ev.LUSGSMatrixInit(self.jd, dtau, dt, alphaDiag, cx)
         cxInc.zero_()
         if self.cfg.gmresCode in (0, 2):
             self._sgs_pair(alphaDiag, cres, cx, cxInc)

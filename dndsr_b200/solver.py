@@ -29,7 +29,8 @@ VR_DEFAULTS = dict(maxOrder=1, intOrder=1, jacobiRelax=1.0, SORInstead=False, an
                    scaleMultiplier=1.0, dirWeightScheme="Factorial", manualDirWeights=(1, 1, 0.5, 1.0 / 6), geomWeightScheme="GWNone",
                    geomWeightBias=0.0, geomWeightPower=0.5, geomWeightPower1=0.0, geomWeightPower2=0.0, bcWeight=1.0)
 EULER_DEFAULTS = dict(nVars=5, riemannSolverType="Roe", rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=1.0, prGas=0.72,
-                      TRef=273.15, CSutherland=110.4, muModel=1, ignoreVis=False, rsMeanValueEig=0)
+                      TRef=273.15, CSutherland=110.4, muModel=1, ignoreVis=False, rsMeanValueEig=0, useScalarJacobian=True,
+                      useRoeJacobian=False)
 
 
 # boundary condition codes, Euler/EulerBC.hpp:35-48
@@ -182,6 +183,14 @@ class EulerEvaluator:
                   ignoreVis=int(bool(s["ignoreVis"])), rsMeanValueEig=int(s["rsMeanValueEig"]))
         self._c = _C().EulerEvaluator(vr._c, cs)
         self.nVars = cs["nVars"]
+        self.SetJacobianMode(bool(s["useScalarJacobian"]) and not bool(s["useRoeJacobian"]), bool(s["useRoeJacobian"]))
+
+    def SetJacobianMode(self, useScalarJacobian=True, useRoeJacobian=False):
+        """EulerEvaluatorSettings useScalarJacobian / useRoeJacobian (EulerEvaluatorSettings.hpp:53-54): the scalar
+        diagonal, block diagonal blocks, or block diagonal blocks with the Roe term; BuildJDiag follows the mode."""
+        self._c.SetJacobianMode(bool(useScalarJacobian), bool(useRoeJacobian))
+        self.blockJacobian = not useScalarJacobian
+        self.useRoeJacobian = bool(useRoeJacobian)
 
     def SetBC(self, types, values):
         """BoundaryHandler of the evaluator (Euler/EulerBC.hpp) as a per-zone table: types[zone]
@@ -272,32 +281,48 @@ class EulerEvaluator:
         return out
 
     def BuildJDiag(self):
-        """Diagonal array of LUSGSMatrixInit: [nCell] (one value per cell), or [nCell][nVars] for the SA model."""
+        """Diagonal array of LUSGSMatrixInit: [nCell] (one value per cell), or [nCell][nVars] for the SA model; in block
+        mode [nCell][2][nVars][nVars], the blocks and their inverses."""
         n = self.vr.mesh.n_cell
+        if self.blockJacobian:
+            return torch.zeros((n, 2, self.nVars, self.nVars), dtype=torch.float64, device="cuda")
         return torch.zeros((n, self.nVars) if self.nVars == 6 else (n,), dtype=torch.float64, device="cuda")
 
-    def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag):
-        self._c.LUSGSMatrixInit(jdiag, dTau, float(dt), float(alphaDiag))
+    def _jd(self, jdiag):
+        """jdiag must have the layout of the Jacobian mode (the library reads it with that size)."""
+        n = self.vr.mesh.n_cell
+        want = n * 2 * self.nVars * self.nVars if self.blockJacobian else n * (self.nVars if self.nVars == 6 else 1)
+        if jdiag.numel() != want or jdiag.dtype != torch.float64:
+            raise ValueError(f"jdiag: {want} float64 values expected for this Jacobian mode (BuildJDiag), got {jdiag.numel()}")
+        return jdiag
+
+    def LUSGSMatrixInit(self, jdiag, dTau, dt, alphaDiag, u=None, uRec=None, jacobianCode=0, t=0.0):
+        """EulerEvaluator.hxx:37-159; u is needed by the Roe Jacobian."""
+        self._jd(jdiag)
+        if u is None and not self.useRoeJacobian:
+            self._c.LUSGSMatrixInit(jdiag, dTau, float(dt), float(alphaDiag))
+        else:
+            self._c.LUSGSMatrixInitFull(jdiag, dTau, float(dt), float(alphaDiag), u, uRec, int(jacobianCode), float(t))
 
     def UpdateSGS(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False, want_sum=True):
-        s = self._c.UpdateSGS(float(alphaDiag), rhs, u, uInc, uIncNew, jdiag, bool(forward), bool(gsUpdate), bool(uIncIsZero), bool(want_sum))
+        s = self._c.UpdateSGS(float(alphaDiag), rhs, u, uInc, uIncNew, self._jd(jdiag), bool(forward), bool(gsUpdate), bool(uIncIsZero), bool(want_sum))
         return s if want_sum else np.zeros(self.nVars)
 
     def UpdateLUSGSForward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
         """EulerEvaluator.hxx:376-451: uIncNew = D^-1 (rhs - lower-neighbour flux increments of uInc).
         uInc may be uIncNew itself (the in-place sweep of the reference's callers)."""
-        self._c.UpdateLUSGSForward(float(alphaDiag), rhs, u, uInc, jdiag, uIncNew)
+        self._c.UpdateLUSGSForward(float(alphaDiag), rhs, u, uInc, self._jd(jdiag), uIncNew)
 
     def UpdateLUSGSBackward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
         """EulerEvaluator.hxx:453-529: uIncNew += D^-1 (- upper-neighbour flux increments of uInc)."""
-        self._c.UpdateLUSGSBackward(float(alphaDiag), rhs, u, uInc, jdiag, uIncNew)
+        self._c.UpdateLUSGSBackward(float(alphaDiag), rhs, u, uInc, self._jd(jdiag), uIncNew)
 
     def FixUMaxFilter(self, u):
         """EulerEvaluator.hxx:1318-1323: the reference's filter returns without changing u."""
         self._c.FixUMaxFilter(u)
 
     def LUSGSMatrixVec(self, alphaDiag, u, uInc, jdiag, AuInc):
-        self._c.LUSGSMatrixVec(float(alphaDiag), u, uInc, jdiag, AuInc)
+        self._c.LUSGSMatrixVec(float(alphaDiag), u, uInc, self._jd(jdiag), AuInc)
 
     def LUSGSMatrixVecT(self, alphaDiag, u, y, jdiag, ATy):
         """ATy = A^T y for the operator A of LUSGSMatrixVec (same lambdaFace, jdiag, alphaDiag)."""

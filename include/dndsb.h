@@ -204,10 +204,29 @@ int dndsb_eval_evaluate_rhs_full(dndsb_eval *ev, double *rhs, double *JSource, c
  * reports (one synchronisation, e.g. once per pseudo-iteration where a residual norm is read anyway). */
 int dndsb_eval_set_deferred_errors(dndsb_eval *ev, int deferred);
 int dndsb_eval_check_errors(dndsb_eval *ev, void *stream);
-/* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, 0, t), EulerEvaluator.hxx:37-159 (scalar Jacobian).
- * jdiag holds one value per cell for 5 variables, and nVars values per cell for the SA model
- * (the shared diagonal plus alphaDiag times JSource of the last RHS). */
+/* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, 0, t), EulerEvaluator.hxx:37-159.  With the
+ * scalar Jacobian jdiag holds one value per cell for 5 variables, and nVars values per cell for the SA model
+ * (the shared diagonal plus alphaDiag times JSource of the last RHS); in block mode (dndsb_eval_set_jacobian_mode)
+ * the block layout.  The Roe Jacobian needs u: dndsb_eval_lusgs_matrix_init_full. */
 int dndsb_eval_lusgs_matrix_init(dndsb_eval *ev, const double *dTau, double dt, double alphaDiag, double *jdiag, void *stream);
+/* EulerEvaluatorSettings useScalarJacobian / useRoeJacobian (EulerEvaluatorSettings.hpp:53-54, mutually
+ * exclusive; an evaluator starts with useScalarJacobian).  With useScalarJacobian = 0 JDiag is block diagonal
+ * (JacobianDiagBlock block mode, EulerJacobian.hpp:42-240): every jdiag argument of the LU-SGS operators
+ * below (matrix_init, update_sgs, update_lusgs_*, matrix_vec) is then [nCell][2][nVars][nVars], the
+ * row-major block and its inverse (GetInvert), and dndsb_eval_solve_linear uses the same blocks.  Without
+ * the Roe term the block is the scalar diagonal.  With useRoeJacobian (EulerEvaluator.hxx:58-131) EvaluateDt
+ * sets lambdaFace0/123/4 to the convective speed, EvaluateRHS records the face integrals of the Riemann
+ * solver's eigenvalues (EvaluateRHS.hxx:527-545), the diagonal block sums (alphaDiag/2)(A_f/V) times the Roe
+ * dissipation matrix plus lambdaVis I over the faces (boundary faces also the linearised ghost) plus
+ * 1/dTau + 1/dt, and the neighbour increments take the Roe form (fluxJacobian0_Right_Times_du,
+ * EulerEvaluator.hpp:1100-1158).  The transposed operators (lusgs_matrix_vec_t, update_sgs_t) take the
+ * scalar Jacobian only. */
+int dndsb_eval_set_jacobian_mode(dndsb_eval *ev, int useScalarJacobian, int useRoeJacobian);
+/* LUSGSMatrixInit(JDiag, JSource, dTau, dt, alphaDiag, u, uRec, jacobianCode, t), EulerEvaluator.hxx:37-159, in
+ * every Jacobian mode: u is read by the Roe term (NULL allowed otherwise), uRec and t by neither branch;
+ * jacobianCode must be 0.  A singular block gives DNDSB_E_NONFINITE (one host synchronisation in block mode). */
+int dndsb_eval_lusgs_matrix_init_full(dndsb_eval *ev, const double *dTau, double dt, double alphaDiag, const double *u, const double *uRec,
+                                      int jacobianCode, double t, double *jdiag, void *stream);
 /* UpdateSGS(alphaDiag, t, rhs, u, uInc, uIncNew, JDiag, forward, gsUpdate, sumInc, uIncIsZero),
  * EulerEvaluator.hxx:550-693, swept colour by colour; sumIncHost [nVars] may be NULL */
 int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,

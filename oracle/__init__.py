@@ -120,6 +120,10 @@ def _declare(L):
     L.orc_eval_rhs.argtypes = [_V, _D, _D, _D, _D]
     L.orc_eval_rhs_full.argtypes = [_V, _D, _D, _D, _D, _D, _D, _D]
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
+    L.orc_set_jacobian_mode.argtypes = [_V, ctypes.c_int]
+    L.orc_roe_fdiff.argtypes = [ctypes.c_int, ctypes.c_double, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
+    L.orc_lusgs_init_block.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D, _D]
+    L.orc_lusgs_init_block.restype = ctypes.c_int
     L.orc_update_sgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
     L.orc_update_lusgs.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int]
     L.orc_lusgs_matvec.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D]
@@ -158,6 +162,21 @@ def riemann(rs, UL, UR, n, gamma=1.4, ULm=None, URm=None, dLambda=0.0, fixScale=
     code = RS[rs] if isinstance(rs, str) else int(rs)
     lib().orc_riemann(code, _p(UL), _p(UR), _p(ULm), _p(URm), _p(n), gamma, dLambda, fixScale, incFScale, _p(F), _p(lam))
     return F, lam
+
+
+def roe_fdiff_matrix(U, UOther, n, lam, gamma=1.4):
+    """The matrix of RoeFluxIncFDiff (Gas.hpp:1149-1243) at the Roe average of (U, UOther) with the eigenvalues
+    lam = (l0, l123, l4): column i is the dissipation of the unit jump e_i."""
+    U, UOther, n = _f64(U), _f64(UOther), _f64(n)
+    nv = len(U)
+    M = np.zeros((nv, nv))
+    for i in range(nv):
+        e = np.zeros(nv)
+        e[i] = 1.0
+        col = np.zeros(nv)
+        lib().orc_roe_fdiff(nv, gamma, _p(U), _p(UOther), _p(n), _p(e), float(lam[0]), float(lam[1]), float(lam[2]), _p(col))
+        M[:, i] = col
+    return M
 
 
 def cell_rhs_alpha(u, res, refRho, refP, gamma=1.4, relax=0.9, compress=2, compressPower=1.0, ppEpsIsRelaxed=False, flag=0):
@@ -318,6 +337,22 @@ class Oracle:
         jd = np.zeros(self.mesh.n_cell * (self.nv if self.nv >= 6 else 1))
         self.L.orc_lusgs_init(self.h, _p(dTau), dt, alphaDiag, _p(jd))
         return jd if self.nv < 6 else jd.reshape(self.mesh.n_cell, self.nv)
+
+    def set_jacobian_mode(self, useScalarJacobian=True, useRoeJacobian=False):
+        """EulerEvaluatorSettings useScalarJacobian / useRoeJacobian (EulerEvaluatorSettings.hpp:53-54, exclusive).
+        Block modes take the jdiag of lusgs_init_block in every LU-SGS operator; useRoeJacobian also makes
+        eval_rhs record the face eigenvalues lambdaFace0 / 123 / 4."""
+        if useScalarJacobian and useRoeJacobian:
+            raise ValueError("useScalarJacobian and useRoeJacobian are mutually exclusive")
+        self.L.orc_set_jacobian_mode(self.h, 2 if useRoeJacobian else (0 if useScalarJacobian else 1))
+
+    def lusgs_init_block(self, dTau, dt, alphaDiag, u):
+        """LUSGSMatrixInit in block mode: [nCell][2][nv][nv], the block and its inverse."""
+        dTau, u = _f64(dTau), _f64(u)
+        jd = np.zeros((self.mesh.n_cell, 2, self.nv, self.nv))
+        if self.L.orc_lusgs_init_block(self.h, _p(dTau), dt, alphaDiag, _p(u), _p(jd)) != 0:
+            raise FloatingPointError("singular diagonal block")
+        return jd
 
     def update_sgs(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False):
         rhs, u, uInc, jdiag = _f64(rhs), _f64(u), _f64(uInc), _f64(jdiag)

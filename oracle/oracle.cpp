@@ -897,6 +897,13 @@ struct Oracle
     std::vector<real> AAInvB, AInvb, matA;
     // evaluator state (EulerEvaluator.hpp lambdaFace*, deltaLambda*)
     std::vector<real> lambdaFace, lambdaFaceC, lambdaFaceVis, lambdaFace0, deltaLambdaFace, deltaLambdaCell;
+    // EulerEvaluator.hpp:187-189 lambdaFace0 / lambdaFace123 / lambdaFace4: the convective speed after
+    // EvaluateDt (EvaluateDt.hxx:995-996), the face integrals of the Riemann solver's eigenvalues after an
+    // EvaluateRHS with useRoeJacobian (EvaluateRHS.hxx:527-545)
+    std::vector<real> lambdaFace123, lambdaFace4;
+    // EulerEvaluatorSettings.hpp:53-54: jacMode 0 = useScalarJacobian (one diagonal), 1 = block diagonal
+    // (useScalarJacobian false, useRoeJacobian false), 2 = block diagonal with the Roe term (useRoeJacobian)
+    int jacMode = 0;
     // SA model (nVars = 6): wall distance per cell Gauss point, major length scale per cell,
     // and the source-term Jacobian diagonal of the last RHS
     std::vector<real> dWall, cellHMax, jSource;
@@ -1673,6 +1680,8 @@ struct Oracle
         lambdaFaceC.assign(nFace, 0);
         lambdaFaceVis.assign(nFace, 0);
         lambdaFace0.assign(nFace, 0);
+        lambdaFace123.assign(nFace, 0);
+        lambdaFace4.assign(nFace, 0);
         deltaLambdaFace.assign(nFace, 0);
         deltaLambdaCell.assign(nCell, 0);
 #pragma omp parallel for schedule(static)
@@ -1711,7 +1720,7 @@ struct Oracle
             lambdaFace[f] = lambdaConvection + lamVis * area * (1. / vol[c0] + 1. / volR);
             lambdaFaceC[f] = abs(veloNMean - vgN) + lamVis * area * (1. / vol[c0] + 1. / volR);
             lambdaFaceVis[f] = lamVis * area * (1. / vol[c0] + 1. / volR);
-            lambdaFace0[f] = lambdaConvection;
+            lambdaFace0[f] = lambdaFace123[f] = lambdaFace4[f] = lambdaConvection;
             real dvn = veloNR - veloNL;
             deltaLambdaFace[f] = max({abs(dvn + aR - aL), abs(dvn - aR + aL), abs(aL - aR)});
         }
@@ -1941,8 +1950,10 @@ struct Oracle
     // mean at the face centre (:198-210), gradient copied from the inside (:360-362), GRP
     // distance from the face centre (:363-386), viscous flux removed on slip, far-field and
     // outflow faces (:423-430, EvaluateDt.hxx:1203-1207)
-    void boundaryFaceFlux(long f, const real *u, const real *uRec, real *fluxEs, const real *uRecG) const
+    // lam3 (may be nullptr): the face integrals of the eigenvalues l0, l123, l4 divided by the area (EvaluateRHS.hxx:527-545)
+    void boundaryFaceFlux(long f, const real *u, const real *uRec, real *fluxEs, const real *uRecG, real *lam3 = nullptr) const
     {
+        real lamEs[3] = {0, 0, 0};
         int nv = es.nVars;
         real gamma = es.gamma;
         long c0 = face2cell[f * 2 + 0];
@@ -2009,7 +2020,11 @@ struct Oracle
             real JD = faceJDet[f * nGf + g];
             for (int v = 0; v < nv; v++)
                 fluxEs[v] += -(F[v] - vis[v]) * JD * w;
+            lamEs[0] += l0 * JD * w, lamEs[1] += l1 * JD * w, lamEs[2] += l4 * JD * w;
         }
+        if (lam3)
+            for (int i = 0; i < 3; i++)
+                lam3[i] = lamEs[i] / faceArea[f];
     }
 
     // EulerEvaluator_EvaluateRHS.hxx:55-818 EvaluateRHS with the flux of
@@ -2029,15 +2044,22 @@ struct Oracle
         std::vector<real> faceFlux(nFace * nv, 0.0);
         if (deltaLambdaCell.empty())
             deltaLambdaCell.assign(nCell, 0.0);
+        const bool recLam = jacMode == 2;
+        if (recLam && (long)lambdaFace0.size() != nFace)
+            lambdaFace0.assign(nFace, 0), lambdaFace123.assign(nFace, 0), lambdaFace4.assign(nFace, 0);
 #pragma omp parallel for schedule(static)
         for (long f = 0; f < nFace; f++)
         {
             long c0 = face2cell[f * 2 + 0], c1 = face2cell[f * 2 + 1];
             if (c1 < 0)
             {
-                boundaryFaceFlux(f, u, uRec, &faceFlux[f * nv], uRecG);
+                real lam3[3];
+                boundaryFaceFlux(f, u, uRec, &faceFlux[f * nv], uRecG, lam3);
+                if (recLam)
+                    lambdaFace0[f] = lam3[0], lambdaFace123[f] = lam3[1], lambdaFace4[f] = lam3[2];
                 continue;
             }
+            real lamEs[3] = {0, 0, 0};
             std::vector<real> T0(4 * NDOF), T1(4 * NDOF);
             real fluxEs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             const real *ULm = u + c0 * nv, *URm = u + c1 * nv;
@@ -2103,9 +2125,12 @@ struct Oracle
                 real JD = faceJDet[f * nGf + g];
                 for (int v = 0; v < nv; v++)
                     fluxEs[v] += -(F[v] - vis[v]) * JD * w;
+                lamEs[0] += l0 * JD * w, lamEs[1] += l1 * JD * w, lamEs[2] += l4 * JD * w;
             }
             for (int v = 0; v < nv; v++)
                 faceFlux[f * nv + v] = fluxEs[v];
+            if (recLam)
+                lambdaFace0[f] = lamEs[0] / faceArea[f], lambdaFace123[f] = lamEs[1] / faceArea[f], lambdaFace4[f] = lamEs[2] / faceArea[f];
         }
         // cell-wise gather (equivalent to the reference's face scatter, EvaluateRHS.hxx:550-562)
 #pragma omp parallel for schedule(static)
@@ -2183,6 +2208,292 @@ struct Oracle
             dF[j] += -1 * lambdaMain * dU[j];
     }
 
+    // Gas.hpp:1149-1181 GetRoeAverage of (U, UOther) and Gas.hpp:1210-1243 RoeFluxIncFDiff: incF += the Roe
+    // dissipation of the jump incU with the eigenvalues l0, l123, l4 (passive scalars carried with l123)
+    void roeFluxIncFDiff(const real *U, const real *UOther, const real n[3], const real *incU, real l0, real l123, real l4, real *incF) const
+    {
+        roeFluxIncFDiffS(es.nVars, es.gamma, U, UOther, n, incU, l0, l123, l4, incF);
+    }
+    static void roeFluxIncFDiffS(int nv, real gamma, const real *U, const real *UOther, const real n[3], const real *incU, real l0, real l123,
+                                 real l4, real *incF)
+    {
+        real vL[3], vR[3];
+        for (int d = 0; d < 3; d++)
+            vL[d] = U[1 + d] / U[0], vR[d] = UOther[1 + d] / UOther[0];
+        real pL, aL2, HL, pR, aR2, HR;
+        idealGasThermal(U[4], U[0], dot3(vL, vL), gamma, pL, aL2, HL);
+        idealGasThermal(UOther[4], UOther[0], dot3(vR, vR), gamma, pR, aR2, HR);
+        real sL = sqrt(U[0]), sR = sqrt(UOther[0]);
+        real vRoe[3];
+        for (int d = 0; d < 3; d++)
+            vRoe[d] = (sL * vL[d] + sR * vR[d]) / (sL + sR);
+        real vsqrRoe = dot3(vRoe, vRoe);
+        real HRoe = (sL * HL + sR * HR) / (sL + sR);
+        real asqrRoe = (gamma - 1) * (HRoe - 0.5 * vsqrRoe);
+        real aRoe = sqrt(asqrRoe);
+        real vn = dot3(vRoe, n);
+        real incU123N = incU[1] * n[0] + incU[2] * n[1] + incU[3] * n[2];
+        real a23[3];
+        for (int d = 0; d < 3; d++)
+            a23[d] = incU[1 + d] - incU[0] * vRoe[d];
+        real a23n = dot3(a23, n);
+        for (int d = 0; d < 3; d++)
+            a23[d] -= n[d] * a23n; // tangential part
+        real incU4b = incU[4] - dot3(a23, vRoe);
+        real alpha1 = (gamma - 1) / asqrRoe * (incU[0] * (HRoe - vn * vn) + vn * incU123N - incU4b);
+        real alpha0 = (incU[0] * (vn + aRoe) - incU123N - aRoe * alpha1) / (2 * aRoe);
+        real alpha4 = incU[0] - (alpha0 + alpha1);
+        alpha0 *= l0, alpha1 *= l123, alpha4 *= l4;
+        for (int d = 0; d < 3; d++)
+            a23[d] *= l123;
+        incF[0] += alpha0 + alpha1 + alpha4;
+        incF[4] += (HRoe - vn * aRoe) * alpha0 + 0.5 * vsqrRoe * alpha1 + (HRoe + vn * aRoe) * alpha4 + dot3(a23, vRoe);
+        for (int d = 0; d < 3; d++)
+            incF[1 + d] += (vRoe[d] - aRoe * n[d]) * alpha0 + (vRoe[d] + aRoe * n[d]) * alpha4 + vRoe[d] * alpha1 + a23[d];
+        for (int j = 5; j < nv; j++)
+            incF[j] += incU[j] * l123;
+    }
+
+    // EulerEvaluator.hpp:1100-1158 fluxJacobian0_Right_Times_du with useRoeTerm != 0:
+    // dF = (omitF ? 0 : A(U; n) dU) + RoeFluxIncFDiff(dU; Roe(U, UOther), s l0, s l123, s l4) + s lambdaVis dU,  s = incFsign
+    void fluxJacRoeTimesDu(const real *U, const real *UOther, const real n[3], const real *dU, real lamVis, real l0, real l123, real l4,
+                           int incFsign, bool omitF, real *dF) const
+    {
+        int nv = es.nVars;
+        if (omitF)
+            for (int j = 0; j < nv; j++)
+                dF[j] = 0;
+        else
+            fluxJacTimesDu(U, n, dU, 0.0, dF);
+        roeFluxIncFDiff(U, UOther, n, dU, incFsign * l0, incFsign * l123, incFsign * l4, dF);
+        for (int j = 0; j < nv; j++)
+            dF[j] += incFsign * lamVis * dU[j];
+    }
+
+    // the flux increment of neighbour o of cell c across face f (UpdateSGS / LUSGSMatrixVec, EulerEvaluator.hxx:226-247):
+    // the scalar form with lambdaFace, or with useRoeJacobian the Roe form with lambda0 / lambda4 swapped on side 1
+    void neighbourFInc(long c, long f, long o, const real *u, const real *dU, real *dF) const
+    {
+        int nv = es.nVars;
+        int side = sideOf(c, f);
+        real n[3];
+        for (int d = 0; d < 3; d++)
+            n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+        if (jacMode == 2)
+        {
+            real l0 = side ? lambdaFace4[f] : lambdaFace0[f], l4 = side ? lambdaFace0[f] : lambdaFace4[f];
+            fluxJacRoeTimesDu(u + o * nv, u + c * nv, n, dU, lambdaFaceVis[f], l0, lambdaFace123[f], l4, -1, false, dF);
+        }
+        else
+            fluxJacTimesDu(u + o * nv, n, dU, lambdaFace[f], dF);
+    }
+
+    // generateBoundaryValue with linMode 1 (EvaluateDt.hxx:1743-1835, generateBV_InviscidWall :2199-2214 and
+    // generateBV_ViscousWall :2241-2270 up to their linMode return): the ghost's derivative, column-major nv x nv
+    void bcLinear(int type, const real n[3], real *J) const
+    {
+        int nv = es.nVars;
+        for (int i = 0; i < nv * nv; i++)
+            J[i] = 0;
+        if (type == 3 || type == 9) // BCWallInvis, BCSym: momentum mirrored
+        {
+            for (int i = 0; i < nv; i++)
+                J[i * nv + i] = 1;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    J[(1 + b) * nv + 1 + a] -= 2 * n[a] * n[b];
+        }
+        else if (type == 2 || type == 4) // BCWall, BCWallIsothermal: momentum reversed
+            for (int i = 0; i < nv; i++)
+                J[i * nv + i] = (i >= 1 && i <= 3) ? -1 : 1;
+        // far field, outflow and inflow types: zero
+    }
+
+    // JacobianDiagBlock::GetInvert (EulerJacobian.hpp:150-180): scale the rows by the inverse diagonal, invert by
+    // Gauss-Jordan elimination with full pivoting, scale the columns back.  Row-major n x n.
+    static bool invertBlock(int n, const real *A, real *Ainv)
+    {
+        real M[64], X[64], D[8];
+        for (int i = 0; i < n; i++)
+        {
+            if (A[i * n + i] == 0)
+                return false;
+            D[i] = 1.0 / A[i * n + i];
+        }
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+                M[i * n + j] = D[i] * A[i * n + j], X[i * n + j] = i == j ? 1 : 0;
+        int colOf[8];
+        for (int i = 0; i < n; i++)
+            colOf[i] = i;
+        for (int k = 0; k < n; k++)
+        {
+            int pr = k, pc = k;
+            real best = -1;
+            for (int i = k; i < n; i++)
+                for (int j = k; j < n; j++)
+                    if (abs(M[i * n + j]) > best)
+                        best = abs(M[i * n + j]), pr = i, pc = j;
+            if (!(best > 0))
+                return false;
+            for (int j = 0; j < n; j++)
+            {
+                std::swap(M[k * n + j], M[pr * n + j]);
+                std::swap(X[k * n + j], X[pr * n + j]);
+            }
+            for (int i = 0; i < n; i++)
+                std::swap(M[i * n + k], M[i * n + pc]);
+            std::swap(colOf[k], colOf[pc]);
+            real ip = 1.0 / M[k * n + k];
+            for (int j = 0; j < n; j++)
+                M[k * n + j] *= ip, X[k * n + j] *= ip;
+            for (int i = 0; i < n; i++)
+            {
+                if (i == k)
+                    continue;
+                real fct = M[i * n + k];
+                if (fct == 0)
+                    continue;
+                for (int j = 0; j < n; j++)
+                    M[i * n + j] -= fct * M[k * n + j], X[i * n + j] -= fct * X[k * n + j];
+            }
+        }
+        // M P = I after the column swaps P, so (D A)^-1 = P X: row colOf[k] of the inverse is row k of X
+        real Y[64];
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                Y[colOf[k] * n + j] = X[k * n + j];
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+                Ainv[i * n + j] = Y[i * n + j] * D[j];
+        return true;
+    }
+
+    // LUSGSMatrixInit (EulerEvaluator.hxx:37-159) in block mode (jacMode 1 / 2): jd [nCell][2][nv][nv] receives
+    // the block (row-major) and its inverse.  With useRoeJacobian every face adds (alpha/2)(A_f/V_c) times the
+    // Roe dissipation matrix of (u_c, u_j) plus lambdaVis I (omitF, incFsign +1), a boundary face also the
+    // Roe-form flux Jacobian of the ghost times the linearised ghost (:98-124); the diagonal then gains
+    // 1/dTau + 1/dt.  Without it the block is the scalar diagonal.  The SA source Jacobian diagonal
+    // (EvaluateDt.hxx:1650-1654, diagonal in block mode too) is added with alphaDiag.  Returns false on a
+    // singular block.
+    bool lusgsInitBlock(const real *dTau, real dt, real alphaDiag, const real *u, real *jd) const
+    {
+        int nv = es.nVars;
+        bool ok = true;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+        for (long c = 0; c < nCell; c++)
+        {
+            real B[64] = {0};
+            real fp = 1.0 / dTau[c] + 1.0 / dt;
+            const real *uc = u + c * nv;
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                fp += (0.5 * alphaDiag) * faceArea[f] * lambdaFace[f] / vol[c];
+                if (jacMode != 2)
+                    continue;
+                long o = otherOf(c, f);
+                int side = sideOf(c, f);
+                real n[3];
+                for (int d = 0; d < 3; d++)
+                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
+                real uj[8];
+                bool bnd = o < 0;
+                if (bnd)
+                {
+                    if (!bcValue(zoneType(f), faceZone[f], uc, n, uj))
+                        std::copy(uc, uc + nv, uj);
+                }
+                else
+                    std::copy(u + o * nv, u + o * nv + nv, uj);
+                real l0 = side ? lambdaFace4[f] : lambdaFace0[f], l4 = side ? lambdaFace0[f] : lambdaFace4[f];
+                real cf = (0.5 * alphaDiag) * faceArea[f] / vol[c];
+                real JII[64], JIJ[64];
+                for (int i = 0; i < nv; i++)
+                {
+                    real e[8] = {0}, col[8];
+                    e[i] = 1;
+                    fluxJacRoeTimesDu(uc, uj, n, e, lambdaFaceVis[f], l0, lambdaFace123[f], l4, +1, true, col);
+                    for (int r = 0; r < nv; r++)
+                        JII[r * nv + i] = col[r];
+                    if (bnd)
+                    {
+                        fluxJacRoeTimesDu(uj, uc, n, e, lambdaFaceVis[f], l0, lambdaFace123[f], l4, -1, false, col);
+                        for (int r = 0; r < nv; r++)
+                            JIJ[r * nv + i] = col[r];
+                    }
+                }
+                if (bnd)
+                {
+                    real JBC[64]; // column-major
+                    bcLinear(zoneType(f), n, JBC);
+                    for (int r = 0; r < nv; r++)
+                        for (int i = 0; i < nv; i++)
+                        {
+                            real acc = 0;
+                            for (int l = 0; l < nv; l++)
+                                acc += JIJ[r * nv + l] * JBC[i * nv + l];
+                            B[r * nv + i] += cf * acc;
+                        }
+                }
+                for (int i = 0; i < nv * nv; i++)
+                    B[i] += cf * JII[i];
+            }
+            for (int i = 0; i < nv; i++)
+            {
+                if (jacMode == 2)
+                    B[i * nv + i] += 1.0 / dTau[c] + 1.0 / dt;
+                else
+                    B[i * nv + i] = fp;
+                if (nv >= 6 && !jSource.empty())
+                    B[i * nv + i] += alphaDiag * jSource[c * nv + i];
+            }
+            real *out = jd + c * 2 * nv * nv;
+            std::copy(B, B + nv * nv, out);
+            ok = invertBlock(nv, B, out + nv * nv) && ok;
+        }
+        return ok;
+    }
+
+    // JDiag^-1 b (JacobianDiagBlock::MatVecLeftInvert) for the jdiag layout of the mode
+    void jdSolve(long c, const real *jdiag, const real *b, real *x) const
+    {
+        int nv = es.nVars;
+        if (jacMode == 0)
+        {
+            for (int v = 0; v < nv; v++)
+                x[v] = b[v] / jdiag[nv >= 6 ? c * nv + v : c];
+            return;
+        }
+        const real *Ai = jdiag + c * 2 * nv * nv + nv * nv;
+        for (int r = 0; r < nv; r++)
+        {
+            real acc = 0;
+            for (int l = 0; l < nv; l++)
+                acc += Ai[r * nv + l] * b[l];
+            x[r] = acc;
+        }
+    }
+    // JDiag x (JacobianDiagBlock::MatVecLeft)
+    void jdMul(long c, const real *jdiag, const real *x, real *y) const
+    {
+        int nv = es.nVars;
+        if (jacMode == 0)
+        {
+            for (int v = 0; v < nv; v++)
+                y[v] = jdiag[nv >= 6 ? c * nv + v : c] * x[v];
+            return;
+        }
+        const real *A = jdiag + c * 2 * nv * nv;
+        for (int r = 0; r < nv; r++)
+        {
+            real acc = 0;
+            for (int l = 0; l < nv; l++)
+                acc += A[r * nv + l] * x[l];
+            y[r] = acc;
+        }
+    }
+
     // EulerEvaluator.hxx:550-693 UpdateSGS (sequential, natural cell order)
     void updateSGS(real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew, const real *jdiag, bool forward,
                    bool gsUpdate, bool uIncIsZero, real *sumInc) const
@@ -2205,20 +2516,18 @@ struct Oracle
                 bool useNew = gsUpdate && (forward ? (o < c) : (o > c));
                 if (uIncIsZero && !useNew)
                     continue;
-                int side = sideOf(c, f);
-                real n[3];
-                for (int d = 0; d < 3; d++)
-                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
                 const real *dU = useNew ? uIncNew + o * nv : uInc + o * nv;
                 real dF[8];
-                fluxJacTimesDu(u + o * nv, n, dU, lambdaFace[f], dF);
+                neighbourFInc(c, f, o, u, dU, dF);
                 for (int v = 0; v < nv; v++)
                     buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
             }
+            real x[8];
+            jdSolve(c, jdiag, buf, x);
             for (int v = 0; v < nv; v++)
             {
                 real old = uIncNew[c * nv + v];
-                uIncNew[c * nv + v] = buf[v] / jdiag[nv >= 6 ? c * nv + v : c];
+                uIncNew[c * nv + v] = x[v];
                 sumInc[v] += abs(uIncNew[c * nv + v] - old);
             }
         }
@@ -2243,20 +2552,15 @@ struct Oracle
                 long o = otherOf(c, f);
                 if (o < 0 || !(forward ? (o < c) : (o > c)))
                     continue;
-                int side = sideOf(c, f);
-                real n[3];
-                for (int d = 0; d < 3; d++)
-                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
                 real dF[8];
-                fluxJacTimesDu(u + o * nv, n, uInc + o * nv, lambdaFace[f], dF);
+                neighbourFInc(c, f, o, u, uInc + o * nv, dF);
                 for (int v = 0; v < nv; v++)
                     buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
             }
+            real x[8];
+            jdSolve(c, jdiag, buf, x);
             for (int v = 0; v < nv; v++)
-            {
-                real x = buf[v] / jdiag[nv >= 6 ? c * nv + v : c];
-                uIncNew[c * nv + v] = forward ? x : uIncNew[c * nv + v] + x;
-            }
+                uIncNew[c * nv + v] = forward ? x[v] : uIncNew[c * nv + v] + x[v];
         }
     }
 
@@ -2274,17 +2578,15 @@ struct Oracle
                 long o = otherOf(c, f);
                 if (o < 0)
                     continue;
-                int side = sideOf(c, f);
-                real n[3];
-                for (int d = 0; d < 3; d++)
-                    n[d] = faceMeanNorm[f * 3 + d] * (side ? -1 : 1);
                 real dF[8];
-                fluxJacTimesDu(u + o * nv, n, uInc + o * nv, lambdaFace[f], dF);
+                neighbourFInc(c, f, o, u, uInc + o * nv, dF);
                 for (int v = 0; v < nv; v++)
                     buf[v] -= (0.5 * alphaDiag) * faceArea[f] / vol[c] * dF[v];
             }
+            real y[8];
+            jdMul(c, jdiag, uInc + c * nv, y);
             for (int v = 0; v < nv; v++)
-                AuInc[c * nv + v] = jdiag[nv >= 6 ? c * nv + v : c] * uInc[c * nv + v] - buf[v];
+                AuInc[c * nv + v] = y[v] - buf[v];
         }
     }
 
@@ -2581,6 +2883,9 @@ extern "C"
         else if (n == "lambdaFace") v = &o->lambdaFace;
         else if (n == "lambdaFaceC") v = &o->lambdaFaceC;
         else if (n == "lambdaFaceVis") v = &o->lambdaFaceVis;
+        else if (n == "lambdaFace0") v = &o->lambdaFace0;
+        else if (n == "lambdaFace123") v = &o->lambdaFace123;
+        else if (n == "lambdaFace4") v = &o->lambdaFace4;
         else if (n == "deltaLambdaCell") v = &o->deltaLambdaCell;
         if (!v)
             return -1;
@@ -2627,6 +2932,14 @@ extern "C"
         ((Oracle *)h)->lusgsInit(dTau, dt, alphaDiag, jdiag);
     }
 
+    // useScalarJacobian / useRoeJacobian as jacMode 0 / 1 / 2 (see Oracle::jacMode)
+    void orc_set_jacobian_mode(void *h, int mode) { ((Oracle *)h)->jacMode = mode; }
+    // block-mode LUSGSMatrixInit: jd [nCell][2][nv][nv]; returns 0, or -1 on a singular block
+    int orc_lusgs_init_block(void *h, const double *dTau, double dt, double alphaDiag, const double *u, double *jd)
+    {
+        return ((Oracle *)h)->lusgsInitBlock(dTau, dt, alphaDiag, u, jd) ? 0 : -1;
+    }
+
     void orc_update_sgs(void *h, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
                         const double *jdiag, int forward, int gsUpdate, int uIncIsZero, double *sumInc)
     {
@@ -2666,6 +2979,13 @@ extern "C"
     {
         real vg[3] = {0, 0, 0};
         riemann(type, UL, UR, ULm, URm, vg, n, gamma, F, dLambda, fixScale, incFScale, lam[0], lam[1], lam[2]);
+    }
+
+    // GetRoeAverage(U, UOther) + RoeFluxIncFDiff (Gas.hpp:1149-1243): incF += the Roe dissipation of incU
+    void orc_roe_fdiff(int nv, double gamma, const double *U, const double *UOther, const double *n, const double *incU, double l0, double l123,
+                       double l4, double *incF)
+    {
+        Oracle::roeFluxIncFDiffS(nv, gamma, U, UOther, n, incU, l0, l123, l4, incF);
     }
 
     void orc_viscous_flux(const double *U, const double *GradU /*3 x 5 cons*/, const double *n, double gamma, double mu, double k, double Cp,

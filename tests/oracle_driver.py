@@ -45,8 +45,23 @@ class OracleEval:
         dt.copy_(torch.tensor(d))
         return mn
 
-    def LUSGSMatrixInit(self, jd, dTau, dt, alphaDiag):
-        jd.copy_(torch.tensor(self.o.lusgs_init(dTau.numpy(), dt, alphaDiag)))
+    blockJacobian = False
+
+    def SetJacobianMode(self, useScalarJacobian=True, useRoeJacobian=False):
+        self.o.set_jacobian_mode(useScalarJacobian, useRoeJacobian)
+        self.blockJacobian = not useScalarJacobian
+
+    def BuildJDiag(self):
+        n, nv = self.vol.shape[0], self.nVars
+        if self.blockJacobian:
+            return torch.zeros((n, 2, nv, nv), dtype=torch.float64)
+        return torch.zeros((n, nv) if nv == 6 else (n,), dtype=torch.float64)
+
+    def LUSGSMatrixInit(self, jd, dTau, dt, alphaDiag, u=None):
+        if self.blockJacobian:
+            jd.copy_(torch.tensor(self.o.lusgs_init_block(dTau.numpy(), dt, alphaDiag, u.numpy())))
+        else:
+            jd.copy_(torch.tensor(self.o.lusgs_init(dTau.numpy(), dt, alphaDiag)))
 
     def UpdateSGS(self, alphaDiag, rhs, u, uInc, uIncNew, jd, forward, gsUpdate=True, uIncIsZero=False, want_sum=True):
         out, s = self.o.update_sgs(alphaDiag, rhs.numpy(), u.numpy(), uInc.numpy(), uIncNew.numpy(), jd.numpy(), forward, gsUpdate,

@@ -1,0 +1,129 @@
+"""The oracle's block / Roe Jacobian restatement (CPU): RoeFluxIncFDiff (Gas.hpp:1149-1243) against the Roe
+eigen-structure and against the oracle's Roe flux (pinned to the reference's Riemann goldens), the block
+inverse, block mode without the Roe term against the scalar operators, the eigenvalue recording of
+EvaluateRHS, and one implicit solve that the Roe Jacobian converges faster than the scalar one."""
+import numpy as np
+import torch
+
+import oracle
+from dndsr_b200 import implicit as I
+from dndsr_b200 import mesh as M
+from tests.bump_case import bump_oracle, perturbed_state
+from tests.oracle_driver import OracleEval, OracleVR
+
+G = 1.4
+
+
+def _state(rho, v, p, extra=()):
+    v = np.asarray(v, float)
+    return np.array([rho, *(rho * v), p / (G - 1) + 0.5 * rho * v @ v, *extra])
+
+
+def test_roe_dissipation_matrix_has_the_roe_eigenstructure():
+    U = _state(1.2, [0.3, -0.2, 0.1], 0.9)
+    n = np.array([0.6, 0.0, 0.8])
+    rho, v, p = U[0], U[1:4] / U[0], 0.9
+    a = np.sqrt(G * p / rho)
+    H = (U[4] + p) / rho
+    vn = v @ n
+    lam = (0.7, 0.3, 1.9)
+    Mx = oracle.roe_fdiff_matrix(U, U, n, lam)
+    # right eigenvectors of the flux Jacobian along n (acoustic, entropy, two shear waves, acoustic)
+    t1 = np.cross(n, [0, 1, 0])
+    t1 /= np.linalg.norm(t1)
+    t2 = np.cross(n, t1)
+    r0 = np.array([1, *(v - a * n), H - vn * a])
+    r4 = np.array([1, *(v + a * n), H + vn * a])
+    r1 = np.array([1, *v, 0.5 * v @ v])
+    rt1 = np.array([0, *t1, v @ t1])
+    rt2 = np.array([0, *t2, v @ t2])
+    for r, l in ((r0, lam[0]), (r4, lam[2]), (r1, lam[1]), (rt1, lam[1]), (rt2, lam[1])):
+        assert np.allclose(Mx @ r, l * r, rtol=1e-13, atol=1e-13)
+    # equal eigenvalues: the identity times the eigenvalue; passive scalars ride with l123
+    assert np.allclose(oracle.roe_fdiff_matrix(U, U, n, (0.8, 0.8, 0.8)), 0.8 * np.eye(5), atol=1e-14)
+    U6 = np.append(U, 0.05)
+    M6 = oracle.roe_fdiff_matrix(U6, U6, n, lam)
+    assert abs(M6[5, 5] - lam[1]) < 1e-15 and np.allclose(M6[:5, :5], Mx, atol=1e-15)
+
+
+def test_roe_dissipation_matches_the_roe_flux():
+    """F_Roe = (F(UL) + F(UR)) / 2 - RoeFluxIncFDiff(UR - UL; Roe(UL, UR), l) / 2 with the flux's own eigenvalues."""
+    rng = np.random.default_rng(1)
+    for _ in range(20):
+        UL = _state(1 + 0.3 * rng.random(), rng.normal(size=3) * 0.4, 1 + 0.2 * rng.random())
+        UR = _state(1 + 0.3 * rng.random(), rng.normal(size=3) * 0.4, 1 + 0.2 * rng.random())
+        n = rng.normal(size=3)
+        n /= np.linalg.norm(n)
+        F, lam = oracle.riemann("Roe", UL, UR, n, fixScale=1.0, incFScale=1.0)
+
+        def phys(U):
+            v = U[1:4] / U[0]
+            p = (G - 1) * (U[4] - 0.5 * U[0] * v @ v)
+            vn = v @ n
+            return np.array([U[0] * vn, *(U[1:4] * vn + p * n), (U[4] + p) * vn])
+
+        Mx = oracle.roe_fdiff_matrix(UL, UR, n, lam)
+        ref = 0.5 * (phys(UL) + phys(UR)) - 0.5 * Mx @ (UR - UL)
+        assert np.allclose(F, ref, rtol=1e-12, atol=1e-13)
+
+
+def _bump():
+    m = M.renumber_by_color(M.bump_channel_tet(5, 3, 2))
+    o, far, types, vals, w = bump_oracle(m, 1, "Roe", 0.0, 1)
+    u0, uRec0 = perturbed_state(m, far, R=o.R)
+    return m, o, far, u0, uRec0
+
+
+def test_block_modes_and_recorded_eigenvalues():
+    m, o, far, u0, uRec0 = _bump()
+    d0, _ = o.eval_dt(u0, 5.0)
+    rhs = o.eval_rhs(u0, uRec0)
+    lamConv = o.get("lambdaFace0")
+    assert np.array_equal(lamConv, o.get("lambdaFace123")) and np.array_equal(lamConv, o.get("lambdaFace4"))
+    jd = o.lusgs_init(d0, 0.1, 0.5)
+    x0 = np.random.default_rng(9).normal(size=u0.shape)
+    A0 = o.lusgs_matvec(0.5, u0, x0, jd)
+    s0, _ = o.update_sgs(0.5, rhs, u0, x0, np.zeros_like(x0), jd, True)
+    o.set_jacobian_mode(False, False)
+    jb = o.lusgs_init_block(d0, 0.1, 0.5, u0)
+    assert np.allclose(jb[:, 0], jd[:, None, None] * np.eye(5), rtol=0, atol=0)
+    assert np.allclose(o.lusgs_matvec(0.5, u0, x0, jb), A0, rtol=1e-15, atol=0)
+    assert np.allclose(o.update_sgs(0.5, rhs, u0, x0, np.zeros_like(x0), jb, True)[0], s0, rtol=1e-14, atol=1e-15)
+    o.set_jacobian_mode(False, True)
+    rhs2 = o.eval_rhs(u0, uRec0)
+    assert np.array_equal(rhs2, rhs)
+    l0, l1, l4 = o.get("lambdaFace0"), o.get("lambdaFace123"), o.get("lambdaFace4")
+    assert (l0 >= 0).all() and (l1 >= 0).all() and (l4 >= 0).all() and not np.array_equal(l0, lamConv)
+    jr = o.lusgs_init_block(d0, 0.1, 0.5, u0)
+    I5 = np.eye(5)
+    assert np.abs(np.einsum("cij,cjk->cik", jr[:, 0], jr[:, 1]) - I5).max() < 1e-13
+    # the trace of a cell without boundary faces: 5 (1/dTau + 1/dt) plus, per face, (alpha/2)(A_f/V) times the
+    # eigenvalue sum l0 + 3 l123 + l4 of the Roe dissipation matrix plus 5 lambdaVis
+    area, vol, lv = o.get("faceArea"), o.get("volume"), o.get("lambdaFaceVis")
+    f2c = np.asarray(m.face2cell)
+    tr = 5 * (1.0 / d0 + 1.0 / 0.1)
+    bnd = np.zeros(m.n_cell, bool)
+    for f, (c0, c1) in enumerate(f2c):
+        t = 0.25 * area[f] * (l0[f] + 3 * l1[f] + l4[f] + 5 * lv[f])
+        tr[c0] += t / vol[c0]
+        if c1 >= 0:
+            tr[c1] += t / vol[c1]
+        else:
+            bnd[c0] = True
+    assert (~bnd).sum() > 10
+    got = np.einsum("cii->c", jr[:, 0])
+    assert np.allclose(got[~bnd], tr[~bnd], rtol=1e-13, atol=0)
+
+
+def test_roe_jacobian_converges_faster_on_the_bump():
+    m, o, far, u0, uRec0 = _bump()
+    drops = {}
+    for roe in (False, True):
+        oe = OracleEval(o)
+        oe.SetJacobianMode(not roe, roe)
+        cfg = I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=20, nTimeStepInternalMin=20, CFL=50.0, gmresCode=1,
+                             nGmresSpace=10)
+        u = torch.tensor(np.tile(far, (m.n_cell, 1)))
+        I.ImplicitSolver(OracleVR(o), oe, cfg).run(u)
+        drops[roe] = cfg.res_history[-1][2]
+    assert drops[True] < 0.7 * drops[False], drops
