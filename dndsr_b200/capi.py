@@ -82,6 +82,8 @@ SIGNATURES = {
     "dndsb_eval_check_errors": [_P, _P],
     "dndsb_eval_lusgs_matrix_init": [_P, _P, _d, _d, _P, _P],
     "dndsb_eval_set_jacobian_mode": [_P, _i, _i],
+    "dndsb_eval_lusgs_matrix_to_jacobian_lu": [_P, _d, _P, _P, _P],
+    "dndsb_eval_lusgs_matrix_solve_jacobian_lu": [_P, _d, _P, _P, _P, _P, _P, _i, _D, _P],
     "dndsb_eval_lusgs_matrix_init_full": [_P, _P, _d, _d, _P, _P, _i, _d, _P, _P],
     "dndsb_eval_update_sgs": [_P, _d, _P, _P, _P, _P, _P, _i, _i, _i, _D, _P],
     "dndsb_eval_lusgs_matrix_vec": [_P, _d, _P, _P, _P, _P, _P],

@@ -594,7 +594,8 @@ extern "C"
         for (void *p : {(void *)e->e.lambdaFace, (void *)e->e.lambdaFaceC, (void *)e->e.lambdaFaceVis, (void *)e->e.lambdaConv,
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
                         (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource,
-                        (void *)e->e.errDeferred, (void *)e->e.fluxWall, (void *)e->e.objDir, (void *)e->e.lambdaFace0})
+                        (void *)e->e.errDeferred, (void *)e->e.fluxWall, (void *)e->e.objDir, (void *)e->e.lambdaFace0, (void *)e->e.luOff,
+                        (void *)e->e.luDinv})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -828,6 +829,32 @@ extern "C"
         return status_msg(rc, "dndsb_eval_lusgs_matrix_init_full");
     }
 
+    int dndsb_eval_lusgs_matrix_to_jacobian_lu(dndsb_eval *e, double alphaDiag, const double *u, const double *jdiag, void *stream)
+    {
+        if (!e || !u || !jdiag)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_to_jacobian_lu: null argument");
+        if (e->e.jacMode == 0)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_to_jacobian_lu: the local LU takes the block Jacobian");
+        int rc = jacobian_lu(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, jdiag, S(stream));
+        if (rc == ST_NONFINITE)
+            return fail(DNDSB_E_NONFINITE, "dndsb_eval_lusgs_matrix_to_jacobian_lu: singular pivot block");
+        return status_msg(rc, "dndsb_eval_lusgs_matrix_to_jacobian_lu");
+    }
+
+    int dndsb_eval_lusgs_matrix_solve_jacobian_lu(dndsb_eval *e, double alphaDiag, const double *rhs, const double *u, const double *uInc,
+                                                  double *uIncNew, const double *jdiag, int uIncIsZero, double *sumIncHost, void *stream)
+    {
+        if (!e || !rhs || !u || !uInc || !uIncNew || !jdiag)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: null argument");
+        if (uInc == uIncNew || rhs == uIncNew) // EulerEvaluator.hxx:919
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: uIncNew must differ from uInc and rhs");
+        if (e->e.jacMode == 0 || !e->e.luOff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: build the local LU first (block Jacobian)");
+        return status_msg(solve_jacobian_lu(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, uIncIsZero, sumIncHost,
+                                            S(stream)),
+                          "dndsb_eval_lusgs_matrix_solve_jacobian_lu");
+    }
+
     int dndsb_eval_update_sgs(dndsb_eval *e, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
                               const double *jdiag, int forward, int gsUpdate, int uIncIsZero, double *sumIncHost, void *stream)
     {
@@ -1019,7 +1046,8 @@ extern "C"
         }
         int rc = linear_solve(e->vr->mesh->d, e->vr->g, e->vr->vr.bnd, e->e, e->lin, s, alphaDiag, dTau, dt, u, rhs, xInc, S(stream));
         if (rc == ST_BADARG)
-            return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..1, nGmresSpace 1..32, precision 0..1");
+            return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..2 (2 with the block Jacobian), nGmresSpace 1..32, "
+                                        "precision 0..1");
         return status_msg(rc, "dndsb_eval_solve_linear");
     }
 

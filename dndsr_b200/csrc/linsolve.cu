@@ -21,6 +21,11 @@
 // both cases.  Reductions use a fixed partition and fixed trees, so results
 // are bitwise reproducible.
 //
+// jacobiCode 2 (block mode): the preconditioner is the reference's local LU (LUSGSMatrixToJacobianLU +
+// LUSGSMatrixSolveJacobianLU, EulerEvaluator.hxx:290-359, 838-927; doPrecondition EulerSolver.hxx:1642-1657) with
+// iluCode 0: a block ILU(0) of the operator factored colour by colour (ilu.cuh) once per solve, applied as two
+// defect-correction steps x += (LU)^-1 (b - A x).
+//
 // Block mode (useScalarJacobian false, optionally useRoeJacobian): the operator is kept as dense blocks,
 // per position the diagonal block and its inverse, per (position, face slot) the off-diagonal block
 // (alpha/2)(A_f/V_c) dF/dU_o (the reference's fluxJacobian0_Right_Times_du_AsMatrix, the same blocks its
@@ -31,6 +36,7 @@
 // captured once into a CUDA graph that later solves replay.
 #include "solver.cuh"
 #include "roejac.cuh"
+#include "ilu.cuh"
 
 namespace dndsb
 {
@@ -126,6 +132,20 @@ DNDSB_GLOBAL void k_copy_T(int64_t n, const T *__restrict__ a, T *b)
 {
     DNDSB_KERNEL_LOOP(i, n)
     b[i] = a[i];
+}
+
+template <typename T>
+DNDSB_GLOBAL void k_sub_T(int64_t n, const T *__restrict__ a, const T *__restrict__ b, T *c) // c = a - b
+{
+    DNDSB_KERNEL_LOOP(i, n)
+    c[i] = a[i] - b[i];
+}
+
+template <typename T>
+DNDSB_GLOBAL void k_add_T(int64_t n, const T *__restrict__ a, T *b) // b += a
+{
+    DNDSB_KERNEL_LOOP(i, n)
+    b[i] += a[i];
 }
 
 // scaled flux-increment Jacobian times dU (EulerEvaluator.hpp:1100-1158 with
@@ -464,6 +484,7 @@ struct LinWs
          *V = nullptr;
     real *H = nullptr, *sc = nullptr, *s2 = nullptr, *red = nullptr;
     void *opB = nullptr, *jdB = nullptr; // block mode: off-diagonal blocks [nCell][nf][nv][nv], diagonal blocks + inverses [nCell][2][nv][nv]
+    void *luB = nullptr, *luD = nullptr, *tmp3 = nullptr; // jacobiCode 2: ILU(0) slot blocks, inverted pivots, scratch
     real *colScale = nullptr; // [33] normalising factors of the stored (unnormalised) Krylov columns
     unsigned *cnt = nullptr;  // ticket counter of the one-launch reductions (zero between launches)
     cudaStream_t cs = nullptr;
@@ -477,7 +498,7 @@ void linws_free(LinWs *w)
 {
     if (!w)
         return;
-    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->opB, w->jdB, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
+    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->opB, w->jdB, w->luB, w->luD, w->tmp3, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
                     (void *)w->sc, (void *)w->s2, (void *)w->red, (void *)w->colScale, (void *)w->cnt})
         dev_free(p);
     graph_free(w->graph);
@@ -501,7 +522,8 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv, int jac
 {
     int k = ls.gmresCode ? ls.nGmresSpace : 0;
     size_t es = ls.precision ? sizeof(float) : sizeof(double);
-    if (w && w->prec == ls.precision && w->k >= k && w->nv == nv && w->nCell == m.nCell && (w->jacMode != 0) == (jacMode != 0))
+    if (w && w->prec == ls.precision && w->k >= k && w->nv == nv && w->nCell == m.nCell && (w->jacMode != 0) == (jacMode != 0) &&
+        (ls.jacobiCode != 2 || w->luB))
     {
         w->jacMode = jacMode; // block with or without the Roe term: same storage, rebuilt by every solve
         return ST_OK;
@@ -524,6 +546,9 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv, int jac
               dev_alloc((void **)&w->colScale, sizeof(real) * 33) == cudaSuccess && dev_alloc((void **)&w->cnt, sizeof(unsigned)) == cudaSuccess;
     if (ok && jacMode)
         ok = dev_alloc(&w->opB, es * nv * nv * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->jdB, es * 2 * nv * nv * m.nCell) == cudaSuccess;
+    if (ok && jacMode && ls.jacobiCode == 2)
+        ok = dev_alloc(&w->luB, es * nv * nv * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->luD, es * nv * nv * m.nCell) == cudaSuccess &&
+             dev_alloc(&w->tmp3, es * n) == cudaSuccess;
     ok = ok && dev_zero(w->V, es * krylov_ld(n) * (k + 1), nullptr) == cudaSuccess; // the column pads stay zero
     ok = ok && dev_zero(w->cnt, sizeof(unsigned), nullptr) == cudaSuccess && dev_zero(w->colScale, sizeof(real) * 33, nullptr) == cudaSuccess;
     if (!ok || stream_create(&w->cs) != cudaSuccess || event_create(&w->evIn) != cudaSuccess || event_create(&w->evOut) != cudaSuccess)
@@ -593,9 +618,42 @@ struct Solve
         }
     }
 
+    // doPrecondition with jacobiCode 2 (EulerSolver.hxx:1642-1657): two LUSGSMatrixSolveJacobianLU steps,
+    // x += (LU)^-1 (rhs - A x) (x = (LU)^-1 rhs from a zero input)
+    void ilu_pair(const T *rhs, T *x, bool zeroIn) const
+    {
+        int64_t nn = n();
+        T *r = (T *)w.tmp2, *ax = (T *)w.tmp3;
+        for (int it = 0; it < 2; it++)
+        {
+            bool zero = zeroIn && it == 0;
+            T *y = zero ? x : r;
+            if (!zero)
+            {
+                FA(x, ax);
+                DNDSB_LAUNCH(k_sub_T<T>, nn, 256, st, nn, rhs, (const T *)ax, r);
+            }
+            auto kl = ilu::k_ilu_lower<T, NV, NF>;
+            auto ku = ilu::k_ilu_upper<T, NV, NF>;
+            for (int ci = 0; ci < m.nColor; ci++)
+                DNDSB_LAUNCH(kl, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
+                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, zero ? rhs : (const T *)r, y);
+            for (int ci = m.nColor - 1; ci >= 0; ci--)
+                DNDSB_LAUNCH(ku, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
+                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, (const T *)w.luD, y);
+            if (!zero)
+                DNDSB_LAUNCH(k_add_T<T>, nn, 256, st, nn, (const T *)r, x);
+        }
+    }
+
     // doPrecondition (EulerSolver.hxx:1605-1635): forward then backward sweep; x in, x out (ping-pong through tmp2)
     void sgs_pair(const T *rhs, T *x, bool zeroIn) const
     {
+        if (ls.jacobiCode == 2)
+        {
+            ilu_pair(rhs, x, zeroIn);
+            return;
+        }
         bool gs = ls.jacobiCode == 1;
         sweep(rhs, x, (T *)w.tmp2, true, gs, zeroIn);
         sweep(rhs, (T *)w.tmp2, x, false, gs, false);
@@ -700,6 +758,14 @@ int run(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs &
         auto kb = k_sgsop_build_blk<T, NV>;
         DNDSB_LAUNCH(kb, m.nCell, 128, cs, m, g, bnd, ev, (int)(w.jacMode == 2), dTau, dt, alphaDiag, u, w.cellPos, w.nbrPos, (T *)w.opB,
                      (T *)w.jdB, ev.errWord);
+        if (ls.jacobiCode == 2) // LUSGSMatrixToJacobianLU + InPlaceDecompose, colour by colour
+        {
+            auto kf = ilu::k_ilu_factor<T, NV, NF>;
+            for (int ci = 0; ci < m.nColor; ci++)
+                DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, cs, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
+                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.opB, (const T *)w.jdB, (int64_t)2 * NV * NV, (T *)w.luB, (T *)w.luD,
+                             ev.errWord);
+        }
     }
     else
         DNDSB_LAUNCH(kbuild, m.nCell, 128, cs, m, g, ev.lambdaFace, dTau, dt, alphaDiag, u, ev.jSource, w.cellPos, w.nbrPos, (T4 *)w.op,
@@ -761,7 +827,9 @@ int run_nf(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinW
 int linear_solve(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag,
                  const real *dTau, real dt, const real *u, const real *rhs, real *xInc, cudaStream_t st)
 {
-    if (ls.gmresCode < 0 || ls.gmresCode > 2 || ls.jacobiCode < 0 || ls.jacobiCode > 1 || ls.sgsIter < 0 || ls.nGmresIter < 0 ||
+    if (ls.jacobiCode == 2 && ev.jacMode == 0) // the local LU takes the block Jacobian
+        return ST_BADARG;
+    if (ls.gmresCode < 0 || ls.gmresCode > 2 || ls.jacobiCode < 0 || ls.jacobiCode > 2 || ls.sgsIter < 0 || ls.nGmresIter < 0 ||
         (ls.gmresCode && (ls.nGmresSpace < 1 || ls.nGmresSpace > 32)) || ls.precision < 0 || ls.precision > 1)
         return ST_BADARG;
     int nv = ev.s.nVars;

@@ -278,6 +278,19 @@ struct Eval
                                              stream()));
     }
     void SetJacobianMode(bool useScalarJacobian, bool useRoeJacobian) { ck(dndsb_eval_set_jacobian_mode(h, useScalarJacobian, useRoeJacobian)); }
+    // EulerEvaluator.hxx:290-359, 838-927
+    void LUSGSMatrixToJacobianLU(double alphaDiag, py::object u, py::object jd)
+    {
+        ck(dndsb_eval_lusgs_matrix_to_jacobian_lu(h, alphaDiag, dp(u, "u"), dp(jd, "jdiag"), stream()));
+    }
+    py::object LUSGSMatrixSolveJacobianLU(double alphaDiag, py::object rhs, py::object u, py::object uInc, py::object uIncNew, py::object jd,
+                                          bool uIncIsZero, bool wantSum)
+    {
+        Arr<double> s(nVars);
+        ck(dndsb_eval_lusgs_matrix_solve_jacobian_lu(h, alphaDiag, dp(rhs, "rhs"), dp(u, "u"), dp(uInc, "uInc"), dp(uIncNew, "uIncNew"),
+                                                     dp(jd, "jdiag"), uIncIsZero, wantSum ? s.mutable_data() : nullptr, stream()));
+        return wantSum ? py::object(s) : py::object(py::none());
+    }
     py::object UpdateSGS(double alphaDiag, py::object rhs, py::object u, py::object uInc, py::object uIncNew, py::object jd, bool forward,
                          bool gsUpdate, bool uIncIsZero, bool wantSum)
     {
@@ -449,6 +462,8 @@ PYBIND11_MODULE(_C, m)
         .def("LUSGSMatrixInit", &Eval::LUSGSMatrixInit)
         .def("LUSGSMatrixInitFull", &Eval::LUSGSMatrixInitFull)
         .def("SetJacobianMode", &Eval::SetJacobianMode)
+        .def("LUSGSMatrixToJacobianLU", &Eval::LUSGSMatrixToJacobianLU)
+        .def("LUSGSMatrixSolveJacobianLU", &Eval::LUSGSMatrixSolveJacobianLU)
         .def("UpdateSGS", &Eval::UpdateSGS)
         .def("UpdateLUSGSForward", &Eval::UpdateLUSGSForward)
         .def("UpdateLUSGSBackward", &Eval::UpdateLUSGSBackward)

@@ -5,6 +5,7 @@
 // scalar kernels, so the sweep order and results match the reference's sequential sweep on a mesh
 // numbered colour by colour.
 #include "roejac.cuh"
+#include "ilu.cuh"
 
 namespace dndsb
 {
@@ -138,7 +139,165 @@ DNDSB_GLOBAL void k_matvec_blk(MeshD m, GeomD g, EvalD ev, int roe, real alphaDi
             AuInc[c * NV + v] = y[v] - buf[v];
     }
 }
+// the slot blocks (alpha/2)(A_f/V_c) dF/dU_o of LUSGSMatrixToJacobianLU (EulerEvaluator.hxx:290-359), cell order
+template <int NV>
+DNDSB_GLOBAL void k_lu_assemble(MeshD m, GeomD g, EvalD ev, int roe, real alphaDiag, const real *__restrict__ u, real *off)
+{
+    DNDSB_KERNEL_LOOP(c, m.nCell)
+    {
+        const real cf = 0.5 * alphaDiag / g.vol[c];
+        for (int k = 0; k < m.nf; k++)
+        {
+            real *ob = off + (c * m.nf + k) * NV * NV;
+            int o = m.cellNbr[c * m.nf + k];
+            if (o < 0 || o == c)
+            {
+                for (int i = 0; i < NV * NV; i++)
+                    ob[i] = 0;
+                continue;
+            }
+            int pk = m.cell2face[c * m.nf + k];
+            int64_t f = pk >> 1;
+            int side = pk & 1;
+            real sg = side ? -1.0 : 1.0;
+            real n[3] = {g.faceMeanNorm[f * 3] * sg, g.faceMeanNorm[f * 3 + 1] * sg, g.faceMeanNorm[f * 3 + 2] * sg};
+            FaceLam L;
+            if (roe)
+                L = face_lam(ev, f, side);
+            else
+                L.main = ev.lambdaFace[f], L.l0 = L.l123 = L.l4 = L.vis = 0;
+            real w = cf * g.faceArea[f];
+            for (int i = 0; i < NV; i++)
+            {
+                real e[NV], col[NV];
+                for (int v = 0; v < NV; v++)
+                    e[v] = v == i ? 1.0 : 0.0;
+                nbr_inc<NV>(roe != 0, u + (int64_t)o * NV, u + c * NV, n, e, L, ev.s.gamma, col);
+                for (int v = 0; v < NV; v++)
+                    ob[v * NV + i] = w * col[v];
+            }
+        }
+    }
+}
+
+DNDSB_GLOBAL void k_sub(int64_t n, const real *__restrict__ a, const real *__restrict__ b, real *c)
+{
+    DNDSB_KERNEL_LOOP(i, n)
+    c[i] = a[i] - b[i];
+}
+
+DNDSB_GLOBAL void k_abs_add(int64_t n, const real *x, real *absOut, const real *__restrict__ add, real *y) // y may be x
+{
+    DNDSB_KERNEL_LOOP(i, n)
+    {
+        absOut[i] = fabs(x[i]);
+        if (add)
+            y[i] = x[i] + add[i];
+    }
+}
+
+template <int NV, int NF>
+void lu_factor_colors(const MeshD &m, EvalD &ev, const real *jd, cudaStream_t st)
+{
+    auto kf = ilu::k_ilu_factor<real, NV, NF>;
+    for (int ci = 0; ci < m.nColor; ci++)
+        DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
+                     m.cellColor, (const real *)ev.luOff, jd, (int64_t)2 * NV * NV, ev.luOff, ev.luDinv, ev.errWord);
+}
+
+template <int NV, int NF>
+void lu_solve_colors(const MeshD &m, EvalD &ev, real *x, cudaStream_t st)
+{
+    auto kl = ilu::k_ilu_lower<real, NV, NF>;
+    auto ku = ilu::k_ilu_upper<real, NV, NF>;
+    for (int ci = 0; ci < m.nColor; ci++)
+        DNDSB_LAUNCH(kl, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
+                     m.cellColor, (const real *)ev.luOff, (const real *)x, x);
+    for (int ci = m.nColor - 1; ci >= 0; ci--)
+        DNDSB_LAUNCH(ku, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
+                     m.cellColor, (const real *)ev.luOff, (const real *)ev.luDinv, x);
+}
+
+template <int NV>
+int lu_dispatch(const MeshD &m, EvalD &ev, const real *jd, real *x, bool factor, cudaStream_t st)
+{
+    switch (m.nf)
+    {
+    case 3:
+        factor ? lu_factor_colors<NV, 3>(m, ev, jd, st) : lu_solve_colors<NV, 3>(m, ev, x, st);
+        return ST_OK;
+    case 4:
+        factor ? lu_factor_colors<NV, 4>(m, ev, jd, st) : lu_solve_colors<NV, 4>(m, ev, x, st);
+        return ST_OK;
+    case 6:
+        factor ? lu_factor_colors<NV, 6>(m, ev, jd, st) : lu_solve_colors<NV, 6>(m, ev, x, st);
+        return ST_OK;
+    }
+    return ST_UNSUPPORTED;
+}
 } // namespace
+
+int jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *jd, cudaStream_t st)
+{
+    int nv = ev.s.nVars;
+    if (ev.jacMode == 0)
+        return ST_BADARG;
+    if (ev.jacMode == 2 && !ev.lambdaFace0)
+        return ST_BADARG;
+    if (nv != 5 && nv != 6)
+        return ST_UNSUPPORTED;
+    if (!ev.luOff && (dev_alloc((void **)&ev.luOff, sizeof(real) * nv * nv * m.nCell * m.nf) != cudaSuccess ||
+                      dev_alloc((void **)&ev.luDinv, sizeof(real) * nv * nv * m.nCell) != cudaSuccess))
+        return ST_CUDA;
+    cudaMemsetAsync(ev.errWord, 0, sizeof(int), st);
+    int roe = ev.jacMode == 2;
+    if (nv == 5)
+        DNDSB_LAUNCH(k_lu_assemble<5>, m.nCell, 128, st, m, g, ev, roe, alphaDiag, u, ev.luOff);
+    else
+        DNDSB_LAUNCH(k_lu_assemble<6>, m.nCell, 128, st, m, g, ev, roe, alphaDiag, u, ev.luOff);
+    int rc = nv == 5 ? lu_dispatch<5>(m, ev, jd, nullptr, true, st) : lu_dispatch<6>(m, ev, jd, nullptr, true, st);
+    if (rc != ST_OK)
+        return rc;
+    if (last_error() != cudaSuccess)
+        return ST_CUDA;
+    int e = 0;
+    d2h(&e, ev.errWord, sizeof(int), st);
+    if (dev_sync(st) != cudaSuccess)
+        return ST_CUDA;
+    return (e & DE_SINGULAR) ? ST_NONFINITE : ST_OK;
+}
+
+int solve_jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew,
+                      const real *jd, int uIncIsZero, real *sumIncHost, cudaStream_t st)
+{
+    int nv = ev.s.nVars;
+    if (!ev.luOff || ev.jacMode == 0)
+        return ST_BADARG;
+    int64_t n = m.nCell * nv;
+    if (uIncIsZero)
+        d2d(uIncNew, rhs, sizeof(real) * n, st);
+    else
+    {
+        real *ax = ev.faceFlux; // [nCell][nv] fits in the [nFace][nv] scratch
+        int rc = lusgs_matvec_block(m, g, ev, alphaDiag, u, uInc, jd, ax, st);
+        if (rc != ST_OK)
+            return rc;
+        DNDSB_LAUNCH(k_sub, n, 256, st, n, rhs, (const real *)ax, uIncNew);
+    }
+    int rc = nv == 5 ? lu_dispatch<5>(m, ev, jd, uIncNew, false, st) : lu_dispatch<6>(m, ev, jd, uIncNew, false, st);
+    if (rc != ST_OK)
+        return rc;
+    real *absX = ev.faceFlux;
+    DNDSB_LAUNCH(k_abs_add, n, 256, st, n, (const real *)uIncNew, absX, uIncIsZero ? nullptr : uInc, uIncNew);
+    if (sumIncHost)
+    {
+        real *res = reduce_cols(0, m.nCell, nv, absX, nullptr, 0, ev.redBuf, st);
+        d2h(sumIncHost, res, sizeof(real) * nv, st);
+        if (dev_sync(st) != cudaSuccess)
+            return ST_CUDA;
+    }
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+}
 
 int lusgs_init_block(const MeshD &m, const GeomD &g, const VRD &vr, EvalD &ev, const real *dTau, real dt, real alphaDiag, const real *u,
                      real *jd, cudaStream_t st)

@@ -162,6 +162,9 @@ struct EvalD
     // EulerEvaluator.hpp:187-189, allocated for jacMode 2 as one [3][nFace] range: the convective speed after
     // EvaluateDt, the face integrals of the Riemann eigenvalues divided by the area after EvaluateRHS
     real *lambdaFace0 = nullptr, *lambdaFace123 = nullptr, *lambdaFace4 = nullptr;
+    // the local LU of LUSGSMatrixToJacobianLU (allocated on first use): slot blocks L / U [nCell][nf][nv][nv],
+    // inverted pivots [nCell][nv][nv]
+    real *luOff = nullptr, *luDinv = nullptr;
 };
 
 // EvaluateRHS flags (EulerEvaluator.hpp:370-378 RHS_* values)
@@ -204,6 +207,11 @@ int update_lusgs_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag
                        real *uIncNew, const real *jd, int forward, cudaStream_t st);
 int lusgs_matvec_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jd, real *AuInc,
                        cudaStream_t st);
+// LUSGSMatrixToJacobianLU + decomposition (block ILU(0), colour by colour) into ev.luOff / ev.luDinv, and
+// LUSGSMatrixSolveJacobianLU with it (roejac.cu); block mode only
+int jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *jd, cudaStream_t st);
+int solve_jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew,
+                      const real *jd, int uIncIsZero, real *sumIncHost, cudaStream_t st);
 // viscous part of the residual derivatives (adjoint_visc.cu): added to the inviscid face
 // cotangents [nFace][2][(R+1) nv] / face flux derivatives [nFace][nv] before their gathers
 int rhs_vjp_visc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *w, const real *u, const real *uRec, real *faceAdj,
@@ -313,7 +321,7 @@ int vr_jvp_generic(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const 
 struct LinSettings
 {
     int gmresCode = 0;   // 0 LU-SGS pairs, 1 GMRES from zero, 2 LU-SGS pairs then GMRES
-    int jacobiCode = 1;  // 1 Gauss-Seidel sweeps, 0 Jacobi sweeps
+    int jacobiCode = 1;  // 1 Gauss-Seidel sweeps, 0 Jacobi sweeps, 2 block ILU(0) (block Jacobian only)
     int sgsIter = 0;     // extra SGS pairs
     int nGmresSpace = 5; // Krylov subspace size (<= 32)
     int nGmresIter = 1;  // restarts

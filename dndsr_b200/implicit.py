@@ -199,7 +199,7 @@ class SolverConfig:
     nGmresIterRec: int = 1
     recThreshold: float = 1e-10
     gmresRecScale: int = 0
-    jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi
+    jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi, 2: the local LU (block ILU(0); block Jacobian)
     sgsIter: int = 0
     gmresCode: int = 0               # 0: LU-SGS only, 1: GMRES preconditioned by SGS
     nGmresSpace: int = 30
@@ -343,8 +343,15 @@ class ImplicitSolver:
         torch.mul(cxInc, self.alphaPP[:, None], out=self.incPP)
         self.ev.AddFixedIncrement(cx, self.incPP, alpha, refRho, refP, cfg.ppEpsIsRelaxed)
 
-    def _sgs_pair(self, alphaDiag, rhs, cx, xinc):
-        """doPrecondition, EulerSolver.hxx:1605-1635: forward then backward sweep."""
+    def _sgs_pair(self, alphaDiag, rhs, cx, xinc, zeroIn=False):
+        """doPrecondition, EulerSolver.hxx:1605-1657: forward then backward sweep, or with jacobiCode 2 two solves with
+        the local LU of the block Jacobian (factored once per linear solve)."""
+        if self.cfg.jacobiCode == 2:
+            for it in range(2):
+                self.ev.LUSGSMatrixSolveJacobianLU(alphaDiag, rhs, cx, xinc, self.tmp, self.jd, zeroIn and it == 0, want_sum=False)
+                xinc.copy_(self.tmp)
+            self.n_sgs += 1
+            return
         gs = self.cfg.jacobiCode == 1
         self.ev.UpdateSGS(alphaDiag, rhs, cx, xinc, self.tmp, self.jd, True, gs, False, want_sum=False)
         xinc.copy_(self.tmp)
@@ -364,9 +371,11 @@ class ImplicitSolver:
         if cfg.linear_precision != "fp64":
             raise ValueError("an FP32 linear solve needs the device evaluator (native_linear)")
         self.ev.LUSGSMatrixInit(self.jd, dtau, dt, alphaDiag, cx)
+        if self.cfg.jacobiCode == 2:
+            self.ev.LUSGSMatrixToJacobianLU(alphaDiag, cx, self.jd)
         cxInc.zero_()
         if self.cfg.gmresCode in (0, 2):
-            self._sgs_pair(alphaDiag, cres, cx, cxInc)
+            self._sgs_pair(alphaDiag, cres, cx, cxInc, zeroIn=True)
             for _ in range(self.cfg.sgsIter):
                 self._sgs_pair(alphaDiag, cres, cx, cxInc)
             if self.cfg.gmresCode == 0:
@@ -378,8 +387,8 @@ class ImplicitSolver:
 
         def FML(v, MLv):
             MLv.zero_()
-            for _ in range(1 + self.cfg.sgsIter):
-                self._sgs_pair(alphaDiag, v, cx, MLv)
+            for i in range(1 + self.cfg.sgsIter):
+                self._sgs_pair(alphaDiag, v, cx, MLv, zeroIn=i == 0)
 
         nv = cres.shape[1]
         ms = [m if m > 0 else 1.0 for m in (list(self.cfg.meanScale) + [1.0] * nv)[:nv]]

@@ -308,6 +308,15 @@ class EulerEvaluator:
         s = self._c.UpdateSGS(float(alphaDiag), rhs, u, uInc, uIncNew, self._jd(jdiag), bool(forward), bool(gsUpdate), bool(uIncIsZero), bool(want_sum))
         return s if want_sum else np.zeros(self.nVars)
 
+    def LUSGSMatrixToJacobianLU(self, alphaDiag, u, jdiag):
+        """EulerEvaluator.hxx:290-359 + JacobianLocalLU::InPlaceDecompose (iluCode 0): the evaluator keeps the factors."""
+        self._c.LUSGSMatrixToJacobianLU(float(alphaDiag), u, self._jd(jdiag))
+
+    def LUSGSMatrixSolveJacobianLU(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, uIncIsZero=False, want_sum=True):
+        """EulerEvaluator.hxx:838-927: uIncNew = (LU)^-1 (rhs - A uInc) + uInc; returns sumInc."""
+        s = self._c.LUSGSMatrixSolveJacobianLU(float(alphaDiag), rhs, u, uInc, uIncNew, self._jd(jdiag), bool(uIncIsZero), bool(want_sum))
+        return s if want_sum else np.zeros(self.nVars)
+
     def UpdateLUSGSForward(self, alphaDiag, rhs, u, uInc, jdiag, uIncNew):
         """EulerEvaluator.hxx:376-451: uIncNew = D^-1 (rhs - lower-neighbour flux increments of uInc).
         uInc may be uIncNew itself (the in-place sweep of the reference's callers)."""

@@ -227,6 +227,15 @@ int dndsb_eval_set_jacobian_mode(dndsb_eval *ev, int useScalarJacobian, int useR
  * jacobianCode must be 0.  A singular block gives DNDSB_E_NONFINITE (one host synchronisation in block mode). */
 int dndsb_eval_lusgs_matrix_init_full(dndsb_eval *ev, const double *dTau, double dt, double alphaDiag, const double *u, const double *uRec,
                                       int jacobianCode, double t, double *jdiag, void *stream);
+/* The local LU of the block Jacobian (jacobiCode 2; block mode only), kept inside the evaluator:
+ * to_jacobian_lu = LUSGSMatrixToJacobianLU (EulerEvaluator.hxx:290-359) with JacobianLocalLU::InPlaceDecompose
+ * (Solver/Direct.hpp:312-405) for iluCode 0 (the face-neighbour pattern, no fill): a block ILU(0) factored colour
+ * by colour, which is the reference's natural-order factorisation on a mesh numbered colour by colour
+ * (dndsb_mesh_colors).  solve_jacobian_lu = LUSGSMatrixSolveJacobianLU (:838-927): uIncNew = (LU)^-1 (rhs - A uInc)
+ * + uInc, or (LU)^-1 rhs with uIncIsZero; sumIncHost [nVars] (may be NULL) the column sums of |(LU)^-1 (...)|. */
+int dndsb_eval_lusgs_matrix_to_jacobian_lu(dndsb_eval *ev, double alphaDiag, const double *u, const double *jdiag, void *stream);
+int dndsb_eval_lusgs_matrix_solve_jacobian_lu(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc,
+                                              double *uIncNew, const double *jdiag, int uIncIsZero, double *sumIncHost, void *stream);
 /* UpdateSGS(alphaDiag, t, rhs, u, uInc, uIncNew, JDiag, forward, gsUpdate, sumInc, uIncIsZero),
  * EulerEvaluator.hxx:550-693, swept colour by colour; sumIncHost [nVars] may be NULL */
 int dndsb_eval_update_sgs(dndsb_eval *ev, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
@@ -335,7 +344,8 @@ int dndsb_eval_pressure_force_coords(dndsb_eval *ev, int zone, const double *dir
 typedef struct dndsb_linear_settings
 {
     int gmresCode;   /* 0 LU-SGS pairs, 1 GMRES from zero, 2 LU-SGS pairs then GMRES */
-    int jacobiCode;  /* 1 Gauss-Seidel sweeps (multicolour), 0 Jacobi sweeps */
+    int jacobiCode;  /* 1 Gauss-Seidel sweeps (multicolour), 0 Jacobi sweeps, 2 the local LU (block ILU(0), two
+                        defect-correction steps per doPrecondition; block Jacobian only) */
     int sgsIter;     /* extra SGS pairs (also inside the GMRES preconditioner) */
     int nGmresSpace; /* Krylov subspace size, 1..32 */
     int nGmresIter;  /* restart cycles */

@@ -121,6 +121,9 @@ def _declare(L):
     L.orc_eval_rhs_full.argtypes = [_V, _D, _D, _D, _D, _D, _D, _D]
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_set_jacobian_mode.argtypes = [_V, ctypes.c_int]
+    L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
+    L.orc_jacobian_lu.restype = ctypes.c_int
+    L.orc_solve_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
     L.orc_roe_fdiff.argtypes = [ctypes.c_int, ctypes.c_double, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
     L.orc_lusgs_init_block.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D, _D]
     L.orc_lusgs_init_block.restype = ctypes.c_int
@@ -353,6 +356,19 @@ class Oracle:
         if self.L.orc_lusgs_init_block(self.h, _p(dTau), dt, alphaDiag, _p(u), _p(jd)) != 0:
             raise FloatingPointError("singular diagonal block")
         return jd
+
+    def jacobian_lu(self, alphaDiag, u, jdiag):
+        """LUSGSMatrixToJacobianLU + InPlaceDecompose (iluCode 0, natural ordering), kept inside the oracle."""
+        if self.L.orc_jacobian_lu(self.h, alphaDiag, _p(_f64(u)), _p(_f64(jdiag))) != 0:
+            raise FloatingPointError("singular pivot block")
+
+    def solve_jacobian_lu(self, alphaDiag, rhs, u, uInc, jdiag, uIncIsZero=False):
+        """LUSGSMatrixSolveJacobianLU: returns (uIncNew, sumInc)."""
+        rhs, u, uInc, jdiag = _f64(rhs), _f64(u), _f64(uInc), _f64(jdiag)
+        out = np.zeros_like(rhs)
+        s = np.zeros(self.nv)
+        self.L.orc_solve_jacobian_lu(self.h, alphaDiag, _p(rhs), _p(u), _p(uInc), _p(out), _p(jdiag), int(uIncIsZero), _p(s))
+        return out, s
 
     def update_sgs(self, alphaDiag, rhs, u, uInc, uIncNew, jdiag, forward, gsUpdate=True, uIncIsZero=False):
         rhs, u, uInc, jdiag = _f64(rhs), _f64(u), _f64(uInc), _f64(jdiag)

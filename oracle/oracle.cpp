@@ -2494,6 +2494,188 @@ struct Oracle
         }
     }
 
+    // LUSGSMatrixToJacobianLU (EulerEvaluator.hxx:290-359) and JacobianLocalLU::InPlaceDecompose
+    // (Solver/Direct.hpp:312-405, InPlaceDecomposeV1) for iluCode 0 (the face-neighbour pattern, no fill), natural
+    // ordering and one partition.  luOff [nCell][nf][nv][nv]: per face slot the block (alpha/2)(A_f/V_c) dF/dU_o,
+    // after the decomposition L (lower neighbours, o < c) or U (upper neighbours); luDinv [nCell][nv][nv]: the
+    // inverted pivots.  Slots of boundary faces and of a cell's periodic image of itself stay zero.
+    std::vector<real> luOff, luDinv;
+    int slotOf(long c, long o) const
+    {
+        for (int k = 0; k < nf; k++)
+        {
+            long f = cell2face[c * nf + k];
+            if (otherOf(c, f) == o)
+                return k;
+        }
+        return -1;
+    }
+    static void blockMulSub(int n, const real *A, const real *B, real *C) // C -= A B
+    {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+            {
+                real acc = 0;
+                for (int l = 0; l < n; l++)
+                    acc += A[i * n + l] * B[l * n + j];
+                C[i * n + j] -= acc;
+            }
+    }
+    bool jacobianLU(real alphaDiag, const real *u, const real *jdiag)
+    {
+        int nv = es.nVars, nn = nv * nv;
+        luOff.assign(nCell * nf * nn, 0);
+        luDinv.assign(nCell * nn, 0);
+        std::vector<real> D(nCell * nn, 0);
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nCell; c++)
+        {
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                long o = otherOf(c, f);
+                if (o < 0 || o == c)
+                    continue;
+                real cf = (0.5 * alphaDiag) * faceArea[f] / vol[c];
+                real *B = &luOff[(c * nf + k) * nn];
+                for (int i = 0; i < nv; i++)
+                {
+                    real e[8] = {0}, col[8];
+                    e[i] = 1;
+                    neighbourFInc(c, f, o, u, e, col);
+                    for (int r = 0; r < nv; r++)
+                        B[r * nv + i] = cf * col[r];
+                }
+            }
+            real e[8] = {0}, y[8];
+            for (int i = 0; i < nv; i++) // JDiag.getValue (the scalar diagonal as a matrix)
+            {
+                std::fill(e, e + 8, 0.0);
+                e[i] = 1;
+                jdMul(c, jdiag, e, y);
+                for (int r = 0; r < nv; r++)
+                    D[c * nn + r * nv + i] = y[r];
+            }
+        }
+        bool ok = true;
+        for (long i = 0; i < nCell; i++)
+        {
+            // lower neighbours in ascending index order
+            std::vector<std::pair<long, int>> low, upp;
+            for (int k = 0; k < nf; k++)
+            {
+                long o = otherOf(i, cell2face[i * nf + k]);
+                if (o >= 0 && o != i)
+                    (o < i ? low : upp).push_back({o, k});
+            }
+            std::sort(low.begin(), low.end());
+            for (size_t a = 0; a < low.size(); a++)
+            {
+                long j = low[a].first;
+                real *Lij = &luOff[(i * nf + low[a].second) * nn];
+                for (size_t b = 0; b < a; b++) // k in lower(i) with k < j and j in upper(k)
+                {
+                    long k = low[b].first;
+                    int sk = slotOf(k, j);
+                    if (sk >= 0)
+                        blockMulSub(nv, &luOff[(i * nf + low[b].second) * nn], &luOff[(k * nf + sk) * nn], Lij);
+                }
+                real T[64];
+                std::copy(Lij, Lij + nn, T);
+                for (int r = 0; r < nv * nv; r++)
+                    Lij[r] = 0;
+                blockMulSub(nv, T, &luDinv[j * nn], Lij); // Lij = -(-T Dinv_j) = T Dinv_j
+                for (int r = 0; r < nn; r++)
+                    Lij[r] = -Lij[r];
+            }
+            real *Di = &D[i * nn];
+            for (auto &lk : low) // D_i -= L_ik U_ki
+            {
+                int si = slotOf(lk.first, i);
+                if (si >= 0)
+                    blockMulSub(nv, &luOff[(i * nf + lk.second) * nn], &luOff[(lk.first * nf + si) * nn], Di);
+            }
+            ok = invertBlock(nv, Di, &luDinv[i * nn]) && ok;
+            for (auto &uj : upp) // U_ij -= L_ik U_kj over k in lower(i) adjacent to j
+            {
+                real *Uij = &luOff[(i * nf + uj.second) * nn];
+                for (auto &lk : low)
+                {
+                    int sk = slotOf(lk.first, uj.first);
+                    if (sk >= 0)
+                        blockMulSub(nv, &luOff[(i * nf + lk.second) * nn], &luOff[(lk.first * nf + sk) * nn], Uij);
+                }
+            }
+        }
+        return ok;
+    }
+
+    // LUSGSMatrixSolveJacobianLU (EulerEvaluator.hxx:838-927) with JacobianLocalLU::Solve (Direct.hpp:487-540):
+    // bBuf = rhs - A uInc (rhs alone when uIncIsZero), uIncNew = (LU)^-1 bBuf (+ uInc); sumInc = |uIncNew| column sums
+    // before adding uInc
+    void solveJacobianLU(real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew, const real *jdiag, bool uIncIsZero,
+                         real *sumInc) const
+    {
+        int nv = es.nVars, nn = nv * nv;
+        std::vector<real> b(nCell * nv);
+        if (uIncIsZero)
+            std::copy(rhs, rhs + nCell * nv, b.begin());
+        else
+        {
+            lusgsMatVec(alphaDiag, u, uInc, jdiag, b.data());
+            for (long i = 0; i < nCell * nv; i++)
+                b[i] = rhs[i] - b[i];
+        }
+        std::vector<real> x(nCell * nv);
+        for (long i = 0; i < nCell; i++)
+        {
+            for (int v = 0; v < nv; v++)
+                x[i * nv + v] = b[i * nv + v];
+            for (int k = 0; k < nf; k++)
+            {
+                long o = otherOf(i, cell2face[i * nf + k]);
+                if (o < 0 || o >= i)
+                    continue;
+                const real *L = &luOff[(i * nf + k) * nn];
+                for (int r = 0; r < nv; r++)
+                    for (int l = 0; l < nv; l++)
+                        x[i * nv + r] -= L[r * nv + l] * x[o * nv + l];
+            }
+        }
+        for (long i = nCell - 1; i >= 0; i--)
+        {
+            for (int k = 0; k < nf; k++)
+            {
+                long o = otherOf(i, cell2face[i * nf + k]);
+                if (o < 0 || o <= i)
+                    continue;
+                const real *U = &luOff[(i * nf + k) * nn];
+                for (int r = 0; r < nv; r++)
+                    for (int l = 0; l < nv; l++)
+                        x[i * nv + r] -= U[r * nv + l] * x[o * nv + l];
+            }
+            real t[8];
+            const real *Di = &luDinv[i * nn];
+            for (int r = 0; r < nv; r++)
+            {
+                real acc = 0;
+                for (int l = 0; l < nv; l++)
+                    acc += Di[r * nv + l] * x[i * nv + l];
+                t[r] = acc;
+            }
+            for (int r = 0; r < nv; r++)
+                x[i * nv + r] = t[r];
+        }
+        for (int v = 0; v < nv; v++)
+            sumInc[v] = 0;
+        for (long i = 0; i < nCell; i++)
+            for (int v = 0; v < nv; v++)
+            {
+                sumInc[v] += abs(x[i * nv + v]);
+                uIncNew[i * nv + v] = x[i * nv + v] + (uIncIsZero ? 0.0 : uInc[i * nv + v]);
+            }
+    }
+
     // EulerEvaluator.hxx:550-693 UpdateSGS (sequential, natural cell order)
     void updateSGS(real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew, const real *jdiag, bool forward,
                    bool gsUpdate, bool uIncIsZero, real *sumInc) const
@@ -2883,6 +3065,8 @@ extern "C"
         else if (n == "lambdaFace") v = &o->lambdaFace;
         else if (n == "lambdaFaceC") v = &o->lambdaFaceC;
         else if (n == "lambdaFaceVis") v = &o->lambdaFaceVis;
+        else if (n == "luOff") v = &o->luOff;
+        else if (n == "luDinv") v = &o->luDinv;
         else if (n == "lambdaFace0") v = &o->lambdaFace0;
         else if (n == "lambdaFace123") v = &o->lambdaFace123;
         else if (n == "lambdaFace4") v = &o->lambdaFace4;
@@ -2930,6 +3114,17 @@ extern "C"
     void orc_lusgs_init(void *h, const double *dTau, double dt, double alphaDiag, double *jdiag)
     {
         ((Oracle *)h)->lusgsInit(dTau, dt, alphaDiag, jdiag);
+    }
+
+    // LUSGSMatrixToJacobianLU with the decomposition (iluCode 0, natural ordering); 0, or -1 on a singular pivot
+    int orc_jacobian_lu(void *h, double alphaDiag, const double *u, const double *jdiag)
+    {
+        return ((Oracle *)h)->jacobianLU(alphaDiag, u, jdiag) ? 0 : -1;
+    }
+    void orc_solve_jacobian_lu(void *h, double alphaDiag, const double *rhs, const double *u, const double *uInc, double *uIncNew,
+                               const double *jdiag, int uIncIsZero, double *sumInc)
+    {
+        ((Oracle *)h)->solveJacobianLU(alphaDiag, rhs, u, uInc, uIncNew, jdiag, uIncIsZero != 0, sumInc);
     }
 
     // useScalarJacobian / useRoeJacobian as jacMode 0 / 1 / 2 (see Oracle::jacMode)

@@ -63,6 +63,14 @@ class OracleEval:
         else:
             jd.copy_(torch.tensor(self.o.lusgs_init(dTau.numpy(), dt, alphaDiag)))
 
+    def LUSGSMatrixToJacobianLU(self, alphaDiag, u, jd):
+        self.o.jacobian_lu(alphaDiag, u.numpy(), jd.numpy())
+
+    def LUSGSMatrixSolveJacobianLU(self, alphaDiag, rhs, u, uInc, uIncNew, jd, uIncIsZero=False, want_sum=True):
+        out, s = self.o.solve_jacobian_lu(alphaDiag, rhs.numpy(), u.numpy(), uInc.numpy(), jd.numpy(), uIncIsZero)
+        uIncNew.copy_(torch.tensor(out))
+        return s
+
     def UpdateSGS(self, alphaDiag, rhs, u, uInc, uIncNew, jd, forward, gsUpdate=True, uIncIsZero=False, want_sum=True):
         out, s = self.o.update_sgs(alphaDiag, rhs.numpy(), u.numpy(), uInc.numpy(), uIncNew.numpy(), jd.numpy(), forward, gsUpdate,
                                    uIncIsZero)

@@ -115,12 +115,20 @@ def test_block_mode_without_roe_term_equals_scalar():
         assert relerr(b.numpy(), a.numpy()) < 1e-13
 
 
-def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, sgsIter, k, nIter):
+def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, sgsIter, k, nIter, jacobi=1):
+    """EulerSolver::solveLinear (EulerSolver.hxx:1407-1579) with doPrecondition (:1605-1657) on the oracle's operators."""
     jd = oe.BuildJDiag()
     oe.LUSGSMatrixInit(jd, dTau, dt, alpha, u)
+    if jacobi == 2:
+        oe.LUSGSMatrixToJacobianLU(alpha, u, jd)
     tmp = torch.zeros_like(rhs)
 
-    def pair(b, x):
+    def pair(b, x, zero):
+        if jacobi == 2:
+            for it in range(2):
+                oe.LUSGSMatrixSolveJacobianLU(alpha, b, u, x, tmp, jd, zero and it == 0)
+                x.copy_(tmp)
+            return
         oe.UpdateSGS(alpha, b, u, x, tmp, jd, True, True, False)
         x.copy_(tmp)
         oe.UpdateSGS(alpha, b, u, x, tmp, jd, False, True, False)
@@ -128,15 +136,15 @@ def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, sgsIter, k, nIter):
 
     x = torch.zeros_like(rhs)
     if code in (0, 2):
-        for _ in range(1 + sgsIter):
-            pair(rhs, x)
+        for i in range(1 + sgsIter):
+            pair(rhs, x, i == 0)
     if code:
         g = I.GMRES(k, x)
 
         def FML(v, Mv):
             Mv.zero_()
-            for _ in range(1 + sgsIter):
-                pair(v, Mv)
+            for i in range(1 + sgsIter):
+                pair(v, Mv, i == 0)
 
         g.solve(lambda v, Av: oe.LUSGSMatrixVec(alpha, u, v, jd, Av), FML, lambda a, b: float((a * b).sum()), rhs, x, nIter,
                 lambda i, r, rb: False)
@@ -144,8 +152,8 @@ def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, sgsIter, k, nIter):
 
 
 @pytest.mark.parametrize("name,mesh,p,rs,mu,bt", [CASES[0], CASES[2], CASES[4]], ids=[CASES[i][0] for i in (0, 2, 4)])
-@pytest.mark.parametrize("code,sgsIter,k,nIter", [(0, 1, 1, 1), (1, 0, 8, 2), (2, 1, 5, 1)])
-def test_roe_jacobian_linear_solve(name, mesh, p, rs, mu, bt, code, sgsIter, k, nIter):
+@pytest.mark.parametrize("code,sgsIter,k,nIter,jacobi", [(0, 1, 1, 1, 1), (1, 0, 8, 2, 1), (2, 1, 5, 1, 1), (0, 1, 1, 1, 2), (1, 0, 8, 1, 2)])
+def test_roe_jacobian_linear_solve(name, mesh, p, rs, mu, bt, code, sgsIter, k, nIter, jacobi):
     m, o, vr, ev, u0, uRec0 = _setup(mesh, p, rs, mu, bt)
     oe = OracleEval(o)
     oe.SetJacobianMode(False, True)
@@ -156,7 +164,7 @@ def test_roe_jacobian_linear_solve(name, mesh, p, rs, mu, bt, code, sgsIter, k, 
     oe.EvaluateRHS(torch.zeros_like(ut), ut, uRt)  # records the eigenvalues
     rhs0 = torch.tensor(np.random.default_rng(3).normal(size=(m.n_cell, 5)))
     alpha, dt = 0.5, 10.0
-    ref = _reference_solve(oe, ut, rhs0, dTau0, dt, alpha, code, sgsIter, k, nIter)
+    ref = _reference_solve(oe, ut, rhs0, dTau0, dt, alpha, code, sgsIter, k, nIter, jacobi)
     u, uRec, rhs = ut.cuda(), uRt.cuda(), rhs0.cuda()
     dTau = torch.zeros(m.n_cell, dtype=torch.float64, device="cuda")
     ev.EvaluateDt(dTau, u, 1e3)
@@ -165,7 +173,7 @@ def test_roe_jacobian_linear_solve(name, mesh, p, rs, mu, bt, code, sgsIter, k, 
         outs = []
         for graph in (True, True, False):
             x = torch.full_like(rhs, 7.0)
-            ev.SolveLinear(alpha, dTau, dt, u, rhs, x, gmresCode=code, jacobiCode=1, sgsIter=sgsIter, nGmresSpace=k, nGmresIter=nIter,
+            ev.SolveLinear(alpha, dTau, dt, u, rhs, x, gmresCode=code, jacobiCode=jacobi, sgsIter=sgsIter, nGmresSpace=k, nGmresIter=nIter,
                            precision=prec, useGraph=graph)
             outs.append(x.cpu())
         assert relerr(outs[0].numpy(), ref.numpy()) < tol, prec
@@ -179,6 +187,55 @@ def test_roe_jacobian_driver_matches_oracle_driver():
     far = M.freestream(0.8)
     kw = dict(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=6, nTimeStepInternalMin=6, CFL=50.0, gmresCode=1,
               nGmresSpace=10, sgsIter=0)
+    oe = OracleEval(o)
+    oe.SetJacobianMode(False, True)
+    ev.SetJacobianMode(False, True)
+    u_o = torch.tensor(np.tile(far, (m.n_cell, 1)))
+    I.ImplicitSolver(OracleVR(o), oe, I.SolverConfig(**kw)).run(u_o)
+    u = torch.tensor(np.tile(far, (m.n_cell, 1)), device="cuda")
+    I.ImplicitSolver(vr, ev, I.SolverConfig(**kw)).run(u)
+    assert relerr(u.cpu().numpy(), u_o.numpy()) < 1e-10
+
+
+@pytest.mark.parametrize("roe", [False, True])
+def test_local_lu_operators(roe):
+    """LUSGSMatrixToJacobianLU + LUSGSMatrixSolveJacobianLU (block ILU(0)) against the oracle's natural-order
+    factorisation on the colour-numbered bump mesh."""
+    m, o, vr, ev, u0, uRec0 = _setup("bump", 1, "Roe", 0.0, (1, 1, 3))
+    o.set_jacobian_mode(False, roe)
+    ev.SetJacobianMode(False, roe)
+    u, uRec = torch.tensor(u0, device="cuda"), torch.tensor(uRec0, device="cuda")
+    dt = torch.zeros(m.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dt, u, 20.0)
+    d0, _ = o.eval_dt(u0, 20.0)
+    rhs = torch.zeros_like(u)
+    ev.EvaluateRHS(rhs, u, uRec)
+    rhs0 = o.eval_rhs(u0, uRec0)
+    jd = ev.BuildJDiag()
+    ev.LUSGSMatrixInit(jd, dt, 1e100, 1.0, u)
+    jd0 = o.lusgs_init_block(d0, 1e100, 1.0, u0)
+    ev.LUSGSMatrixToJacobianLU(1.0, u, jd)
+    o.jacobian_lu(1.0, u0, jd0)
+    x0 = np.random.default_rng(7).normal(size=u0.shape)
+    x = torch.tensor(x0, device="cuda")
+    out = torch.zeros_like(u)
+    for zero in (True, False):
+        s = ev.LUSGSMatrixSolveJacobianLU(1.0, rhs, u, x, out, jd, zero)
+        ref, s0 = o.solve_jacobian_lu(1.0, rhs0, u0, x0, jd0, zero)
+        assert relerr(out.cpu().numpy(), ref) < 1e-11, zero
+        assert relerr(np.asarray(s), s0) < 1e-11
+    from dndsr_b200.capi import DndsbError
+    with pytest.raises(DndsbError):  # uIncNew must not alias uInc
+        ev.LUSGSMatrixSolveJacobianLU(1.0, rhs, u, out, out, jd, False)
+
+
+def test_local_lu_driver_matches_oracle_driver():
+    """The reference's Roe-Jacobian configuration (jacobiCode 2 without GMRES): six BDF1 pseudo-time iterations of
+    the steady bump at CFL 50, the GPU driver (native block ILU(0) solve) against the same driver on the oracle."""
+    m, o, vr, ev, u0, uRec0 = _setup("bump", 1, "Roe", 0.0, (1, 1, 3))
+    far = M.freestream(0.8)
+    kw = dict(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=6, nTimeStepInternalMin=6, CFL=50.0, gmresCode=0, jacobiCode=2,
+              sgsIter=0)
     oe = OracleEval(o)
     oe.SetJacobianMode(False, True)
     ev.SetJacobianMode(False, True)

@@ -127,3 +127,57 @@ def test_roe_jacobian_converges_faster_on_the_bump():
         I.ImplicitSolver(OracleVR(o), oe, cfg).run(u)
         drops[roe] = cfg.res_history[-1][2]
     assert drops[True] < 0.7 * drops[False], drops
+
+
+def _dense(o, n, nv, f):
+    """The n nv x n nv matrix of the linear map f (column by column)."""
+    A = np.zeros((n * nv, n * nv))
+    for i in range(n * nv):
+        e = np.zeros((n, nv))
+        e.flat[i] = 1.0
+        A[:, i] = f(e).ravel()
+    return A
+
+
+def test_block_ilu0_factors_match_the_operator_on_its_pattern():
+    """JacobianLocalLU with iluCode 0: L U equals the LUSGSMatrixVec operator A on A's block pattern, and the
+    LU solve inverts L U exactly; one defect-correction step reduces the residual of A x = b."""
+    m = M.renumber_by_color(M.bump_channel_tet(3, 2, 2))
+    o, far, types, vals, w = bump_oracle(m, 1, "Roe", 0.0, 1)
+    u0, uRec0 = perturbed_state(m, far, R=o.R)
+    o.set_jacobian_mode(False, True)
+    d0, _ = o.eval_dt(u0, 20.0)
+    o.eval_rhs(u0, uRec0)
+    jd = o.lusgs_init_block(d0, 1e100, 1.0, u0)
+    n, nv = m.n_cell, 5
+    A = _dense(o, n, nv, lambda x: o.lusgs_matvec(1.0, u0, x, jd))
+    o.jacobian_lu(1.0, u0, jd)
+    off = o.get("luOff").reshape(n, -1, nv, nv)
+    dinv = o.get("luDinv").reshape(n, nv, nv)
+    f2c = np.asarray(m.face2cell)
+    c2f = np.asarray(m.cell2face)
+    L, U = np.eye(n * nv), np.zeros((n * nv, n * nv))
+    pattern = np.zeros((n, n), bool)
+    for i in range(n):
+        U[i * nv:(i + 1) * nv, i * nv:(i + 1) * nv] = np.linalg.inv(dinv[i])
+        pattern[i, i] = True
+        for k, f in enumerate(c2f[i]):
+            c0, c1 = f2c[f]
+            j = c1 if c0 == i else c0
+            if j < 0 or j == i:
+                continue
+            pattern[i, j] = True
+            blk = (L if j < i else U)
+            blk[i * nv:(i + 1) * nv, j * nv:(j + 1) * nv] = off[i, k]
+    LU = L @ U
+    mask = np.kron(pattern, np.ones((nv, nv), bool))
+    assert np.abs((LU - A)[mask]).max() < 1e-12 * np.abs(A).max()
+    assert np.abs(LU[~mask]).max() > 0  # the incomplete factorisation drops fill on this mesh
+    b = np.random.default_rng(5).normal(size=(n, nv))
+    x, s = o.solve_jacobian_lu(1.0, b, u0, np.zeros_like(b), jd, uIncIsZero=True)
+    assert np.allclose(LU @ x.ravel(), b.ravel(), rtol=0, atol=1e-12 * np.abs(b).max())
+    assert np.allclose(s, np.abs(x).sum(0))
+    x2, _ = o.solve_jacobian_lu(1.0, b, u0, x, jd, uIncIsZero=False)
+    r1 = np.linalg.norm(b.ravel() - A @ x.ravel())
+    r2 = np.linalg.norm(b.ravel() - A @ x2.ravel())
+    assert r2 < 0.5 * r1, (r1, r2)
