@@ -216,18 +216,26 @@ def run_steady(args):
     """Wall time to a 1e-10 residual drop, mixed vs FP64, on the steady transonic bump (BCFar in/out, BCWallInvis
     floor/ceiling, BCSym sides, Mach 0.8, VR degree 1, Roe_M2): BDF1 dual time at CFL 200, GMRES(30) preconditioned
     by one SGS pair, FP64 or FP32 linear solve inside the FP64 defect correction, each precision from the free
-    stream after a two-iteration warm-up; on the configuration's ~2M-tet mesh and on a 250k-tet one."""
+    stream after a two-iteration warm-up; on the configuration's ~2M-tet mesh and on a 250k-tet one.  With the Roe
+    Jacobian (roe_jacobian): the same runs with the block Roe Jacobian and the local LU preconditioner."""
     import torch
     from dndsr_b200 import implicit as I
 
-    def solve(vr, ev, far, prec, iters, thr):
+    # the scalar Jacobian: CFL 200, GMRES(30) preconditioned by one SGS pair, one VR sweep per iteration;
+    # the Roe Jacobian (useRoeJacobian, block diagonal): CFL 1e4, GMRES(10) preconditioned by the local LU
+    # (jacobiCode 2, block ILU(0)), four VR sweeps per iteration
+    SCALAR = dict(CFL=200.0, gmresCode=1, nGmresSpace=30, jacobiCode=1, nInternalRecStep=1)
+    ROE = dict(CFL=1e4, gmresCode=1, nGmresSpace=10, jacobiCode=2, nInternalRecStep=4)
+
+    def solve(vr, ev, far, prec, iters, thr, lin=SCALAR):
+        ev.SetJacobianMode(lin is SCALAR, lin is ROE)
         u = vr.BuildUDof(5)
         u[:] = torch.tensor(far, device="cuda")
         I.ImplicitSolver(vr, ev, I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=2, nTimeStepInternalMin=2,
-                                                CFL=200.0, gmresCode=1, nGmresSpace=30, linear_precision=prec)).run(u)
+                                                linear_precision=prec, **lin)).run(u)
         u[:] = torch.tensor(far, device="cuda")
-        cfg = I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=iters, nTimeStepInternalMin=5, CFL=200.0,
-                             gmresCode=1, nGmresSpace=30, nGmresIter=1, sgsIter=0, rhsThresholdInternal=thr, linear_precision=prec)
+        cfg = I.SolverConfig(odeCode=1, dtImplicit=1e100, nTimeStep=1, nTimeStepInternal=iters, nTimeStepInternalMin=5, nGmresIter=1, sgsIter=0,
+                             rhsThresholdInternal=thr, linear_precision=prec, **lin)
         solver = I.ImplicitSolver(vr, ev, cfg)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -268,6 +276,21 @@ def run_steady(args):
                "final_drop_fp64": a[3], "final_drop_mixed": b[3],
                "state_rel_diff": float((a[0] - b[0]).abs().max() / a[0].abs().max()),
                "ms_vr_sweep_plus_rhs": comp["fp64"][0], "ms_linear_solve_fp64": comp["fp64"][1], "ms_linear_solve_fp32": comp["fp32"][1]}
+        if args.steady_roe:
+            roe = {}
+            for prec in ("fp64", "fp32"):
+                roe[prec] = solve(vr, ev, far, prec, iters, 1e-10, ROE)
+            c, d = roe["fp64"], roe["fp32"]
+            res["roe_jacobian"] = {
+                "settings": "useRoeJacobian (block diagonal), CFL 1e4, GMRES(10) preconditioned by the local LU (jacobiCode 2, block "
+                            "ILU(0) in colour order), nInternalRecStep 4",
+                "converged_fp64": c[3] < 1e-10, "converged_mixed": d[3] < 1e-10, "iterations_fp64": c[2], "iterations_mixed": d[2],
+                "fp64_s": c[1], "mixed_s": d[1], "mixed_over_fp64_time": d[1] / c[1], "fp64_ms_per_iter": 1e3 * c[1] / c[2],
+                "mixed_ms_per_iter": 1e3 * d[1] / d[2], "final_drop_fp64": c[3], "final_drop_mixed": d[3],
+                "fp64_over_scalar_fp64_time": c[1] / a[1], "mixed_over_scalar_fp64_time": d[1] / a[1],
+                "state_rel_diff_vs_scalar": float((c[0] - a[0]).abs().max() / a[0].abs().max())}
+            del roe, c, d
+            ev.SetJacobianMode(True, False)
         del out, vr, ev
         torch.cuda.empty_cache()
         return res
@@ -846,6 +869,7 @@ def main():
     ap.add_argument("--steady-iters", type=int, default=3000)
     ap.add_argument("--steady-big-mesh", type=int, nargs=3, default=(160, 80, 26))
     ap.add_argument("--steady-big-iters", type=int, default=4000)
+    ap.add_argument("--no-steady-roe", dest="steady_roe", action="store_false", help="skip the Roe-Jacobian steady runs")
     ap.add_argument("--adjoint-mesh", type=int, nargs=3, default=(80, 40, 13))
     ap.add_argument("--no-sa", action="store_true")
     # the extra measurement blocks after the headline, comma separated (a subset for profiling runs)

@@ -5,8 +5,11 @@
 // solved) in one launch.  On a mesh numbered colour by colour this is the reference's natural-order
 // factorisation.
 //
-// Storage per row r: off [r][NF][NV][NV] (slot blocks of A, then L for lower and U for upper neighbours) and
-// dinv [r][NV][NV] (the inverted pivots).  nbr [r][NF] holds the neighbour row of each slot (-1: none).
+// Storage: off holds per row r and slot k the block of A (then L for lower and U for upper neighbours), dinv the
+// inverted pivots, D the diagonal blocks of A.  BlockLay places element e of row r (E elements per row) in tiles
+// of 2^s rows: rows of a tile innermost, so that the 32 threads of a warp read one element of 32 consecutive rows
+// as one contiguous 256-byte line and a warp's rows share one contiguous range; s = 0 is rows outermost
+// ([row][E]).  nbr [r][NF] holds the neighbour row of each slot (-1: none).
 #pragma once
 #include "roejac.cuh"
 
@@ -14,6 +17,15 @@ namespace dndsb
 {
 namespace ilu
 {
+struct BlockLay
+{
+    int64_t E; // elements per row
+    int s;     // log2 of the rows per tile
+    DNDSB_HD int64_t at(int64_t r, int64_t e) const { return ((((r >> s) * E) + e) << s) + (r & ((int64_t(1) << s) - 1)); }
+};
+// rows allocated for a tiled layout of n rows
+inline int64_t padded_rows(int64_t n, int s) { return ((n + (int64_t(1) << s) - 1) >> s) << s; }
+
 template <int NV>
 DNDSB_HD void mul_sub(const real *A, const real *B, real *C) // C -= A B (row-major NV x NV)
 {
@@ -36,16 +48,24 @@ DNDSB_HD int slot_of(const int32_t *nbr, int64_t r, int64_t target)
     return -1;
 }
 
+// the block of elements e0 .. e0 + NV NV - 1 of row r
 template <typename T, int NV>
-DNDSB_HD void load(const T *src, real *dst)
+DNDSB_HD void load(const T *src, BlockLay L, int64_t r, int e0, real *dst)
 {
     for (int i = 0; i < NV * NV; i++)
-        dst[i] = (real)src[i];
+        dst[i] = (real)src[L.at(r, e0 + i)];
+}
+template <typename T, int NV>
+DNDSB_HD void store(const real *v, T *dst, BlockLay L, int64_t r, int e0)
+{
+    for (int i = 0; i < NV * NV; i++)
+        dst[L.at(r, e0 + i)] = (T)v[i];
 }
 
-// one row of the factorisation: A (the operator's slot blocks), D (the diagonal block), both of row r
+// one row of the factorisation: A (the operator's slot blocks) and D (diagonal blocks) in, off / dinv out
 template <typename T, int NV, int NF>
-DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, const T *A, const T *D, T *off, T *dinv)
+DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, const T *A, const T *D, BlockLay offL, BlockLay dL, BlockLay DL,
+                         T *off, T *dinv)
 {
     constexpr int NN = NV * NV;
     auto rk = [&](int64_t x) { return rank ? (int64_t)rank[x] : x; };
@@ -72,7 +92,7 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
     {
         int64_t j = nbr[r * NF + low[a]];
         real *Lij = L + a * NN;
-        load<T, NV>(A + (r * NF + low[a]) * NN, Lij);
+        load<T, NV>(A, offL, r, low[a] * NN, Lij);
         for (int b = 0; b < a; b++)
         {
             int64_t k = nbr[r * NF + low[b]];
@@ -80,12 +100,12 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
             if (s >= 0)
             {
                 real Ukj[NN];
-                load<T, NV>(off + (k * NF + s) * NN, Ukj);
+                load<T, NV>(off, offL, k, s * NN, Ukj);
                 mul_sub<NV>(L + b * NN, Ukj, Lij);
             }
         }
         real Dj[NN], t[NN];
-        load<T, NV>(dinv + j * NN, Dj);
+        load<T, NV>(dinv, dL, j, 0, Dj);
         for (int i = 0; i < NN; i++)
             t[i] = 0;
         mul_sub<NV>(Lij, Dj, t);
@@ -93,7 +113,7 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
             Lij[i] = -t[i];
     }
     real Di[NN], Dinv[NN];
-    load<T, NV>(D, Di);
+    load<T, NV>(D, DL, r, 0, Di);
     for (int b = 0; b < nLow; b++)
     {
         int64_t k = nbr[r * NF + low[b]];
@@ -101,18 +121,20 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
         if (s >= 0)
         {
             real Uki[NN];
-            load<T, NV>(off + (k * NF + s) * NN, Uki);
+            load<T, NV>(off, offL, k, s * NN, Uki);
             mul_sub<NV>(L + b * NN, Uki, Di);
         }
     }
     bool ok = roej::block_inv<NV>(Di, Dinv);
-    for (int i = 0; i < NN; i++)
-        dinv[r * NN + i] = ok ? (T)Dinv[i] : T(0);
+    if (!ok)
+        for (int i = 0; i < NN; i++)
+            Dinv[i] = 0;
+    store<T, NV>(Dinv, dinv, dL, r, 0);
     for (int a = 0; a < nUpp; a++)
     {
         int64_t j = nbr[r * NF + upp[a]];
         real Uij[NN];
-        load<T, NV>(A + (r * NF + upp[a]) * NN, Uij);
+        load<T, NV>(A, offL, r, upp[a] * NN, Uij);
         for (int b = 0; b < nLow; b++)
         {
             int64_t k = nbr[r * NF + low[b]];
@@ -120,37 +142,37 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
             if (s >= 0)
             {
                 real Ukj[NN];
-                load<T, NV>(off + (k * NF + s) * NN, Ukj);
+                load<T, NV>(off, offL, k, s * NN, Ukj);
                 mul_sub<NV>(L + b * NN, Ukj, Uij);
             }
         }
-        for (int i = 0; i < NN; i++)
-            off[(r * NF + upp[a]) * NN + i] = (T)Uij[i];
+        store<T, NV>(Uij, off, offL, r, upp[a] * NN);
     }
     for (int a = 0; a < nLow; a++)
-        for (int i = 0; i < NN; i++)
-            off[(r * NF + low[a]) * NN + i] = (T)L[a * NN + i];
+        store<T, NV>(L + a * NN, off, offL, r, low[a] * NN);
     // slots without a neighbour (boundary faces) and a row's periodic image of itself carry nothing
+    real zero[NN];
+    for (int i = 0; i < NN; i++)
+        zero[i] = 0;
     for (int k = 0; k < NF; k++)
     {
         int64_t q = nbr[r * NF + k];
         if (q < 0 || q == r)
-            for (int i = 0; i < NN; i++)
-                off[(r * NF + k) * NN + i] = T(0);
+            store<T, NV>(zero, off, offL, r, k * NN);
     }
     return ok;
 }
 
-// rows: the rows of one colour (nullptr: the contiguous range [beg, end)); dStride: elements between diagonal blocks
+// rows: the rows of one colour (nullptr: the contiguous range [beg, end))
 template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_ilu_factor(int64_t beg, int64_t end, const int32_t *__restrict__ rows, const int32_t *__restrict__ nbr,
-                               const int32_t *__restrict__ rank, const T *A, const T *__restrict__ D, int64_t dStride, T *off, T *dinv,
-                               int *err) // A may be off (factored in place)
+                               const int32_t *__restrict__ rank, const T *A, const T *__restrict__ D, BlockLay offL, BlockLay dL, BlockLay DL,
+                               T *off, T *dinv, int *err) // A may be off (factored in place)
 {
     DNDSB_KERNEL_LOOP(ii, end - beg)
     {
         int64_t r = rows ? (int64_t)rows[beg + ii] : beg + ii;
-        if (!factor_row<T, NV, NF>(r, nbr, rank, A, D + r * dStride, off, dinv))
+        if (!factor_row<T, NV, NF>(r, nbr, rank, A, D, offL, dL, DL, off, dinv))
             atomicOr(err, (int)DE_SINGULAR);
     }
 }
@@ -159,8 +181,9 @@ DNDSB_GLOBAL void k_ilu_factor(int64_t beg, int64_t end, const int32_t *__restri
 // in place on x (= y)
 template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_ilu_lower(int64_t beg, int64_t end, const int32_t *__restrict__ rows, const int32_t *__restrict__ nbr,
-                              const int32_t *__restrict__ rank, const T *__restrict__ off, const T *b, T *x) // b may be x
+                              const int32_t *__restrict__ rank, const T *__restrict__ off, BlockLay offL, const T *b, T *x) // b may be x
 {
+    constexpr int NN = NV * NV;
     DNDSB_KERNEL_LOOP(ii, end - beg)
     {
         int64_t r = rows ? (int64_t)rows[beg + ii] : beg + ii;
@@ -174,12 +197,14 @@ DNDSB_GLOBAL void k_ilu_lower(int64_t beg, int64_t end, const int32_t *__restric
             int64_t q = nbr[r * NF + k];
             if (q < 0 || q == r || (rank ? (int64_t)rank[q] : q) >= rr)
                 continue;
-            const T *L = off + (r * NF + k) * NV * NV;
+            T xq[NV];
+            for (int l = 0; l < NV; l++)
+                xq[l] = x[q * NV + l];
             for (int i = 0; i < NV; i++)
             {
                 T s = 0;
                 for (int l = 0; l < NV; l++)
-                    s += L[i * NV + l] * x[q * NV + l];
+                    s += off[offL.at(r, k * NN + i * NV + l)] * xq[l];
                 acc[i] -= s;
             }
         }
@@ -190,13 +215,15 @@ DNDSB_GLOBAL void k_ilu_lower(int64_t beg, int64_t end, const int32_t *__restric
 
 template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_ilu_upper(int64_t beg, int64_t end, const int32_t *__restrict__ rows, const int32_t *__restrict__ nbr,
-                              const int32_t *__restrict__ rank, const T *__restrict__ off, const T *__restrict__ dinv, T *x)
+                              const int32_t *__restrict__ rank, const T *__restrict__ off, BlockLay offL, const T *__restrict__ dinv, BlockLay dL,
+                              T *x)
 {
+    constexpr int NN = NV * NV;
     DNDSB_KERNEL_LOOP(ii, end - beg)
     {
         int64_t r = rows ? (int64_t)rows[beg + ii] : beg + ii;
         int64_t rr = rank ? (int64_t)rank[r] : r;
-        T acc[NV], y[NV];
+        T acc[NV];
         for (int v = 0; v < NV; v++)
             acc[v] = x[r * NV + v];
 #pragma unroll
@@ -205,18 +232,24 @@ DNDSB_GLOBAL void k_ilu_upper(int64_t beg, int64_t end, const int32_t *__restric
             int64_t q = nbr[r * NF + k];
             if (q < 0 || q == r || (rank ? (int64_t)rank[q] : q) <= rr)
                 continue;
-            const T *U = off + (r * NF + k) * NV * NV;
+            T xq[NV];
+            for (int l = 0; l < NV; l++)
+                xq[l] = x[q * NV + l];
             for (int i = 0; i < NV; i++)
             {
                 T s = 0;
                 for (int l = 0; l < NV; l++)
-                    s += U[i * NV + l] * x[q * NV + l];
+                    s += off[offL.at(r, k * NN + i * NV + l)] * xq[l];
                 acc[i] -= s;
             }
         }
-        roej::block_mul<NV>(dinv + r * NV * NV, acc, y);
-        for (int v = 0; v < NV; v++)
-            x[r * NV + v] = y[v];
+        for (int i = 0; i < NV; i++)
+        {
+            T s = 0;
+            for (int l = 0; l < NV; l++)
+                s += dinv[dL.at(r, i * NV + l)] * acc[l];
+            x[r * NV + i] = s;
+        }
     }
 }
 } // namespace ilu

@@ -238,71 +238,152 @@ DNDSB_GLOBAL void k_matvec_pos(int64_t n, const int32_t *__restrict__ nbrPos, co
     }
 }
 
-// block operator build: diagonal block + inverse [p][2][NV][NV], off-diagonal blocks [p][NF][NV][NV] (zero on boundaries)
-template <typename T, int NV>
+// block operator build.  Storage is tiled by 32 positions (ilu::BlockLay, s = 5): element k NV NV + e of a position's
+// row of opB is element e of slot k's off-diagonal block (zero on boundaries); elements e and NV NV + e of jdB are
+// the diagonal block and its inverse.  A warp reads one element of its 32 positions as one 256-byte line
+// (FP64).  Per face slot the Roe dissipation
+// matrix M of the face (Roe average of the two cells, the eigenvalues seen from this cell) is formed once: the
+// diagonal block gains w (M + lambdaVis I) (and on a boundary face w (A(u_g) - M - lambdaVis I) dGhost/du), the
+// off-diagonal block is w (A(u_o) - M - lambdaVis I); without the Roe term w (A(u_o) - lambdaFace I) and the
+// scalar diagonal.  The same blocks as roej::cell_block and the neighbour increments, summed in the same order.
+template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_sgsop_build_blk(MeshD m, GeomD g, BoundaryD bnd, EvalD ev, int roe, const real *__restrict__ dTau, real dt, real alphaDiag,
                                     const real *__restrict__ u, const int32_t *__restrict__ cellPos, int32_t *nbrPos, T *opB, T *jdB, int *err)
 {
     using namespace roej;
+    constexpr int NN = NV * NV;
+    const ilu::BlockLay oL{NF * NN, 5}, dL{2 * NN, 5};
+    const real gamma = ev.s.gamma;
     DNDSB_KERNEL_LOOP(p, m.nCell)
     {
         int64_t c = m.colorCells[p];
-        real B[NV * NV], Bi[NV * NV];
-        cell_block<NV>(m, g, bnd, ev, roe != 0, dTau, dt, alphaDiag, u, c, B);
+        const real *uc = u + c * NV;
+        real B[NN];
+        for (int i = 0; i < NN; i++)
+            B[i] = 0;
+        real fp = 1.0 / dTau[c] + 1.0 / dt;
+        const real iv = 1.0 / g.vol[c];
+#pragma unroll 1
+        for (int k = 0; k < NF; k++)
+        {
+            int o = m.cellNbr[c * NF + k];
+            nbrPos[p * NF + k] = o < 0 ? -1 : cellPos[o];
+            int pk = m.cell2face[c * NF + k];
+            int64_t f = pk >> 1;
+            int side = pk & 1;
+            fp += (0.5 * alphaDiag) * g.faceArea[f] * ev.lambdaFace[f] * iv;
+            real sg = side ? -1.0 : 1.0;
+            real nn[3] = {g.faceMeanNorm[f * 3] * sg, g.faceMeanNorm[f * 3 + 1] * sg, g.faceMeanNorm[f * 3 + 2] * sg};
+            real w = (0.5 * alphaDiag) * g.faceArea[f] * iv;
+            real O[NN]; // the off-diagonal block (before w), zero on boundaries
+            for (int i = 0; i < NN; i++)
+                O[i] = 0;
+            real uj[NV];
+            if (o >= 0)
+            {
+                for (int v = 0; v < NV; v++)
+                    uj[v] = u[(int64_t)o * NV + v];
+                for (int i = 0; i < NV; i++) // A(u_o) by columns
+                {
+                    real e[NV], col[NV];
+                    for (int v = 0; v < NV; v++)
+                        e[v] = v == i ? 1.0 : 0.0;
+                    flux_inc<NV>(uj, nn, e, gamma, col);
+                    for (int v = 0; v < NV; v++)
+                        O[v * NV + i] = col[v];
+                }
+            }
+            if (!roe)
+            {
+                if (o >= 0)
+                    for (int i = 0; i < NV; i++)
+                        O[i * NV + i] -= ev.lambdaFace[f];
+            }
+            else
+            {
+                int zone = m.faceZone[f];
+                if (o < 0 && !bc_value<NV>(bnd, zone, uc, nn, uj))
+                    for (int v = 0; v < NV; v++)
+                        uj[v] = uc[v];
+                FaceLam L = face_lam(ev, f, side);
+                RoeAvg r;
+                roe_average(uc, uj, gamma, r);
+                real M[NN];
+                for (int i = 0; i < NV; i++)
+                {
+                    real e[NV], col[NV];
+                    for (int v = 0; v < NV; v++)
+                        e[v] = v == i ? 1.0 : 0.0, col[v] = 0;
+                    roe_fdiff_add<NV>(e, nn, r, gamma, L.l0, L.l123, L.l4, col);
+                    for (int v = 0; v < NV; v++)
+                        M[v * NV + i] = col[v] + (v == i ? L.vis : 0.0);
+                }
+                for (int i = 0; i < NN; i++)
+                    B[i] += w * M[i];
+                if (o >= 0)
+                    for (int i = 0; i < NN; i++)
+                        O[i] -= M[i];
+                else
+                {
+                    // (A(u_g) - M) JBC with the linearised ghost JBC (column-major)
+                    int bt = (zone >= 0 && zone < bnd.nZone) ? bnd.type[zone] : 0;
+                    real JBC[NN];
+                    bc_linear<NV>(bt, nn, JBC);
+                    for (int i = 0; i < NV; i++)
+                    {
+                        real dcol[NV], col[NV];
+                        bool zero = true;
+                        for (int v = 0; v < NV; v++)
+                            dcol[v] = JBC[i * NV + v], zero = zero && dcol[v] == 0;
+                        if (zero)
+                            continue;
+                        flux_inc<NV>(uj, nn, dcol, gamma, col);
+                        for (int v = 0; v < NV; v++)
+                        {
+                            real md = 0;
+                            for (int l = 0; l < NV; l++)
+                                md += M[v * NV + l] * dcol[l];
+                            B[v * NV + i] += w * (col[v] - md);
+                        }
+                    }
+                }
+            }
+            for (int i = 0; i < NN; i++)
+                opB[oL.at(p, k * NN + i)] = (T)(w * O[i]);
+        }
+        for (int i = 0; i < NV; i++)
+        {
+            if (roe)
+                B[i * NV + i] += 1.0 / dTau[c] + 1.0 / dt;
+            else
+                B[i * NV + i] = fp;
+            if (NV >= 6 && ev.jSource)
+                B[i * NV + i] += alphaDiag * ev.jSource[c * NV + i];
+        }
+        real Bi[NN];
         if (!block_inv<NV>(B, Bi))
         {
             atomicOr(err, (int)DE_SINGULAR);
-            for (int i = 0; i < NV * NV; i++)
+            for (int i = 0; i < NN; i++)
                 Bi[i] = 0;
         }
-        T *jo = jdB + p * 2 * NV * NV;
-        for (int i = 0; i < NV * NV; i++)
-            jo[i] = (T)B[i], jo[NV * NV + i] = (T)Bi[i];
-        const real cf = 0.5 * alphaDiag / g.vol[c];
-        for (int k = 0; k < m.nf; k++)
-        {
-            int o = m.cellNbr[c * m.nf + k];
-            nbrPos[p * m.nf + k] = o < 0 ? -1 : cellPos[o];
-            T *ob = opB + (p * m.nf + k) * NV * NV;
-            if (o < 0)
-            {
-                for (int i = 0; i < NV * NV; i++)
-                    ob[i] = 0;
-                continue;
-            }
-            int pk = m.cell2face[c * m.nf + k];
-            int64_t f = pk >> 1;
-            int side = pk & 1;
-            real sg = side ? -1.0 : 1.0;
-            real n[3] = {g.faceMeanNorm[f * 3] * sg, g.faceMeanNorm[f * 3 + 1] * sg, g.faceMeanNorm[f * 3 + 2] * sg};
-            FaceLam L;
-            if (roe)
-                L = face_lam(ev, f, side);
-            else
-                L.main = ev.lambdaFace[f], L.l0 = L.l123 = L.l4 = L.vis = 0;
-            real w = cf * g.faceArea[f];
-            for (int i = 0; i < NV; i++)
-            {
-                real e[NV], col[NV];
-                for (int v = 0; v < NV; v++)
-                    e[v] = v == i ? 1.0 : 0.0;
-                nbr_inc<NV>(roe != 0, u + (int64_t)o * NV, u + c * NV, n, e, L, ev.s.gamma, col);
-                for (int v = 0; v < NV; v++)
-                    ob[v * NV + i] = (T)(w * col[v]);
-            }
-        }
+        for (int i = 0; i < NN; i++)
+            jdB[dL.at(p, i)] = (T)B[i], jdB[dL.at(p, NN + i)] = (T)Bi[i];
     }
 }
 
 // one colour class of a sweep with the block operator: x_p = D_p^-1 (rhs_p - sum_k O_pk x_q)
 template <typename T, int NV, int NF>
-DNDSB_GLOBAL void k_sgs_pos_blk(int64_t pBeg, int64_t pEnd, const int32_t *__restrict__ nbrPos, const T *__restrict__ opB, const T *__restrict__ jdB,
-                                const T *__restrict__ rhs, const T *__restrict__ xOld, T *xNew, int forward, int gsUpdate, int uIncIsZero)
+DNDSB_GLOBAL void k_sgs_pos_blk(int64_t n, int64_t pBeg, int64_t pEnd, const int32_t *__restrict__ nbrPos, const T *__restrict__ opB,
+                                const T *__restrict__ jdB, const T *__restrict__ rhs, const T *__restrict__ xOld, T *xNew, int forward, int gsUpdate,
+                                int uIncIsZero)
 {
+    constexpr int NN = NV * NV;
+    const ilu::BlockLay oL{NF * NN, 5}, dL{2 * NN, 5};
     DNDSB_KERNEL_LOOP(ii, pEnd - pBeg)
     {
         int64_t p = pBeg + ii;
-        T buf[NV], x[NV];
+        T buf[NV];
         for (int v = 0; v < NV; v++)
             buf[v] = rhs[p * NV + v];
 #pragma unroll
@@ -315,18 +396,24 @@ DNDSB_GLOBAL void k_sgs_pos_blk(int64_t pBeg, int64_t pEnd, const int32_t *__res
             if (uIncIsZero && !useNew)
                 continue;
             const T *dU = (useNew ? xNew : xOld) + (int64_t)q * NV;
-            const T *ob = opB + (p * NF + k) * NV * NV;
+            T xq[NV];
+            for (int l = 0; l < NV; l++)
+                xq[l] = dU[l];
             for (int r = 0; r < NV; r++)
             {
                 T acc = 0;
                 for (int l = 0; l < NV; l++)
-                    acc += ob[r * NV + l] * dU[l];
+                    acc += opB[oL.at(p, k * NN + r * NV + l)] * xq[l];
                 buf[r] -= acc;
             }
         }
-        roej::block_mul<NV>(jdB + p * 2 * NV * NV + NV * NV, buf, x);
-        for (int v = 0; v < NV; v++)
-            xNew[p * NV + v] = x[v];
+        for (int r = 0; r < NV; r++)
+        {
+            T acc = 0;
+            for (int l = 0; l < NV; l++)
+                acc += jdB[dL.at(p, NN + r * NV + l)] * buf[l];
+            xNew[p * NV + r] = acc;
+        }
     }
 }
 
@@ -334,24 +421,35 @@ template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_matvec_pos_blk(int64_t n, const int32_t *__restrict__ nbrPos, const T *__restrict__ opB, const T *__restrict__ jdB,
                                    const T *__restrict__ x, T *Ax, const real *__restrict__ xs)
 {
+    constexpr int NN = NV * NV;
+    const ilu::BlockLay oL{NF * NN, 5}, dL{2 * NN, 5};
     const T sx = xs ? (T)*xs : T(1);
     DNDSB_KERNEL_LOOP(p, n)
     {
-        T y[NV];
-        roej::block_mul<NV>(jdB + p * 2 * NV * NV, x + p * NV, y);
+        T xp[NV], y[NV];
+        for (int l = 0; l < NV; l++)
+            xp[l] = x[p * NV + l];
+        for (int r = 0; r < NV; r++)
+        {
+            T acc = 0;
+            for (int l = 0; l < NV; l++)
+                acc += jdB[dL.at(p, r * NV + l)] * xp[l];
+            y[r] = acc;
+        }
 #pragma unroll
         for (int k = 0; k < NF; k++)
         {
             int q = nbrPos[p * NF + k];
             if (q < 0)
                 continue;
-            const T *ob = opB + (p * NF + k) * NV * NV;
-            const T *xq = x + (int64_t)q * NV;
+            T xq[NV];
+            for (int l = 0; l < NV; l++)
+                xq[l] = x[(int64_t)q * NV + l];
             for (int r = 0; r < NV; r++)
             {
                 T acc = 0;
                 for (int l = 0; l < NV; l++)
-                    acc += ob[r * NV + l] * xq[l];
+                    acc += opB[oL.at(p, k * NN + r * NV + l)] * xq[l];
                 y[r] += acc;
             }
         }
@@ -544,10 +642,11 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv, int jac
               dev_alloc((void **)&w->s2, sizeof(real) * 8) == cudaSuccess &&
               dev_alloc((void **)&w->red, sizeof(real) * kRedBufLenK) == cudaSuccess &&
               dev_alloc((void **)&w->colScale, sizeof(real) * 33) == cudaSuccess && dev_alloc((void **)&w->cnt, sizeof(unsigned)) == cudaSuccess;
+    const int64_t nPad = ilu::padded_rows(m.nCell, 5); // the block arrays are tiled by 32 positions
     if (ok && jacMode)
-        ok = dev_alloc(&w->opB, es * nv * nv * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->jdB, es * 2 * nv * nv * m.nCell) == cudaSuccess;
+        ok = dev_alloc(&w->opB, es * nv * nv * nPad * m.nf) == cudaSuccess && dev_alloc(&w->jdB, es * 2 * nv * nv * nPad) == cudaSuccess;
     if (ok && jacMode && ls.jacobiCode == 2)
-        ok = dev_alloc(&w->luB, es * nv * nv * m.nCell * m.nf) == cudaSuccess && dev_alloc(&w->luD, es * nv * nv * m.nCell) == cudaSuccess &&
+        ok = dev_alloc(&w->luB, es * nv * nv * nPad * m.nf) == cudaSuccess && dev_alloc(&w->luD, es * nv * nv * nPad) == cudaSuccess &&
              dev_alloc(&w->tmp3, es * n) == cudaSuccess;
     ok = ok && dev_zero(w->V, es * krylov_ld(n) * (k + 1), nullptr) == cudaSuccess; // the column pads stay zero
     ok = ok && dev_zero(w->cnt, sizeof(unsigned), nullptr) == cudaSuccess && dev_zero(w->colScale, sizeof(real) * 33, nullptr) == cudaSuccess;
@@ -589,15 +688,16 @@ struct Solve
             auto kb = k_sgs_pos_blk<T, NV, NF>;
             if (!gs)
             {
-                DNDSB_LAUNCH(kb, m.nCell, 128, st, 0, m.nCell, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, rhs, xOld, xNew, (int)forward, 0,
-                             (int)zeroIn);
+                DNDSB_LAUNCH(kb, m.nCell, 128, st, m.nCell, 0, m.nCell, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, rhs, xOld, xNew, (int)forward,
+                             0, (int)zeroIn);
                 return;
             }
             for (int ci = 0; ci < m.nColor; ci++)
             {
                 int col = forward ? ci : m.nColor - 1 - ci;
                 int64_t b = m.colorStart[col], e = m.colorStart[col + 1];
-                DNDSB_LAUNCH(kb, e - b, 128, st, b, e, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, rhs, xOld, xNew, (int)forward, 1, (int)zeroIn);
+                DNDSB_LAUNCH(kb, e - b, 128, st, m.nCell, b, e, w.nbrPos, (const T *)w.opB, (const T *)w.jdB, rhs, xOld, xNew, (int)forward, 1,
+                             (int)zeroIn);
             }
             return;
         }
@@ -635,12 +735,13 @@ struct Solve
             }
             auto kl = ilu::k_ilu_lower<T, NV, NF>;
             auto ku = ilu::k_ilu_upper<T, NV, NF>;
+            const ilu::BlockLay lay{NF * NV * NV, 5}, dlay{NV * NV, 5};
             for (int ci = 0; ci < m.nColor; ci++)
                 DNDSB_LAUNCH(kl, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
-                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, zero ? rhs : (const T *)r, y);
+                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, lay, zero ? rhs : (const T *)r, y);
             for (int ci = m.nColor - 1; ci >= 0; ci--)
                 DNDSB_LAUNCH(ku, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
-                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, (const T *)w.luD, y);
+                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, lay, (const T *)w.luD, dlay, y);
             if (!zero)
                 DNDSB_LAUNCH(k_add_T<T>, nn, 256, st, nn, (const T *)r, x);
         }
@@ -755,15 +856,16 @@ int run(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs &
     {
         if (w.jacMode == 2 && (!ev.lambdaFace0 || (m.nBndFace > 0 && !bnd.type)))
             return ST_BADARG;
-        auto kb = k_sgsop_build_blk<T, NV>;
+        auto kb = k_sgsop_build_blk<T, NV, NF>;
         DNDSB_LAUNCH(kb, m.nCell, 128, cs, m, g, bnd, ev, (int)(w.jacMode == 2), dTau, dt, alphaDiag, u, w.cellPos, w.nbrPos, (T *)w.opB,
                      (T *)w.jdB, ev.errWord);
         if (ls.jacobiCode == 2) // LUSGSMatrixToJacobianLU + InPlaceDecompose, colour by colour
         {
             auto kf = ilu::k_ilu_factor<T, NV, NF>;
+            const ilu::BlockLay lay{NF * NV * NV, 5}, dlay{NV * NV, 5}, jlay{2 * NV * NV, 5};
             for (int ci = 0; ci < m.nColor; ci++)
                 DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, cs, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
-                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.opB, (const T *)w.jdB, (int64_t)2 * NV * NV, (T *)w.luB, (T *)w.luD,
+                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.opB, (const T *)w.jdB, lay, dlay, jlay, (T *)w.luB, (T *)w.luD,
                              ev.errWord);
         }
     }

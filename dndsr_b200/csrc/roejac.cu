@@ -200,9 +200,11 @@ template <int NV, int NF>
 void lu_factor_colors(const MeshD &m, EvalD &ev, const real *jd, cudaStream_t st)
 {
     auto kf = ilu::k_ilu_factor<real, NV, NF>;
+    constexpr int64_t NN = NV * NV;
     for (int ci = 0; ci < m.nColor; ci++)
         DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
-                     m.cellColor, (const real *)ev.luOff, jd, (int64_t)2 * NV * NV, ev.luOff, ev.luDinv, ev.errWord);
+                     m.cellColor, (const real *)ev.luOff, jd, ilu::BlockLay{NF * NN, 0}, ilu::BlockLay{NN, 0}, ilu::BlockLay{2 * NN, 0}, ev.luOff,
+                     ev.luDinv, ev.errWord);
 }
 
 template <int NV, int NF>
@@ -210,12 +212,14 @@ void lu_solve_colors(const MeshD &m, EvalD &ev, real *x, cudaStream_t st)
 {
     auto kl = ilu::k_ilu_lower<real, NV, NF>;
     auto ku = ilu::k_ilu_upper<real, NV, NF>;
+    constexpr int64_t NN = NV * NV;
+    const ilu::BlockLay offL{NF * NN, 0}, dL{NN, 0};
     for (int ci = 0; ci < m.nColor; ci++)
         DNDSB_LAUNCH(kl, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
-                     m.cellColor, (const real *)ev.luOff, (const real *)x, x);
+                     m.cellColor, (const real *)ev.luOff, offL, (const real *)x, x);
     for (int ci = m.nColor - 1; ci >= 0; ci--)
         DNDSB_LAUNCH(ku, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
-                     m.cellColor, (const real *)ev.luOff, (const real *)ev.luDinv, x);
+                     m.cellColor, (const real *)ev.luOff, offL, (const real *)ev.luDinv, dL, x);
 }
 
 template <int NV>
