@@ -244,3 +244,58 @@ def test_local_lu_driver_matches_oracle_driver():
     u = torch.tensor(np.tile(far, (m.n_cell, 1)), device="cuda")
     I.ImplicitSolver(vr, ev, I.SolverConfig(**kw)).run(u)
     assert relerr(u.cpu().numpy(), u_o.numpy()) < 1e-10
+
+
+@pytest.mark.parametrize("roe", [False, True])
+def test_sa_block_operators(roe):
+    """6 variables (the SA model, no-slip wall, far field): the block diagonal with the SA source Jacobian, with
+    and without the Roe term, its products and sweeps, the local LU and the native solve against the oracle."""
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    from tests.plate_case import plate_oracle, plate_perturbed
+    m = M.renumber_by_color(M.flat_plate_hex(12, 10, 3, y1=1e-3, growth=1.3))
+    o, far, mu, types, vals, w = plate_oracle(m, 1, "Roe", 5)
+    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1, intOrder=5)).construct(w)
+    ev = EulerEvaluator(vr, dict(nVars=6, riemannSolverType="Roe", muGas=mu, muModel=0, prGas=0.72))
+    ev.SetBC(types, vals)
+    ev.SetWallDistance(M.plate_wall_distance(vr.get("cellPP").reshape(m.n_cell, -1, 3)))
+    o.set_jacobian_mode(False, roe)
+    ev.SetJacobianMode(False, roe)
+    u0, uRec0 = plate_perturbed(m, far, R=o.R)
+    u, uRec = torch.tensor(u0, device="cuda"), torch.tensor(uRec0, device="cuda")
+    dt = torch.zeros(m.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dt, u, 5.0)
+    d0, _ = o.eval_dt(u0, 5.0)
+    rhs = torch.zeros_like(u)
+    ev.EvaluateRHS(rhs, u, uRec)
+    r0 = o.eval_rhs(u0, uRec0)
+    assert relerr(rhs.cpu().numpy(), r0) < TOL
+    if roe:
+        for nm in ("lambdaFace0", "lambdaFace123", "lambdaFace4"):
+            assert relerr(ev.get(nm), o.get(nm)) < TOL, nm
+    jd = ev.BuildJDiag()
+    assert jd.shape == (m.n_cell, 2, 6, 6)
+    ev.LUSGSMatrixInit(jd, dt, 0.1, 0.5, u)
+    jd0 = o.lusgs_init_block(d0, 0.1, 0.5, u0)
+    assert relerr(jd[:, 0].cpu().numpy(), jd0[:, 0]) < TOL
+    assert relerr(jd[:, 1].cpu().numpy(), jd0[:, 1]) < 1e-11
+    x0 = np.random.default_rng(2).normal(size=u0.shape)
+    x = torch.tensor(x0, device="cuda")
+    Ax = torch.zeros_like(u)
+    ev.LUSGSMatrixVec(0.5, u, x, jd, Ax)
+    assert relerr(Ax.cpu().numpy(), o.lusgs_matvec(0.5, u0, x0, jd0)) < TOL
+    out = torch.zeros_like(u)
+    ev.UpdateSGS(0.5, rhs, u, x, out, jd, True, True, False)
+    ref, _ = o.update_sgs(0.5, r0, u0, x0, np.zeros_like(x0), jd0, True, True, False)
+    assert relerr(out.cpu().numpy(), ref) < 1e-11
+    ev.LUSGSMatrixToJacobianLU(0.5, u, jd)
+    o.jacobian_lu(0.5, u0, jd0)
+    ev.LUSGSMatrixSolveJacobianLU(0.5, rhs, u, x, out, jd, False)
+    ref, _ = o.solve_jacobian_lu(0.5, r0, u0, x0, jd0, False)
+    assert relerr(out.cpu().numpy(), ref) < 1e-11
+    oe = OracleEval(o)
+    oe.SetJacobianMode(False, roe)
+    refx = _reference_solve(oe, torch.tensor(u0), torch.tensor(r0), torch.tensor(d0), 0.1, 0.5, 1, 0, 6, 1, 2)
+    for prec, tol in [("fp64", 1e-10), ("fp32", 1e-5)]:
+        xs = torch.zeros_like(u)
+        ev.SolveLinear(0.5, dt, 0.1, u, rhs, xs, gmresCode=1, nGmresSpace=6, jacobiCode=2, precision=prec)
+        assert relerr(xs.cpu().numpy(), refx.numpy()) < tol, prec
