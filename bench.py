@@ -304,6 +304,43 @@ def run_steady(args):
     return res
 
 
+def run_linear_solve(args):
+    """One native linear solve (dndsb_eval_solve_linear) on the steady bump at a perturbed free stream, CUDA events over
+    5 calls after 2: the scalar Jacobian with GMRES(30) and one SGS pair, the Roe Jacobian with GMRES(10) and the local
+    LU (block ILU(0)), each FP64 and FP32; 'build_factor_pair' is gmresCode 0 (the operator build, the ILU
+    factorisation and one preconditioner application)."""
+    import torch
+    nx, ny, nz = args.linear_mesh
+    mesh, vr, ev, far = _bump_c3(nx, ny, nz)
+    u = vr.BuildUDof(5)
+    u[:] = torch.tensor(far, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(1)
+    u[:, 0] *= 1 + 0.01 * torch.rand(mesh.n_cell, device="cuda", dtype=torch.float64, generator=g)
+    uRec = vr.BuildURec(5)
+    dt = torch.zeros(mesh.n_cell, dtype=torch.float64, device="cuda")
+    rhs = torch.zeros_like(u)
+    out = {"workload": f"steady bump, {mesh.n_cell} tets, VR degree 1, Roe_M2, local pseudo time step at CFL 1e4, dt = 1e100",
+           "cells": mesh.n_cell}
+    for mode, cases in (("scalar", ((1, 30, 1, "gmres30_sgs"),)), ("roe", ((1, 10, 2, "gmres10_ilu"), (0, 1, 2, "build_factor_pair")))):
+        ev.SetJacobianMode(mode == "scalar", mode == "roe")
+        ev.EvaluateDt(dt, u, 1e4)
+        ev.EvaluateRHS(rhs, u, uRec)
+        for code, k, jac, name in cases:
+            for prec in ("fp64", "fp32"):
+                x = torch.zeros_like(u)
+                for _ in range(2):
+                    ev.SolveLinear(1.0, dt, 1e100, u, rhs, x, gmresCode=code, nGmresSpace=k, jacobiCode=jac, precision=prec)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                for _ in range(5):
+                    ev.SolveLinear(1.0, dt, 1e100, u, rhs, x, gmresCode=code, nGmresSpace=k, jacobiCode=jac, precision=prec)
+                b.record()
+                torch.cuda.synchronize()
+                out[f"{mode}_{name}_{prec}_ms"] = a.elapsed_time(b) / 5
+    ev.SetJacobianMode(True, False)
+    return out
+
+
 def run_dual_time(args):
     """Wall time to a 1e-10 residual drop, mixed vs FP64, where the defect correction converges: one ESDIRK4
     step of the TGV workload (dt 0.02, local pseudo time step at CFL 50, GMRES(30) preconditioned by one SGS
@@ -836,6 +873,8 @@ def run_ours(args, rank, world, local_rank):
             line["time_to_1e-10"] = run_dual_time(args)
         if "steady" in blocks:
             line["steady"] = run_steady(args)
+        if "linear_solve" in blocks:
+            line["linear_solve"] = run_linear_solve(args)
         if "adjoint_cost" in blocks:
             line["adjoint_cost"] = run_adjoint_cost(args)
         if not args.no_sa and "sa_plate" in blocks:
@@ -870,10 +909,11 @@ def main():
     ap.add_argument("--steady-big-mesh", type=int, nargs=3, default=(160, 80, 26))
     ap.add_argument("--steady-big-iters", type=int, default=4000)
     ap.add_argument("--no-steady-roe", dest="steady_roe", action="store_false", help="skip the Roe-Jacobian steady runs")
+    ap.add_argument("--linear-mesh", type=int, nargs=3, default=(160, 80, 26))
     ap.add_argument("--adjoint-mesh", type=int, nargs=3, default=(80, 40, 13))
     ap.add_argument("--no-sa", action="store_true")
     # the extra measurement blocks after the headline, comma separated (a subset for profiling runs)
-    ap.add_argument("--blocks", default="time_to_1e-10,steady,adjoint_cost,sa_plate")
+    ap.add_argument("--blocks", default="time_to_1e-10,steady,linear_solve,adjoint_cost,sa_plate")
     ap.add_argument("--sa-mesh", type=int, nargs=3, default=(300, 100, 100))
     ap.add_argument("--sa-iters", type=int, default=30)
     args = ap.parse_args()

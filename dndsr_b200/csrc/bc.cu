@@ -82,6 +82,114 @@ DNDSB_GLOBAL void k_vr_bc(MeshD m, GeomD g, VRD vr, const TC *__restrict__ AAInv
     }
 }
 
+// DoReconstructionIter with SORInstead (VariationalReconstruction_Reconstruction.hxx:534-611): one colour class of an
+// in-place sweep, row_c = (1 - relax) row_c + relax sum over faces in cell2face order of A^-1 B_k uRec_o + A^-1 b_k (u_o - u_c)
+// (interior) or A^-1 GetBoundaryRHS (boundary, evaluated from the cell's partially updated row, as the reference's
+// in-place update reads it).  Cells of one colour are not adjacent, so a colour is one launch and the sweep equals the
+// reference's sequential one on a mesh numbered colour by colour.
+template <int DIM, int P, int NV>
+DNDSB_GLOBAL void k_vr_sor(MeshD m, GeomD g, VRD vr, int64_t cBeg, int64_t cEnd, real *uRec, const real *__restrict__ u, real relax)
+{
+    constexpr int NDOF = ndof_of<DIM>(P), R = NDOF - 1;
+    DNDSB_KERNEL_LOOP(ii, cEnd - cBeg)
+    {
+        int64_t c = m.colorCells[cBeg + ii];
+        const real *uc = u + c * NV;
+        real row[R * NV];
+        for (int i = 0; i < R * NV; i++)
+            row[i] = uRec[c * R * NV + i] * (1 - relax);
+        for (int k = 0; k < m.nf; k++)
+        {
+            int o = m.cellNbr[c * m.nf + k];
+            real t[R * NV];
+            if (o >= 0)
+            {
+                const real *M = vr.AAInvB + ((c * (m.nf + 1) + 1 + k) * R) * R;
+                const real *b = vr.AInvb + (c * m.nf + k) * R;
+                const real *ro = o == c ? row : uRec + (int64_t)o * R * NV; // a periodic image of itself: the current row
+                for (int i = 0; i < R; i++)
+                    for (int v = 0; v < NV; v++)
+                    {
+                        real acc = 0;
+                        for (int j = 0; j < R; j++)
+                            acc += M[i * R + j] * ro[j * NV + v];
+                        t[i * NV + v] = acc + b[i] * (u[(int64_t)o * NV + v] - uc[v]);
+                    }
+            }
+            else
+            {
+                int64_t f = m.cell2face[c * m.nf + k] >> 1;
+                real BCC[R * NV];
+                for (int i = 0; i < R * NV; i++)
+                    BCC[i] = 0;
+                real w0 = vr.faceWeight[f * (P + 1)];
+                int zone = m.faceZone[f];
+                if (w0 != 0)
+                    for (int q = 0; q < g.nGf; q++)
+                    {
+                        const real *p = &g.facePP[(f * g.nGf + q) * 3];
+                        const real *n = &g.faceNorm[(f * g.nGf + q) * 3];
+                        real T[NDOF];
+                        cell_basis<DIM, NDOF>(&g.cellCent[c * 3], &g.cellScale[c * 3], &vr.baseMoment[c * NDOF], vr.s.anisotropicLengths, p, 1, T);
+                        real UL[NV], ULf[NV], UB[NV];
+                        for (int v = 0; v < NV; v++)
+                        {
+                            real a = uc[v];
+                            for (int j = 0; j < R; j++)
+                                a += T[1 + j] * row[j * NV + v];
+                            UL[v] = a;
+                        }
+                        compress_rec<NV>(uc, UL, ULf);
+                        if (!bc_value_fix<NV>(vr.bnd, zone, ULf, n, UB))
+                            for (int v = 0; v < NV; v++)
+                                UB[v] = ULf[v];
+                        real JW = g.faceJDet[f * g.nGf + q] * g.faceQw[q] * w0 * w0;
+                        for (int i = 0; i < R; i++)
+                            for (int v = 0; v < NV; v++)
+                                BCC[i * NV + v] += T[1 + i] * (UB[v] - uc[v]) * JW;
+                    }
+                const real *Ai = vr.AAInvB + c * (m.nf + 1) * R * R;
+                for (int i = 0; i < R; i++)
+                    for (int v = 0; v < NV; v++)
+                    {
+                        real acc = 0;
+                        for (int j = 0; j < R; j++)
+                            acc += Ai[i * R + j] * BCC[j * NV + v];
+                        t[i * NV + v] = acc;
+                    }
+            }
+            for (int i = 0; i < R * NV; i++)
+                row[i] += relax * t[i];
+        }
+        for (int i = 0; i < R * NV; i++)
+            uRec[c * R * NV + i] = row[i];
+    }
+}
+
+template <int DIM, int NV>
+int vr_sor_p(const MeshD &m, const GeomD &g, const VRD &vr, real *uRec, const real *u, cudaStream_t st)
+{
+    for (int ci = 0; ci < m.nColor; ci++)
+    {
+        int64_t b = m.colorStart[ci], e = m.colorStart[ci + 1];
+        switch (vr.P)
+        {
+        case 1:
+            DNDSB_LAUNCH((k_vr_sor<DIM, 1, NV>), e - b, 64, st, m, g, vr, b, e, uRec, u, vr.s.jacobiRelax);
+            break;
+        case 2:
+            DNDSB_LAUNCH((k_vr_sor<DIM, 2, NV>), e - b, 64, st, m, g, vr, b, e, uRec, u, vr.s.jacobiRelax);
+            break;
+        case 3:
+            DNDSB_LAUNCH((k_vr_sor<DIM, 3, NV>), e - b, 64, st, m, g, vr, b, e, uRec, u, vr.s.jacobiRelax);
+            break;
+        default:
+            return ST_UNSUPPORTED;
+        }
+    }
+    return ST_OK;
+}
+
 // EulerEvaluator_EvaluateRHS.hxx:171-562 on a boundary face: ghost state at every Gauss
 // point, Roe means from the ghost of the cell mean at the face centre (:198-210), the inner
 // gradient on both sides (:360-362), GRP distance from the face centre (:363-386) and no
@@ -264,6 +372,20 @@ int vr_iter_bc(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real
     else if (nv == 6)
         rc = m.dim == 2 ? vr_bc_p<2, 6>(m, g, vr, uRec, uRecNew, u, recordInc, useFP32, st)
                         : vr_bc_p<3, 6>(m, g, vr, uRec, uRecNew, u, recordInc, useFP32, st);
+    if (rc != ST_OK)
+        return rc;
+    return last_error() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int vr_iter_sor(const MeshD &m, const GeomD &g, const VRD &vr, int nv, real *uRec, const real *u, cudaStream_t st)
+{
+    if (m.nBndFace > 0 && !vr.bnd.type)
+        return ST_BADARG;
+    int rc = ST_UNSUPPORTED;
+    if (nv == 5)
+        rc = m.dim == 2 ? vr_sor_p<2, 5>(m, g, vr, uRec, u, st) : vr_sor_p<3, 5>(m, g, vr, uRec, u, st);
+    else if (nv == 6)
+        rc = m.dim == 2 ? vr_sor_p<2, 6>(m, g, vr, uRec, u, st) : vr_sor_p<3, 6>(m, g, vr, uRec, u, st);
     if (rc != ST_OK)
         return rc;
     return last_error() == cudaSuccess ? ST_OK : ST_CUDA;

@@ -280,8 +280,6 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_vr_create: null argument");
         if (s->maxOrder < 1 || s->maxOrder > 3 || s->intOrder < 0 || s->intOrder > 6)
             return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_create: maxOrder must be 1..3 and intOrder 0..6");
-        if (s->SORInstead)
-            return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_create: SORInstead is not available; use the Jacobi sweep");
         auto *v = new dndsb_vr();
         v->mesh = mesh;
         VRSettingsD &d = v->vr.s;
@@ -416,6 +414,15 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: the mesh has boundary faces; set their boundary table first");
         if (v->vr.bnd.nZone > 0 && nVars != v->bndNVars)
             return fail(DNDSB_E_BADARG, "dndsb_vr_do_reconstruction_iter: nVars differs from the boundary table's");
+        if (v->vr.s.SORInstead && !recordInc) // _Reconstruction.hxx:534-611: in place on uRec, then swapped into uRecNew with putIntoNew
+        {
+            if (precision != 0)
+                return fail(DNDSB_E_UNSUPPORTED, "dndsb_vr_do_reconstruction_iter: the SOR sweep takes FP64 coefficients");
+            int rc = vr_iter_sor(v->mesh->d, v->g, v->vr, nVars, uRec, u, S(stream));
+            if (rc == ST_OK && putIntoNew)
+                rc = vr_swap(v->mesh->d.nCell * v->vr.R * nVars, uRec, uRecNew, S(stream));
+            return status_msg(rc, "dndsb_vr_do_reconstruction_iter");
+        }
         int rc = vr_iter(v->mesh->d, v->g, v->vr, nVars, uRec, uRecNew, u, recordInc, uRecIsZero, precision, S(stream));
         if (rc == ST_OK && !putIntoNew && !recordInc)
             rc = vr_swap(v->mesh->d.nCell * v->vr.R * nVars, uRec, uRecNew, S(stream));

@@ -254,6 +254,8 @@ real *reduce_cols(int op, int64_t n, int ncol, const real *x, const real *w, int
 // adds relax A^-1 BCC (GetBoundaryRHS) of every boundary cell to uRecNew
 int vr_iter_bc(const MeshD &m, const GeomD &g, const VRD &vr, int nv, const real *uRec, real *uRecNew, const real *u, int recordInc,
                int uRecIsZero, int useFP32, cudaStream_t st);
+// DoReconstructionIter with SORInstead: one in-place sweep of uRec, colour by colour (5 or 6 variables, FP64 coefficients)
+int vr_iter_sor(const MeshD &m, const GeomD &g, const VRD &vr, int nv, real *uRec, const real *u, cudaStream_t st);
 // writes the face flux of every boundary face
 // uRecG: the reconstruction of the inner gradients (uRecUnlim)
 int rhs_bc(const MeshD &m, const GeomD &g, const VRD &vr, const EvalD &ev, const real *u, const real *uRec, const real *uRecG, real *ff,

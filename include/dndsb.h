@@ -119,7 +119,13 @@ int dndsb_vr_get_array(const dndsb_vr *vr, const char *name, double *hostOut, in
 /* DoReconstructionIter(uRec, uRecNew, u, FBoundary, putIntoNew, recordInc, uRecIsZero),
  * VariationalReconstruction_Reconstruction.hxx:485-615 (Jacobi sweep).
  * putIntoNew = 0 swaps the contents of uRec and uRecNew afterwards, like the reference.
- * precision: 0 FP64 coefficients, 1 FP32 coefficients (FP64 state and accumulation). */
+ * precision: 0 FP64 coefficients, 1 FP32 coefficients (FP64 state and accumulation).
+ * With SORInstead (VRSettings.hpp:43; the reference's default) and without recordInc the sweep is the
+ * reference's in-place SOR (:534-611): uRec is updated in place colour by colour (equal to the reference's
+ * sequential sweep on a mesh numbered colour by colour), a boundary face's term taken from the cell's
+ * partially updated row as the reference's in-place update reads it; putIntoNew = 1 then swaps the contents
+ * so that the result is in uRecNew; FP64 coefficients only.  The sweep derivatives below are those of the
+ * Jacobi sweep, as the reference's DoReconstructionIterDiff. */
 int dndsb_vr_do_reconstruction_iter(dndsb_vr *vr, double *uRec, double *uRecNew, const double *u, int nVars, int putIntoNew,
                                     int recordInc, int uRecIsZero, int precision, void *stream);
 

@@ -121,6 +121,7 @@ def _declare(L):
     L.orc_eval_rhs_full.argtypes = [_V, _D, _D, _D, _D, _D, _D, _D]
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_set_jacobian_mode.argtypes = [_V, ctypes.c_int]
+    L.orc_vr_iter_sor.argtypes = [_V, _D, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
     L.orc_jacobian_lu.restype = ctypes.c_int
     L.orc_solve_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
@@ -304,6 +305,12 @@ class Oracle:
         uRec, u = _f64(uRec), _f64(u)
         out = np.zeros_like(uRec)
         self.L.orc_vr_iter(self.h, _p(uRec), _p(out), _p(u), int(recordInc), int(uRecIsZero))
+        return out
+
+    def vr_iter_sor(self, uRec, u):
+        """One SOR sweep (SORInstead) from uRec, in natural cell order; returns the new uRec."""
+        out = np.array(uRec, dtype=np.float64, copy=True, order="C")
+        self.L.orc_vr_iter_sor(self.h, _p(out), _p(_f64(u)))
         return out
 
     def eval_dt(self, u, CFL, MaxDt=1e100, useLocalDt=True):

@@ -1651,6 +1651,56 @@ struct Oracle
         }
     }
 
+    // DoReconstructionIter with SORInstead (VariationalReconstruction_Reconstruction.hxx:534-611, not recordInc): uRec is
+    // updated in place in natural cell order, row_c = (1 - relax) row_c + relax sum_k (A^-1 B_k uRec_o + A^-1 b_k (u_o - u_c))
+    // with the neighbours' current rows; a boundary face's GetBoundaryRHS reads the cell's partially updated row, since the
+    // reference adds each face's term to uRec[iCell] as it goes
+    void vrIterSOR(real *uRec, const real *u) const
+    {
+        int nv = es.nVars;
+        real relax = vs.jacobiRelax;
+        std::vector<real> t(R * nv), BCC(R * nv);
+        for (long c = 0; c < nCell; c++)
+        {
+            real *row = uRec + c * R * nv;
+            for (int i = 0; i < R * nv; i++)
+                row[i] *= 1 - relax;
+            for (int k = 0; k < nf; k++)
+            {
+                long f = cell2face[c * nf + k];
+                long o = otherOf(c, f);
+                if (o < 0)
+                {
+                    boundaryRHS(c, f, uRec, u, BCC.data());
+                    const real *Ai = &AAInvB[(c * (nf + 1)) * R * R];
+                    for (int i = 0; i < R; i++)
+                        for (int v = 0; v < nv; v++)
+                        {
+                            real acc = 0;
+                            for (int j = 0; j < R; j++)
+                                acc += Ai[i * R + j] * BCC[j * nv + v];
+                            t[i * nv + v] = acc;
+                        }
+                }
+                else
+                {
+                    const real *M = &AAInvB[(c * (nf + 1) + 1 + k) * R * R];
+                    const real *b = &AInvb[(c * nf + k) * R];
+                    for (int i = 0; i < R; i++)
+                        for (int v = 0; v < nv; v++)
+                        {
+                            real acc = 0;
+                            for (int j = 0; j < R; j++)
+                                acc += M[i * R + j] * uRec[(o * R + j) * nv + v];
+                            t[i * nv + v] = acc + b[i] * (u[o * nv + v] - u[c * nv + v]);
+                        }
+                }
+                for (int i = 0; i < R * nv; i++)
+                    row[i] += relax * t[i];
+            }
+        }
+    }
+
     // EulerEvaluator.hpp:751-789 muEff
     real muEff(const real *U, real T) const
     {
@@ -3090,6 +3140,9 @@ extern "C"
     {
         ((Oracle *)h)->vrIterJacobi(uRec, uRecNew, u, recordInc, uRecIsZero);
     }
+
+    // one SOR sweep in place (SORInstead)
+    void orc_vr_iter_sor(void *h, double *uRec, const double *u) { ((Oracle *)h)->vrIterSOR(uRec, u); }
 
     void orc_eval_dt(void *h, const double *u, double CFL, double MaxDt, int useLocalDt, double *dt, double *dtMin)
     {
