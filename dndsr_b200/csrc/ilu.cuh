@@ -62,12 +62,17 @@ DNDSB_HD void store(const real *v, T *dst, BlockLay L, int64_t r, int e0)
         dst[L.at(r, e0 + i)] = (T)v[i];
 }
 
-// one row of the factorisation: A (the operator's slot blocks) and D (diagonal blocks) in, off / dinv out
+// one row of the factorisation: A (the operator's slot blocks) and D (diagonal blocks) in, off / dinv out.
+// cnbr (may be nullptr): compact slot order for the factors — slot j < cnlow[r] holds the j-th lower neighbour in
+// ascending rank, the upper neighbours follow, cnbr [r][NF] their rows (-1 after the last); the triangular solves
+// then read the lower (or upper) blocks of a row from consecutive slots, so the threads of a warp load the same
+// slots.  Without it the factors keep the operator's slot order.
 template <typename T, int NV, int NF>
 DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, const T *A, const T *D, BlockLay offL, BlockLay dL, BlockLay DL,
-                         T *off, T *dinv)
+                         T *off, T *dinv, int32_t *cnbr = nullptr, int32_t *cnlow = nullptr)
 {
     constexpr int NN = NV * NV;
+    const int32_t *fnbr = cnbr ? cnbr : nbr; // the slot lists of the factored rows
     auto rk = [&](int64_t x) { return rank ? (int64_t)rank[x] : x; };
     const int64_t rr = rk(r);
     int low[NF], nLow = 0, upp[NF], nUpp = 0;
@@ -96,7 +101,7 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
         for (int b = 0; b < a; b++)
         {
             int64_t k = nbr[r * NF + low[b]];
-            int s = slot_of<NF>(nbr, k, j);
+            int s = slot_of<NF>(fnbr, k, j);
             if (s >= 0)
             {
                 real Ukj[NN];
@@ -117,7 +122,7 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
     for (int b = 0; b < nLow; b++)
     {
         int64_t k = nbr[r * NF + low[b]];
-        int s = slot_of<NF>(nbr, k, r);
+        int s = slot_of<NF>(fnbr, k, r);
         if (s >= 0)
         {
             real Uki[NN];
@@ -138,7 +143,7 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
         for (int b = 0; b < nLow; b++)
         {
             int64_t k = nbr[r * NF + low[b]];
-            int s = slot_of<NF>(nbr, k, j);
+            int s = slot_of<NF>(fnbr, k, j);
             if (s >= 0)
             {
                 real Ukj[NN];
@@ -146,14 +151,23 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
                 mul_sub<NV>(L + b * NN, Ukj, Uij);
             }
         }
-        store<T, NV>(Uij, off, offL, r, upp[a] * NN);
+        store<T, NV>(Uij, off, offL, r, (cnbr ? nLow + a : upp[a]) * NN);
     }
     for (int a = 0; a < nLow; a++)
-        store<T, NV>(L + a * NN, off, offL, r, low[a] * NN);
-    // slots without a neighbour (boundary faces) and a row's periodic image of itself carry nothing
+        store<T, NV>(L + a * NN, off, offL, r, (cnbr ? a : low[a]) * NN);
     real zero[NN];
     for (int i = 0; i < NN; i++)
         zero[i] = 0;
+    if (cnbr)
+    {
+        for (int j = 0; j < NF; j++)
+            cnbr[r * NF + j] = j < nLow ? nbr[r * NF + low[j]] : (j < nLow + nUpp ? nbr[r * NF + upp[j - nLow]] : -1);
+        cnlow[r] = nLow;
+        for (int j = nLow + nUpp; j < NF; j++)
+            store<T, NV>(zero, off, offL, r, j * NN);
+        return ok;
+    }
+    // slots without a neighbour (boundary faces) and a row's periodic image of itself carry nothing
     for (int k = 0; k < NF; k++)
     {
         int64_t q = nbr[r * NF + k];
@@ -167,13 +181,90 @@ DNDSB_HD bool factor_row(int64_t r, const int32_t *nbr, const int32_t *rank, con
 template <typename T, int NV, int NF>
 DNDSB_GLOBAL void k_ilu_factor(int64_t beg, int64_t end, const int32_t *__restrict__ rows, const int32_t *__restrict__ nbr,
                                const int32_t *__restrict__ rank, const T *A, const T *__restrict__ D, BlockLay offL, BlockLay dL, BlockLay DL,
-                               T *off, T *dinv, int *err) // A may be off (factored in place)
+                               T *off, T *dinv, int *err, int32_t *cnbr, int32_t *cnlow) // A may be off (factored in place)
 {
     DNDSB_KERNEL_LOOP(ii, end - beg)
     {
         int64_t r = rows ? (int64_t)rows[beg + ii] : beg + ii;
-        if (!factor_row<T, NV, NF>(r, nbr, rank, A, D, offL, dL, DL, off, dinv))
+        if (!factor_row<T, NV, NF>(r, nbr, rank, A, D, offL, dL, DL, off, dinv, cnbr, cnlow))
             atomicOr(err, (int)DE_SINGULAR);
+    }
+}
+
+// the triangular solves on compact factors (cnbr / cnlow of factor_row), rows [beg, end) of one colour:
+// forward y_r = b_r - sum_{j < nLow} L_j y_q; backward x_r = dinv_r (y_r - sum_{j >= nLow} U_j x_q), in place
+template <typename T, int NV, int NF>
+DNDSB_GLOBAL void k_ilu_lower_c(int64_t beg, int64_t end, const int32_t *__restrict__ cnbr, const int32_t *__restrict__ cnlow,
+                                const T *__restrict__ off, BlockLay offL, const T *b, T *x) // b may be x
+{
+    constexpr int NN = NV * NV;
+    DNDSB_KERNEL_LOOP(ii, end - beg)
+    {
+        int64_t r = beg + ii;
+        T acc[NV];
+        for (int v = 0; v < NV; v++)
+            acc[v] = b[r * NV + v];
+        const int nl = cnlow[r];
+#pragma unroll
+        for (int j = 0; j < NF; j++)
+        {
+            if (j >= nl)
+                break;
+            int64_t q = cnbr[r * NF + j];
+            T xq[NV];
+            for (int l = 0; l < NV; l++)
+                xq[l] = x[q * NV + l];
+            for (int i = 0; i < NV; i++)
+            {
+                T s = 0;
+                for (int l = 0; l < NV; l++)
+                    s += off[offL.at(r, j * NN + i * NV + l)] * xq[l];
+                acc[i] -= s;
+            }
+        }
+        for (int v = 0; v < NV; v++)
+            x[r * NV + v] = acc[v];
+    }
+}
+
+template <typename T, int NV, int NF>
+DNDSB_GLOBAL void k_ilu_upper_c(int64_t beg, int64_t end, const int32_t *__restrict__ cnbr, const int32_t *__restrict__ cnlow,
+                                const T *__restrict__ off, BlockLay offL, const T *__restrict__ dinv, BlockLay dL, T *x)
+{
+    constexpr int NN = NV * NV;
+    DNDSB_KERNEL_LOOP(ii, end - beg)
+    {
+        int64_t r = beg + ii;
+        T acc[NV];
+        for (int v = 0; v < NV; v++)
+            acc[v] = x[r * NV + v];
+        const int nl = cnlow[r];
+#pragma unroll
+        for (int j = 0; j < NF; j++)
+        {
+            if (j < nl)
+                continue;
+            int64_t q = cnbr[r * NF + j];
+            if (q < 0)
+                break;
+            T xq[NV];
+            for (int l = 0; l < NV; l++)
+                xq[l] = x[q * NV + l];
+            for (int i = 0; i < NV; i++)
+            {
+                T s = 0;
+                for (int l = 0; l < NV; l++)
+                    s += off[offL.at(r, j * NN + i * NV + l)] * xq[l];
+                acc[i] -= s;
+            }
+        }
+        for (int i = 0; i < NV; i++)
+        {
+            T s = 0;
+            for (int l = 0; l < NV; l++)
+                s += dinv[dL.at(r, i * NV + l)] * acc[l];
+            x[r * NV + i] = s;
+        }
     }
 }
 

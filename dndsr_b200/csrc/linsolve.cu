@@ -583,6 +583,7 @@ struct LinWs
     real *H = nullptr, *sc = nullptr, *s2 = nullptr, *red = nullptr;
     void *opB = nullptr, *jdB = nullptr; // block mode: off-diagonal blocks [nCell][nf][nv][nv], diagonal blocks + inverses [nCell][2][nv][nv]
     void *luB = nullptr, *luD = nullptr, *tmp3 = nullptr; // jacobiCode 2: ILU(0) slot blocks, inverted pivots, scratch
+    int32_t *luNbr = nullptr, *luNLow = nullptr;          // the factors' compact slot order: neighbour positions, lower count
     real *colScale = nullptr; // [33] normalising factors of the stored (unnormalised) Krylov columns
     unsigned *cnt = nullptr;  // ticket counter of the one-launch reductions (zero between launches)
     cudaStream_t cs = nullptr;
@@ -596,7 +597,8 @@ void linws_free(LinWs *w)
 {
     if (!w)
         return;
-    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->opB, w->jdB, w->luB, w->luD, w->tmp3, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
+    for (void *p : {(void *)w->cellPos, (void *)w->nbrPos, w->op, w->jd, w->opB, w->jdB, w->luB, w->luD, w->tmp3, (void *)w->luNbr,
+                    (void *)w->luNLow, w->uT, w->rhsT, w->x, w->tmp, w->tmp2, w->MLb, w->V, (void *)w->H,
                     (void *)w->sc, (void *)w->s2, (void *)w->red, (void *)w->colScale, (void *)w->cnt})
         dev_free(p);
     graph_free(w->graph);
@@ -647,7 +649,8 @@ int ws_prepare(const MeshD &m, LinWs *&w, const LinSettings &ls, int nv, int jac
         ok = dev_alloc(&w->opB, es * nv * nv * nPad * m.nf) == cudaSuccess && dev_alloc(&w->jdB, es * 2 * nv * nv * nPad) == cudaSuccess;
     if (ok && jacMode && ls.jacobiCode == 2)
         ok = dev_alloc(&w->luB, es * nv * nv * nPad * m.nf) == cudaSuccess && dev_alloc(&w->luD, es * nv * nv * nPad) == cudaSuccess &&
-             dev_alloc(&w->tmp3, es * n) == cudaSuccess;
+             dev_alloc(&w->tmp3, es * n) == cudaSuccess && dev_alloc((void **)&w->luNbr, sizeof(int32_t) * m.nCell * m.nf) == cudaSuccess &&
+             dev_alloc((void **)&w->luNLow, sizeof(int32_t) * m.nCell) == cudaSuccess;
     ok = ok && dev_zero(w->V, es * krylov_ld(n) * (k + 1), nullptr) == cudaSuccess; // the column pads stay zero
     ok = ok && dev_zero(w->cnt, sizeof(unsigned), nullptr) == cudaSuccess && dev_zero(w->colScale, sizeof(real) * 33, nullptr) == cudaSuccess;
     if (!ok || stream_create(&w->cs) != cudaSuccess || event_create(&w->evIn) != cudaSuccess || event_create(&w->evOut) != cudaSuccess)
@@ -733,15 +736,15 @@ struct Solve
                 FA(x, ax);
                 DNDSB_LAUNCH(k_sub_T<T>, nn, 256, st, nn, rhs, (const T *)ax, r);
             }
-            auto kl = ilu::k_ilu_lower<T, NV, NF>;
-            auto ku = ilu::k_ilu_upper<T, NV, NF>;
+            auto kl = ilu::k_ilu_lower_c<T, NV, NF>;
+            auto ku = ilu::k_ilu_upper_c<T, NV, NF>;
             const ilu::BlockLay lay{NF * NV * NV, 5}, dlay{NV * NV, 5};
             for (int ci = 0; ci < m.nColor; ci++)
-                DNDSB_LAUNCH(kl, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
-                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, lay, zero ? rhs : (const T *)r, y);
+                DNDSB_LAUNCH(kl, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)w.luNbr,
+                             (const int32_t *)w.luNLow, (const T *)w.luB, lay, zero ? rhs : (const T *)r, y);
             for (int ci = m.nColor - 1; ci >= 0; ci--)
-                DNDSB_LAUNCH(ku, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
-                             w.nbrPos, (const int32_t *)nullptr, (const T *)w.luB, lay, (const T *)w.luD, dlay, y);
+                DNDSB_LAUNCH(ku, m.colorStart[ci + 1] - m.colorStart[ci], 128, st, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)w.luNbr,
+                             (const int32_t *)w.luNLow, (const T *)w.luB, lay, (const T *)w.luD, dlay, y);
             if (!zero)
                 DNDSB_LAUNCH(k_add_T<T>, nn, 256, st, nn, (const T *)r, x);
         }
@@ -866,7 +869,7 @@ int run(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs &
             for (int ci = 0; ci < m.nColor; ci++)
                 DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, cs, m.colorStart[ci], m.colorStart[ci + 1], (const int32_t *)nullptr,
                              w.nbrPos, (const int32_t *)nullptr, (const T *)w.opB, (const T *)w.jdB, lay, dlay, jlay, (T *)w.luB, (T *)w.luD,
-                             ev.errWord);
+                             ev.errWord, w.luNbr, w.luNLow);
         }
     }
     else

@@ -204,7 +204,7 @@ void lu_factor_colors(const MeshD &m, EvalD &ev, const real *jd, cudaStream_t st
     for (int ci = 0; ci < m.nColor; ci++)
         DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
                      m.cellColor, (const real *)ev.luOff, jd, ilu::BlockLay{NF * NN, 0}, ilu::BlockLay{NN, 0}, ilu::BlockLay{2 * NN, 0}, ev.luOff,
-                     ev.luDinv, ev.errWord);
+                     ev.luDinv, ev.errWord, (int32_t *)nullptr, (int32_t *)nullptr);
 }
 
 template <int NV, int NF>
