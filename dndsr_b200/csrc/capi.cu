@@ -602,7 +602,7 @@ extern "C"
                         (void *)e->e.deltaLambdaFace, (void *)e->e.deltaLambdaCell, (void *)e->e.faceFlux, (void *)e->e.redBuf, (void *)e->e.errWord,
                         (void *)e->e.facePt, (void *)e->e.cellPar, (void *)e->e.adjBuf, (void *)e->e.dWall, (void *)e->e.jSource,
                         (void *)e->e.errDeferred, (void *)e->e.fluxWall, (void *)e->e.objDir, (void *)e->e.lambdaFace0, (void *)e->e.luOff,
-                        (void *)e->e.luDinv})
+                        (void *)e->e.luDinv, (void *)e->e.luDiag})
             dev_free(p);
         linws_free(e->lin);
         delete e;
@@ -840,8 +840,6 @@ extern "C"
     {
         if (!e || !u || !jdiag)
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_to_jacobian_lu: null argument");
-        if (e->e.jacMode == 0)
-            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_to_jacobian_lu: the local LU takes the block Jacobian");
         int rc = jacobian_lu(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, u, jdiag, S(stream));
         if (rc == ST_NONFINITE)
             return fail(DNDSB_E_NONFINITE, "dndsb_eval_lusgs_matrix_to_jacobian_lu: singular pivot block");
@@ -855,8 +853,8 @@ extern "C"
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: null argument");
         if (uInc == uIncNew || rhs == uIncNew) // EulerEvaluator.hxx:919
             return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: uIncNew must differ from uInc and rhs");
-        if (e->e.jacMode == 0 || !e->e.luOff)
-            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: build the local LU first (block Jacobian)");
+        if (!e->e.luOff)
+            return fail(DNDSB_E_BADARG, "dndsb_eval_lusgs_matrix_solve_jacobian_lu: build the local LU first (lusgs_matrix_to_jacobian_lu)");
         return status_msg(solve_jacobian_lu(e->vr->mesh->d, e->vr->g, e->e, alphaDiag, rhs, u, uInc, uIncNew, jdiag, uIncIsZero, sumIncHost,
                                             S(stream)),
                           "dndsb_eval_lusgs_matrix_solve_jacobian_lu");
@@ -1053,8 +1051,7 @@ extern "C"
         }
         int rc = linear_solve(e->vr->mesh->d, e->vr->g, e->vr->vr.bnd, e->e, e->lin, s, alphaDiag, dTau, dt, u, rhs, xInc, S(stream));
         if (rc == ST_BADARG)
-            return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..2 (2 with the block Jacobian), nGmresSpace 1..32, "
-                                        "precision 0..1");
+            return fail(DNDSB_E_BADARG, "dndsb_eval_solve_linear: gmresCode 0..2, jacobiCode 0..2, nGmresSpace 1..32, precision 0..1");
         return status_msg(rc, "dndsb_eval_solve_linear");
     }
 

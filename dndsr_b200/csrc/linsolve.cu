@@ -21,10 +21,11 @@
 // both cases.  Reductions use a fixed partition and fixed trees, so results
 // are bitwise reproducible.
 //
-// jacobiCode 2 (block mode): the preconditioner is the reference's local LU (LUSGSMatrixToJacobianLU +
+// jacobiCode 2: the preconditioner is the reference's local LU (LUSGSMatrixToJacobianLU +
 // LUSGSMatrixSolveJacobianLU, EulerEvaluator.hxx:290-359, 838-927; doPrecondition EulerSolver.hxx:1642-1657) with
 // iluCode 0: a block ILU(0) of the operator factored colour by colour (ilu.cuh) once per solve, applied as two
-// defect-correction steps x += (LU)^-1 (b - A x).
+// defect-correction steps x += (LU)^-1 (b - A x).  With the scalar Jacobian the operator is kept in block form
+// (the scalar diagonal and the scalar flux increments as blocks) for it.
 //
 // Block mode (useScalarJacobian false, optionally useRoeJacobian): the operator is kept as dense blocks,
 // per position the diagonal block and its inverse, per (position, face slot) the off-diagonal block
@@ -932,13 +933,15 @@ int run_nf(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinW
 int linear_solve(const MeshD &m, const GeomD &g, const BoundaryD &bnd, EvalD &ev, LinWs *&ws, const LinSettings &ls, real alphaDiag,
                  const real *dTau, real dt, const real *u, const real *rhs, real *xInc, cudaStream_t st)
 {
-    if (ls.jacobiCode == 2 && ev.jacMode == 0) // the local LU takes the block Jacobian
-        return ST_BADARG;
     if (ls.gmresCode < 0 || ls.gmresCode > 2 || ls.jacobiCode < 0 || ls.jacobiCode > 2 || ls.sgsIter < 0 || ls.nGmresIter < 0 ||
         (ls.gmresCode && (ls.nGmresSpace < 1 || ls.nGmresSpace > 32)) || ls.precision < 0 || ls.precision > 1)
         return ST_BADARG;
     int nv = ev.s.nVars;
-    int rc = ws_prepare(m, ws, ls, nv, ev.jacMode);
+    // the local LU works on blocks: with the scalar Jacobian its diagonal blocks are the scalar diagonal and the
+    // neighbour blocks the scalar form of the flux increment (LUSGSMatrixToJacobianLU takes JDiag.getValue), which is
+    // the block operator without the Roe term
+    const int mode = ev.jacMode ? ev.jacMode : (ls.jacobiCode == 2 ? 1 : 0);
+    int rc = ws_prepare(m, ws, ls, nv, mode);
     if (rc != ST_OK)
         return rc;
     if (nv == 5)

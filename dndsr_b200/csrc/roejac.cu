@@ -180,6 +180,18 @@ DNDSB_GLOBAL void k_lu_assemble(MeshD m, GeomD g, EvalD ev, int roe, real alphaD
     }
 }
 
+// the scalar Jacobian's diagonal (one value, or one per variable) as diagonal blocks
+template <int NV>
+DNDSB_GLOBAL void k_diag_blocks(int64_t nCell, const real *__restrict__ jd, int nd, real *out)
+{
+    DNDSB_KERNEL_LOOP(c, nCell)
+    {
+        for (int i = 0; i < NV; i++)
+            for (int j = 0; j < NV; j++)
+                out[c * NV * NV + i * NV + j] = i == j ? jd[c * nd + (nd > 1 ? i : 0)] : 0.0;
+    }
+}
+
 DNDSB_GLOBAL void k_sub(int64_t n, const real *__restrict__ a, const real *__restrict__ b, real *c)
 {
     DNDSB_KERNEL_LOOP(i, n)
@@ -196,15 +208,17 @@ DNDSB_GLOBAL void k_abs_add(int64_t n, const real *x, real *absOut, const real *
     }
 }
 
+// jd: the block jdiag [nCell][2][NV][NV], or (scalar Jacobian) ev.luDiag [nCell][NV][NV]
 template <int NV, int NF>
 void lu_factor_colors(const MeshD &m, EvalD &ev, const real *jd, cudaStream_t st)
 {
     auto kf = ilu::k_ilu_factor<real, NV, NF>;
     constexpr int64_t NN = NV * NV;
+    const ilu::BlockLay DL{ev.jacMode ? 2 * NN : NN, 0};
     for (int ci = 0; ci < m.nColor; ci++)
         DNDSB_LAUNCH(kf, m.colorStart[ci + 1] - m.colorStart[ci], 64, st, m.colorStart[ci], m.colorStart[ci + 1], m.colorCells, m.cellNbr,
-                     m.cellColor, (const real *)ev.luOff, jd, ilu::BlockLay{NF * NN, 0}, ilu::BlockLay{NN, 0}, ilu::BlockLay{2 * NN, 0}, ev.luOff,
-                     ev.luDinv, ev.errWord, (int32_t *)nullptr, (int32_t *)nullptr);
+                     m.cellColor, (const real *)ev.luOff, jd, ilu::BlockLay{NF * NN, 0}, ilu::BlockLay{NN, 0}, DL, ev.luOff, ev.luDinv, ev.errWord,
+                     (int32_t *)nullptr, (int32_t *)nullptr);
 }
 
 template <int NV, int NF>
@@ -244,8 +258,6 @@ int lu_dispatch(const MeshD &m, EvalD &ev, const real *jd, real *x, bool factor,
 int jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *jd, cudaStream_t st)
 {
     int nv = ev.s.nVars;
-    if (ev.jacMode == 0)
-        return ST_BADARG;
     if (ev.jacMode == 2 && !ev.lambdaFace0)
         return ST_BADARG;
     if (nv != 5 && nv != 6)
@@ -253,6 +265,16 @@ int jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const
     if (!ev.luOff && (dev_alloc((void **)&ev.luOff, sizeof(real) * nv * nv * m.nCell * m.nf) != cudaSuccess ||
                       dev_alloc((void **)&ev.luDinv, sizeof(real) * nv * nv * m.nCell) != cudaSuccess))
         return ST_CUDA;
+    if (ev.jacMode == 0) // JDiag.getValue of the scalar Jacobian: its diagonal as blocks
+    {
+        if (!ev.luDiag && dev_alloc((void **)&ev.luDiag, sizeof(real) * nv * nv * m.nCell) != cudaSuccess)
+            return ST_CUDA;
+        if (nv == 5)
+            DNDSB_LAUNCH(k_diag_blocks<5>, m.nCell, 256, st, m.nCell, jd, 1, ev.luDiag);
+        else
+            DNDSB_LAUNCH(k_diag_blocks<6>, m.nCell, 256, st, m.nCell, jd, 6, ev.luDiag);
+        jd = ev.luDiag;
+    }
     cudaMemsetAsync(ev.errWord, 0, sizeof(int), st);
     int roe = ev.jacMode == 2;
     if (nv == 5)
@@ -275,7 +297,7 @@ int solve_jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag,
                       const real *jd, int uIncIsZero, real *sumIncHost, cudaStream_t st)
 {
     int nv = ev.s.nVars;
-    if (!ev.luOff || ev.jacMode == 0)
+    if (!ev.luOff)
         return ST_BADARG;
     int64_t n = m.nCell * nv;
     if (uIncIsZero)
@@ -283,7 +305,7 @@ int solve_jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag,
     else
     {
         real *ax = ev.faceFlux; // [nCell][nv] fits in the [nFace][nv] scratch
-        int rc = lusgs_matvec_block(m, g, ev, alphaDiag, u, uInc, jd, ax, st);
+        int rc = ev.jacMode ? lusgs_matvec_block(m, g, ev, alphaDiag, u, uInc, jd, ax, st) : lusgs_matvec(m, g, ev, alphaDiag, u, uInc, jd, ax, st);
         if (rc != ST_OK)
             return rc;
         DNDSB_LAUNCH(k_sub, n, 256, st, n, rhs, (const real *)ax, uIncNew);

@@ -165,6 +165,7 @@ struct EvalD
     // the local LU of LUSGSMatrixToJacobianLU (allocated on first use): slot blocks L / U [nCell][nf][nv][nv],
     // inverted pivots [nCell][nv][nv]
     real *luOff = nullptr, *luDinv = nullptr;
+    real *luDiag = nullptr; // with the scalar Jacobian: its diagonal as blocks [nCell][nv][nv] (JDiag.getValue)
 };
 
 // EvaluateRHS flags (EulerEvaluator.hpp:370-378 RHS_* values)
@@ -208,7 +209,7 @@ int update_lusgs_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag
 int lusgs_matvec_block(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *uInc, const real *jd, real *AuInc,
                        cudaStream_t st);
 // LUSGSMatrixToJacobianLU + decomposition (block ILU(0), colour by colour) into ev.luOff / ev.luDinv, and
-// LUSGSMatrixSolveJacobianLU with it (roejac.cu); block mode only
+// LUSGSMatrixSolveJacobianLU with it (roejac.cu); jd in the layout of the evaluator's Jacobian mode
 int jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *u, const real *jd, cudaStream_t st);
 int solve_jacobian_lu(const MeshD &m, const GeomD &g, EvalD &ev, real alphaDiag, const real *rhs, const real *u, const real *uInc, real *uIncNew,
                       const real *jd, int uIncIsZero, real *sumIncHost, cudaStream_t st);

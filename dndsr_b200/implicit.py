@@ -199,7 +199,7 @@ class SolverConfig:
     nGmresIterRec: int = 1
     recThreshold: float = 1e-10
     gmresRecScale: int = 0
-    jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi, 2: the local LU (block ILU(0); block Jacobian)
+    jacobiCode: int = 1              # 1: Gauss-Seidel sweeps, 0: Jacobi, 2: the local LU (block ILU(0))
     sgsIter: int = 0
     gmresCode: int = 0               # 0: LU-SGS only, 1: GMRES preconditioned by SGS
     nGmresSpace: int = 30

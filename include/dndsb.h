@@ -233,7 +233,8 @@ int dndsb_eval_set_jacobian_mode(dndsb_eval *ev, int useScalarJacobian, int useR
  * jacobianCode must be 0.  A singular block gives DNDSB_E_NONFINITE (one host synchronisation in block mode). */
 int dndsb_eval_lusgs_matrix_init_full(dndsb_eval *ev, const double *dTau, double dt, double alphaDiag, const double *u, const double *uRec,
                                       int jacobianCode, double t, double *jdiag, void *stream);
-/* The local LU of the block Jacobian (jacobiCode 2; block mode only), kept inside the evaluator:
+/* The local LU (jacobiCode 2), kept inside the evaluator, in every Jacobian mode (with the scalar Jacobian its
+ * diagonal blocks are the scalar diagonal, JDiag.getValue, and the neighbour blocks the scalar flux increment):
  * to_jacobian_lu = LUSGSMatrixToJacobianLU (EulerEvaluator.hxx:290-359) with JacobianLocalLU::InPlaceDecompose
  * (Solver/Direct.hpp:312-405) for iluCode 0 (the face-neighbour pattern, no fill): a block ILU(0) factored colour
  * by colour, which is the reference's natural-order factorisation on a mesh numbered colour by colour
@@ -351,7 +352,7 @@ typedef struct dndsb_linear_settings
 {
     int gmresCode;   /* 0 LU-SGS pairs, 1 GMRES from zero, 2 LU-SGS pairs then GMRES */
     int jacobiCode;  /* 1 Gauss-Seidel sweeps (multicolour), 0 Jacobi sweeps, 2 the local LU (block ILU(0), two
-                        defect-correction steps per doPrecondition; block Jacobian only) */
+                        defect-correction steps per doPrecondition) */
     int sgsIter;     /* extra SGS pairs (also inside the GMRES preconditioner) */
     int nGmresSpace; /* Krylov subspace size, 1..32 */
     int nGmresIter;  /* restart cycles */

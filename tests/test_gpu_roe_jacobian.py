@@ -24,7 +24,8 @@ CASES = [("bump-p1-Roe-euler", "bump", 1, "Roe", 0.0, (1, 1, 3)),
          ("bump-p2-RoeM2-euler", "bump", 2, "Roe_M2", 0.0, (1, 1, 3)),
          ("bump-p1-HLLEP-ns-in-outp-isothermal", "bump", 1, "HLLEP", 1e-3, (6, 7, 4)),
          ("bump-p2-Roe-ns-wall", "bump", 2, "Roe", 1e-3, (5, 1, 2)),
-         ("tgv-p2-HLLEP-ns", "tgv", 2, "HLLEP", 1 / 1600, None)]
+         ("tgv-p2-HLLEP-ns", "tgv", 2, "HLLEP", 1 / 1600, None),
+         ("iv2d-p2-RoeM1-euler", "iv", 2, "Roe_M1", 0.0, None)]
 
 
 def _setup(mesh, p, rs, mu, bt):
@@ -38,12 +39,14 @@ def _setup(mesh, p, rs, mu, bt):
         ev.SetBC(types, vals)
         u0, uRec0 = perturbed_state(m, far, R=o.R)
     else:
-        m = M.renumber_by_color(M.tgv_mesh(4))
+        m = M.renumber_by_color(M.tgv_mesh(4) if mesh == "tgv" else M.iv_mesh(8))
         o = oracle_for(m, p, rs, mu, ignoreVis=int(iv))
         vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=p)).construct()
         ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType=rs, muGas=mu, muModel=0, ignoreVis=iv))
-        u0 = o.init_field(3)
+        u0 = o.init_field(3) if mesh == "tgv" else o.init_field(2, 5.0)
         uRec0 = 0.05 * np.random.default_rng(4).normal(size=(m.n_cell, o.R, 5)) * np.abs(u0[:, None, :])
+        if mesh == "iv":  # 2-D: no z momentum
+            uRec0[:, :, 3] = 0
     return m, o, vr, ev, u0, uRec0
 
 
@@ -151,13 +154,15 @@ def _reference_solve(oe, u, rhs, dTau, dt, alpha, code, sgsIter, k, nIter, jacob
     return x
 
 
-@pytest.mark.parametrize("name,mesh,p,rs,mu,bt", [CASES[0], CASES[2], CASES[4]], ids=[CASES[i][0] for i in (0, 2, 4)])
-@pytest.mark.parametrize("code,sgsIter,k,nIter,jacobi", [(0, 1, 1, 1, 1), (1, 0, 8, 2, 1), (2, 1, 5, 1, 1), (0, 1, 1, 1, 2), (1, 0, 8, 1, 2)])
-def test_roe_jacobian_linear_solve(name, mesh, p, rs, mu, bt, code, sgsIter, k, nIter, jacobi):
+@pytest.mark.parametrize("name,mesh,p,rs,mu,bt", [CASES[0], CASES[2], CASES[4], CASES[5]], ids=[CASES[i][0] for i in (0, 2, 4, 5)])
+@pytest.mark.parametrize("code,sgsIter,k,nIter,jacobi,roe", [(0, 1, 1, 1, 1, True), (1, 0, 8, 2, 1, True), (2, 1, 5, 1, 1, True),
+                                                             (0, 1, 1, 1, 2, True), (1, 0, 8, 1, 2, True), (1, 0, 8, 1, 2, False)])
+def test_roe_jacobian_linear_solve(name, mesh, p, rs, mu, bt, code, sgsIter, k, nIter, jacobi, roe):
+    """The native solve with the Roe Jacobian (SGS pairs or the local LU), and the local LU with the scalar Jacobian."""
     m, o, vr, ev, u0, uRec0 = _setup(mesh, p, rs, mu, bt)
     oe = OracleEval(o)
-    oe.SetJacobianMode(False, True)
-    ev.SetJacobianMode(False, True)
+    oe.SetJacobianMode(not roe, roe)
+    ev.SetJacobianMode(not roe, roe)
     ut, uRt = torch.tensor(u0), torch.tensor(uRec0)
     dTau0 = torch.zeros(m.n_cell, dtype=torch.float64)
     oe.EvaluateDt(dTau0, ut, 1e3)
@@ -197,13 +202,15 @@ def test_roe_jacobian_driver_matches_oracle_driver():
     assert relerr(u.cpu().numpy(), u_o.numpy()) < 1e-10
 
 
-@pytest.mark.parametrize("roe", [False, True])
-def test_local_lu_operators(roe):
+@pytest.mark.parametrize("mode", ["scalar", "block", "roe"])
+def test_local_lu_operators(mode):
     """LUSGSMatrixToJacobianLU + LUSGSMatrixSolveJacobianLU (block ILU(0)) against the oracle's natural-order
-    factorisation on the colour-numbered bump mesh."""
+    factorisation on the colour-numbered bump mesh, with the scalar Jacobian (the reference's RotPeriodicIV
+    setting: its diagonal as blocks), the block diagonal and the Roe Jacobian."""
     m, o, vr, ev, u0, uRec0 = _setup("bump", 1, "Roe", 0.0, (1, 1, 3))
-    o.set_jacobian_mode(False, roe)
-    ev.SetJacobianMode(False, roe)
+    roe = mode == "roe"
+    o.set_jacobian_mode(mode == "scalar", roe)
+    ev.SetJacobianMode(mode == "scalar", roe)
     u, uRec = torch.tensor(u0, device="cuda"), torch.tensor(uRec0, device="cuda")
     dt = torch.zeros(m.n_cell, dtype=torch.float64, device="cuda")
     ev.EvaluateDt(dt, u, 20.0)
@@ -213,7 +220,7 @@ def test_local_lu_operators(roe):
     rhs0 = o.eval_rhs(u0, uRec0)
     jd = ev.BuildJDiag()
     ev.LUSGSMatrixInit(jd, dt, 1e100, 1.0, u)
-    jd0 = o.lusgs_init_block(d0, 1e100, 1.0, u0)
+    jd0 = o.lusgs_init(d0, 1e100, 1.0) if mode == "scalar" else o.lusgs_init_block(d0, 1e100, 1.0, u0)
     ev.LUSGSMatrixToJacobianLU(1.0, u, jd)
     o.jacobian_lu(1.0, u0, jd0)
     x0 = np.random.default_rng(7).normal(size=u0.shape)
