@@ -181,3 +181,23 @@ def test_block_ilu0_factors_match_the_operator_on_its_pattern():
     r1 = np.linalg.norm(b.ravel() - A @ x.ravel())
     r2 = np.linalg.norm(b.ravel() - A @ x2.ravel())
     assert r2 < 0.5 * r1, (r1, r2)
+
+
+def test_local_lu_with_the_scalar_jacobian_equals_block_mode():
+    """LUSGSMatrixToJacobianLU takes JDiag.getValue: with the scalar Jacobian the diagonal blocks are the scalar
+    diagonal, so its local LU equals the one of the block mode without the Roe term."""
+    m = M.renumber_by_color(M.bump_channel_tet(3, 2, 2))
+    o, far, types, vals, w = bump_oracle(m, 1, "Roe", 0.0, 1)
+    u0, uRec0 = perturbed_state(m, far, R=o.R)
+    d0, _ = o.eval_dt(u0, 20.0)
+    rhs = o.eval_rhs(u0, uRec0)
+    b = np.random.default_rng(6).normal(size=rhs.shape)
+    out = {}
+    for block in (False, True):
+        o.set_jacobian_mode(not block, False)
+        jd = o.lusgs_init_block(d0, 1e100, 1.0, u0) if block else o.lusgs_init(d0, 1e100, 1.0)
+        o.jacobian_lu(1.0, u0, jd)
+        out[block] = (o.get("luOff"), o.get("luDinv"), o.solve_jacobian_lu(1.0, b, u0, np.zeros_like(b), jd, True)[0],
+                      o.solve_jacobian_lu(1.0, b, u0, 0.1 * b, jd, False)[0])
+    for a, c in zip(out[False], out[True]):
+        assert np.allclose(a, c, rtol=1e-14, atol=1e-14 * np.abs(c).max())
