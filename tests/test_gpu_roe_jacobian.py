@@ -306,3 +306,41 @@ def test_sa_block_operators(roe):
         xs = torch.zeros_like(u)
         ev.SolveLinear(0.5, dt, 0.1, u, rhs, xs, gmresCode=1, nGmresSpace=6, jacobiCode=2, precision=prec)
         assert relerr(xs.cpu().numpy(), refx.numpy()) < tol, prec
+
+
+def test_local_lu_with_triangles_in_the_cell_graph():
+    """A 3-periodic hexahedral grid: each row of three cells is a triangle of face neighbours, so the ILU(0)
+    corrections between neighbours that share a lower neighbour run (standalone local LU and native solve)."""
+    from dndsr_b200.solver import EulerEvaluator, VariationalReconstruction
+    m = M.renumber_by_color(M.tgv_mesh(3))
+    o = oracle_for(m, 1, "Roe", 1e-3, ignoreVis=0)
+    vr = VariationalReconstruction(m, dict(VR_HQM_PY, maxOrder=1)).construct()
+    ev = EulerEvaluator(vr, dict(nVars=5, riemannSolverType="Roe", muGas=1e-3, muModel=0))
+    o.set_jacobian_mode(False, True)
+    ev.SetJacobianMode(False, True)
+    u0 = o.init_field(3)
+    uRec0 = 0.02 * np.random.default_rng(1).normal(size=(m.n_cell, o.R, 5))
+    u, uRec = torch.tensor(u0, device="cuda"), torch.tensor(uRec0, device="cuda")
+    dt = torch.zeros(m.n_cell, dtype=torch.float64, device="cuda")
+    ev.EvaluateDt(dt, u, 10.0)
+    d0, _ = o.eval_dt(u0, 10.0)
+    rhs = torch.zeros_like(u)
+    ev.EvaluateRHS(rhs, u, uRec)
+    r0 = o.eval_rhs(u0, uRec0)
+    jd = ev.BuildJDiag()
+    ev.LUSGSMatrixInit(jd, dt, 1e100, 1.0, u)
+    jd0 = o.lusgs_init_block(d0, 1e100, 1.0, u0)
+    ev.LUSGSMatrixToJacobianLU(1.0, u, jd)
+    o.jacobian_lu(1.0, u0, jd0)
+    x0 = np.random.default_rng(3).normal(size=u0.shape)
+    out = torch.zeros_like(u)
+    for zero in (True, False):
+        ev.LUSGSMatrixSolveJacobianLU(1.0, rhs, u, torch.tensor(x0, device="cuda"), out, jd, zero)
+        ref, _ = o.solve_jacobian_lu(1.0, r0, u0, x0, jd0, zero)
+        assert relerr(out.cpu().numpy(), ref) < 1e-11, zero
+    oe = OracleEval(o)
+    oe.SetJacobianMode(False, True)
+    refx = _reference_solve(oe, torch.tensor(u0), torch.tensor(r0), torch.tensor(d0), 1e100, 1.0, 1, 0, 6, 1, 2)
+    xs = torch.zeros_like(u)
+    ev.SolveLinear(1.0, dt, 1e100, u, rhs, xs, gmresCode=1, nGmresSpace=6, jacobiCode=2)
+    assert relerr(xs.cpu().numpy(), refx.numpy()) < 1e-10

@@ -201,3 +201,49 @@ def test_local_lu_with_the_scalar_jacobian_equals_block_mode():
                       o.solve_jacobian_lu(1.0, b, u0, 0.1 * b, jd, False)[0])
     for a, c in zip(out[False], out[True]):
         assert np.allclose(a, c, rtol=1e-14, atol=1e-14 * np.abs(c).max())
+
+
+def test_block_ilu0_with_triangles_in_the_cell_graph():
+    """On a 3-periodic hexahedral grid each row of three cells is a triangle of face neighbours, so the ILU(0)
+    updates between two neighbours that share a lower neighbour (L_ij -= L_ik U_kj, U_ij -= L_ik U_kj) run; the
+    factors still reproduce A on its pattern."""
+    import oracle
+    from tests.util import VR_HQM
+    m = M.renumber_by_color(M.tgv_mesh(3))
+    es = dict(nVars=5, rsType=oracle.RS["Roe"], rsFixScale=1.0, rsIncFScale=1.0, gamma=1.4, Rgas=1.0, muGas=1e-3, prGas=0.72, TRef=273.15,
+              CSutherland=110.4, muModel=0, ignoreVis=0)
+    o = oracle.Oracle(m, dict(VR_HQM, maxOrder=1), es)
+    assert o.construct() == 0
+    u0 = o.init_field(3)
+    uRec0 = 0.02 * np.random.default_rng(1).normal(size=(m.n_cell, o.R, 5))
+    o.set_jacobian_mode(False, True)
+    d0, _ = o.eval_dt(u0, 10.0)
+    o.eval_rhs(u0, uRec0)
+    jd = o.lusgs_init_block(d0, 1e100, 1.0, u0)
+    n, nv = m.n_cell, 5
+    A = _dense(o, n, nv, lambda x: o.lusgs_matvec(1.0, u0, x, jd))
+    o.jacobian_lu(1.0, u0, jd)
+    off = o.get("luOff").reshape(n, -1, nv, nv)
+    dinv = o.get("luDinv").reshape(n, nv, nv)
+    f2c, c2f = np.asarray(m.face2cell), np.asarray(m.cell2face)
+    L, U = np.eye(n * nv), np.zeros((n * nv, n * nv))
+    pattern = np.zeros((n, n), bool)
+    tri = 0
+    nb = [set() for _ in range(n)]
+    for i in range(n):
+        U[i * nv:(i + 1) * nv, i * nv:(i + 1) * nv] = np.linalg.inv(dinv[i])
+        pattern[i, i] = True
+        for k, f in enumerate(c2f[i]):
+            c0, c1 = f2c[f]
+            j = c1 if c0 == i else c0
+            if j < 0 or j == i:
+                continue
+            nb[i].add(j)
+            pattern[i, j] = True
+            (L if j < i else U)[i * nv:(i + 1) * nv, j * nv:(j + 1) * nv] = off[i, k]
+    for i in range(n):
+        for j in nb[i]:
+            tri += len(nb[i] & nb[j])
+    assert tri > 0  # the cell graph has triangles
+    mask = np.kron(pattern, np.ones((nv, nv), bool))
+    assert np.abs((L @ U - A)[mask]).max() < 1e-12 * np.abs(A).max()
