@@ -122,6 +122,8 @@ def _declare(L):
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_set_jacobian_mode.argtypes = [_V, ctypes.c_int]
     L.orc_vr_iter_sor.argtypes = [_V, _D, _D]
+    L.orc_wbap_l2_biway.argtypes = [ctypes.c_long, _D, _D, ctypes.c_double, _D]
+    L.orc_wbap_l2_multiway.argtypes = [ctypes.c_long, ctypes.c_int, _D, ctypes.c_double, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
     L.orc_jacobian_lu.restype = ctypes.c_int
     L.orc_solve_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
@@ -166,6 +168,22 @@ def riemann(rs, UL, UR, n, gamma=1.4, ULm=None, URm=None, dLambda=0.0, fixScale=
     code = RS[rs] if isinstance(rs, str) else int(rs)
     lib().orc_riemann(code, _p(UL), _p(UR), _p(ULm), _p(URm), _p(n), gamma, dLambda, fixScale, incFScale, _p(F), _p(lam))
     return F, lam
+
+
+def wbap_l2_biway(u1, u2, n=1.0):
+    """Limiters.hpp FWBAP_L2_Biway entry by entry (the limiter function of the oracle's WBAP_C)."""
+    u1, u2 = _f64(u1), _f64(u2)
+    out = np.zeros_like(u1)
+    lib().orc_wbap_l2_biway(u1.size, _p(u1), _p(u2), float(n), _p(out))
+    return out
+
+
+def wbap_l2_multiway(others, n1=1.0):
+    """Limiters.hpp FWBAP_L2_Multiway entry by entry; others [nOther][...] with the cell's own values first."""
+    o = _f64(others)
+    out = np.zeros(o.shape[1:])
+    lib().orc_wbap_l2_multiway(int(np.prod(o.shape[1:])), o.shape[0], _p(o), float(n1), _p(out))
+    return out
 
 
 def roe_fdiff_matrix(U, UOther, n, lam, gamma=1.4):

@@ -3643,10 +3643,51 @@ void ocCharTransform(const double *uL, const double *uR, const double *n, double
 
 double ocSign(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
 const double kPDiP = 1e-50; // verySmallReal^(1/4)
+
+// Limiters.hpp:432-466 FWBAP_L2_Biway (the fast version) for one entry: u1 (n + th^3) / (n + th^4) |sign(u2)|,
+// th = u1 / (|u2| + eps) sign(u2)
+double ocWbapBiway(double u1, double u2, double n)
+{
+    double fr = u1 / (abs(u2) + kPDiP) * ocSign(u2);
+    double t1 = fr * fr * fr, t2 = (fr * fr) * (fr * fr);
+    return u1 * (n + t1) / (n + t2) * abs(ocSign(u2));
+}
+
+// Limiters.hpp:361-385 FWBAP_L2_Multiway (the fast version) for one entry: others[0] is the cell's own value
+double ocWbapMultiway(const double *others, int nOther, double n1)
+{
+    double up = 0, down = 0, cent = others[0];
+    for (int q = 1; q < nOther; q++)
+    {
+        double ti = others[0] / (abs(others[q]) + kPDiP) * ocSign(others[q]);
+        down += (ti * ti) * (ti * ti);
+        up += ti * ti * ti;
+        cent *= abs(ocSign(others[q]));
+    }
+    return cent * (up + n1) / (down + n1);
+}
 } // namespace
 
 extern "C"
 {
+    // the limiter functions on arrays of entries (the reference's FWBAP_L2_Biway / FWBAP_L2_Multiway test surface):
+    // biway out[i] = f(u1[i], u2[i]); multiway out[i] = f(others[0][i], ..., others[nOther - 1][i]), others [nOther][n]
+    void orc_wbap_l2_biway(long n, const double *u1, const double *u2, double nPar, double *out)
+    {
+        for (long i = 0; i < n; i++)
+            out[i] = ocWbapBiway(u1[i], u2[i], nPar);
+    }
+    void orc_wbap_l2_multiway(long n, int nOther, const double *others, double n1, double *out)
+    {
+        double vals[16];
+        for (long i = 0; i < n; i++)
+        {
+            for (int q = 0; q < nOther && q < 16; q++)
+                vals[q] = others[(long)q * n + i];
+            out[i] = ocWbapMultiway(vals, nOther < 16 ? nOther : 16, n1);
+        }
+    }
+
     // VariationalReconstruction_LimiterProcedure.hxx:40-108 DoCalculateSmoothIndicator, varsSee {0, 4}
     void orc_smooth_indicator(void *h, const double *u, const double *uRec, double *si)
     {
@@ -3784,12 +3825,7 @@ extern "C"
                     ocCharTransform(uL, uR, n, gamma, true, nr, nv, tin.data());
                     std::vector<double> lim(nr * nv);
                     for (int i = 0; i < nr * nv; i++)
-                    {
-                        double u1 = tin[i], u2 = oin[i];
-                        double fr = u1 / (abs(u2) + kPDiP) * ocSign(u2);
-                        double t1 = fr * fr * fr, t2 = (fr * fr) * (fr * fr);
-                        lim[i] = u1 * (1 + t1) / (1 + t2) * abs(ocSign(u2));
-                    }
+                        lim[i] = ocWbapBiway(tin[i], oin[i], 1.0);
                     ocCharTransform(uL, uR, n, gamma, false, nr, nv, lim.data());
                     for (int i = 0; i < nr * nv; i++)
                         uf[ls * nv + i] = lim[i];
@@ -3797,15 +3833,10 @@ extern "C"
                 }
                 for (int i = 0; i < nr * nv; i++)
                 {
-                    double up = 0, down = 0, cent = others[0][i];
-                    for (size_t q = 1; q < others.size(); q++)
-                    {
-                        double ti = others[0][i] / (abs(others[q][i]) + kPDiP) * ocSign(others[q][i]);
-                        down += (ti * ti) * (ti * ti);
-                        up += ti * ti * ti;
-                        cent *= abs(ocSign(others[q][i]));
-                    }
-                    out[ls * nv + i] = cent * (up + nStd) / (down + nStd);
+                    double vals[16];
+                    for (size_t q = 0; q < others.size(); q++)
+                        vals[q] = others[q][i];
+                    out[ls * nv + i] = ocWbapMultiway(vals, (int)others.size(), nStd);
                 }
             }
         }

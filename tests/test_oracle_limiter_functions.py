@@ -1,0 +1,59 @@
+"""The oracle's WBAP-L2 limiter functions against the reference's own unit cases for them
+(test/cpp/CFV/test_Limiters.cpp:244-286 FWBAP_L2_Biway and :315-343 FWBAP_L2_Multiway), restated with seeded random
+arrays in place of Eigen's setRandom (uniform on [-1, 1]); plus the exact values the formulas give."""
+import numpy as np
+
+import oracle
+
+
+def _rand(rng, *shape):
+    return rng.uniform(-1.0, 1.0, size=shape)
+
+
+def test_biway_identical_inputs_pass_through():  # test_Limiters.cpp:244-257
+    u1 = _rand(np.random.default_rng(1), 2, 3)
+    out = oracle.wbap_l2_biway(u1, u1.copy(), 1.0)
+    assert np.allclose(out, u1, rtol=1e-10, atol=0)
+
+
+def test_biway_no_nan_for_random_inputs():  # :259-266
+    rng = np.random.default_rng(2)
+    out = oracle.wbap_l2_biway(_rand(rng, 3, 5), _rand(rng, 3, 5), 1.0)
+    assert not np.isnan(out).any()
+
+
+def test_biway_output_non_negative_for_same_sign():  # :268-286
+    rng = np.random.default_rng(3)
+    u1 = np.abs(_rand(rng, 1, 100)) + 0.1
+    u2 = np.abs(_rand(rng, 1, 100)) + 0.1
+    out = oracle.wbap_l2_biway(u1, u2, 1.0)
+    assert (out >= -1e-10).all()
+
+
+def test_biway_values():
+    # th = u1 / |u2| sign(u2): u1 (n + th^3) / (n + th^4); opposite signs and a zero neighbour limit to 0 or u1 ...
+    u1 = np.array([2.0, 2.0, -1.0, 3.0])
+    u2 = np.array([1.0, -1.0, 2.0, 0.0])
+    out = oracle.wbap_l2_biway(u1, u2, 1.0)
+    th = np.array([2.0, -2.0, -0.5, 0.0])
+    ref = u1 * (1 + th ** 3) / (1 + th ** 4) * np.abs(np.sign(u2))
+    assert np.allclose(out, ref, rtol=1e-14, atol=1e-300)
+    assert out[3] == 0.0  # a zero neighbour value cuts the slope
+
+
+def test_multiway_identical_inputs_pass_through():  # :315-330
+    u0 = _rand(np.random.default_rng(4), 2, 3)
+    out = oracle.wbap_l2_multiway(np.stack([u0] * 4), 1.0)
+    assert np.allclose(out, u0, rtol=1e-8, atol=0)
+
+
+def test_multiway_no_nan_for_random_inputs():  # :332-343
+    rng = np.random.default_rng(5)
+    out = oracle.wbap_l2_multiway(np.stack([_rand(rng, 3, 4) for _ in range(5)]), 1.0)
+    assert not np.isnan(out).any()
+
+
+def test_multiway_equals_biway_for_two_inputs():
+    rng = np.random.default_rng(6)
+    a, b = _rand(rng, 50), _rand(rng, 50)
+    assert np.allclose(oracle.wbap_l2_multiway(np.stack([a, b]), 1.0), oracle.wbap_l2_biway(a, b, 1.0), rtol=1e-14, atol=1e-300)
