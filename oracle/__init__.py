@@ -123,6 +123,8 @@ def _declare(L):
     L.orc_set_jacobian_mode.argtypes = [_V, ctypes.c_int]
     L.orc_vr_iter_sor.argtypes = [_V, _D, _D]
     L.orc_wbap_l2_biway.argtypes = [ctypes.c_long, _D, _D, ctypes.c_double, _D]
+    L.orc_pp_compression_ratio.argtypes = [_D, _D, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+    L.orc_pp_compression_ratio.restype = ctypes.c_double
     L.orc_wbap_l2_multiway.argtypes = [ctypes.c_long, ctypes.c_int, _D, ctypes.c_double, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
     L.orc_jacobian_lu.restype = ctypes.c_int
@@ -168,6 +170,14 @@ def riemann(rs, UL, UR, n, gamma=1.4, ULm=None, URm=None, dLambda=0.0, fixScale=
     code = RS[rs] if isinstance(rs, str) else int(rs)
     lib().orc_riemann(code, _p(UL), _p(UR), _p(ULm), _p(URm), _p(n), gamma, dLambda, fixScale, incFScale, _p(F), _p(lam))
     return F, lam
+
+
+def pp_compression_ratio(u, inc, newRhoE=0.0):
+    """Gas.hpp IdealGasGetCompressionRatioPressure (scheme 0): the largest alpha in [0, 1) keeping rhoE(u + alpha inc)
+    above newRhoE; returns (alpha, bad)."""
+    bad = ctypes.c_int(0)
+    a = lib().orc_pp_compression_ratio(_p(_f64(u)), _p(_f64(inc)), float(newRhoE), ctypes.byref(bad))
+    return a, bool(bad.value)
 
 
 def wbap_l2_biway(u1, u2, n=1.0):

@@ -3409,6 +3409,16 @@ void ppCompressInc(int nv, double gamma, const double *u, const double *inc, dou
 }
 } // namespace
 
+// Gas.hpp IdealGasGetCompressionRatioPressure, exported for its unit cases; *bad receives the quadratic's failure flag
+extern "C" double orc_pp_compression_ratio(const double *u, const double *inc, double newRhoE, int *bad)
+{
+    bool b = false;
+    double a = ppCompressionRatio(u, inc, newRhoE, b);
+    if (bad)
+        *bad = b;
+    return a;
+}
+
 extern "C"
 {
     // EulerEvaluator.hxx:1938-2062 EvaluateCellRHSAlpha (refRho, refP = refUPrim(0), refUPrim(I4));

@@ -1,6 +1,7 @@
-"""The oracle's WBAP-L2 limiter functions against the reference's own unit cases for them
-(test/cpp/CFV/test_Limiters.cpp:244-286 FWBAP_L2_Biway and :315-343 FWBAP_L2_Multiway), restated with seeded random
-arrays in place of Eigen's setRandom (uniform on [-1, 1]); plus the exact values the formulas give."""
+"""The oracle's WBAP-L2 limiter functions and its pressure compression ratio against the reference's own unit cases
+for them (test/cpp/CFV/test_Limiters.cpp:244-286 FWBAP_L2_Biway and :315-343 FWBAP_L2_Multiway,
+test/cpp/Euler/test_GasThermo.cpp:447-475 IdealGasGetCompressionRatioPressure), restated with seeded random arrays in
+place of Eigen's setRandom (uniform on [-1, 1]); plus the exact values the formulas give."""
 import numpy as np
 
 import oracle
@@ -57,3 +58,23 @@ def test_multiway_equals_biway_for_two_inputs():
     rng = np.random.default_rng(6)
     a, b = _rand(rng, 50), _rand(rng, 50)
     assert np.allclose(oracle.wbap_l2_multiway(np.stack([a, b]), 1.0), oracle.wbap_l2_biway(a, b, 1.0), rtol=1e-14, atol=1e-300)
+
+
+def _prim_to_cons(rho, vx, vy, vz, p, gamma=1.4):
+    v = np.array([vx, vy, vz])
+    return np.array([rho, *(rho * v), p / (gamma - 1) + 0.5 * rho * v @ v])
+
+
+def test_compression_ratio_zero_increment():  # test/cpp/Euler/test_GasThermo.cpp:447-456
+    U = _prim_to_cons(1.225, 100.0, -50.0, 25.0, 101325.0)
+    alpha, bad = oracle.pp_compression_ratio(U, np.zeros(5), 0.0)
+    assert abs(alpha) <= 1e-14 and not bad
+
+
+def test_compression_ratio_in_unit_interval_and_keeps_internal_energy():  # test_GasThermo.cpp:458-475
+    U = _prim_to_cons(1.0, 0.0, 0.0, 0.0, 1.0)
+    dU = np.array([0.0, 0.0, 0.0, 0.0, -100.0])
+    alpha, bad = oracle.pp_compression_ratio(U, dU, 0.0)
+    assert 0.0 <= alpha <= 1.0
+    Un = U + alpha * dU
+    assert Un[4] - 0.5 * Un[0] * np.sum((Un[1:4] / Un[0]) ** 2) >= -1e-10
