@@ -124,6 +124,7 @@ def _declare(L):
     L.orc_vr_iter_sor.argtypes = [_V, _D, _D]
     L.orc_wbap_l2_biway.argtypes = [ctypes.c_long, _D, _D, ctypes.c_double, _D]
     L.orc_pp_compression_ratio.argtypes = [_D, _D, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+    L.orc_euler_eigen.argtypes = [_D, ctypes.c_double, _D, _D]
     L.orc_pp_compression_ratio.restype = ctypes.c_double
     L.orc_wbap_l2_multiway.argtypes = [ctypes.c_long, ctypes.c_int, _D, ctypes.c_double, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
@@ -170,6 +171,13 @@ def riemann(rs, UL, UR, n, gamma=1.4, ULm=None, URm=None, dLambda=0.0, fixScale=
     code = RS[rs] if isinstance(rs, str) else int(rs)
     lib().orc_riemann(code, _p(UL), _p(UR), _p(ULm), _p(URm), _p(n), gamma, dLambda, fixScale, incFScale, _p(F), _p(lam))
     return F, lam
+
+
+def euler_eigen(U, gamma=1.4):
+    """(R, L): the right and left eigenvectors of the Euler flux Jacobian at the conservative state U (x direction)."""
+    R, L = np.zeros((5, 5)), np.zeros((5, 5))
+    lib().orc_euler_eigen(_p(_f64(U)), float(gamma), _p(R), _p(L))
+    return R, L
 
 
 def pp_compression_ratio(u, inc, newRhoE=0.0):

@@ -3680,6 +3680,17 @@ double ocWbapMultiway(const double *others, int nOther, double n1)
 
 extern "C"
 {
+    // Gas.hpp IdealGas_EulerGasRight/LeftEigenVector of a conservative state (the characteristic projection of the
+    // limiter), R and L row-major 5 x 5
+    void orc_euler_eigen(const double *U, double gamma, double *R, double *L)
+    {
+        double Rv[5][5], Lv[5][5];
+        ocEigen(U, gamma, Rv, Lv);
+        for (int i = 0; i < 5; i++)
+            for (int j = 0; j < 5; j++)
+                R[i * 5 + j] = Rv[i][j], L[i * 5 + j] = Lv[i][j];
+    }
+
     // the limiter functions on arrays of entries (the reference's FWBAP_L2_Biway / FWBAP_L2_Multiway test surface):
     // biway out[i] = f(u1[i], u2[i]); multiway out[i] = f(others[0][i], ..., others[nOther - 1][i]), others [nOther][n]
     void orc_wbap_l2_biway(long n, const double *u1, const double *u2, double nPar, double *out)

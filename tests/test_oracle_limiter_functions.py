@@ -78,3 +78,9 @@ def test_compression_ratio_in_unit_interval_and_keeps_internal_energy():  # test
     assert 0.0 <= alpha <= 1.0
     Un = U + alpha * dU
     assert Un[4] - 0.5 * Un[0] * np.sum((Un[1:4] / Un[0]) ** 2) >= -1e-10
+
+
+def test_characteristic_eigenvectors_invert_each_other():  # test/cpp/Euler/test_GasThermo.cpp:174-238
+    for rho, v, p in ((1.0, (1.5, -0.3, 0.7), 1.0), (1.225, (300.0, -150.0, 75.0), 101325.0), (1.225, (100.0, -50.0, 25.0), 101325.0)):
+        R, L = oracle.euler_eigen(_prim_to_cons(rho, *v, p))
+        assert np.abs(L @ R - np.eye(5)).max() < 1e-10, (rho, v, p)
