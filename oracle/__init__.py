@@ -127,6 +127,9 @@ def _declare(L):
     L.orc_euler_eigen.argtypes = [_D, ctypes.c_double, _D, _D]
     L.orc_pp_compression_ratio.restype = ctypes.c_double
     L.orc_wbap_l2_multiway.argtypes = [ctypes.c_long, ctypes.c_int, _D, ctypes.c_double, _D]
+    L.orc_block_ilu0.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), _D, _D, _D]
+    L.orc_block_ilu0.restype = ctypes.c_int
+    L.orc_block_ilu0_solve.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), _D, _D, _D, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
     L.orc_jacobian_lu.restype = ctypes.c_int
     L.orc_solve_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
@@ -202,6 +205,32 @@ def wbap_l2_multiway(others, n1=1.0):
     out = np.zeros(o.shape[1:])
     lib().orc_wbap_l2_multiway(int(np.prod(o.shape[1:])), o.shape[0], _p(o), float(n1), _p(out))
     return out
+
+
+def block_ilu0(nbr, off, diag):
+    """Block ILU(0) in natural order on a general neighbour table (JacobianLocalLU::InPlaceDecompose with
+    iluCode 0, Solver/Direct.hpp:312-405).  nbr [n][K] (-1: none), off [n][K][bs][bs] the blocks A_(i, nbr[i][k]),
+    diag [n][bs][bs].  Returns (factors [n][K][bs][bs]: L for lower neighbours, U for upper; dinv [n][bs][bs])."""
+    nbr = np.ascontiguousarray(nbr, dtype=np.int64)
+    n, K = nbr.shape
+    bs = np.asarray(diag).shape[-1]
+    f = _f64(off).reshape(n, K, bs, bs).copy()
+    d = _f64(diag).reshape(n, bs, bs)
+    dinv = np.zeros_like(d)
+    if lib().orc_block_ilu0(n, bs, K, _p(nbr, ctypes.POINTER(ctypes.c_int64)), _p(f), _p(d), _p(dinv)) != 0:
+        raise ValueError("block_ilu0: singular pivot or block size above 8")
+    return f, dinv
+
+
+def block_ilu0_solve(nbr, factors, dinv, b):
+    """x = (L U)^-1 b with the factors of block_ilu0 (JacobianLocalLU::Solve, Solver/Direct.hpp:487-540)."""
+    nbr = np.ascontiguousarray(nbr, dtype=np.int64)
+    n, K = nbr.shape
+    bs = np.asarray(dinv).shape[-1]
+    b = _f64(b).reshape(n, bs)
+    x = np.zeros_like(b)
+    lib().orc_block_ilu0_solve(n, bs, K, _p(nbr, ctypes.POINTER(ctypes.c_int64)), _p(_f64(factors)), _p(_f64(dinv)), _p(b), _p(x))
+    return x
 
 
 def roe_fdiff_matrix(U, UOther, n, lam, gamma=1.4):

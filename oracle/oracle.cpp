@@ -3865,4 +3865,138 @@ extern "C"
     }
 }
 
+// ---------------------------------------------------------------------------
+// Block ILU(0) of a general block-sparse matrix with a symmetric pattern, natural order: the restatement of
+// JacobianLocalLU::InPlaceDecompose (Solver/Direct.hpp:312-405) with iluCode 0 and of its Solve
+// (Direct.hpp:487-540) on an arbitrary neighbour table, in the same update order as Oracle::jacobianLU.  It is
+// checked against the reference's own unit case of the local LU (test/cpp/Solver/test_Direct.cpp: a periodic
+// grid with 2 x 2 blocks) and against Oracle::jacobianLU on mesh operators.
+// nbr [n][K]: neighbour indices, -1 for none; off [n][K][bs][bs]: A_(i, nbr[i][k]) in, L (neighbour < i) or U
+// (neighbour > i) out; diag [n][bs][bs]: A_ii; dinv [n][bs][bs] out: the inverted pivots.  bs <= 8.
+// ---------------------------------------------------------------------------
+namespace
+{
+int ocSlot(const int64_t *nbr, int K, int64_t c, int64_t o)
+{
+    for (int k = 0; k < K; k++)
+        if (nbr[c * K + k] == o)
+            return k;
+    return -1;
+}
+
+bool ocBlockIlu0(int64_t n, int bs, int K, const int64_t *nbr, double *off, const double *diag, double *dinv)
+{
+    const int nn = bs * bs;
+    bool ok = true;
+    std::vector<double> Di(nn), T(nn);
+    for (int64_t i = 0; i < n; i++)
+    {
+        std::vector<std::pair<int64_t, int>> low, upp;
+        for (int k = 0; k < K; k++)
+        {
+            int64_t o = nbr[i * K + k];
+            if (o >= 0 && o != i)
+                (o < i ? low : upp).push_back({o, k});
+        }
+        std::sort(low.begin(), low.end());
+        for (size_t a = 0; a < low.size(); a++) // L_ij = (A_ij - sum_{k < j} L_ik U_kj) Dinv_j
+        {
+            int64_t j = low[a].first;
+            double *Lij = off + (i * K + low[a].second) * nn;
+            for (size_t b = 0; b < a; b++)
+            {
+                int sk = ocSlot(nbr, K, low[b].first, j);
+                if (sk >= 0)
+                    Oracle::blockMulSub(bs, off + (i * K + low[b].second) * nn, off + (low[b].first * K + sk) * nn, Lij);
+            }
+            std::copy(Lij, Lij + nn, T.begin());
+            for (int r = 0; r < bs; r++)
+                for (int c = 0; c < bs; c++)
+                {
+                    double acc = 0;
+                    for (int l = 0; l < bs; l++)
+                        acc += T[r * bs + l] * dinv[j * nn + l * bs + c];
+                    Lij[r * bs + c] = acc;
+                }
+        }
+        std::copy(diag + i * nn, diag + (i + 1) * nn, Di.begin());
+        for (auto &lk : low) // D_i = A_ii - sum_k L_ik U_ki
+        {
+            int si = ocSlot(nbr, K, lk.first, i);
+            if (si >= 0)
+                Oracle::blockMulSub(bs, off + (i * K + lk.second) * nn, off + (lk.first * K + si) * nn, Di.data());
+        }
+        ok = Oracle::invertBlock(bs, Di.data(), dinv + i * nn) && ok;
+        for (auto &uj : upp) // U_ij = A_ij - sum_{k < i} L_ik U_kj
+        {
+            double *Uij = off + (i * K + uj.second) * nn;
+            for (auto &lk : low)
+            {
+                int sk = ocSlot(nbr, K, lk.first, uj.first);
+                if (sk >= 0)
+                    Oracle::blockMulSub(bs, off + (i * K + lk.second) * nn, off + (lk.first * K + sk) * nn, Uij);
+            }
+        }
+    }
+    return ok;
+}
+
+void ocBlockIlu0Solve(int64_t n, int bs, int K, const int64_t *nbr, const double *off, const double *dinv, const double *b, double *x)
+{
+    const int nn = bs * bs;
+    for (int64_t i = 0; i < n; i++) // (L + I) y = b, lower neighbours in slot order
+    {
+        for (int r = 0; r < bs; r++)
+            x[i * bs + r] = b[i * bs + r];
+        for (int k = 0; k < K; k++)
+        {
+            int64_t o = nbr[i * K + k];
+            if (o < 0 || o >= i)
+                continue;
+            for (int r = 0; r < bs; r++)
+                for (int l = 0; l < bs; l++)
+                    x[i * bs + r] -= off[(i * K + k) * nn + r * bs + l] * x[o * bs + l];
+        }
+    }
+    double t[8];
+    for (int64_t i = n - 1; i >= 0; i--) // (D + U) x = y
+    {
+        for (int k = 0; k < K; k++)
+        {
+            int64_t o = nbr[i * K + k];
+            if (o < 0 || o <= i)
+                continue;
+            for (int r = 0; r < bs; r++)
+                for (int l = 0; l < bs; l++)
+                    x[i * bs + r] -= off[(i * K + k) * nn + r * bs + l] * x[o * bs + l];
+        }
+        for (int r = 0; r < bs; r++)
+        {
+            double acc = 0;
+            for (int l = 0; l < bs; l++)
+                acc += dinv[i * nn + r * bs + l] * x[i * bs + l];
+            t[r] = acc;
+        }
+        for (int r = 0; r < bs; r++)
+            x[i * bs + r] = t[r];
+    }
+}
+} // namespace
+
+extern "C"
+{
+    // block ILU(0) in place on a general neighbour table (see ocBlockIlu0); 0, or -1 on a singular pivot or bs > 8
+    int orc_block_ilu0(int64_t n, int bs, int K, const int64_t *nbr, double *off, const double *diag, double *dinv)
+    {
+        if (bs < 1 || bs > 8)
+            return -1;
+        return ocBlockIlu0(n, bs, K, nbr, off, diag, dinv) ? 0 : -1;
+    }
+    // x = (L U)^-1 b with the factors of orc_block_ilu0
+    void orc_block_ilu0_solve(int64_t n, int bs, int K, const int64_t *nbr, const double *off, const double *dinv, const double *b, double *x)
+    {
+        ocBlockIlu0Solve(n, bs, K, nbr, off, dinv, b, x);
+    }
+}
+
 #endif // ORC_OPCOUNT
