@@ -130,6 +130,9 @@ def _declare(L):
     L.orc_block_ilu0.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), _D, _D, _D]
     L.orc_block_ilu0.restype = ctypes.c_int
     L.orc_block_ilu0_solve.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), _D, _D, _D, _D]
+    L.orc_quad_npoints.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.orc_quad_npoints.restype = ctypes.c_int
+    L.orc_quad_point.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
     L.orc_jacobian_lu.restype = ctypes.c_int
     L.orc_solve_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
@@ -205,6 +208,20 @@ def wbap_l2_multiway(others, n1=1.0):
     out = np.zeros(o.shape[1:])
     lib().orc_wbap_l2_multiway(int(np.prod(o.shape[1:])), o.shape[0], _p(o), float(n1), _p(out))
     return out
+
+
+QUAD_ELEM = dict(line=0, tri=1, quad=2, tet=3, hex=4)
+
+
+def quad_rule(elem, order):
+    """The oracle's quadrature rule (QuadratureHub.hpp:39-380) for an element kind of QUAD_ELEM and an integration
+    order on the reference element: points [n][3] and weights [n]."""
+    e = QUAD_ELEM[elem]
+    n = lib().orc_quad_npoints(e, order)
+    pts, w = np.zeros((n, 3)), np.zeros(n)
+    for i in range(n):
+        lib().orc_quad_point(e, order, i, _p(pts[i]), _p(w[i:i + 1]))
+    return pts, w
 
 
 def block_ilu0(nbr, off, diag):

@@ -3992,6 +3992,18 @@ extern "C"
             return -1;
         return ocBlockIlu0(n, bs, K, nbr, off, diag, dinv) ? 0 : -1;
     }
+    // the quadrature rules of QuadratureHub.hpp:39-380 on the reference element (elem: 0 line [-1, 1], 1 triangle
+    // (0,0)-(1,0)-(0,1), 2 quadrilateral [-1, 1]^2, 3 tetrahedron (0,0,0)-(1,0,0)-(0,1,0)-(0,0,1), 4 hexahedron
+    // [-1, 1]^3): the number of points of an integration order, and point iG with its weight
+    int orc_quad_npoints(int elem, int order) { return quadNPoints(elem, order); }
+    void orc_quad_point(int elem, int order, int iG, double *p, double *w)
+    {
+        real pp[3], ww;
+        quadPoint(elem, order, iG, pp, ww);
+        for (int d = 0; d < 3; d++)
+            p[d] = pp[d];
+        *w = ww;
+    }
     // x = (L U)^-1 b with the factors of orc_block_ilu0
     void orc_block_ilu0_solve(int64_t n, int bs, int K, const int64_t *nbr, const double *off, const double *dinv, const double *b, double *x)
     {
