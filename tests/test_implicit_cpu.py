@@ -2,7 +2,7 @@
 
 * the dual-time ESDIRK4 / SDIRK4 / backward-Euler steppers reach their orders
   on the harmonic oscillator of test/cpp/Solver/test_ODE.cpp:55-118, 183-200;
-* GMRES on a small nonsymmetric system (test/cpp/Solver/test_Linear.cpp);
+* GMRES on a small nonsymmetric system and the reference's own GMRES cases (test/cpp/Solver/test_Linear.cpp:44-150);
 * the whole driver (frhs / fdtau / fsolve) running on the oracle advances an
   isentropic vortex stably.
 """
@@ -73,6 +73,50 @@ def test_gmres_small_system():
     g.solve(lambda v, Av: Av.copy_(At @ v), lambda v, Mv: Mv.copy_(v), lambda a, c: float(a @ c), torch.tensor(b), x, 10,
             lambda i, r, rb: r < 1e-12 * rb)
     np.testing.assert_allclose(x.numpy(), np.linalg.solve(A, b), rtol=1e-9, atol=1e-11)
+
+
+def _gmres(A, b, k, n_restart, tol, diag_prec=False):
+    At = torch.tensor(A)
+    dinv = torch.tensor(1.0 / np.diag(A))
+    g = I.GMRES(k, torch.zeros(len(b), dtype=torch.float64))
+    x = torch.zeros(len(b), dtype=torch.float64)
+    seen = []
+
+    def stop(i, r, rb):
+        seen.append(i)
+        return r < tol * rb
+    ok = g.solve(lambda v, Av: Av.copy_(At @ v), (lambda v, Mv: Mv.copy_(dinv * v)) if diag_prec else (lambda v, Mv: Mv.copy_(v)),
+                 lambda a, c: float(a @ c), torch.tensor(b, dtype=torch.float64), x, n_restart, stop)
+    return ok, x.numpy(), seen[-1]
+
+
+def test_gmres_reference_3x3_spd():
+    # test_Linear.cpp:44-71: GMRES(3), 10 restarts, stop at 1e-14, error below 1e-12
+    A = np.array([[4.0, 1, 0], [1, 3, 1], [0, 1, 2]])
+    b = np.array([1.0, 2, 3])
+    ok, x, _ = _gmres(A, b, 3, 10, 1e-14)
+    assert ok and np.linalg.norm(x - np.linalg.solve(A, b)) < 1e-12
+
+
+def test_gmres_reference_10x10_random_spd():
+    # test_Linear.cpp:73-98: A = R^T R + 10 I with R uniform in [-1, 1] (seeded here), GMRES(10), 20 restarts
+    R = np.random.default_rng(11).uniform(-1, 1, size=(10, 10))
+    A = R.T @ R + 10 * np.eye(10)
+    b = np.ones(10)
+    ok, x, _ = _gmres(A, b, 10, 20, 1e-12)
+    assert ok and np.linalg.norm(x - np.linalg.solve(A, b)) < 1e-10
+
+
+def test_gmres_reference_diagonal_preconditioner():
+    # test_Linear.cpp:100-150: diag (i + 1) 10 with A01 = A10 = 1, GMRES(3), 50 restarts; the diagonal
+    # preconditioner converges in no more restarts and to 1e-10
+    A = np.diag((np.arange(10) + 1) * 10.0)
+    A[0, 1] = A[1, 0] = 1.0
+    b = np.ones(10)
+    _, _, r_npc = _gmres(A, b, 3, 50, 1e-12)
+    ok, x, r_pc = _gmres(A, b, 3, 50, 1e-12, diag_prec=True)
+    assert np.linalg.norm(x - np.linalg.solve(A, b)) < 1e-10
+    assert r_pc <= r_npc
 
 
 @pytest.mark.parametrize("gmres", [0, 1])

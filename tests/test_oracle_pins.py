@@ -51,6 +51,47 @@ def test_riemann_symmetry(rs):
     np.testing.assert_allclose(F1, -F2, rtol=1e-10, atol=1e-10 * np.abs(F1).max())
 
 
+def _approx(a, b, eps):  # doctest's Approx: |a - b| < eps (1 + max(|a|, |b|))
+    return np.all(np.abs(a - b) < eps * (1 + np.maximum(np.abs(a), np.abs(b))))
+
+
+@pytest.mark.parametrize("rs", ["Roe", "HLLC", "HLLEP"])
+def test_riemann_sod_flux_finite_and_mass_flux_non_negative(rs):
+    # test_RiemannSolvers.cpp:188-238: Sod states (1, 0, 1) | (0.125, 0, 0.1) along x
+    F, _ = oracle.riemann(rs, _prim2cons(1.0, 0, 0, 0, 1.0), _prim2cons(0.125, 0, 0, 0, 0.1), np.array([1.0, 0, 0]))
+    assert np.all(np.isfinite(F)) and F[0] >= -1e-10
+
+
+def test_riemann_quiescent_gas_gives_the_pressure_flux():
+    # test_RiemannSolvers.cpp:297-313: rho = 1, v = 0, p = 1, every solver gives the exact flux to 1e-12
+    U = _prim2cons(1.0, 0, 0, 0, 1.0)
+    n = np.array([1.0, 0, 0])
+    for rs in ("Roe", "HLLC", "HLLEP"):
+        F, _ = oracle.riemann(rs, U, U, n)
+        assert _approx(F, _exact_flux(U, n), 1e-12), rs
+
+
+def test_roe_eigenvalue_output_subsonic():
+    # test_RiemannSolvers.cpp:319-336: |u - a|, |u|, |u + a| are non-negative and |u + a| >= |u|
+    _, lam = oracle.riemann("Roe", _prim2cons(1.0, 50.0, 0, 0, 100000.0), _prim2cons(1.1, 55.0, 0, 0, 105000.0), np.array([1.0, 0, 0]))
+    assert np.all(lam >= 0) and lam[2] >= lam[1]
+
+
+def test_roe_consistency_on_a_diagonal_normal():
+    # test_RiemannSolvers.cpp:342-357
+    U = _prim2cons(2.0, 100.0, 200.0, 300.0, 200000.0)
+    n = np.ones(3) / np.sqrt(3.0)
+    F, _ = oracle.riemann("Roe", U, U, n)
+    assert _approx(F, _exact_flux(U, n), 1e-8)
+
+
+def test_viscous_flux_of_a_zero_gradient_is_zero():
+    # test_GasThermo.cpp:479-494: mu 1.8e-5, k 0.025, Cp 1005, n = x
+    F = oracle.viscous_flux(_prim2cons(1.225, 100.0, -50.0, 25.0, 101325.0), np.zeros((3, 5)), np.array([1.0, 0, 0]), 1.4, 1.8e-5,
+                            0.025, 1005.0)
+    assert _approx(F, np.zeros(5), 1e-10)
+
+
 def _vr_error(n, p, hqm, f):
     m = M.periodic_quad_2d(n, L=10.0, jitter=0.0)
     vr = dict(maxOrder=p, intOrder=max(p + 2, 5), jacobiRelax=1.0, SORInstead=0, scaleType=1, scaleMultiplier=1.0,
