@@ -92,8 +92,8 @@ def test_viscous_flux_of_a_zero_gradient_is_zero():
     assert _approx(F, np.zeros(5), 1e-10)
 
 
-def _vr_error(n, p, hqm, f):
-    m = M.periodic_quad_2d(n, L=10.0, jitter=0.0)
+def _vr_error(n, p, hqm, f, mesh=None):
+    m = M.periodic_quad_2d(n, L=10.0, jitter=0.0) if mesh is None else mesh
     vr = dict(maxOrder=p, intOrder=max(p + 2, 5), jacobiRelax=1.0, SORInstead=0, scaleType=1, scaleMultiplier=1.0,
               dirWeightScheme=1 if hqm else 0, geomWeightScheme=1 if hqm else 0, geomWeightBias=1.0,
               geomWeightPower=0.5, bcWeight=1.0)
@@ -197,3 +197,29 @@ def test_update_lusgs_inplace_is_gauss_seidel():
         Ax = o.lusgs_matvec(1.0, u, x, jd)  # row c: sum_{o<c} w dF(x_o) (x_c = 0)
         ref[c] = (rhs[c] - Ax[c]) / jd[c]
     np.testing.assert_allclose(gs, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+
+
+_K3 = 2 * np.pi
+_FUNCS3 = {
+    "sinCos3D": lambda x: np.sin(_K3 * x[..., 0]) * np.cos(_K3 * x[..., 1]) * np.cos(_K3 * x[..., 2]),
+    "cosPlusCos3D": lambda x: np.cos(_K3 * x[..., 0]) + np.cos(_K3 * x[..., 1]) + np.cos(_K3 * x[..., 2]),
+}
+
+
+@pytest.fixture(scope="module")
+def uniform32_3d():
+    return M.periodic_hex_3d(32, L=1.0, jitter=0.0)
+
+
+@pytest.mark.parametrize("case", GOLD["vr_uniform32_3d"]["cases"], ids=lambda c: f"{c['func']}-p{c['p']}")
+def test_vr_uniform32_3d_golden(case, uniform32_3d):
+    # test_Reconstruction3D.cpp:394-407: VFV HQM (HQM_OPT / HQM_SD, power 0.5, bias 1), intOrder max(p + 2, 5),
+    # Jacobi sweeps to an RMS increment below 1e-14 or 200 sweeps, L1 error at the cell quadrature points / volume
+    err = _vr_error(None, case["p"], True, _FUNCS3[case["func"]], mesh=uniform32_3d)
+    assert abs(err - case["golden"]) <= GOLD["vr_uniform32_3d"]["rel_tol"] * case["golden"], err
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_vr_3d_constant_exactness(p, uniform32_3d):
+    # test_Reconstruction3D.cpp:347-366: a constant is reconstructed with an error below 1e-12
+    assert _vr_error(None, p, True, lambda x: np.ones(x.shape[:-1]), mesh=uniform32_3d) < 1e-12
