@@ -47,7 +47,7 @@ RHS_TRAFFIC_PER_CELL = 273.1e6 / 48 ** 3
 RHS_FP64_PIPE_PCT = 30.5  # sm__pipe_fp64_cycles_active of the same capture
 # algorithmic flops per cell (F_alg), counted by the op-counting build of the oracle on this workload
 # (python -m oracle.falg: +, -, *, / and sqrt one each; profiles/falg_tgv_p2.md)
-F_RHS = {2: 50067.0, 1: 30303.0}
+F_RHS = {2: 50310.0, 1: 30546.0}
 F_VR = {2: 6300.0, 1: 1020.0}
 # the reference's published TGV throughput for this path: 71.8 M cell-iterations/s on 10,240 CPU ranks
 REF_PUBLISHED_MCIPS = 71.8

@@ -83,9 +83,22 @@ _I = ctypes.POINTER(ctypes.c_int)
 _V = ctypes.c_void_p
 
 
+_I64 = ctypes.POINTER(ctypes.c_int64)
+
+
 def _optional_decls():
-    # entry points of the limiter and positivity restatements (the op-counting build leaves them out)
+    # entry points that the op-counting build leaves out (limiter, positivity, the reference unit-case surfaces of
+    # the limiter functions, eigenvectors, compression ratio, local LU and quadrature): name -> argtypes, or
+    # (argtypes, restype)
     return {
+        "orc_wbap_l2_biway": [ctypes.c_long, _D, _D, ctypes.c_double, _D],
+        "orc_wbap_l2_multiway": [ctypes.c_long, ctypes.c_int, _D, ctypes.c_double, _D],
+        "orc_pp_compression_ratio": ([_D, _D, ctypes.c_double, ctypes.POINTER(ctypes.c_int)], ctypes.c_double),
+        "orc_euler_eigen": [_D, ctypes.c_double, _D, _D],
+        "orc_block_ilu0": ([ctypes.c_int64, ctypes.c_int, ctypes.c_int, _I64, _D, _D, _D], ctypes.c_int),
+        "orc_block_ilu0_solve": [ctypes.c_int64, ctypes.c_int, ctypes.c_int, _I64, _D, _D, _D, _D],
+        "orc_quad_npoints": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "orc_quad_point": [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D],
         "orc_smooth_indicator": [_V, _D, _D, _D],
         "orc_limiter_wbap_c": [_V, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double],
         "orc_cell_rhs_alpha": [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
@@ -98,9 +111,13 @@ def _optional_decls():
 
 
 def _declare(L):
-    for name, args in _optional_decls().items():  # absent from the op-counting build
+    for name, decl in _optional_decls().items():  # absent from the op-counting build
         if hasattr(L, name):
-            getattr(L, name).argtypes = args
+            fn = getattr(L, name)
+            if isinstance(decl, tuple):
+                fn.argtypes, fn.restype = decl
+            else:
+                fn.argtypes = decl
     L.orc_create.restype = _V
     L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, _D, ctypes.c_long, ctypes.c_int, _L, _D,
                              ctypes.c_long, ctypes.c_int, _L, _D, _L, _I, _D, ctypes.c_int, _L,
@@ -122,17 +139,6 @@ def _declare(L):
     L.orc_lusgs_init.argtypes = [_V, _D, ctypes.c_double, ctypes.c_double, _D]
     L.orc_set_jacobian_mode.argtypes = [_V, ctypes.c_int]
     L.orc_vr_iter_sor.argtypes = [_V, _D, _D]
-    L.orc_wbap_l2_biway.argtypes = [ctypes.c_long, _D, _D, ctypes.c_double, _D]
-    L.orc_pp_compression_ratio.argtypes = [_D, _D, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
-    L.orc_euler_eigen.argtypes = [_D, ctypes.c_double, _D, _D]
-    L.orc_pp_compression_ratio.restype = ctypes.c_double
-    L.orc_wbap_l2_multiway.argtypes = [ctypes.c_long, ctypes.c_int, _D, ctypes.c_double, _D]
-    L.orc_block_ilu0.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), _D, _D, _D]
-    L.orc_block_ilu0.restype = ctypes.c_int
-    L.orc_block_ilu0_solve.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), _D, _D, _D, _D]
-    L.orc_quad_npoints.argtypes = [ctypes.c_int, ctypes.c_int]
-    L.orc_quad_npoints.restype = ctypes.c_int
-    L.orc_quad_point.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D]
     L.orc_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D]
     L.orc_jacobian_lu.restype = ctypes.c_int
     L.orc_solve_jacobian_lu.argtypes = [_V, ctypes.c_double, _D, _D, _D, _D, _D, ctypes.c_int, _D]
