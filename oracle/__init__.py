@@ -99,6 +99,7 @@ def _optional_decls():
         "orc_block_ilu0_solve": [ctypes.c_int64, ctypes.c_int, ctypes.c_int, _I64, _D, _D, _D, _D],
         "orc_quad_npoints": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "orc_quad_point": [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D],
+        "orc_shape": [ctypes.c_int, _D, _D, _D],
         "orc_smooth_indicator": [_V, _D, _D, _D],
         "orc_limiter_wbap_c": [_V, _D, _D, _D, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double],
         "orc_cell_rhs_alpha": [ctypes.c_long, ctypes.c_int, ctypes.c_double, _D, _D, _D, ctypes.c_double, ctypes.c_double,
@@ -228,6 +229,15 @@ def quad_rule(elem, order):
     for i in range(n):
         lib().orc_quad_point(e, order, i, _p(pts[i]), _p(w[i:i + 1]))
     return pts, w
+
+
+def shape(elem, p):
+    """The oracle's shape functions (Geom/Elements/*.hpp) of an element kind of QUAD_ELEM at a parametric point:
+    N [nNode], dN [3][nNode]."""
+    nn = dict(line=2, tri=3, quad=4, tet=4, hex=8)[elem]
+    N, dN = np.zeros(8), np.zeros((3, 8))
+    lib().orc_shape(QUAD_ELEM[elem], _p(_f64(np.asarray(p, float).reshape(3))), _p(N), _p(dN))
+    return N[:nn], dN[:, :nn]
 
 
 def block_ilu0(nbr, off, diag):

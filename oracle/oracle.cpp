@@ -4004,6 +4004,19 @@ extern "C"
             p[d] = pp[d];
         *w = ww;
     }
+    // the shape functions of Geom/Elements/{Line2,Tri3,Quad4,Tet4,Hex8}.hpp (elem as in orc_quad_point) at a
+    // parametric point: N [nNode], dN [3][8] (d/dxi, d/deta, d/dzeta by node)
+    void orc_shape(int elem, const double *p, double *N, double *dN)
+    {
+        real pp[3] = {p[0], p[1], p[2]}, Nv[8], dNv[3][8];
+        shapeD01(elem, pp, Nv, dNv);
+        for (int i = 0; i < elemNNode(elem); i++)
+        {
+            N[i] = Nv[i];
+            for (int d = 0; d < 3; d++)
+                dN[d * 8 + i] = dNv[d][i];
+        }
+    }
     // x = (L U)^-1 b with the factors of orc_block_ilu0
     void orc_block_ilu0_solve(int64_t n, int bs, int K, const int64_t *nbr, const double *off, const double *dinv, const double *b, double *x)
     {
